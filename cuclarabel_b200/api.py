@@ -1,0 +1,367 @@
+"""Python mirror of Clarabel's user API on top of libclgpu.
+
+``Solver(P, q, A, b, cones, settings)`` + ``solve()`` follow
+src/solver.jl:5-70 (constructor, dict cones) and :231-422 (solve!) of the
+CuClarabel tree; ``Settings`` carries the fields of src/settings.jl:70-148;
+statuses follow src/statuscodes.jl:24-36.  ``BatchSolver`` solves many
+independent problems in one lock-step device loop.
+"""
+import ctypes
+import enum
+from dataclasses import dataclass, field, fields
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+
+
+# ---------------------------------------------------------------- cones
+class SupportedCone:
+    code = -1
+
+    def spec(self):
+        raise NotImplementedError
+
+    def nvars(self):
+        raise NotImplementedError
+
+
+@dataclass(frozen=True)
+class ZeroConeT(SupportedCone):
+    dim: int
+    code = 0
+
+    def spec(self):
+        return (0, int(self.dim), 0.0)
+
+    def nvars(self):
+        return int(self.dim)
+
+
+@dataclass(frozen=True)
+class NonnegativeConeT(SupportedCone):
+    dim: int
+    code = 1
+
+    def spec(self):
+        return (1, int(self.dim), 0.0)
+
+    def nvars(self):
+        return int(self.dim)
+
+
+@dataclass(frozen=True)
+class SecondOrderConeT(SupportedCone):
+    dim: int
+    code = 2
+
+    def spec(self):
+        return (2, int(self.dim), 0.0)
+
+    def nvars(self):
+        return int(self.dim)
+
+
+@dataclass(frozen=True)
+class ExponentialConeT(SupportedCone):
+    code = 3
+
+    def spec(self):
+        return (3, 3, 0.0)
+
+    def nvars(self):
+        return 3
+
+
+@dataclass(frozen=True)
+class PowerConeT(SupportedCone):
+    alpha: float
+    code = 4
+
+    def spec(self):
+        return (4, 3, float(self.alpha))
+
+    def nvars(self):
+        return 3
+
+
+@dataclass(frozen=True)
+class PSDTriangleConeT(SupportedCone):
+    dim: int
+    code = 5
+
+    def spec(self):
+        return (5, int(self.dim), 0.0)
+
+    def nvars(self):
+        d = int(self.dim)
+        return d * (d + 1) // 2
+
+
+def cones_from_dict(cone):
+    """SCS-style dict -> cone list (src/solver.jl:35-70)."""
+    out = []
+    if "f" in cone:
+        out.append(ZeroConeT(cone["f"]))
+    if "l" in cone:
+        out.append(NonnegativeConeT(cone["l"]))
+    for d in cone.get("q", []):
+        out.append(SecondOrderConeT(d))
+    for d in cone.get("s", []):
+        out.append(PSDTriangleConeT(d))
+    for _ in range(cone.get("ep", 0)):
+        out.append(ExponentialConeT())
+    for a in cone.get("p", []):
+        out.append(PowerConeT(a))
+    return out
+
+
+class SolverStatus(enum.IntEnum):
+    UNSOLVED = 0
+    SOLVED = 1
+    PRIMAL_INFEASIBLE = 2
+    DUAL_INFEASIBLE = 3
+    ALMOST_SOLVED = 4
+    ALMOST_PRIMAL_INFEASIBLE = 5
+    ALMOST_DUAL_INFEASIBLE = 6
+    MAX_ITERATIONS = 7
+    MAX_TIME = 8
+    NUMERICAL_ERROR = 9
+    INSUFFICIENT_PROGRESS = 10
+
+
+_METHODS = {"cudss": 0, "gpu": 0, "fp64": 0, "cudssmixed": 1, "gpumixed": 1, "mixed": 1}
+
+
+@dataclass
+class Settings:
+    """Solver settings (src/settings.jl:70-148).  ``direct_solve_method``
+    accepts the reference names "cudss" (FP64 factorisation) and
+    "cudssmixed" (FP32 factorisation + FP64 iterative refinement); both run
+    this library's batched LDL^T."""
+    max_iter: int = 200
+    time_limit: float = float("inf")
+    verbose: bool = False
+    max_step_fraction: float = 0.99
+    tol_gap_abs: float = 1e-8
+    tol_gap_rel: float = 1e-8
+    tol_feas: float = 1e-8
+    tol_infeas_abs: float = 1e-8
+    tol_infeas_rel: float = 1e-8
+    tol_ktratio: float = 1e-6
+    reduced_tol_gap_abs: float = 5e-5
+    reduced_tol_gap_rel: float = 5e-5
+    reduced_tol_feas: float = 1e-4
+    reduced_tol_infeas_abs: float = 5e-12
+    reduced_tol_infeas_rel: float = 5e-5
+    reduced_tol_ktratio: float = 1e-4
+    equilibrate_enable: bool = True
+    equilibrate_max_iter: int = 10
+    equilibrate_min_scaling: float = 1e-4
+    equilibrate_max_scaling: float = 1e4
+    linesearch_backtrack_step: float = 0.8
+    min_switch_step_length: float = 1e-2
+    min_terminate_step_length: float = 1e-4
+    direct_kkt_solver: bool = True
+    direct_solve_method: str = "cudss"
+    static_regularization_enable: bool = True
+    static_regularization_constant: float = 1e-8
+    static_regularization_proportional: float = np.finfo(float).eps ** 2
+    dynamic_regularization_enable: bool = True
+    dynamic_regularization_eps: float = 1e-13
+    dynamic_regularization_delta: float = 2e-7
+    iterative_refinement_enable: bool = True
+    iterative_refinement_reltol: float = 1e-12
+    iterative_refinement_abstol: float = 1e-12
+    iterative_refinement_max_iter: int = 10
+    iterative_refinement_stop_ratio: float = 5.0
+    presolve_enable: bool = True
+    chordal_decomposition_enable: bool = True
+    soc_threshold: int = 5
+    setup_threads: int = 0
+
+    def to_c(self):
+        if self.direct_solve_method not in _METHODS:
+            raise ValueError("Unsupported direct LDL linear solver :%s" % self.direct_solve_method)
+        c = _lib.ClgpuSettings()
+        _lib.load().clgpu_default_settings(ctypes.byref(c))
+        for f, _ in _lib.ClgpuSettings._fields_:
+            if f == "direct_solve_method":
+                c.direct_solve_method = _METHODS[self.direct_solve_method]
+            elif hasattr(self, f):
+                v = getattr(self, f)
+                setattr(c, f, int(v) if isinstance(v, (bool, np.bool_)) else v)
+        return c
+
+
+def settings_from(settings=None, **kwargs):
+    s = Settings() if settings is None else settings
+    if isinstance(s, dict):
+        kwargs = {**s, **kwargs}
+        s = Settings()
+    names = {f.name for f in fields(Settings)}
+    for k, v in kwargs.items():
+        if k not in names:
+            raise TypeError("unknown setting %r" % k)
+        setattr(s, k, v)
+    return s
+
+
+@dataclass
+class DefaultSolution:
+    """src/types.jl DefaultSolution."""
+    x: np.ndarray
+    z: np.ndarray
+    s: np.ndarray
+    status: SolverStatus
+    obj_val: float
+    obj_val_dual: float
+    solve_time: float
+    iterations: int
+    r_prim: float
+    r_dual: float
+    info: dict = field(default_factory=dict)
+
+
+def _prep_problem(P, q, A, b, cones):
+    q = np.ascontiguousarray(q, dtype=np.float64).ravel()
+    b = np.ascontiguousarray(b, dtype=np.float64).ravel()
+    n, m = len(q), len(b)
+    if isinstance(cones, dict):
+        cones = cones_from_dict(cones)
+    cones = list(cones)
+    P = sp.csc_matrix(P) if P is not None else sp.csc_matrix((n, n))
+    A = sp.csc_matrix(A) if A is not None else sp.csc_matrix((m, n))
+    # _check_dimensions (src/solver.jl:199-211)
+    if A.shape[0] != m:
+        raise ValueError("A and b incompatible dimensions.")
+    if sum(c.nvars() for c in cones) != m:
+        raise ValueError("Constraint dimensions inconsistent with size of cones.")
+    if A.shape[1] != n:
+        raise ValueError("A and q incompatible dimensions.")
+    if P.shape[0] != n:
+        raise ValueError("P and q incompatible dimensions.")
+    if P.shape[0] != P.shape[1]:
+        raise ValueError("P not square.")
+    P = sp.triu(P, format="csc")
+    P.sum_duplicates()
+    P.sort_indices()
+    A.sum_duplicates()
+    A.sort_indices()
+    specs = [c.spec() for c in cones]
+    keep = dict(
+        Pp=np.ascontiguousarray(P.indptr, np.int32), Pi=np.ascontiguousarray(P.indices, np.int32),
+        Px=np.ascontiguousarray(P.data, np.float64), q=q,
+        Ap=np.ascontiguousarray(A.indptr, np.int32), Ai=np.ascontiguousarray(A.indices, np.int32),
+        Ax=np.ascontiguousarray(A.data, np.float64), b=b,
+        ct=np.array([s[0] for s in specs] or [0], np.int32),
+        cd=np.array([s[1] for s in specs] or [0], np.int32),
+        cp=np.array([s[2] for s in specs] or [0.0], np.float64))
+    cp = _lib.ClgpuProblem()
+    cp.n, cp.m = n, m
+
+    def D(a):
+        return a.ctypes.data_as(_lib.dp)
+
+    def I(a):
+        return a.ctypes.data_as(_lib.ip)
+    cp.Pp, cp.Pi, cp.Px, cp.q = I(keep["Pp"]), I(keep["Pi"]), D(keep["Px"]), D(q)
+    cp.Ap, cp.Ai, cp.Ax, cp.b = I(keep["Ap"]), I(keep["Ai"]), D(keep["Ax"]), D(b)
+    cp.ncones = len(specs)
+    cp.cone_types, cp.cone_dims, cp.cone_params = I(keep["ct"]), I(keep["cd"]), D(keep["cp"])
+    return cp, keep, n, m
+
+
+class BatchSolver:
+    """Many independent problems solved in one lock-step device loop."""
+
+    def __init__(self, problems, settings=None, **kwargs):
+        self.settings = settings_from(settings, **kwargs)
+        L = _lib.load()
+        arr = (_lib.ClgpuProblem * len(problems))()
+        self._keep = []
+        self.dims = []
+        for k, pb in enumerate(problems):
+            cp, keep, n, m = _prep_problem(*pb)
+            arr[k] = cp
+            self._keep.append(keep)
+            self.dims.append((n, m))
+        cs = self.settings.to_c()
+        h = ctypes.c_void_p()
+        rc = L.clgpu_solver_create(arr, len(problems), ctypes.byref(cs), ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_create failed with code %d" % rc)
+        self._h = h
+        self._keep = None  # host arrays are copied by the library
+        self.nx = sum(d[0] for d in self.dims)
+        self.mz = sum(d[1] for d in self.dims)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.load().clgpu_solver_destroy(h)
+            self._h = None
+
+    def solve(self, stream=0):
+        L = _lib.load()
+        rc = L.clgpu_solver_solve(self._h, ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_solve failed with code %d" % rc)
+        return self.solutions()
+
+    def solutions(self):
+        L = _lib.load()
+        B = len(self.dims)
+        x = np.zeros(max(self.nx, 1))
+        s = np.zeros(max(self.mz, 1))
+        z = np.zeros(max(self.mz, 1))
+        infos = (_lib.ClgpuInfo * B)()
+        rc = L.clgpu_solver_get_solutions(self._h, x.ctypes.data_as(_lib.dp),
+                                          s.ctypes.data_as(_lib.dp), z.ctypes.data_as(_lib.dp),
+                                          infos)
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_get_solutions failed with code %d" % rc)
+        out = []
+        xo = mo = 0
+        for k, (n, m) in enumerate(self.dims):
+            inf = infos[k]
+            d = {f: getattr(inf, f) for f, _ in _lib.ClgpuInfo._fields_}
+            out.append(DefaultSolution(
+                x=x[xo:xo + n].copy(), z=z[mo:mo + m].copy(), s=s[mo:mo + m].copy(),
+                status=SolverStatus(inf.status), obj_val=inf.obj_val,
+                obj_val_dual=inf.obj_val_dual, solve_time=inf.solve_time,
+                iterations=inf.iterations, r_prim=inf.res_primal, r_dual=inf.res_dual,
+                info=d))
+            xo += n
+            mo += m
+        return out
+
+    def device_bytes(self):
+        return _lib.load().clgpu_solver_device_bytes(self._h)
+
+    def launch_count(self):
+        return _lib.load().clgpu_solver_launch_count(self._h)
+
+    def profile(self):
+        vals = [ctypes.c_double() for _ in range(5)]
+        passes = ctypes.c_int()
+        _lib.load().clgpu_solver_get_profile(self._h, *[ctypes.byref(v) for v in vals],
+                                             ctypes.byref(passes))
+        return dict(ms_total=vals[0].value, passes=passes.value)
+
+
+class Solver(BatchSolver):
+    """Clarabel.Solver(P, q, A, b, cones, settings) for one problem."""
+
+    def __init__(self, P, q, A, b, cones, settings=None, **kwargs):
+        super().__init__([(P, q, A, b, cones)], settings, **kwargs)
+        self.solution = None
+
+    def solve(self, stream=0):
+        self.solution = super().solve(stream)[0]
+        return self.solution
+
+    @property
+    def info(self):
+        return None if self.solution is None else self.solution.info

@@ -1,0 +1,1799 @@
+// cones.cu -- per-cone kernels for sm_100a.
+//
+// Reference behaviour followed (CuClarabel tree):
+//   nonnegative  src/gpucones/coneops_nncone_gpu.jl (CPU twin src/cones/coneops_nncone.jl)
+//   second-order src/gpucones/coneops_socone_gpu.jl (CPU twin coneops_socone.jl:372-814)
+//   exponential  src/gpucones/coneops_expcone_gpu.jl (CPU twin coneops_expcone.jl)
+//   power        src/gpucones/coneops_powcone_gpu.jl (CPU twin coneops_powcone.jl)
+//   nonsym share src/gpucones/coneops_nonsymmetric_common_gpu.jl
+//   PSD triangle src/gpucones/coneops_psdtrianglecone_gpu.jl (CPU twin coneops_psdtrianglecone.jl)
+//
+// Mapping to the hardware (not a translation of the reference's one thread
+// per cone):
+//   * nonnegative rows: one thread per row over a contiguous type-major range
+//     (coalesced FP64 streams);
+//   * second-order cones: a group of G lanes per cone (G = next power of two
+//     of the largest cone dim, <= 32), elements strided across the group,
+//     norms/dots by shuffle reductions inside the group;
+//   * exponential/power cones: one thread per cone (FP64 transcendental work);
+//   * PSD cones: one warp per cone with its n x n matrices in shared memory
+//     (Cholesky, one-sided Jacobi SVD, Jacobi eigenvalues, small GEMMs).  The
+//     t x t Hs block is never stored: the KKT refresh evaluates the symmetric
+//     Kronecker product entries from R R^T on the fly.
+#include <cstdio>
+
+#include "cones.cuh"
+
+namespace clgpu {
+
+static constexpr int kBlock = 256;
+static constexpr int kPsdWarps = 2;  // warps (cones) per PSD block
+
+__device__ __forceinline__ bool active_inst(const ConeSet &cs, int inst) {
+  return cs.inst_active == nullptr || cs.inst_active[inst] != 0;
+}
+
+// =================================================================== NN
+__global__ void k_nn_update_scaling(ConeSet cs, const double *__restrict__ s,
+                                    const double *__restrict__ z) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  int g = cs.nn_begin + e;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  double si = s[g], zi = z[g];
+  cs.nn_lambda[e] = sqrt(si * zi);
+  cs.nn_w[e] = sqrt(si / zi);
+}
+
+// =================================================================== SOC
+// group helpers --------------------------------------------------------
+template <int G>
+struct SocCtx {
+  int c, lane, off, dim, inst;
+  bool valid;
+  __device__ SocCtx(const ConeSet &cs) {
+    int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    lane = threadIdx.x & (G - 1);
+    valid = gid < cs.n_soc;
+    c = valid ? gid : cs.n_soc - 1;
+    off = cs.soc_off[c];
+    dim = cs.soc_dim[c];
+    inst = cs.soc_inst[c];
+    if (valid && !active_inst(cs, inst)) valid = false;
+  }
+};
+#define SOC_FOR(i) for (int i = ctx.lane; i < ctx.dim; i += G)
+
+template <int G>
+__device__ __forceinline__ double soc_tail_sq(const double *x, const SocCtx<G> &ctx) {
+  double t = 0;
+  SOC_FOR(i) if (i > 0) t += x[i] * x[i];
+  return group_sum<G>(t);
+}
+template <int G>
+__device__ __forceinline__ double soc_tail_dot(const double *x, const double *y,
+                                               const SocCtx<G> &ctx) {
+  double t = 0;
+  SOC_FOR(i) if (i > 0) t += x[i] * y[i];
+  return group_sum<G>(t);
+}
+// (x0 - |x1|)(x0 + |x1|), coneops_socone.jl:716-720
+__device__ __forceinline__ double soc_res(double x0, double x1sq) {
+  double n1 = sqrt(x1sq);
+  return (x0 - n1) * (x0 + n1);
+}
+
+// coneops_socone.jl:372-451 (and the sparse d/u/v of
+// coneops_socone_gpu.jl:338-470, kept unscaled as on the CPU side)
+template <int G>
+__global__ void k_soc_update_scaling(ConeSet cs, const double *__restrict__ s_,
+                                     const double *__restrict__ z_, int *scale_ok) {
+  SocCtx<G> ctx(cs);
+  const double *s = s_ + ctx.off, *z = z_ + ctx.off;
+  int r = ctx.off - cs.soc_begin;
+  double *w = cs.soc_w + r, *lam = cs.soc_lambda + r;
+  double s0 = s[0], z0 = z[0];
+  double zs = soc_res(z0, soc_tail_sq<G>(z, ctx));
+  double ss = soc_res(s0, soc_tail_sq<G>(s, ctx));
+  double zscale = zs > 0.0 ? sqrt(zs) : 0.0;
+  double sscale = ss > 0.0 ? sqrt(ss) : 0.0;
+  bool fail = (zscale == 0.0 || sscale == 0.0);
+  if (fail) {
+    if (ctx.valid && ctx.lane == 0) scale_ok[ctx.inst] = 0;
+    zscale = sscale = 1.0;  // keep lanes in lock step; results discarded
+  }
+  double eta = sqrt(sscale / zscale);
+  // w = s/sscale + (z0, -z1)/zscale
+  double wl[4];  // per-lane cache (dim <= 4*G handled in registers)
+  int k = 0;
+  double w1sq_a = 0;
+  SOC_FOR(i) {
+    double wi = s[i] / sscale + (i == 0 ? z[i] : -z[i]) / zscale;
+    if (k < 4) wl[k] = wi;
+    ++k;
+    if (i > 0) w1sq_a += wi * wi;
+  }
+  double w0pre = s0 / sscale + z0 / zscale;
+  double wres = soc_res(w0pre, group_sum<G>(w1sq_a));
+  double wscale = wres > 0.0 ? sqrt(wres) : 0.0;
+  if (wscale == 0.0) {
+    if (ctx.valid && ctx.lane == 0) scale_ok[ctx.inst] = 0;
+    fail = true;
+    wscale = 1.0;
+  }
+  double w1sq = 0;
+  k = 0;
+  SOC_FOR(i) {
+    double wi = (k < 4 ? wl[k] : (s[i] / sscale + (i == 0 ? z[i] : -z[i]) / zscale)) / wscale;
+    if (k < 4) wl[k] = wi;
+    ++k;
+    if (i > 0) w1sq += wi * wi;
+  }
+  w1sq = group_sum<G>(w1sq);
+  double w0 = sqrt(1 + w1sq);
+  double gamma = 0.5 * wscale;
+  double c1 = (gamma + z0 / zscale) / sscale;
+  double c2 = (gamma + s0 / sscale) / zscale;
+  double inv = 1.0 / (s0 / sscale + z0 / zscale + 2 * gamma);
+  double sc = sqrt(sscale * zscale);
+  bool sparse = cs.soc_sparse[ctx.c] != 0;
+  double u0 = 0, u1 = 0, v1 = 0, dd = 0;
+  if (sparse) {
+    double wsq = w0 * w0 + w1sq;
+    double wsqinv = 1 / wsq;
+    dd = wsqinv / 2;
+    u0 = sqrt(wsq - dd);
+    u1 = 2 * w0 / u0;
+    v1 = sqrt(2 * (2 + wsqinv) / (2 * wsq - wsqinv));
+  }
+  if (!ctx.valid || fail) return;
+  k = 0;
+  SOC_FOR(i) {
+    double wi = (k < 4) ? wl[k]
+                        : (s[i] / sscale + (i == 0 ? z[i] : -z[i]) / zscale) / wscale;
+    ++k;
+    if (i == 0) {
+      w[0] = w0;
+      lam[0] = gamma * sc;
+      if (sparse) {
+        cs.soc_u[r] = u0;
+        cs.soc_v[r] = 0.0;
+      }
+    } else {
+      w[i] = wi;
+      lam[i] = ((c1 * s[i] + c2 * z[i]) * inv) * sc;
+      if (sparse) {
+        cs.soc_u[r + i] = u1 * wi;
+        cs.soc_v[r + i] = v1 * wi;
+      }
+    }
+  }
+  if (ctx.lane == 0) {
+    cs.soc_eta[ctx.c] = eta;
+    if (sparse) cs.soc_d[ctx.c] = dd;
+  }
+}
+
+// =============================================================== exp / pow
+struct M3 {
+  double a[9];  // column-major
+  __device__ double &operator()(int i, int j) { return a[i + 3 * j]; }
+  __device__ double operator()(int i, int j) const { return a[i + 3 * j]; }
+};
+
+// coneops_expcone.jl:655-711 (Wright omega; the third Taylor term keeps the
+// reference's unassigned "q * zinv" statement)
+__device__ double wright_omega(double z) {
+  if (z < 0) return CUDART_INF;
+  double w;
+  if (z < 1.0 + 3.141592653589793) {
+    double zm1 = z - 1.0, p = zm1;
+    w = 1 + 0.5 * p;
+    p *= zm1;
+    w += (1 / 16.0) * p;
+    p *= zm1;
+    w -= (1 / 192.0) * p;
+    p *= zm1;
+    w -= (1 / 3072.0) * p;
+    p *= zm1;
+    w += (13 / 61440.0) * p;
+  } else {
+    double logz = logsafe(z), zinv = 1.0 / z;
+    w = z - logz;
+    double q = logz * zinv;
+    w += q;
+    q *= zinv;
+    w += q * (logz / 2 - 1.0);
+    w += q * (logz * logz / 3. - (3 / 2.) * logz + 1.0);
+  }
+  double r = z - w - logsafe(w);
+  for (int i = 0; i < 2; ++i) {
+    double wp1 = w + 1.0;
+    double t = wp1 * (wp1 + (2. * r) / 3.0);
+    w *= 1 + (r / wp1) * (t - 0.5 * r) / (t - r);
+    double wp2 = wp1 * wp1, wp6 = wp2 * wp2 * wp2;
+    r = (2 * w * w - 8 * w - 1) / (72.0 * wp6) * r * r * r * r;
+  }
+  return w;
+}
+
+struct ExpOps {
+  __device__ static void grad_primal(const double *s, double *g, double) {
+    double o = wright_omega(1 - s[0] / s[1] - logsafe(s[1] / s[2]));
+    g[0] = 1.0 / ((o - 1.0) * s[1]);
+    g[1] = g[0] + g[0] * logsafe(o * s[1] / s[2]) - 1.0 / s[1];
+    g[2] = o / ((1.0 - o) * s[2]);
+  }
+  __device__ static void dual_grad_H(const double *z, double *grad, M3 &H, double) {
+    double l = logsafe(-z[2] / z[0]);
+    double r = -z[0] * l - z[0] + z[1];
+    double c2 = 1.0 / r;
+    grad[0] = c2 * l - 1 / z[0];
+    grad[1] = -c2;
+    grad[2] = (c2 * z[0] - 1) / z[2];
+    H(0, 0) = ((r * r - z[0] * r + l * l * z[0] * z[0]) / (r * z[0] * z[0] * r));
+    H(0, 1) = (-l / (r * r));
+    H(1, 0) = H(0, 1);
+    H(1, 1) = (1 / (r * r));
+    H(0, 2) = ((z[1] - z[0]) / (r * r * z[2]));
+    H(2, 0) = H(0, 2);
+    H(1, 2) = (-z[0] / (r * r * z[2]));
+    H(2, 1) = H(1, 2);
+    H(2, 2) = ((r * r - z[0] * r + z[0] * z[0]) / (r * r * z[2] * z[2]));
+  }
+  __device__ static bool primal_feasible(const double *s, double) {
+    if (s[2] > 0 && s[1] > 0) {
+      double res = s[1] * logsafe(s[2] / s[1]) - s[0];
+      if (res > 0) return true;
+    }
+    return false;
+  }
+  __device__ static bool dual_feasible(const double *z, double) {
+    if (z[2] > 0 && z[0] < 0) {
+      double res = z[1] - z[0] - z[0] * logsafe(-z[2] / z[0]);
+      if (res > 0) return true;
+    }
+    return false;
+  }
+  __device__ static double barrier_dual(const double *z, double) {
+    double l = logsafe(-z[2] / z[0]);
+    return -logsafe(-z[2] * z[0]) - logsafe(z[1] - z[0] - z[0] * l);
+  }
+  __device__ static double barrier_primal(const double *s, double) {
+    double o = wright_omega(1 - s[0] / s[1] - logsafe(s[1] / s[2]));
+    o = (o - 1) * (o - 1) / o;
+    return -logsafe(o) - 2 * logsafe(s[1]) - logsafe(s[2]) - 3;
+  }
+  // coneops_expcone.jl:530-577
+  __device__ static void higher_correction(const M3 &Hd, const double *z,
+                                           const double *u, const double *v,
+                                           double *eta, double) {
+    eta[1] = 1.0;
+    eta[2] = -z[0] / z[2];
+    eta[0] = logsafe(eta[2]);
+    double psi = z[0] * eta[0] - z[0] + z[1];
+    double dotpu = eta[0] * u[0] + eta[1] * u[1] + eta[2] * u[2];
+    double dotpv = eta[0] * v[0] + eta[1] * v[1] + eta[2] * v[2];
+    double coef = ((u[0] * (v[0] / z[0] - v[2] / z[2]) +
+                    u[2] * (z[0] * v[2] / z[2] - v[0]) / z[2]) * psi -
+                   2 * dotpu * dotpv) / (psi * psi * psi);
+    for (int i = 0; i < 3; ++i) eta[i] *= coef;
+    double ip2 = 1.0 / psi / psi;
+    eta[0] += (1 / psi - 2 / z[0]) * u[0] * v[0] / (z[0] * z[0]) -
+              u[2] * v[2] / (z[2] * z[2]) / psi +
+              dotpu * ip2 * (v[0] / z[0] - v[2] / z[2]) +
+              dotpv * ip2 * (u[0] / z[0] - u[2] / z[2]);
+    eta[2] += 2 * (z[0] / psi - 1) * u[2] * v[2] / (z[2] * z[2] * z[2]) -
+              (u[2] * v[0] + u[0] * v[2]) / (z[2] * z[2]) / psi +
+              dotpu * ip2 * (z[0] * v[2] / (z[2] * z[2]) - v[0] / z[2]) +
+              dotpv * ip2 * (z[0] * u[2] / (z[2] * z[2]) - u[0] / z[2]);
+    for (int i = 0; i < 3; ++i) eta[i] /= 2;
+    (void)Hd;
+  }
+  __device__ static void unit_init(double *s, double) {
+    s[0] = -1.051383945322714;
+    s[1] = 0.556409619469370;
+    s[2] = 1.258967884768947;
+  }
+};
+
+// coneops_powcone.jl:449-478 restated (Newton-Raphson from the left)
+__device__ double pow_nr(double s3, double phi, double a) {
+  double x0 = -1.0 / s3 + (2 * s3 + sqrt(phi * phi / s3 / s3 + 3 * phi)) / (phi - s3 * s3);
+  double t0 = -2 * a * logsafe(a) - 2 * (1 - a) * logsafe(1 - a);
+  double x = x0;
+  for (int iter = 0; iter < 100; ++iter) {
+    double t1 = x * x, t2 = x * 2 / s3;
+    double dfdx = 2 * a * a / (a * x + (1 + a) / s3) +
+                  2 * (1 - a) * (1 - a) / ((1 - a) * x + (2 - a) / s3) -
+                  2 * (x + 1 / s3) / (t1 + t2);
+    t2 = 2 * x / s3;
+    double f0 = 2 * a * logsafe(2 * a * t1 + (1 + a) * t2) +
+                2 * (1 - a) * logsafe(2 * (1 - a) * t1 + (2 - a) * t2) -
+                logsafe(phi) - logsafe(t1 + t2) - 2 * logsafe(t2) + t0;
+    double dx = -f0 / dfdx;
+    if (dx < kDEps || fabs(dx / x) < sqrt(kDEps) || fabs(dfdx) < kDEps) break;
+    x += dx;
+  }
+  return x;
+}
+
+struct PowOps {
+  __device__ static void grad_primal(const double *s, double *g, double a) {
+    double phi = pow(s[0], 2 * a) * pow(s[1], 2 - 2 * a);
+    double abs_s = fabs(s[2]);
+    if (abs_s > kDEps) {
+      g[2] = pow_nr(abs_s, phi, a);
+      if (s[2] < 0) g[2] = -g[2];
+      g[0] = -(a * g[2] * s[2] + 1 + a) / s[0];
+      g[1] = -((1 - a) * g[2] * s[2] + 2 - a) / s[1];
+    } else {
+      g[2] = 0;
+      g[0] = -(1 + a) / s[0];
+      g[1] = -(2 - a) / s[1];
+    }
+  }
+  // coneops_powcone.jl:408-440
+  __device__ static void dual_grad_H(const double *z, double *grad, M3 &H, double a) {
+    double phi = pow(z[0] / a, 2 * a) * pow(z[1] / (1 - a), 2 - 2 * a);
+    double psi = phi - z[2] * z[2];
+    double g0 = 2 * a * phi / (z[0] * psi);
+    double g1 = 2 * (1 - a) * phi / (z[1] * psi);
+    double g2 = -2 * z[2] / psi;
+    H(0, 0) = g0 * g0 - 2 * a * (2 * a - 1) * phi / (z[0] * z[0] * psi) + (1 - a) / (z[0] * z[0]);
+    H(0, 1) = g0 * g1 - 4 * a * (1 - a) * phi / (z[0] * z[1] * psi);
+    H(1, 0) = H(0, 1);
+    H(1, 1) = g1 * g1 - 2 * (1 - a) * (1 - 2 * a) * phi / (z[1] * z[1] * psi) + a / (z[1] * z[1]);
+    H(0, 2) = g0 * g2;
+    H(2, 0) = H(0, 2);
+    H(1, 2) = g1 * g2;
+    H(2, 1) = H(1, 2);
+    H(2, 2) = g2 * g2 + 2 / psi;
+    grad[0] = -2 * a * phi / (z[0] * psi) - (1 - a) / z[0];
+    grad[1] = -2 * (1 - a) * phi / (z[1] * psi) - a / z[1];
+    grad[2] = 2 * z[2] / psi;
+  }
+  __device__ static bool primal_feasible(const double *s, double a) {
+    if (s[0] > 0 && s[1] > 0) {
+      double res = exp(2 * a * logsafe(s[0]) + 2 * (1 - a) * logsafe(s[1])) - s[2] * s[2];
+      if (res > 0) return true;
+    }
+    return false;
+  }
+  __device__ static bool dual_feasible(const double *z, double a) {
+    if (z[0] > 0 && z[1] > 0) {
+      double res = exp(2 * a * logsafe(z[0] / a) + 2 * (1 - a) * logsafe(z[1] / (1 - a))) -
+                   z[2] * z[2];
+      if (res > 0) return true;
+    }
+    return false;
+  }
+  __device__ static double barrier_dual(const double *z, double a) {
+    return -logsafe(pow(z[0] / a, 2 * a) * pow(z[1] / (1 - a), 2 - 2 * a) - z[2] * z[2]) -
+           (1 - a) * logsafe(z[0]) - a * logsafe(z[1]);
+  }
+  __device__ static double barrier_primal(const double *s, double a) {
+    double g[3];
+    grad_primal(s, g, a);
+    return logsafe(pow(-g[0] / a, 2 * a) * pow(-g[1] / (1 - a), 2 - 2 * a) - g[2] * g[2]) +
+           (1 - a) * logsafe(-g[0]) + a * logsafe(-g[1]) - 3;
+  }
+  // coneops_powcone.jl:329-404
+  __device__ static void higher_correction(const M3 &Hd, const double *z,
+                                           const double *u, const double *v,
+                                           double *eta, double a) {
+    double phi = pow(z[0] / a, 2 * a) * pow(z[1] / (1 - a), 2 - 2 * a);
+    double psi = phi - z[2] * z[2];
+    eta[0] = 2 * a * phi / z[0];
+    eta[1] = 2 * (1 - a) * phi / z[1];
+    eta[2] = -2 * z[2];
+    double H11 = 2 * a * (2 * a - 1) * phi / (z[0] * z[0]);
+    double H12 = 4 * a * (1 - a) * phi / (z[0] * z[1]);
+    double H22 = 2 * (1 - a) * (1 - 2 * a) * phi / (z[1] * z[1]);
+    double dotpu = eta[0] * u[0] + eta[1] * u[1] + eta[2] * u[2];
+    double dotpv = eta[0] * v[0] + eta[1] * v[1] + eta[2] * v[2];
+    double Hv0 = H11 * v[0] + H12 * v[1], Hv1 = H12 * v[0] + H22 * v[1], Hv2 = -2 * v[2];
+    double coef = ((u[0] * Hv0 + u[1] * Hv1 + u[2] * Hv2) * psi - 2 * dotpu * dotpv) /
+                  (psi * psi * psi);
+    double coef2 = 4 * a * (2 * a - 1) * (1 - a) * phi * (u[0] / z[0] - u[1] / z[1]) *
+                   (v[0] / z[0] - v[1] / z[1]) / psi;
+    double ip2 = 1 / psi / psi;
+    eta[0] = coef * eta[0] - 2 * (1 - a) * u[0] * v[0] / (z[0] * z[0] * z[0]) +
+             coef2 / z[0] + Hv0 * dotpu * ip2;
+    eta[1] = coef * eta[1] - 2 * a * u[1] * v[1] / (z[1] * z[1] * z[1]) -
+             coef2 / z[1] + Hv1 * dotpu * ip2;
+    eta[2] = coef * eta[2] + Hv2 * dotpu * ip2;
+    double Hu0 = H11 * u[0] + H12 * u[1], Hu1 = H12 * u[0] + H22 * u[1], Hu2 = -2 * u[2];
+    eta[0] = (eta[0] + Hu0 * dotpv * ip2) / 2;
+    eta[1] = (eta[1] + Hu1 * dotpv * ip2) / 2;
+    eta[2] = (eta[2] + Hu2 * dotpv * ip2) / 2;
+    (void)Hd;
+  }
+  __device__ static void unit_init(double *s, double a) {
+    s[0] = sqrt(1.0 + a);
+    s[1] = sqrt(1.0 + (1.0 - a));
+    s[2] = 0.0;
+  }
+};
+
+// mathutils.jl:381-420
+__device__ bool chol3(const M3 &A, M3 &L) {
+  for (int i = 0; i < 9; ++i) L.a[i] = 0;
+  double t = A(0, 0);
+  if (t <= 0) return false;
+  L(0, 0) = sqrt(t);
+  L(1, 0) = A(1, 0) / L(0, 0);
+  t = A(1, 1) - L(1, 0) * L(1, 0);
+  if (t <= 0) return false;
+  L(1, 1) = sqrt(t);
+  L(2, 0) = A(2, 0) / L(0, 0);
+  L(2, 1) = (A(2, 1) - L(1, 0) * L(2, 0)) / L(1, 1);
+  t = A(2, 2) - L(2, 0) * L(2, 0) - L(2, 1) * L(2, 1);
+  if (t <= 0) return false;
+  L(2, 2) = sqrt(t);
+  return true;
+}
+__device__ void chol3_solve(const M3 &L, const double *b, double *x) {
+  double L11 = L(0, 0), L21 = L(1, 0), L31 = L(2, 0), L22 = L(1, 1), L32 = L(2, 1), L33 = L(2, 2);
+  double c1 = b[0] / L11;
+  double c2 = (b[1] * L11 - b[0] * L21) / (L11 * L22);
+  double c3 = (b[2] * L11 * L22 - b[1] * L11 * L32 + b[0] * L21 * L32 - b[0] * L22 * L31) /
+              (L11 * L22 * L33);
+  x[0] = (c1 * L22 * L33 - c2 * L21 * L33 + c3 * L21 * L32 - c3 * L22 * L31) / (L11 * L22 * L33);
+  x[1] = (c2 * L33 - c3 * L32) / (L22 * L33);
+  x[2] = c3 / L33;
+}
+
+template <class Ops>
+struct NonsymArgs {
+  int n, begin;
+  const int *inst;
+  const double *alpha;  // pow only
+  double *Hd, *Hs, *grad, *zs;
+};
+
+// coneops_nonsymmetric_common.jl:50-164 (dual and primal-dual scalings)
+template <class Ops>
+__global__ void k_nonsym_update_scaling(ConeSet cs, NonsymArgs<Ops> a,
+                                        const double *__restrict__ s_,
+                                        const double *__restrict__ z_,
+                                        const double *mu_, const int *scaling) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n) return;
+  int inst = a.inst[c];
+  if (!active_inst(cs, inst)) return;
+  double pa = a.alpha ? a.alpha[c] : 0.0;
+  const double *s = s_ + a.begin + 3 * c, *z = z_ + a.begin + 3 * c;
+  double sv[3] = {s[0], s[1], s[2]}, zv[3] = {z[0], z[1], z[2]};
+  double grad[3];
+  M3 Hd, Hs;
+  Ops::dual_grad_H(zv, grad, Hd, pa);
+  double mu = mu_[inst];
+  bool dual = scaling[inst] == 1;
+  bool used_pd = false;
+  if (!dual) {
+    const double *st = grad;
+    double zt[3];
+    Ops::grad_primal(sv, zt, pa);
+    double dot_sz = zv[0] * sv[0] + zv[1] * sv[1] + zv[2] * sv[2];
+    double mu_l = dot_sz / 3;
+    double mut = (zt[0] * st[0] + zt[1] * st[1] + zt[2] * st[2]) / 3;
+    double ds[3], dz[3];
+    for (int i = 0; i < 3; ++i) {
+      ds[i] = sv[i] + mu_l * st[i];
+      dz[i] = zv[i] + mu_l * zt[i];
+    }
+    double dot_dsz = ds[0] * dz[0] + ds[1] * dz[1] + ds[2] * dz[2];
+    double de1 = mu_l * mut - 1;
+    double Hz[3];
+    for (int i = 0; i < 3; ++i) Hz[i] = Hd(i, 0) * zt[0] + Hd(i, 1) * zt[1] + Hd(i, 2) * zt[2];
+    double de2 = zt[0] * Hz[0] + zt[1] * Hz[1] + zt[2] * Hz[2] - 3 * mut * mut;
+    if (fabs(de1) > sqrt(kDEps) && fabs(de2) > kDEps && dot_sz > 0 && dot_dsz > 0) {
+      double tmp[3];
+      for (int i = 0; i < 3; ++i) tmp[i] = mut * st[i] - Hz[i];
+      for (int i = 0; i < 9; ++i) Hs.a[i] = Hd.a[i];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Hs(i, j) -= st[i] * st[j] / 3 + tmp[i] * tmp[j] / de2;
+      double fro = 0;
+      for (int i = 0; i < 9; ++i) fro += Hs.a[i] * Hs.a[i];
+      double t = mu_l * sqrt(fro);
+      double ax[3] = {zv[1] * zt[2] - zv[2] * zt[1], zv[2] * zt[0] - zv[0] * zt[2],
+                      zv[0] * zt[1] - zv[1] * zt[0]};
+      double an = sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+      for (int i = 0; i < 3; ++i) ax[i] /= an;
+      for (int i = 0; i < 3; ++i)
+        for (int j = i; j < 3; ++j)
+          Hs(i, j) = sv[i] * sv[j] / dot_sz + ds[i] * ds[j] / dot_dsz + t * ax[i] * ax[j];
+      Hs(1, 0) = Hs(0, 1);
+      Hs(2, 0) = Hs(0, 2);
+      Hs(2, 1) = Hs(1, 2);
+      used_pd = true;
+    } else {
+      mu = mu_l;  // central-path fallback uses the local mu
+    }
+  }
+  if (!used_pd)
+    for (int i = 0; i < 9; ++i) Hs.a[i] = mu * Hd.a[i];
+  for (int i = 0; i < 9; ++i) {
+    a.Hd[9 * c + i] = Hd.a[i];
+    a.Hs[9 * c + i] = Hs.a[i];
+  }
+  for (int i = 0; i < 3; ++i) {
+    a.grad[3 * c + i] = grad[i];
+    a.zs[3 * c + i] = zv[i];
+  }
+}
+
+// =================================================================== PSD
+// Warp-per-cone helpers on column-major n x n matrices in shared memory.
+struct PsdCtx {
+  int c, lane, n, t, off, inst;
+  bool valid;
+};
+
+__device__ __forceinline__ void svec_to_mat(int n, const double *x, double *M, int lane) {
+  const double is2 = 0.70710678118654752440;  // 1/sqrt(2)
+  int t = n * (n + 1) / 2;
+  for (int k = lane; k < t; k += 32) {
+    int col = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+    while ((col + 1) * (col + 2) / 2 <= k) ++col;
+    while (col * (col + 1) / 2 > k) --col;
+    int row = k - col * (col + 1) / 2;
+    double v = x[k];
+    if (row == col)
+      M[row + n * col] = v;
+    else {
+      M[row + n * col] = v * is2;
+      M[col + n * row] = v * is2;
+    }
+  }
+}
+__device__ __forceinline__ void mat_to_svec(int n, const double *M, double *x, int lane) {
+  const double is2 = 0.70710678118654752440;
+  int t = n * (n + 1) / 2;
+  for (int k = lane; k < t; k += 32) {
+    int col = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+    while ((col + 1) * (col + 2) / 2 <= k) ++col;
+    while (col * (col + 1) / 2 > k) --col;
+    int row = k - col * (col + 1) / 2;
+    x[k] = row == col ? M[row + n * col] : (M[row + n * col] + M[col + n * row]) * is2;
+  }
+}
+// C = op(A) * op(B)   (n x n), ta/tb: transpose flags
+__device__ void mm(int n, const double *A, bool ta, const double *B, bool tb, double *C,
+                   int lane) {
+  for (int e = lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n;
+    double t = 0;
+    for (int k = 0; k < n; ++k) {
+      double a = ta ? A[k + n * i] : A[i + n * k];
+      double b = tb ? B[j + n * k] : B[k + n * j];
+      t += a * b;
+    }
+    C[e] = t;
+  }
+  __syncwarp();
+}
+// in-place lower Cholesky; returns false if not positive definite
+__device__ bool warp_chol(int n, double *A, int lane) {
+  bool ok = true;
+  for (int j = 0; j < n; ++j) {
+    double d = A[j + n * j];
+    for (int k = 0; k < j; ++k) d -= A[j + n * k] * A[j + n * k];
+    if (!(d > 0)) ok = false;
+    d = ok ? sqrt(d) : 1.0;
+    __syncwarp();
+    for (int i = j + 1 + lane; i < n; i += 32) {
+      double t = A[i + n * j];
+      for (int k = 0; k < j; ++k) t -= A[i + n * k] * A[j + n * k];
+      A[i + n * j] = t / d;
+    }
+    if (lane == 0) A[j + n * j] = d;
+    for (int i = lane; i < j; i += 32) A[i + n * j] = 0;
+    __syncwarp();
+  }
+  return ok;
+}
+// one-sided Jacobi SVD: M = U diag(S) V^T; S descending.  M overwritten by U.
+__device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, int lane) {
+  for (int e = lane; e < n * n; e += 32) V[e] = (e % n == e / n) ? 1.0 : 0.0;
+  __syncwarp();
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    int rotated = 0;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double a = 0, b = 0, g = 0;
+        if (lane < n) {
+          double mp = M[lane + n * p], mq = M[lane + n * q];
+          a = mp * mp;
+          b = mq * mq;
+          g = mp * mq;
+        }
+        a = warp_sum(a);
+        b = warp_sum(b);
+        g = warp_sum(g);
+        if (fabs(g) <= 1e-15 * sqrt(a * b) || g == 0) continue;
+        rotated = 1;
+        double zeta = (b - a) / (2 * g);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
+        double cs = 1 / sqrt(1 + t * t), sn = cs * t;
+        if (lane < n) {
+          double mp = M[lane + n * p], mq = M[lane + n * q];
+          M[lane + n * p] = cs * mp - sn * mq;
+          M[lane + n * q] = sn * mp + cs * mq;
+          double vp = V[lane + n * p], vq = V[lane + n * q];
+          V[lane + n * p] = cs * vp - sn * vq;
+          V[lane + n * q] = sn * vp + cs * vq;
+        }
+        __syncwarp();
+      }
+    if (!rotated) break;
+  }
+  // column norms, sort descending (selection on lane 0 into tmp perm)
+  if (lane < n) {
+    double t = 0;
+    for (int k = 0; k < n; ++k) t += M[k + n * lane] * M[k + n * lane];
+    S[lane] = sqrt(t);
+  }
+  __syncwarp();
+  int *perm = reinterpret_cast<int *>(tmp + n * n);
+  if (lane == 0) {
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j)
+        if (S[perm[j]] > S[perm[i]]) {
+          int x = perm[i];
+          perm[i] = perm[j];
+          perm[j] = x;
+        }
+  }
+  __syncwarp();
+  // tmp <- U (sorted), M <- V (sorted) via copies
+  for (int e = lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n, pj = perm[j];
+    double sj = S[pj];
+    tmp[e] = sj > 0 ? M[i + n * pj] / sj : 0.0;
+  }
+  __syncwarp();
+  for (int e = lane; e < n * n; e += 32) M[e] = tmp[e];
+  __syncwarp();
+  for (int e = lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n;
+    tmp[e] = V[i + n * perm[j]];
+  }
+  double sl = lane < n ? S[perm[lane]] : 0.0;
+  __syncwarp();
+  for (int e = lane; e < n * n; e += 32) V[e] = tmp[e];
+  if (lane < n) S[lane] = sl;
+  __syncwarp();
+}
+// cyclic Jacobi eigenvalues of symmetric A (destroyed); returns min eigenvalue,
+// and if ev != null writes all eigenvalues.
+__device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0, tot = 0;
+    for (int e = lane; e < n * n; e += 32) {
+      double a = A[e] * A[e];
+      tot += a;
+      if (e % n != e / n) off += a;
+    }
+    off = warp_sum(off);
+    tot = warp_sum(tot);
+    if (off <= 1e-30 * tot || off == 0) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = A[p + n * q];
+        if (apq == 0) continue;
+        double app = A[p + n * p], aqq = A[q + n * q];
+        double theta = (aqq - app) / (2 * apq);
+        double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+        double c = 1 / sqrt(t * t + 1), s = t * c;
+        __syncwarp();
+        if (lane < n) {
+          double akp = A[lane + n * p], akq = A[lane + n * q];
+          A[lane + n * p] = c * akp - s * akq;
+          A[lane + n * q] = s * akp + c * akq;
+        }
+        __syncwarp();
+        if (lane < n) {
+          double apk = A[p + n * lane], aqk = A[q + n * lane];
+          A[p + n * lane] = c * apk - s * aqk;
+          A[q + n * lane] = s * apk + c * aqk;
+        }
+        __syncwarp();
+      }
+  }
+  double v = lane < n ? A[lane + n * lane] : CUDART_INF;
+  if (ev && lane < n) ev[lane] = v;
+  __syncwarp();
+  return warp_min(v);
+}
+
+__device__ __forceinline__ PsdCtx psd_ctx(const ConeSet &cs) {
+  PsdCtx p;
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  p.lane = threadIdx.x & 31;
+  p.valid = w < cs.n_psd;
+  p.c = p.valid ? w : cs.n_psd - 1;
+  p.n = cs.psd_n[p.c];
+  p.t = p.n * (p.n + 1) / 2;
+  p.off = cs.psd_off[p.c];
+  p.inst = cs.psd_inst[p.c];
+  if (p.valid && !active_inst(cs, p.inst)) p.valid = false;
+  return p;
+}
+__device__ __forceinline__ double *psd_smem(int nmax, int nmats) {
+  extern __shared__ double smem[];
+  int wib = threadIdx.x >> 5;
+  return smem + (size_t)wib * nmats * nmax * nmax;
+}
+
+// coneops_psdtrianglecone.jl:79-142
+__global__ void k_psd_update_scaling(ConeSet cs, const double *__restrict__ s,
+                                     const double *__restrict__ z, int *scale_ok) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;  // whole warp shares p.valid
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *L1 = psd_smem(nm, 7), *L2 = L1 + nn, *M = L2 + nn, *V = M + nn,
+         *T = V + nn, *S = T + 2 * nn;
+  for (int e = p.lane; e < n * n; e += 32) L1[e] = L2[e] = 0;
+  __syncwarp();
+  svec_to_mat(n, s + p.off, L1, p.lane);
+  svec_to_mat(n, z + p.off, L2, p.lane);
+  __syncwarp();
+  bool ok1 = warp_chol(n, L1, p.lane);
+  bool ok2 = warp_chol(n, L2, p.lane);
+  if (!(ok1 && ok2)) {
+    if (p.lane == 0) scale_ok[p.inst] = 0;
+    return;
+  }
+  mm(n, L2, true, L1, false, M, p.lane);  // M = L2' L1
+  warp_svd(n, M, V, S, T, p.lane);        // M <- U
+  double *R = cs.psd_R + (size_t)p.c * nn, *Ri = cs.psd_Rinv + (size_t)p.c * nn;
+  double *lam = cs.psd_lam + (size_t)p.c * nm;
+  // R = L1 V Lis ; Rinv = Lis U' L2'
+  for (int e = p.lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n;
+    double t = 0, u = 0;
+    for (int k = 0; k < n; ++k) {
+      t += L1[i + n * k] * V[k + n * j];
+      u += M[k + n * i] * L2[j + n * k];
+    }
+    R[e] = t * (1.0 / sqrt(S[j]));
+    Ri[e] = (1.0 / sqrt(S[i])) * u;
+  }
+  if (p.lane < n) lam[p.lane] = S[p.lane];
+}
+
+// y = a*op(Rx)... helper: Y = Rx' X Rx (trans=false) or Rx X Rx' (trans=true)
+__device__ void psd_wmul(int n, const double *Rx, bool trans, const double *X, double *Y,
+                         double *T, int lane) {
+  if (trans) {
+    mm(n, X, false, Rx, true, T, lane);   // T = X Rx'
+    mm(n, Rx, false, T, false, Y, lane);  // Y = Rx T
+  } else {
+    mm(n, Rx, true, X, false, T, lane);   // T = Rx' X
+    mm(n, T, false, Rx, false, Y, lane);  // Y = T Rx
+  }
+}
+
+// ================================================================ refresh
+// SOC dense Hs entry (row r <= col c), coneops_socone.jl:453-490
+__device__ __forceinline__ double soc_dense_hs(const double *w, int r, int c, double e2) {
+  double v;
+  if (r == 0 && c == 0) {
+    const double s2 = 1.4142135623730951;
+    v = (s2 * w[0] - 1.0) * (s2 * w[0] + 1.0);
+  } else {
+    v = 2 * w[r] * w[c];
+    if (r == c) v += 1.0;
+  }
+  return v * e2;
+}
+// symmetric Kronecker entry of A (x)_s A at svec (row=(i,j), col=(k,l)),
+// coneops_psdtrianglecone.jl:509-547
+__device__ __forceinline__ double skron_entry(const double *A, int n, int i, int j, int k,
+                                              int l) {
+  const double sqrt2 = 1.4142135623730951;
+  bool ij = (i == j), kl = (k == l);
+  double Ajl = A[j + n * l], Ajk = A[j + n * k];
+  if (!ij && !kl) return A[i + n * k] * Ajl + A[i + n * l] * Ajk;
+  if (ij && !kl) return sqrt2 * Ajl * Ajk;
+  if (!ij && kl) return sqrt2 * A[i + n * l] * Ajk;
+  return Ajl * Ajl;
+}
+__device__ __forceinline__ void tri_coord(int k, int &row, int &col) {
+  col = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+  while ((col + 1) * (col + 2) / 2 <= k) ++col;
+  while (col * (col + 1) / 2 > k) --col;
+  row = k - col * (col + 1) / 2;
+}
+
+__global__ void k_nn_refresh(ConeSet cs, const int *__restrict__ pos, double *kv) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  if (!active_inst(cs, cs.row_inst[cs.nn_begin + e])) return;
+  double w = cs.nn_w[e];
+  kv[pos[e]] = -(w * w);
+}
+
+template <int G>
+__global__ void k_soc_refresh(ConeSet cs, KKTMapDev map, double *kv) {
+  SocCtx<G> ctx(cs);
+  if (!ctx.valid) return;
+  int r = ctx.off - cs.soc_begin;
+  const double *w = cs.soc_w + r;
+  double eta = cs.soc_eta[ctx.c], e2 = eta * eta;
+  if (cs.soc_sparse[ctx.c]) {
+    double d = cs.soc_d[ctx.c];
+    SOC_FOR(i) {
+      double hd = (i == 0) ? e2 * d : e2;
+      kv[map.socs_diag[r + i]] = -hd;
+      const int *uv = map.socs_uv + 4 * (size_t)(r + i);
+      double vv = -e2 * cs.soc_v[r + i], uu = -e2 * cs.soc_u[r + i];
+      kv[uv[0]] = vv;
+      kv[uv[1]] = vv;
+      kv[uv[2]] = uu;
+      kv[uv[3]] = uu;
+    }
+    if (ctx.lane == 0) {
+      kv[map.socs_D[2 * ctx.c]] = -e2;
+      kv[map.socs_D[2 * ctx.c + 1]] = e2;
+    }
+  } else {
+    int t = ctx.dim * (ctx.dim + 1) / 2;
+    const int *pp = map.socd_pos + 2 * (size_t)map.socd_off[ctx.c];
+    for (int k = ctx.lane; k < t; k += G) {
+      int row, col;
+      tri_coord(k, row, col);
+      double v = -soc_dense_hs(w, row, col, e2);
+      kv[pp[2 * k]] = v;
+      if (pp[2 * k + 1] >= 0) kv[pp[2 * k + 1]] = v;
+    }
+  }
+}
+
+__global__ void k_nonsym_refresh(ConeSet cs, int nc, const int *inst, const double *Hs,
+                                 const int *pos, double *kv) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  if (!active_inst(cs, inst[c])) return;
+  const double *H = Hs + 9 * c;
+  // triu entries in pack order: (0,0),(0,1),(1,1),(0,2),(1,2),(2,2)
+  const int ri[6] = {0, 0, 1, 0, 1, 2}, ci[6] = {0, 1, 1, 2, 2, 2};
+  for (int k = 0; k < 6; ++k) {
+    double v = -H[ri[k] + 3 * ci[k]];
+    kv[pos[12 * c + 2 * k]] = v;
+    int q = pos[12 * c + 2 * k + 1];
+    if (q >= 0) kv[q] = v;
+  }
+}
+
+__global__ void k_psd_refresh(ConeSet cs, KKTMapDev map, double *kv) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *A = psd_smem(nm, 1);
+  const double *R = cs.psd_R + (size_t)p.c * nn;
+  mm(n, R, false, R, true, A, p.lane);  // A = R R'
+  int tt = p.t * (p.t + 1) / 2;
+  const int *pp = map.psd_pos + 2 * (size_t)map.psd_off[p.c];
+  for (int e = p.lane; e < tt; e += 32) {
+    int row, col;
+    tri_coord(e, row, col);  // svec indices (row <= col)
+    int i, j, k, l;
+    tri_coord(row, i, j);
+    tri_coord(col, k, l);
+    double v = -skron_entry(A, n, i, j, k, l);
+    kv[pp[2 * e]] = v;
+    if (pp[2 * e + 1] >= 0) kv[pp[2 * e + 1]] = v;
+  }
+}
+
+// get_Hs! into reference-layout blocks (used by the cone-level ABI only)
+__global__ void k_nn_get_hs(ConeSet cs, const int *blk, double *Hs) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  double w = cs.nn_w[e];
+  Hs[blk[e]] = w * w;
+}
+template <int G>
+__global__ void k_soc_get_hs(ConeSet cs, const int *blk, double *Hs) {
+  SocCtx<G> ctx(cs);
+  if (!ctx.valid) return;
+  int r = ctx.off - cs.soc_begin;
+  const double *w = cs.soc_w + r;
+  double eta = cs.soc_eta[ctx.c], e2 = eta * eta;
+  double *out = Hs + blk[ctx.c];
+  if (cs.soc_sparse[ctx.c]) {
+    SOC_FOR(i) out[i] = (i == 0) ? e2 * cs.soc_d[ctx.c] : e2;
+  } else {
+    int t = ctx.dim * (ctx.dim + 1) / 2;
+    for (int k = ctx.lane; k < t; k += G) {
+      int row, col;
+      tri_coord(k, row, col);
+      out[k] = soc_dense_hs(w, row, col, e2);
+    }
+  }
+}
+__global__ void k_nonsym_get_hs(int nc, const double *Hsd, const int *blk, double *Hs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double *H = Hsd + 9 * c;
+  double *o = Hs + blk[c];
+  o[0] = H[0];
+  o[1] = H[3];
+  o[2] = H[4];
+  o[3] = H[6];
+  o[4] = H[7];
+  o[5] = H[8];
+}
+__global__ void k_psd_get_hs(ConeSet cs, const int *blk, double *Hs) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *A = psd_smem(nm, 1);
+  const double *R = cs.psd_R + (size_t)p.c * nn;
+  mm(n, R, false, R, true, A, p.lane);
+  int tt = p.t * (p.t + 1) / 2;
+  double *o = Hs + blk[p.c];
+  for (int e = p.lane; e < tt; e += 32) {
+    int row, col, i, j, k, l;
+    tri_coord(e, row, col);
+    tri_coord(row, i, j);
+    tri_coord(col, k, l);
+    o[e] = skron_entry(A, n, i, j, k, l);
+  }
+}
+
+// ================================================================= mul_Hs
+__global__ void k_zero_fill(ConeSet cs, double *y) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_zero) return;
+  int g = cs.zero_begin + e;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  y[g] = 0.0;
+}
+__global__ void k_nn_mul_hs(ConeSet cs, double *y, const double *__restrict__ x) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  int g = cs.nn_begin + e;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  double w = cs.nn_w[e];
+  y[g] = w * (w * x[g]);
+}
+template <int G>
+__global__ void k_soc_mul_hs(ConeSet cs, double *y_, const double *__restrict__ x_) {
+  SocCtx<G> ctx(cs);
+  int r = ctx.off - cs.soc_begin;
+  const double *w = cs.soc_w + r, *x = x_ + ctx.off;
+  double t = 0;
+  SOC_FOR(i) t += w[i] * x[i];
+  double c = 2 * group_sum<G>(t);
+  if (!ctx.valid) return;
+  double eta = cs.soc_eta[ctx.c], e2 = eta * eta;
+  double *y = y_ + ctx.off;
+  SOC_FOR(i) {
+    double v = (i == 0) ? -x[0] : x[i];
+    y[i] = (v + c * w[i]) * e2;
+  }
+}
+__global__ void k_nonsym_mul_hs(ConeSet cs, int nc, int begin, const int *inst,
+                                const double *Hs, double *y, const double *x) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  if (!active_inst(cs, inst[c])) return;
+  const double *H = Hs + 9 * c;
+  const double *xv = x + begin + 3 * c;
+  double x0 = xv[0], x1 = xv[1], x2 = xv[2];
+  double *yv = y + begin + 3 * c;
+  for (int i = 0; i < 3; ++i) yv[i] = H[i] * x0 + H[i + 3] * x1 + H[i + 6] * x2;
+}
+__global__ void k_psd_mul_hs(ConeSet cs, double *y, const double *__restrict__ x) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *X = psd_smem(nm, 3), *Y = X + nn, *T = Y + nn;
+  const double *R = cs.psd_R + (size_t)p.c * nn;
+  svec_to_mat(n, x + p.off, X, p.lane);
+  __syncwarp();
+  psd_wmul(n, R, false, X, Y, T, p.lane);  // Y = R' X R   (W x)
+  mat_to_svec(n, Y, T, p.lane);            // svec round trip of W x
+  __syncwarp();
+  svec_to_mat(n, T, Y, p.lane);
+  __syncwarp();
+  psd_wmul(n, R, true, Y, X, T, p.lane);   // X = R Y R'   (W^T W x)
+  mat_to_svec(n, X, y + p.off, p.lane);
+}
+
+// ============================================================== affine_ds
+__global__ void k_nn_affine_ds(ConeSet cs, double *ds) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  int g = cs.nn_begin + e;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  double l = cs.nn_lambda[e];
+  ds[g] = l * l;
+}
+template <int G>
+__global__ void k_soc_affine_ds(ConeSet cs, double *ds_) {
+  SocCtx<G> ctx(cs);
+  int r = ctx.off - cs.soc_begin;
+  const double *l = cs.soc_lambda + r;
+  double t = 0;
+  SOC_FOR(i) t += l[i] * l[i];
+  t = group_sum<G>(t);
+  if (!ctx.valid) return;
+  double *ds = ds_ + ctx.off;
+  double l0 = l[0];
+  SOC_FOR(i) ds[i] = (i == 0) ? t : (l0 * l[i] + l0 * l[i]);
+}
+__global__ void k_nonsym_copy(ConeSet cs, int nc, int begin, const int *inst, double *dst,
+                              const double *src) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * nc) return;
+  if (!active_inst(cs, inst[e / 3])) return;
+  dst[begin + e] = src[begin + e];
+}
+__global__ void k_psd_affine_ds(ConeSet cs, double *ds) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  const double *lam = cs.psd_lam + (size_t)p.c * cs.psd_nmax;
+  for (int k = p.lane; k < p.t; k += 32) {
+    int row, col;
+    tri_coord(k, row, col);
+    ds[p.off + k] = (row == col) ? lam[row] * lam[row] : 0.0;
+  }
+}
+
+// ======================================================= combined_ds_shift
+// symmetric cones: shift = (W^{-T} ds) o (W dz) - sigma*mu*e
+// (coneops_defaults.jl:335-368); step_z/step_s are not written back.
+__global__ void k_nn_combined(ConeSet cs, double *shift, const double *__restrict__ dz,
+                              const double *__restrict__ ds, const double *sm) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  int g = cs.nn_begin + e;
+  int inst = cs.row_inst[g];
+  if (!active_inst(cs, inst)) return;
+  double w = cs.nn_w[e];
+  double wz = dz[g] * w, ws = ds[g] / w;
+  shift[g] = ws * wz - sm[inst];
+}
+template <int G>
+__global__ void k_soc_combined(ConeSet cs, double *shift_, const double *__restrict__ dz_,
+                               const double *__restrict__ ds_, const double *sm) {
+  SocCtx<G> ctx(cs);
+  int r = ctx.off - cs.soc_begin;
+  const double *w = cs.soc_w + r, *dz = dz_ + ctx.off, *ds = ds_ + ctx.off;
+  double eta = cs.soc_eta[ctx.c], w0 = w[0];
+  double zz = soc_tail_dot<G>(w, dz, ctx);
+  double zs = soc_tail_dot<G>(w, ds, ctx);
+  double cz = dz[0] + zz / (1 + w0);
+  double csn = -ds[0] + zs / (1 + w0);
+  // Wz and Ws elements, then circ
+  double wz0 = eta * (w0 * dz[0] + zz);
+  double ws0 = (1 / eta) * (w0 * ds[0] - zs);
+  double dot = 0;
+  SOC_FOR(i) {
+    double a = (i == 0) ? wz0 : eta * (dz[i] + cz * w[i]);
+    double b = (i == 0) ? ws0 : (1 / eta) * (ds[i] + csn * w[i]);
+    dot += a * b;
+  }
+  dot = group_sum<G>(dot);
+  if (!ctx.valid) return;
+  double *sh = shift_ + ctx.off;
+  double smv = sm[ctx.inst];
+  SOC_FOR(i) {
+    if (i == 0) {
+      sh[0] = dot - smv;
+    } else {
+      double a = eta * (dz[i] + cz * w[i]);
+      double b = (1 / eta) * (ds[i] + csn * w[i]);
+      sh[i] = ws0 * a + wz0 * b;
+    }
+  }
+}
+// asymmetric: shift = grad*sigma*mu - eta(3rd order correction)
+template <class Ops>
+__global__ void k_nonsym_combined(ConeSet cs, NonsymArgs<Ops> a, double *shift,
+                                  const double *__restrict__ dz,
+                                  const double *__restrict__ ds, const double *sm) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n) return;
+  int inst = a.inst[c];
+  if (!active_inst(cs, inst)) return;
+  double pa = a.alpha ? a.alpha[c] : 0.0;
+  M3 Hd, L;
+  for (int i = 0; i < 9; ++i) Hd.a[i] = a.Hd[9 * c + i];
+  const double *zs = a.zs + 3 * c;
+  double z[3] = {zs[0], zs[1], zs[2]};
+  int b = a.begin + 3 * c;
+  double v[3] = {dz[b], dz[b + 1], dz[b + 2]};
+  double dsv[3] = {ds[b], ds[b + 1], ds[b + 2]};
+  double eta[3] = {0, 0, 0};
+  if (chol3(Hd, L)) {
+    double u[3];
+    chol3_solve(L, dsv, u);
+    Ops::higher_correction(Hd, z, u, v, eta, pa);
+  }
+  double smv = sm[inst];
+  for (int i = 0; i < 3; ++i) shift[b + i] = a.grad[3 * c + i] * smv - eta[i];
+}
+__global__ void k_psd_combined(ConeSet cs, double *shift, const double *__restrict__ dz,
+                               const double *__restrict__ ds, const double *sm) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *X = psd_smem(nm, 5), *Z = X + nn, *S = Z + nn, *T = S + nn, *Y = T + nn;
+  const double *R = cs.psd_R + (size_t)p.c * nn, *Ri = cs.psd_Rinv + (size_t)p.c * nn;
+  for (int e = p.lane; e < n * n; e += 32) X[e] = 0;
+  __syncwarp();
+  svec_to_mat(n, dz + p.off, X, p.lane);
+  __syncwarp();
+  psd_wmul(n, R, false, X, Z, T, p.lane);  // Z = R' dZ R   (W dz)
+  svec_to_mat(n, ds + p.off, X, p.lane);
+  __syncwarp();
+  psd_wmul(n, Ri, true, X, S, T, p.lane);  // S = Ri dS Ri'  (W^{-T} ds)
+  // svec round trip (the reference stores W dz and W^{-T} ds as svec)
+  mat_to_svec(n, Z, Y, p.lane);
+  __syncwarp();
+  svec_to_mat(n, Y, Z, p.lane);
+  mat_to_svec(n, S, Y, p.lane);
+  __syncwarp();
+  svec_to_mat(n, Y, S, p.lane);
+  __syncwarp();
+  // X = (S Z + Z S)/2
+  for (int e = p.lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n;
+    double t = 0;
+    for (int k = 0; k < n; ++k) t += S[i + n * k] * Z[k + n * j] + Z[i + n * k] * S[k + n * j];
+    X[e] = 0.5 * t;
+  }
+  __syncwarp();
+  double smv = sm[p.inst];
+  double *out = shift + p.off;
+  mat_to_svec(n, X, out, p.lane);
+  __syncwarp();
+  for (int k = p.lane; k < n; k += 32) out[(k + 1) * (k + 2) / 2 - 1] -= smv;
+}
+
+// ===================================================== ds_from_dz_offset
+__global__ void k_nn_ds_offset(ConeSet cs, double *out, const double *__restrict__ ds,
+                               const double *__restrict__ z) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  int g = cs.nn_begin + e;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  out[g] = ds[g] / z[g];
+}
+// coneops_socone.jl:539-566
+template <int G>
+__global__ void k_soc_ds_offset(ConeSet cs, double *out_, const double *__restrict__ ds_,
+                                const double *__restrict__ z_) {
+  SocCtx<G> ctx(cs);
+  int r = ctx.off - cs.soc_begin;
+  const double *w = cs.soc_w + r, *l = cs.soc_lambda + r, *ds = ds_ + ctx.off,
+               *z = z_ + ctx.off;
+  double resz = soc_res(z[0], soc_tail_sq<G>(z, ctx));
+  double l1ds1 = soc_tail_dot<G>(l, ds, ctx);
+  double w1ds1 = soc_tail_dot<G>(w, ds, ctx);
+  if (!ctx.valid) return;
+  double eta = cs.soc_eta[ctx.c];
+  double c = l[0] * ds[0] - l1ds1;
+  double il = 1 / l[0];
+  double *out = out_ + ctx.off;
+  SOC_FOR(i) {
+    double o;
+    if (i == 0) {
+      o = z[0] * (c / resz);
+      o += eta * w1ds1;
+    } else {
+      o = -z[i] * (c / resz);
+      o += eta * (ds[i] + w1ds1 / (1 + w[0]) * w[i]);
+    }
+    out[i] = o * il;
+  }
+}
+__global__ void k_psd_ds_offset(ConeSet cs, double *out, const double *__restrict__ ds) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *X = psd_smem(nm, 4), *Z = X + nn, *T = Z + nn, *Y = T + nn;
+  const double *R = cs.psd_R + (size_t)p.c * nn;
+  const double *lam = cs.psd_lam + (size_t)p.c * nm;
+  svec_to_mat(n, ds + p.off, Z, p.lane);
+  __syncwarp();
+  for (int e = p.lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n;
+    X[e] = 2 * Z[e] / (lam[i] + lam[j]);
+  }
+  __syncwarp();
+  // work stored as svec then re-expanded (as the reference does)
+  mat_to_svec(n, X, Y, p.lane);
+  __syncwarp();
+  svec_to_mat(n, Y, X, p.lane);
+  __syncwarp();
+  psd_wmul(n, R, true, X, Z, T, p.lane);  // Z = R X R'
+  mat_to_svec(n, Z, out + p.off, p.lane);
+}
+
+// ============================================================ step length
+__global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
+                          const double *__restrict__ ds, const double *__restrict__ z,
+                          const double *__restrict__ s, double *alpha) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double a = CUDART_INF;
+  if (e < cs.n_nn) {
+    int g = cs.nn_begin + e;
+    inst = cs.row_inst[g];
+    if (active_inst(cs, inst)) {
+      double dzi = dz[g], dsi = ds[g];
+      if (dzi < 0) a = fmin(a, -z[g] / dzi);
+      if (dsi < 0) a = fmin(a, -s[g] / dsi);
+      if (a == CUDART_INF) inst = -1;
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_min_nonneg(alpha, inst, a);
+}
+
+// coneops_socone.jl:745-814 with group reductions
+template <int G>
+__device__ double soc_step_component(const double *x, const double *y, double amax,
+                                     const SocCtx<G> &ctx) {
+  double x0 = x[0], y0 = y[0];
+  double ysq = soc_tail_sq<G>(y, ctx);
+  double xsq = soc_tail_sq<G>(x, ctx);
+  double xy = soc_tail_dot<G>(x, y, ctx);
+  if (x0 >= 0 && y0 < 0) amax = fmin(amax, -x0 / y0);
+  double a = soc_res(y0, ysq);
+  double b = 2 * (x0 * y0 - xy);
+  double c = fmax(0.0, soc_res(x0, xsq));
+  double d = b * b - 4 * a * c;
+  if ((a > 0 && b > 0) || d < 0) return amax;
+  if (a == 0) return amax;
+  if (c == 0) return a >= 0 ? amax : 0.0;
+  double t = (b >= 0) ? (-b - sqrt(d)) : (-b + sqrt(d));
+  double r1 = (2 * c) / t, r2 = t / (2 * a);
+  r1 = r1 < 0 ? kDMax : r1;
+  r2 = r2 < 0 ? kDMax : r2;
+  return fmin(amax, fmin(r1, r2));
+}
+template <int G>
+__global__ void k_soc_step(ConeSet cs, const double *__restrict__ dz,
+                           const double *__restrict__ ds, const double *__restrict__ z,
+                           const double *__restrict__ s, double *alpha) {
+  SocCtx<G> ctx(cs);
+  double amax = alpha[ctx.inst];  // upper bound already there (atomic min target)
+  double az = soc_step_component<G>(z + ctx.off, dz + ctx.off, amax, ctx);
+  double as = soc_step_component<G>(s + ctx.off, ds + ctx.off, amax, ctx);
+  if (ctx.valid && ctx.lane == 0) atomic_min_nonneg(alpha + ctx.inst, fmin(az, as));
+}
+__global__ void k_psd_step(ConeSet cs, const double *__restrict__ dz,
+                           const double *__restrict__ ds, double *alpha) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
+  double *X = psd_smem(nm, 4), *Y = X + nn, *T = Y + nn, *V = T + nn;
+  const double *R = cs.psd_R + (size_t)p.c * nn, *Ri = cs.psd_Rinv + (size_t)p.c * nn;
+  const double *lam = cs.psd_lam + (size_t)p.c * nm;
+  double amax = alpha[p.inst];
+  double res = amax;
+  for (int side = 0; side < 2; ++side) {
+    svec_to_mat(n, (side == 0 ? dz : ds) + p.off, X, p.lane);
+    __syncwarp();
+    if (side == 0)
+      psd_wmul(n, R, false, X, Y, T, p.lane);  // W dz = R' dZ R
+    else
+      psd_wmul(n, Ri, true, X, Y, T, p.lane);  // W^{-T} ds = Ri dS Ri'
+    // svec round trip then scale by Lis both sides
+    mat_to_svec(n, Y, V, p.lane);
+    __syncwarp();
+    svec_to_mat(n, V, Y, p.lane);
+    __syncwarp();
+    for (int e = p.lane; e < n * n; e += 32) {
+      int i = e % n, j = e / n;
+      Y[e] *= (1.0 / sqrt(lam[i])) * (1.0 / sqrt(lam[j]));
+    }
+    __syncwarp();
+    double gmin = warp_eig_min(n, Y, nullptr, p.lane);
+    double a = gmin < 0 ? fmin(1.0 / (-gmin), amax) : amax;
+    res = fmin(res, a);
+  }
+  if (p.lane == 0) atomic_min_nonneg(alpha + p.inst, res);
+}
+// coneops_nonsymmetric_common.jl:5-34 backtracking, per cone
+template <class Ops>
+__global__ void k_nonsym_step(ConeSet cs, NonsymArgs<Ops> a, const double *__restrict__ dz,
+                              const double *__restrict__ ds, const double *__restrict__ z,
+                              const double *__restrict__ s, const double *astart,
+                              double *alpha, double step, double amin) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n) return;
+  int inst = a.inst[c];
+  if (!active_inst(cs, inst)) return;
+  double pa = a.alpha ? a.alpha[c] : 0.0;
+  int b = a.begin + 3 * c;
+  double a0 = astart[inst];
+  double res = a0;
+  for (int side = 0; side < 2; ++side) {
+    const double *q = side == 0 ? z : s;
+    const double *dq = side == 0 ? dz : ds;
+    double al = a0, wq[3];
+    while (true) {
+      for (int i = 0; i < 3; ++i) wq[i] = q[b + i] + al * dq[b + i];
+      bool ok = side == 0 ? Ops::dual_feasible(wq, pa) : Ops::primal_feasible(wq, pa);
+      if (ok) break;
+      if ((al *= step) < amin) {
+        al = 0;
+        break;
+      }
+    }
+    res = fmin(res, al);
+  }
+  atomic_min_nonneg(alpha + inst, res);
+}
+
+// ================================================================ barrier
+__global__ void k_nn_barrier(ConeSet cs, const double *__restrict__ z,
+                             const double *__restrict__ s, const double *__restrict__ dz,
+                             const double *__restrict__ ds, const double *alpha,
+                             const int *bt, double *bar) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double v = 0;
+  if (e < cs.n_nn) {
+    int g = cs.nn_begin + e;
+    inst = cs.row_inst[g];
+    if (active_inst(cs, inst) && bt[inst]) {
+      double a = alpha[inst];
+      double si = s[g] + a * ds[g], zi = z[g] + a * dz[g];
+      v = -logsafe(si * zi);
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(bar, 0, inst, v);
+}
+template <int G>
+__global__ void k_soc_barrier(ConeSet cs, const double *__restrict__ z_,
+                              const double *__restrict__ s_, const double *__restrict__ dz_,
+                              const double *__restrict__ ds_, const double *alpha,
+                              const int *bt, double *bar) {
+  SocCtx<G> ctx(cs);
+  double a = alpha[ctx.inst];
+  const double *z = z_ + ctx.off, *s = s_ + ctx.off, *dz = dz_ + ctx.off,
+               *ds = ds_ + ctx.off;
+  double sq = 0, zq = 0;
+  SOC_FOR(i) if (i > 0) {
+    double si = s[i] + a * ds[i], zi = z[i] + a * dz[i];
+    sq += si * si;
+    zq += zi * zi;
+  }
+  sq = group_sum<G>(sq);
+  zq = group_sum<G>(zq);
+  if (!ctx.valid || !bt[ctx.inst] || ctx.lane != 0) return;
+  double rs = soc_res(s[0] + a * ds[0], sq), rz = soc_res(z[0] + a * dz[0], zq);
+  double v = (rs > 0 && rz > 0) ? -logsafe(rs * rz) / 2 : CUDART_INF;
+  atomicAdd(bar + ctx.inst, v);
+}
+template <class Ops>
+__global__ void k_nonsym_barrier(ConeSet cs, NonsymArgs<Ops> a, const double *__restrict__ z,
+                                 const double *__restrict__ s, const double *__restrict__ dz,
+                                 const double *__restrict__ ds, const double *alpha,
+                                 const int *bt, double *bar) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n) return;
+  int inst = a.inst[c];
+  if (!active_inst(cs, inst) || !bt[inst]) return;
+  double pa = a.alpha ? a.alpha[c] : 0.0;
+  double al = alpha[inst];
+  int b = a.begin + 3 * c;
+  double cz[3], csv[3];
+  for (int i = 0; i < 3; ++i) {
+    cz[i] = z[b + i] + al * dz[b + i];
+    csv[i] = s[b + i] + al * ds[b + i];
+  }
+  atomicAdd(bar + inst, Ops::barrier_dual(cz, pa) + Ops::barrier_primal(csv, pa));
+}
+__global__ void k_psd_barrier(ConeSet cs, const double *__restrict__ z,
+                              const double *__restrict__ s, const double *__restrict__ dz,
+                              const double *__restrict__ ds, const double *alpha,
+                              const int *bt, double *bar) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid || !bt[p.inst]) return;
+  int n = p.n, nm = cs.psd_nmax;
+  double *Q = psd_smem(nm, 2), *q = Q + nm * nm;
+  double a = alpha[p.inst];
+  double total = 0;
+  for (int side = 0; side < 2; ++side) {
+    const double *x = side == 0 ? z : s, *dx = side == 0 ? dz : ds;
+    for (int k = p.lane; k < p.t; k += 32) q[k] = x[p.off + k] + a * dx[p.off + k];
+    __syncwarp();
+    svec_to_mat(n, q, Q, p.lane);
+    __syncwarp();
+    bool ok = warp_chol(n, Q, p.lane);
+    double ld;
+    if (ok) {
+      double t = p.lane < n ? log(Q[p.lane + n * p.lane]) : 0.0;
+      ld = 2 * warp_sum(t);
+    } else {
+      ld = CUDART_INF;
+    }
+    total -= ld;
+    __syncwarp();
+  }
+  if (p.lane == 0) atomicAdd(bar + p.inst, total);
+}
+
+// ================================================================ margins
+__global__ void k_nn_margins(ConeSet cs, const double *__restrict__ z, double *amin,
+                             double *asum) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double v = 0;
+  if (e < cs.n_nn) {
+    int g = cs.nn_begin + e;
+    inst = cs.row_inst[g];
+    if (active_inst(cs, inst)) {
+      v = z[g];
+      atomic_min_any(amin + inst, v);
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(asum, 0, inst, v > 0 ? v : 0.0);
+}
+template <int G>
+__global__ void k_soc_margins(ConeSet cs, const double *__restrict__ z_, double *amin,
+                              double *asum) {
+  SocCtx<G> ctx(cs);
+  const double *z = z_ + ctx.off;
+  double t = soc_tail_sq<G>(z, ctx);
+  if (!ctx.valid || ctx.lane != 0) return;
+  double a = z[0] - sqrt(t);
+  atomic_min_any(amin + ctx.inst, a);
+  atomicAdd(asum + ctx.inst, fmax(0.0, a));
+}
+__global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z, double *amin,
+                              double *asum) {
+  PsdCtx p = psd_ctx(cs);
+  if (!p.valid) return;
+  int n = p.n, nm = cs.psd_nmax;
+  double *Z = psd_smem(nm, 2), *ev = Z + nm * nm;
+  if (n == 0) return;
+  svec_to_mat(n, z + p.off, Z, p.lane);
+  __syncwarp();
+  double mn = warp_eig_min(n, Z, ev, p.lane);
+  double pos = (p.lane < n && ev[p.lane] > 0) ? ev[p.lane] : 0.0;
+  pos = warp_sum(pos);
+  if (p.lane == 0) {
+    atomic_min_any(amin + p.inst, mn);
+    atomicAdd(asum + p.inst, pos);
+  }
+}
+
+// ============================================ shifts, unit init, identity
+__global__ void k_zero_shift(ConeSet cs, double *z, int pd) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_zero) return;
+  int g = cs.zero_begin + e;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (pd == 0) z[g] = 0.0;
+}
+__global__ void k_nn_shift(ConeSet cs, double *z, const double *alpha) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cs.n_nn) return;
+  int g = cs.nn_begin + e;
+  int inst = cs.row_inst[g];
+  if (!active_inst(cs, inst)) return;
+  z[g] += alpha[inst];
+}
+__global__ void k_soc_shift(ConeSet cs, double *z, const double *alpha) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cs.n_soc) return;
+  int inst = cs.soc_inst[c];
+  if (!active_inst(cs, inst)) return;
+  z[cs.soc_off[c]] += alpha[inst];
+}
+__global__ void k_psd_shift(ConeSet cs, double *z, const double *alpha) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cs.n_psd) return;
+  int inst = cs.psd_inst[c];
+  if (!active_inst(cs, inst)) return;
+  int n = cs.psd_n[c];
+  for (int k = 1; k <= n; ++k) z[cs.psd_off[c] + k * (k + 1) / 2 - 1] += alpha[inst];
+}
+__global__ void k_unit_init(ConeSet cs, double *z, double *s) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= cs.m_total) return;
+  if (!active_inst(cs, cs.row_inst[g])) return;
+  double v = 0.0;
+  if (g >= cs.nn_begin && g < cs.nn_begin + cs.n_nn) v = 1.0;
+  s[g] = v;
+  z[g] = v;
+}
+__global__ void k_unit_init_cones(ConeSet cs, double *z, double *s) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int total = cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd;
+  if (c >= total) return;
+  if (c < cs.n_soc) {
+    if (!active_inst(cs, cs.soc_inst[c])) return;
+    int o = cs.soc_off[c];
+    s[o] += 1.0;
+    z[o] += 1.0;
+    return;
+  }
+  c -= cs.n_soc;
+  if (c < cs.n_exp) {
+    if (!active_inst(cs, cs.exp_inst[c])) return;
+    double v[3];
+    ExpOps::unit_init(v, 0);
+    int b = cs.exp_begin + 3 * c;
+    for (int i = 0; i < 3; ++i) s[b + i] = z[b + i] = v[i];
+    return;
+  }
+  c -= cs.n_exp;
+  if (c < cs.n_pow) {
+    if (!active_inst(cs, cs.pow_inst[c])) return;
+    double v[3];
+    PowOps::unit_init(v, cs.pow_alpha[c]);
+    int b = cs.pow_begin + 3 * c;
+    for (int i = 0; i < 3; ++i) s[b + i] = z[b + i] = v[i];
+    return;
+  }
+  c -= cs.n_pow;
+  if (!active_inst(cs, cs.psd_inst[c])) return;
+  int n = cs.psd_n[c];
+  for (int k = 1; k <= n; ++k) {
+    int idx = cs.psd_off[c] + k * (k + 1) / 2 - 1;
+    s[idx] += 1.0;
+    z[idx] += 1.0;
+  }
+}
+__global__ void k_identity(ConeSet cs) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < cs.n_nn) {
+    if (active_inst(cs, cs.row_inst[cs.nn_begin + t])) cs.nn_w[t] = 1.0;
+  }
+  if (t < cs.soc_rows) {
+    int g = cs.soc_begin + t;
+    if (active_inst(cs, cs.row_inst[g])) {
+      // first element of its cone?  soc rows are contiguous per cone; a row is
+      // a head iff it equals the cone's offset -- found by the cone loop below
+      cs.soc_w[t] = 0.0;
+      cs.soc_u[t] = 0.0;
+      cs.soc_v[t] = 0.0;
+    }
+  }
+}
+__global__ void k_identity_cones(ConeSet cs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < cs.n_soc) {
+    if (!active_inst(cs, cs.soc_inst[c])) return;
+    int r = cs.soc_off[c] - cs.soc_begin;
+    cs.soc_w[r] = 1.0;
+    cs.soc_eta[c] = 1.0;
+    if (cs.soc_sparse[c]) {
+      cs.soc_d[c] = 0.5;
+      cs.soc_u[r] = sqrt(0.5);
+    }
+    return;
+  }
+  c -= cs.n_soc;
+  if (c < cs.n_psd) {
+    if (!active_inst(cs, cs.psd_inst[c])) return;
+    int nm = cs.psd_nmax, n = cs.psd_n[c];
+    double *R = cs.psd_R + (size_t)c * nm * nm, *Ri = cs.psd_Rinv + (size_t)c * nm * nm;
+    for (int e = 0; e < n * n; ++e) {
+      double v = (e % n == e / n) ? 1.0 : 0.0;
+      R[e] = v;
+      Ri[e] = v;
+    }
+  }
+}
+
+// =============================================================== launchers
+static inline int blocks_for(long long n, int b = kBlock) {
+  return n <= 0 ? 0 : ceil_div(n, b);
+}
+#define LAUNCH_SOC(KERNEL, ...)                                                        \
+  do {                                                                                 \
+    if (cs.n_soc > 0) {                                                                \
+      int G = cs.soc_group;                                                            \
+      int nb = blocks_for((long long)cs.n_soc * G);                                    \
+      switch (G) {                                                                     \
+        case 2: KERNEL<2><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                  \
+        case 4: KERNEL<4><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                  \
+        case 8: KERNEL<8><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                  \
+        case 16: KERNEL<16><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                \
+        default: KERNEL<32><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                \
+      }                                                                                \
+    }                                                                                  \
+  } while (0)
+
+static inline void psd_launch_dims(const ConeSet &cs, int nmats, int &nb, int &nt,
+                                   size_t &smem) {
+  nt = 32 * kPsdWarps;
+  nb = blocks_for((long long)cs.n_psd * 32, nt);
+  smem = (size_t)kPsdWarps * nmats * cs.psd_nmax * cs.psd_nmax * sizeof(double) + 256;
+}
+#define LAUNCH_PSD(KERNEL, NMATS, ...)                                                 \
+  do {                                                                                 \
+    if (cs.n_psd > 0) {                                                                \
+      int _nb, _nt;                                                                    \
+      size_t _smem;                                                                    \
+      psd_launch_dims(cs, NMATS, _nb, _nt, _smem);                                     \
+      KERNEL<<<_nb, _nt, _smem, st>>>(__VA_ARGS__);                                    \
+    }                                                                                  \
+  } while (0)
+
+static NonsymArgs<ExpOps> exp_args(const ConeSet &cs) {
+  return NonsymArgs<ExpOps>{cs.n_exp, cs.exp_begin, cs.exp_inst, nullptr,
+                            cs.exp_Hd, cs.exp_Hs, cs.exp_grad, cs.exp_z};
+}
+static NonsymArgs<PowOps> pow_args(const ConeSet &cs) {
+  return NonsymArgs<PowOps>{cs.n_pow, cs.pow_begin, cs.pow_inst, cs.pow_alpha,
+                            cs.pow_Hd, cs.pow_Hs, cs.pow_grad, cs.pow_z};
+}
+
+void cones_update_scaling(const ConeSet &cs, const double *s, const double *z,
+                          const double *mu, const int *scaling, int *scale_ok,
+                          cudaStream_t st) {
+  if (cs.n_nn) k_nn_update_scaling<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, s, z);
+  LAUNCH_SOC(k_soc_update_scaling, cs, s, z, scale_ok);
+  if (cs.n_exp)
+    k_nonsym_update_scaling<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
+        cs, exp_args(cs), s, z, mu, scaling);
+  if (cs.n_pow)
+    k_nonsym_update_scaling<PowOps><<<blocks_for(cs.n_pow, 128), 128, 0, st>>>(
+        cs, pow_args(cs), s, z, mu, scaling);
+  LAUNCH_PSD(k_psd_update_scaling, 7, cs, s, z, scale_ok);
+}
+
+void cones_refresh_kkt(const ConeSet &cs, const KKTMapDev &map, double *kv,
+                       cudaStream_t st) {
+  if (cs.n_nn) k_nn_refresh<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, map.nn_pos, kv);
+  LAUNCH_SOC(k_soc_refresh, cs, map, kv);
+  if (cs.n_exp)
+    k_nonsym_refresh<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_inst,
+                                                             cs.exp_Hs, map.exp_pos, kv);
+  if (cs.n_pow)
+    k_nonsym_refresh<<<blocks_for(cs.n_pow), kBlock, 0, st>>>(cs, cs.n_pow, cs.pow_inst,
+                                                             cs.pow_Hs, map.pow_pos, kv);
+  LAUNCH_PSD(k_psd_refresh, 1, cs, map, kv);
+}
+
+void cones_get_Hs(const ConeSet &cs, const int *nn_blk, const int *soc_blk,
+                  const int *exp_blk, const int *pow_blk, const int *psd_blk, double *Hs,
+                  cudaStream_t st) {
+  if (cs.n_nn) k_nn_get_hs<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, nn_blk, Hs);
+  LAUNCH_SOC(k_soc_get_hs, cs, soc_blk, Hs);
+  if (cs.n_exp)
+    k_nonsym_get_hs<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs.n_exp, cs.exp_Hs, exp_blk, Hs);
+  if (cs.n_pow)
+    k_nonsym_get_hs<<<blocks_for(cs.n_pow), kBlock, 0, st>>>(cs.n_pow, cs.pow_Hs, pow_blk, Hs);
+  LAUNCH_PSD(k_psd_get_hs, 1, cs, psd_blk, Hs);
+}
+
+void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st) {
+  if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, y);
+  if (cs.n_nn) k_nn_mul_hs<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, y, x);
+  LAUNCH_SOC(k_soc_mul_hs, cs, y, x);
+  if (cs.n_exp)
+    k_nonsym_mul_hs<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
+                                                            cs.exp_inst, cs.exp_Hs, y, x);
+  if (cs.n_pow)
+    k_nonsym_mul_hs<<<blocks_for(cs.n_pow), kBlock, 0, st>>>(cs, cs.n_pow, cs.pow_begin,
+                                                            cs.pow_inst, cs.pow_Hs, y, x);
+  LAUNCH_PSD(k_psd_mul_hs, 3, cs, y, x);
+}
+
+void cones_affine_ds(const ConeSet &cs, double *ds, const double *s, cudaStream_t st) {
+  if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, ds);
+  if (cs.n_nn) k_nn_affine_ds<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, ds);
+  LAUNCH_SOC(k_soc_affine_ds, cs, ds);
+  if (cs.n_exp)
+    k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
+                                                              cs.exp_inst, ds, s);
+  if (cs.n_pow)
+    k_nonsym_copy<<<blocks_for(3 * cs.n_pow), kBlock, 0, st>>>(cs, cs.n_pow, cs.pow_begin,
+                                                              cs.pow_inst, ds, s);
+  LAUNCH_PSD(k_psd_affine_ds, 0, cs, ds);
+}
+
+void cones_combined_ds_shift(const ConeSet &cs, double *shift, const double *dz,
+                             const double *ds, const double *sm, cudaStream_t st) {
+  if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, shift);
+  if (cs.n_nn) k_nn_combined<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, shift, dz, ds, sm);
+  LAUNCH_SOC(k_soc_combined, cs, shift, dz, ds, sm);
+  if (cs.n_exp)
+    k_nonsym_combined<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
+        cs, exp_args(cs), shift, dz, ds, sm);
+  if (cs.n_pow)
+    k_nonsym_combined<PowOps><<<blocks_for(cs.n_pow, 128), 128, 0, st>>>(
+        cs, pow_args(cs), shift, dz, ds, sm);
+  LAUNCH_PSD(k_psd_combined, 5, cs, shift, dz, ds, sm);
+}
+
+void cones_ds_from_dz_offset(const ConeSet &cs, double *out, const double *ds,
+                             const double *z, cudaStream_t st) {
+  if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, out);
+  if (cs.n_nn) k_nn_ds_offset<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, out, ds, z);
+  LAUNCH_SOC(k_soc_ds_offset, cs, out, ds, z);
+  if (cs.n_exp)
+    k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
+                                                              cs.exp_inst, out, ds);
+  if (cs.n_pow)
+    k_nonsym_copy<<<blocks_for(3 * cs.n_pow), kBlock, 0, st>>>(cs, cs.n_pow, cs.pow_begin,
+                                                              cs.pow_inst, out, ds);
+  LAUNCH_PSD(k_psd_ds_offset, 4, cs, out, ds);
+}
+
+void cones_step_length_sym(const ConeSet &cs, const double *dz, const double *ds,
+                           const double *z, const double *s, double *alpha,
+                           cudaStream_t st) {
+  if (cs.n_nn) k_nn_step<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, dz, ds, z, s, alpha);
+  LAUNCH_SOC(k_soc_step, cs, dz, ds, z, s, alpha);
+  LAUNCH_PSD(k_psd_step, 4, cs, dz, ds, alpha);
+}
+
+void cones_step_length_asym(const ConeSet &cs, const double *dz, const double *ds,
+                            const double *z, const double *s, const double *astart,
+                            double *alpha, double step, double amin, cudaStream_t st) {
+  if (cs.n_exp)
+    k_nonsym_step<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
+        cs, exp_args(cs), dz, ds, z, s, astart, alpha, step, amin);
+  if (cs.n_pow)
+    k_nonsym_step<PowOps><<<blocks_for(cs.n_pow, 128), 128, 0, st>>>(
+        cs, pow_args(cs), dz, ds, z, s, astart, alpha, step, amin);
+}
+
+void cones_barrier(const ConeSet &cs, const double *z, const double *s, const double *dz,
+                   const double *ds, const double *alpha, const int *bt, double *bar,
+                   cudaStream_t st) {
+  if (cs.n_nn)
+    k_nn_barrier<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, z, s, dz, ds, alpha, bt, bar);
+  LAUNCH_SOC(k_soc_barrier, cs, z, s, dz, ds, alpha, bt, bar);
+  if (cs.n_exp)
+    k_nonsym_barrier<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
+        cs, exp_args(cs), z, s, dz, ds, alpha, bt, bar);
+  if (cs.n_pow)
+    k_nonsym_barrier<PowOps><<<blocks_for(cs.n_pow, 128), 128, 0, st>>>(
+        cs, pow_args(cs), z, s, dz, ds, alpha, bt, bar);
+  LAUNCH_PSD(k_psd_barrier, 2, cs, z, s, dz, ds, alpha, bt, bar);
+}
+
+void cones_margins(const ConeSet &cs, const double *z, int pd, double *amin, double *asum,
+                   cudaStream_t st) {
+  (void)pd;
+  if (cs.n_nn) k_nn_margins<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, z, amin, asum);
+  LAUNCH_SOC(k_soc_margins, cs, z, amin, asum);
+  LAUNCH_PSD(k_psd_margins, 2, cs, z, amin, asum);
+}
+
+void cones_scaled_unit_shift(const ConeSet &cs, double *z, const double *alpha, int pd,
+                             cudaStream_t st) {
+  if (cs.n_zero) k_zero_shift<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, z, pd);
+  if (cs.n_nn) k_nn_shift<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, z, alpha);
+  if (cs.n_soc) k_soc_shift<<<blocks_for(cs.n_soc), kBlock, 0, st>>>(cs, z, alpha);
+  if (cs.n_psd) k_psd_shift<<<blocks_for(cs.n_psd), kBlock, 0, st>>>(cs, z, alpha);
+}
+
+void cones_unit_initialization(const ConeSet &cs, double *z, double *s, cudaStream_t st) {
+  if (cs.m_total) k_unit_init<<<blocks_for(cs.m_total), kBlock, 0, st>>>(cs, z, s);
+  int total = cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd;
+  if (total) k_unit_init_cones<<<blocks_for(total), kBlock, 0, st>>>(cs, z, s);
+}
+
+void cones_set_identity_scaling(const ConeSet &cs, cudaStream_t st) {
+  int t = cs.n_nn > cs.soc_rows ? cs.n_nn : cs.soc_rows;
+  if (t) k_identity<<<blocks_for(t), kBlock, 0, st>>>(cs);
+  int c = cs.n_soc + cs.n_psd;
+  if (c) k_identity_cones<<<blocks_for(c), kBlock, 0, st>>>(cs);
+}
+
+}  // namespace clgpu

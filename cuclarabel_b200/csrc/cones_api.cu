@@ -1,0 +1,302 @@
+// cones_api.cu -- cone-level C ABI (the CompositeConeGPU method table of
+// src/gpucones/coneops_compositecone_gpu.jl), one problem, device pointers
+// borrowed from the caller in the reference's sorted cone order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/clgpu.h"
+#include "cones.cuh"
+#include "devbuf.hpp"
+
+using namespace clgpu;
+
+struct clgpu_cones {
+  DevArena arena;
+  ConeSet cs{};
+  int numel = 0, degree = 0, hs_len = 0;
+  bool symmetric = true;
+  int *d_nn_blk = nullptr, *d_soc_blk = nullptr, *d_exp_blk = nullptr, *d_pow_blk = nullptr,
+      *d_psd_blk = nullptr;
+  double *d_scal = nullptr;  // small scalar workspace [8]
+  int *d_iscal = nullptr;    // [4]
+};
+
+extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
+                                  const double *params, int soc_threshold,
+                                  clgpu_cones **out) {
+  if (!out || ncones < 0 || (ncones > 0 && (!types || !dims))) return -1;
+  for (int c = 1; c < ncones; ++c)
+    if (types[c] < types[c - 1]) return -2;  // compositecone_type_gpu.jl:75-79
+  auto *h = new clgpu_cones();
+  ConeSet &cs = h->cs;
+  DevArena &A = h->arena;
+  std::vector<int> row_inst, soc_off, soc_dim, soc_inst, soc_sparse, exp_inst, pow_inst,
+      psd_off, psd_n, psd_inst, nn_blk, soc_blk, exp_blk, pow_blk, psd_blk;
+  std::vector<double> pow_alpha;
+  int row = 0, blk = 0, soc_max = 0, psd_max = 1;
+  int tbeg[6] = {-1, -1, -1, -1, -1, -1}, trows[6] = {0, 0, 0, 0, 0, 0};
+  for (int c = 0; c < ncones; ++c) {
+    int t = types[c], d = dims[c];
+    if (t < 0 || t > 5 || d < 0) {
+      delete h;
+      return -1;
+    }
+    int nv = (t == 3 || t == 4) ? 3 : (t == 5 ? d * (d + 1) / 2 : d);
+    if (tbeg[t] < 0) tbeg[t] = row;
+    trows[t] += nv;
+    bool sparse = (t == 2 && d > soc_threshold);
+    bool diag = (t == 0 || t == 1 || sparse);
+    int bl = diag ? nv : nv * (nv + 1) / 2;
+    switch (t) {
+      case 0: h->degree += 0; break;
+      case 1:
+        for (int k = 0; k < nv; ++k) nn_blk.push_back(blk + k);
+        h->degree += d;
+        break;
+      case 2:
+        soc_off.push_back(row);
+        soc_dim.push_back(d);
+        soc_inst.push_back(0);
+        soc_sparse.push_back(sparse ? 1 : 0);
+        soc_blk.push_back(blk);
+        soc_max = std::max(soc_max, d);
+        h->degree += 1;
+        break;
+      case 3:
+        exp_inst.push_back(0);
+        exp_blk.push_back(blk);
+        h->degree += 3;
+        h->symmetric = false;
+        break;
+      case 4:
+        pow_inst.push_back(0);
+        pow_alpha.push_back(params ? params[c] : 0.5);
+        pow_blk.push_back(blk);
+        h->degree += 3;
+        h->symmetric = false;
+        break;
+      case 5:
+        if (d > 16) {
+          delete h;
+          return -3;
+        }
+        psd_off.push_back(row);
+        psd_n.push_back(d);
+        psd_inst.push_back(0);
+        psd_blk.push_back(blk);
+        psd_max = std::max(psd_max, d);
+        h->degree += d;
+        break;
+    }
+    row += nv;
+    blk += bl;
+  }
+  for (int r = 0; r < row; ++r) row_inst.push_back(0);
+  h->numel = row;
+  h->hs_len = blk;
+  cs.B = 1;
+  cs.m_total = row;
+  cs.zero_begin = tbeg[0] < 0 ? 0 : tbeg[0];
+  cs.n_zero = trows[0];
+  cs.nn_begin = tbeg[1] < 0 ? 0 : tbeg[1];
+  cs.n_nn = trows[1];
+  cs.soc_begin = tbeg[2] < 0 ? 0 : tbeg[2];
+  cs.soc_rows = trows[2];
+  cs.exp_begin = tbeg[3] < 0 ? 0 : tbeg[3];
+  cs.pow_begin = tbeg[4] < 0 ? 0 : tbeg[4];
+  cs.psd_begin = tbeg[5] < 0 ? 0 : tbeg[5];
+  cs.n_soc = (int)soc_off.size();
+  cs.n_exp = (int)exp_inst.size();
+  cs.n_pow = (int)pow_inst.size();
+  cs.n_psd = (int)psd_off.size();
+  int G = 2;
+  while (G < soc_max && G < 32) G <<= 1;
+  cs.soc_group = G;
+  cs.psd_nmax = psd_max;
+  cs.row_inst = A.upload(row_inst);
+  cs.soc_off = A.upload(soc_off);
+  cs.soc_dim = A.upload(soc_dim);
+  cs.soc_inst = A.upload(soc_inst);
+  cs.soc_sparse = A.upload(soc_sparse);
+  cs.exp_inst = A.upload(exp_inst);
+  cs.pow_inst = A.upload(pow_inst);
+  cs.pow_alpha = A.upload(pow_alpha);
+  cs.psd_off = A.upload(psd_off);
+  cs.psd_n = A.upload(psd_n);
+  cs.psd_inst = A.upload(psd_inst);
+  cs.nn_w = A.alloc<double>(cs.n_nn);
+  cs.nn_lambda = A.alloc<double>(cs.n_nn);
+  cs.soc_w = A.alloc<double>(cs.soc_rows);
+  cs.soc_lambda = A.alloc<double>(cs.soc_rows);
+  cs.soc_u = A.alloc<double>(cs.soc_rows);
+  cs.soc_v = A.alloc<double>(cs.soc_rows);
+  cs.soc_eta = A.alloc<double>(cs.n_soc);
+  cs.soc_d = A.alloc<double>(cs.n_soc);
+  cs.exp_Hd = A.alloc<double>(9 * (size_t)cs.n_exp);
+  cs.exp_Hs = A.alloc<double>(9 * (size_t)cs.n_exp);
+  cs.exp_grad = A.alloc<double>(3 * (size_t)cs.n_exp);
+  cs.exp_z = A.alloc<double>(3 * (size_t)cs.n_exp);
+  cs.pow_Hd = A.alloc<double>(9 * (size_t)cs.n_pow);
+  cs.pow_Hs = A.alloc<double>(9 * (size_t)cs.n_pow);
+  cs.pow_grad = A.alloc<double>(3 * (size_t)cs.n_pow);
+  cs.pow_z = A.alloc<double>(3 * (size_t)cs.n_pow);
+  size_t nn2 = (size_t)psd_max * psd_max;
+  cs.psd_R = A.alloc<double>(nn2 * cs.n_psd);
+  cs.psd_Rinv = A.alloc<double>(nn2 * cs.n_psd);
+  cs.psd_lam = A.alloc<double>((size_t)psd_max * cs.n_psd);
+  cs.inst_active = nullptr;
+  h->d_nn_blk = A.upload(nn_blk);
+  h->d_soc_blk = A.upload(soc_blk);
+  h->d_exp_blk = A.upload(exp_blk);
+  h->d_pow_blk = A.upload(pow_blk);
+  h->d_psd_blk = A.upload(psd_blk);
+  h->d_scal = A.alloc<double>(8);
+  h->d_iscal = A.alloc<int>(4);
+  int one = 1;
+  cudaMemcpy(h->d_iscal + 2, &one, sizeof(int), cudaMemcpyHostToDevice);  // bt active
+  if (A.err != cudaSuccess) {
+    int e = -1000 - (int)A.err;
+    delete h;
+    return e;
+  }
+  *out = h;
+  return 0;
+}
+
+extern "C" int clgpu_cones_destroy(clgpu_cones *h) {
+  if (!h) return -1;
+  delete h;
+  return 0;
+}
+extern "C" int clgpu_cones_numel(const clgpu_cones *h) { return h ? h->numel : -1; }
+extern "C" int clgpu_cones_degree(const clgpu_cones *h) { return h ? h->degree : -1; }
+extern "C" int clgpu_cones_hs_len(const clgpu_cones *h) { return h ? h->hs_len : -1; }
+
+static int finish(cudaStream_t st) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return -1000 - (int)e;
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return -1000 - (int)e;
+  return 0;
+}
+
+extern "C" int clgpu_update_scaling(clgpu_cones *h, const double *s, const double *z,
+                                    double mu, int strategy, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  int iv[2] = {strategy, 1};
+  cudaMemcpyAsync(h->d_scal, &mu, sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(h->d_iscal, iv, 2 * sizeof(int), cudaMemcpyHostToDevice, st);
+  cones_update_scaling(h->cs, s, z, h->d_scal, h->d_iscal, h->d_iscal + 1, st);
+  int ok = 0;
+  cudaMemcpyAsync(&ok, h->d_iscal + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  int rc = finish(st);
+  if (rc) return rc;
+  return ok ? 0 : 1;
+}
+extern "C" int clgpu_set_identity_scaling(clgpu_cones *h, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cones_set_identity_scaling(h->cs, (cudaStream_t)stream);
+  return finish((cudaStream_t)stream);
+}
+extern "C" int clgpu_get_Hs(clgpu_cones *h, double *Hs, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(Hs, 0, (size_t)std::max(h->hs_len, 1) * sizeof(double), st);
+  cones_get_Hs(h->cs, h->d_nn_blk, h->d_soc_blk, h->d_exp_blk, h->d_pow_blk, h->d_psd_blk, Hs,
+               st);
+  return finish(st);
+}
+extern "C" int clgpu_mul_Hs(clgpu_cones *h, double *y, const double *x, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cones_mul_Hs(h->cs, y, x, (cudaStream_t)stream);
+  return finish((cudaStream_t)stream);
+}
+extern "C" int clgpu_affine_ds(clgpu_cones *h, double *ds, const double *s,
+                               clgpu_stream_t stream) {
+  if (!h) return -1;
+  cones_affine_ds(h->cs, ds, s, (cudaStream_t)stream);
+  return finish((cudaStream_t)stream);
+}
+extern "C" int clgpu_combined_ds_shift(clgpu_cones *h, double *shift, const double *step_z,
+                                       const double *step_s, const double *z, double sigma_mu,
+                                       clgpu_stream_t stream) {
+  if (!h) return -1;
+  (void)z;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemcpyAsync(h->d_scal + 1, &sigma_mu, sizeof(double), cudaMemcpyHostToDevice, st);
+  cones_combined_ds_shift(h->cs, shift, step_z, step_s, h->d_scal + 1, st);
+  return finish(st);
+}
+extern "C" int clgpu_ds_from_dz_offset(clgpu_cones *h, double *out, const double *ds,
+                                       const double *z, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cones_ds_from_dz_offset(h->cs, out, ds, z, (cudaStream_t)stream);
+  return finish((cudaStream_t)stream);
+}
+extern "C" int clgpu_step_length(clgpu_cones *h, const double *dz, const double *ds,
+                                 const double *z, const double *s, double alpha_max,
+                                 double max_step_fraction, double backtrack_step,
+                                 double alpha_min, double *alpha, clgpu_stream_t stream) {
+  if (!h || !alpha) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemcpyAsync(h->d_scal + 2, &alpha_max, sizeof(double), cudaMemcpyHostToDevice, st);
+  cones_step_length_sym(h->cs, dz, ds, z, s, h->d_scal + 2, st);
+  double a = 0;
+  cudaMemcpyAsync(&a, h->d_scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
+  int rc = finish(st);
+  if (rc) return rc;
+  if (!h->symmetric) {
+    a = std::min(a, max_step_fraction);
+    cudaMemcpyAsync(h->d_scal + 2, &a, sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h->d_scal + 3, &a, sizeof(double), cudaMemcpyHostToDevice, st);
+    cones_step_length_asym(h->cs, dz, ds, z, s, h->d_scal + 2, h->d_scal + 3, backtrack_step,
+                           alpha_min, st);
+    cudaMemcpyAsync(&a, h->d_scal + 3, sizeof(double), cudaMemcpyDeviceToHost, st);
+    rc = finish(st);
+    if (rc) return rc;
+  }
+  *alpha = a;
+  return 0;
+}
+extern "C" int clgpu_compute_barrier(clgpu_cones *h, const double *z, const double *s,
+                                     const double *dz, const double *ds, double alpha,
+                                     double *barrier, clgpu_stream_t stream) {
+  if (!h || !barrier) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  double init[2] = {alpha, 0.0};
+  cudaMemcpyAsync(h->d_scal + 4, init, 2 * sizeof(double), cudaMemcpyHostToDevice, st);
+  cones_barrier(h->cs, z, s, dz, ds, h->d_scal + 4, h->d_iscal + 2, h->d_scal + 5, st);
+  cudaMemcpyAsync(barrier, h->d_scal + 5, sizeof(double), cudaMemcpyDeviceToHost, st);
+  return finish(st);
+}
+extern "C" int clgpu_margins(clgpu_cones *h, const double *z, int pd, double *alpha,
+                             double *beta, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  double init[2] = {DBL_MAX, 0.0};
+  cudaMemcpyAsync(h->d_scal + 6, init, 2 * sizeof(double), cudaMemcpyHostToDevice, st);
+  cones_margins(h->cs, z, pd, h->d_scal + 6, h->d_scal + 7, st);
+  double out[2];
+  cudaMemcpyAsync(out, h->d_scal + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  int rc = finish(st);
+  if (rc) return rc;
+  if (alpha) *alpha = out[0];
+  if (beta) *beta = out[1];
+  return 0;
+}
+extern "C" int clgpu_scaled_unit_shift(clgpu_cones *h, double *z, double alpha, int pd,
+                                       clgpu_stream_t stream) {
+  if (!h) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemcpyAsync(h->d_scal, &alpha, sizeof(double), cudaMemcpyHostToDevice, st);
+  cones_scaled_unit_shift(h->cs, z, h->d_scal, pd, st);
+  return finish(st);
+}
+extern "C" int clgpu_unit_initialization(clgpu_cones *h, double *z, double *s,
+                                         clgpu_stream_t stream) {
+  if (!h) return -1;
+  cones_unit_initialization(h->cs, z, s, (cudaStream_t)stream);
+  return finish((cudaStream_t)stream);
+}

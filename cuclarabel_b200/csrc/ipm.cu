@@ -1,0 +1,1603 @@
+// ipm.cu -- device-resident homogeneous-embedding IPM for a batch of
+// independent problems (B = 1 is the plain path).
+//
+// The iteration, termination and strategy logic follow src/solver.jl:231-582,
+// src/variables.jl, src/residuals.jl, src/info.jl and src/kktsystem_gpu.jl of
+// the CuClarabel tree.  Every scalar of the reference loop (tau, kappa, mu,
+// sigma, alpha, status, scaling strategy, ...) is a per-instance device value
+// and every host-side decision of the reference is an instance kernel with one
+// thread per instance, so a whole pass over the loop body is issued without a
+// single device->host copy.  The host reads one counter per pass (how many
+// instances are still running).
+//
+// Lock-step semantics: an instance that would "continue" in the reference
+// (new scaling strategy) sets its skip flag and sits out the rest of the pass;
+// an instance that would "break" sets done and is frozen.  All vector kernels
+// read the per-instance active mask.
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+#include "cones.cuh"
+#include "devbuf.hpp"
+#include "ldl.cuh"
+#include "setup.hpp"
+
+namespace clgpu {
+
+static constexpr int TB = 256;
+static inline int nblk(long long n) { return n <= 0 ? 1 : (int)((n + TB - 1) / TB); }
+
+// masks for k_set_mask
+enum MaskMode { M_PASS = 0, M_SYM, M_ASYM, M_SYM_QP, M_SYM_LP, M_BT, M_ALL_UNDONE };
+
+struct Dev {
+  int B = 0, nx = 0, mz = 0;
+  // data
+  const int *Pp, *Pj, *Ap, *Aj, *Atp, *Atj;
+  const double *Px, *Ax, *Atx;
+  const double *q, *b, *d, *dinv, *e, *einv, *negq;
+  const int *col_inst, *row_inst;
+  // variables
+  double *x, *s, *z, *px, *ps, *pz;       // current, previous
+  double *rhs_x, *rhs_s, *rhs_z;          // step_rhs
+  double *dx, *ds, *dz;                   // step_lhs
+  double *rx, *rz, *rx_inf, *rz_inf, *Px_; // residuals
+  double *x1, *z1, *x2, *z2, *workz, *wconic, *zerox, *zeroz;
+  double *S;
+  int *I;
+  int *active;
+  int *counter;
+};
+__device__ __forceinline__ double &SF(const Dev &d, int f, int i) { return d.S[f * d.B + i]; }
+__device__ __forceinline__ int &IF(const Dev &d, int f, int i) { return d.I[f * d.B + i]; }
+
+// per-instance constants kept beside the scalar block
+struct InstConst {
+  const int *degree;
+  const int *sym;
+};
+
+struct SettingsDev {
+  int max_iter;
+  double time_limit, max_step_fraction;
+  double tol_gap_abs, tol_gap_rel, tol_feas, tol_infeas_abs, tol_infeas_rel, tol_ktratio;
+  double r_gap_abs, r_gap_rel, r_feas, r_infeas_abs, r_infeas_rel, r_ktratio;
+  double bt_step, min_switch, min_terminate;
+};
+
+// =============================================================== masks
+__global__ void k_set_mask(Dev d, InstConst ic, int mode) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  bool undone = IF(d, I_DONE, i) == 0;
+  bool v = false;
+  switch (mode) {
+    case M_PASS: v = undone && IF(d, I_SKIP, i) == 0; break;
+    case M_SYM: v = undone && ic.sym[i]; break;
+    case M_ASYM: v = undone && !ic.sym[i]; break;
+    case M_SYM_QP: v = undone && ic.sym[i] && IF(d, I_PNNZ, i); break;
+    case M_SYM_LP: v = undone && ic.sym[i] && !IF(d, I_PNNZ, i); break;
+    case M_BT: v = undone && IF(d, I_SKIP, i) == 0 && IF(d, I_BT_ACTIVE, i); break;
+    case M_ALL_UNDONE: v = undone; break;
+  }
+  d.active[i] = v ? 1 : 0;
+}
+
+__global__ void k_zero_fields(Dev d, int f0, int nf, double v) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf * d.B) return;
+  d.S[f0 * d.B + t] = v;
+}
+
+// =============================================================== init
+__global__ void k_init_state(Dev d, const double *c, const double *normq,
+                             const double *normb, const int *pnnz) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  for (int f = 0; f < NUM_SCALARS; ++f) SF(d, f, i) = 0.0;
+  for (int f = 0; f < NUM_INTS; ++f) IF(d, f, i) = 0;
+  SF(d, F_TAU, i) = 1.0;
+  SF(d, F_KAPPA, i) = 1.0;
+  SF(d, F_SIGMA, i) = 1.0;
+  SF(d, F_MU, i) = kDMax;
+  const double inf = CUDART_INF;
+  SF(d, F_PREV_COST_P, i) = inf;
+  SF(d, F_PREV_COST_D, i) = inf;
+  SF(d, F_PREV_RES_P, i) = inf;
+  SF(d, F_PREV_RES_D, i) = inf;
+  SF(d, F_PREV_GAP_ABS, i) = inf;
+  SF(d, F_PREV_GAP_REL, i) = inf;
+  SF(d, F_EQ_C, i) = c[i];
+  SF(d, F_NORMQ, i) = normq[i];
+  SF(d, F_NORMB, i) = normb[i];
+  IF(d, I_PNNZ, i) = pnnz[i];
+  IF(d, I_SCALING, i) = 0;  // PrimalDual (every supported cone allows it)
+  IF(d, I_KKT_OK, i) = 1;
+  IF(d, I_SCALE_OK, i) = 1;
+}
+
+// x = 0 for the asymmetric (unit) start, tau = kappa = 1
+__global__ void k_zero_x_masked(Dev d) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.nx) return;
+  if (!d.active[d.col_inst[j]]) return;
+  d.x[j] = 0.0;
+}
+__global__ void k_negate_s_masked(Dev d) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.mz) return;
+  if (!d.active[d.row_inst[g]]) return;
+  d.s[g] = -d.s[g];
+}
+__global__ void k_s_from_neg_z_masked(Dev d) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.mz) return;
+  if (!d.active[d.row_inst[g]]) return;
+  d.s[g] = -d.z[g];
+}
+// _shift_to_cone_interior! (variables.jl:276-304): two shift amounts per
+// instance from the margins
+__global__ void k_shift_amounts(Dev d, InstConst ic, int fmin, int fsum, int fa1, int fa2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  double mm = SF(d, fmin, i), pm = SF(d, fsum, i);
+  int deg = ic.degree[i];
+  double target = fmax(1.0, 0.1 * pm / deg);
+  double a1, a2;
+  if (mm <= 0) {
+    a1 = -mm;
+    a2 = target;
+  } else if (mm < target) {
+    a1 = target - mm;
+    a2 = 0.0;
+  } else {
+    a1 = 0.0;
+    a2 = 0.0;
+  }
+  SF(d, fa1, i) = a1;
+  SF(d, fa2, i) = a2;
+}
+__global__ void k_set_tau_kappa_one(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  SF(d, F_TAU, i) = 1.0;
+  SF(d, F_KAPPA, i) = 1.0;
+}
+
+// =============================================================== residuals
+// residuals.jl:39-75 fused with the scaled norms of info.jl:66-133
+__global__ void k_resid_x(Dev d) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double v_qx = 0, v_xpx = 0, n_x = 0, n_rxinf = 0, n_px = 0, n_rx = 0;
+  if (j < d.nx) {
+    inst = d.col_inst[j];
+    if (d.active[inst]) {
+      double px = 0;
+      for (int p = d.Pp[j]; p < d.Pp[j + 1]; ++p) px += d.Px[p] * d.x[d.Pj[p]];
+      double atz = 0;
+      for (int p = d.Atp[j]; p < d.Atp[j + 1]; ++p) atz += d.Atx[p] * d.z[d.Atj[p]];
+      double rxinf = -atz;
+      double tau = SF(d, F_TAU, inst);
+      double xj = d.x[j];
+      double rx = rxinf - px - d.q[j] * tau;
+      d.Px_[j] = px;
+      d.rx_inf[j] = rxinf;
+      d.rx[j] = rx;
+      v_qx = d.q[j] * xj;
+      v_xpx = xj * px;
+      double t = d.d[j] * xj;
+      n_x = t * t;
+      t = d.dinv[j] * rxinf;
+      n_rxinf = t * t;
+      t = d.dinv[j] * px;
+      n_px = t * t;
+      t = d.dinv[j] * rx;
+      n_rx = t * t;
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(d.S + F_DOT_QX * d.B, 0, inst, v_qx);
+  seg_atomic_add(d.S + F_DOT_XPX * d.B, 0, inst, v_xpx);
+  seg_atomic_add(d.S + F_NRM_X * d.B, 0, inst, n_x);
+  seg_atomic_add(d.S + F_NRM_RXINF * d.B, 0, inst, n_rxinf);
+  seg_atomic_add(d.S + F_NRM_PX * d.B, 0, inst, n_px);
+  seg_atomic_add(d.S + F_NRM_RX * d.B, 0, inst, n_rx);
+}
+__global__ void k_resid_z(Dev d) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double v_bz = 0, v_sz = 0, n_z = 0, n_s = 0, n_rzinf = 0, n_rz = 0;
+  if (g < d.mz) {
+    inst = d.row_inst[g];
+    if (d.active[inst]) {
+      double ax = 0;
+      for (int p = d.Ap[g]; p < d.Ap[g + 1]; ++p) ax += d.Ax[p] * d.x[d.Aj[p]];
+      double sg = d.s[g], zg = d.z[g];
+      double rzinf = ax + sg;
+      double rz = rzinf - d.b[g] * SF(d, F_TAU, inst);
+      d.rz_inf[g] = rzinf;
+      d.rz[g] = rz;
+      v_bz = d.b[g] * zg;
+      v_sz = sg * zg;
+      double t = d.e[g] * zg;
+      n_z = t * t;
+      t = d.einv[g] * sg;
+      n_s = t * t;
+      t = d.einv[g] * rzinf;
+      n_rzinf = t * t;
+      t = d.einv[g] * rz;
+      n_rz = t * t;
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(d.S + F_DOT_BZ * d.B, 0, inst, v_bz);
+  seg_atomic_add(d.S + F_DOT_SZ * d.B, 0, inst, v_sz);
+  seg_atomic_add(d.S + F_NRM_Z * d.B, 0, inst, n_z);
+  seg_atomic_add(d.S + F_NRM_S * d.B, 0, inst, n_s);
+  seg_atomic_add(d.S + F_NRM_RZINF * d.B, 0, inst, n_rzinf);
+  seg_atomic_add(d.S + F_NRM_RZ * d.B, 0, inst, n_rz);
+}
+
+__device__ void check_convergence(const Dev &d, int i, double tga, double tgr, double tf,
+                                  double tia, double tir, double tkt, int ss, int ps,
+                                  int ds) {
+  double kt = SF(d, F_KTRATIO, i);
+  double gabs = SF(d, F_GAP_ABS, i), grel = SF(d, F_GAP_REL, i);
+  double rp = SF(d, F_RES_P, i), rd = SF(d, F_RES_D, i);
+  if (kt <= 1.0 && ((gabs < tga || grel < tgr) && rp < tf && rd < tf)) {
+    IF(d, I_STATUS, i) = ss;
+  } else if (kt > 1000. / tkt) {
+    double bz = SF(d, F_DOT_BZ, i), qx = SF(d, F_DOT_QX, i);
+    if (bz < -tia && SF(d, F_RES_PINF, i) < -tir * bz)
+      IF(d, I_STATUS, i) = ps;
+    else if (qx < -tia && SF(d, F_RES_DINF, i) < -tir * qx)
+      IF(d, I_STATUS, i) = ds;
+  }
+}
+
+// mu, info_update!, info_check_termination!, insufficient-progress checkpoint
+// (solver.jl:267-295, info.jl:66-190, solver.jl:521-540)
+__global__ void k_info_termination(Dev d, InstConst ic, SettingsDev st, double elapsed,
+                                   int *reset_flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  reset_flag[i] = 0;
+  if (!d.active[i]) return;
+  double tau = SF(d, F_TAU, i), kappa = SF(d, F_KAPPA, i);
+  double mu = (SF(d, F_DOT_SZ, i) + tau * kappa) / (ic.degree[i] + 1);
+  SF(d, F_MU, i) = mu;
+  double tinv = 1.0 / tau;
+  double cinv = 1.0 / SF(d, F_EQ_C, i);
+  double xPx = SF(d, F_DOT_XPX, i) * tinv * tinv / 2;
+  double cp = (SF(d, F_DOT_QX, i) * tinv + xPx) * cinv;
+  double cd = (-SF(d, F_DOT_BZ, i) * tinv - xPx) * cinv;
+  SF(d, F_COST_P, i) = cp;
+  SF(d, F_COST_D, i) = cd;
+  double normx = sqrt(SF(d, F_NRM_X, i));
+  double normz = sqrt(SF(d, F_NRM_Z, i)) * cinv;
+  double norms = sqrt(SF(d, F_NRM_S, i));
+  SF(d, F_RES_PINF, i) = (sqrt(SF(d, F_NRM_RXINF, i)) * cinv) / fmax(1.0, normz);
+  SF(d, F_RES_DINF, i) = fmax(sqrt(SF(d, F_NRM_PX, i)) / fmax(1.0, normx),
+                              sqrt(SF(d, F_NRM_RZINF, i)) / fmax(1.0, normx + norms));
+  normx *= tinv;
+  normz *= tinv;
+  norms *= tinv;
+  SF(d, F_RES_P, i) = sqrt(SF(d, F_NRM_RZ, i)) * tinv /
+                      fmax(1.0, SF(d, F_NORMB, i) + normx + norms);
+  SF(d, F_RES_D, i) = sqrt(SF(d, F_NRM_RX, i)) * tinv * cinv /
+                      fmax(1.0, SF(d, F_NORMQ, i) + normx + normz);
+  double gabs = fabs(cp - cd);
+  SF(d, F_GAP_ABS, i) = gabs;
+  SF(d, F_GAP_REL, i) = gabs / fmax(1.0, fmin(fabs(cp), fabs(cd)));
+  SF(d, F_KTRATIO, i) = kappa * tinv;
+  // info_save_scalars(mu, alpha, sigma, iter)
+  SF(d, F_SOLVE_TIME, i) = elapsed;
+  int iter = IF(d, I_ITER, i);
+  // termination
+  IF(d, I_STATUS, i) = ST_UNSOLVED;
+  check_convergence(d, i, st.tol_gap_abs, st.tol_gap_rel, st.tol_feas, st.tol_infeas_abs,
+                    st.tol_infeas_rel, st.tol_ktratio, ST_SOLVED, ST_PRIMAL_INFEASIBLE,
+                    ST_DUAL_INFEASIBLE);
+  double rd = SF(d, F_RES_D, i), rp = SF(d, F_RES_P, i);
+  double prd = SF(d, F_PREV_RES_D, i), prp = SF(d, F_PREV_RES_P, i);
+  double kt = SF(d, F_KTRATIO, i);
+  if (IF(d, I_STATUS, i) == ST_UNSOLVED && iter > 1 && (rd > prd || rp > prp)) {
+    if (kt < 100 * kDEps &&
+        (SF(d, F_PREV_GAP_ABS, i) < st.tol_gap_abs || SF(d, F_PREV_GAP_REL, i) < st.tol_gap_rel))
+      IF(d, I_STATUS, i) = ST_INSUFFICIENT_PROGRESS;
+    if (kt < 1.0) {
+      if ((rd > 100 * st.tol_feas && rd > 100 * prd) || (rp > 100 * st.tol_feas && rp > 100 * prp))
+        IF(d, I_STATUS, i) = ST_INSUFFICIENT_PROGRESS;
+    }
+  }
+  if (IF(d, I_STATUS, i) == ST_UNSOLVED) {
+    if (st.max_iter == iter)
+      IF(d, I_STATUS, i) = ST_MAX_ITERATIONS;
+    else if (elapsed > st.time_limit)
+      IF(d, I_STATUS, i) = ST_MAX_TIME;
+  }
+  int status = IF(d, I_STATUS, i);
+  if (status != ST_UNSOLVED) {
+    if (status != ST_INSUFFICIENT_PROGRESS) {
+      IF(d, I_DONE, i) = 1;
+    } else {
+      // info_reset_to_prev_iterate
+      SF(d, F_COST_P, i) = SF(d, F_PREV_COST_P, i);
+      SF(d, F_COST_D, i) = SF(d, F_PREV_COST_D, i);
+      SF(d, F_RES_P, i) = SF(d, F_PREV_RES_P, i);
+      SF(d, F_RES_D, i) = SF(d, F_PREV_RES_D, i);
+      SF(d, F_GAP_ABS, i) = SF(d, F_PREV_GAP_ABS, i);
+      SF(d, F_GAP_REL, i) = SF(d, F_PREV_GAP_REL, i);
+      SF(d, F_TAU, i) = SF(d, F_PREV_TAU, i);
+      SF(d, F_KAPPA, i) = SF(d, F_PREV_KAPPA, i);
+      reset_flag[i] = 1;
+      if (!ic.sym[i] && IF(d, I_SCALING, i) == 0) {
+        IF(d, I_STATUS, i) = ST_UNSOLVED;
+        IF(d, I_SCALING, i) = 1;
+        IF(d, I_SKIP, i) = 1;
+      } else {
+        IF(d, I_DONE, i) = 1;
+      }
+    }
+  }
+  // record for the final "alpha == 0" re-save
+  SF(d, F_SIGMA_MU, i) = 0;
+}
+
+__global__ void k_reset_vars(Dev d, const int *reset_flag) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.nx && reset_flag[d.col_inst[t]]) d.x[t] = d.px[t];
+  if (t < d.mz && reset_flag[d.row_inst[t]]) {
+    d.s[t] = d.ps[t];
+    d.z[t] = d.pz[t];
+  }
+}
+
+// after update_scaling (solver.jl:300-313)
+__global__ void k_after_scaling(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  if (!IF(d, I_SCALE_OK, i)) {
+    IF(d, I_STATUS, i) = ST_NUMERICAL_ERROR;
+    IF(d, I_DONE, i) = 1;
+    return;
+  }
+  IF(d, I_ITER, i) += 1;
+  IF(d, I_KKT_OK, i) = 1;
+}
+
+// ============================================================ KKT glue
+// workz = dsc - rhs_z (kktsystem_gpu.jl:168)
+__global__ void k_workz(Dev d, const double *dsc) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.mz || !d.active[d.row_inst[g]]) return;
+  d.workz[g] = dsc[g] - d.rhs_z[g];
+}
+// the three P products and five dots of the tau solve (kktsystem_gpu.jl:179-200)
+__global__ void k_tau_dots_x(Dev d) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+  if (j < d.nx) {
+    inst = d.col_inst[j];
+    if (d.active[inst] && IF(d, I_KKT_OK, inst)) {
+      double tau = SF(d, F_TAU, inst);
+      double px1 = 0, pxm = 0, px2 = 0;
+      for (int p = d.Pp[j]; p < d.Pp[j + 1]; ++p) {
+        int k = d.Pj[p];
+        double v = d.Px[p];
+        px1 += v * d.x1[k];
+        pxm += v * (d.x[k] / tau - d.x2[k]);
+        px2 += v * d.x2[k];
+      }
+      double xi = d.x[j] / tau;
+      a1 = d.q[j] * d.x1[j];
+      a2 = xi * px1;
+      a3 = d.q[j] * d.x2[j];
+      a4 = (xi - d.x2[j]) * pxm;
+      a5 = d.x2[j] * px2;
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(d.S + F_DOT_Q_X1 * d.B, 0, inst, a1);
+  seg_atomic_add(d.S + F_DOT_XI_PX1 * d.B, 0, inst, a2);
+  seg_atomic_add(d.S + F_DOT_Q_X2 * d.B, 0, inst, a3);
+  seg_atomic_add(d.S + F_QF1 * d.B, 0, inst, a4);
+  seg_atomic_add(d.S + F_QF2 * d.B, 0, inst, a5);
+}
+__global__ void k_tau_dots_z(Dev d) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double a1 = 0, a2 = 0;
+  if (g < d.mz) {
+    inst = d.row_inst[g];
+    if (d.active[inst] && IF(d, I_KKT_OK, inst)) {
+      a1 = d.b[g] * d.z1[g];
+      a2 = d.b[g] * d.z2[g];
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(d.S + F_DOT_B_Z1 * d.B, 0, inst, a1);
+  seg_atomic_add(d.S + F_DOT_B_Z2 * d.B, 0, inst, a2);
+}
+__global__ void k_tau_solve(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double tau = SF(d, F_TAU, i), kappa = SF(d, F_KAPPA, i);
+  double num = SF(d, F_RHS_TAU, i) - SF(d, F_RHS_KAPPA, i) / tau + SF(d, F_DOT_Q_X1, i) +
+               SF(d, F_DOT_B_Z1, i) + 2 * SF(d, F_DOT_XI_PX1, i);
+  double den = kappa / tau - SF(d, F_DOT_Q_X2, i) - SF(d, F_DOT_B_Z2, i);
+  den += SF(d, F_QF1, i) - SF(d, F_QF2, i);
+  SF(d, F_STEP_TAU, i) = num / den;
+}
+__global__ void k_lhs_xz(Dev d) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.nx) {
+    int inst = d.col_inst[t];
+    if (d.active[inst] && IF(d, I_KKT_OK, inst))
+      d.dx[t] = d.x1[t] + SF(d, F_STEP_TAU, inst) * d.x2[t];
+  }
+  if (t < d.mz) {
+    int inst = d.row_inst[t];
+    if (d.active[inst] && IF(d, I_KKT_OK, inst))
+      d.dz[t] = d.z1[t] + SF(d, F_STEP_TAU, inst) * d.z2[t];
+  }
+}
+// ds = -(Hs dz + dsc); dkappa (kktsystem_gpu.jl:213-220)
+__global__ void k_lhs_s(Dev d, const double *dsc) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.mz) return;
+  int inst = d.row_inst[g];
+  if (!d.active[inst] || !IF(d, I_KKT_OK, inst)) return;
+  d.ds[g] = -(d.ds[g] + dsc[g]);
+}
+__global__ void k_lhs_kappa(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double tau = SF(d, F_TAU, i);
+  SF(d, F_STEP_KAPPA, i) = -(SF(d, F_RHS_KAPPA, i) + SF(d, F_KAPPA, i) * SF(d, F_STEP_TAU, i)) / tau;
+}
+
+// affine rhs (variables.jl:161-175)
+__global__ void k_affine_rhs(Dev d) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.nx && d.active[d.col_inst[t]]) d.rhs_x[t] = d.rx[t];
+  if (t < d.mz && d.active[d.row_inst[t]]) d.rhs_z[t] = d.rz[t];
+  if (t < d.B && d.active[t]) {
+    double rtau = SF(d, F_DOT_QX, t) + SF(d, F_DOT_BZ, t) + SF(d, F_KAPPA, t) +
+                  SF(d, F_DOT_XPX, t) / SF(d, F_TAU, t);
+    SF(d, F_RTAU, t) = rtau;
+    SF(d, F_RHS_TAU, t) = rtau;
+    SF(d, F_RHS_KAPPA, t) = SF(d, F_TAU, t) * SF(d, F_KAPPA, t);
+  }
+}
+
+// ============================================================ step length
+// variables.jl:14-43
+__global__ void k_step_prep(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double dt = SF(d, F_STEP_TAU, i), dk = SF(d, F_STEP_KAPPA, i);
+  double at = dt < 0 ? -SF(d, F_TAU, i) / dt : kDMax;
+  double ak = dk < 0 ? -SF(d, F_KAPPA, i) / dk : kDMax;
+  SF(d, F_STEP_SYM, i) = fmin(fmin(at, ak), 1.0);
+}
+__global__ void k_step_mid(Dev d, InstConst ic, double msf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double a = SF(d, F_STEP_SYM, i);
+  if (!ic.sym[i]) a = fmin(a, msf);
+  SF(d, F_STEP_SYM, i) = a;
+  SF(d, F_STEP, i) = a;
+}
+__global__ void k_step_final(Dev d, int combined, double msf, int out_field) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double a = SF(d, F_STEP, i);
+  if (combined) a *= msf;
+  SF(d, out_field, i) = a;
+}
+
+// sigma, mfac and the combined tau/kappa rhs (solver.jl:344-357,
+// variables.jl:218-258)
+__global__ void k_combined_scalars(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double a = SF(d, F_ALPHA_AFF, i);
+  double sigma = (1 - a) * (1 - a) * (1 - a);
+  SF(d, F_SIGMA, i) = sigma;
+  double mfac = IF(d, I_ITER, i) > 1 ? 1.0 : a;
+  SF(d, F_MFAC, i) = mfac;
+  double mu = SF(d, F_MU, i);
+  double sm = sigma * mu;
+  SF(d, F_SIGMA_MU, i) = sm;
+  double dt = SF(d, F_STEP_TAU, i), dk = SF(d, F_STEP_KAPPA, i);
+  SF(d, F_RHS_TAU, i) = (1 - sigma) * SF(d, F_RTAU, i);
+  SF(d, F_RHS_KAPPA, i) = -sm + mfac * dt * dk + SF(d, F_TAU, i) * SF(d, F_KAPPA, i);
+}
+__global__ void k_combined_pre(Dev d) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.nx) {
+    int inst = d.col_inst[t];
+    if (d.active[inst] && IF(d, I_KKT_OK, inst))
+      d.rhs_x[t] = (1 - SF(d, F_SIGMA, inst)) * d.rx[t];
+  }
+  if (t < d.mz) {
+    int inst = d.row_inst[t];
+    if (d.active[inst] && IF(d, I_KKT_OK, inst)) {
+      double mf = SF(d, F_MFAC, inst);
+      if (mf != 1.0) d.dz[t] *= mf;
+    }
+  }
+}
+// d.s += shift (held in rhs_z) ; d.z = (1-sigma) rz
+__global__ void k_combined_post(Dev d) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.mz) return;
+  int inst = d.row_inst[g];
+  if (!d.active[inst] || !IF(d, I_KKT_OK, inst)) return;
+  d.rhs_s[g] += d.rhs_z[g];
+  d.rhs_z[g] = (1 - SF(d, F_SIGMA, inst)) * d.rz[g];
+}
+
+// _strategy_checkpoint_numerical_error (solver.jl:543-557)
+__global__ void k_check_numerical(Dev d, InstConst ic) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  if (IF(d, I_KKT_OK, i)) return;
+  SF(d, F_ALPHA, i) = 0.0;
+  if (!ic.sym[i] && IF(d, I_SCALING, i) == 0) {
+    IF(d, I_SCALING, i) = 1;
+    IF(d, I_SKIP, i) = 1;
+  } else {
+    IF(d, I_STATUS, i) = ST_NUMERICAL_ERROR;
+    IF(d, I_DONE, i) = 1;
+  }
+}
+
+// barrier backtracking setup (solver.jl:449-485)
+__global__ void k_bt_setup(Dev d, InstConst ic) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  bool bt = d.active[i] && !ic.sym[i] && IF(d, I_SCALING, i) == 1;
+  IF(d, I_BT_ACTIVE, i) = bt ? 1 : 0;
+  if (bt) atomicAdd(d.counter + 1, 1);
+}
+__global__ void k_dot_shifted(Dev d) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int inst = -1;
+  double v = 0;
+  if (g < d.mz) {
+    inst = d.row_inst[g];
+    if (d.active[inst]) {
+      double a = SF(d, F_ALPHA, inst);
+      v = (d.z[g] + a * d.dz[g]) * (d.s[g] + a * d.ds[g]);
+    } else {
+      inst = -1;
+    }
+  }
+  seg_atomic_add(d.S + F_TAU_NUM * d.B, 0, inst, v);
+}
+__global__ void k_bt_central(Dev d, InstConst ic) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  double a = SF(d, F_ALPHA, i);
+  double cc = ic.degree[i] + 1;
+  double ct = SF(d, F_TAU, i) + a * SF(d, F_STEP_TAU, i);
+  double ck = SF(d, F_KAPPA, i) + a * SF(d, F_STEP_KAPPA, i);
+  double mu = (SF(d, F_TAU_NUM, i) + ct * ck) / cc;
+  SF(d, F_BARRIER, i) = cc * logsafe(mu) - logsafe(ct) - logsafe(ck);
+}
+__global__ void k_bt_check(Dev d, double step) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  if (SF(d, F_BARRIER, i) < 1.0) {
+    IF(d, I_BT_ACTIVE, i) = 0;
+  } else {
+    SF(d, F_ALPHA, i) *= step;
+    atomicAdd(d.counter + 1, 1);
+  }
+}
+
+// _strategy_checkpoint_small_step (solver.jl:560-573)
+__global__ void k_check_small_step(Dev d, InstConst ic, SettingsDev st) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  double a = SF(d, F_ALPHA, i);
+  if (!ic.sym[i] && IF(d, I_SCALING, i) == 0 && a < st.min_switch) {
+    IF(d, I_SCALING, i) = 1;
+    SF(d, F_ALPHA, i) = 0.0;
+    IF(d, I_SKIP, i) = 1;
+  } else if (a <= fmax(0.0, st.min_terminate)) {
+    IF(d, I_STATUS, i) = ST_INSUFFICIENT_PROGRESS;
+    SF(d, F_ALPHA, i) = 0.0;
+    IF(d, I_DONE, i) = 1;
+  }
+}
+
+// info_save_prev_iterate + variables_add_step! (solver.jl:389-391)
+__global__ void k_add_step(Dev d) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.nx) {
+    int inst = d.col_inst[t];
+    if (d.active[inst]) {
+      double a = SF(d, F_ALPHA, inst);
+      d.px[t] = d.x[t];
+      d.x[t] += a * d.dx[t];
+    }
+  }
+  if (t < d.mz) {
+    int inst = d.row_inst[t];
+    if (d.active[inst]) {
+      double a = SF(d, F_ALPHA, inst);
+      d.ps[t] = d.s[t];
+      d.pz[t] = d.z[t];
+      d.s[t] += a * d.ds[t];
+      d.z[t] += a * d.dz[t];
+    }
+  }
+}
+__global__ void k_add_step_scalars(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B || !d.active[i]) return;
+  SF(d, F_PREV_COST_P, i) = SF(d, F_COST_P, i);
+  SF(d, F_PREV_COST_D, i) = SF(d, F_COST_D, i);
+  SF(d, F_PREV_RES_P, i) = SF(d, F_RES_P, i);
+  SF(d, F_PREV_RES_D, i) = SF(d, F_RES_D, i);
+  SF(d, F_PREV_GAP_ABS, i) = SF(d, F_GAP_ABS, i);
+  SF(d, F_PREV_GAP_REL, i) = SF(d, F_GAP_REL, i);
+  SF(d, F_PREV_TAU, i) = SF(d, F_TAU, i);
+  SF(d, F_PREV_KAPPA, i) = SF(d, F_KAPPA, i);
+  double a = SF(d, F_ALPHA, i);
+  SF(d, F_TAU, i) += a * SF(d, F_STEP_TAU, i);
+  SF(d, F_KAPPA, i) += a * SF(d, F_STEP_KAPPA, i);
+}
+__global__ void k_count_running(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  if (IF(d, I_DONE, i) == 0) {
+    IF(d, I_SKIP, i) = 0;
+    atomicAdd(d.counter, 1);
+  }
+}
+
+// ============================================================ post-process
+// info_post_process! + solution_post_process! + variables_unscale!
+// (info.jl:275-291, solution.jl:2-50, variables.jl:373-403)
+__global__ void k_post_status(Dev d, SettingsDev st) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  int s = IF(d, I_STATUS, i);
+  if (s == ST_NUMERICAL_ERROR || s == ST_INSUFFICIENT_PROGRESS || s == ST_MAX_ITERATIONS ||
+      s == ST_MAX_TIME)
+    check_convergence(d, i, st.r_gap_abs, st.r_gap_rel, st.r_feas, st.r_infeas_abs,
+                      st.r_infeas_rel, st.r_ktratio, ST_ALMOST_SOLVED,
+                      ST_ALMOST_PRIMAL_INFEASIBLE, ST_ALMOST_DUAL_INFEASIBLE);
+}
+__device__ __forceinline__ bool status_infeasible(int s) {
+  return s == ST_PRIMAL_INFEASIBLE || s == ST_DUAL_INFEASIBLE ||
+         s == ST_ALMOST_PRIMAL_INFEASIBLE || s == ST_ALMOST_DUAL_INFEASIBLE;
+}
+// out_x: instance-concatenated; out_s/out_z: instance-concatenated in user row
+// order, zmap[k] = global type-major row of output slot k
+__global__ void k_unscale(Dev d, const int *zmap, const int *zinst, double *ox, double *os,
+                          double *oz) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.nx) {
+    int inst = d.col_inst[t];
+    int s = IF(d, I_STATUS, inst);
+    double sinv = status_infeasible(s) ? 1.0 / SF(d, F_KAPPA, inst) : 1.0 / SF(d, F_TAU, inst);
+    ox[t] = d.x[t] * d.d[t] * sinv;
+  }
+  if (t < d.mz) {
+    int g = zmap[t];
+    int inst = zinst[t];
+    int s = IF(d, I_STATUS, inst);
+    double sinv = status_infeasible(s) ? 1.0 / SF(d, F_KAPPA, inst) : 1.0 / SF(d, F_TAU, inst);
+    double c = SF(d, F_EQ_C, inst);
+    oz[t] = d.z[g] * d.e[g] * (sinv / c);
+    os[t] = d.s[g] * d.einv[g] * sinv;
+  }
+}
+
+}  // namespace clgpu
+
+// ====================================================================== host
+using namespace clgpu;
+
+struct clgpu_solver {
+  clgpu_settings st{};
+  int B = 0, nx = 0, mz = 0;
+  bool mixed = false;
+  DevArena arena;
+  Dev dv{};
+  ConeSet cs{};
+  KKTMapDev map{};
+  KKTDev kk{};
+  LDLParams lp{};
+  SettingsDev sd{};
+  InstConst ic{};
+  int *d_reset = nullptr;
+  double *d_c = nullptr, *d_normq = nullptr, *d_normb = nullptr;
+  int *d_pnnz = nullptr;
+  int *d_zmap = nullptr, *d_zinst = nullptr;
+  double *d_out = nullptr;  // nx + 2*mz
+  int *h_counter = nullptr;  // pinned
+  std::vector<int> h_n, h_m, h_xoff, h_moff;
+  bool any_asym = false, any_sym = false;
+  std::vector<clgpu_info> info;
+  std::vector<double> sol;  // host copy of x, s, z (concatenated)
+  bool solved = false;
+  long long launches = 0;
+  bool profiling = false;
+  double prof[5] = {0, 0, 0, 0, 0};
+  int passes = 0;
+  double last_ms = 0;
+  ~clgpu_solver() {
+    if (h_counter) cudaFreeHost(h_counter);
+  }
+};
+
+static SettingsDev make_sd(const clgpu_settings &s) {
+  SettingsDev d;
+  d.max_iter = s.max_iter;
+  d.time_limit = s.time_limit;
+  d.max_step_fraction = s.max_step_fraction;
+  d.tol_gap_abs = s.tol_gap_abs;
+  d.tol_gap_rel = s.tol_gap_rel;
+  d.tol_feas = s.tol_feas;
+  d.tol_infeas_abs = s.tol_infeas_abs;
+  d.tol_infeas_rel = s.tol_infeas_rel;
+  d.tol_ktratio = s.tol_ktratio;
+  d.r_gap_abs = s.reduced_tol_gap_abs;
+  d.r_gap_rel = s.reduced_tol_gap_rel;
+  d.r_feas = s.reduced_tol_feas;
+  d.r_infeas_abs = s.reduced_tol_infeas_abs;
+  d.r_infeas_rel = s.reduced_tol_infeas_rel;
+  d.r_ktratio = s.reduced_tol_ktratio;
+  d.bt_step = s.linesearch_backtrack_step;
+  d.min_switch = s.min_switch_step_length;
+  d.min_terminate = s.min_terminate_step_length;
+  return d;
+}
+
+extern "C" int clgpu_default_settings(clgpu_settings *s) {
+  if (!s) return -1;
+  std::memset(s, 0, sizeof(*s));
+  s->max_iter = 200;
+  s->time_limit = INFINITY;
+  s->max_step_fraction = 0.99;
+  s->tol_gap_abs = 1e-8;
+  s->tol_gap_rel = 1e-8;
+  s->tol_feas = 1e-8;
+  s->tol_infeas_abs = 1e-8;
+  s->tol_infeas_rel = 1e-8;
+  s->tol_ktratio = 1e-6;
+  s->reduced_tol_gap_abs = 5e-5;
+  s->reduced_tol_gap_rel = 5e-5;
+  s->reduced_tol_feas = 1e-4;
+  s->reduced_tol_infeas_abs = 5e-12;
+  s->reduced_tol_infeas_rel = 5e-5;
+  s->reduced_tol_ktratio = 1e-4;
+  s->equilibrate_enable = 1;
+  s->equilibrate_max_iter = 10;
+  s->equilibrate_min_scaling = 1e-4;
+  s->equilibrate_max_scaling = 1e4;
+  s->linesearch_backtrack_step = 0.8;
+  s->min_switch_step_length = 1e-2;
+  s->min_terminate_step_length = 1e-4;
+  s->static_regularization_enable = 1;
+  s->static_regularization_constant = 1e-8;
+  s->static_regularization_proportional = kDEps * kDEps;
+  s->dynamic_regularization_enable = 1;
+  s->dynamic_regularization_eps = 1e-13;
+  s->dynamic_regularization_delta = 2e-7;
+  s->iterative_refinement_enable = 1;
+  s->iterative_refinement_reltol = 1e-12;
+  s->iterative_refinement_abstol = 1e-12;
+  s->iterative_refinement_max_iter = 10;
+  s->iterative_refinement_stop_ratio = 5;
+  s->direct_solve_method = CLGPU_METHOD_FP64;
+  s->soc_threshold = 5;
+  s->verbose = 0;
+  s->setup_threads = 0;
+  return 0;
+}
+
+// Builds every device structure of a batch from prepared instances.
+static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
+  DevArena &A = h->arena;
+  const int B = (int)prep.size();
+  h->B = B;
+  // ---------------- sizes and offsets
+  std::vector<int> xoff(B + 1, 0), moff(B + 1, 0);
+  for (int i = 0; i < B; ++i) {
+    xoff[i + 1] = xoff[i] + prep[i].n;
+    moff[i + 1] = moff[i] + prep[i].m;
+  }
+  const int nx = xoff[B], mz = moff[B];
+  h->nx = nx;
+  h->mz = mz;
+  h->h_xoff = xoff;
+  h->h_moff = moff;
+  // type-major global row of (instance, local type-major row)
+  std::vector<long long> type_total(6, 0);
+  for (auto &p : prep)
+    for (int t = 0; t < 6; ++t) type_total[t] += p.type_rows[t];
+  std::vector<int> type_begin(7, 0);
+  for (int t = 0; t < 6; ++t) type_begin[t + 1] = type_begin[t] + (int)type_total[t];
+  std::vector<std::vector<int>> grow(B);  // local type-major row -> global row
+  {
+    std::vector<int> cursor(type_begin.begin(), type_begin.end() - 1);
+    for (int i = 0; i < B; ++i) {
+      auto &p = prep[i];
+      grow[i].resize(p.m);
+      int lr = 0;
+      for (int t = 0; t < 6; ++t)
+        for (int k = 0; k < p.type_rows[t]; ++k) grow[i][lr++] = cursor[t]++;
+    }
+  }
+  std::vector<int> row_inst(mz), col_inst(nx);
+  for (int i = 0; i < B; ++i) {
+    for (int g : grow[i]) row_inst[g] = i;
+    for (int j = xoff[i]; j < xoff[i + 1]; ++j) col_inst[j] = i;
+  }
+  // ---------------- problem data in global CSR form
+  std::vector<int> Pp(nx + 1, 0), Pj, Ap(mz + 1, 0), Aj, Atp(nx + 1, 0), Atj;
+  std::vector<double> Pxv, Axv, Atxv, q(nx), b(mz), dd(nx), ddinv(nx), ee(mz), eeinv(mz);
+  {
+    // P: full symmetric CSC == CSR by symmetry
+    for (int i = 0; i < B; ++i) {
+      auto &p = prep[i];
+      for (int j = 0; j < p.n; ++j) {
+        for (int k = p.Pfull.p[j]; k < p.Pfull.p[j + 1]; ++k) {
+          Pj.push_back(xoff[i] + p.Pfull.i[k]);
+          Pxv.push_back(p.Pfull.x[k]);
+        }
+        Pp[xoff[i] + j + 1] = (int)Pj.size();
+        q[xoff[i] + j] = p.q[j];
+        dd[xoff[i] + j] = p.d[j];
+        ddinv[xoff[i] + j] = 1.0 / p.d[j];
+      }
+      // A^T rows = A columns (CSC of A)
+      for (int j = 0; j < p.n; ++j) {
+        for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k) {
+          int lr_type = -1;
+          (void)lr_type;
+          Atj.push_back(0);  // fixed below
+          Atxv.push_back(p.A.x[k]);
+        }
+        Atp[xoff[i] + j + 1] = (int)Atj.size();
+      }
+    }
+    // fix At column indices (global rows) now that sizes are known
+    int pos = 0;
+    for (int i = 0; i < B; ++i) {
+      auto &p = prep[i];
+      std::vector<int> local_of_user(p.m);
+      for (int lr = 0; lr < p.m; ++lr) local_of_user[p.user_row_of[lr]] = lr;
+      for (int j = 0; j < p.n; ++j)
+        for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k)
+          Atj[pos++] = grow[i][local_of_user[p.A.i[k]]];
+      for (int lr = 0; lr < p.m; ++lr) {
+        int g = grow[i][lr], ur = p.user_row_of[lr];
+        b[g] = p.b[ur];
+        ee[g] = p.e[ur];
+        eeinv[g] = 1.0 / p.e[ur];
+      }
+    }
+    // A rows (global) from At
+    std::vector<int> cnt(mz + 1, 0);
+    for (int g : Atj) cnt[g + 1]++;
+    for (int g = 0; g < mz; ++g) Ap[g + 1] = Ap[g] + cnt[g + 1];
+    Aj.assign(Atj.size(), 0);
+    Axv.assign(Atj.size(), 0.0);
+    std::vector<int> next(Ap.begin(), Ap.end() - 1);
+    for (int j = 0; j < nx; ++j)
+      for (int k = Atp[j]; k < Atp[j + 1]; ++k) {
+        int qd = next[Atj[k]]++;
+        Aj[qd] = j;
+        Axv[qd] = Atxv[k];
+      }
+  }
+  std::vector<double> negq(nx);
+  for (int j = 0; j < nx; ++j) negq[j] = -q[j];
+  // ---------------- per-instance constants
+  std::vector<double> c(B), nq(B), nb(B);
+  std::vector<int> pnnz(B), deg(B), sym(B);
+  for (int i = 0; i < B; ++i) {
+    c[i] = prep[i].c;
+    nq[i] = prep[i].normq;
+    nb[i] = prep[i].normb;
+    pnnz[i] = prep[i].p_nnz > 0 ? 1 : 0;
+    deg[i] = prep[i].degree;
+    sym[i] = prep[i].symmetric ? 1 : 0;
+    if (sym[i]) h->any_sym = true; else h->any_asym = true;
+  }
+  // ---------------- cones
+  ConeSet &cs = h->cs;
+  cs.B = B;
+  cs.m_total = mz;
+  cs.zero_begin = type_begin[0];
+  cs.n_zero = (int)type_total[0];
+  cs.nn_begin = type_begin[1];
+  cs.n_nn = (int)type_total[1];
+  cs.soc_begin = type_begin[2];
+  cs.soc_rows = (int)type_total[2];
+  cs.exp_begin = type_begin[3];
+  cs.pow_begin = type_begin[4];
+  cs.psd_begin = type_begin[5];
+  std::vector<int> soc_off, soc_dim, soc_inst, soc_sparse, exp_inst, pow_inst, psd_off, psd_n,
+      psd_inst;
+  std::vector<double> pow_alpha;
+  int soc_maxdim = 0, psd_nmax = 0;
+  for (int i = 0; i < B; ++i) {
+    auto &p = prep[i];
+    for (size_t k = 0; k < p.ctype.size(); ++k) {
+      int t = p.ctype[k], g = p.m ? grow[i][p.cstart[k]] : 0;
+      if (t == CLGPU_CONE_SOC) {
+        soc_off.push_back(g);
+        soc_dim.push_back(p.cdim[k]);
+        soc_inst.push_back(i);
+        soc_sparse.push_back(p.cdim[k] > h->st.soc_threshold ? 1 : 0);
+        soc_maxdim = std::max(soc_maxdim, p.cdim[k]);
+      } else if (t == CLGPU_CONE_EXP) {
+        exp_inst.push_back(i);
+      } else if (t == CLGPU_CONE_POW) {
+        pow_inst.push_back(i);
+        pow_alpha.push_back(p.cparam[k]);
+      } else if (t == CLGPU_CONE_PSD) {
+        psd_off.push_back(g);
+        psd_n.push_back(p.cdim[k]);
+        psd_inst.push_back(i);
+        psd_nmax = std::max(psd_nmax, p.cdim[k]);
+      }
+    }
+  }
+  cs.n_soc = (int)soc_off.size();
+  cs.n_exp = (int)exp_inst.size();
+  cs.n_pow = (int)pow_inst.size();
+  cs.n_psd = (int)psd_off.size();
+  int G = 2;
+  while (G < soc_maxdim && G < 32) G <<= 1;
+  cs.soc_group = G;
+  cs.psd_nmax = std::max(psd_nmax, 1);
+  if (psd_nmax > 16) return -3;  // PSD side limited to 16 (warp-per-cone kernels)
+  cs.row_inst = A.upload(row_inst);
+  cs.soc_off = A.upload(soc_off);
+  cs.soc_dim = A.upload(soc_dim);
+  cs.soc_inst = A.upload(soc_inst);
+  cs.soc_sparse = A.upload(soc_sparse);
+  cs.exp_inst = A.upload(exp_inst);
+  cs.pow_inst = A.upload(pow_inst);
+  cs.pow_alpha = A.upload(pow_alpha);
+  cs.psd_off = A.upload(psd_off);
+  cs.psd_n = A.upload(psd_n);
+  cs.psd_inst = A.upload(psd_inst);
+  cs.nn_w = A.alloc<double>(cs.n_nn);
+  cs.nn_lambda = A.alloc<double>(cs.n_nn);
+  cs.soc_w = A.alloc<double>(cs.soc_rows);
+  cs.soc_lambda = A.alloc<double>(cs.soc_rows);
+  cs.soc_u = A.alloc<double>(cs.soc_rows);
+  cs.soc_v = A.alloc<double>(cs.soc_rows);
+  cs.soc_eta = A.alloc<double>(cs.n_soc);
+  cs.soc_d = A.alloc<double>(cs.n_soc);
+  cs.exp_Hd = A.alloc<double>(9 * (size_t)cs.n_exp);
+  cs.exp_Hs = A.alloc<double>(9 * (size_t)cs.n_exp);
+  cs.exp_grad = A.alloc<double>(3 * (size_t)cs.n_exp);
+  cs.exp_z = A.alloc<double>(3 * (size_t)cs.n_exp);
+  cs.pow_Hd = A.alloc<double>(9 * (size_t)cs.n_pow);
+  cs.pow_Hs = A.alloc<double>(9 * (size_t)cs.n_pow);
+  cs.pow_grad = A.alloc<double>(3 * (size_t)cs.n_pow);
+  cs.pow_z = A.alloc<double>(3 * (size_t)cs.n_pow);
+  size_t nn2 = (size_t)cs.psd_nmax * cs.psd_nmax;
+  cs.psd_R = A.alloc<double>(nn2 * cs.n_psd);
+  cs.psd_Rinv = A.alloc<double>(nn2 * cs.n_psd);
+  cs.psd_lam = A.alloc<double>((size_t)cs.psd_nmax * cs.n_psd);
+  // ---------------- KKT arrays (concatenate with global positions)
+  std::vector<int> N(B), voff(B + 1, 0), poff(B, 0);
+  long long knz = 0, lnz = 0, rnz = 0;
+  for (int i = 0; i < B; ++i) {
+    N[i] = prep[i].N;
+    voff[i + 1] = voff[i] + N[i];
+    poff[i] = voff[i] + i;
+    knz += prep[i].Kj.size();
+    lnz += prep[i].Li.size();
+    rnz += prep[i].Rk.size();
+  }
+  if (knz > 2000000000LL || lnz > 2000000000LL) return -4;
+  const int VT = voff[B], PT = voff[B] + B;
+  std::vector<int> Kp(PT), Kj((size_t)knz), Kdiag(VT), Lp(PT), Li((size_t)lnz), Rp(PT),
+      Rk((size_t)rnz), Rpos((size_t)rnz), gsrc(VT);
+  std::vector<double> Kx((size_t)knz);
+  std::vector<signed char> Dsign(VT);
+  std::vector<int> nn_pos, socd_off, socd_pos, socs_diag, socs_uv, socs_D, exp_pos, pow_pos,
+      psdo, psd_pos;
+  long long kb = 0, lb = 0, rb = 0;
+  int max_small = 0;
+  bool has_small = false, has_large = false;
+  const int tsize = h->mixed ? 4 : 8;
+  // NN / SOC / etc. refresh maps must follow the global cone order: type by
+  // type, instance by instance -- collect per type.
+  std::vector<std::vector<int>> nn_by_inst(B);
+  for (int i = 0; i < B; ++i) {
+    auto &p = prep[i];
+    int n = p.n, m = p.m;
+    for (int r = 0; r <= N[i]; ++r) {
+      Kp[poff[i] + r] = (int)(kb + p.Kp[r]);
+      Lp[poff[i] + r] = (int)(lb + p.Lp[r]);
+      Rp[poff[i] + r] = (int)(rb + p.Rp[r]);
+    }
+    for (size_t k = 0; k < p.Kj.size(); ++k) {
+      Kj[kb + k] = p.Kj[k];
+      Kx[kb + k] = p.Kx[k];
+    }
+    for (size_t k = 0; k < p.Li.size(); ++k) Li[lb + k] = p.Li[k];
+    for (size_t k = 0; k < p.Rk.size(); ++k) {
+      Rk[rb + k] = p.Rk[k];
+      Rpos[rb + k] = (int)(lb + p.Rpos[k]);
+    }
+    for (int r = 0; r < N[i]; ++r) {
+      Kdiag[voff[i] + r] = (int)(kb + p.Kdiag[r]);
+      Dsign[voff[i] + r] = p.Dsign[r];
+      int o = p.perm[r];
+      int code;
+      if (o < n)
+        code = xoff[i] + o;
+      else if (o < n + m)
+        code = -grow[i][o - n] - 2;
+      else
+        code = -1;
+      gsrc[voff[i] + r] = code;
+    }
+    if ((long long)N[i] * tsize <= 48 * 1024) {
+      has_small = true;
+      max_small = std::max(max_small, N[i]);
+    } else {
+      has_large = true;
+    }
+    kb += p.Kj.size();
+    lb += p.Li.size();
+    rb += p.Rk.size();
+  }
+  // refresh maps in global cone order
+  auto addk = [&](int i, int v) { return v < 0 ? -1 : (int)(v + (Kp[poff[i]])); };
+  for (int i = 0; i < B; ++i)
+    for (int v : prep[i].nn_pos) nn_pos.push_back(addk(i, v));
+  {
+    int dense_entries = 0;
+    for (int i = 0; i < B; ++i) {
+      auto &p = prep[i];
+      size_t sc = 0;
+      for (size_t k = 0; k < p.ctype.size(); ++k) {
+        if (p.ctype[k] != CLGPU_CONE_SOC) continue;
+        int st0 = p.socd_start[sc];
+        if (st0 < 0) {
+          socd_off.push_back(0);
+        } else {
+          socd_off.push_back(dense_entries);
+          int dim = p.cdim[k];
+          int t = dim * (dim + 1) / 2;
+          for (int e2 = 0; e2 < t; ++e2) {
+            socd_pos.push_back(addk(i, p.socd_pos[2 * (st0 + e2)]));
+            socd_pos.push_back(addk(i, p.socd_pos[2 * (st0 + e2) + 1]));
+          }
+          dense_entries += t;
+        }
+        socs_D.push_back(addk(i, p.socs_D[2 * sc]));
+        socs_D.push_back(addk(i, p.socs_D[2 * sc + 1]));
+        ++sc;
+      }
+      for (int v : p.socs_diag) socs_diag.push_back(addk(i, v));
+      for (int v : p.socs_uv) socs_uv.push_back(addk(i, v));
+      for (int v : p.exp_pos) exp_pos.push_back(addk(i, v));
+      for (int v : p.pow_pos) pow_pos.push_back(addk(i, v));
+    }
+    int psd_entries = 0;
+    for (int i = 0; i < B; ++i) {
+      auto &p = prep[i];
+      size_t pc = 0;
+      for (size_t k = 0; k < p.ctype.size(); ++k) {
+        if (p.ctype[k] != CLGPU_CONE_PSD) continue;
+        int st0 = p.psd_start[pc++];
+        int t = p.cdim[k] * (p.cdim[k] + 1) / 2;
+        int tt = t * (t + 1) / 2;
+        psdo.push_back(psd_entries);
+        for (int e2 = 0; e2 < tt; ++e2) {
+          psd_pos.push_back(addk(i, p.psd_pos[2 * (st0 + e2)]));
+          psd_pos.push_back(addk(i, p.psd_pos[2 * (st0 + e2) + 1]));
+        }
+        psd_entries += tt;
+      }
+    }
+  }
+  KKTMapDev &mp = h->map;
+  mp.nn_pos = A.upload(nn_pos);
+  mp.socd_off = A.upload(socd_off);
+  mp.socd_pos = A.upload(socd_pos);
+  mp.socs_diag = A.upload(socs_diag);
+  mp.socs_uv = A.upload(socs_uv);
+  mp.socs_D = A.upload(socs_D);
+  mp.exp_pos = A.upload(exp_pos);
+  mp.pow_pos = A.upload(pow_pos);
+  mp.psd_off = A.upload(psdo);
+  mp.psd_pos = A.upload(psd_pos);
+  KKTDev &kk = h->kk;
+  kk.B = B;
+  kk.N = A.upload(N);
+  kk.voff = A.upload(voff);
+  kk.poff = A.upload(poff);
+  kk.Kp = A.upload(Kp);
+  kk.Kj = A.upload(Kj);
+  kk.Kx = A.upload(Kx);
+  kk.Kdiag = A.upload(Kdiag);
+  kk.Dsign = A.upload(Dsign);
+  kk.gsrc = A.upload(gsrc);
+  kk.Lp = A.upload(Lp);
+  kk.Li = A.upload(Li);
+  kk.Rp = A.upload(Rp);
+  kk.Rk = A.upload(Rk);
+  kk.Rpos = A.upload(Rpos);
+  if (h->mixed) {
+    kk.Lx = A.alloc<float>((size_t)lnz);
+    kk.D = A.alloc<float>(VT);
+    kk.Dinv = A.alloc<float>(VT);
+    kk.yf = A.alloc<float>(VT);
+    kk.w = A.alloc<float>(VT);
+  } else {
+    kk.Lx = A.alloc<double>((size_t)lnz);
+    kk.D = A.alloc<double>(VT);
+    kk.Dinv = A.alloc<double>(VT);
+    kk.yf = A.alloc<double>(VT);
+    kk.w = A.alloc<double>(VT);
+  }
+  kk.max_small_N = max_small;
+  kk.has_small = has_small;
+  kk.has_large = has_large;
+  kk.b = A.alloc<double>(VT);
+  kk.x = A.alloc<double>(VT);
+  kk.e = A.alloc<double>(VT);
+  kk.dx = A.alloc<double>(VT);
+  // ---------------- vectors and scalars
+  Dev &dv = h->dv;
+  dv.B = B;
+  dv.nx = nx;
+  dv.mz = mz;
+  dv.Pp = A.upload(Pp);
+  dv.Pj = A.upload(Pj);
+  dv.Px = A.upload(Pxv);
+  dv.Ap = A.upload(Ap);
+  dv.Aj = A.upload(Aj);
+  dv.Ax = A.upload(Axv);
+  dv.Atp = A.upload(Atp);
+  dv.Atj = A.upload(Atj);
+  dv.Atx = A.upload(Atxv);
+  dv.q = A.upload(q);
+  dv.negq = A.upload(negq);
+  dv.b = A.upload(b);
+  dv.d = A.upload(dd);
+  dv.dinv = A.upload(ddinv);
+  dv.e = A.upload(ee);
+  dv.einv = A.upload(eeinv);
+  dv.col_inst = A.upload(col_inst);
+  dv.row_inst = cs.row_inst;
+  double **xv[] = {&dv.x, &dv.px, &dv.rhs_x, &dv.dx, &dv.rx, &dv.rx_inf, &dv.Px_, &dv.x1,
+                   &dv.x2, &dv.zerox};
+  for (auto p : xv) *p = A.alloc<double>(nx);
+  double **zv[] = {&dv.s, &dv.z, &dv.ps, &dv.pz, &dv.rhs_s, &dv.rhs_z, &dv.ds, &dv.dz,
+                   &dv.rz, &dv.rz_inf, &dv.z1, &dv.z2, &dv.workz, &dv.wconic, &dv.zeroz};
+  for (auto p : zv) *p = A.alloc<double>(mz);
+  dv.S = A.alloc<double>((size_t)NUM_SCALARS * B);
+  dv.I = A.alloc<int>((size_t)NUM_INTS * B);
+  dv.active = A.alloc<int>(B);
+  dv.counter = A.alloc<int>(4);
+  cs.inst_active = dv.active;
+  h->ic.degree = A.upload(deg);
+  h->ic.sym = A.upload(sym);
+  cs.inst_sym = h->ic.sym;
+  h->d_reset = A.alloc<int>(B);
+  // per-instance constants for init
+  h->d_c = A.upload(c);
+  h->d_normq = A.upload(nq);
+  h->d_normb = A.upload(nb);
+  h->d_pnnz = A.upload(pnnz);
+  // output map (user order)
+  std::vector<int> zmap(mz), zinst(mz);
+  for (int i = 0; i < B; ++i)
+    for (int lr = 0; lr < prep[i].m; ++lr) {
+      int ur = prep[i].user_row_of[lr];
+      zmap[moff[i] + ur] = grow[i][lr];
+      zinst[moff[i] + ur] = i;
+    }
+  h->d_zmap = A.upload(zmap);
+  h->d_zinst = A.upload(zinst);
+  h->d_out = A.alloc<double>((size_t)nx + 2 * (size_t)mz);
+  h->h_n.resize(B);
+  h->h_m.resize(B);
+  for (int i = 0; i < B; ++i) {
+    h->h_n[i] = prep[i].n;
+    h->h_m[i] = prep[i].m;
+  }
+  cudaMallocHost(&h->h_counter, 4 * sizeof(int));
+  if (A.err != cudaSuccess) return -1000 - (int)A.err;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return -1000 - (int)e;
+  return 0;
+}
+
+extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
+                                   const clgpu_settings *settings, clgpu_solver **out) {
+  if (!probs || nprob < 1 || !out) return -1;
+  auto *h = new clgpu_solver();
+  if (settings)
+    h->st = *settings;
+  else
+    clgpu_default_settings(&h->st);
+  h->mixed = h->st.direct_solve_method == CLGPU_METHOD_MIXED;
+  if (h->mixed) h->st.static_regularization_constant = std::sqrt(1.1920928955078125e-07);
+  SetupOptions opt;
+  opt.soc_threshold = h->st.soc_threshold;
+  opt.equilibrate_enable = h->st.equilibrate_enable;
+  opt.equilibrate_max_iter = h->st.equilibrate_max_iter;
+  opt.equilibrate_min_scaling = h->st.equilibrate_min_scaling;
+  opt.equilibrate_max_scaling = h->st.equilibrate_max_scaling;
+  std::vector<Prepared> prep(nprob);
+  std::vector<int> okv(nprob, 0);
+  int nth = h->st.setup_threads > 0 ? h->st.setup_threads
+                                    : (int)std::max(1u, std::thread::hardware_concurrency());
+  nth = std::min(nth, nprob);
+  {
+    std::vector<std::thread> th;
+    std::atomic<int> next{0};
+    for (int t = 0; t < nth; ++t)
+      th.emplace_back([&]() {
+        while (true) {
+          int i = next.fetch_add(1);
+          if (i >= nprob) break;
+          okv[i] = prepare_instance(probs[i], opt, prep[i]) ? 1 : 0;
+        }
+      });
+    for (auto &t : th) t.join();
+  }
+  for (int i = 0; i < nprob; ++i)
+    if (!okv[i]) {
+      if (h->st.verbose)
+        std::fprintf(stderr, "clgpu: instance %d rejected: %s\n", i, prep[i].error.c_str());
+      delete h;
+      return -2;
+    }
+  int rc = build_batch(h, prep);
+  if (rc != 0) {
+    delete h;
+    return rc;
+  }
+  h->lp.static_reg = h->st.static_regularization_enable;
+  h->lp.static_c = h->st.static_regularization_constant;
+  h->lp.static_prop = h->st.static_regularization_proportional;
+  h->lp.dyn_reg = h->st.dynamic_regularization_enable;
+  h->lp.dyn_eps = h->st.dynamic_regularization_eps;
+  h->lp.dyn_delta = h->st.dynamic_regularization_delta;
+  h->lp.ir_enable = h->st.iterative_refinement_enable;
+  h->lp.ir_maxiter = h->st.iterative_refinement_max_iter;
+  h->lp.ir_reltol = h->st.iterative_refinement_reltol;
+  h->lp.ir_abstol = h->st.iterative_refinement_abstol;
+  h->lp.ir_stopratio = h->st.iterative_refinement_stop_ratio;
+  h->sd = make_sd(h->st);
+  h->info.assign(nprob, clgpu_info{});
+  *out = h;
+  return 0;
+}
+
+// ------------------------------------------------------------ solve phases
+struct Phase {
+  clgpu_solver *h;
+  cudaStream_t st;
+  Dev &d() { return h->dv; }
+  void mask(int mode) {
+    k_set_mask<<<nblk(h->B), TB, 0, st>>>(h->dv, h->ic, mode);
+    h->launches++;
+  }
+  void zero(int f0, int nf, double v = 0.0) {
+    k_zero_fields<<<nblk((long long)nf * h->B), TB, 0, st>>>(h->dv, f0, nf, v);
+    h->launches++;
+  }
+  // kkt_update!: Hs refresh, regularise + refactor, constant rhs solve
+  void kkt_update() {
+    cones_refresh_kkt(h->cs, h->map, h->kk.Kx, st);
+    int *ok = h->dv.I + I_KKT_OK * h->B;
+    ldl_factor(h->kk, h->mixed, h->lp, h->dv.active, ok, h->dv.S + F_KKT_EPS * h->B, st);
+    ldl_solve(h->kk, h->mixed, h->lp, h->dv.active, h->dv.negq, h->dv.b, h->dv.x2, h->dv.z2,
+              ok, st);
+    h->launches += 12;
+  }
+  // kkt_solve! (kktsystem_gpu.jl:139-227)
+  void kkt_solve(bool affine) {
+    Dev &dv = h->dv;
+    const double *dsc;
+    if (affine) {
+      dsc = dv.s;
+    } else {
+      cones_ds_from_dz_offset(h->cs, dv.wconic, dv.rhs_s, dv.z, st);
+      dsc = dv.wconic;
+    }
+    k_workz<<<nblk(dv.mz), TB, 0, st>>>(dv, dsc);
+    int *ok = dv.I + I_KKT_OK * h->B;
+    ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.rhs_x, dv.workz, dv.x1, dv.z1, ok, st);
+    zero(F_DOT_Q_X1, 1);
+    zero(F_DOT_B_Z1, 1);
+    zero(F_DOT_XI_PX1, 1);
+    zero(F_DOT_Q_X2, 1);
+    zero(F_DOT_B_Z2, 1);
+    zero(F_QF1, 2);
+    k_tau_dots_x<<<nblk(dv.nx), TB, 0, st>>>(dv);
+    k_tau_dots_z<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    k_tau_solve<<<nblk(h->B), TB, 0, st>>>(dv);
+    k_lhs_xz<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
+    cones_mul_Hs(h->cs, dv.ds, dv.dz, st);
+    k_lhs_s<<<nblk(dv.mz), TB, 0, st>>>(dv, dsc);
+    k_lhs_kappa<<<nblk(h->B), TB, 0, st>>>(dv);
+    h->launches += 30;
+  }
+  void step_length(bool combined, int out_field) {
+    Dev &dv = h->dv;
+    k_step_prep<<<nblk(h->B), TB, 0, st>>>(dv);
+    cones_step_length_sym(h->cs, dv.dz, dv.ds, dv.z, dv.s, dv.S + F_STEP_SYM * h->B, st);
+    k_step_mid<<<nblk(h->B), TB, 0, st>>>(dv, h->ic, h->st.max_step_fraction);
+    if (h->any_asym)
+      cones_step_length_asym(h->cs, dv.dz, dv.ds, dv.z, dv.s, dv.S + F_STEP_SYM * h->B,
+                             dv.S + F_STEP * h->B, h->st.linesearch_backtrack_step,
+                             h->st.min_terminate_step_length, st);
+    k_step_final<<<nblk(h->B), TB, 0, st>>>(dv, combined ? 1 : 0, h->st.max_step_fraction,
+                                           out_field);
+    h->launches += 8;
+  }
+  void residuals() {
+    Dev &dv = h->dv;
+    zero(F_DOT_QX, 4);   // QX, BZ, SZ, XPX
+    zero(F_NRM_X, 8);    // the norm accumulators
+    k_resid_x<<<nblk(dv.nx), TB, 0, st>>>(dv);
+    k_resid_z<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    h->launches += 4;
+  }
+  int read_counter(int which) {
+    cudaMemcpyAsync(h->h_counter, h->dv.counter, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return h->h_counter[which];
+  }
+};
+
+extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto t0 = std::chrono::steady_clock::now();
+  Phase P{h, st};
+  Dev &dv = h->dv;
+  const int B = h->B;
+  h->launches = 0;
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0, st);
+  // (re)initialise every per-instance scalar; solve! may be called repeatedly
+  k_init_state<<<nblk(B), TB, 0, st>>>(dv, h->d_c, h->d_normq, h->d_normb, h->d_pnnz);
+  k_set_mask<<<nblk(B), TB, 0, st>>>(dv, h->ic, M_ALL_UNDONE);
+  // solver_default_start! (solver.jl:425-446)
+  if (h->any_sym) {
+    P.mask(M_SYM);
+    cones_set_identity_scaling(h->cs, st);
+    P.kkt_update();
+    // QP instances: [x; z] = K \ [-q; b], s = -z
+    P.mask(M_SYM_QP);
+    ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.negq, dv.b, dv.x, dv.z,
+              dv.I + I_KKT_OK * B, st);
+    k_s_from_neg_z_masked<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    // LP instances: [x; -s] = K \ [0; b], then z from K \ [-q; 0]
+    P.mask(M_SYM_LP);
+    ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.zerox, dv.b, dv.x, dv.s,
+              dv.I + I_KKT_OK * B, st);
+    k_negate_s_masked<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.negq, dv.zeroz, nullptr, dv.z,
+              dv.I + I_KKT_OK * B, st);
+    // shift s (primal) and z (dual) into the cone interior
+    P.mask(M_SYM);
+    for (int pd = 0; pd < 2; ++pd) {
+      double *v = pd == 0 ? dv.s : dv.z;
+      k_zero_fields<<<nblk(B), TB, 0, st>>>(dv, F_MARGIN_MIN, 1, kDMax);
+      P.zero(F_MARGIN_SUM, 1);
+      cones_margins(h->cs, v, pd, dv.S + F_MARGIN_MIN * B, dv.S + F_MARGIN_SUM * B, st);
+      k_shift_amounts<<<nblk(B), TB, 0, st>>>(dv, h->ic, F_MARGIN_MIN, F_MARGIN_SUM, F_TAU_NUM,
+                                              F_TAU_DEN);
+      cones_scaled_unit_shift(h->cs, v, dv.S + F_TAU_NUM * B, pd, st);
+      cones_scaled_unit_shift(h->cs, v, dv.S + F_TAU_DEN * B, pd, st);
+    }
+    k_set_tau_kappa_one<<<nblk(B), TB, 0, st>>>(dv);
+  }
+  if (h->any_asym) {
+    P.mask(M_ASYM);
+    cones_unit_initialization(h->cs, dv.z, dv.s, st);
+    k_zero_x_masked<<<nblk(dv.nx), TB, 0, st>>>(dv);
+    k_set_tau_kappa_one<<<nblk(B), TB, 0, st>>>(dv);
+  }
+  // ----------------------------------------------------------- main loop
+  int passes = 0;
+  const int max_passes = 4 * (h->st.max_iter + 5);
+  while (passes < max_passes) {
+    ++passes;
+    double elapsed =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    P.mask(M_PASS);
+    P.residuals();
+    k_info_termination<<<nblk(B), TB, 0, st>>>(dv, h->ic, h->sd, elapsed, h->d_reset);
+    k_reset_vars<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_reset);
+    P.mask(M_PASS);
+    // update_scaling
+    cones_update_scaling(h->cs, dv.s, dv.z, dv.S + F_MU * B, dv.I + I_SCALING * B,
+                         dv.I + I_SCALE_OK * B, st);
+    k_after_scaling<<<nblk(B), TB, 0, st>>>(dv);
+    P.mask(M_PASS);
+    // KKT update and affine step
+    P.kkt_update();
+    k_affine_rhs<<<nblk(std::max(std::max(dv.nx, dv.mz), B)), TB, 0, st>>>(dv);
+    cones_affine_ds(h->cs, dv.rhs_s, dv.s, st);
+    P.kkt_solve(true);
+    P.step_length(false, F_ALPHA_AFF);
+    k_combined_scalars<<<nblk(B), TB, 0, st>>>(dv);
+    k_combined_pre<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
+    cones_combined_ds_shift(h->cs, dv.rhs_z, dv.dz, dv.ds, dv.S + F_SIGMA_MU * B, st);
+    k_combined_post<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    P.kkt_solve(false);
+    k_check_numerical<<<nblk(B), TB, 0, st>>>(dv, h->ic);
+    P.mask(M_PASS);
+    P.step_length(true, F_ALPHA);
+    if (h->any_asym) {
+      cudaMemsetAsync(dv.counter + 1, 0, sizeof(int), st);
+      k_bt_setup<<<nblk(B), TB, 0, st>>>(dv, h->ic);
+      if (P.read_counter(1) > 0) {
+        P.mask(M_BT);
+        for (int j = 0; j < 50; ++j) {
+          P.zero(F_TAU_NUM, 1);
+          P.zero(F_BARRIER, 1);
+          k_dot_shifted<<<nblk(dv.mz), TB, 0, st>>>(dv);
+          k_bt_central<<<nblk(B), TB, 0, st>>>(dv, h->ic);
+          cones_barrier(h->cs, dv.z, dv.s, dv.dz, dv.ds, dv.S + F_ALPHA * B,
+                        dv.I + I_BT_ACTIVE * B, dv.S + F_BARRIER * B, st);
+          cudaMemsetAsync(dv.counter + 1, 0, sizeof(int), st);
+          k_bt_check<<<nblk(B), TB, 0, st>>>(dv, h->st.linesearch_backtrack_step);
+          P.mask(M_BT);
+          if (P.read_counter(1) == 0) break;
+        }
+        P.mask(M_PASS);
+      }
+    }
+    k_check_small_step<<<nblk(B), TB, 0, st>>>(dv, h->ic, h->sd);
+    P.mask(M_PASS);
+    k_add_step<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
+    k_add_step_scalars<<<nblk(B), TB, 0, st>>>(dv);
+    cudaMemsetAsync(dv.counter, 0, sizeof(int), st);
+    k_count_running<<<nblk(B), TB, 0, st>>>(dv);
+    h->launches += 25;
+    if (P.read_counter(0) == 0) break;
+  }
+  h->passes = passes;
+  // post-process
+  k_post_status<<<nblk(B), TB, 0, st>>>(dv, h->sd);
+  double *ox = h->d_out, *os = ox + dv.nx, *oz = os + dv.mz;
+  k_unscale<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_zmap, h->d_zinst, ox, os, oz);
+  cudaEventRecord(ev1, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return -1000 - (int)e;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return -1000 - (int)e;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  h->last_ms = ms;
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  // copy results back
+  std::vector<double> S((size_t)NUM_SCALARS * B);
+  std::vector<int> I((size_t)NUM_INTS * B);
+  cudaMemcpy(S.data(), dv.S, S.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(I.data(), dv.I, I.size() * sizeof(int), cudaMemcpyDeviceToHost);
+  h->sol.resize((size_t)dv.nx + 2 * (size_t)dv.mz);
+  cudaMemcpy(h->sol.data(), h->d_out, h->sol.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (int i = 0; i < B; ++i) {
+    clgpu_info &inf = h->info[i];
+    auto s = [&](int f) { return S[(size_t)f * B + i]; };
+    inf.status = I[(size_t)I_STATUS * B + i];
+    inf.iterations = I[(size_t)I_ITER * B + i];
+    inf.cost_primal = s(F_COST_P);
+    inf.cost_dual = s(F_COST_D);
+    bool infeas = inf.status == ST_PRIMAL_INFEASIBLE || inf.status == ST_DUAL_INFEASIBLE ||
+                  inf.status == ST_ALMOST_PRIMAL_INFEASIBLE ||
+                  inf.status == ST_ALMOST_DUAL_INFEASIBLE;
+    inf.obj_val = infeas ? NAN : inf.cost_primal;
+    inf.obj_val_dual = infeas ? NAN : inf.cost_dual;
+    inf.res_primal = s(F_RES_P);
+    inf.res_dual = s(F_RES_D);
+    inf.res_primal_inf = s(F_RES_PINF);
+    inf.res_dual_inf = s(F_RES_DINF);
+    inf.gap_abs = s(F_GAP_ABS);
+    inf.gap_rel = s(F_GAP_REL);
+    inf.ktratio = s(F_KTRATIO);
+    inf.mu = s(F_MU);
+    inf.sigma = s(F_SIGMA);
+    inf.step_length = s(F_ALPHA);
+    inf.solve_time = elapsed;
+  }
+  h->solved = true;
+  return 0;
+}
+
+extern "C" int clgpu_solver_get_info(clgpu_solver *h, int inst, clgpu_info *info) {
+  if (!h || !info || inst < 0 || inst >= h->B) return -1;
+  *info = h->info[inst];
+  return 0;
+}
+
+extern "C" int clgpu_solver_get_solution(clgpu_solver *h, int inst, double *x, double *s,
+                                         double *z) {
+  if (!h || inst < 0 || inst >= h->B || !h->solved) return -1;
+  const double *ox = h->sol.data(), *os = ox + h->nx, *oz = os + h->mz;
+  int n = h->h_n[inst], m = h->h_m[inst];
+  if (x) std::memcpy(x, ox + h->h_xoff[inst], n * sizeof(double));
+  if (s) std::memcpy(s, os + h->h_moff[inst], m * sizeof(double));
+  if (z) std::memcpy(z, oz + h->h_moff[inst], m * sizeof(double));
+  return 0;
+}
+
+extern "C" int clgpu_solver_get_solutions(clgpu_solver *h, double *x, double *s, double *z,
+                                          clgpu_info *info) {
+  if (!h || !h->solved) return -1;
+  const double *ox = h->sol.data(), *os = ox + h->nx, *oz = os + h->mz;
+  if (x) std::memcpy(x, ox, h->nx * sizeof(double));
+  if (s) std::memcpy(s, os, h->mz * sizeof(double));
+  if (z) std::memcpy(z, oz, h->mz * sizeof(double));
+  if (info) std::memcpy(info, h->info.data(), h->B * sizeof(clgpu_info));
+  return 0;
+}
+
+extern "C" long long clgpu_solver_device_bytes(const clgpu_solver *h) {
+  return h ? h->arena.bytes : -1;
+}
+extern "C" long long clgpu_solver_launch_count(const clgpu_solver *h) {
+  return h ? h->launches : -1;
+}
+extern "C" int clgpu_solver_set_profiling(clgpu_solver *h, int enable) {
+  if (!h) return -1;
+  h->profiling = enable != 0;
+  return 0;
+}
+extern "C" int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
+                                        double *ms_factor, double *ms_solve, double *ms_cones,
+                                        double *ms_residual, int *passes) {
+  if (!h) return -1;
+  if (ms_total) *ms_total = h->last_ms;
+  if (ms_factor) *ms_factor = h->prof[0];
+  if (ms_solve) *ms_solve = h->prof[1];
+  if (ms_cones) *ms_cones = h->prof[2];
+  if (ms_residual) *ms_residual = h->prof[3];
+  if (passes) *passes = h->passes;
+  return 0;
+}
+extern "C" int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,
+                                      const double *b) {
+  (void)h;
+  (void)inst;
+  (void)q;
+  (void)b;
+  return -10;  // not implemented yet
+}
+extern "C" int clgpu_solver_destroy(clgpu_solver *h) {
+  if (!h) return -1;
+  delete h;
+  return 0;
+}

@@ -1,0 +1,59 @@
+// ldl.cuh -- batched sparse LDL^T of the quasi-definite KKT systems.
+//
+// Stands in for the reference's cuDSS calls (src/kktsolvers/gpu/
+// directldl_cudss.jl:30-59 and directldl_mixed_cudss.jl:42-78), which are not
+// available in this environment.  The host computes a fill-reducing ordering
+// and the symbolic factorisation once per instance (setup.cpp); the device
+// refactors every IPM iteration and solves with iterative refinement
+// (kktsolver_directldl_gpu.jl:300-409).
+#pragma once
+#include "common.cuh"
+
+namespace clgpu {
+
+struct KKTDev {
+  int B;
+  const int *N;     // [B] KKT dimension of each instance
+  const int *voff;  // [B+1] offsets of per-instance vectors (sum of N)
+  const int *poff;  // [B]   offsets into the (N+1)-long pointer arrays
+  // permuted full KKT (both triangles), CSR with global positions
+  const int *Kp, *Kj;
+  double *Kx;
+  const int *Kdiag;          // [sum N] position of the diagonal of each row
+  const signed char *Dsign;  // [sum N] +1 / -1
+  const int *gsrc;           // [sum N] rhs gather / solution scatter codes
+  // factor L (strict lower, CSC with global positions) and D
+  const int *Lp, *Li;
+  void *Lx, *D, *Dinv;  // double or float (mixed precision)
+  // row pattern of L: for column j the list (k, pos of L(j,k))
+  const int *Rp, *Rk, *Rpos;
+  // scratch (global, per instance, sum N each)
+  int max_small_N;       // largest N among single-warp (shared memory) instances
+  int has_small, has_large;
+  void *w;        // factor accumulator (factor type)
+  void *yf;       // solve work (factor type)
+  double *b, *x, *e, *dx;
+};
+
+struct LDLParams {
+  int static_reg;
+  double static_c, static_prop;
+  int dyn_reg;
+  double dyn_eps, dyn_delta;
+  int ir_enable, ir_maxiter;
+  double ir_reltol, ir_abstol, ir_stopratio;
+};
+
+// numeric refactorisation of every instance with run[i] != 0; sets
+// ok[i] = 0 if a pivot is not finite; eps_out[i] receives the static
+// regulariser used (diagonal_regularizer of the reference)
+void ldl_factor(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
+                int *ok, double *eps_out, cudaStream_t st);
+// solve K [lx; lz; *] = [rx; rz; 0] with iterative refinement for every
+// instance with run[i] != 0.  rx/lx are indexed by global x index, rz/lz by
+// global s/z row; lx or lz may be null.  ok[i] cleared on non-finite results.
+void ldl_solve(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
+               const double *rx, const double *rz, double *lx, double *lz,
+               int *ok, cudaStream_t st);
+
+}  // namespace clgpu

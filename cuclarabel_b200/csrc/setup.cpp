@@ -1,0 +1,607 @@
+// setup.cpp -- host-side preparation of one problem instance.
+//
+// Follows the reference's GPU setup chain (src/solver.jl:129-195):
+//   gpu_data_copy!           P upper triangle symmetrised to full (:618-630)
+//   DefaultProblemDataGPU    b capped at 1e20, norms of q and b
+//                            (src/problemdata.jl:73-136)
+//   data_equilibrate! (GPU)  Ruiz scaling with full-P row norms
+//                            (src/problemdata.jl:286-374, mathutils_gpu.jl)
+//   CompositeConeGPU         cones ordered zero, nonneg, soc, exp, pow, psd
+//                            (compositecone_type_gpu.jl:72-216).  Unlike the
+//                            reference, unsorted cone lists are accepted and
+//                            placed type-major; the solution is returned in
+//                            the caller's row order.
+//   _assemble_full_kkt_matrix  full KKT [P A'; A -Hs] with two extra rows and
+//                            columns per second-order cone above the
+//                            threshold (directgpu_kkt_assembly.jl:69-170)
+// plus the ordering and symbolic factorisation that cuDSS's analysis phase
+// performs in the reference (directldl_cudss.jl:20-23).
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <set>
+
+#include "setup.hpp"
+
+namespace clgpu {
+
+static inline int tri(int k) { return k * (k + 1) / 2; }
+static inline double clip(double s, double lo, double hi) {
+  return s < lo ? lo : (s > hi ? hi : s);
+}
+
+// ---------------------------------------------------------------- ordering
+// Minimum-degree ordering on the explicit elimination graph.  Each step
+// eliminates a vertex of smallest current degree and turns its neighbourhood
+// into a clique.  Vertices whose initial degree exceeds 10*sqrt(n) are
+// treated as dense and ordered last (as AMD does).
+std::vector<int> amd_order(int n, std::vector<std::vector<int>> &adj) {
+  for (auto &a : adj) {
+    std::sort(a.begin(), a.end());
+    a.erase(std::unique(a.begin(), a.end()), a.end());
+  }
+  double dense_thr = std::max(16.0, 10.0 * std::sqrt((double)n));
+  std::vector<char> dense(n, 0), done(n, 0);
+  std::set<std::pair<int, int>> pq;
+  for (int i = 0; i < n; ++i) {
+    if ((double)adj[i].size() > dense_thr)
+      dense[i] = 1;
+    else
+      pq.insert({(int)adj[i].size(), i});
+  }
+  // dense vertices are dropped from the graph during the elimination
+  if (std::any_of(dense.begin(), dense.end(), [](char c) { return c != 0; }))
+    for (int i = 0; i < n; ++i) {
+      if (dense[i]) continue;
+      auto &a = adj[i];
+      size_t w = 0;
+      for (size_t r = 0; r < a.size(); ++r)
+        if (!dense[a[r]]) a[w++] = a[r];
+      if (w != a.size()) {
+        pq.erase({(int)a.size(), i});
+        a.resize(w);
+        pq.insert({(int)a.size(), i});
+      }
+    }
+  std::vector<int> order;
+  order.reserve(n);
+  std::vector<int> nb, tmp;
+  while (!pq.empty()) {
+    int v = pq.begin()->second;
+    pq.erase(pq.begin());
+    done[v] = 1;
+    order.push_back(v);
+    nb.clear();
+    for (int u : adj[v])
+      if (!done[u]) nb.push_back(u);
+    for (int u : nb) {
+      pq.erase({(int)adj[u].size(), u});
+      tmp.clear();
+      std::set_union(adj[u].begin(), adj[u].end(), nb.begin(), nb.end(),
+                     std::back_inserter(tmp));
+      auto &a = adj[u];
+      a.clear();
+      for (int w : tmp)
+        if (w != u && !done[w]) a.push_back(w);
+      pq.insert({(int)a.size(), u});
+    }
+    std::vector<int>().swap(adj[v]);
+  }
+  for (int i = 0; i < n; ++i)
+    if (dense[i]) order.push_back(i);
+  return order;
+}
+
+// ---------------------------------------------------------------- helpers
+static void csc_transpose(const HostCSC &A, HostCSC &T) {
+  T.m = A.n;
+  T.n = A.m;
+  T.p.assign(A.m + 1, 0);
+  for (int k = 0; k < A.p[A.n]; ++k) T.p[A.i[k] + 1]++;
+  for (int r = 0; r < A.m; ++r) T.p[r + 1] += T.p[r];
+  std::vector<int> next(T.p.begin(), T.p.end() - 1);
+  T.i.assign(A.p[A.n], 0);
+  T.x.assign(A.p[A.n], 0.0);
+  for (int j = 0; j < A.n; ++j)
+    for (int k = A.p[j]; k < A.p[j + 1]; ++k) {
+      int q = next[A.i[k]]++;
+      T.i[q] = j;
+      T.x[q] = A.x[k];
+    }
+}
+
+bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared &out) {
+  const int n = pb.n, m = pb.m;
+  out = Prepared();
+  out.n = n;
+  out.m = m;
+  if (n < 0 || m < 0) {
+    out.error = "negative dimensions";
+    return false;
+  }
+  // ---- cones: sizes and type-major order
+  int rows = 0;
+  std::vector<int> user_start(pb.ncones);
+  for (int c = 0; c < pb.ncones; ++c) {
+    int t = pb.cone_types[c], d = pb.cone_dims[c];
+    int nv;
+    if (t == CLGPU_CONE_EXP || t == CLGPU_CONE_POW)
+      nv = 3;
+    else if (t == CLGPU_CONE_PSD)
+      nv = tri(d);
+    else if (t >= 0 && t <= 5)
+      nv = d;
+    else {
+      out.error = "unknown cone type";
+      return false;
+    }
+    if (d < 0) {
+      out.error = "negative cone dimension";
+      return false;
+    }
+    if (t == CLGPU_CONE_POW) {
+      double a = pb.cone_params ? pb.cone_params[c] : 0.0;
+      if (!(a > 0 && a < 1)) {
+        out.error = "power cone alpha must lie in (0,1)";
+        return false;
+      }
+    }
+    user_start[c] = rows;
+    rows += nv;
+  }
+  if (rows != m) {
+    out.error = "Constraint dimensions inconsistent with size of cones.";
+    return false;
+  }
+  out.type_rows.assign(6, 0);
+  out.type_cones.assign(6, 0);
+  out.user_row_of.assign(m, 0);
+  {
+    int lr = 0;
+    for (int t = 0; t < 6; ++t) {
+      for (int c = 0; c < pb.ncones; ++c) {
+        if (pb.cone_types[c] != t) continue;
+        int d = pb.cone_dims[c];
+        int nv = (t == 3 || t == 4) ? 3 : (t == 5 ? tri(d) : d);
+        if (t == CLGPU_CONE_PSD && d == 0) continue;  // empty PSD cone: no rows
+        out.ctype.push_back(t);
+        out.cdim.push_back(t == 3 || t == 4 ? 3 : d);
+        out.cparam.push_back(pb.cone_params ? pb.cone_params[c] : 0.0);
+        out.cstart.push_back(lr);
+        for (int k = 0; k < nv; ++k) out.user_row_of[lr + k] = user_start[c] + k;
+        out.type_rows[t] += nv;
+        out.type_cones[t] += 1;
+        lr += nv;
+        if (t == 3 || t == 4) out.symmetric = false;
+        out.degree += (t == 0) ? 0 : (t == 2 ? 1 : (t == 3 || t == 4 ? 3 : d));
+      }
+    }
+  }
+  // ---- data: triu P -> full; A; q; b (capped)
+  HostCSC Pu;
+  Pu.m = Pu.n = n;
+  Pu.p.assign(n + 1, 0);
+  for (int j = 0; j < n; ++j) {
+    for (int k = pb.Pp[j]; k < pb.Pp[j + 1]; ++k)
+      if (pb.Pi[k] <= j) {
+        Pu.i.push_back(pb.Pi[k]);
+        Pu.x.push_back(pb.Px[k]);
+      }
+    Pu.p[j + 1] = (int)Pu.i.size();
+  }
+  out.p_nnz = Pu.p[n];
+  {
+    // full = triu + strict triu transposed
+    std::vector<std::vector<std::pair<int, double>>> cols(n);
+    for (int j = 0; j < n; ++j)
+      for (int k = Pu.p[j]; k < Pu.p[j + 1]; ++k) {
+        int i = Pu.i[k];
+        cols[j].push_back({i, Pu.x[k]});
+        if (i != j) cols[i].push_back({j, Pu.x[k]});
+      }
+    HostCSC &F = out.Pfull;
+    F.m = F.n = n;
+    F.p.assign(n + 1, 0);
+    for (int j = 0; j < n; ++j) {
+      std::sort(cols[j].begin(), cols[j].end());
+      for (auto &pr : cols[j]) {
+        F.i.push_back(pr.first);
+        F.x.push_back(pr.second);
+      }
+      F.p[j + 1] = (int)F.i.size();
+    }
+  }
+  out.A.m = m;
+  out.A.n = n;
+  out.A.p.assign(pb.Ap, pb.Ap + n + 1);
+  out.A.i.assign(pb.Ai, pb.Ai + pb.Ap[n]);
+  out.A.x.assign(pb.Ax, pb.Ax + pb.Ap[n]);
+  for (int k = 0; k < out.A.p[n]; ++k)
+    if (out.A.i[k] < 0 || out.A.i[k] >= m) {
+      out.error = "A row index out of range";
+      return false;
+    }
+  out.q.assign(pb.q, pb.q + n);
+  out.b.assign(pb.b, pb.b + m);
+  for (auto &v : out.b) v = std::min(v, 1e20);
+  out.normq = 0;
+  for (double v : out.q) out.normq = std::max(out.normq, std::fabs(v));
+  out.normb = 0;
+  for (double v : out.b) out.normb = std::max(out.normb, std::fabs(v));
+  // ---- Ruiz equilibration (GPU path semantics)
+  std::vector<double> &d = out.d, &e = out.e;
+  d.assign(n, 1.0);
+  e.assign(m, 1.0);
+  out.c = 1.0;
+  HostCSC &P = out.Pfull, &A = out.A;
+  auto scale_data = [&](const std::vector<double> *dw, const std::vector<double> &ew) {
+    if (dw) {
+      for (int j = 0; j < n; ++j)
+        for (int k = P.p[j]; k < P.p[j + 1]; ++k) P.x[k] *= (*dw)[P.i[k]] * (*dw)[j];
+      for (int j = 0; j < n; ++j)
+        for (int k = A.p[j]; k < A.p[j + 1]; ++k) A.x[k] *= ew[A.i[k]] * (*dw)[j];
+      for (int i = 0; i < n; ++i) out.q[i] *= (*dw)[i];
+    } else {
+      for (int k = 0; k < A.p[n]; ++k) A.x[k] *= ew[A.i[k]];
+    }
+    for (int i = 0; i < m; ++i) out.b[i] *= ew[i];
+  };
+  if (opt.equilibrate_enable) {
+    double smin = opt.equilibrate_min_scaling, smax = opt.equilibrate_max_scaling;
+    std::vector<double> dw(n), ew(m);
+    for (int it = 0; it < opt.equilibrate_max_iter; ++it) {
+      std::fill(dw.begin(), dw.end(), 0.0);
+      std::fill(ew.begin(), ew.end(), 0.0);
+      for (int j = 0; j < n; ++j)
+        for (int k = P.p[j]; k < P.p[j + 1]; ++k)
+          dw[j] = std::max(dw[j], std::fabs(P.x[k]));
+      for (int j = 0; j < n; ++j)
+        for (int k = A.p[j]; k < A.p[j + 1]; ++k) {
+          double t = std::fabs(A.x[k]);
+          dw[j] = std::max(dw[j], t);
+          ew[A.i[k]] = std::max(ew[A.i[k]], t);
+        }
+      for (auto &v : dw) v = (v == 0.0) ? 1.0 : v;
+      for (auto &v : ew) v = (v == 0.0) ? 1.0 : v;
+      for (auto &v : dw) v = 1.0 / std::sqrt(v);
+      for (auto &v : ew) v = 1.0 / std::sqrt(v);
+      for (int i = 0; i < n; ++i) dw[i] = clip(dw[i], smin / d[i], smax / d[i]);
+      for (int i = 0; i < m; ++i) ew[i] = clip(ew[i], smin / e[i], smax / e[i]);
+      scale_data(&dw, ew);
+      for (int i = 0; i < n; ++i) d[i] *= dw[i];
+      for (int i = 0; i < m; ++i) e[i] *= ew[i];
+      // mean of the row norms of the (full) scaled P
+      std::fill(dw.begin(), dw.end(), 0.0);
+      for (int j = 0; j < n; ++j)
+        for (int k = P.p[j]; k < P.p[j + 1]; ++k)
+          dw[j] = std::max(dw[j], std::fabs(P.x[k]));
+      double mean = 0;
+      for (double v : dw) mean += v;
+      mean = n > 0 ? mean / n : 0.0;
+      double inf_q = 0;
+      for (double v : out.q) inf_q = std::max(inf_q, std::fabs(v));
+      if (mean != 0.0 && inf_q != 0.0) {
+        double sc = std::max(inf_q, mean);
+        double ct = clip(1.0 / sc, smin / out.c, smax / out.c);
+        for (auto &v : P.x) v *= ct;
+        for (auto &v : out.q) v *= ct;
+        out.c *= ct;
+      }
+    }
+    // rectify_equilibration!: cones without elementwise scaling get
+    // delta = mean(e)/e over the cone (coneops_defaults.jl:32-44)
+    bool any = false;
+    std::vector<double> delta(m, 1.0);
+    for (size_t c = 0; c < out.ctype.size(); ++c) {
+      int t = out.ctype[c];
+      if (t == CLGPU_CONE_ZERO || t == CLGPU_CONE_NONNEG) continue;
+      int nv = (t == 3 || t == 4) ? 3 : (t == 5 ? tri(out.cdim[c]) : out.cdim[c]);
+      if (nv == 0) continue;
+      any = true;
+      double mu = 0;
+      for (int k = 0; k < nv; ++k) mu += e[out.user_row_of[out.cstart[c] + k]];
+      mu /= nv;
+      for (int k = 0; k < nv; ++k) {
+        int r = out.user_row_of[out.cstart[c] + k];
+        delta[r] = mu / e[r];
+      }
+    }
+    if (any) {
+      scale_data(nullptr, delta);
+      for (int i = 0; i < m; ++i) e[i] *= delta[i];
+    }
+  }
+
+  // ---- KKT pattern (local): x 0..n-1, z rows n..n+m-1 in type-major local
+  // order, 2 extra per sparse SOC after that.
+  std::vector<int> local_of_user(m);
+  for (int lr = 0; lr < m; ++lr) local_of_user[out.user_row_of[lr]] = lr;
+  int nsparse = 0;
+  std::vector<int> sparse_idx(out.ctype.size(), -1);
+  for (size_t c = 0; c < out.ctype.size(); ++c)
+    if (out.ctype[c] == CLGPU_CONE_SOC && out.cdim[c] > opt.soc_threshold)
+      sparse_idx[c] = nsparse++;
+  const int N = n + m + 2 * nsparse;
+  out.N = N;
+  // entries (r <= c); source tags resolved later by position lookups
+  struct Ent {
+    int r, c;
+    double v;
+  };
+  std::vector<Ent> ents;
+  ents.reserve(P.p[n] + A.p[n] + N + 16);
+  for (int j = 0; j < n; ++j) {
+    bool hasdiag = false;
+    for (int k = P.p[j]; k < P.p[j + 1]; ++k) {
+      int i = P.i[k];
+      if (i <= j) ents.push_back({i, j, P.x[k]});
+      if (i == j) hasdiag = true;
+    }
+    if (!hasdiag) ents.push_back({j, j, 0.0});
+  }
+  for (int j = 0; j < n; ++j)
+    for (int k = A.p[j]; k < A.p[j + 1]; ++k)
+      ents.push_back({j, n + local_of_user[A.i[k]], A.x[k]});
+  for (size_t c = 0; c < out.ctype.size(); ++c) {
+    int t = out.ctype[c], st = n + out.cstart[c];
+    int nv = (t == 3 || t == 4) ? 3 : (t == 5 ? tri(out.cdim[c]) : out.cdim[c]);
+    bool diag = (t == CLGPU_CONE_ZERO || t == CLGPU_CONE_NONNEG || sparse_idx[c] >= 0);
+    if (diag) {
+      for (int k = 0; k < nv; ++k) ents.push_back({st + k, st + k, 0.0});
+    } else {
+      for (int col = 0; col < nv; ++col)
+        for (int row = 0; row <= col; ++row) ents.push_back({st + row, st + col, 0.0});
+    }
+    if (sparse_idx[c] >= 0) {
+      int pc = n + m + 2 * sparse_idx[c];
+      for (int k = 0; k < nv; ++k) {
+        ents.push_back({st + k, pc, 0.0});
+        ents.push_back({st + k, pc + 1, 0.0});
+      }
+      ents.push_back({pc, pc, 0.0});
+      ents.push_back({pc + 1, pc + 1, 0.0});
+    }
+  }
+  // ---- ordering
+  {
+    std::vector<std::vector<int>> adj(N);
+    for (auto &en : ents)
+      if (en.r != en.c) {
+        adj[en.r].push_back(en.c);
+        adj[en.c].push_back(en.r);
+      }
+    out.perm = amd_order(N, adj);
+  }
+  out.iperm.assign(N, 0);
+  for (int k = 0; k < N; ++k) out.iperm[out.perm[k]] = k;
+  // ---- permuted full CSR (sorted columns, duplicates summed)
+  std::vector<std::vector<std::pair<int, double>>> rowsv(N);
+  for (auto &en : ents) {
+    int a = out.iperm[en.r], bb = out.iperm[en.c];
+    rowsv[a].push_back({bb, en.v});
+    if (a != bb) rowsv[bb].push_back({a, en.v});
+  }
+  out.Kp.assign(N + 1, 0);
+  out.Kdiag.assign(N, -1);
+  for (int r = 0; r < N; ++r) {
+    auto &rv = rowsv[r];
+    std::sort(rv.begin(), rv.end(),
+              [](const std::pair<int, double> &x, const std::pair<int, double> &y) {
+                return x.first < y.first;
+              });
+    int start = (int)out.Kj.size();
+    for (size_t t = 0; t < rv.size(); ++t) {
+      if (!out.Kj.empty() && (int)out.Kj.size() > start && out.Kj.back() == rv[t].first) {
+        out.Kx.back() += rv[t].second;
+        continue;
+      }
+      out.Kj.push_back(rv[t].first);
+      out.Kx.push_back(rv[t].second);
+      if (rv[t].first == r) out.Kdiag[r] = (int)out.Kj.size() - 1;
+    }
+    out.Kp[r + 1] = (int)out.Kj.size();
+    std::vector<std::pair<int, double>>().swap(rv);
+  }
+  auto pos_of = [&](int lr, int lc) -> int {  // local unpermuted (lr, lc)
+    int a = out.iperm[lr], bb = out.iperm[lc];
+    auto beg = out.Kj.begin() + out.Kp[a], end = out.Kj.begin() + out.Kp[a + 1];
+    auto it = std::lower_bound(beg, end, bb);
+    return (it != end && *it == bb) ? (int)(it - out.Kj.begin()) : -1;
+  };
+  // Dsigns: +1 x, -1 z, (-1,+1) per sparse SOC pair
+  out.Dsign.assign(N, 1);
+  for (int o = 0; o < N; ++o) {
+    signed char sgn = 1;
+    if (o >= n && o < n + m) sgn = -1;
+    if (o >= n + m) sgn = ((o - n - m) % 2 == 0) ? -1 : 1;
+    out.Dsign[out.iperm[o]] = sgn;
+  }
+  // ---- symbolic LDL^T on the permuted matrix
+  {
+    std::vector<int> parent(N, -1), Lnz(N, 0), work(N, -1);
+    for (int k = 0; k < N; ++k) {
+      work[k] = k;
+      for (int p = out.Kp[k]; p < out.Kp[k + 1]; ++p) {
+        int i = out.Kj[p];
+        if (i >= k) break;
+        while (work[i] != k) {
+          if (parent[i] == -1) parent[i] = k;
+          Lnz[i]++;
+          work[i] = k;
+          i = parent[i];
+        }
+      }
+    }
+    out.Lp.assign(N + 1, 0);
+    for (int i = 0; i < N; ++i) out.Lp[i + 1] = out.Lp[i] + Lnz[i];
+    long long lnz = out.Lp[N];
+    if (lnz > 1500000000LL) {
+      out.error = "factor too large";
+      return false;
+    }
+    out.Li.assign(lnz, 0);
+    out.Rp.assign(N + 1, 0);
+    out.Rk.reserve(lnz);
+    out.Rpos.reserve(lnz);
+    std::vector<int> next(out.Lp.begin(), out.Lp.end() - 1);
+    std::fill(work.begin(), work.end(), -1);
+    for (int k = 0; k < N; ++k) {
+      work[k] = k;
+      for (int p = out.Kp[k]; p < out.Kp[k + 1]; ++p) {
+        int i = out.Kj[p];
+        if (i >= k) break;
+        while (work[i] != k) {
+          int q = next[i]++;
+          out.Li[q] = k;
+          out.Rk.push_back(i);
+          out.Rpos.push_back(q);
+          work[i] = k;
+          i = parent[i];
+        }
+      }
+      out.Rp[k + 1] = (int)out.Rk.size();
+    }
+  }
+  // ---- refresh positions
+  for (size_t c = 0; c < out.ctype.size(); ++c) {
+    int t = out.ctype[c], st = n + out.cstart[c];
+    int nv = (t == 3 || t == 4) ? 3 : (t == 5 ? tri(out.cdim[c]) : out.cdim[c]);
+    if (t == CLGPU_CONE_NONNEG) {
+      for (int k = 0; k < nv; ++k) out.nn_pos.push_back(pos_of(st + k, st + k));
+    } else if (t == CLGPU_CONE_SOC) {
+      if (sparse_idx[c] >= 0) {
+        int pc = n + m + 2 * sparse_idx[c];
+        out.socd_start.push_back(-1);
+        for (int k = 0; k < nv; ++k) {
+          out.socs_diag.push_back(pos_of(st + k, st + k));
+          out.socs_uv.push_back(pos_of(st + k, pc));
+          out.socs_uv.push_back(pos_of(pc, st + k));
+          out.socs_uv.push_back(pos_of(st + k, pc + 1));
+          out.socs_uv.push_back(pos_of(pc + 1, st + k));
+        }
+        out.socs_D.push_back(pos_of(pc, pc));
+        out.socs_D.push_back(pos_of(pc + 1, pc + 1));
+      } else {
+        out.socd_start.push_back((int)out.socd_pos.size() / 2);
+        for (int col = 0; col < nv; ++col)
+          for (int row = 0; row <= col; ++row) {
+            out.socd_pos.push_back(pos_of(st + row, st + col));
+            out.socd_pos.push_back(row == col ? -1 : pos_of(st + col, st + row));
+          }
+        for (int k = 0; k < nv; ++k) {
+          out.socs_diag.push_back(-1);
+          for (int q = 0; q < 4; ++q) out.socs_uv.push_back(-1);
+        }
+        out.socs_D.push_back(-1);
+        out.socs_D.push_back(-1);
+      }
+    } else if (t == CLGPU_CONE_EXP || t == CLGPU_CONE_POW) {
+      std::vector<int> &pp = (t == CLGPU_CONE_EXP) ? out.exp_pos : out.pow_pos;
+      const int ri[6] = {0, 0, 1, 0, 1, 2}, ci[6] = {0, 1, 1, 2, 2, 2};
+      for (int k = 0; k < 6; ++k) {
+        pp.push_back(pos_of(st + ri[k], st + ci[k]));
+        pp.push_back(ri[k] == ci[k] ? -1 : pos_of(st + ci[k], st + ri[k]));
+      }
+    } else if (t == CLGPU_CONE_PSD) {
+      out.psd_start.push_back((int)out.psd_pos.size() / 2);
+      for (int col = 0; col < nv; ++col)
+        for (int row = 0; row <= col; ++row) {
+          out.psd_pos.push_back(pos_of(st + row, st + col));
+          out.psd_pos.push_back(row == col ? -1 : pos_of(st + col, st + row));
+        }
+    }
+  }
+  for (int v : out.nn_pos)
+    if (v < 0) {
+      out.error = "internal: missing KKT position";
+      return false;
+    }
+  return true;
+}
+
+}  // namespace clgpu
+
+// ------------------------------------------------------------------ check
+// Host replay of the device factorisation/solve on the prepared structures.
+// Used by tests (no GPU needed) to validate the ordering, symbolic
+// factorisation and every refresh map before any kernel reads them.
+extern "C" int clgpu_debug_check_instance(const clgpu_problem *pb, const clgpu_settings *st,
+                                          double *resid) {
+  using namespace clgpu;
+  SetupOptions opt;
+  if (st) {
+    opt.soc_threshold = st->soc_threshold;
+    opt.equilibrate_enable = st->equilibrate_enable;
+    opt.equilibrate_max_iter = st->equilibrate_max_iter;
+  }
+  Prepared p;
+  if (!prepare_instance(*pb, opt, p)) return -2;
+  const int N = p.N;
+  const int knz = (int)p.Kj.size(), lnz = (int)p.Li.size();
+  // bounds of every index structure the kernels use
+  if ((int)p.Kp.size() != N + 1 || p.Kp[N] != knz) return -10;
+  for (int r = 0; r < N; ++r) {
+    if (p.Kdiag[r] < p.Kp[r] || p.Kdiag[r] >= p.Kp[r + 1]) return -11;
+    for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q)
+      if (p.Kj[q] < 0 || p.Kj[q] >= N || (q > p.Kp[r] && p.Kj[q] <= p.Kj[q - 1])) return -12;
+  }
+  if ((int)p.Lp.size() != N + 1 || p.Lp[N] != lnz || (int)p.Rp.size() != N + 1) return -13;
+  for (int j = 0; j < N; ++j)
+    for (int q = p.Lp[j]; q < p.Lp[j + 1]; ++q)
+      if (p.Li[q] <= j || p.Li[q] >= N || (q > p.Lp[j] && p.Li[q] <= p.Li[q - 1])) return -14;
+  for (int j = 0; j < N; ++j)
+    for (int q = p.Rp[j]; q < p.Rp[j + 1]; ++q) {
+      int k = p.Rk[q], pos = p.Rpos[q];
+      if (k < 0 || k >= j || pos < p.Lp[k] || pos >= p.Lp[k + 1] || p.Li[pos] != j) return -15;
+    }
+  auto inK = [&](int v, bool allow_neg) { return (allow_neg && v == -1) || (v >= 0 && v < knz); };
+  for (int v : p.nn_pos) if (!inK(v, false)) return -16;
+  for (int v : p.socd_pos) if (!inK(v, true)) return -17;
+  for (int v : p.socs_diag) if (!inK(v, true)) return -18;
+  for (int v : p.socs_uv) if (!inK(v, true)) return -19;
+  for (int v : p.socs_D) if (!inK(v, true)) return -20;
+  for (int v : p.exp_pos) if (!inK(v, true)) return -21;
+  for (int v : p.pow_pos) if (!inK(v, true)) return -22;
+  for (int v : p.psd_pos) if (!inK(v, true)) return -23;
+  // a quasi-definite test matrix on the KKT pattern: +/-(1 + 1e-3*rowsum)
+  std::vector<double> Kx(knz, 0.0);
+  for (int r = 0; r < N; ++r)
+    for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) {
+      int c = p.Kj[q];
+      if (c != r) Kx[q] = 0.01 * std::sin(1.0 + r + 7.0 * c) * std::sin(1.0 + c + 7.0 * r);
+    }
+  for (int r = 0; r < N; ++r) Kx[p.Kdiag[r]] = p.Dsign[r] * 2.0;
+  // left-looking factorisation, same loops as the kernel
+  std::vector<double> w(N, 0.0), Lx(lnz, 0.0), D(N, 0.0);
+  for (int j = 0; j < N; ++j) {
+    for (int q = p.Kp[j]; q < p.Kp[j + 1]; ++q)
+      if (p.Kj[q] >= j) w[p.Kj[q]] = Kx[q];
+    for (int q = p.Rp[j]; q < p.Rp[j + 1]; ++q) {
+      int k = p.Rk[q], pos = p.Rpos[q];
+      double f = Lx[pos] * D[k];
+      for (int t = pos; t < p.Lp[k + 1]; ++t) w[p.Li[t]] -= Lx[t] * f;
+    }
+    D[j] = w[j];
+    for (int t = p.Lp[j]; t < p.Lp[j + 1]; ++t) {
+      Lx[t] = w[p.Li[t]] / D[j];
+      w[p.Li[t]] = 0;
+    }
+    w[j] = 0;
+  }
+  std::vector<double> b(N), y(N);
+  for (int i = 0; i < N; ++i) b[i] = std::cos(0.3 * i);
+  y = b;
+  for (int j = 0; j < N; ++j)
+    for (int t = p.Lp[j]; t < p.Lp[j + 1]; ++t) y[p.Li[t]] -= Lx[t] * y[j];
+  for (int j = 0; j < N; ++j) y[j] /= D[j];
+  for (int j = N - 1; j >= 0; --j)
+    for (int t = p.Lp[j]; t < p.Lp[j + 1]; ++t) y[j] -= Lx[t] * y[p.Li[t]];
+  double mx = 0;
+  for (int r = 0; r < N; ++r) {
+    double t = 0;
+    for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) t += Kx[q] * y[p.Kj[q]];
+    mx = std::max(mx, std::fabs(t - b[r]));
+  }
+  if (resid) *resid = mx;
+  return 0;
+}

@@ -1,0 +1,212 @@
+/*
+ * clgpu.h -- C ABI of libclgpu, the B200 (sm_100a) implementation of the
+ * Clarabel GPU interior-point hot path.
+ *
+ * Two levels of entry points:
+ *
+ *  1. Solver level.  Replaces the GPU branch of Clarabel.Solver / setup! /
+ *     solve! (src/solver.jl:5-17, :129-195, :231-422 of the CuClarabel tree)
+ *     for one problem (the plain path) or for a batch of independent problems
+ *     solved in lock step (the batched path).  Problem data is passed as host
+ *     CSC arrays exactly as the reference's CPU-side constructor receives it
+ *     (P upper triangle, src/solver.jl:618-630).
+ *
+ *  2. Cone level.  Replaces the CompositeConeGPU method table
+ *     (src/gpucones/coneops_compositecone_gpu.jl) for callers that keep their
+ *     own IPM loop: every vector argument is a DEVICE pointer borrowed for the
+ *     duration of the call, laid out in the reference's order (cones sorted
+ *     zero, nonnegative, second-order, exponential, power, PSD; the same order
+ *     rule as src/gpucones/compositecone_type_gpu.jl:75-79).
+ *
+ * Conventions: every function returns int status, 0 = success, > 0 =
+ * numerical failure (maps to NUMERICAL_ERROR / the Dual-scaling fallback of
+ * the reference), < 0 = argument or CUDA error.  A cudaStream_t may be passed
+ * as NULL (legacy default stream).  Handles are not thread safe; use one
+ * handle per host thread or stream.  The library never frees caller memory.
+ */
+#ifndef CLGPU_H
+#define CLGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *clgpu_stream_t; /* == cudaStream_t */
+
+/* cone type codes, reference order of src/cones/cone_api.jl:93-108 */
+enum {
+  CLGPU_CONE_ZERO = 0,
+  CLGPU_CONE_NONNEG = 1,
+  CLGPU_CONE_SOC = 2,
+  CLGPU_CONE_EXP = 3,
+  CLGPU_CONE_POW = 4,
+  CLGPU_CONE_PSD = 5 /* dim = side n of the n x n matrix */
+};
+
+/* direct_solve_method (src/settings.jl:113-114, gpu_solver_list of
+ * src/Clarabel.jl:27).  The reference names :cudss and :cudssmixed; this
+ * library's own batched LDL^T takes their place with the same precision
+ * policy. */
+enum { CLGPU_METHOD_FP64 = 0 /* :cudss */, CLGPU_METHOD_MIXED = 1 /* :cudssmixed */ };
+
+/* mirrors Settings (src/settings.jl:70-148), numeric fields only */
+typedef struct {
+  int max_iter;
+  double time_limit;
+  double max_step_fraction;
+  double tol_gap_abs, tol_gap_rel, tol_feas, tol_infeas_abs, tol_infeas_rel,
+      tol_ktratio;
+  double reduced_tol_gap_abs, reduced_tol_gap_rel, reduced_tol_feas,
+      reduced_tol_infeas_abs, reduced_tol_infeas_rel, reduced_tol_ktratio;
+  int equilibrate_enable, equilibrate_max_iter;
+  double equilibrate_min_scaling, equilibrate_max_scaling;
+  double linesearch_backtrack_step, min_switch_step_length,
+      min_terminate_step_length;
+  int static_regularization_enable;
+  double static_regularization_constant, static_regularization_proportional;
+  int dynamic_regularization_enable;
+  double dynamic_regularization_eps, dynamic_regularization_delta;
+  int iterative_refinement_enable;
+  double iterative_refinement_reltol, iterative_refinement_abstol;
+  int iterative_refinement_max_iter;
+  double iterative_refinement_stop_ratio;
+  int direct_solve_method; /* CLGPU_METHOD_* */
+  int soc_threshold;       /* src/settings.jl:147 */
+  int verbose;
+  int setup_threads;       /* host threads for per-instance setup; 0 = all */
+} clgpu_settings;
+
+/* mirrors DefaultInfo (src/types.jl:227-255) plus solution scalars */
+typedef struct {
+  int status; /* SolverStatus, src/statuscodes.jl:24-36 */
+  int iterations;
+  double obj_val, obj_val_dual;
+  double cost_primal, cost_dual;
+  double res_primal, res_dual, res_primal_inf, res_dual_inf;
+  double gap_abs, gap_rel, ktratio, mu, sigma, step_length;
+  double solve_time;
+} clgpu_info;
+
+/* one problem instance, host memory, borrowed for the create call */
+typedef struct {
+  int n, m;
+  const int *Pp, *Pi;  /* P (n x n) CSC, upper triangle used */
+  const double *Px;
+  const double *q;     /* n */
+  const int *Ap, *Ai;  /* A (m x n) CSC */
+  const double *Ax;
+  const double *b;     /* m */
+  int ncones;
+  const int *cone_types;    /* CLGPU_CONE_* (any order) */
+  const int *cone_dims;     /* zero/nonneg/soc: dim; psd: side n; exp/pow: 3 */
+  const double *cone_params;/* power-cone alpha, else ignored (may be NULL) */
+} clgpu_problem;
+
+typedef struct clgpu_solver clgpu_solver;
+typedef struct clgpu_cones clgpu_cones;
+
+/* src/settings.jl defaults */
+int clgpu_default_settings(clgpu_settings *s);
+
+/* ---------------------------------------------------------------- solver */
+/* Solver(P,q,A,b,cones,settings) + setup! for nprob >= 1 instances
+ * (src/solver.jl:5-17, :129-195).  nprob == 1 is the plain path. */
+int clgpu_solver_create(const clgpu_problem *probs, int nprob,
+                        const clgpu_settings *settings, clgpu_solver **out);
+/* solve! (src/solver.jl:231-422) for every instance, on the given stream;
+ * returns after the stream work has completed. */
+int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream);
+/* DefaultInfo of one instance after solve */
+int clgpu_solver_get_info(clgpu_solver *h, int inst, clgpu_info *info);
+/* solution (unscaled, user row order) of one instance into HOST buffers;
+ * any pointer may be NULL.  src/solution.jl:2-50 */
+int clgpu_solver_get_solution(clgpu_solver *h, int inst, double *x, double *s,
+                              double *z);
+/* all instances at once: x/s/z concatenated in instance order (sum n / sum m),
+ * info array of nprob entries; any pointer may be NULL */
+int clgpu_solver_get_solutions(clgpu_solver *h, double *x, double *s,
+                               double *z, clgpu_info *info);
+/* replace q and b of one instance (same sizes) before the next solve;
+ * the equilibration computed at setup is reused (src/data_updating.jl) */
+int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,
+                           const double *b);
+/* device-memory footprint of the handle in bytes */
+long long clgpu_solver_device_bytes(const clgpu_solver *h);
+/* number of kernel launches issued by the last solve */
+long long clgpu_solver_launch_count(const clgpu_solver *h);
+/* timing of the last solve: total ms and the per-kernel-class ms measured
+ * with CUDA events (0 if profiling was not requested) */
+int clgpu_solver_set_profiling(clgpu_solver *h, int enable);
+int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
+                             double *ms_factor, double *ms_solve,
+                             double *ms_cones, double *ms_residual,
+                             int *passes);
+int clgpu_solver_destroy(clgpu_solver *h);
+
+/* --------------------------------------------------------------- cones */
+/* CompositeConeGPU{T}(cones, soc_threshold)
+ * (src/gpucones/compositecone_type_gpu.jl:72-216).  Cones must be sorted
+ * by type (zero, nonneg, soc, exp, pow, psd); returns -2 otherwise. */
+int clgpu_cones_create(int ncones, const int *types, const int *dims,
+                       const double *params, int soc_threshold,
+                       clgpu_cones **out);
+int clgpu_cones_destroy(clgpu_cones *h);
+int clgpu_cones_numel(const clgpu_cones *h);
+int clgpu_cones_degree(const clgpu_cones *h);
+/* length of the packed Hsblocks vector (rng_blocks, compositecone_type.jl:251) */
+int clgpu_cones_hs_len(const clgpu_cones *h);
+/* update_scaling! (coneops_compositecone_gpu.jl:185); strategy 0 PrimalDual,
+ * 1 Dual; returns 1 if a cone is not strictly interior */
+int clgpu_update_scaling(clgpu_cones *h, const double *s, const double *z,
+                         double mu, int strategy, clgpu_stream_t st);
+/* set_identity_scaling! (:161) */
+int clgpu_set_identity_scaling(clgpu_cones *h, clgpu_stream_t st);
+/* get_Hs! (:252) into the packed reference layout */
+int clgpu_get_Hs(clgpu_cones *h, double *Hsblocks, clgpu_stream_t st);
+/* mul_Hs! (:315) y = Hs x */
+int clgpu_mul_Hs(clgpu_cones *h, double *y, const double *x,
+                 clgpu_stream_t st);
+/* affine_ds! (:409) */
+int clgpu_affine_ds(clgpu_cones *h, double *ds, const double *s,
+                    clgpu_stream_t st);
+/* combined_ds_shift! (:458).  step_z/step_s are read only here (the
+ * reference overwrites them with W dz and W^{-T} ds as scratch). */
+int clgpu_combined_ds_shift(clgpu_cones *h, double *shift,
+                            const double *step_z, const double *step_s,
+                            const double *z, double sigma_mu,
+                            clgpu_stream_t st);
+/* Δs_from_Δz_offset! (:515) */
+int clgpu_ds_from_dz_offset(clgpu_cones *h, double *out, const double *ds,
+                            const double *z, clgpu_stream_t st);
+/* step_length (:566): returns the common step in *alpha (host) */
+int clgpu_step_length(clgpu_cones *h, const double *dz, const double *ds,
+                      const double *z, const double *s, double alpha_max,
+                      double max_step_fraction, double backtrack_step,
+                      double alpha_min, double *alpha, clgpu_stream_t st);
+/* compute_barrier (:650) */
+int clgpu_compute_barrier(clgpu_cones *h, const double *z, const double *s,
+                          const double *dz, const double *ds, double alpha,
+                          double *barrier, clgpu_stream_t st);
+/* margins (:42): pd 0 primal, 1 dual */
+int clgpu_margins(clgpu_cones *h, const double *z, int pd, double *alpha,
+                  double *beta, clgpu_stream_t st);
+/* scaled_unit_shift! (:81) */
+int clgpu_scaled_unit_shift(clgpu_cones *h, double *z, double alpha, int pd,
+                            clgpu_stream_t st);
+/* unit_initialization! (:115) */
+int clgpu_unit_initialization(clgpu_cones *h, double *z, double *s,
+                              clgpu_stream_t st);
+
+/* --------------------------------------------------------------- checks */
+/* Host-only replay of the device factorisation on the structures prepared
+ * for one instance: validates the ordering, the symbolic factorisation and
+ * every index map, then factors a quasi-definite test matrix on the KKT
+ * pattern and returns the solve residual.  No reference counterpart
+ * (diagnostic); needs no GPU. */
+int clgpu_debug_check_instance(const clgpu_problem *prob,
+                               const clgpu_settings *settings, double *resid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,183 @@
+"""Per-operation parity of the cone kernels (cone-level C ABI, device
+pointers) against the CPU oracle's restatement of src/cones/*.jl."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from cuclarabel_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12  # relative, FP64 cone arithmetic
+
+
+def interior(rng, spec, scale=1.0):
+    t, d, p = spec
+    if t == 0:
+        return rng.standard_normal(d) * scale
+    if t == 1:
+        return rng.uniform(0.5, 2, d)
+    if t == 2:
+        tail = rng.standard_normal(d - 1)
+        return np.concatenate([[1.0 + np.linalg.norm(tail) * rng.uniform(1.05, 2)], tail])
+    if t == 3:
+        return np.array([-1.051383945322714, 0.556409619469370, 1.258967884768947]) * \
+            rng.uniform(0.5, 2) + rng.normal(0, 0.02, 3)
+    if t == 4:
+        return np.array([np.sqrt(1 + p), np.sqrt(2 - p), 0.0]) * rng.uniform(0.5, 2) + \
+            np.array([0, 0, rng.normal(0, 0.1)])
+    E = rng.standard_normal((d, d)) * 0.2
+    M = np.eye(d) + (E + E.T) / 2
+    out = []
+    for j in range(d):
+        for i in range(j + 1):
+            out.append(M[i, j] if i == j else M[i, j] * np.sqrt(2))
+    return np.array(out)
+
+
+SPECS = {
+    "nn": [(1, 7, 0.0)],
+    "soc_dense": [(2, 3, 0.0), (2, 5, 0.0), (2, 4, 0.0)],
+    "soc_sparse": [(2, 10, 0.0), (2, 6, 0.0), (2, 40, 0.0)],
+    "exp": [(3, 3, 0.0)] * 5,
+    "pow": [(4, 3, 0.3), (4, 3, 0.7), (4, 3, 0.55)],
+    "psd": [(5, 3, 0.0), (5, 10, 0.0)],
+    "mixed": [(0, 2, 0.0), (1, 4, 0.0), (2, 3, 0.0), (2, 8, 0.0), (3, 3, 0.0), (4, 3, 0.4),
+              (5, 4, 0.0)],
+}
+
+
+class GPUCones:
+    def __init__(self, specs):
+        import torch
+        self.torch = torch
+        self.L = _lib.load()
+        t = np.array([s[0] for s in specs], np.int32)
+        d = np.array([s[1] for s in specs], np.int32)
+        p = np.array([s[2] for s in specs], np.float64)
+        h = ctypes.c_void_p()
+        rc = self.L.clgpu_cones_create(len(t), t.ctypes.data_as(_lib.ip),
+                                       d.ctypes.data_as(_lib.ip), p.ctypes.data_as(_lib.dp), 5,
+                                       ctypes.byref(h))
+        assert rc == 0
+        self.h = h
+        self.numel = self.L.clgpu_cones_numel(h)
+        self.hs_len = self.L.clgpu_cones_hs_len(h)
+
+    def dev(self, a):
+        return self.torch.tensor(np.asarray(a, np.float64), device="cuda")
+
+    def empty(self, n):
+        return self.torch.zeros(max(n, 1), dtype=self.torch.float64, device="cuda")
+
+    def __del__(self):
+        self.L.clgpu_cones_destroy(self.h)
+
+
+def setup(name, seed=0):
+    specs = SPECS[name]
+    rng = np.random.default_rng(seed)
+    s = np.concatenate([interior(rng, sp) for sp in specs])
+    z = np.concatenate([interior(rng, sp) for sp in specs])
+    return specs, rng, s, z
+
+
+def close(a, b, tol=TOL):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.allclose(a, b, rtol=tol, atol=tol * max(1.0, np.abs(b).max(initial=0)))
+
+
+@pytest.mark.parametrize("name", list(SPECS))
+@pytest.mark.parametrize("strategy", [0, 1])
+def test_update_scaling_hs_and_products(cuda_device, name, strategy):
+    specs, rng, s, z = setup(name)
+    mu = float(s @ z / 10)
+    C = oracle.Cones(specs)
+    G = GPUCones(specs)
+    assert C.update_scaling(s, z, mu, strategy) == 0
+    ds_, dz_ = G.dev(s), G.dev(z)
+    assert G.L.clgpu_update_scaling(G.h, ds_.data_ptr(), dz_.data_ptr(), mu, strategy, None) == 0
+    # Hs blocks (invariant to the SVD sign choices of the PSD scaling)
+    hs = G.empty(G.hs_len)
+    assert G.L.clgpu_get_Hs(G.h, hs.data_ptr(), None) == 0
+    assert close(hs.cpu().numpy()[:C.hs_len], C.get_Hs(), 1e-11)
+    # mul_Hs
+    x = rng.standard_normal(C.numel)
+    y = G.empty(C.numel)
+    assert G.L.clgpu_mul_Hs(G.h, y.data_ptr(), G.dev(x).data_ptr(), None) == 0
+    assert close(y.cpu().numpy(), C.mul_Hs(x), 1e-11)
+    # affine_ds
+    out = G.empty(C.numel)
+    assert G.L.clgpu_affine_ds(G.h, out.data_ptr(), ds_.data_ptr(), None) == 0
+    assert close(out.cpu().numpy(), C.affine_ds(s), 1e-11)
+    # combined_ds_shift
+    stz, sts = rng.standard_normal(C.numel) * 0.1, rng.standard_normal(C.numel) * 0.1
+    sm = 0.37 * mu
+    sh = G.empty(C.numel)
+    assert G.L.clgpu_combined_ds_shift(G.h, sh.data_ptr(), G.dev(stz).data_ptr(),
+                                       G.dev(sts).data_ptr(), dz_.data_ptr(), sm, None) == 0
+    assert close(sh.cpu().numpy(), C.combined_ds_shift(stz, sts, z, sm), 1e-10)
+    # ds_from_dz_offset
+    dsv = rng.standard_normal(C.numel)
+    o = G.empty(C.numel)
+    assert G.L.clgpu_ds_from_dz_offset(G.h, o.data_ptr(), G.dev(dsv).data_ptr(),
+                                       dz_.data_ptr(), None) == 0
+    assert close(o.cpu().numpy(), C.ds_from_dz_offset(dsv, z), 1e-10)
+
+
+@pytest.mark.parametrize("name", list(SPECS))
+def test_step_length_and_barrier(cuda_device, name):
+    specs, rng, s, z = setup(name, seed=3)
+    C = oracle.Cones(specs)
+    G = GPUCones(specs)
+    C.update_scaling(s, z, 1.0, 0)
+    G.L.clgpu_update_scaling(G.h, G.dev(s).data_ptr(), G.dev(z).data_ptr(), 1.0, 0, None)
+    for trial in range(4):
+        dz = rng.standard_normal(C.numel) * (0.5 + trial)
+        ds = rng.standard_normal(C.numel) * (0.5 + trial)
+        ref = C.step_length(dz, ds, z, s, 1.0)
+        a = ctypes.c_double()
+        assert G.L.clgpu_step_length(G.h, G.dev(dz).data_ptr(), G.dev(ds).data_ptr(),
+                                     G.dev(z).data_ptr(), G.dev(s).data_ptr(), 1.0, 0.99, 0.8,
+                                     1e-4, ctypes.byref(a), None) == 0
+        assert abs(a.value - ref) <= 1e-10 * max(1.0, ref), (a.value, ref)
+        alpha = 0.5 * ref
+        bref = C.compute_barrier(z, s, dz, ds, alpha)
+        bar = ctypes.c_double()
+        assert G.L.clgpu_compute_barrier(G.h, G.dev(z).data_ptr(), G.dev(s).data_ptr(),
+                                         G.dev(dz).data_ptr(), G.dev(ds).data_ptr(), alpha,
+                                         ctypes.byref(bar), None) == 0
+        assert abs(bar.value - bref) <= 1e-9 * max(1.0, abs(bref))
+
+
+@pytest.mark.parametrize("name", ["nn", "soc_dense", "soc_sparse", "psd"])
+def test_margins_shift_and_init(cuda_device, name):
+    specs, rng, s, z = setup(name, seed=5)
+    C = oracle.Cones(specs)
+    G = GPUCones(specs)
+    v = rng.standard_normal(C.numel)
+    for pd in (0, 1):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        assert G.L.clgpu_margins(G.h, G.dev(v).data_ptr(), pd, ctypes.byref(a), ctypes.byref(b),
+                                 None) == 0
+        ra, rb = C.margins(v, pd)
+        assert abs(a.value - ra) < 1e-11 and abs(b.value - rb) < 1e-10
+        t = G.dev(v)
+        assert G.L.clgpu_scaled_unit_shift(G.h, t.data_ptr(), 0.75, pd, None) == 0
+        assert close(t.cpu().numpy(), C.scaled_unit_shift(v, 0.75, pd), 1e-14)
+    zz, ss = G.empty(C.numel), G.empty(C.numel)
+    assert G.L.clgpu_unit_initialization(G.h, zz.data_ptr(), ss.data_ptr(), None) == 0
+    rz, rs = C.unit_initialization()
+    assert close(zz.cpu().numpy(), rz, 1e-15) and close(ss.cpu().numpy(), rs, 1e-15)
+
+
+def test_scaling_failure_reported(cuda_device):
+    """A point outside the cone is reported as a numerical failure (return 1),
+    as the CPU path's update_scaling! does (coneops_socone.jl:385-387)."""
+    specs = [(2, 4, 0.0)]
+    G = GPUCones(specs)
+    s = np.array([0.1, 1.0, 0.0, 0.0])  # not interior
+    z = np.array([2.0, 0.1, 0.1, 0.1])
+    assert G.L.clgpu_update_scaling(G.h, G.dev(s).data_ptr(), G.dev(z).data_ptr(), 1.0, 0,
+                                    None) == 1

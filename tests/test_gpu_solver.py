@@ -1,0 +1,90 @@
+"""Full-solve parity of the B200 library against the CPU oracle.
+
+Bar (north-star parity): same status, objective within 1e-7 relative,
+primal/dual residuals below tol_feas, iteration count within +-2."""
+import numpy as np
+import pytest
+
+import oracle
+from cuclarabel_b200 import BatchSolver, Solver, SolverStatus, problems
+from helpers import ITER_TOL, OBJ_RTOL, golden_cases, rel_err, to_cone_objects
+
+pytestmark = pytest.mark.gpu
+CASES = golden_cases()
+
+
+def check_parity(sol, ref, name=""):
+    assert sol.status.name == ref["status_name"], (name, sol.status.name, ref["status_name"])
+    assert abs(sol.iterations - ref["iterations"]) <= ITER_TOL, (name, sol.iterations,
+                                                                 ref["iterations"])
+    if sol.status == SolverStatus.SOLVED:
+        assert rel_err(sol.obj_val, ref["obj_val"]) < OBJ_RTOL, (name, sol.obj_val,
+                                                                ref["obj_val"])
+        assert sol.r_prim < 1e-8 and sol.r_dual < 1e-8
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_golden_reference_cases(cuda_device, case):
+    name, P, q, A, b, cones, e = case
+    s = Solver(P, q, A, b, to_cone_objects(cones))
+    sol = s.solve()
+    if "status" in e:
+        assert sol.status.name == e["status"]
+    if "x" in e:
+        assert np.linalg.norm(sol.x - np.array(e["x"])) < e["tol"]
+    if "obj_val" in e:
+        assert abs(sol.obj_val - e["obj_val"]) < e["tol"]
+    if "cost_primal" in e:
+        assert abs(sol.info["cost_primal"] - e["cost_primal"]) < e["tol"]
+    if e.get("obj_nan"):
+        assert np.isnan(sol.obj_val)
+    check_parity(sol, oracle.solve(P, q, A, b, cones), name)
+
+
+def test_portfolio_config1(cuda_device):
+    pb = problems.portfolio(seed=1)
+    sol = Solver(*pb).solve()
+    check_parity(sol, oracle.solve(*pb), "portfolio")
+
+
+@pytest.mark.parametrize("method", ["cudss", "cudssmixed"])
+def test_mpc_batch_matches_per_instance_oracle(cuda_device, method):
+    pbs = problems.mpc_batch(48, seed0=100)
+    sols = BatchSolver(pbs, direct_solve_method=method).solve()
+    for k, (pb, sol) in enumerate(zip(pbs, sols)):
+        ref = oracle.solve(*pb, **({"static_regularization_constant": np.sqrt(np.finfo(np.float32).eps)}
+                                   if method == "cudssmixed" else {}))
+        check_parity(sol, ref, "mpc%d" % k)
+
+
+def test_batch_equals_single(cuda_device):
+    """Each instance gives the same answer alone and in a batch."""
+    pbs = problems.mpc_batch(6, seed0=7)
+    batch = BatchSolver(pbs).solve()
+    for pb, sb in zip(pbs, batch):
+        s1 = Solver(*pb).solve()
+        assert s1.status == sb.status
+        assert s1.iterations == sb.iterations
+        assert rel_err(s1.obj_val, sb.obj_val) < 1e-9
+        assert np.allclose(s1.x, sb.x, rtol=1e-7, atol=1e-7)
+
+
+def test_mixed_socp_scaled(cuda_device):
+    pb = problems.mixed_socp(scale=0.02, seed=2)
+    sol = Solver(*pb).solve()
+    check_parity(sol, oracle.solve(*pb), "mixed_socp")
+
+
+def test_exp_pow_psd_scaled(cuda_device):
+    pb = problems.exp_pow_psd(scale=0.004, seed=3)
+    sol = Solver(*pb).solve()
+    check_parity(sol, oracle.solve(*pb), "exp_pow_psd")
+
+
+def test_repeat_solve_is_identical(cuda_device):
+    pb = problems.mpc_qp(3)
+    s = Solver(*pb)
+    a = s.solve()
+    b = s.solve()
+    assert a.status == b.status and a.iterations == b.iterations
+    assert rel_err(a.obj_val, b.obj_val) < 1e-12

@@ -1,0 +1,42 @@
+"""Host-side validation of the per-instance structures the device kernels
+read (ordering, symbolic LDL^T, refresh maps): the library replays the
+left-looking factorisation on the CPU and solves a test system.  No GPU."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cuclarabel_b200 import _lib, problems
+from cuclarabel_b200.api import Settings, _prep_problem
+from helpers import golden_cases, to_cone_objects
+
+
+def check(pb, **kw):
+    cp, keep, n, m = _prep_problem(*pb)
+    st = Settings(**kw).to_c()
+    r = ctypes.c_double()
+    rc = _lib.load().clgpu_debug_check_instance(ctypes.byref(cp), ctypes.byref(st),
+                                                ctypes.byref(r))
+    return rc, r.value
+
+
+@pytest.mark.parametrize("case", golden_cases(), ids=[c[0] for c in golden_cases()])
+def test_golden_structures(case):
+    name, P, q, A, b, cones, e = case
+    rc, res = check((P, q, A, b, to_cone_objects(cones)))
+    assert rc == 0 and res < 1e-10
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_mpc_structures(seed):
+    rc, res = check(problems.mpc_qp(seed))
+    assert rc == 0 and res < 1e-9
+
+
+def test_config_families():
+    for pb in (problems.portfolio(), problems.mixed_socp(0.01), problems.exp_pow_psd(0.003)):
+        rc, res = check(pb)
+        assert rc == 0 and res < 1e-9
+    # dense SOC path (threshold above every cone)
+    rc, res = check(problems.mpc_qp(3), soc_threshold=100)
+    assert rc == 0 and res < 1e-9
