@@ -1,0 +1,381 @@
+"""Benchmark: batched solves/s at 1e-8 for the batched MPC QP/SOCP workload
+(4096 independent MPC-style QP/SOCPs, n ~ U{20..400}, m ~ 2n, instance i
+seeded with i), compared with the plain one-instance-at-a-time GPU path and
+the CPU reference path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--instances B] [--method cudssmixed|cudss]
+
+One step = one solve! of the whole batch (every instance to termination).
+`value` is solved instances per second with the problem data resident on
+the device (setup excluded, L2 flushed between steps); `e2e` is the same
+metric through the public API from host CSC data: Solver(...) setup with its
+host->device copies, solve!, and the solutions read back to the host.
+Under torchrun each rank solves its own 4096 instances (weak scaling, no
+collective on the data path; NCCL only for the barrier and the max-time
+reduction).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def gen_problems(count, seed0):
+    from cuclarabel_b200 import problems
+    return [problems.mpc_qp(seed0 + i) for i in range(count)]
+
+
+def algorithmic_bytes_update_scaling(pbs, soc_threshold=5):
+    """Bytes of update_scaling per batch launch (NN 32 B/row; SOC 32 B/row +
+    8 B/cone, sparse SOC +16 B/row (u, v) + 8 B/cone (d))."""
+    total = 0
+    for pb in pbs:
+        for c in pb[4]:
+            t, d, _ = c.spec()
+            if t == 1:
+                total += 32 * d
+            elif t == 2:
+                total += 32 * d + 8
+                if d > soc_threshold:
+                    total += 16 * d + 8
+    return total
+
+
+def problem_bytes(pbs):
+    b = 0
+    for P, q, A, bb, c in pbs:
+        b += P.nnz * 12 + (P.shape[1] + 1) * 4 + A.nnz * 12 + (A.shape[1] + 1) * 4
+        b += q.nbytes + bb.nbytes + len(c) * 12
+    return b
+
+
+def run_reference(args, rank, world):
+    """CPU reference path (the oracle restatement of the reference's CPU
+    Clarabel path) on the host cores, bounded sample per step."""
+    if rank != 0:
+        return
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    sample = args.ref_sample
+    pbs = gen_problems(sample, 0)
+    ctx = mp.get_context("spawn")
+    os.environ["OMP_NUM_THREADS"] = "1"
+    with ProcessPoolExecutor(max_workers=cores, mp_context=ctx,
+                             initializer=_ref_init) as ex:
+        list(ex.map(_ref_solve, range(min(cores, sample))))  # warm the workers
+        times, solved = [], 0
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = list(ex.map(_ref_solve, range(sample), chunksize=4))
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append(dt)
+                solved += sum(1 for r in res if r == "SOLVED")
+    total = sum(times)
+    val = solved / total
+    line = {
+        "metric": "solves/s at 1e-8 (batched MPC QP/SOCP)",
+        "value": val, "unit": "solves/s", "impl": "reference", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "MPC QP/SOCP batch (sample of %d of 4096)" % sample,
+                   "instances_per_step": sample},
+        "cpu_baseline": {"value": val, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "%d MPC QP/SOCP instances per step, one process per core" % sample},
+        "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+_REF_PBS = None
+
+
+def _ref_init():
+    global _REF_PBS
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+
+
+def _ref_solve(i):
+    global _REF_PBS
+    import oracle
+    from cuclarabel_b200 import problems
+    if _REF_PBS is None:
+        _REF_PBS = {}
+    pb = _REF_PBS.get(i)
+    if pb is None:
+        pb = problems.mpc_qp(i)
+        _REF_PBS[i] = pb
+    return oracle.solve(*pb, gpu_equilibration=1)["status_name"]
+
+
+def cpu_baseline_sample(sample):
+    """Bounded CPU sample for the GPU arm's cpu_baseline field."""
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=cores, mp_context=ctx, initializer=_ref_init) as ex:
+        list(ex.map(_ref_solve, range(min(cores, sample))))
+        t0 = time.perf_counter()
+        res = list(ex.map(_ref_solve, range(sample), chunksize=4))
+        dt = time.perf_counter() - t0
+    solved = sum(1 for r in res if r == "SOLVED")
+    return {"value": solved / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": "%d MPC QP/SOCP instances, one process per core, %.1f s wall" % (sample, dt)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours")
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--method", default="cudss")
+    ap.add_argument("--plain-sample", type=int, default=48)
+    ap.add_argument("--ref-sample", type=int, default=512)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from cuclarabel_b200 import BatchSolver, Solver, SolverStatus
+
+    B = args.instances
+    seed0 = rank * B
+    pbs = gen_problems(B, seed0)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    solver = BatchSolver(pbs, direct_solve_method=args.method)
+    dev_bytes = solver.device_bytes()
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
+
+    def flush_l2():
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        solver.solve(sh)
+    # profiled (untimed) pass for the phase breakdown
+    solver.set_profiling(True)
+    sols = solver.solve(sh)
+    prof = solver.profile()
+    solver.set_profiling(False)
+    launches_per_solve = solver.launch_count()
+
+    sampler = ClockSampler(local)
+    times = []
+    solved_total = 0
+    sampler.start()
+    for _ in range(args.steps):
+        flush_l2()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sols = solver.solve(sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1000.0)
+        solved_total += sum(1 for s in sols if s.status == SolverStatus.SOLVED)
+    clocks = sampler.stop()
+    elapsed = sum(times)
+    if dist:
+        t = torch.tensor([elapsed, float(solved_total)], device="cuda", dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        elapsed = tmax[0].item()
+        solved_total = int(tsum[1].item())
+    value = solved_total / elapsed
+    n_solved_last = sum(1 for s in sols if s.status == SolverStatus.SOLVED)
+    status_counts = {}
+    for s in sols:
+        status_counts[s.status.name] = status_counts.get(s.status.name, 0) + 1
+    iters = [s.iterations for s in sols]
+
+    # ---- e2e through the public API (host data -> device -> host)
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_t = 0.0
+    e2e_solved = 0
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = BatchSolver(pbs, direct_solve_method=args.method)
+        out = s2.solve(sh)
+        torch.cuda.synchronize()
+        e2e_t += time.perf_counter() - t0
+        e2e_solved += sum(1 for s in out if s.status == SolverStatus.SOLVED)
+        del s2
+    h2d = problem_bytes(pbs)
+    d2h = sum((p[1].nbytes + 2 * p[3].nbytes) for p in pbs) + B * 136
+    e2e_val = e2e_solved / e2e_t
+    if dist:
+        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = e2e_solved * world / t.item()
+
+    # ---- plain path: one instance at a time on the same GPU (FP64, B = 1)
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        ps = [Solver(*pbs[i]) for i in range(args.plain_sample)]
+        for s in ps[:3]:
+            s.solve(sh)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lat = []
+        nsol = 0
+        for s in ps:
+            a = time.perf_counter()
+            r = s.solve(sh)
+            lat.append(time.perf_counter() - a)
+            nsol += r.status == SolverStatus.SOLVED
+        dt = time.perf_counter() - t0
+        plain = {"value": nsol / dt, "unit": "solves/s", "sample": args.plain_sample,
+                 "p50_ms": 1000 * float(np.percentile(lat, 50)),
+                 "p99_ms": 1000 * float(np.percentile(lat, 99)), "method": "cudss"}
+
+    # ---- roofline of the dominant device phase and of update_scaling
+    peaks, peak_kind = load_peaks()
+    hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    phases = prof["phases"]
+    dom = max(phases.items(), key=lambda kv: kv[1][0])
+    us_ms, us_calls = phases["update_scaling"]
+    us_bytes = algorithmic_bytes_update_scaling(pbs)
+    us_achieved = us_bytes / (us_ms / max(us_calls, 1) / 1000.0) / 1e9 if us_ms > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(args.ref_sample)
+
+    if rank == 0:
+        roof = {"bound": "hbm", "kernel": "update_scaling (nonneg + SOC, whole batch)",
+                "achieved": us_achieved, "peak": hbm, "unit": "GB/s",
+                "frac": us_achieved / hbm, "traffic": None,
+                "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
+                "measured" else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": us_bytes,
+                "avg_launch_ms": us_ms / max(us_calls, 1)}
+        line = {
+            "metric": "solves/s at 1e-8 (batched MPC QP/SOCP)",
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (LDL factor stored f32)" if args.method == "cudssmixed" else "f64",
+            "data": "synthetic (seeded PCG64, MPC batch shapes)",
+            "config": {"workload": "%d MPC-style QP/SOCPs per GPU, n~U{20..400}, "
+                                   "m~2n, 5-20 SOC(3..8)" % B,
+                       "instances_per_gpu": B, "method": args.method,
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "device_bytes": dev_bytes},
+            "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": "includes host setup (Ruiz, ordering, symbolic LDL)"},
+            "gpu_launches": launches_per_solve * args.steps,
+            "roofline": roof,
+            "phases_ms": {k: round(v[0], 3) for k, v in phases.items()},
+            "dominant_phase": {"name": dom[0], "ms": dom[1][0], "calls": dom[1][1]},
+            "batch": {"status": status_counts, "iters_mean": float(np.mean(iters)),
+                      "iters_max": int(np.max(iters)),
+                      "batch_latency_ms": 1000 * elapsed / args.steps},
+            "plain_gpu": plain,
+            "batched_vs_plain": (value / plain["value"]) if plain else None,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -343,12 +343,22 @@ class BatchSolver:
     def launch_count(self):
         return _lib.load().clgpu_solver_launch_count(self._h)
 
+    def set_profiling(self, enable=True):
+        _lib.load().clgpu_solver_set_profiling(self._h, 1 if enable else 0)
+
     def profile(self):
+        """Device time of the last solve: total and per phase (ms)."""
+        L = _lib.load()
         vals = [ctypes.c_double() for _ in range(5)]
         passes = ctypes.c_int()
-        _lib.load().clgpu_solver_get_profile(self._h, *[ctypes.byref(v) for v in vals],
-                                             ctypes.byref(passes))
-        return dict(ms_total=vals[0].value, passes=passes.value)
+        L.clgpu_solver_get_profile(self._h, *[ctypes.byref(v) for v in vals],
+                                   ctypes.byref(passes))
+        ms = (ctypes.c_double * 5)()
+        calls = (ctypes.c_longlong * 5)()
+        L.clgpu_solver_get_phase_times(self._h, ms, calls)
+        names = ["ldl_factor", "ldl_solve", "kkt_refresh", "residual", "update_scaling"]
+        return dict(ms_total=vals[0].value, passes=passes.value,
+                    phases={n: (ms[i], calls[i]) for i, n in enumerate(names)})
 
 
 class Solver(BatchSolver):

@@ -67,6 +67,13 @@ struct ConeSet {
   // per-instance flags
   const int *inst_active;  // [B] nonzero -> instance takes part
   const int *inst_sym;     // [B] 1 if every cone of the instance is symmetric
+  // per-instance ranges (cones of each type are stored instance by instance):
+  // [2*i] first index, [2*i+1] count -- nonneg rows (element index), SOC,
+  // exp, pow and PSD cones (cone index)
+  const int *rng_nn, *rng_soc, *rng_exp, *rng_pow, *rng_psd;
+  // per-cone scratch for deterministic per-instance reductions, indexed
+  // soc | exp | pow | psd (n_soc + n_exp + n_pow + n_psd entries each)
+  double *cone_tmp, *cone_tmp2;
 };
 
 // KKT value positions touched by the Hs refresh (global indices into the

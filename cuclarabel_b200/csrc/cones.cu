@@ -1338,31 +1338,14 @@ __global__ void k_nonsym_step(ConeSet cs, NonsymArgs<Ops> a, const double *__res
 }
 
 // ================================================================ barrier
-__global__ void k_nn_barrier(ConeSet cs, const double *__restrict__ z,
-                             const double *__restrict__ s, const double *__restrict__ dz,
-                             const double *__restrict__ ds, const double *alpha,
-                             const int *bt, double *bar) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double v = 0;
-  if (e < cs.n_nn) {
-    int g = cs.nn_begin + e;
-    inst = cs.row_inst[g];
-    if (active_inst(cs, inst) && bt[inst]) {
-      double a = alpha[inst];
-      double si = s[g] + a * ds[g], zi = z[g] + a * dz[g];
-      v = -logsafe(si * zi);
-    } else {
-      inst = -1;
-    }
-  }
-  seg_atomic_add(bar, 0, inst, v);
-}
+// Per-cone values go to cs.cone_tmp (soc | exp | pow | psd) and one block per
+// instance sums them, with the nonnegative rows, in a fixed order, so the
+// barrier of an instance does not depend on the rest of the batch.
 template <int G>
 __global__ void k_soc_barrier(ConeSet cs, const double *__restrict__ z_,
                               const double *__restrict__ s_, const double *__restrict__ dz_,
                               const double *__restrict__ ds_, const double *alpha,
-                              const int *bt, double *bar) {
+                              const int *bt) {
   SocCtx<G> ctx(cs);
   double a = alpha[ctx.inst];
   const double *z = z_ + ctx.off, *s = s_ + ctx.off, *dz = dz_ + ctx.off,
@@ -1377,14 +1360,13 @@ __global__ void k_soc_barrier(ConeSet cs, const double *__restrict__ z_,
   zq = group_sum<G>(zq);
   if (!ctx.valid || !bt[ctx.inst] || ctx.lane != 0) return;
   double rs = soc_res(s[0] + a * ds[0], sq), rz = soc_res(z[0] + a * dz[0], zq);
-  double v = (rs > 0 && rz > 0) ? -logsafe(rs * rz) / 2 : CUDART_INF;
-  atomicAdd(bar + ctx.inst, v);
+  cs.cone_tmp[ctx.c] = (rs > 0 && rz > 0) ? -logsafe(rs * rz) / 2 : CUDART_INF;
 }
 template <class Ops>
-__global__ void k_nonsym_barrier(ConeSet cs, NonsymArgs<Ops> a, const double *__restrict__ z,
-                                 const double *__restrict__ s, const double *__restrict__ dz,
-                                 const double *__restrict__ ds, const double *alpha,
-                                 const int *bt, double *bar) {
+__global__ void k_nonsym_barrier(ConeSet cs, NonsymArgs<Ops> a, int slot0,
+                                 const double *__restrict__ z, const double *__restrict__ s,
+                                 const double *__restrict__ dz, const double *__restrict__ ds,
+                                 const double *alpha, const int *bt) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.n) return;
   int inst = a.inst[c];
@@ -1397,12 +1379,12 @@ __global__ void k_nonsym_barrier(ConeSet cs, NonsymArgs<Ops> a, const double *__
     cz[i] = z[b + i] + al * dz[b + i];
     csv[i] = s[b + i] + al * ds[b + i];
   }
-  atomicAdd(bar + inst, Ops::barrier_dual(cz, pa) + Ops::barrier_primal(csv, pa));
+  cs.cone_tmp[slot0 + c] = Ops::barrier_dual(cz, pa) + Ops::barrier_primal(csv, pa);
 }
 __global__ void k_psd_barrier(ConeSet cs, const double *__restrict__ z,
                               const double *__restrict__ s, const double *__restrict__ dz,
                               const double *__restrict__ ds, const double *alpha,
-                              const int *bt, double *bar) {
+                              const int *bt) {
   PsdCtx p = psd_ctx(cs);
   if (!p.valid || !bt[p.inst]) return;
   int n = p.n, nm = cs.psd_nmax;
@@ -1426,40 +1408,52 @@ __global__ void k_psd_barrier(ConeSet cs, const double *__restrict__ z,
     total -= ld;
     __syncwarp();
   }
-  if (p.lane == 0) atomicAdd(bar + p.inst, total);
+  if (p.lane == 0) cs.cone_tmp[cs.n_soc + cs.n_exp + cs.n_pow + p.c] = total;
+}
+// bar[i] += nonneg rows + sum of the instance's per-cone values (fixed order)
+__global__ void k_barrier_inst(ConeSet cs, const double *__restrict__ z,
+                               const double *__restrict__ s, const double *__restrict__ dz,
+                               const double *__restrict__ ds, const double *alpha,
+                               const int *bt, double *bar) {
+  const int i = blockIdx.x;
+  if (!active_inst(cs, i) || !bt[i]) return;
+  __shared__ double red[32];
+  const double a = alpha[i];
+  double t = 0;
+  const int e0 = cs.rng_nn[2 * i], en = cs.rng_nn[2 * i + 1];
+  for (int e = threadIdx.x; e < en; e += blockDim.x) {
+    const int g = cs.nn_begin + e0 + e;
+    const double si = s[g] + a * ds[g], zi = z[g] + a * dz[g];
+    t -= logsafe(si * zi);
+  }
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    const int o_exp = cs.n_soc, o_pow = o_exp + cs.n_exp, o_psd = o_pow + cs.n_pow;
+    for (int c = 0; c < cs.rng_soc[2 * i + 1]; ++c) tot += cs.cone_tmp[cs.rng_soc[2 * i] + c];
+    for (int c = 0; c < cs.rng_exp[2 * i + 1]; ++c)
+      tot += cs.cone_tmp[o_exp + cs.rng_exp[2 * i] + c];
+    for (int c = 0; c < cs.rng_pow[2 * i + 1]; ++c)
+      tot += cs.cone_tmp[o_pow + cs.rng_pow[2 * i] + c];
+    for (int c = 0; c < cs.rng_psd[2 * i + 1]; ++c)
+      tot += cs.cone_tmp[o_psd + cs.rng_psd[2 * i] + c];
+    bar[i] += tot;
+  }
 }
 
 // ================================================================ margins
-__global__ void k_nn_margins(ConeSet cs, const double *__restrict__ z, double *amin,
-                             double *asum) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double v = 0;
-  if (e < cs.n_nn) {
-    int g = cs.nn_begin + e;
-    inst = cs.row_inst[g];
-    if (active_inst(cs, inst)) {
-      v = z[g];
-      atomic_min_any(amin + inst, v);
-    } else {
-      inst = -1;
-    }
-  }
-  seg_atomic_add(asum, 0, inst, v > 0 ? v : 0.0);
-}
 template <int G>
-__global__ void k_soc_margins(ConeSet cs, const double *__restrict__ z_, double *amin,
-                              double *asum) {
+__global__ void k_soc_margins(ConeSet cs, const double *__restrict__ z_) {
   SocCtx<G> ctx(cs);
   const double *z = z_ + ctx.off;
   double t = soc_tail_sq<G>(z, ctx);
   if (!ctx.valid || ctx.lane != 0) return;
-  double a = z[0] - sqrt(t);
-  atomic_min_any(amin + ctx.inst, a);
-  atomicAdd(asum + ctx.inst, fmax(0.0, a));
+  cs.cone_tmp[ctx.c] = z[0] - sqrt(t);
 }
-__global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z, double *amin,
-                              double *asum) {
+__global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z) {
   PsdCtx p = psd_ctx(cs);
   if (!p.valid) return;
   int n = p.n, nm = cs.psd_nmax;
@@ -1471,8 +1465,52 @@ __global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z, double *
   double pos = (p.lane < n && ev[p.lane] > 0) ? ev[p.lane] : 0.0;
   pos = warp_sum(pos);
   if (p.lane == 0) {
-    atomic_min_any(amin + p.inst, mn);
-    atomicAdd(asum + p.inst, pos);
+    const int slot = cs.n_soc + cs.n_exp + cs.n_pow + p.c;
+    cs.cone_tmp[slot] = mn;
+    cs.cone_tmp2[slot] = pos;
+  }
+}
+// margins of each instance: minimum over its cones, sum of the positive
+// parts (coneops_nncone.jl:19-39, coneops_socone.jl:310-319,
+// coneops_psdtrianglecone.jl:10-28), fixed summation order
+__global__ void k_margins_inst(ConeSet cs, const double *__restrict__ z, double *amin,
+                               double *asum) {
+  const int i = blockIdx.x;
+  if (!active_inst(cs, i)) return;
+  __shared__ double rmin[32], rsum[32];
+  double mn = kDMax, sm = 0;
+  const int e0 = cs.rng_nn[2 * i], en = cs.rng_nn[2 * i + 1];
+  for (int e = threadIdx.x; e < en; e += blockDim.x) {
+    const double v = z[cs.nn_begin + e0 + e];
+    mn = fmin(mn, v);
+    sm += v > 0 ? v : 0.0;
+  }
+  mn = warp_min(mn);
+  sm = warp_sum(sm);
+  if ((threadIdx.x & 31) == 0) {
+    rmin[threadIdx.x >> 5] = mn;
+    rsum[threadIdx.x >> 5] = sm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = kDMax, t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      m = fmin(m, rmin[w]);
+      t += rsum[w];
+    }
+    for (int c = 0; c < cs.rng_soc[2 * i + 1]; ++c) {
+      const double a = cs.cone_tmp[cs.rng_soc[2 * i] + c];
+      m = fmin(m, a);
+      t += fmax(0.0, a);
+    }
+    const int o_psd = cs.n_soc + cs.n_exp + cs.n_pow;
+    for (int c = 0; c < cs.rng_psd[2 * i + 1]; ++c) {
+      const int slot = o_psd + cs.rng_psd[2 * i] + c;
+      m = fmin(m, cs.cone_tmp[slot]);
+      t += cs.cone_tmp2[slot];
+    }
+    amin[i] = m;
+    asum[i] = t;
   }
 }
 
@@ -1755,24 +1793,23 @@ void cones_step_length_asym(const ConeSet &cs, const double *dz, const double *d
 void cones_barrier(const ConeSet &cs, const double *z, const double *s, const double *dz,
                    const double *ds, const double *alpha, const int *bt, double *bar,
                    cudaStream_t st) {
-  if (cs.n_nn)
-    k_nn_barrier<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, z, s, dz, ds, alpha, bt, bar);
-  LAUNCH_SOC(k_soc_barrier, cs, z, s, dz, ds, alpha, bt, bar);
+  LAUNCH_SOC(k_soc_barrier, cs, z, s, dz, ds, alpha, bt);
   if (cs.n_exp)
     k_nonsym_barrier<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
-        cs, exp_args(cs), z, s, dz, ds, alpha, bt, bar);
+        cs, exp_args(cs), cs.n_soc, z, s, dz, ds, alpha, bt);
   if (cs.n_pow)
     k_nonsym_barrier<PowOps><<<blocks_for(cs.n_pow, 128), 128, 0, st>>>(
-        cs, pow_args(cs), z, s, dz, ds, alpha, bt, bar);
-  LAUNCH_PSD(k_psd_barrier, 2, cs, z, s, dz, ds, alpha, bt, bar);
+        cs, pow_args(cs), cs.n_soc + cs.n_exp, z, s, dz, ds, alpha, bt);
+  LAUNCH_PSD(k_psd_barrier, 2, cs, z, s, dz, ds, alpha, bt);
+  k_barrier_inst<<<cs.B, 128, 0, st>>>(cs, z, s, dz, ds, alpha, bt, bar);
 }
 
 void cones_margins(const ConeSet &cs, const double *z, int pd, double *amin, double *asum,
                    cudaStream_t st) {
   (void)pd;
-  if (cs.n_nn) k_nn_margins<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, z, amin, asum);
-  LAUNCH_SOC(k_soc_margins, cs, z, amin, asum);
-  LAUNCH_PSD(k_psd_margins, 2, cs, z, amin, asum);
+  LAUNCH_SOC(k_soc_margins, cs, z);
+  LAUNCH_PSD(k_psd_margins, 2, cs, z);
+  k_margins_inst<<<cs.B, 128, 0, st>>>(cs, z, amin, asum);
 }
 
 void cones_scaled_unit_shift(const ConeSet &cs, double *z, const double *alpha, int pd,

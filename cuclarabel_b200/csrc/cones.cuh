@@ -44,11 +44,12 @@ void cones_step_length_asym(const ConeSet &cs, const double *dz,
                             double backtrack, double alpha_min,
                             cudaStream_t st);
 // compute_barrier: adds each instance's cone barrier at alpha[i] into bar[i]
+// (deterministic: per-cone values reduced per instance in a fixed order)
 void cones_barrier(const ConeSet &cs, const double *z, const double *s,
                    const double *dz, const double *ds, const double *alpha,
                    const int *bt_active, double *bar, cudaStream_t st);
-// margins: min margin (atomic) into amin[i] (pre-set to DBL_MAX), sum of
-// positive margins into asum[i] (pre-set to 0)
+// margins: min margin into amin[i], sum of positive margins into asum[i]
+// (deterministic per-instance reduction; outputs overwritten)
 void cones_margins(const ConeSet &cs, const double *z, int pd, double *amin,
                    double *asum, cudaStream_t st);
 void cones_scaled_unit_shift(const ConeSet &cs, double *z,

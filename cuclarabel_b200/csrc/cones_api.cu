@@ -145,6 +145,17 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
   cs.psd_R = A.alloc<double>(nn2 * cs.n_psd);
   cs.psd_Rinv = A.alloc<double>(nn2 * cs.n_psd);
   cs.psd_lam = A.alloc<double>((size_t)psd_max * cs.n_psd);
+  cs.cone_tmp = A.alloc<double>((size_t)cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd);
+  cs.cone_tmp2 = A.alloc<double>((size_t)cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd);
+  {
+    std::vector<int> rnn = {0, cs.n_nn}, rsoc = {0, cs.n_soc}, rexp = {0, cs.n_exp},
+                     rpow = {0, cs.n_pow}, rpsd = {0, cs.n_psd};
+    cs.rng_nn = A.upload(rnn);
+    cs.rng_soc = A.upload(rsoc);
+    cs.rng_exp = A.upload(rexp);
+    cs.rng_pow = A.upload(rpow);
+    cs.rng_psd = A.upload(rpsd);
+  }
   cs.inst_active = nullptr;
   h->d_nn_blk = A.upload(nn_blk);
   h->d_soc_blk = A.upload(soc_blk);
@@ -275,8 +286,6 @@ extern "C" int clgpu_margins(clgpu_cones *h, const double *z, int pd, double *al
                              double *beta, clgpu_stream_t stream) {
   if (!h) return -1;
   cudaStream_t st = (cudaStream_t)stream;
-  double init[2] = {DBL_MAX, 0.0};
-  cudaMemcpyAsync(h->d_scal + 6, init, 2 * sizeof(double), cudaMemcpyHostToDevice, st);
   cones_margins(h->cs, z, pd, h->d_scal + 6, h->d_scal + 7, st);
   double out[2];
   cudaMemcpyAsync(out, h->d_scal + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);

@@ -28,6 +28,7 @@
 namespace clgpu {
 
 static constexpr int TB = 256;
+static constexpr int kRedThreads = 128;  // threads of the per-instance reduction blocks
 static inline int nblk(long long n) { return n <= 0 ? 1 : (int)((n + TB - 1) / TB); }
 
 // masks for k_set_mask
@@ -40,6 +41,8 @@ struct Dev {
   const double *Px, *Ax, *Atx;
   const double *q, *b, *d, *dinv, *e, *einv, *negq;
   const int *col_inst, *row_inst;
+  const int *xoff;              // [B+1]
+  const int *zbeg, *zcnt;       // [6*B] per instance and cone type: global z rows
   // variables
   double *x, *s, *z, *px, *ps, *pz;       // current, previous
   double *rhs_x, *rhs_s, *rhs_z;          // step_rhs
@@ -168,80 +171,84 @@ __global__ void k_set_tau_kappa_one(Dev d) {
 }
 
 // =============================================================== residuals
-// residuals.jl:39-75 fused with the scaled norms of info.jl:66-133
-__global__ void k_resid_x(Dev d) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double v_qx = 0, v_xpx = 0, n_x = 0, n_rxinf = 0, n_px = 0, n_rx = 0;
-  if (j < d.nx) {
-    inst = d.col_inst[j];
-    if (d.active[inst]) {
-      double px = 0;
-      for (int p = d.Pp[j]; p < d.Pp[j + 1]; ++p) px += d.Px[p] * d.x[d.Pj[p]];
-      double atz = 0;
-      for (int p = d.Atp[j]; p < d.Atp[j + 1]; ++p) atz += d.Atx[p] * d.z[d.Atj[p]];
-      double rxinf = -atz;
-      double tau = SF(d, F_TAU, inst);
-      double xj = d.x[j];
-      double rx = rxinf - px - d.q[j] * tau;
-      d.Px_[j] = px;
-      d.rx_inf[j] = rxinf;
-      d.rx[j] = rx;
-      v_qx = d.q[j] * xj;
-      v_xpx = xj * px;
-      double t = d.d[j] * xj;
-      n_x = t * t;
-      t = d.dinv[j] * rxinf;
-      n_rxinf = t * t;
-      t = d.dinv[j] * px;
-      n_px = t * t;
-      t = d.dinv[j] * rx;
-      n_rx = t * t;
-    } else {
-      inst = -1;
-    }
+// Deterministic per-instance block reduction: every thread accumulates a
+// fixed strided subset in a fixed order, warps reduce by shuffles, warp
+// partials are combined in warp order.  Results do not depend on the batch.
+template <int NV, int NTH>
+__device__ __forceinline__ void block_reduce_store(double (&acc)[NV], double *S, int B,
+                                                   const int (&field)[NV], int inst) {
+  __shared__ double red[NTH / 32][NV];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double t = warp_sum(acc[v]);
+    if (lane == 0) red[wid][v] = t;
   }
-  seg_atomic_add(d.S + F_DOT_QX * d.B, 0, inst, v_qx);
-  seg_atomic_add(d.S + F_DOT_XPX * d.B, 0, inst, v_xpx);
-  seg_atomic_add(d.S + F_NRM_X * d.B, 0, inst, n_x);
-  seg_atomic_add(d.S + F_NRM_RXINF * d.B, 0, inst, n_rxinf);
-  seg_atomic_add(d.S + F_NRM_PX * d.B, 0, inst, n_px);
-  seg_atomic_add(d.S + F_NRM_RX * d.B, 0, inst, n_rx);
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0;
+    for (int w = 0; w < NTH / 32; ++w) t += red[w][threadIdx.x];
+    S[field[threadIdx.x] * B + inst] = t;
+  }
 }
-__global__ void k_resid_z(Dev d) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double v_bz = 0, v_sz = 0, n_z = 0, n_s = 0, n_rzinf = 0, n_rz = 0;
-  if (g < d.mz) {
-    inst = d.row_inst[g];
-    if (d.active[inst]) {
+
+// residuals.jl:39-75 fused with the scaled norms of info.jl:66-133; one
+// block per instance
+template <int NTH>
+__global__ void __launch_bounds__(NTH) k_residuals(Dev d) {
+  const int i = blockIdx.x;
+  if (!d.active[i]) return;
+  double acc[12];
+#pragma unroll
+  for (int v = 0; v < 12; ++v) acc[v] = 0.0;
+  const double tau = SF(d, F_TAU, i);
+  for (int j = d.xoff[i] + threadIdx.x; j < d.xoff[i + 1]; j += NTH) {
+    double px = 0;
+    for (int p = d.Pp[j]; p < d.Pp[j + 1]; ++p) px += d.Px[p] * d.x[d.Pj[p]];
+    double atz = 0;
+    for (int p = d.Atp[j]; p < d.Atp[j + 1]; ++p) atz += d.Atx[p] * d.z[d.Atj[p]];
+    const double rxinf = -atz;
+    const double xj = d.x[j];
+    const double rx = rxinf - px - d.q[j] * tau;
+    d.Px_[j] = px;
+    d.rx_inf[j] = rxinf;
+    d.rx[j] = rx;
+    acc[0] += d.q[j] * xj;
+    acc[1] += xj * px;
+    double t = d.d[j] * xj;
+    acc[2] += t * t;
+    t = d.dinv[j] * rxinf;
+    acc[3] += t * t;
+    t = d.dinv[j] * px;
+    acc[4] += t * t;
+    t = d.dinv[j] * rx;
+    acc[5] += t * t;
+  }
+  for (int ty = 0; ty < 6; ++ty) {
+    const int g0 = d.zbeg[6 * i + ty], g1 = g0 + d.zcnt[6 * i + ty];
+    for (int g = g0 + threadIdx.x; g < g1; g += NTH) {
       double ax = 0;
       for (int p = d.Ap[g]; p < d.Ap[g + 1]; ++p) ax += d.Ax[p] * d.x[d.Aj[p]];
-      double sg = d.s[g], zg = d.z[g];
-      double rzinf = ax + sg;
-      double rz = rzinf - d.b[g] * SF(d, F_TAU, inst);
+      const double sg = d.s[g], zg = d.z[g];
+      const double rzinf = ax + sg;
+      const double rz = rzinf - d.b[g] * tau;
       d.rz_inf[g] = rzinf;
       d.rz[g] = rz;
-      v_bz = d.b[g] * zg;
-      v_sz = sg * zg;
+      acc[6] += d.b[g] * zg;
+      acc[7] += sg * zg;
       double t = d.e[g] * zg;
-      n_z = t * t;
+      acc[8] += t * t;
       t = d.einv[g] * sg;
-      n_s = t * t;
+      acc[9] += t * t;
       t = d.einv[g] * rzinf;
-      n_rzinf = t * t;
+      acc[10] += t * t;
       t = d.einv[g] * rz;
-      n_rz = t * t;
-    } else {
-      inst = -1;
+      acc[11] += t * t;
     }
   }
-  seg_atomic_add(d.S + F_DOT_BZ * d.B, 0, inst, v_bz);
-  seg_atomic_add(d.S + F_DOT_SZ * d.B, 0, inst, v_sz);
-  seg_atomic_add(d.S + F_NRM_Z * d.B, 0, inst, n_z);
-  seg_atomic_add(d.S + F_NRM_S * d.B, 0, inst, n_s);
-  seg_atomic_add(d.S + F_NRM_RZINF * d.B, 0, inst, n_rzinf);
-  seg_atomic_add(d.S + F_NRM_RZ * d.B, 0, inst, n_rz);
+  const int fields[12] = {F_DOT_QX, F_DOT_XPX, F_NRM_X, F_NRM_RXINF, F_NRM_PX, F_NRM_RX,
+                          F_DOT_BZ, F_DOT_SZ, F_NRM_Z, F_NRM_S, F_NRM_RZINF, F_NRM_RZ};
+  block_reduce_store<12, NTH>(acc, d.S, d.B, fields, i);
 }
 
 __device__ void check_convergence(const Dev &d, int i, double tga, double tgr, double tf,
@@ -379,54 +386,42 @@ __global__ void k_workz(Dev d, const double *dsc) {
   if (g >= d.mz || !d.active[d.row_inst[g]]) return;
   d.workz[g] = dsc[g] - d.rhs_z[g];
 }
-// the three P products and five dots of the tau solve (kktsystem_gpu.jl:179-200)
-__global__ void k_tau_dots_x(Dev d) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
-  if (j < d.nx) {
-    inst = d.col_inst[j];
-    if (d.active[inst] && IF(d, I_KKT_OK, inst)) {
-      double tau = SF(d, F_TAU, inst);
-      double px1 = 0, pxm = 0, px2 = 0;
-      for (int p = d.Pp[j]; p < d.Pp[j + 1]; ++p) {
-        int k = d.Pj[p];
-        double v = d.Px[p];
-        px1 += v * d.x1[k];
-        pxm += v * (d.x[k] / tau - d.x2[k]);
-        px2 += v * d.x2[k];
-      }
-      double xi = d.x[j] / tau;
-      a1 = d.q[j] * d.x1[j];
-      a2 = xi * px1;
-      a3 = d.q[j] * d.x2[j];
-      a4 = (xi - d.x2[j]) * pxm;
-      a5 = d.x2[j] * px2;
-    } else {
-      inst = -1;
+// the three P products and seven dots of the tau solve
+// (kktsystem_gpu.jl:179-200); one block per instance
+template <int NTH>
+__global__ void __launch_bounds__(NTH) k_tau_dots(Dev d) {
+  const int i = blockIdx.x;
+  if (!d.active[i] || !IF(d, I_KKT_OK, i)) return;
+  double acc[7];
+#pragma unroll
+  for (int v = 0; v < 7; ++v) acc[v] = 0.0;
+  const double tau = SF(d, F_TAU, i);
+  for (int j = d.xoff[i] + threadIdx.x; j < d.xoff[i + 1]; j += NTH) {
+    double px1 = 0, pxm = 0, px2 = 0;
+    for (int p = d.Pp[j]; p < d.Pp[j + 1]; ++p) {
+      const int k = d.Pj[p];
+      const double v = d.Px[p];
+      px1 += v * d.x1[k];
+      pxm += v * (d.x[k] / tau - d.x2[k]);
+      px2 += v * d.x2[k];
+    }
+    const double xi = d.x[j] / tau;
+    acc[0] += d.q[j] * d.x1[j];
+    acc[1] += xi * px1;
+    acc[2] += d.q[j] * d.x2[j];
+    acc[3] += (xi - d.x2[j]) * pxm;
+    acc[4] += d.x2[j] * px2;
+  }
+  for (int ty = 0; ty < 6; ++ty) {
+    const int g0 = d.zbeg[6 * i + ty], g1 = g0 + d.zcnt[6 * i + ty];
+    for (int g = g0 + threadIdx.x; g < g1; g += NTH) {
+      acc[5] += d.b[g] * d.z1[g];
+      acc[6] += d.b[g] * d.z2[g];
     }
   }
-  seg_atomic_add(d.S + F_DOT_Q_X1 * d.B, 0, inst, a1);
-  seg_atomic_add(d.S + F_DOT_XI_PX1 * d.B, 0, inst, a2);
-  seg_atomic_add(d.S + F_DOT_Q_X2 * d.B, 0, inst, a3);
-  seg_atomic_add(d.S + F_QF1 * d.B, 0, inst, a4);
-  seg_atomic_add(d.S + F_QF2 * d.B, 0, inst, a5);
-}
-__global__ void k_tau_dots_z(Dev d) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double a1 = 0, a2 = 0;
-  if (g < d.mz) {
-    inst = d.row_inst[g];
-    if (d.active[inst] && IF(d, I_KKT_OK, inst)) {
-      a1 = d.b[g] * d.z1[g];
-      a2 = d.b[g] * d.z2[g];
-    } else {
-      inst = -1;
-    }
-  }
-  seg_atomic_add(d.S + F_DOT_B_Z1 * d.B, 0, inst, a1);
-  seg_atomic_add(d.S + F_DOT_B_Z2 * d.B, 0, inst, a2);
+  const int fields[7] = {F_DOT_Q_X1, F_DOT_XI_PX1, F_DOT_Q_X2, F_QF1, F_QF2, F_DOT_B_Z1,
+                         F_DOT_B_Z2};
+  block_reduce_store<7, NTH>(acc, d.S, d.B, fields, i);
 }
 __global__ void k_tau_solve(Dev d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -571,20 +566,20 @@ __global__ void k_bt_setup(Dev d, InstConst ic) {
   IF(d, I_BT_ACTIVE, i) = bt ? 1 : 0;
   if (bt) atomicAdd(d.counter + 1, 1);
 }
-__global__ void k_dot_shifted(Dev d) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  int inst = -1;
-  double v = 0;
-  if (g < d.mz) {
-    inst = d.row_inst[g];
-    if (d.active[inst]) {
-      double a = SF(d, F_ALPHA, inst);
-      v = (d.z[g] + a * d.dz[g]) * (d.s[g] + a * d.ds[g]);
-    } else {
-      inst = -1;
-    }
+// dot_shifted (mathutils.jl:23-43) per instance, deterministic
+template <int NTH>
+__global__ void __launch_bounds__(NTH) k_dot_shifted(Dev d) {
+  const int i = blockIdx.x;
+  if (!d.active[i]) return;
+  double acc[1] = {0.0};
+  const double a = SF(d, F_ALPHA, i);
+  for (int ty = 0; ty < 6; ++ty) {
+    const int g0 = d.zbeg[6 * i + ty], g1 = g0 + d.zcnt[6 * i + ty];
+    for (int g = g0 + threadIdx.x; g < g1; g += NTH)
+      acc[0] += (d.z[g] + a * d.dz[g]) * (d.s[g] + a * d.ds[g]);
   }
-  seg_atomic_add(d.S + F_TAU_NUM * d.B, 0, inst, v);
+  const int fields[1] = {F_TAU_NUM};
+  block_reduce_store<1, NTH>(acc, d.S, d.B, fields, i);
 }
 __global__ void k_bt_central(Dev d, InstConst ic) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -738,11 +733,55 @@ struct clgpu_solver {
   bool solved = false;
   long long launches = 0;
   bool profiling = false;
+  // per-phase device time of the last solve (ms): factor, ldl solve, cone
+  // kernels, residual/vector kernels, update_scaling alone
   double prof[5] = {0, 0, 0, 0, 0};
+  long long prof_calls[5] = {0, 0, 0, 0, 0};
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<int, int>>> ev_marks;  // class, (ev begin, ev end)
+  size_t ev_next = 0;
+  int prof_open = -1, prof_open_ev = -1;
   int passes = 0;
   double last_ms = 0;
   ~clgpu_solver() {
     if (h_counter) cudaFreeHost(h_counter);
+    for (auto e : ev_pool) cudaEventDestroy(e);
+  }
+  int next_event() {
+    if (ev_next == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    return (int)ev_next++;
+  }
+  void prof_begin(int cls, cudaStream_t st) {
+    if (!profiling) return;
+    int e = next_event();
+    cudaEventRecord(ev_pool[e], st);
+    prof_open = cls;
+    prof_open_ev = e;
+  }
+  void prof_end(cudaStream_t st) {
+    if (!profiling || prof_open < 0) return;
+    int e = next_event();
+    cudaEventRecord(ev_pool[e], st);
+    ev_marks.push_back({prof_open, {prof_open_ev, e}});
+    prof_open = -1;
+  }
+  void prof_collect() {
+    for (int c = 0; c < 5; ++c) {
+      prof[c] = 0;
+      prof_calls[c] = 0;
+    }
+    for (auto &m : ev_marks) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev_pool[m.second.first], ev_pool[m.second.second]);
+      prof[m.first] += ms;
+      prof_calls[m.first] += 1;
+    }
+    ev_marks.clear();
+    ev_next = 0;
   }
 };
 
@@ -870,8 +909,6 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
       // A^T rows = A columns (CSC of A)
       for (int j = 0; j < p.n; ++j) {
         for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k) {
-          int lr_type = -1;
-          (void)lr_type;
           Atj.push_back(0);  // fixed below
           Atxv.push_back(p.A.x[k]);
         }
@@ -971,6 +1008,36 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   cs.soc_group = G;
   cs.psd_nmax = std::max(psd_nmax, 1);
   if (psd_nmax > 16) return -3;  // PSD side limited to 16 (warp-per-cone kernels)
+  {
+    // per-instance ranges of each cone type (cones are stored instance by
+    // instance inside each type list)
+    std::vector<int> rnn(2 * (size_t)B), rsoc(2 * (size_t)B), rexp(2 * (size_t)B),
+        rpow(2 * (size_t)B), rpsd(2 * (size_t)B);
+    int cnn = 0, csoc = 0, cexp = 0, cpow = 0, cpsd = 0;
+    for (int i = 0; i < B; ++i) {
+      auto &p = prep[i];
+      rnn[2 * i] = cnn;
+      rnn[2 * i + 1] = p.type_rows[1];
+      cnn += p.type_rows[1];
+      rsoc[2 * i] = csoc;
+      rsoc[2 * i + 1] = p.type_cones[2];
+      csoc += p.type_cones[2];
+      rexp[2 * i] = cexp;
+      rexp[2 * i + 1] = p.type_cones[3];
+      cexp += p.type_cones[3];
+      rpow[2 * i] = cpow;
+      rpow[2 * i + 1] = p.type_cones[4];
+      cpow += p.type_cones[4];
+      rpsd[2 * i] = cpsd;
+      rpsd[2 * i + 1] = p.type_cones[5];
+      cpsd += p.type_cones[5];
+    }
+    cs.rng_nn = A.upload(rnn);
+    cs.rng_soc = A.upload(rsoc);
+    cs.rng_exp = A.upload(rexp);
+    cs.rng_pow = A.upload(rpow);
+    cs.rng_psd = A.upload(rpsd);
+  }
   cs.row_inst = A.upload(row_inst);
   cs.soc_off = A.upload(soc_off);
   cs.soc_dim = A.upload(soc_dim);
@@ -1002,8 +1069,10 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   cs.psd_R = A.alloc<double>(nn2 * cs.n_psd);
   cs.psd_Rinv = A.alloc<double>(nn2 * cs.n_psd);
   cs.psd_lam = A.alloc<double>((size_t)cs.psd_nmax * cs.n_psd);
+  cs.cone_tmp = A.alloc<double>((size_t)cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd);
+  cs.cone_tmp2 = A.alloc<double>((size_t)cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd);
   // ---------------- KKT arrays (concatenate with global positions)
-  std::vector<int> N(B), voff(B + 1, 0), poff(B, 0);
+  std::vector<int> N(B), voff(B + 1, 0), poff(B, 0), lvl_off(B), nlev(B), lvl_ptr, lvl_nodes;
   long long knz = 0, lnz = 0, rnz = 0;
   for (int i = 0; i < B; ++i) {
     N[i] = prep[i].N;
@@ -1012,6 +1081,10 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
     knz += prep[i].Kj.size();
     lnz += prep[i].Li.size();
     rnz += prep[i].Rk.size();
+    lvl_off[i] = (int)lvl_ptr.size();
+    nlev[i] = (int)prep[i].lvl_ptr.size() - 1;
+    lvl_ptr.insert(lvl_ptr.end(), prep[i].lvl_ptr.begin(), prep[i].lvl_ptr.end());
+    lvl_nodes.insert(lvl_nodes.end(), prep[i].lvl_nodes.begin(), prep[i].lvl_nodes.end());
   }
   if (knz > 2000000000LL || lnz > 2000000000LL) return -4;
   const int VT = voff[B], PT = voff[B] + B;
@@ -1024,7 +1097,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   long long kb = 0, lb = 0, rb = 0;
   int max_small = 0;
   bool has_small = false, has_large = false;
-  const int tsize = h->mixed ? 4 : 8;
+  const int tsize = 8;  // work vectors are FP64 in both precision forms
   // NN / SOC / etc. refresh maps must follow the global cone order: type by
   // type, instance by instance -- collect per type.
   std::vector<std::vector<int>> nn_by_inst(B);
@@ -1146,19 +1219,23 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   kk.Rp = A.upload(Rp);
   kk.Rk = A.upload(Rk);
   kk.Rpos = A.upload(Rpos);
+  kk.lvl_off = A.upload(lvl_off);
+  kk.nlev = A.upload(nlev);
+  kk.lvl_ptr = A.upload(lvl_ptr);
+  kk.lvl_nodes = A.upload(lvl_nodes);
   if (h->mixed) {
     kk.Lx = A.alloc<float>((size_t)lnz);
     kk.D = A.alloc<float>(VT);
     kk.Dinv = A.alloc<float>(VT);
-    kk.yf = A.alloc<float>(VT);
-    kk.w = A.alloc<float>(VT);
+    kk.Lacc = A.alloc<double>((size_t)lnz);
   } else {
     kk.Lx = A.alloc<double>((size_t)lnz);
     kk.D = A.alloc<double>(VT);
     kk.Dinv = A.alloc<double>(VT);
-    kk.yf = A.alloc<double>(VT);
-    kk.w = A.alloc<double>(VT);
+    kk.Lacc = nullptr;
   }
+  kk.yf = A.alloc<double>(VT);
+  kk.w = A.alloc<double>(VT);
   kk.max_small_N = max_small;
   kk.has_small = has_small;
   kk.has_large = has_large;
@@ -1189,6 +1266,21 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   dv.einv = A.upload(eeinv);
   dv.col_inst = A.upload(col_inst);
   dv.row_inst = cs.row_inst;
+  {
+    std::vector<int> zb(6 * (size_t)B, 0), zc(6 * (size_t)B, 0);
+    for (int i = 0; i < B; ++i) {
+      int lr = 0;
+      for (int t = 0; t < 6; ++t) {
+        int cnt = prep[i].type_rows[t];
+        zc[6 * i + t] = cnt;
+        zb[6 * i + t] = cnt > 0 ? grow[i][lr] : 0;
+        lr += cnt;
+      }
+    }
+    dv.xoff = A.upload(xoff);
+    dv.zbeg = A.upload(zb);
+    dv.zcnt = A.upload(zc);
+  }
   double **xv[] = {&dv.x, &dv.px, &dv.rhs_x, &dv.dx, &dv.rx, &dv.rx_inf, &dv.Px_, &dv.x1,
                    &dv.x2, &dv.zerox};
   for (auto p : xv) *p = A.alloc<double>(nx);
@@ -1311,11 +1403,17 @@ struct Phase {
   }
   // kkt_update!: Hs refresh, regularise + refactor, constant rhs solve
   void kkt_update() {
+    h->prof_begin(2, st);
     cones_refresh_kkt(h->cs, h->map, h->kk.Kx, st);
+    h->prof_end(st);
     int *ok = h->dv.I + I_KKT_OK * h->B;
+    h->prof_begin(0, st);
     ldl_factor(h->kk, h->mixed, h->lp, h->dv.active, ok, h->dv.S + F_KKT_EPS * h->B, st);
+    h->prof_end(st);
+    h->prof_begin(1, st);
     ldl_solve(h->kk, h->mixed, h->lp, h->dv.active, h->dv.negq, h->dv.b, h->dv.x2, h->dv.z2,
               ok, st);
+    h->prof_end(st);
     h->launches += 12;
   }
   // kkt_solve! (kktsystem_gpu.jl:139-227)
@@ -1330,15 +1428,10 @@ struct Phase {
     }
     k_workz<<<nblk(dv.mz), TB, 0, st>>>(dv, dsc);
     int *ok = dv.I + I_KKT_OK * h->B;
+    h->prof_begin(1, st);
     ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.rhs_x, dv.workz, dv.x1, dv.z1, ok, st);
-    zero(F_DOT_Q_X1, 1);
-    zero(F_DOT_B_Z1, 1);
-    zero(F_DOT_XI_PX1, 1);
-    zero(F_DOT_Q_X2, 1);
-    zero(F_DOT_B_Z2, 1);
-    zero(F_QF1, 2);
-    k_tau_dots_x<<<nblk(dv.nx), TB, 0, st>>>(dv);
-    k_tau_dots_z<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    h->prof_end(st);
+    k_tau_dots<kRedThreads><<<h->B, kRedThreads, 0, st>>>(dv);
     k_tau_solve<<<nblk(h->B), TB, 0, st>>>(dv);
     k_lhs_xz<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
     cones_mul_Hs(h->cs, dv.ds, dv.dz, st);
@@ -1361,10 +1454,9 @@ struct Phase {
   }
   void residuals() {
     Dev &dv = h->dv;
-    zero(F_DOT_QX, 4);   // QX, BZ, SZ, XPX
-    zero(F_NRM_X, 8);    // the norm accumulators
-    k_resid_x<<<nblk(dv.nx), TB, 0, st>>>(dv);
-    k_resid_z<<<nblk(dv.mz), TB, 0, st>>>(dv);
+    h->prof_begin(3, st);
+    k_residuals<kRedThreads><<<h->B, kRedThreads, 0, st>>>(dv);
+    h->prof_end(st);
     h->launches += 4;
   }
   int read_counter(int which) {
@@ -1439,8 +1531,10 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     k_reset_vars<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_reset);
     P.mask(M_PASS);
     // update_scaling
+    h->prof_begin(4, st);
     cones_update_scaling(h->cs, dv.s, dv.z, dv.S + F_MU * B, dv.I + I_SCALING * B,
                          dv.I + I_SCALE_OK * B, st);
+    h->prof_end(st);
     k_after_scaling<<<nblk(B), TB, 0, st>>>(dv);
     P.mask(M_PASS);
     // KKT update and affine step
@@ -1463,9 +1557,8 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
       if (P.read_counter(1) > 0) {
         P.mask(M_BT);
         for (int j = 0; j < 50; ++j) {
-          P.zero(F_TAU_NUM, 1);
           P.zero(F_BARRIER, 1);
-          k_dot_shifted<<<nblk(dv.mz), TB, 0, st>>>(dv);
+          k_dot_shifted<kRedThreads><<<B, kRedThreads, 0, st>>>(dv);
           k_bt_central<<<nblk(B), TB, 0, st>>>(dv, h->ic);
           cones_barrier(h->cs, dv.z, dv.s, dv.dz, dv.ds, dv.S + F_ALPHA * B,
                         dv.I + I_BT_ACTIVE * B, dv.S + F_BARRIER * B, st);
@@ -1484,9 +1577,28 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     cudaMemsetAsync(dv.counter, 0, sizeof(int), st);
     k_count_running<<<nblk(B), TB, 0, st>>>(dv);
     h->launches += 25;
-    if (P.read_counter(0) == 0) break;
+    int running = P.read_counter(0);
+    if (h->st.verbose) {
+      // per-pass trace of instance 0 (same columns as the CPU oracle's)
+      double sv[NUM_SCALARS];
+      int iv[NUM_INTS];
+      for (int f = 0; f < NUM_SCALARS; ++f)
+        cudaMemcpy(&sv[f], dv.S + (size_t)f * B, sizeof(double), cudaMemcpyDeviceToHost);
+      for (int f = 0; f < NUM_INTS; ++f)
+        cudaMemcpy(&iv[f], dv.I + (size_t)f * B, sizeof(int), cudaMemcpyDeviceToHost);
+      std::fprintf(stderr,
+                   "%3d  %+.8e  %+.8e  %.2e %.2e %.2e %.2e %.2e  a=%.3e st=%d sc=%d ok=%d\n",
+                   iv[I_ITER], sv[F_COST_P], sv[F_COST_D], sv[F_GAP_REL], sv[F_RES_P],
+                   sv[F_RES_D], sv[F_KTRATIO], sv[F_MU], sv[F_ALPHA], iv[I_STATUS],
+                   iv[I_SCALING], iv[I_KKT_OK]);
+    }
+    if (running == 0) break;
   }
   h->passes = passes;
+  if (h->profiling) {
+    cudaStreamSynchronize(st);
+    h->prof_collect();
+  }
   // post-process
   k_post_status<<<nblk(B), TB, 0, st>>>(dv, h->sd);
   double *ox = h->d_out, *os = ox + dv.nx, *oz = os + dv.mz;
@@ -1586,6 +1698,14 @@ extern "C" int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
   if (ms_cones) *ms_cones = h->prof[2];
   if (ms_residual) *ms_residual = h->prof[3];
   if (passes) *passes = h->passes;
+  return 0;
+}
+extern "C" int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms, long long *calls) {
+  if (!h) return -1;
+  for (int c = 0; c < 5; ++c) {
+    if (ms) ms[c] = h->prof[c];
+    if (calls) calls[c] = h->prof_calls[c];
+  }
   return 0;
 }
 extern "C" int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,

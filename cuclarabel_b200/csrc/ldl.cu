@@ -2,25 +2,39 @@
 //
 // One thread block per instance.  Instances whose KKT dimension fits keep
 // their dense work vector in shared memory and run on a single warp (NT=32:
-// __syncwarp between dependent steps, no block barriers); larger instances
-// run on 256 threads with the work vector in global scratch.
+// __syncwarp between dependent steps); larger instances run on 256 threads
+// with the work vector in global scratch.
 //
-// Factorisation: left-looking by columns on the permuted matrix.  For column
-// j the lower part of K(:,j) (row j of the symmetric permuted CSR, entries
-// with col >= j) is scattered into w, every earlier column k with L(j,k) != 0
-// is applied as w(j:) -= L(j:,k) * (L(j,k) D(k)) (the (k, pos) list of row j
-// is precomputed by the symbolic phase), then D(j) = w(j) and
-// L(j+1:,j) = w / D(j).  Static regularisation (kktsolver_directldl_gpu.jl:
-// 216-260: eps = c + prop*||diag||_inf, diag +/- eps by the expected sign)
-// is applied inside the scatter so the stored KKT keeps its true diagonal
-// for the refinement residual; dynamic regularisation follows the CPU path
+// Both the factorisation and the triangular solves are scheduled by
+// elimination-tree levels (computed once by the symbolic phase): a column
+// depends only on columns of lower levels, so every column of a level is
+// processed concurrently and one barrier separates levels.  The KKT trees of
+// the interior-point systems are bushy (height ~ N/10), which turns the
+// O(N) chain of dependent steps into O(height).
+//
+// Factorisation, left-looking:
+//   * wide level (>= NT/2 columns): one thread per column.  The column's
+//     entries are accumulated in place: the lower part of K(:,j) and every
+//     update column k (k in row j of L) are merged into column j's sorted
+//     row list (the etree guarantees struct(L(j+1:,k)) is a subset of
+//     struct(L(:,j))).
+//   * narrow level: the whole block cooperates on one column through a dense
+//     accumulator indexed by row; the update columns are applied one after
+//     another with the threads spread over each column's rows.
+// No floating-point atomics are used, so the factor of an instance is
+// bitwise identical whether it is solved alone or inside any batch.
+// Static regularisation (kktsolver_directldl_gpu.jl:216-260: eps = c +
+// prop*||diag||_inf, diag +/- eps by the expected sign) is applied when the
+// diagonal is read, so the stored KKT keeps its true diagonal for the
+// refinement residual; dynamic regularisation follows the CPU path
 // (sign*D(j) <= eps_dyn -> D(j) = sign*delta).
 //
-// Solve: forward (column-oriented scatter), diagonal, backward (column dot
-// products with a warp reduction), then iterative refinement against the
-// unregularised KKT exactly as kktsolver_directldl_gpu.jl:349-409.  In the
-// mixed-precision form L, D and the triangular solves are FP32 while the
-// refinement residual, the right-hand side and the iterate stay FP64.
+// Solve: forward substitution gathers each row of L (row pattern), backward
+// substitution gathers each column, both level by level; then iterative
+// refinement against the unregularised KKT exactly as
+// kktsolver_directldl_gpu.jl:349-409.  In the mixed-precision form (the
+// reference's :cudssmixed) L and D are STORED in FP32; accumulation,
+// substitution arithmetic, the refinement residual and the iterate are FP64.
 #include "ldl.cuh"
 
 namespace clgpu {
@@ -71,8 +85,20 @@ __device__ __forceinline__ double block_max(double v, double *red) {
 }
 
 // class of an instance: 1 = small (single warp, smem), 2 = large
-__device__ __forceinline__ int inst_class(int N, int tsize) {
-  return (long long)N * tsize <= kSmemLimitBytes ? 1 : 2;
+__device__ __forceinline__ int inst_class(int N) {
+  return (long long)N * (long long)sizeof(double) <= kSmemLimitBytes ? 1 : 2;
+}
+
+template <typename T>
+__device__ __forceinline__ double pivot(double dj, signed char sg, const LDLParams &prm,
+                                        T &djs) {
+  if (prm.dyn_reg) {
+    double sgn = double(sg);
+    if (sgn * dj <= prm.dyn_eps) dj = prm.dyn_delta * sgn;
+  }
+  // rounded to the storage precision first so D and Dinv stay consistent
+  djs = T(dj);
+  return 1.0 / double(djs);
 }
 
 template <typename T, int NT, bool SMEM>
@@ -81,21 +107,23 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
   int inst = blockIdx.x;
   if (!run[inst]) return;
   int N = k.N[inst];
-  if (inst_class(N, sizeof(T)) != (SMEM ? 1 : 2)) return;
+  if (inst_class(N) != (SMEM ? 1 : 2)) return;
   __shared__ double red[NT / 32 + 1];
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  int vo = k.voff[inst], po = k.poff[inst];
-  T *w = SMEM ? reinterpret_cast<T *>(sm_raw) : reinterpret_cast<T *>(k.w) + vo;
+  const int vo = k.voff[inst], po = k.poff[inst];
+  double *w = SMEM ? reinterpret_cast<double *>(sm_raw) : k.w + vo;
   T *Lx = reinterpret_cast<T *>(k.Lx);
+  double *Lacc = k.Lacc ? k.Lacc : reinterpret_cast<double *>(k.Lx);  // FP64 accumulator
   T *D = reinterpret_cast<T *>(k.D) + vo;
   T *Dinv = reinterpret_cast<T *>(k.Dinv) + vo;
   const int *Kp = k.Kp + po, *Lp = k.Lp + po, *Rp = k.Rp + po;
   const int *Kdiag = k.Kdiag + vo;
+  const int *nodes = k.lvl_nodes + vo;
+  const int *lptr = k.lvl_ptr + k.lvl_off[inst];
+  const int nlev = k.nlev[inst];
   const signed char *sg = k.Dsign + vo;
-  int tid = threadIdx.x, lane = tid & 31;
-  if (SMEM)
-    for (int i = tid; i < N; i += NT) w[i] = T(0);
-  // static regulariser from the true diagonal
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += NT) w[i] = 0.0;
   double eps = 0;
   if (prm.static_reg) {
     double mx = 0;
@@ -105,85 +133,172 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
   }
   bar_sync<NT>();
   bool finite = true;
-  for (int j = 0; j < N; ++j) {
-    // scatter the lower part of column j (row j, cols >= j)
-    for (int p = Kp[j] + tid; p < Kp[j + 1]; p += NT) {
-      int c = k.Kj[p];
-      if (c > j)
-        w[c] = T(k.Kx[p]);
-      else if (c == j)
-        w[c] = T(k.Kx[p] + (sg[j] > 0 ? eps : -eps));
-    }
-    bar_sync<NT>();
-    // left-looking updates from the columns in row j of L
-    int q0 = Rp[j], q1 = Rp[j + 1];
-    for (int qb = q0; qb < q1; qb += 32) {
-      int myk = 0, mypos = 0, myend = 0;
-      T myf = T(0);
-      if (qb + lane < q1) {
-        myk = k.Rk[qb + lane];
-        mypos = k.Rpos[qb + lane];
-        myend = Lp[myk + 1];
-        myf = Lx[mypos] * D[myk];
+  for (int l = 0; l < nlev; ++l) {
+    const int a = lptr[l], b = lptr[l + 1];
+    if (b - a >= NT / 2) {
+      // ---- wide level: one thread per column, merge into the column
+      for (int idx = a + tid; idx < b; idx += NT) {
+        const int j = nodes[idx];
+        const int q0 = Lp[j], q1 = Lp[j + 1];
+        for (int q = q0; q < q1; ++q) Lacc[q] = 0.0;
+        double dj = 0.0;
+        int q = q0;
+        for (int p = Kp[j]; p < Kp[j + 1]; ++p) {
+          int c = k.Kj[p];
+          if (c < j) continue;
+          if (c == j) {
+            dj = k.Kx[p] + (sg[j] > 0 ? eps : -eps);
+            continue;
+          }
+          while (q < q1 && k.Li[q] != c) ++q;
+          if (q < q1) Lacc[q] = k.Kx[p];
+        }
+        for (int r = Rp[j]; r < Rp[j + 1]; ++r) {
+          const int kk = k.Rk[r], pos = k.Rpos[r];
+          const double ljk = double(Lx[pos]);
+          const double f = ljk * double(D[kk]);
+          dj -= ljk * f;
+          const int pe = Lp[kk + 1];
+          q = q0;
+          for (int p = pos + 1; p < pe; ++p) {
+            const int i = k.Li[p];
+            while (q < q1 && k.Li[q] != i) ++q;
+            if (q < q1) Lacc[q] -= double(Lx[p]) * f;
+          }
+        }
+        T djs;
+        double dinv = pivot<T>(dj, sg[j], prm, djs);
+        if (!isfinite(dinv) || !isfinite(double(djs))) finite = false;
+        for (int qq = q0; qq < q1; ++qq) Lx[qq] = T(Lacc[qq] * dinv);
+        D[j] = djs;
+        Dinv[j] = T(dinv);
       }
-      int cnt = min(32, q1 - qb);
-      for (int t = 0; t < cnt; ++t) {
-        int pos = __shfl_sync(0xffffffffu, mypos, t);
-        int end = __shfl_sync(0xffffffffu, myend, t);
-        T f = __shfl_sync(0xffffffffu, myf, t);
-        for (int p = pos + tid; p < end; p += NT) w[k.Li[p]] -= Lx[p] * f;
+      bar_sync<NT>();
+    } else {
+      // ---- narrow level: the block cooperates on each column
+      for (int idx = a; idx < b; ++idx) {
+        const int j = nodes[idx];
+        for (int p = Kp[j] + tid; p < Kp[j + 1]; p += NT) {
+          int c = k.Kj[p];
+          if (c > j)
+            w[c] = k.Kx[p];
+          else if (c == j)
+            w[c] = k.Kx[p] + (sg[j] > 0 ? eps : -eps);
+        }
+        bar_sync<NT>();
+        // update columns applied one after another (threads over the rows
+        // of each update column, fixed order: the result is bitwise
+        // reproducible and independent of the batch composition)
+        const int r0 = Rp[j], r1 = Rp[j + 1];
+        for (int rb = r0; rb < r1; rb += 32) {
+          const int lane = tid & 31;
+          int mypos = 0, myend = 0;
+          double myf = 0.0, myl = 0.0;
+          if (rb + lane < r1) {
+            const int kk = k.Rk[rb + lane];
+            mypos = k.Rpos[rb + lane];
+            myend = Lp[kk + 1];
+            myl = double(Lx[mypos]);
+            myf = myl * double(D[kk]);
+          }
+          const int cnt = min(32, r1 - rb);
+          for (int t = 0; t < cnt; ++t) {
+            const int pos = __shfl_sync(0xffffffffu, mypos, t);
+            const int pe = __shfl_sync(0xffffffffu, myend, t);
+            const double f = __shfl_sync(0xffffffffu, myf, t);
+            const double ljk = __shfl_sync(0xffffffffu, myl, t);
+            if (tid == 0) w[j] -= ljk * f;
+            for (int p = pos + 1 + tid; p < pe; p += NT) w[k.Li[p]] -= double(Lx[p]) * f;
+            bar_sync<NT>();
+          }
+        }
+        const double dj = w[j];
+        T djs;
+        const double dinv = pivot<T>(dj, sg[j], prm, djs);
+        if (!isfinite(dinv) || !isfinite(double(djs))) finite = false;
+        for (int q = Lp[j] + tid; q < Lp[j + 1]; q += NT) {
+          const int i = k.Li[q];
+          Lx[q] = T(w[i] * dinv);
+          w[i] = 0.0;
+        }
+        bar_sync<NT>();
+        if (tid == 0) {
+          D[j] = djs;
+          Dinv[j] = T(dinv);
+          w[j] = 0.0;
+        }
         bar_sync<NT>();
       }
     }
-    T dj = w[j];
-    if (prm.dyn_reg) {
-      T sgn = T(sg[j]);
-      if (sgn * dj <= T(prm.dyn_eps)) dj = T(prm.dyn_delta) * sgn;
-    }
-    T dinv = T(1) / dj;
-    if (!isfinite((double)dinv)) finite = false;
-    for (int p = Lp[j] + tid; p < Lp[j + 1]; p += NT) {
-      int i = k.Li[p];
-      Lx[p] = w[i] * dinv;
-      w[i] = T(0);
-    }
-    if (tid == 0) {
-      D[j] = dj;
-      Dinv[j] = dinv;
-      w[j] = T(0);
-    }
-    bar_sync<NT>();
   }
+  double bad = block_max<NT>(finite ? 0.0 : 1.0, red);
   if (tid == 0) {
-    if (!finite) ok[inst] = 0;
+    if (bad > 0) ok[inst] = 0;
     if (eps_out) eps_out[inst] = eps;
   }
 }
 
-// y <- L^{-T} D^{-1} L^{-1} y  (y in factor precision)
+// y <- L^{-T} D^{-1} L^{-1} y, level-scheduled gathers
 template <typename T, int NT>
-__device__ void ldl_trisolve(const KKTDev &k, int N, int vo, int po, T *y, double *red) {
+__device__ void ldl_trisolve(const KKTDev &k, int inst, int N, int vo, int po, double *y,
+                             double *red) {
   const T *Lx = reinterpret_cast<const T *>(k.Lx);
   const T *Dinv = reinterpret_cast<const T *>(k.Dinv) + vo;
-  const int *Lp = k.Lp + po;
-  int tid = threadIdx.x;
-  for (int j = 0; j < N; ++j) {
-    T yj = y[j];
-    for (int p = Lp[j] + tid; p < Lp[j + 1]; p += NT) y[k.Li[p]] -= Lx[p] * yj;
-    bar_sync<NT>();
+  const int *Lp = k.Lp + po, *Rp = k.Rp + po;
+  const int *nodes = k.lvl_nodes + vo;
+  const int *lptr = k.lvl_ptr + k.lvl_off[inst];
+  const int nlev = k.nlev[inst];
+  const int tid = threadIdx.x;
+  // forward: y_i -= sum_k L(i,k) y_k over the row pattern of i
+  for (int l = 0; l < nlev; ++l) {
+    const int a = lptr[l], b = lptr[l + 1];
+    if (b - a >= NT / 2) {
+      for (int idx = a + tid; idx < b; idx += NT) {
+        const int i = nodes[idx];
+        double t = y[i];
+        for (int r = Rp[i]; r < Rp[i + 1]; ++r) t -= double(Lx[k.Rpos[r]]) * y[k.Rk[r]];
+        y[i] = t;
+      }
+      bar_sync<NT>();
+    } else {
+      for (int idx = a; idx < b; ++idx) {
+        const int i = nodes[idx];
+        double t = 0.0;
+        for (int r = Rp[i] + tid; r < Rp[i + 1]; r += NT)
+          t += double(Lx[k.Rpos[r]]) * y[k.Rk[r]];
+        t = block_sum<NT>(t, red);
+        if (tid == 0) y[i] -= t;
+        bar_sync<NT>();
+      }
+    }
   }
-  for (int i = tid; i < N; i += NT) y[i] *= Dinv[i];
+  for (int i = tid; i < N; i += NT) y[i] *= double(Dinv[i]);
   bar_sync<NT>();
-  for (int j = N - 1; j >= 0; --j) {
-    double t = 0;
-    for (int p = Lp[j] + tid; p < Lp[j + 1]; p += NT) t += double(Lx[p] * y[k.Li[p]]);
-    t = block_sum<NT>(t, red);
-    if (tid == 0) y[j] -= T(t);
-    bar_sync<NT>();
+  // backward: y_j -= sum_i L(i,j) y_i over column j (ancestors)
+  for (int l = nlev - 1; l >= 0; --l) {
+    const int a = lptr[l], b = lptr[l + 1];
+    if (b - a >= NT / 2) {
+      for (int idx = a + tid; idx < b; idx += NT) {
+        const int j = nodes[idx];
+        double t = y[j];
+        for (int p = Lp[j]; p < Lp[j + 1]; ++p) t -= double(Lx[p]) * y[k.Li[p]];
+        y[j] = t;
+      }
+      bar_sync<NT>();
+    } else {
+      for (int idx = a; idx < b; ++idx) {
+        const int j = nodes[idx];
+        double t = 0.0;
+        for (int p = Lp[j] + tid; p < Lp[j + 1]; p += NT) t += double(Lx[p]) * y[k.Li[p]];
+        t = block_sum<NT>(t, red);
+        if (tid == 0) y[j] -= t;
+        bar_sync<NT>();
+      }
+    }
   }
 }
 
-// e = b - K xi ; returns ||e||_inf (NaN/Inf propagate)
+// e = b - K xi ; returns ||e||_inf (non-finite -> +inf)
 template <int NT>
 __device__ double refine_error(const KKTDev &k, int N, int po, const double *b,
                                const double *xi, double *e, double *red) {
@@ -210,27 +325,26 @@ __global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const
   int inst = blockIdx.x;
   if (!run[inst] || !ok[inst]) return;
   int N = k.N[inst];
-  if (inst_class(N, sizeof(T)) != (SMEM ? 1 : 2)) return;
+  if (inst_class(N) != (SMEM ? 1 : 2)) return;
   __shared__ double red[NT / 32 + 1];
   extern __shared__ __align__(16) unsigned char sm_raw[];
   int vo = k.voff[inst], po = k.poff[inst];
   int tid = threadIdx.x;
-  T *y = SMEM ? reinterpret_cast<T *>(sm_raw) : reinterpret_cast<T *>(k.yf) + vo;
+  double *y = SMEM ? reinterpret_cast<double *>(sm_raw) : k.yf + vo;
   double *b = k.b + vo, *x = k.x + vo, *e = k.e + vo, *dx = k.dx + vo;
   const int *gs = k.gsrc + vo;
-  // gather the right-hand side in permuted order
   double nb = 0;
   for (int i = tid; i < N; i += NT) {
     int g = gs[i];
     double v = g >= 0 ? rx[g] : (g == -1 ? 0.0 : rz[-g - 2]);
     b[i] = v;
-    y[i] = T(v);
+    y[i] = v;
     nb = fmax(nb, fabs(v));
   }
   double normb = block_max<NT>(nb, red);
   bar_sync<NT>();
-  ldl_trisolve<T, NT>(k, N, vo, po, y, red);
-  for (int i = tid; i < N; i += NT) x[i] = double(y[i]);
+  ldl_trisolve<T, NT>(k, inst, N, vo, po, y, red);
+  for (int i = tid; i < N; i += NT) x[i] = y[i];
   bar_sync<NT>();
   bool good = true;
   if (prm.ir_enable) {
@@ -239,10 +353,10 @@ __global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const
     for (int it = 0; good && it < prm.ir_maxiter; ++it) {
       if (norme <= prm.ir_abstol + prm.ir_reltol * normb) break;
       double last = norme;
-      for (int i = tid; i < N; i += NT) y[i] = T(e[i]);
+      for (int i = tid; i < N; i += NT) y[i] = e[i];
       bar_sync<NT>();
-      ldl_trisolve<T, NT>(k, N, vo, po, y, red);
-      for (int i = tid; i < N; i += NT) dx[i] = double(y[i]) + x[i];
+      ldl_trisolve<T, NT>(k, inst, N, vo, po, y, red);
+      for (int i = tid; i < N; i += NT) dx[i] = y[i] + x[i];
       bar_sync<NT>();
       norme = refine_error<NT>(k, N, po, b, dx, e, red);
       if (!isfinite(norme)) {
@@ -286,7 +400,7 @@ __global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const
 template <typename T>
 static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, int *ok,
                           double *eps_out, cudaStream_t st) {
-  size_t sm = ((size_t)k.max_small_N * sizeof(T) + 15) & ~(size_t)15;
+  size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
   if (k.has_small)
     k_ldl_factor<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
   if (k.has_large)
@@ -296,7 +410,7 @@ template <typename T>
 static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
                          const double *rx, const double *rz, double *lx, double *lz, int *ok,
                          cudaStream_t st) {
-  size_t sm = ((size_t)k.max_small_N * sizeof(T) + 15) & ~(size_t)15;
+  size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
   if (k.has_small)
     k_ldl_solve<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, rx, rz, lx, lz, ok);
   if (k.has_large)

@@ -27,11 +27,15 @@ struct KKTDev {
   void *Lx, *D, *Dinv;  // double or float (mixed precision)
   // row pattern of L: for column j the list (k, pos of L(j,k))
   const int *Rp, *Rk, *Rpos;
-  // scratch (global, per instance, sum N each)
+  // elimination-tree levels: nodes of level l of instance i are
+  // lvl_nodes[voff[i] + lvl_ptr[lvl_off[i] + l] .. lvl_ptr[lvl_off[i] + l + 1])
+  const int *lvl_off, *nlev, *lvl_ptr, *lvl_nodes;
   int max_small_N;       // largest N among single-warp (shared memory) instances
   int has_small, has_large;
-  void *w;        // factor accumulator (factor type)
-  void *yf;       // solve work (factor type)
+  // scratch (global, per instance, sum N each)
+  double *w;       // dense factor accumulator (large instances)
+  double *yf;      // substitution work vector (large instances)
+  double *Lacc;    // FP64 column accumulator of the FP32-stored factor (or null)
   double *b, *x, *e, *dx;
 };
 

@@ -461,6 +461,21 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
       }
       out.Rp[k + 1] = (int)out.Rk.size();
     }
+    // elimination-tree levels (longest path from a leaf): every node of a
+    // level depends only on nodes of lower levels, so a level's columns can
+    // be factored and substituted concurrently
+    std::vector<int> lev(N, 0);
+    int nlev = 0;
+    for (int j = 0; j < N; ++j) {
+      if (parent[j] >= 0) lev[parent[j]] = std::max(lev[parent[j]], lev[j] + 1);
+      nlev = std::max(nlev, lev[j] + 1);
+    }
+    out.lvl_ptr.assign(nlev + 1, 0);
+    for (int j = 0; j < N; ++j) out.lvl_ptr[lev[j] + 1]++;
+    for (int l = 0; l < nlev; ++l) out.lvl_ptr[l + 1] += out.lvl_ptr[l];
+    out.lvl_nodes.assign(N, 0);
+    std::vector<int> cur(out.lvl_ptr.begin(), out.lvl_ptr.end() - 1);
+    for (int j = 0; j < N; ++j) out.lvl_nodes[cur[lev[j]]++] = j;
   }
   // ---- refresh positions
   for (size_t c = 0; c < out.ctype.size(); ++c) {
@@ -571,31 +586,92 @@ extern "C" int clgpu_debug_check_instance(const clgpu_problem *pb, const clgpu_s
       if (c != r) Kx[q] = 0.01 * std::sin(1.0 + r + 7.0 * c) * std::sin(1.0 + c + 7.0 * r);
     }
   for (int r = 0; r < N; ++r) Kx[p.Kdiag[r]] = p.Dsign[r] * 2.0;
-  // left-looking factorisation, same loops as the kernel
+  // level-scheduled left-looking factorisation, same loops as the kernel:
+  // wide levels merge every update into the column's own sorted row list
+  // (a row that is not found is a structure error), narrow levels use the
+  // dense accumulator
+  const int nlev = (int)p.lvl_ptr.size() - 1;
+  if (nlev < 1 || p.lvl_ptr[nlev] != N) return -24;
+  {
+    std::vector<int> seen(N, 0), lvl(N, -1);
+    for (int l = 0; l < nlev; ++l)
+      for (int t = p.lvl_ptr[l]; t < p.lvl_ptr[l + 1]; ++t) {
+        int j = p.lvl_nodes[t];
+        if (j < 0 || j >= N || seen[j]) return -25;
+        seen[j] = 1;
+        lvl[j] = l;
+      }
+    for (int j = 0; j < N; ++j)
+      for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r)
+        if (lvl[p.Rk[r]] >= lvl[j]) return -26;  // dependency must be on a lower level
+  }
   std::vector<double> w(N, 0.0), Lx(lnz, 0.0), D(N, 0.0);
-  for (int j = 0; j < N; ++j) {
-    for (int q = p.Kp[j]; q < p.Kp[j + 1]; ++q)
-      if (p.Kj[q] >= j) w[p.Kj[q]] = Kx[q];
-    for (int q = p.Rp[j]; q < p.Rp[j + 1]; ++q) {
-      int k = p.Rk[q], pos = p.Rpos[q];
-      double f = Lx[pos] * D[k];
-      for (int t = pos; t < p.Lp[k + 1]; ++t) w[p.Li[t]] -= Lx[t] * f;
+  const int narrow_below = 16;  // NT/2 for the single-warp kernel
+  for (int l = 0; l < nlev; ++l) {
+    const int a = p.lvl_ptr[l], bnd = p.lvl_ptr[l + 1];
+    for (int t = a; t < bnd; ++t) {
+      const int j = p.lvl_nodes[t];
+      const int q0 = p.Lp[j], q1 = p.Lp[j + 1];
+      if (bnd - a >= narrow_below) {
+        for (int q = q0; q < q1; ++q) Lx[q] = 0.0;
+        double dj = 0;
+        int q = q0;
+        for (int pp = p.Kp[j]; pp < p.Kp[j + 1]; ++pp) {
+          int c = p.Kj[pp];
+          if (c < j) continue;
+          if (c == j) {
+            dj = Kx[pp];
+            continue;
+          }
+          while (q < q1 && p.Li[q] != c) ++q;
+          if (q >= q1) return -27;
+          Lx[q] = Kx[pp];
+        }
+        for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) {
+          int k = p.Rk[r], pos = p.Rpos[r];
+          double f = Lx[pos] * D[k];
+          dj -= Lx[pos] * f;
+          q = q0;
+          for (int tt = pos + 1; tt < p.Lp[k + 1]; ++tt) {
+            while (q < q1 && p.Li[q] != p.Li[tt]) ++q;
+            if (q >= q1) return -28;
+            Lx[q] -= Lx[tt] * f;
+          }
+        }
+        D[j] = dj;
+        for (int qq = q0; qq < q1; ++qq) Lx[qq] /= dj;
+      } else {
+        for (int pp = p.Kp[j]; pp < p.Kp[j + 1]; ++pp)
+          if (p.Kj[pp] >= j) w[p.Kj[pp]] = Kx[pp];
+        for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) {
+          int k = p.Rk[r], pos = p.Rpos[r];
+          double f = Lx[pos] * D[k];
+          w[j] -= Lx[pos] * f;
+          for (int tt = pos + 1; tt < p.Lp[k + 1]; ++tt) w[p.Li[tt]] -= Lx[tt] * f;
+        }
+        D[j] = w[j];
+        for (int qq = q0; qq < q1; ++qq) {
+          Lx[qq] = w[p.Li[qq]] / D[j];
+          w[p.Li[qq]] = 0;
+        }
+        w[j] = 0;
+      }
     }
-    D[j] = w[j];
-    for (int t = p.Lp[j]; t < p.Lp[j + 1]; ++t) {
-      Lx[t] = w[p.Li[t]] / D[j];
-      w[p.Li[t]] = 0;
-    }
-    w[j] = 0;
   }
   std::vector<double> b(N), y(N);
   for (int i = 0; i < N; ++i) b[i] = std::cos(0.3 * i);
   y = b;
-  for (int j = 0; j < N; ++j)
-    for (int t = p.Lp[j]; t < p.Lp[j + 1]; ++t) y[p.Li[t]] -= Lx[t] * y[j];
+  for (int l = 0; l < nlev; ++l)
+    for (int t = p.lvl_ptr[l]; t < p.lvl_ptr[l + 1]; ++t) {
+      int i = p.lvl_nodes[t];
+      for (int r = p.Rp[i]; r < p.Rp[i + 1]; ++r) y[i] -= Lx[p.Rpos[r]] * y[p.Rk[r]];
+    }
   for (int j = 0; j < N; ++j) y[j] /= D[j];
-  for (int j = N - 1; j >= 0; --j)
-    for (int t = p.Lp[j]; t < p.Lp[j + 1]; ++t) y[j] -= Lx[t] * y[p.Li[t]];
+  for (int l = nlev - 1; l >= 0; --l)
+    for (int t = p.lvl_ptr[l]; t < p.lvl_ptr[l + 1]; ++t) {
+      int j = p.lvl_nodes[t];
+      for (int tt = p.Lp[j]; tt < p.Lp[j + 1]; ++tt) y[j] -= Lx[tt] * y[p.Li[tt]];
+    }
   double mx = 0;
   for (int r = 0; r < N; ++r) {
     double t = 0;

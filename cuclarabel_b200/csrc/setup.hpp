@@ -46,6 +46,7 @@ struct Prepared {
   std::vector<double> Kx;          // constant P/A entries (others 0)
   std::vector<signed char> Dsign;  // permuted
   std::vector<int> Lp, Li, Rp, Rk, Rpos;
+  std::vector<int> lvl_ptr, lvl_nodes;  // elimination-tree levels (leaves first)
   // refresh positions (local CSR positions)
   std::vector<int> nn_pos;                   // per NN row (type-major order)
   std::vector<int> socd_pos;                 // dense SOC triu pairs (concat over cones)

@@ -184,19 +184,24 @@ def mpc_qp(seed, n=None):
     r = _rng(seed)
     if n is None:
         n = int(r.integers(20, 401))
-    # P: diag U(0.1,1) + band-2 N(0,0.1) symmetrised, shifted to PSD
-    Pd = sp.diags(r.uniform(0.1, 1, n))
-    band = sp.diags([r.normal(0, 0.1, n - k) for k in (1, 2)], [1, 2], shape=(n, n))
-    P = (Pd + band + band.T).toarray()
-    lmin = np.linalg.eigvalsh(P).min()
-    if lmin < 1e-3:
-        P += (1e-3 - lmin) * np.eye(n)
-    P = sp.csc_matrix(P)
-    # banded equality rows (dynamics-like), bandwidth 4
+    # P: diag U(0.1,1) + band-2 N(0,0.1) symmetrised, shifted to PSD (a
+    # Gershgorin shift: every diagonal entry is raised until it dominates its
+    # row by 1e-3)
+    dg = r.uniform(0.1, 1, n)
+    b1, b2 = r.normal(0, 0.1, n - 1), r.normal(0, 0.1, n - 2)
+    rowsum = np.zeros(n)
+    rowsum[:-1] += np.abs(b1)
+    rowsum[1:] += np.abs(b1)
+    rowsum[:-2] += np.abs(b2)
+    rowsum[2:] += np.abs(b2)
+    dg = np.maximum(dg, rowsum + 1e-3)
+    P = sp.diags([dg, b1, b1, b2, b2], [0, 1, -1, 2, -2], shape=(n, n), format="csc")
+    # banded equality rows (dynamics-like), bandwidth 4; the windows start at
+    # distinct, evenly spaced columns so the rows are independent
     neq = n // 4
     erow, ecol, eval_ = [], [], []
     for i in range(neq):
-        j0 = int(r.integers(0, n - 4)) if n > 4 else 0
+        j0 = (i * (n - 4)) // max(1, neq - 1) if neq > 1 else 0
         for j in range(j0, min(n, j0 + 4)):
             erow.append(i); ecol.append(j); eval_.append(r.standard_normal())
     # SOC cones
@@ -211,9 +216,12 @@ def mpc_qp(seed, n=None):
     for j in range(nbox_vars):
         rows += [r0, r0 + 1]; cols += [j, j]; vals += [1.0, -1.0]
         r0 += 2
+    # each SOC acts on one stage: a window of consecutive variables, two
+    # N(0,1) coefficients per row
     for d in sdims:
+        w0 = int(r.integers(0, max(1, n - d - 1)))
         for k in range(d):
-            for j in r.choice(n, size=2, replace=False):
+            for j in (w0 + k, min(n - 1, w0 + k + 1)):
                 rows.append(r0 + k); cols.append(int(j)); vals.append(r.standard_normal())
         r0 += d
     m = r0

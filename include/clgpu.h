@@ -141,6 +141,13 @@ int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
                              double *ms_factor, double *ms_solve,
                              double *ms_cones, double *ms_residual,
                              int *passes);
+/* per-phase device time of the last profiled solve (CUDA events on the solve
+ * stream): ms[0] LDL factorisation, ms[1] LDL solves + refinement, ms[2] KKT
+ * refresh (Hs scatter), ms[3] residual kernels, ms[4] update_scaling; calls
+ * receives the number of timed launches of each phase.  No reference
+ * counterpart (the reference times host phases with TimerOutputs). */
+int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms,
+                                 long long *calls);
 int clgpu_solver_destroy(clgpu_solver *h);
 
 /* --------------------------------------------------------------- cones */

@@ -61,6 +61,8 @@ class OracleSettings(ctypes.Structure):
         ("iterative_refinement_max_iter", ctypes.c_int),
         ("iterative_refinement_stop_ratio", ctypes.c_double),
         ("verbose", ctypes.c_int),
+        ("gpu_equilibration", ctypes.c_int),
+        ("factor_fp32", ctypes.c_int),
     ]
 
 

@@ -69,6 +69,13 @@ typedef struct {
   int iterative_refinement_max_iter;
   double iterative_refinement_stop_ratio;
   int verbose;
+  /* 0: Ruiz cost scaling as the CPU path (mean of triu column norms of P,
+   *    src/problemdata.jl:250-251); 1: as the GPU path (mean of full-P row
+   *    norms, src/problemdata.jl:337-338) */
+  int gpu_equilibration;
+  /* 1: round L, D to FP32 after every factorisation (models a factor held
+   *    in single precision; refinement stays FP64) */
+  int factor_fp32;
 } oracle_settings;
 
 typedef struct {

@@ -128,6 +128,7 @@ struct LDL {
   std::vector<double> Lx, D, Dinv;
   std::vector<int> Dsigns;                // permuted signs
   bool reg_enable = true;
+  bool round_fp32 = false;
   double reg_eps = 1e-13, reg_delta = 2e-7;
   int reg_count = 0;
   // workspaces

@@ -193,6 +193,13 @@ bool LDL::refactor() {
     }
     Dinv[k] = 1.0 / D[k];
   }
+  if (round_fp32) {
+    for (auto &v : Lx) v = (double)(float)v;
+    for (int k = 0; k < n; ++k) {
+      D[k] = (double)(float)D[k];
+      Dinv[k] = (double)(float)(1.0 / D[k]);
+    }
+  }
   for (int k = 0; k < n; ++k)
     if (!std::isfinite(Dinv[k])) return false;
   return true;

@@ -232,6 +232,7 @@ struct KKTSolver {
     ldl.reg_enable = st->dynamic_regularization_enable != 0;
     ldl.reg_eps = st->dynamic_regularization_eps;
     ldl.reg_delta = st->dynamic_regularization_delta;
+    ldl.round_fp32 = st->factor_fp32 != 0;
     ldl.setup(N, K.p, K.i, Dsigns);
     for (int q = 0; q < K.p[N]; ++q) ldl.Ax[ldl.mapK[q]] = K.x[q];
   }
@@ -392,11 +393,14 @@ struct Solver {
       scale_data(&dwork, ework);
       for (int i = 0; i < n; ++i) eq.d[i] *= dwork[i];
       for (int i = 0; i < m; ++i) eq.e[i] *= ework[i];
-      // col_norms!(dwork, P): triu column norms
+      // col_norms!(dwork, P): triu column norms (CPU path), or the row norms
+      // of the full symmetric P (GPU path, row_norms_gpu!)
       std::fill(dwork.begin(), dwork.end(), 0.0);
       for (int j = 0; j < n; ++j)
-        for (int k = P.p[j]; k < P.p[j + 1]; ++k)
+        for (int k = P.p[j]; k < P.p[j + 1]; ++k) {
           dwork[j] = std::max(dwork[j], std::fabs(P.x[k]));
+          if (st.gpu_equilibration) dwork[P.i[k]] = std::max(dwork[P.i[k]], std::fabs(P.x[k]));
+        }
       double mean = 0;
       for (double v : dwork) mean += v;
       mean /= n;
@@ -886,6 +890,8 @@ void oracle_default_settings(oracle_settings *s) {
   s->iterative_refinement_max_iter = 10;
   s->iterative_refinement_stop_ratio = 5;
   s->verbose = 0;
+  s->gpu_equilibration = 0;
+  s->factor_fp32 = 0;
 }
 
 int oracle_solve(int n, int m, const int *Pp, const int *Pi, const double *Px,

@@ -105,7 +105,8 @@ def test_update_scaling_hs_and_products(cuda_device, name, strategy):
     # mul_Hs
     x = rng.standard_normal(C.numel)
     y = G.empty(C.numel)
-    assert G.L.clgpu_mul_Hs(G.h, y.data_ptr(), G.dev(x).data_ptr(), None) == 0
+    d_x = G.dev(x)
+    assert G.L.clgpu_mul_Hs(G.h, y.data_ptr(), d_x.data_ptr(), None) == 0
     assert close(y.cpu().numpy(), C.mul_Hs(x), 1e-11)
     # affine_ds
     out = G.empty(C.numel)
@@ -115,13 +116,15 @@ def test_update_scaling_hs_and_products(cuda_device, name, strategy):
     stz, sts = rng.standard_normal(C.numel) * 0.1, rng.standard_normal(C.numel) * 0.1
     sm = 0.37 * mu
     sh = G.empty(C.numel)
-    assert G.L.clgpu_combined_ds_shift(G.h, sh.data_ptr(), G.dev(stz).data_ptr(),
-                                       G.dev(sts).data_ptr(), dz_.data_ptr(), sm, None) == 0
+    d_stz, d_sts = G.dev(stz), G.dev(sts)
+    assert G.L.clgpu_combined_ds_shift(G.h, sh.data_ptr(), d_stz.data_ptr(),
+                                       d_sts.data_ptr(), dz_.data_ptr(), sm, None) == 0
     assert close(sh.cpu().numpy(), C.combined_ds_shift(stz, sts, z, sm), 1e-10)
     # ds_from_dz_offset
     dsv = rng.standard_normal(C.numel)
     o = G.empty(C.numel)
-    assert G.L.clgpu_ds_from_dz_offset(G.h, o.data_ptr(), G.dev(dsv).data_ptr(),
+    d_dsv = G.dev(dsv)
+    assert G.L.clgpu_ds_from_dz_offset(G.h, o.data_ptr(), d_dsv.data_ptr(),
                                        dz_.data_ptr(), None) == 0
     assert close(o.cpu().numpy(), C.ds_from_dz_offset(dsv, z), 1e-10)
 
@@ -132,21 +135,23 @@ def test_step_length_and_barrier(cuda_device, name):
     C = oracle.Cones(specs)
     G = GPUCones(specs)
     C.update_scaling(s, z, 1.0, 0)
-    G.L.clgpu_update_scaling(G.h, G.dev(s).data_ptr(), G.dev(z).data_ptr(), 1.0, 0, None)
+    d_s, d_z = G.dev(s), G.dev(z)
+    G.L.clgpu_update_scaling(G.h, d_s.data_ptr(), d_z.data_ptr(), 1.0, 0, None)
     for trial in range(4):
         dz = rng.standard_normal(C.numel) * (0.5 + trial)
         ds = rng.standard_normal(C.numel) * (0.5 + trial)
         ref = C.step_length(dz, ds, z, s, 1.0)
         a = ctypes.c_double()
-        assert G.L.clgpu_step_length(G.h, G.dev(dz).data_ptr(), G.dev(ds).data_ptr(),
-                                     G.dev(z).data_ptr(), G.dev(s).data_ptr(), 1.0, 0.99, 0.8,
+        d_dz, d_ds = G.dev(dz), G.dev(ds)
+        assert G.L.clgpu_step_length(G.h, d_dz.data_ptr(), d_ds.data_ptr(),
+                                     d_z.data_ptr(), d_s.data_ptr(), 1.0, 0.99, 0.8,
                                      1e-4, ctypes.byref(a), None) == 0
         assert abs(a.value - ref) <= 1e-10 * max(1.0, ref), (a.value, ref)
         alpha = 0.5 * ref
         bref = C.compute_barrier(z, s, dz, ds, alpha)
         bar = ctypes.c_double()
-        assert G.L.clgpu_compute_barrier(G.h, G.dev(z).data_ptr(), G.dev(s).data_ptr(),
-                                         G.dev(dz).data_ptr(), G.dev(ds).data_ptr(), alpha,
+        assert G.L.clgpu_compute_barrier(G.h, d_z.data_ptr(), d_s.data_ptr(),
+                                         d_dz.data_ptr(), d_ds.data_ptr(), alpha,
                                          ctypes.byref(bar), None) == 0
         assert abs(bar.value - bref) <= 1e-9 * max(1.0, abs(bref))
 
@@ -159,7 +164,8 @@ def test_margins_shift_and_init(cuda_device, name):
     v = rng.standard_normal(C.numel)
     for pd in (0, 1):
         a, b = ctypes.c_double(), ctypes.c_double()
-        assert G.L.clgpu_margins(G.h, G.dev(v).data_ptr(), pd, ctypes.byref(a), ctypes.byref(b),
+        d_v = G.dev(v)
+        assert G.L.clgpu_margins(G.h, d_v.data_ptr(), pd, ctypes.byref(a), ctypes.byref(b),
                                  None) == 0
         ra, rb = C.margins(v, pd)
         assert abs(a.value - ra) < 1e-11 and abs(b.value - rb) < 1e-10
@@ -179,5 +185,5 @@ def test_scaling_failure_reported(cuda_device):
     G = GPUCones(specs)
     s = np.array([0.1, 1.0, 0.0, 0.0])  # not interior
     z = np.array([2.0, 0.1, 0.1, 0.1])
-    assert G.L.clgpu_update_scaling(G.h, G.dev(s).data_ptr(), G.dev(z).data_ptr(), 1.0, 0,
-                                    None) == 1
+    d_s, d_z = G.dev(s), G.dev(z)
+    assert G.L.clgpu_update_scaling(G.h, d_s.data_ptr(), d_z.data_ptr(), 1.0, 0, None) == 1
