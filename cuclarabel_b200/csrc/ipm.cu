@@ -1228,11 +1228,13 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
     kk.D = A.alloc<float>(VT);
     kk.Dinv = A.alloc<float>(VT);
     kk.Lacc = A.alloc<double>((size_t)lnz);
+    kk.Dacc = A.alloc<double>(VT);
   } else {
     kk.Lx = A.alloc<double>((size_t)lnz);
     kk.D = A.alloc<double>(VT);
     kk.Dinv = A.alloc<double>(VT);
     kk.Lacc = nullptr;
+    kk.Dacc = nullptr;
   }
   kk.yf = A.alloc<double>(VT);
   kk.w = A.alloc<double>(VT);

@@ -35,6 +35,7 @@
 // kktsolver_directldl_gpu.jl:349-409.  In the mixed-precision form (the
 // reference's :cudssmixed) L and D are STORED in FP32; accumulation,
 // substitution arithmetic, the refinement residual and the iterate are FP64.
+#include <type_traits>
 #include "ldl.cuh"
 
 namespace clgpu {
@@ -89,16 +90,34 @@ __device__ __forceinline__ int inst_class(int N) {
   return (long long)N * (long long)sizeof(double) <= kSmemLimitBytes ? 1 : 2;
 }
 
-template <typename T>
-__device__ __forceinline__ double pivot(double dj, signed char sg, const LDLParams &prm,
-                                        T &djs) {
+// Dynamic regularisation of pivot dj (kktsolver_directldl.jl:224-229 via
+// QDLDL's Dsigns check): the FP64 pivot the elimination continues with.
+__device__ __forceinline__ double pivot_value(double dj, signed char sg, const LDLParams &prm) {
   if (prm.dyn_reg) {
-    double sgn = double(sg);
+    const double sgn = double(sg);
     if (sgn * dj <= prm.dyn_eps) dj = prm.dyn_delta * sgn;
   }
-  // rounded to the storage precision first so D and Dinv stay consistent
-  djs = T(dj);
-  return 1.0 / double(djs);
+  return dj;
+}
+// Stores pivot j: D and Dinv in the storage type T (Dinv is the inverse of
+// the stored pivot so the solves see a consistent pair) and the FP64 pivot
+// in Dacc, which aliases D in FP64 mode.  False if a stored value is not
+// finite.
+template <typename T>
+__device__ __forceinline__ bool store_pivot(T *D, T *Dinv, double *Dacc, int j, double dj) {
+  const T djs = T(dj);
+  const T dis = T(1.0 / double(djs));
+  D[j] = djs;
+  Dinv[j] = dis;
+  Dacc[j] = dj;
+  return isfinite(double(djs)) && isfinite(double(dis));
+}
+// Stores factor entry q: the storage copy, and the FP64 value the rest of the
+// elimination reads when the two differ.
+template <typename T>
+__device__ __forceinline__ void store_l(T *Lx, double *Lacc, int q, double v) {
+  Lx[q] = T(v);
+  if (!std::is_same<T, double>::value) Lacc[q] = v;
 }
 
 template <typename T, int NT, bool SMEM>
@@ -113,9 +132,11 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
   const int vo = k.voff[inst], po = k.poff[inst];
   double *w = SMEM ? reinterpret_cast<double *>(sm_raw) : k.w + vo;
   T *Lx = reinterpret_cast<T *>(k.Lx);
-  double *Lacc = k.Lacc ? k.Lacc : reinterpret_cast<double *>(k.Lx);  // FP64 accumulator
+  // FP64 factor values the elimination reads (aliases Lx / D in FP64 mode)
+  double *Lacc = k.Lacc ? k.Lacc : reinterpret_cast<double *>(k.Lx);
   T *D = reinterpret_cast<T *>(k.D) + vo;
   T *Dinv = reinterpret_cast<T *>(k.Dinv) + vo;
+  double *Dacc = (k.Dacc ? k.Dacc : reinterpret_cast<double *>(k.D)) + vo;
   const int *Kp = k.Kp + po, *Lp = k.Lp + po, *Rp = k.Rp + po;
   const int *Kdiag = k.Kdiag + vo;
   const int *nodes = k.lvl_nodes + vo;
@@ -155,23 +176,22 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
         }
         for (int r = Rp[j]; r < Rp[j + 1]; ++r) {
           const int kk = k.Rk[r], pos = k.Rpos[r];
-          const double ljk = double(Lx[pos]);
-          const double f = ljk * double(D[kk]);
+          const double ljk = Lacc[pos];
+          const double f = ljk * Dacc[kk];
           dj -= ljk * f;
           const int pe = Lp[kk + 1];
           q = q0;
           for (int p = pos + 1; p < pe; ++p) {
             const int i = k.Li[p];
             while (q < q1 && k.Li[q] != i) ++q;
-            if (q < q1) Lacc[q] -= double(Lx[p]) * f;
+            if (q < q1) Lacc[q] -= Lacc[p] * f;
           }
         }
-        T djs;
-        double dinv = pivot<T>(dj, sg[j], prm, djs);
-        if (!isfinite(dinv) || !isfinite(double(djs))) finite = false;
-        for (int qq = q0; qq < q1; ++qq) Lx[qq] = T(Lacc[qq] * dinv);
-        D[j] = djs;
-        Dinv[j] = T(dinv);
+        dj = pivot_value(dj, sg[j], prm);
+        const double dinv = 1.0 / dj;
+        if (!isfinite(dinv)) finite = false;
+        for (int qq = q0; qq < q1; ++qq) store_l(Lx, Lacc, qq, Lacc[qq] * dinv);
+        if (!store_pivot(D, Dinv, Dacc, j, dj)) finite = false;
       }
       bar_sync<NT>();
     } else {
@@ -198,8 +218,8 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
             const int kk = k.Rk[rb + lane];
             mypos = k.Rpos[rb + lane];
             myend = Lp[kk + 1];
-            myl = double(Lx[mypos]);
-            myf = myl * double(D[kk]);
+            myl = Lacc[mypos];
+            myf = myl * Dacc[kk];
           }
           const int cnt = min(32, r1 - rb);
           for (int t = 0; t < cnt; ++t) {
@@ -208,23 +228,21 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
             const double f = __shfl_sync(0xffffffffu, myf, t);
             const double ljk = __shfl_sync(0xffffffffu, myl, t);
             if (tid == 0) w[j] -= ljk * f;
-            for (int p = pos + 1 + tid; p < pe; p += NT) w[k.Li[p]] -= double(Lx[p]) * f;
+            for (int p = pos + 1 + tid; p < pe; p += NT) w[k.Li[p]] -= Lacc[p] * f;
             bar_sync<NT>();
           }
         }
-        const double dj = w[j];
-        T djs;
-        const double dinv = pivot<T>(dj, sg[j], prm, djs);
-        if (!isfinite(dinv) || !isfinite(double(djs))) finite = false;
+        const double dj = pivot_value(w[j], sg[j], prm);
+        const double dinv = 1.0 / dj;
+        if (!isfinite(dinv)) finite = false;
         for (int q = Lp[j] + tid; q < Lp[j + 1]; q += NT) {
           const int i = k.Li[q];
-          Lx[q] = T(w[i] * dinv);
+          store_l(Lx, Lacc, q, w[i] * dinv);
           w[i] = 0.0;
         }
         bar_sync<NT>();
         if (tid == 0) {
-          D[j] = djs;
-          Dinv[j] = T(dinv);
+          if (!store_pivot(D, Dinv, Dacc, j, dj)) finite = false;
           w[j] = 0.0;
         }
         bar_sync<NT>();

@@ -35,7 +35,10 @@ struct KKTDev {
   // scratch (global, per instance, sum N each)
   double *w;       // dense factor accumulator (large instances)
   double *yf;      // substitution work vector (large instances)
-  double *Lacc;    // FP64 column accumulator of the FP32-stored factor (or null)
+  // FP32-stored factor only (null otherwise): the FP64 factor values and
+  // pivots the factorisation itself runs on; the solves read the FP32 copy
+  double *Lacc;
+  double *Dacc;
   double *b, *x, *e, *dx;
 };
 
