@@ -82,7 +82,7 @@ EXPORTED = [
     "clgpu_get_Hs", "clgpu_mul_Hs", "clgpu_affine_ds", "clgpu_combined_ds_shift",
     "clgpu_ds_from_dz_offset", "clgpu_step_length", "clgpu_compute_barrier",
     "clgpu_margins", "clgpu_scaled_unit_shift", "clgpu_unit_initialization",
-    "clgpu_debug_check_instance",
+    "clgpu_debug_check_instance", "clgpu_margins_static",
 ]
 
 
@@ -119,6 +119,7 @@ def _declare(L):
                                     c_double, dp, c_void_p]
     L.clgpu_compute_barrier.argtypes = [c_void_p, V, V, V, V, c_double, dp, c_void_p]
     L.clgpu_margins.argtypes = [c_void_p, V, c_int, dp, dp, c_void_p]
+    L.clgpu_margins_static.argtypes = [c_int, ip, ip, V, c_int, dp, dp, c_void_p]
     L.clgpu_scaled_unit_shift.argtypes = [c_void_p, V, c_double, c_int, c_void_p]
     L.clgpu_unit_initialization.argtypes = [c_void_p, V, V, c_void_p]
     L.clgpu_debug_check_instance.argtypes = [ctypes.POINTER(ClgpuProblem),

@@ -197,6 +197,19 @@ int clgpu_compute_barrier(clgpu_cones *h, const double *z, const double *s,
 /* margins (:42): pd 0 primal, 1 dual */
 int clgpu_margins(clgpu_cones *h, const double *z, int pd, double *alpha,
                   double *beta, clgpu_stream_t st);
+/* Margins without a handle and without any device allocation: no
+ * counterpart in the reference.  Same result as clgpu_margins on a handle
+ * made from the same (types, dims) with clgpu_cones_create.  The cone layout
+ * and the per-cone temporaries live in a fixed static device array, so at
+ * most CLGPU_MARGINS_STATIC_MAX_CONES second-order plus PSD cones are
+ * accepted (CLGPU_ERR_STATIC_TOO_LARGE above that).  The first call on each
+ * device looks up that array's address and should come before any stream
+ * capture.  The array is shared per device: overlapping calls race. */
+#define CLGPU_MARGINS_STATIC_MAX_CONES 32768
+#define CLGPU_ERR_STATIC_TOO_LARGE (-20)
+int clgpu_margins_static(int ncones, const int *types, const int *dims,
+                         const double *z, int pd, double *alpha, double *beta,
+                         clgpu_stream_t st);
 /* scaled_unit_shift! (:81) */
 int clgpu_scaled_unit_shift(clgpu_cones *h, double *z, double alpha, int pd,
                             clgpu_stream_t st);
