@@ -224,19 +224,43 @@ class DefaultSolution:
     info: dict = field(default_factory=dict)
 
 
+def _as_csc(M, shape):
+    """CSC view of M without a copy when it already is CSC with canonical
+    (sorted, duplicate-free) indices."""
+    if M is None:
+        return sp.csc_matrix(shape)
+    if not (sp.issparse(M) and M.format == "csc"):
+        M = sp.csc_matrix(M)
+    if not M.has_canonical_format:
+        M = M.copy()
+        M.sum_duplicates()
+    return M
+
+
+def _i32(a):
+    return a if (a.dtype == np.int32 and a.flags.c_contiguous) else np.ascontiguousarray(a, np.int32)
+
+
+def _f64(a):
+    return a if (a.dtype == np.float64 and a.flags.c_contiguous) else np.ascontiguousarray(a, np.float64)
+
+
 def _prep_problem(P, q, A, b, cones):
-    q = np.ascontiguousarray(q, dtype=np.float64).ravel()
-    b = np.ascontiguousarray(b, dtype=np.float64).ravel()
+    """Host arrays of one problem for clgpu_problem.  P may be full or upper
+    triangular: the library reads its upper triangle (src/solver.jl:618-630
+    applies triu on the same path)."""
+    q = _f64(np.asarray(q, dtype=np.float64).ravel())
+    b = _f64(np.asarray(b, dtype=np.float64).ravel())
     n, m = len(q), len(b)
     if isinstance(cones, dict):
         cones = cones_from_dict(cones)
-    cones = list(cones)
-    P = sp.csc_matrix(P) if P is not None else sp.csc_matrix((n, n))
-    A = sp.csc_matrix(A) if A is not None else sp.csc_matrix((m, n))
+    specs = [c.spec() for c in cones]
+    P = _as_csc(P, (n, n))
+    A = _as_csc(A, (m, n))
     # _check_dimensions (src/solver.jl:199-211)
     if A.shape[0] != m:
         raise ValueError("A and b incompatible dimensions.")
-    if sum(c.nvars() for c in cones) != m:
+    if sum(_nvars(s) for s in specs) != m:
         raise ValueError("Constraint dimensions inconsistent with size of cones.")
     if A.shape[1] != n:
         raise ValueError("A and q incompatible dimensions.")
@@ -244,33 +268,72 @@ def _prep_problem(P, q, A, b, cones):
         raise ValueError("P and q incompatible dimensions.")
     if P.shape[0] != P.shape[1]:
         raise ValueError("P not square.")
-    P = sp.triu(P, format="csc")
-    P.sum_duplicates()
-    P.sort_indices()
-    A.sum_duplicates()
-    A.sort_indices()
-    specs = [c.spec() for c in cones]
-    keep = dict(
-        Pp=np.ascontiguousarray(P.indptr, np.int32), Pi=np.ascontiguousarray(P.indices, np.int32),
-        Px=np.ascontiguousarray(P.data, np.float64), q=q,
-        Ap=np.ascontiguousarray(A.indptr, np.int32), Ai=np.ascontiguousarray(A.indices, np.int32),
-        Ax=np.ascontiguousarray(A.data, np.float64), b=b,
-        ct=np.array([s[0] for s in specs] or [0], np.int32),
-        cd=np.array([s[1] for s in specs] or [0], np.int32),
-        cp=np.array([s[2] for s in specs] or [0.0], np.float64))
-    cp = _lib.ClgpuProblem()
-    cp.n, cp.m = n, m
-
-    def D(a):
-        return a.ctypes.data_as(_lib.dp)
-
-    def I(a):
-        return a.ctypes.data_as(_lib.ip)
-    cp.Pp, cp.Pi, cp.Px, cp.q = I(keep["Pp"]), I(keep["Pi"]), D(keep["Px"]), D(q)
-    cp.Ap, cp.Ai, cp.Ax, cp.b = I(keep["Ap"]), I(keep["Ai"]), D(keep["Ax"]), D(b)
-    cp.ncones = len(specs)
-    cp.cone_types, cp.cone_dims, cp.cone_params = I(keep["ct"]), I(keep["cd"]), D(keep["cp"])
+    keep = (_i32(P.indptr), _i32(P.indices), _f64(P.data), q,
+            _i32(A.indptr), _i32(A.indices), _f64(A.data), b,
+            np.array([s[0] for s in specs] or [0], np.int32),
+            np.array([s[1] for s in specs] or [0], np.int32),
+            np.array([s[2] for s in specs] or [0.0], np.float64))
+    cp = _lib.ClgpuProblem(
+        n, m, *(a.ctypes.data_as(_lib.dp if a.dtype == np.float64 else _lib.ip)
+                for a in keep[:8]),
+        len(specs), *(a.ctypes.data_as(_lib.dp if a.dtype == np.float64 else _lib.ip)
+                      for a in keep[8:]))
     return cp, keep, n, m
+
+
+_PROBLEM_DTYPE = np.dtype([
+    ("n", np.int32), ("m", np.int32),
+    ("Pp", np.uint64), ("Pi", np.uint64), ("Px", np.uint64), ("q", np.uint64),
+    ("Ap", np.uint64), ("Ai", np.uint64), ("Ax", np.uint64), ("b", np.uint64),
+    ("ncones", np.int32), ("pad", np.int32),
+    ("cone_types", np.uint64), ("cone_dims", np.uint64), ("cone_params", np.uint64)])
+
+
+def _pack_batch(problems):
+    """clgpu_problem array for a batch: each field's arrays are concatenated
+    once and every instance's pointers are computed from offsets, so the
+    per-instance host cost is the validation alone."""
+    parts = {k: [] for k in ("Pp", "Pi", "Px", "q", "Ap", "Ai", "Ax", "b", "ct", "cd", "cp")}
+    nm = np.zeros((len(problems), 3), np.int64)
+    for k, (P, q, A, b, cones) in enumerate(problems):
+        q = np.asarray(q, dtype=np.float64).ravel()
+        b = np.asarray(b, dtype=np.float64).ravel()
+        n, m = len(q), len(b)
+        if isinstance(cones, dict):
+            cones = cones_from_dict(cones)
+        specs = [c.spec() for c in cones]
+        P = _as_csc(P, (n, n))
+        A = _as_csc(A, (m, n))
+        if (A.shape != (m, n) or P.shape != (n, n)
+                or sum(_nvars(sp_) for sp_ in specs) != m):
+            _prep_problem(P, q, A, b, cones)  # raises the reference's message
+        parts["Pp"].append(P.indptr); parts["Pi"].append(P.indices); parts["Px"].append(P.data)
+        parts["q"].append(q)
+        parts["Ap"].append(A.indptr); parts["Ai"].append(A.indices); parts["Ax"].append(A.data)
+        parts["b"].append(b)
+        parts["ct"].append([t for t, _, _ in specs])
+        parts["cd"].append([d for _, d, _ in specs])
+        parts["cp"].append([a for _, _, a in specs])
+        nm[k] = (n, m, len(specs))
+    keep = {}
+    arr = np.zeros(len(problems), _PROBLEM_DTYPE)
+    arr["n"], arr["m"], arr["ncones"] = nm[:, 0], nm[:, 1], nm[:, 2]
+    for f, dt in (("Pp", np.int32), ("Pi", np.int32), ("Px", np.float64), ("q", np.float64),
+                  ("Ap", np.int32), ("Ai", np.int32), ("Ax", np.float64), ("b", np.float64),
+                  ("ct", np.int32), ("cd", np.int32), ("cp", np.float64)):
+        lens = np.fromiter((len(a) for a in parts[f]), np.int64, len(problems))
+        flat = np.concatenate([np.asarray(a, dt) for a in parts[f]] + [np.zeros(1, dt)])
+        keep[f] = flat
+        offs = np.concatenate([[0], np.cumsum(lens)[:-1]]) * flat.itemsize
+        field = {"ct": "cone_types", "cd": "cone_dims", "cp": "cone_params"}.get(f, f)
+        arr[field] = np.uint64(flat.ctypes.data) + offs.astype(np.uint64)
+    keep["arr"] = arr
+    return arr, keep, [(int(n), int(m)) for n, m, _ in nm]
+
+
+def _nvars(spec):
+    t, d, _ = spec
+    return 3 if t in (3, 4) else (d * (d + 1) // 2 if t == 5 else d)
 
 
 class BatchSolver:
@@ -279,28 +342,24 @@ class BatchSolver:
     def __init__(self, problems, settings=None, **kwargs):
         self.settings = settings_from(settings, **kwargs)
         L = _lib.load()
-        arr = (_lib.ClgpuProblem * len(problems))()
-        self._keep = []
-        self.dims = []
-        for k, pb in enumerate(problems):
-            cp, keep, n, m = _prep_problem(*pb)
-            arr[k] = cp
-            self._keep.append(keep)
-            self.dims.append((n, m))
+        arr, keep, self.dims = _pack_batch(problems)
         cs = self.settings.to_c()
         h = ctypes.c_void_p()
-        rc = L.clgpu_solver_create(arr, len(problems), ctypes.byref(cs), ctypes.byref(h))
+        rc = L.clgpu_solver_create(arr.ctypes.data_as(ctypes.POINTER(_lib.ClgpuProblem)),
+                                   len(problems), ctypes.byref(cs), ctypes.byref(h))
+        del keep
         if rc != 0:
             raise RuntimeError("clgpu_solver_create failed with code %d" % rc)
-        self._h = h
-        self._keep = None  # host arrays are copied by the library
+        self._h = h  # host arrays were copied by the library
+        self._destroy = L.clgpu_solver_destroy  # held for interpreter shutdown
         self.nx = sum(d[0] for d in self.dims)
         self.mz = sum(d[1] for d in self.dims)
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib.load().clgpu_solver_destroy(h)
+        destroy = getattr(self, "_destroy", None)
+        if h and destroy is not None:
+            destroy(h)
             self._h = None
 
     def solve(self, stream=0):

@@ -1223,13 +1223,128 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   kk.nlev = A.upload(nlev);
   kk.lvl_ptr = A.upload(lvl_ptr);
   kk.lvl_nodes = A.upload(lvl_nodes);
+  {
+    std::vector<int4> fsched(VT), bsched(VT);
+    for (int i = 0; i < B; ++i) {
+      const int nl = nlev[i];
+      const int *lp = lvl_ptr.data() + lvl_off[i];
+      const int *nodes = lvl_nodes.data() + voff[i];
+      for (int l = 0; l < nl; ++l)
+        for (int t = lp[l]; t < lp[l + 1]; ++t) {
+          const int j = nodes[t];
+          fsched[voff[i] + t] = make_int4(j, Rp[poff[i] + j], Rp[poff[i] + j + 1], 0);
+          const int bp = N[i] - lp[l + 1] + (t - lp[l]);
+          bsched[voff[i] + bp] = make_int4(j, Lp[poff[i] + j], Lp[poff[i] + j + 1], 0);
+        }
+    }
+    kk.fsched = A.upload(fsched);
+    kk.bsched = A.upload(bsched);
+    // level-ordered nonzero streams (single-warp substitution) and K rows
+    std::vector<int2> fent((size_t)lnz), bent((size_t)lnz);
+    std::vector<int> fpos((size_t)lnz), bpos((size_t)lnz), flev(lvl_ptr.size()),
+        blev(lvl_ptr.size());
+    std::vector<int2> kent((size_t)knz);
+    for (int i = 0; i < B; ++i) {
+      const auto &p = prep[i];
+      const int nl = nlev[i];
+      const int *lp = p.lvl_ptr.data();
+      const long long base = Lp[poff[i]];
+      long long f = base;
+      for (int l = 0; l < nl; ++l) {
+        flev[lvl_off[i] + l] = (int)f;
+        for (int t = lp[l]; t < lp[l + 1]; ++t) {
+          const int node = p.lvl_nodes[t];
+          for (int r = p.Rp[node]; r < p.Rp[node + 1]; ++r) {
+            fent[f] = make_int2(node, p.Rk[r]);
+            fpos[f] = (int)(base + p.Rpos[r]);
+            ++f;
+          }
+        }
+      }
+      flev[lvl_off[i] + nl] = (int)f;
+      long long g = base;
+      for (int l = nl - 1, t2 = 0; l >= 0; --l, ++t2) {
+        blev[lvl_off[i] + t2] = (int)g;
+        for (int t = lp[l]; t < lp[l + 1]; ++t) {
+          const int node = p.lvl_nodes[t];
+          for (int q = p.Lp[node]; q < p.Lp[node + 1]; ++q) {
+            bent[g] = make_int2(node, p.Li[q]);
+            bpos[g] = (int)(base + q);
+            ++g;
+          }
+        }
+      }
+      blev[lvl_off[i] + nl] = (int)g;
+      const long long kbase = Kp[poff[i]];
+      for (int r = 0; r < N[i]; ++r)
+        for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) kent[kbase + q] = make_int2(r, p.Kj[q]);
+    }
+    // encode segment positions and build the chunk tables (entries of one
+    // level at most 32 per chunk; the residual stream is a single level)
+    std::vector<int> fch, bch, kch, fch_off(B + 1, 0), bch_off(B + 1, 0), kch_off(B + 1, 0);
+    auto encode = [](int2 *e, long long n) {
+      long long q = 0;
+      while (q < n) {
+        long long r = q;
+        while (r + 1 < n && e[r + 1].x == e[q].x) ++r;
+        for (long long t = q; t <= r; ++t) {
+          const int pos = (int)std::min<long long>(t - q, 31);
+          e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << 21);
+        }
+        q = r + 1;
+      }
+    };
+    auto chunks = [](std::vector<int> &out, const int *lev, int nl, long long base) {
+      for (int l = 0; l < nl; ++l)
+        for (long long c = lev[l]; c < lev[l + 1]; c += 32) {
+          const long long cnt = std::min<long long>(32, lev[l + 1] - c);
+          out.push_back((int)((c - base) | ((cnt - 1) << 26)));
+        }
+    };
+    for (int i = 0; i < B; ++i) {
+      const long long base = Lp[poff[i]], n_l = Lp[poff[i] + N[i]] - base;
+      const long long kbase = Kp[poff[i]], n_k = Kp[poff[i] + N[i]] - kbase;
+      const bool small = (long long)N[i] * tsize <= 48 * 1024;
+      if (small) {
+        encode(fent.data() + base, n_l);
+        encode(bent.data() + base, n_l);
+        encode(kent.data() + kbase, n_k);
+        chunks(fch, flev.data() + lvl_off[i], nlev[i], base);
+        chunks(bch, blev.data() + lvl_off[i], nlev[i], base);
+        const int klev[2] = {(int)kbase, (int)(kbase + n_k)};
+        chunks(kch, klev, 1, kbase);
+      }
+      fch_off[i + 1] = (int)fch.size();
+      bch_off[i + 1] = (int)bch.size();
+      kch_off[i + 1] = (int)kch.size();
+    }
+    kk.fch = A.upload(fch);
+    kk.bch = A.upload(bch);
+    kk.kch = A.upload(kch);
+    kk.fch_off = A.upload(fch_off);
+    kk.bch_off = A.upload(bch_off);
+    kk.kch_off = A.upload(kch_off);
+    kk.fent = A.upload(fent);
+    kk.bent = A.upload(bent);
+    kk.fpos = A.upload(fpos);
+    kk.bpos = A.upload(bpos);
+    kk.flev = A.upload(flev);
+    kk.blev = A.upload(blev);
+    kk.kent = A.upload(kent);
+  }
   if (h->mixed) {
+    kk.LxF = A.alloc<float>((size_t)lnz);
+    kk.LxB = A.alloc<float>((size_t)lnz);
+    kk.LxR = A.alloc<float>((size_t)lnz);
     kk.Lx = A.alloc<float>((size_t)lnz);
     kk.D = A.alloc<float>(VT);
     kk.Dinv = A.alloc<float>(VT);
     kk.Lacc = A.alloc<double>((size_t)lnz);
     kk.Dacc = A.alloc<double>(VT);
   } else {
+    kk.LxF = A.alloc<double>((size_t)lnz);
+    kk.LxB = A.alloc<double>((size_t)lnz);
+    kk.LxR = A.alloc<double>((size_t)lnz);
     kk.Lx = A.alloc<double>((size_t)lnz);
     kk.D = A.alloc<double>(VT);
     kk.Dinv = A.alloc<double>(VT);

@@ -121,7 +121,7 @@ __device__ __forceinline__ void store_l(T *Lx, double *Lacc, int q, double v) {
 }
 
 template <typename T, int NT, bool SMEM>
-__global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, const int *run,
+__global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, LDLParams prm, const int *run,
                                                    int *ok, double *eps_out) {
   int inst = blockIdx.x;
   if (!run[inst]) return;
@@ -249,6 +249,20 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
       }
     }
   }
+  // copies of L in the order the substitutions read it (every level ended
+  // with a barrier, so all of Lx is written): level-ordered streams for the
+  // single-warp solve, row order for the block solve
+  if (SMEM) {
+    T *LxF = reinterpret_cast<T *>(k.LxF), *LxB = reinterpret_cast<T *>(k.LxB);
+    for (int r = Lp[0] + tid; r < Lp[N]; r += NT) {
+      LxF[r] = Lx[k.fpos[r]];
+      LxB[r] = Lx[k.bpos[r]];
+    }
+  } else {
+    T *LxR = reinterpret_cast<T *>(k.LxR);
+    const int rbeg = Rp[0], rend = Rp[N];
+    for (int r = rbeg + tid; r < rend; r += NT) LxR[r] = Lx[k.Rpos[r]];
+  }
   double bad = block_max<NT>(finite ? 0.0 : 1.0, red);
   if (tid == 0) {
     if (bad > 0) ok[inst] = 0;
@@ -256,63 +270,97 @@ __global__ void __launch_bounds__(NT) k_ldl_factor(KKTDev k, LDLParams prm, cons
   }
 }
 
-// y <- L^{-T} D^{-1} L^{-1} y, level-scheduled gathers
+// One node at a time over a run of consecutive narrow levels [a, e) of a
+// schedule: y[node] -= sum_r V[r] * y[I[r]] over the node's entries
+// [s.y, s.z), the block sharing each sum.  Nothing but y depends on the
+// previous node, so each thread loads its first entry of the NEXT node (and
+// that node's schedule record) before it reduces the current one; thread t
+// accumulates entries s.y + t, s.y + t + NT, ... in order, as a plain loop
+// would, so the result does not depend on the prefetch.
 template <typename T, int NT>
-__device__ void ldl_trisolve(const KKTDev &k, int inst, int N, int vo, int po, double *y,
-                             double *red) {
+__device__ __forceinline__ void narrow_run(const int4 *__restrict__ sched, int a, int e,
+                                           const T *__restrict__ V,
+                                           const int *__restrict__ I, double *y,
+                                           double *red, int tid) {
+  int4 s = sched[a];
+  double pv = 0.0;
+  int pk = -1;
+  if (s.y + tid < s.z) {
+    pv = double(V[s.y + tid]);
+    pk = I[s.y + tid];
+  }
+  for (int idx = a; idx < e; ++idx) {
+    int4 sn = make_int4(0, 0, 0, 0);
+    if (idx + 1 < e) sn = sched[idx + 1];
+    double nv = 0.0;
+    int nk = -1;
+    if (sn.y + tid < sn.z) {
+      nv = double(V[sn.y + tid]);
+      nk = I[sn.y + tid];
+    }
+    double t = 0.0;
+    if (pk >= 0) t += pv * y[pk];
+    for (int r = s.y + tid + NT; r < s.z; r += NT) t += double(V[r]) * y[I[r]];
+    t = block_sum<NT>(t, red);
+    if (tid == 0) y[s.x] -= t;
+    bar_sync<NT>();
+    s = sn;
+    pv = nv;
+    pk = nk;
+  }
+}
+
+// y <- L^{-T} D^{-1} L^{-1} y, level-scheduled gathers.  Wide levels: one
+// thread per node walks the node's row (forward) or column (backward).
+// Runs of narrow levels: narrow_run.
+template <typename T, int NT>
+__device__ void ldl_trisolve(const KKTDev &k, int inst, int N, int vo, double *y,
+                             double *red, int tid) {
   const T *Lx = reinterpret_cast<const T *>(k.Lx);
+  const T *LxR = reinterpret_cast<const T *>(k.LxR);
   const T *Dinv = reinterpret_cast<const T *>(k.Dinv) + vo;
-  const int *Lp = k.Lp + po, *Rp = k.Rp + po;
-  const int *nodes = k.lvl_nodes + vo;
+  const int4 *fs = k.fsched + vo, *bs = k.bsched + vo;
   const int *lptr = k.lvl_ptr + k.lvl_off[inst];
   const int nlev = k.nlev[inst];
-  const int tid = threadIdx.x;
   // forward: y_i -= sum_k L(i,k) y_k over the row pattern of i
-  for (int l = 0; l < nlev; ++l) {
+  for (int l = 0; l < nlev;) {
     const int a = lptr[l], b = lptr[l + 1];
     if (b - a >= NT / 2) {
       for (int idx = a + tid; idx < b; idx += NT) {
-        const int i = nodes[idx];
-        double t = y[i];
-        for (int r = Rp[i]; r < Rp[i + 1]; ++r) t -= double(Lx[k.Rpos[r]]) * y[k.Rk[r]];
-        y[i] = t;
+        const int4 sc = fs[idx];
+        double t = y[sc.x];
+        for (int r = sc.y; r < sc.z; ++r) t -= double(LxR[r]) * y[k.Rk[r]];
+        y[sc.x] = t;
       }
       bar_sync<NT>();
-    } else {
-      for (int idx = a; idx < b; ++idx) {
-        const int i = nodes[idx];
-        double t = 0.0;
-        for (int r = Rp[i] + tid; r < Rp[i + 1]; r += NT)
-          t += double(Lx[k.Rpos[r]]) * y[k.Rk[r]];
-        t = block_sum<NT>(t, red);
-        if (tid == 0) y[i] -= t;
-        bar_sync<NT>();
-      }
+      ++l;
+      continue;
     }
+    int l2 = l + 1;
+    while (l2 < nlev && lptr[l2 + 1] - lptr[l2] < NT / 2) ++l2;
+    narrow_run<T, NT>(fs, a, lptr[l2], LxR, k.Rk, y, red, tid);
+    l = l2;
   }
   for (int i = tid; i < N; i += NT) y[i] *= double(Dinv[i]);
   bar_sync<NT>();
-  // backward: y_j -= sum_i L(i,j) y_i over column j (ancestors)
-  for (int l = nlev - 1; l >= 0; --l) {
-    const int a = lptr[l], b = lptr[l + 1];
+  // backward: y_j -= sum_i L(i,j) y_i over column j (ancestors), root first
+  for (int l = nlev - 1; l >= 0;) {
+    const int a = N - lptr[l + 1], b = N - lptr[l];
     if (b - a >= NT / 2) {
       for (int idx = a + tid; idx < b; idx += NT) {
-        const int j = nodes[idx];
-        double t = y[j];
-        for (int p = Lp[j]; p < Lp[j + 1]; ++p) t -= double(Lx[p]) * y[k.Li[p]];
-        y[j] = t;
+        const int4 sc = bs[idx];
+        double t = y[sc.x];
+        for (int p = sc.y; p < sc.z; ++p) t -= double(Lx[p]) * y[k.Li[p]];
+        y[sc.x] = t;
       }
       bar_sync<NT>();
-    } else {
-      for (int idx = a; idx < b; ++idx) {
-        const int j = nodes[idx];
-        double t = 0.0;
-        for (int p = Lp[j] + tid; p < Lp[j + 1]; p += NT) t += double(Lx[p]) * y[k.Li[p]];
-        t = block_sum<NT>(t, red);
-        if (tid == 0) y[j] -= t;
-        bar_sync<NT>();
-      }
+      --l;
+      continue;
     }
+    int l2 = l - 1;
+    while (l2 >= 0 && lptr[l2 + 1] - lptr[l2] < NT / 2) --l2;
+    narrow_run<T, NT>(bs, a, N - lptr[l2 + 1], Lx, k.Li, y, red, tid);
+    l = l2;
   }
 }
 
@@ -337,7 +385,7 @@ __device__ double refine_error(const KKTDev &k, int N, int po, const double *b,
 }
 
 template <typename T, int NT, bool SMEM>
-__global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const int *run,
+__global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, LDLParams prm, const int *run,
                                                   const double *rx, const double *rz,
                                                   double *lx, double *lz, int *ok) {
   int inst = blockIdx.x;
@@ -361,7 +409,7 @@ __global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const
   }
   double normb = block_max<NT>(nb, red);
   bar_sync<NT>();
-  ldl_trisolve<T, NT>(k, inst, N, vo, po, y, red);
+  ldl_trisolve<T, NT>(k, inst, N, vo, y, red, tid);
   for (int i = tid; i < N; i += NT) x[i] = y[i];
   bar_sync<NT>();
   bool good = true;
@@ -373,7 +421,7 @@ __global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const
       double last = norme;
       for (int i = tid; i < N; i += NT) y[i] = e[i];
       bar_sync<NT>();
-      ldl_trisolve<T, NT>(k, inst, N, vo, po, y, red);
+      ldl_trisolve<T, NT>(k, inst, N, vo, y, red, tid);
       for (int i = tid; i < N; i += NT) dx[i] = y[i] + x[i];
       bar_sync<NT>();
       norme = refine_error<NT>(k, N, po, b, dx, e, red);
@@ -414,6 +462,254 @@ __global__ void __launch_bounds__(NT) k_ldl_solve(KKTDev k, LDLParams prm, const
   }
 }
 
+// ------------------------------------------------------------------------
+// Single-warp solve.  Each substitution pass, and the refinement residual,
+// streams its nonzeros in chunks of at most 32 entries of one level.  None
+// of a chunk's entries or values depends on earlier results, so they are
+// copied into a shared-memory ring kRing chunks ahead with cp.async: the
+// warp's global-memory latency overlaps the reduction of the chunks before.
+// Within a chunk the products are summed per segment (a node of the pass,
+// or a KKT row) by a segmented warp scan; a segment running into the next
+// chunk of the same level carries its partial sum across, so every segment
+// is written once.  Chunks never straddle a level, and a level's writes are
+// complete (__syncwarp) before the next level gathers them.  The summation
+// order depends only on the instance's own layout, never on the batch.
+
+constexpr int kRing = 8;  // chunks in flight per warp (power of two)
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(BYTES));
+}
+
+// Segmented inclusive scan of one chunk: lane l adds lane l-d's partial when
+// both lie in the same segment, i.e. d <= its position in the segment (pos,
+// clamped to 31) and d <= l.
+__device__ __forceinline__ double seg_scan_pos(double v, int pos, int lane) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double o = __shfl_up_sync(0xffffffffu, v, d);
+    if (d <= pos && d <= lane) v += o;
+  }
+  return v;
+}
+
+// One pass over an encoded stream (entries ent / values val from stream
+// position base), chunk by chunk as listed in chunks[0..nch):
+//   RESID = false:  y[seg] -= sum val * y[idx]     (out == y)
+//   RESID = true:   out[seg] = sum val * y[idx]
+// Chunk words are read 32 at a time, one per lane, two blocks ahead of use.
+template <typename T, bool RESID>
+__device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
+                          const int2 *__restrict__ ent, const T *__restrict__ val,
+                          const double *y, double *out, int2 *re, T *rv, int lane) {
+  const unsigned full = 0xffffffffu;
+  if (nch == 0) return;
+  int d0 = lane < nch ? chunks[lane] : 0;
+  int d1 = lane + 32 < nch ? chunks[lane + 32] : 0;
+  int d2 = lane + 64 < nch ? chunks[lane + 64] : 0;
+  int blk = 0;  // d0 holds chunks [32 blk, 32 blk + 32)
+  auto word = [&](int c) {
+    const int r = c - 32 * blk;  // 0 <= r < 64
+    return __shfl_sync(full, r < 32 ? d0 : d1, r & 31);
+  };
+  auto issue = [&](int c, int slot) {
+    if (c < nch) {
+      const int w = word(c);
+      const int p = base + (w & 0x3ffffff);
+      const int cnt = ((unsigned)w >> 26) + 1;
+      if (lane < cnt) {
+        cp_async<8>(&re[slot * 32 + lane], &ent[p + lane]);
+        cp_async<sizeof(T)>(&rv[slot * 32 + lane], &val[p + lane]);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+#pragma unroll
+  for (int c = 0; c < kRing; ++c) issue(c, c);
+  double carry = 0.0;
+  for (int c = 0; c < nch; ++c) {
+    if (c > 0 && (c & 31) == 0) {
+      ++blk;
+      d0 = d1;
+      d1 = d2;
+      const int q = 32 * (blk + 2) + lane;
+      d2 = q < nch ? chunks[q] : 0;
+    }
+    const int cnt = ((unsigned)word(c) >> 26) + 1;
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
+    __syncwarp();
+    const int slot = c & (kRing - 1);
+    const bool v = lane < cnt;
+    const int2 en = v ? re[slot * 32 + lane] : make_int2(0, 0);
+    const int pos = (en.x >> 16) & 31;
+    double x = v ? double(rv[slot * 32 + lane]) * y[en.y] : 0.0;
+    if (lane == 0 && pos > 0) x += carry;  // segment continued from the last chunk
+    x = seg_scan_pos(x, pos, lane);
+    if (v && ((en.x >> 21) & 1)) {
+      const int seg = en.x & 0xffff;
+      if (RESID)
+        out[seg] = x;
+      else
+        out[seg] -= x;
+    }
+    carry = __shfl_sync(full, x, cnt - 1);
+    __syncwarp();
+    issue(c + kRing, slot);
+  }
+  asm volatile("cp.async.wait_all;\n" ::);
+  __syncwarp();
+}
+
+// Vector loops of the single-warp solve: each lane handles elements
+// lane, lane + 32, ...; kVecU of them are loaded before any is used so the
+// loads of one lane are in flight together rather than one round trip each.
+constexpr int kVecU = 8;
+#define VEC_LOOP(i, N, BODY_LOAD, BODY_USE)                       \
+  for (int i##0 = lane; i##0 < (N); i##0 += 32 * kVecU) {         \
+    _Pragma("unroll") for (int u = 0; u < kVecU; ++u) {           \
+      const int i = i##0 + 32 * u;                                \
+      if (i < (N)) { BODY_LOAD }                                  \
+    }                                                             \
+    _Pragma("unroll") for (int u = 0; u < kVecU; ++u) {           \
+      const int i = i##0 + 32 * u;                                \
+      if (i < (N)) { BODY_USE }                                   \
+    }                                                             \
+  }
+
+template <typename T>
+__global__ void __launch_bounds__(32, 16)
+    k_ldl_solve_warp(KKTDev k, LDLParams prm, const int *run, const double *__restrict__ rx,
+                     const double *__restrict__ rz, double *lx, double *lz, int *ok,
+                     int ymax) {
+  const int inst = blockIdx.x;
+  if (!run[inst] || !ok[inst]) return;
+  const int N = k.N[inst];
+  if (inst_class(N) != 1) return;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double *y = reinterpret_cast<double *>(sm_raw);
+  int2 *re = reinterpret_cast<int2 *>(sm_raw + (((size_t)ymax * 8 + 15) & ~(size_t)15));
+  T *rv = reinterpret_cast<T *>(re + kRing * 32);
+  const int vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x;
+  double *__restrict__ b = k.b + vo;
+  double *__restrict__ x = k.x + vo;
+  double *__restrict__ e = k.e + vo;
+  const int *__restrict__ gs = k.gsrc + vo;
+  const int lbase = k.Lp[po], kbase = k.Kp[po];
+  const int *fch = k.fch + k.fch_off[inst], *bch = k.bch + k.bch_off[inst],
+            *kch = k.kch + k.kch_off[inst];
+  const int nfch = k.fch_off[inst + 1] - k.fch_off[inst];
+  const int nbch = k.bch_off[inst + 1] - k.bch_off[inst];
+  const int nkch = k.kch_off[inst + 1] - k.kch_off[inst];
+  const T *LxF = reinterpret_cast<const T *>(k.LxF), *LxB = reinterpret_cast<const T *>(k.LxB);
+  const T *__restrict__ Dinv = reinterpret_cast<const T *>(k.Dinv) + vo;
+  double nb = 0;
+  {
+    int g[kVecU];
+    double v[kVecU];
+    for (int i0 = lane; i0 < N; i0 += 32 * kVecU) {
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u) {
+        const int i = i0 + 32 * u;
+        g[u] = i < N ? gs[i] : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u)
+        v[u] = g[u] >= 0 ? rx[g[u]] : (g[u] == -1 ? 0.0 : rz[-g[u] - 2]);
+#pragma unroll
+      for (int u = 0; u < kVecU; ++u) {
+        const int i = i0 + 32 * u;
+        if (i < N) {
+          b[i] = v[u];
+          y[i] = v[u];
+          nb = fmax(nb, fabs(v[u]));
+        }
+      }
+    }
+  }
+  const double normb = warp_max(nb);
+  __syncwarp();
+  double tv[kVecU];
+  auto trisolve = [&]() {
+    ring_pass<T, false>(fch, nfch, lbase, k.fent, LxF, y, y, re, rv, lane);
+    VEC_LOOP(i, N, tv[u] = double(Dinv[i]);, y[i] *= tv[u];)
+    __syncwarp();
+    ring_pass<T, false>(bch, nbch, lbase, k.bent, LxB, y, y, re, rv, lane);
+  };
+  // e = b - K y, returns ||e||_inf (+inf when not finite)
+  auto residual = [&]() {
+    ring_pass<double, true>(kch, nkch, kbase, k.kent, k.Kx, y, e, re,
+                            reinterpret_cast<double *>(rv), lane);
+    __syncwarp();
+    double mx = 0.0;
+    bool bad = false;
+    double tb[kVecU];
+    VEC_LOOP(i, N, tb[u] = b[i]; tv[u] = e[i];, {
+      const double er = tb[u] - tv[u];
+      e[i] = er;
+      if (!isfinite(er)) bad = true;
+      mx = fmax(mx, fabs(er));
+    })
+    __syncwarp();
+    mx = warp_max(mx);
+    return __any_sync(0xffffffffu, bad) ? CUDART_INF : mx;
+  };
+  trisolve();
+  bool good = true;
+  if (prm.ir_enable) {
+    // x keeps the accepted iterate; y holds the candidate the residual reads
+    double norme = residual();
+    for (int i = lane; i < N; i += 32) x[i] = y[i];
+    __syncwarp();
+    if (!isfinite(norme)) good = false;
+    for (int it = 0; good && it < prm.ir_maxiter; ++it) {
+      if (norme <= prm.ir_abstol + prm.ir_reltol * normb) break;
+      const double last = norme;
+      VEC_LOOP(i, N, tv[u] = e[i];, y[i] = tv[u];)
+      __syncwarp();
+      trisolve();
+      VEC_LOOP(i, N, tv[u] = x[i];, y[i] += tv[u];)
+      __syncwarp();
+      norme = residual();
+      if (!isfinite(norme)) {
+        good = false;
+        break;
+      }
+      // kktsolver_directldl_gpu.jl:390-400: keep the candidate if it improved
+      // on the last error; stop when the improvement ratio is below stopratio
+      const double ratio = last / norme;
+      if (ratio > 1.0 || ratio >= prm.ir_stopratio)
+        for (int i = lane; i < N; i += 32) x[i] = y[i];
+      __syncwarp();
+      if (ratio < prm.ir_stopratio) break;
+    }
+  } else {
+    bool bad = false;
+    for (int i = lane; i < N; i += 32) {
+      x[i] = y[i];
+      if (!isfinite(y[i])) bad = true;
+    }
+    if (__any_sync(0xffffffffu, bad)) good = false;
+    __syncwarp();
+  }
+  if (!good) {
+    if (lane == 0) ok[inst] = 0;
+    return;
+  }
+  {
+    int g[kVecU];
+    VEC_LOOP(i, N, g[u] = gs[i]; tv[u] = x[i];, {
+      if (g[u] >= 0) {
+        if (lx) lx[g[u]] = tv[u];
+      } else if (g[u] <= -2) {
+        if (lz) lz[-g[u] - 2] = tv[u];
+      }
+    })
+  }
+}
+#undef VEC_LOOP
+
 // dynamic shared memory = the largest single-warp instance's work vector
 template <typename T>
 static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, int *ok,
@@ -429,8 +725,12 @@ static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
                          const double *rx, const double *rz, double *lx, double *lz, int *ok,
                          cudaStream_t st) {
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
-  if (k.has_small)
-    k_ldl_solve<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, rx, rz, lx, lz, ok);
+  if (k.has_small) {
+    // y, then the cp.async ring (entries + values, FP64 values for the residual)
+    const size_t smw = sm + (size_t)kRing * 32 * (sizeof(int2) + sizeof(double));
+    k_ldl_solve_warp<T><<<k.B, kSmallNT, smw, st>>>(k, p, run, rx, rz, lx, lz, ok,
+                                                     k.max_small_N);
+  }
   if (k.has_large)
     k_ldl_solve<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, rx, rz, lx, lz, ok);
 }
@@ -442,10 +742,11 @@ static void set_attrs() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
-  cudaFuncSetAttribute(k_ldl_solve<double, kSmallNT, true>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
-  cudaFuncSetAttribute(k_ldl_solve<float, kSmallNT, true>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
+  const int ring_bytes = kRing * 32 * (int)(sizeof(int2) + sizeof(double));
+  cudaFuncSetAttribute(k_ldl_solve_warp<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kSmemLimitBytes + 16 + ring_bytes);
+  cudaFuncSetAttribute(k_ldl_solve_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kSmemLimitBytes + 16 + ring_bytes);
   g_attr_done = true;
 }
 

@@ -30,6 +30,36 @@ struct KKTDev {
   // elimination-tree levels: nodes of level l of instance i are
   // lvl_nodes[voff[i] + lvl_ptr[lvl_off[i] + l] .. lvl_ptr[lvl_off[i] + l + 1])
   const int *lvl_off, *nlev, *lvl_ptr, *lvl_nodes;
+  // substitution schedules, one int4 per node:
+  //   fsched[voff[i] + t] = {node, Rp[node], Rp[node+1], 0} in level order
+  //     (leaves first);
+  //   bsched[voff[i] + t] = {node, Lp[node], Lp[node+1], 0} in backward order
+  //     (root level first: level l occupies [N - lvl_ptr[l+1], N - lvl_ptr[l]))
+  const int4 *fsched, *bsched;
+  // copy of L's values in row-pattern order (LxR[r] = Lx[Rpos[r]]), written at
+  // the end of every factorisation so the forward substitution reads L rows
+  // contiguously; same element type as Lx
+  void *LxR;
+  // Single-warp instances substitute by streaming nonzeros in level order.
+  // Forward stream: the row patterns of the nodes of level 0, 1, ... (node
+  // by node), entry {seg = row node i, idx = column k}; backward stream: the
+  // columns of the nodes from the root level down, entry {seg = column node
+  // j, idx = row i}.  Both occupy the instance's L positions [Lp[0], Lp[N]);
+  // flev / blev (nlev + 1 per instance, at lvl_off) give each level's start
+  // in processing order.  LxF / LxB hold L's values in stream order (copied
+  // from Lx[fpos] / Lx[bpos] after every factorisation).  kent is {row,
+  // column} of every KKT entry (CSR order) for the refinement residual.
+  const int2 *fent, *bent, *kent;
+  const int *fpos, *bpos, *flev, *blev;
+  void *LxF, *LxB;
+  // Entry encoding of the three streams (single-warp instances only):
+  //   .x = segment | min(position in segment, 31) << 16 | last-of-segment << 21
+  //   .y = gathered index
+  // Chunk tables: a pass is a list of chunks of <= 32 consecutive entries of
+  // one level; chunk word = start relative to the instance's stream base
+  // (bits 0..25) | (count - 1) << 26.  Instance i's chunks of the forward,
+  // backward and residual passes are fch[fch_off[i] .. fch_off[i+1]) etc.
+  const int *fch, *bch, *kch, *fch_off, *bch_off, *kch_off;
   int max_small_N;       // largest N among single-warp (shared memory) instances
   int has_small, has_large;
   // scratch (global, per instance, sum N each)

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <cstdint>
 #include <set>
 
 #include "setup.hpp"
@@ -86,6 +87,206 @@ std::vector<int> amd_order(int n, std::vector<std::vector<int>> &adj) {
       pq.insert({(int)a.size(), u});
     }
     std::vector<int>().swap(adj[v]);
+  }
+  for (int i = 0; i < n; ++i)
+    if (dense[i]) order.push_back(i);
+  return order;
+}
+
+// Nested dissection (George's level-structure bisection).  A connected
+// vertex set larger than kNdLeaf is split by a middle level of a breadth-first
+// level structure rooted at a pseudo-peripheral vertex; only the vertices of
+// that level with a neighbour in the next level form the separator.  The two
+// halves are ordered first (recursively), the separator last, so the halves
+// become independent subtrees of the elimination tree.  Small sets are
+// ordered by minimum degree.  The KKT graphs of stage-structured problems
+// are long and thin: minimum degree eliminates them from both ends inward
+// and leaves an elimination tree of height ~N/2, while dissection keeps the
+// height near (separator size) x log2(N), which is what bounds the
+// level-scheduled factorisation and substitutions.  Dense vertices (degree
+// above max(16, 10 sqrt(n))) are ordered last, as in amd_order.
+std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
+  constexpr int kNdLeaf = 8;
+  for (auto &a : adj) {
+    std::sort(a.begin(), a.end());
+    a.erase(std::unique(a.begin(), a.end()), a.end());
+  }
+  const double dense_thr = std::max(16.0, 10.0 * std::sqrt((double)n));
+  std::vector<char> dense(n, 0);
+  for (int i = 0; i < n; ++i) dense[i] = (double)adj[i].size() > dense_thr;
+  // CSR of the graph without dense vertices
+  std::vector<int> xadj(n + 1, 0), adjncy;
+  for (int i = 0; i < n; ++i) {
+    if (!dense[i])
+      for (int u : adj[i])
+        if (!dense[u]) adjncy.push_back(u);
+    xadj[i + 1] = (int)adjncy.size();
+  }
+  std::vector<int> order;
+  order.reserve(n);
+  std::vector<int> mark(n, -1), level(n, -1), queue(n);
+  int stamp = 0;
+  // task: a vertex set and whether it is emitted as is (a separator)
+  struct Task {
+    std::vector<int> v;
+    bool emit;
+  };
+  std::vector<Task> stack;
+  {
+    Task t;
+    t.emit = false;
+    for (int i = 0; i < n; ++i)
+      if (!dense[i]) t.v.push_back(i);
+    if (!t.v.empty()) stack.push_back(std::move(t));
+  }
+  auto deg_in = [&](int v, int sid) {
+    int d = 0;
+    for (int p = xadj[v]; p < xadj[v + 1]; ++p) d += mark[adjncy[p]] == sid;
+    return d;
+  };
+  // breadth-first levels of the set marked sid from src; returns the depth
+  // and fills queue[0..cnt) in visiting order
+  auto bfs = [&](int src, int sid, int &cnt) {
+    for (int i = 0; i < cnt; ++i) level[queue[i]] = -1;
+    int head = 0, tail = 0, depth = 0;
+    queue[tail++] = src;
+    level[src] = 0;
+    while (head < tail) {
+      int v = queue[head++];
+      depth = std::max(depth, level[v] + 1);
+      for (int p = xadj[v]; p < xadj[v + 1]; ++p) {
+        int u = adjncy[p];
+        if (mark[u] == sid && level[u] < 0) {
+          level[u] = level[v] + 1;
+          queue[tail++] = u;
+        }
+      }
+    }
+    cnt = tail;
+    return depth;
+  };
+  auto md_leaf = [&](const std::vector<int> &S) {
+    const int k = (int)S.size();
+    const int sid = ++stamp;
+    for (int a = 0; a < k; ++a) {
+      mark[S[a]] = sid;
+      level[S[a]] = a;  // local index
+    }
+    std::vector<std::vector<int>> la(k);
+    for (int a = 0; a < k; ++a)
+      for (int p = xadj[S[a]]; p < xadj[S[a] + 1]; ++p)
+        if (mark[adjncy[p]] == sid) la[a].push_back(level[adjncy[p]]);
+    for (int a = 0; a < k; ++a) level[S[a]] = -1;
+    std::vector<int> lp = amd_order(k, la);
+    for (int a : lp) order.push_back(S[a]);
+  };
+  while (!stack.empty()) {
+    Task t = std::move(stack.back());
+    stack.pop_back();
+    std::vector<int> &S = t.v;
+    if (t.emit) {
+      for (int v : S) order.push_back(v);
+      continue;
+    }
+    if ((int)S.size() <= kNdLeaf) {
+      md_leaf(S);
+      continue;
+    }
+    const int sid = ++stamp;
+    for (int v : S) {
+      mark[v] = sid;
+      level[v] = -1;
+    }
+    // connected components: dissect each on its own
+    int cnt = 0;
+    bfs(S[0], sid, cnt);
+    if (cnt < (int)S.size()) {
+      for (int i = 0; i < cnt; ++i) level[queue[i]] = -1;
+      std::vector<std::vector<int>> comps;
+      int comp_id = ++stamp;  // vertices already assigned get mark comp_id
+      for (int v : S) {
+        if (mark[v] == comp_id) continue;
+        int c = 0;
+        // restrict the BFS to unassigned vertices of S
+        bfs(v, sid, c);
+        comps.emplace_back(queue.begin(), queue.begin() + c);
+        for (int i = 0; i < c; ++i) {
+          mark[queue[i]] = comp_id;
+          level[queue[i]] = -1;
+        }
+      }
+      for (auto it = comps.rbegin(); it != comps.rend(); ++it) stack.push_back({std::move(*it), false});
+      continue;
+    }
+    // pseudo-peripheral root
+    int root = S[0], best = INT32_MAX;
+    for (int v : S) {
+      int d = deg_in(v, sid);
+      if (d < best) {
+        best = d;
+        root = v;
+      }
+    }
+    int depth = bfs(root, sid, cnt);
+    for (int it = 0; it < 5; ++it) {
+      int cand = -1, cd = INT32_MAX;
+      for (int i = 0; i < cnt; ++i) {
+        int v = queue[i];
+        if (level[v] == depth - 1) {
+          int d = deg_in(v, sid);
+          if (d < cd) {
+            cd = d;
+            cand = v;
+          }
+        }
+      }
+      int c2 = cnt;  // the set is connected: every call visits all of it
+      int d2 = bfs(cand, sid, c2);
+      if (d2 > depth) {
+        depth = d2;
+        root = cand;
+        cnt = c2;
+      } else {
+        bfs(root, sid, cnt);  // restore the levels of the deeper structure
+        break;
+      }
+    }
+    if (depth < 3) {
+      md_leaf(S);
+      continue;
+    }
+    std::vector<int> lcount(depth, 0);
+    for (int v : S) lcount[level[v]]++;
+    int ell = 1, cum = 0;
+    for (int l = 0; l < depth; ++l) {
+      cum += lcount[l];
+      if (2 * cum >= (int)S.size()) {
+        ell = std::max(1, std::min(depth - 2, l));
+        break;
+      }
+    }
+    Task A, B, sep;
+    A.emit = B.emit = false;
+    sep.emit = true;
+    for (int v : S) {
+      const int lv = level[v];
+      if (lv < ell) {
+        A.v.push_back(v);
+      } else if (lv > ell) {
+        B.v.push_back(v);
+      } else {
+        bool touches_next = false;
+        for (int p = xadj[v]; p < xadj[v + 1] && !touches_next; ++p) {
+          int u = adjncy[p];
+          touches_next = mark[u] == sid && level[u] == ell + 1;
+        }
+        (touches_next ? sep.v : A.v).push_back(v);
+      }
+    }
+    for (int v : S) level[v] = -1;
+    stack.push_back(std::move(sep));
+    if (!B.v.empty()) stack.push_back(std::move(B));
+    if (!A.v.empty()) stack.push_back(std::move(A));
   }
   for (int i = 0; i < n; ++i)
     if (dense[i]) order.push_back(i);
@@ -370,7 +571,7 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
         adj[en.r].push_back(en.c);
         adj[en.c].push_back(en.r);
       }
-    out.perm = amd_order(N, adj);
+    out.perm = nd_order(N, adj);
   }
   out.iperm.assign(N, 0);
   for (int k = 0; k < N; ++k) out.iperm[out.perm[k]] = k;

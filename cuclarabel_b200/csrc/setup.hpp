@@ -71,5 +71,8 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt,
 // fill-reducing ordering of a symmetric pattern given as an adjacency list
 // (no self loops); returns perm (perm[k] = original index eliminated k-th)
 std::vector<int> amd_order(int n, std::vector<std::vector<int>> &adj);
+// nested-dissection ordering (minimum degree on the small parts); same
+// contract as amd_order
+std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj);
 
 }  // namespace clgpu
