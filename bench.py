@@ -118,83 +118,128 @@ def problem_bytes(pbs):
     return b
 
 
+def _ref_worker(w, nworkers, count, conn):
+    """One CPU worker: owns instances w, w + nworkers, ... of the workload,
+    generates them once, then solves its slice with the oracle each time the
+    parent says go; reports (solved, seconds)."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    import oracle
+    from cuclarabel_b200 import problems
+    mine = [problems.mpc_qp(i) for i in range(w, count, nworkers)]
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg != "go":
+            break
+        t0 = time.perf_counter()
+        solved = sum(1 for pb in mine
+                     if oracle.solve(*pb, gpu_equilibration=1)["status_name"] == "SOLVED")
+        conn.send((solved, time.perf_counter() - t0))
+
+
+class RefPool:
+    """The CPU reference path (the oracle's restatement of the reference's
+    CPU solver) over all host cores, one process per core, each owning a
+    fixed slice of the workload so that problem generation stays outside the
+    timed region."""
+
+    def __init__(self, count):
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.cores = os.cpu_count() or 1
+        self.count = count
+        self.conns, self.procs = [], []
+        for w in range(self.cores):
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_ref_worker, args=(w, self.cores, count, b), daemon=True)
+            p.start()
+            self.conns.append(a)
+            self.procs.append(p)
+        for c in self.conns:
+            assert c.recv() == "ready"
+
+    def step(self):
+        t0 = time.perf_counter()
+        for c in self.conns:
+            c.send("go")
+        solved = 0
+        for c in self.conns:
+            s, _ = c.recv()
+            solved += s
+        return solved, time.perf_counter() - t0
+
+    def close(self):
+        for c in self.conns:
+            c.send("stop")
+        for p in self.procs:
+            p.join(timeout=10)
+
+
 def run_reference(args, rank, world):
-    """CPU reference path (the oracle restatement of the reference's CPU
-    Clarabel path) on the host cores, bounded sample per step."""
+    """`--impl reference`: the reference's CPU algorithm (the oracle port) on
+    the host cores for the same workload, metric and unit as the GPU arm.
+    Under torchrun only rank 0 runs; the other ranks exit without work."""
     if rank != 0:
         return
-    from concurrent.futures import ProcessPoolExecutor
-    import multiprocessing as mp
-    cores = os.cpu_count() or 1
-    sample = args.ref_sample
-    pbs = gen_problems(sample, 0)
-    ctx = mp.get_context("spawn")
-    os.environ["OMP_NUM_THREADS"] = "1"
-    with ProcessPoolExecutor(max_workers=cores, mp_context=ctx,
-                             initializer=_ref_init) as ex:
-        list(ex.map(_ref_solve, range(min(cores, sample))))  # warm the workers
-        times, solved = [], 0
-        for step in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            res = list(ex.map(_ref_solve, range(sample), chunksize=4))
-            dt = time.perf_counter() - t0
-            if step >= args.warmup:
-                times.append(dt)
-                solved += sum(1 for r in res if r == "SOLVED")
+    B = args.instances
+    pool = RefPool(B)
+    times, solved = [], 0
+    for step in range(args.warmup + args.steps):
+        s, dt = pool.step()
+        if step >= args.warmup:
+            times.append(dt)
+            solved += s
+    pool.close()
     total = sum(times)
     val = solved / total
     line = {
-        "metric": "solves/s at 1e-8 (batched MPC QP/SOCP)",
-        "value": val, "unit": "solves/s", "impl": "reference", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC, "value": val, "unit": "solves/s", "impl": "reference",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "MPC QP/SOCP batch (sample of %d of 4096)" % sample,
-                   "instances_per_step": sample},
-        "cpu_baseline": {"value": val, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": "%d MPC QP/SOCP instances per step, one process per core" % sample},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64, MPC batch shapes)",
+        "config": workload_config(B, "reference CPU path (oracle port)"),
+        "cpu_baseline": {"value": val, "unit": "solves/s", "cores": pool.cores, "kind": "port",
+                         "sample": "the full %d-instance workload per step, one process per "
+                                   "core, each owning a fixed slice" % B},
         "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-_REF_PBS = None
+def cpu_baseline_sample(count):
+    """One step of the CPU reference path over `count` instances (the GPU
+    arm's cpu_baseline field; ~5 ms of CPU per instance)."""
+    pool = RefPool(count)
+    solved, dt = pool.step()
+    pool.close()
+    return {"value": solved / dt, "unit": "solves/s", "cores": pool.cores, "kind": "port",
+            "sample": "%d MPC QP/SOCP instances (the workload's first %d), one process per "
+                      "core, %.1f s wall" % (count, count, dt)}
 
 
-def _ref_init():
-    global _REF_PBS
-    os.environ["OMP_NUM_THREADS"] = "1"
-    sys.path.insert(0, ROOT)
+METRIC = "solves/s at 1e-8 (batched MPC QP/SOCP)"
 
 
-def _ref_solve(i):
-    global _REF_PBS
-    import oracle
-    from cuclarabel_b200 import problems
-    if _REF_PBS is None:
-        _REF_PBS = {}
-    pb = _REF_PBS.get(i)
-    if pb is None:
-        pb = problems.mpc_qp(i)
-        _REF_PBS[i] = pb
-    return oracle.solve(*pb, gpu_equilibration=1)["status_name"]
+def workload_config(B, method):
+    return {"workload": "%d MPC-style QP/SOCPs per GPU, n~U{20..400}, m~2n, 5-20 SOC(3..8)"
+                        % B, "instances_per_gpu": B, "method": method}
 
 
-def cpu_baseline_sample(sample):
-    """Bounded CPU sample for the GPU arm's cpu_baseline field."""
-    from concurrent.futures import ProcessPoolExecutor
-    import multiprocessing as mp
-    cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ProcessPoolExecutor(max_workers=cores, mp_context=ctx, initializer=_ref_init) as ex:
-        list(ex.map(_ref_solve, range(min(cores, sample))))
-        t0 = time.perf_counter()
-        res = list(ex.map(_ref_solve, range(sample), chunksize=4))
-        dt = time.perf_counter() - t0
-    solved = sum(1 for r in res if r == "SOLVED")
-    return {"value": solved / dt, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": "%d MPC QP/SOCP instances, one process per core, %.1f s wall" % (sample, dt)}
+def ncu_traffic():
+    """DRAM bytes per launch of the single-warp LDL solve from the committed
+    ncu summary (profiles/ldl_solve_mpc4096.md), or None."""
+    p = os.path.join(ROOT, "profiles", "ldl_solve_mpc4096.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
 
 
 def main():
@@ -206,7 +251,7 @@ def main():
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--method", default="cudss")
     ap.add_argument("--plain-sample", type=int, default=48)
-    ap.add_argument("--ref-sample", type=int, default=512)
+    ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
 
@@ -323,44 +368,59 @@ def main():
                  "p50_ms": 1000 * float(np.percentile(lat, 50)),
                  "p99_ms": 1000 * float(np.percentile(lat, 99)), "method": "cudss"}
 
-    # ---- roofline of the dominant device phase and of update_scaling
+    # ---- roofline: the dominant device phase (an LDL kernel), plus the
+    # update_scaling cone kernels for reference
     peaks, peak_kind = load_peaks()
     hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    peak_note = ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                 else "fallback 6.65 TB/s")
     phases = prof["phases"]
     dom = max(phases.items(), key=lambda kv: kv[1][0])
+    kernels = {"ldl_solve": "k_ldl_solve_warp (single-warp LDL solve + refinement)",
+               "ldl_factor": "k_ldl_factor (single-warp LDL factorisation)"}
+
+    def roofline(name):
+        ms, calls = phases[name]
+        by = prof["bytes"].get(name, 0.0)
+        ach = by / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+        return {"bound": "hbm", "kernel": kernels.get(name, name), "achieved": ach,
+                "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": ncu_traffic() if name == "ldl_solve" else None,
+                "peak_kind": peak_note,
+                "algorithmic_bytes_per_launch": by / max(calls, 1),
+                "avg_launch_ms": ms / max(calls, 1), "launches": calls}
     us_ms, us_calls = phases["update_scaling"]
     us_bytes = algorithmic_bytes_update_scaling(pbs)
-    us_achieved = us_bytes / (us_ms / max(us_calls, 1) / 1000.0) / 1e9 if us_ms > 0 else 0.0
+    us_ach = us_bytes / (us_ms / max(us_calls, 1) / 1000.0) / 1e9 if us_ms > 0 else 0.0
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(args.ref_sample)
 
     if rank == 0:
-        roof = {"bound": "hbm", "kernel": "update_scaling (nonneg + SOC, whole batch)",
-                "achieved": us_achieved, "peak": hbm, "unit": "GB/s",
-                "frac": us_achieved / hbm, "traffic": None,
-                "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
-                "measured" else "fallback 6.65 TB/s",
-                "algorithmic_bytes_per_launch": us_bytes,
-                "avg_launch_ms": us_ms / max(us_calls, 1)}
+        roof = roofline(dom[0] if dom[0] in kernels else "ldl_solve")
         line = {
-            "metric": "solves/s at 1e-8 (batched MPC QP/SOCP)",
-            "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (LDL factor stored f32)" if args.method == "cudssmixed" else "f64",
             "data": "synthetic (seeded PCG64, MPC batch shapes)",
-            "config": {"workload": "%d MPC-style QP/SOCPs per GPU, n~U{20..400}, "
-                                   "m~2n, 5-20 SOC(3..8)" % B,
-                       "instances_per_gpu": B, "method": args.method,
-                       "l2": "flushed (256 MB write) between timed steps",
-                       "device_bytes": dev_bytes},
+            "config": dict(workload_config(B, args.method),
+                           l2="flushed (256 MB write) between timed steps",
+                           device_bytes=dev_bytes),
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "note": "includes host setup (Ruiz, ordering, symbolic LDL)"},
             "gpu_launches": launches_per_solve * args.steps,
             "roofline": roof,
+            "roofline_other": {
+                "ldl_factor" if roof["kernel"] == kernels["ldl_solve"] else "ldl_solve":
+                    roofline("ldl_factor" if roof["kernel"] == kernels["ldl_solve"]
+                             else "ldl_solve"),
+                "update_scaling": {"achieved": us_ach, "frac": us_ach / hbm, "unit": "GB/s",
+                                   "algorithmic_bytes_per_launch": us_bytes,
+                                   "avg_launch_ms": us_ms / max(us_calls, 1)}},
             "phases_ms": {k: round(v[0], 3) for k, v in phases.items()},
             "dominant_phase": {"name": dom[0], "ms": dom[1][0], "calls": dom[1][1]},
             "batch": {"status": status_counts, "iters_mean": float(np.mean(iters)),

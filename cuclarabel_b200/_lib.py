@@ -76,6 +76,7 @@ EXPORTED = [
     "clgpu_solver_get_info", "clgpu_solver_get_solution", "clgpu_solver_get_solutions",
     "clgpu_solver_update_qb", "clgpu_solver_device_bytes", "clgpu_solver_launch_count",
     "clgpu_solver_set_profiling", "clgpu_solver_get_profile", "clgpu_solver_get_phase_times",
+    "clgpu_solver_get_phase_bytes",
     "clgpu_solver_destroy",
     "clgpu_cones_create", "clgpu_cones_destroy", "clgpu_cones_numel", "clgpu_cones_degree",
     "clgpu_cones_hs_len", "clgpu_update_scaling", "clgpu_set_identity_scaling",
@@ -102,6 +103,7 @@ def _declare(L):
     L.clgpu_solver_set_profiling.argtypes = [c_void_p, c_int]
     L.clgpu_solver_get_profile.argtypes = [c_void_p, dp, dp, dp, dp, dp, ip]
     L.clgpu_solver_get_phase_times.argtypes = [c_void_p, dp, ctypes.POINTER(c_ll)]
+    L.clgpu_solver_get_phase_bytes.argtypes = [c_void_p, dp]
     L.clgpu_solver_destroy.argtypes = [c_void_p]
     L.clgpu_cones_create.argtypes = [c_int, ip, ip, dp, c_int, ctypes.POINTER(c_void_p)]
     L.clgpu_cones_destroy.argtypes = [c_void_p]

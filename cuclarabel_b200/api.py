@@ -416,8 +416,11 @@ class BatchSolver:
         calls = (ctypes.c_longlong * 5)()
         L.clgpu_solver_get_phase_times(self._h, ms, calls)
         names = ["ldl_factor", "ldl_solve", "kkt_refresh", "residual", "update_scaling"]
+        by = (ctypes.c_double * 2)()
+        L.clgpu_solver_get_phase_bytes(self._h, by)
         return dict(ms_total=vals[0].value, passes=passes.value,
-                    phases={n: (ms[i], calls[i]) for i, n in enumerate(names)})
+                    phases={n: (ms[i], calls[i]) for i, n in enumerate(names)},
+                    bytes={"ldl_factor": by[0], "ldl_solve": by[1]})
 
 
 class Solver(BatchSolver):

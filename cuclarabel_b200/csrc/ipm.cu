@@ -743,6 +743,8 @@ struct clgpu_solver {
   int prof_open = -1, prof_open_ev = -1;
   int passes = 0;
   double last_ms = 0;
+  double *d_prof_bytes = nullptr;  // [2B] algorithmic bytes (profiling)
+  double prof_bytes[2] = {0, 0};   // factor, solve: sums of the last profiled solve
   ~clgpu_solver() {
     if (h_counter) cudaFreeHost(h_counter);
     for (auto e : ev_pool) cudaEventDestroy(e);
@@ -770,6 +772,15 @@ struct clgpu_solver {
     prof_open = -1;
   }
   void prof_collect() {
+    if (d_prof_bytes) {
+      std::vector<double> hb(2 * (size_t)B);
+      cudaMemcpy(hb.data(), d_prof_bytes, hb.size() * sizeof(double), cudaMemcpyDeviceToHost);
+      prof_bytes[0] = prof_bytes[1] = 0;
+      for (int i = 0; i < B; ++i) {
+        prof_bytes[0] += hb[i];
+        prof_bytes[1] += hb[(size_t)B + i];
+      }
+    }
     for (int c = 0; c < 5; ++c) {
       prof[c] = 0;
       prof_calls[c] = 0;
@@ -852,10 +863,46 @@ extern "C" int clgpu_default_settings(clgpu_settings *s) {
 }
 
 // Builds every device structure of a batch from prepared instances.
-static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
+// Runs f(i) for i in [0, n) on nth host threads (blocks of 16 indices).
+template <class F>
+static void par_for(int n, int nth, F f) {
+  if (nth <= 1 || n < 64) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  for (int t = 0; t < nth; ++t)
+    th.emplace_back([&]() {
+      for (int i0; (i0 = next.fetch_add(16)) < n;)
+        for (int i = i0; i < std::min(n, i0 + 16); ++i) f(i);
+    });
+  for (auto &t : th) t.join();
+}
+
+// Exclusive prefix sum of counts[0..n) into off[0..n] (off[n] = total).
+template <class T>
+static std::vector<long long> prefix(const std::vector<T> &counts) {
+  std::vector<long long> off(counts.size() + 1, 0);
+  for (size_t i = 0; i < counts.size(); ++i) off[i + 1] = off[i] + (long long)counts[i];
+  return off;
+}
+
+// Concatenates the prepared instances into the batch layout and uploads it.
+// Every per-instance copy runs on nth host threads: offsets first (prefix
+// sums over instances), then each instance fills its own disjoint slices.
+static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   DevArena &A = h->arena;
   const int B = (int)prep.size();
   h->B = B;
+  auto tmark = std::chrono::steady_clock::now();
+  auto mark = [&](const char *what) {  // setup timing, printed when verbose
+    if (!h->st.verbose) return;
+    auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "clgpu setup: %-22s %8.1f ms\n", what,
+                 std::chrono::duration<double, std::milli>(now - tmark).count());
+    tmark = now;
+  };
   // ---------------- sizes and offsets
   std::vector<int> xoff(B + 1, 0), moff(B + 1, 0);
   for (int i = 0; i < B; ++i) {
@@ -867,86 +914,93 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   h->mz = mz;
   h->h_xoff = xoff;
   h->h_moff = moff;
-  // type-major global row of (instance, local type-major row)
+  // type-major global rows: instance i's rows of type t start at tcur[6i+t]
   std::vector<long long> type_total(6, 0);
   for (auto &p : prep)
     for (int t = 0; t < 6; ++t) type_total[t] += p.type_rows[t];
   std::vector<int> type_begin(7, 0);
   for (int t = 0; t < 6; ++t) type_begin[t + 1] = type_begin[t] + (int)type_total[t];
-  std::vector<std::vector<int>> grow(B);  // local type-major row -> global row
+  std::vector<int> tcur(6 * (size_t)B);
   {
     std::vector<int> cursor(type_begin.begin(), type_begin.end() - 1);
-    for (int i = 0; i < B; ++i) {
-      auto &p = prep[i];
-      grow[i].resize(p.m);
-      int lr = 0;
-      for (int t = 0; t < 6; ++t)
-        for (int k = 0; k < p.type_rows[t]; ++k) grow[i][lr++] = cursor[t]++;
-    }
+    for (int i = 0; i < B; ++i)
+      for (int t = 0; t < 6; ++t) {
+        tcur[6 * i + t] = cursor[t];
+        cursor[t] += prep[i].type_rows[t];
+      }
   }
+  std::vector<std::vector<int>> grow(B);  // local type-major row -> global row
   std::vector<int> row_inst(mz), col_inst(nx);
-  for (int i = 0; i < B; ++i) {
+  par_for(B, nth, [&](int i) {
+    auto &p = prep[i];
+    grow[i].resize(p.m);
+    int lr = 0;
+    for (int t = 0; t < 6; ++t)
+      for (int k = 0; k < p.type_rows[t]; ++k) grow[i][lr++] = tcur[6 * i + t] + k;
     for (int g : grow[i]) row_inst[g] = i;
     for (int j = xoff[i]; j < xoff[i + 1]; ++j) col_inst[j] = i;
-  }
+  });
   // ---------------- problem data in global CSR form
-  std::vector<int> Pp(nx + 1, 0), Pj, Ap(mz + 1, 0), Aj, Atp(nx + 1, 0), Atj;
-  std::vector<double> Pxv, Axv, Atxv, q(nx), b(mz), dd(nx), ddinv(nx), ee(mz), eeinv(mz);
-  {
-    // P: full symmetric CSC == CSR by symmetry
-    for (int i = 0; i < B; ++i) {
-      auto &p = prep[i];
-      for (int j = 0; j < p.n; ++j) {
-        for (int k = p.Pfull.p[j]; k < p.Pfull.p[j + 1]; ++k) {
-          Pj.push_back(xoff[i] + p.Pfull.i[k]);
-          Pxv.push_back(p.Pfull.x[k]);
-        }
-        Pp[xoff[i] + j + 1] = (int)Pj.size();
-        q[xoff[i] + j] = p.q[j];
-        dd[xoff[i] + j] = p.d[j];
-        ddinv[xoff[i] + j] = 1.0 / p.d[j];
-      }
-      // A^T rows = A columns (CSC of A)
-      for (int j = 0; j < p.n; ++j) {
-        for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k) {
-          Atj.push_back(0);  // fixed below
-          Atxv.push_back(p.A.x[k]);
-        }
-        Atp[xoff[i] + j + 1] = (int)Atj.size();
-      }
-    }
-    // fix At column indices (global rows) now that sizes are known
-    int pos = 0;
-    for (int i = 0; i < B; ++i) {
-      auto &p = prep[i];
-      std::vector<int> local_of_user(p.m);
-      for (int lr = 0; lr < p.m; ++lr) local_of_user[p.user_row_of[lr]] = lr;
-      for (int j = 0; j < p.n; ++j)
-        for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k)
-          Atj[pos++] = grow[i][local_of_user[p.A.i[k]]];
-      for (int lr = 0; lr < p.m; ++lr) {
-        int g = grow[i][lr], ur = p.user_row_of[lr];
-        b[g] = p.b[ur];
-        ee[g] = p.e[ur];
-        eeinv[g] = 1.0 / p.e[ur];
-      }
-    }
-    // A rows (global) from At
-    std::vector<int> cnt(mz + 1, 0);
-    for (int g : Atj) cnt[g + 1]++;
-    for (int g = 0; g < mz; ++g) Ap[g + 1] = Ap[g] + cnt[g + 1];
-    Aj.assign(Atj.size(), 0);
-    Axv.assign(Atj.size(), 0.0);
-    std::vector<int> next(Ap.begin(), Ap.end() - 1);
-    for (int j = 0; j < nx; ++j)
-      for (int k = Atp[j]; k < Atp[j + 1]; ++k) {
-        int qd = next[Atj[k]]++;
-        Aj[qd] = j;
-        Axv[qd] = Atxv[k];
-      }
+  std::vector<long long> pcnt(B), acnt(B);
+  for (int i = 0; i < B; ++i) {
+    pcnt[i] = prep[i].Pfull.p[prep[i].n];
+    acnt[i] = prep[i].A.p[prep[i].n];
   }
-  std::vector<double> negq(nx);
-  for (int j = 0; j < nx; ++j) negq[j] = -q[j];
+  const auto poffs = prefix(pcnt), aoffs = prefix(acnt);
+  if (poffs[B] > 2000000000LL || aoffs[B] > 2000000000LL) return -4;
+  std::vector<int> Pp(nx + 1, 0), Ap(mz + 1, 0), Atp(nx + 1, 0);
+  hvec<int> Pj(poffs[B]), Aj(aoffs[B]), Atj(aoffs[B]);
+  hvec<double> Pxv(poffs[B]), Axv(aoffs[B]), Atxv(aoffs[B]), q(nx), negq(nx), b(mz), dd(nx),
+      ddinv(nx), ee(mz), eeinv(mz);
+  std::vector<int> arow_cnt(mz, 0);
+  par_for(B, nth, [&](int i) {
+    auto &p = prep[i];
+    // P: full symmetric CSC == CSR by symmetry
+    const long long pb = poffs[i];
+    for (int j = 0; j < p.n; ++j) {
+      for (int k = p.Pfull.p[j]; k < p.Pfull.p[j + 1]; ++k) {
+        Pj[pb + k] = xoff[i] + p.Pfull.i[k];
+        Pxv[pb + k] = p.Pfull.x[k];
+      }
+      Pp[xoff[i] + j + 1] = (int)(pb + p.Pfull.p[j + 1]);
+      q[xoff[i] + j] = p.q[j];
+      negq[xoff[i] + j] = -p.q[j];
+      dd[xoff[i] + j] = p.d[j];
+      ddinv[xoff[i] + j] = 1.0 / p.d[j];
+    }
+    // A^T rows = A columns (CSC of A), column indices = global rows
+    std::vector<int> local_of_user(p.m);
+    for (int lr = 0; lr < p.m; ++lr) local_of_user[p.user_row_of[lr]] = lr;
+    const long long ab = aoffs[i];
+    for (int j = 0; j < p.n; ++j) {
+      for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k) {
+        const int g = grow[i][local_of_user[p.A.i[k]]];
+        Atj[ab + k] = g;
+        Atxv[ab + k] = p.A.x[k];
+        arow_cnt[g]++;  // rows belong to this instance only
+      }
+      Atp[xoff[i] + j + 1] = (int)(ab + p.A.p[j + 1]);
+    }
+    for (int lr = 0; lr < p.m; ++lr) {
+      const int g = grow[i][lr], ur = p.user_row_of[lr];
+      b[g] = p.b[ur];
+      ee[g] = p.e[ur];
+      eeinv[g] = 1.0 / p.e[ur];
+    }
+  });
+  // A rows (global, type-major order) from A^T, columns ascending per row
+  for (int g = 0; g < mz; ++g) Ap[g + 1] = Ap[g] + arow_cnt[g];
+  {
+    std::vector<int> next(Ap.begin(), Ap.end() - 1);
+    par_for(B, nth, [&](int i) {  // an instance touches only its own rows
+      for (int j = xoff[i]; j < xoff[i + 1]; ++j)
+        for (int k = Atp[j]; k < Atp[j + 1]; ++k) {
+          const int qd = next[Atj[k]]++;
+          Aj[qd] = j;
+          Axv[qd] = Atxv[k];
+        }
+    });
+  }
   // ---------------- per-instance constants
   std::vector<double> c(B), nq(B), nb(B);
   std::vector<int> pnnz(B), deg(B), sym(B);
@@ -959,7 +1013,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
     sym[i] = prep[i].symmetric ? 1 : 0;
     if (sym[i]) h->any_sym = true; else h->any_asym = true;
   }
-  // ---------------- cones
+  // ---------------- cones (type lists, instance by instance)
   ConeSet &cs = h->cs;
   cs.B = B;
   cs.m_total = mz;
@@ -972,65 +1026,70 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   cs.exp_begin = type_begin[3];
   cs.pow_begin = type_begin[4];
   cs.psd_begin = type_begin[5];
-  std::vector<int> soc_off, soc_dim, soc_inst, soc_sparse, exp_inst, pow_inst, psd_off, psd_n,
-      psd_inst;
-  std::vector<double> pow_alpha;
+  std::vector<int> nsoc(B), nexp(B), npow(B), npsd(B);
   int soc_maxdim = 0, psd_nmax = 0;
   for (int i = 0; i < B; ++i) {
-    auto &p = prep[i];
-    for (size_t k = 0; k < p.ctype.size(); ++k) {
-      int t = p.ctype[k], g = p.m ? grow[i][p.cstart[k]] : 0;
-      if (t == CLGPU_CONE_SOC) {
-        soc_off.push_back(g);
-        soc_dim.push_back(p.cdim[k]);
-        soc_inst.push_back(i);
-        soc_sparse.push_back(p.cdim[k] > h->st.soc_threshold ? 1 : 0);
-        soc_maxdim = std::max(soc_maxdim, p.cdim[k]);
-      } else if (t == CLGPU_CONE_EXP) {
-        exp_inst.push_back(i);
-      } else if (t == CLGPU_CONE_POW) {
-        pow_inst.push_back(i);
-        pow_alpha.push_back(p.cparam[k]);
-      } else if (t == CLGPU_CONE_PSD) {
-        psd_off.push_back(g);
-        psd_n.push_back(p.cdim[k]);
-        psd_inst.push_back(i);
-        psd_nmax = std::max(psd_nmax, p.cdim[k]);
-      }
+    nsoc[i] = prep[i].type_cones[2];
+    nexp[i] = prep[i].type_cones[3];
+    npow[i] = prep[i].type_cones[4];
+    npsd[i] = prep[i].type_cones[5];
+    for (size_t k = 0; k < prep[i].ctype.size(); ++k) {
+      if (prep[i].ctype[k] == CLGPU_CONE_SOC) soc_maxdim = std::max(soc_maxdim, prep[i].cdim[k]);
+      if (prep[i].ctype[k] == CLGPU_CONE_PSD) psd_nmax = std::max(psd_nmax, prep[i].cdim[k]);
     }
   }
-  cs.n_soc = (int)soc_off.size();
-  cs.n_exp = (int)exp_inst.size();
-  cs.n_pow = (int)pow_inst.size();
-  cs.n_psd = (int)psd_off.size();
+  if (psd_nmax > 16) return -3;  // PSD side limited to 16 (warp-per-cone kernels)
+  const auto osoc = prefix(nsoc), oexp = prefix(nexp), opow = prefix(npow), opsd = prefix(npsd);
+  std::vector<int> soc_off(osoc[B]), soc_dim(osoc[B]), soc_inst(osoc[B]), soc_sparse(osoc[B]),
+      exp_inst(oexp[B]), pow_inst(opow[B]), psd_off(opsd[B]), psd_n(opsd[B]), psd_inst(opsd[B]);
+  std::vector<double> pow_alpha(opow[B]);
+  par_for(B, nth, [&](int i) {
+    auto &p = prep[i];
+    long long a = osoc[i], e = oexp[i], w = opow[i], s = opsd[i];
+    for (size_t k = 0; k < p.ctype.size(); ++k) {
+      const int t = p.ctype[k], g = p.m ? grow[i][p.cstart[k]] : 0;
+      if (t == CLGPU_CONE_SOC) {
+        soc_off[a] = g;
+        soc_dim[a] = p.cdim[k];
+        soc_inst[a] = i;
+        soc_sparse[a] = p.cdim[k] > h->st.soc_threshold ? 1 : 0;
+        ++a;
+      } else if (t == CLGPU_CONE_EXP) {
+        exp_inst[e++] = i;
+      } else if (t == CLGPU_CONE_POW) {
+        pow_inst[w] = i;
+        pow_alpha[w++] = p.cparam[k];
+      } else if (t == CLGPU_CONE_PSD) {
+        psd_off[s] = g;
+        psd_n[s] = p.cdim[k];
+        psd_inst[s++] = i;
+      }
+    }
+  });
+  cs.n_soc = (int)osoc[B];
+  cs.n_exp = (int)oexp[B];
+  cs.n_pow = (int)opow[B];
+  cs.n_psd = (int)opsd[B];
   int G = 2;
   while (G < soc_maxdim && G < 32) G <<= 1;
   cs.soc_group = G;
   cs.psd_nmax = std::max(psd_nmax, 1);
-  if (psd_nmax > 16) return -3;  // PSD side limited to 16 (warp-per-cone kernels)
   {
     // per-instance ranges of each cone type (cones are stored instance by
     // instance inside each type list)
     std::vector<int> rnn(2 * (size_t)B), rsoc(2 * (size_t)B), rexp(2 * (size_t)B),
         rpow(2 * (size_t)B), rpsd(2 * (size_t)B);
-    int cnn = 0, csoc = 0, cexp = 0, cpow = 0, cpsd = 0;
     for (int i = 0; i < B; ++i) {
-      auto &p = prep[i];
-      rnn[2 * i] = cnn;
-      rnn[2 * i + 1] = p.type_rows[1];
-      cnn += p.type_rows[1];
-      rsoc[2 * i] = csoc;
-      rsoc[2 * i + 1] = p.type_cones[2];
-      csoc += p.type_cones[2];
-      rexp[2 * i] = cexp;
-      rexp[2 * i + 1] = p.type_cones[3];
-      cexp += p.type_cones[3];
-      rpow[2 * i] = cpow;
-      rpow[2 * i + 1] = p.type_cones[4];
-      cpow += p.type_cones[4];
-      rpsd[2 * i] = cpsd;
-      rpsd[2 * i + 1] = p.type_cones[5];
-      cpsd += p.type_cones[5];
+      rnn[2 * i] = tcur[6 * i + 1] - type_begin[1];
+      rnn[2 * i + 1] = prep[i].type_rows[1];
+      rsoc[2 * i] = (int)osoc[i];
+      rsoc[2 * i + 1] = nsoc[i];
+      rexp[2 * i] = (int)oexp[i];
+      rexp[2 * i + 1] = nexp[i];
+      rpow[2 * i] = (int)opow[i];
+      rpow[2 * i + 1] = npow[i];
+      rpsd[2 * i] = (int)opsd[i];
+      rpsd[2 * i + 1] = npsd[i];
     }
     cs.rng_nn = A.upload(rnn);
     cs.rng_soc = A.upload(rsoc);
@@ -1071,127 +1130,137 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   cs.psd_lam = A.alloc<double>((size_t)cs.psd_nmax * cs.n_psd);
   cs.cone_tmp = A.alloc<double>((size_t)cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd);
   cs.cone_tmp2 = A.alloc<double>((size_t)cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd);
+  mark("data + cones");
   // ---------------- KKT arrays (concatenate with global positions)
-  std::vector<int> N(B), voff(B + 1, 0), poff(B, 0), lvl_off(B), nlev(B), lvl_ptr, lvl_nodes;
-  long long knz = 0, lnz = 0, rnz = 0;
+  std::vector<int> N(B), voff(B + 1, 0), poff(B, 0), nlev(B);
+  std::vector<long long> kcnt(B), lcnt(B), lvcnt(B);
   for (int i = 0; i < B; ++i) {
     N[i] = prep[i].N;
     voff[i + 1] = voff[i] + N[i];
     poff[i] = voff[i] + i;
-    knz += prep[i].Kj.size();
-    lnz += prep[i].Li.size();
-    rnz += prep[i].Rk.size();
-    lvl_off[i] = (int)lvl_ptr.size();
+    kcnt[i] = (long long)prep[i].Kj.size();
+    lcnt[i] = (long long)prep[i].Li.size();
+    lvcnt[i] = (long long)prep[i].lvl_ptr.size();
     nlev[i] = (int)prep[i].lvl_ptr.size() - 1;
-    lvl_ptr.insert(lvl_ptr.end(), prep[i].lvl_ptr.begin(), prep[i].lvl_ptr.end());
-    lvl_nodes.insert(lvl_nodes.end(), prep[i].lvl_nodes.begin(), prep[i].lvl_nodes.end());
   }
+  const auto kof = prefix(kcnt), lof = prefix(lcnt), lvof = prefix(lvcnt);
+  const long long knz = kof[B], lnz = lof[B];
   if (knz > 2000000000LL || lnz > 2000000000LL) return -4;
+  std::vector<int> lvl_off(B);
+  for (int i = 0; i < B; ++i) lvl_off[i] = (int)lvof[i];
   const int VT = voff[B], PT = voff[B] + B;
-  std::vector<int> Kp(PT), Kj((size_t)knz), Kdiag(VT), Lp(PT), Li((size_t)lnz), Rp(PT),
-      Rk((size_t)rnz), Rpos((size_t)rnz), gsrc(VT);
-  std::vector<double> Kx((size_t)knz);
-  std::vector<signed char> Dsign(VT);
-  std::vector<int> nn_pos, socd_off, socd_pos, socs_diag, socs_uv, socs_D, exp_pos, pow_pos,
-      psdo, psd_pos;
-  long long kb = 0, lb = 0, rb = 0;
+  hvec<int> Kp(PT), Kj((size_t)knz), Kdiag(VT), Lp(PT), Li((size_t)lnz), Rp(PT), Rk((size_t)lnz),
+      Rpos((size_t)lnz), gsrc(VT), lvl_ptr(lvof[B]), lvl_nodes(VT);
+  hvec<double> Kx((size_t)knz);
+  hvec<signed char> Dsign(VT);
+  const int tsize = 8;  // work vectors are FP64 in both precision forms
   int max_small = 0;
   bool has_small = false, has_large = false;
-  const int tsize = 8;  // work vectors are FP64 in both precision forms
-  // NN / SOC / etc. refresh maps must follow the global cone order: type by
-  // type, instance by instance -- collect per type.
-  std::vector<std::vector<int>> nn_by_inst(B);
   for (int i = 0; i < B; ++i) {
-    auto &p = prep[i];
-    int n = p.n, m = p.m;
-    for (int r = 0; r <= N[i]; ++r) {
-      Kp[poff[i] + r] = (int)(kb + p.Kp[r]);
-      Lp[poff[i] + r] = (int)(lb + p.Lp[r]);
-      Rp[poff[i] + r] = (int)(rb + p.Rp[r]);
-    }
-    for (size_t k = 0; k < p.Kj.size(); ++k) {
-      Kj[kb + k] = p.Kj[k];
-      Kx[kb + k] = p.Kx[k];
-    }
-    for (size_t k = 0; k < p.Li.size(); ++k) Li[lb + k] = p.Li[k];
-    for (size_t k = 0; k < p.Rk.size(); ++k) {
-      Rk[rb + k] = p.Rk[k];
-      Rpos[rb + k] = (int)(lb + p.Rpos[k]);
-    }
-    for (int r = 0; r < N[i]; ++r) {
-      Kdiag[voff[i] + r] = (int)(kb + p.Kdiag[r]);
-      Dsign[voff[i] + r] = p.Dsign[r];
-      int o = p.perm[r];
-      int code;
-      if (o < n)
-        code = xoff[i] + o;
-      else if (o < n + m)
-        code = -grow[i][o - n] - 2;
-      else
-        code = -1;
-      gsrc[voff[i] + r] = code;
-    }
     if ((long long)N[i] * tsize <= 48 * 1024) {
       has_small = true;
       max_small = std::max(max_small, N[i]);
     } else {
       has_large = true;
     }
-    kb += p.Kj.size();
-    lb += p.Li.size();
-    rb += p.Rk.size();
   }
-  // refresh maps in global cone order
-  auto addk = [&](int i, int v) { return v < 0 ? -1 : (int)(v + (Kp[poff[i]])); };
-  for (int i = 0; i < B; ++i)
-    for (int v : prep[i].nn_pos) nn_pos.push_back(addk(i, v));
-  {
-    int dense_entries = 0;
-    for (int i = 0; i < B; ++i) {
-      auto &p = prep[i];
-      size_t sc = 0;
-      for (size_t k = 0; k < p.ctype.size(); ++k) {
-        if (p.ctype[k] != CLGPU_CONE_SOC) continue;
-        int st0 = p.socd_start[sc];
-        if (st0 < 0) {
-          socd_off.push_back(0);
-        } else {
-          socd_off.push_back(dense_entries);
-          int dim = p.cdim[k];
-          int t = dim * (dim + 1) / 2;
-          for (int e2 = 0; e2 < t; ++e2) {
-            socd_pos.push_back(addk(i, p.socd_pos[2 * (st0 + e2)]));
-            socd_pos.push_back(addk(i, p.socd_pos[2 * (st0 + e2) + 1]));
-          }
-          dense_entries += t;
-        }
-        socs_D.push_back(addk(i, p.socs_D[2 * sc]));
-        socs_D.push_back(addk(i, p.socs_D[2 * sc + 1]));
+  par_for(B, nth, [&](int i) {
+    auto &p = prep[i];
+    const int n = p.n, m = p.m;
+    const long long kb = kof[i], lb = lof[i];
+    for (int r = 0; r <= N[i]; ++r) {
+      Kp[poff[i] + r] = (int)(kb + p.Kp[r]);
+      Lp[poff[i] + r] = (int)(lb + p.Lp[r]);
+      Rp[poff[i] + r] = (int)(lb + p.Rp[r]);
+    }
+    std::copy(p.Kj.begin(), p.Kj.end(), Kj.begin() + kb);
+    std::copy(p.Kx.begin(), p.Kx.end(), Kx.begin() + kb);
+    std::copy(p.Li.begin(), p.Li.end(), Li.begin() + lb);
+    std::copy(p.Rk.begin(), p.Rk.end(), Rk.begin() + lb);
+    for (size_t k = 0; k < p.Rpos.size(); ++k) Rpos[lb + k] = (int)(lb + p.Rpos[k]);
+    std::copy(p.lvl_ptr.begin(), p.lvl_ptr.end(), lvl_ptr.begin() + lvof[i]);
+    std::copy(p.lvl_nodes.begin(), p.lvl_nodes.end(), lvl_nodes.begin() + voff[i]);
+    for (int r = 0; r < N[i]; ++r) {
+      Kdiag[voff[i] + r] = (int)(kb + p.Kdiag[r]);
+      Dsign[voff[i] + r] = p.Dsign[r];
+      const int o = p.perm[r];
+      gsrc[voff[i] + r] = o < n ? xoff[i] + o : (o < n + m ? -grow[i][o - n] - 2 : -1);
+    }
+  });
+  // refresh maps in global cone order (type lists, instance by instance)
+  std::vector<long long> c_nn(B), c_sde(B), c_srow(B), c_exp(B), c_pow(B), c_pse(B);
+  for (int i = 0; i < B; ++i) {
+    auto &p = prep[i];
+    c_nn[i] = (long long)p.nn_pos.size();
+    c_srow[i] = (long long)p.socs_diag.size();
+    c_exp[i] = (long long)p.exp_pos.size();
+    c_pow[i] = (long long)p.pow_pos.size();
+    long long de = 0, pe = 0;
+    size_t sc = 0, pc = 0;
+    for (size_t k = 0; k < p.ctype.size(); ++k) {
+      if (p.ctype[k] == CLGPU_CONE_SOC) {
+        if (p.socd_start[sc] >= 0) de += (long long)p.cdim[k] * (p.cdim[k] + 1) / 2;
         ++sc;
-      }
-      for (int v : p.socs_diag) socs_diag.push_back(addk(i, v));
-      for (int v : p.socs_uv) socs_uv.push_back(addk(i, v));
-      for (int v : p.exp_pos) exp_pos.push_back(addk(i, v));
-      for (int v : p.pow_pos) pow_pos.push_back(addk(i, v));
-    }
-    int psd_entries = 0;
-    for (int i = 0; i < B; ++i) {
-      auto &p = prep[i];
-      size_t pc = 0;
-      for (size_t k = 0; k < p.ctype.size(); ++k) {
-        if (p.ctype[k] != CLGPU_CONE_PSD) continue;
-        int st0 = p.psd_start[pc++];
-        int t = p.cdim[k] * (p.cdim[k] + 1) / 2;
-        int tt = t * (t + 1) / 2;
-        psdo.push_back(psd_entries);
-        for (int e2 = 0; e2 < tt; ++e2) {
-          psd_pos.push_back(addk(i, p.psd_pos[2 * (st0 + e2)]));
-          psd_pos.push_back(addk(i, p.psd_pos[2 * (st0 + e2) + 1]));
-        }
-        psd_entries += tt;
+      } else if (p.ctype[k] == CLGPU_CONE_PSD) {
+        const long long t = (long long)p.cdim[k] * (p.cdim[k] + 1) / 2;
+        pe += t * (t + 1) / 2;
+        ++pc;
       }
     }
+    c_sde[i] = de;
+    c_pse[i] = pe;
   }
+  const auto o_nn = prefix(c_nn), o_sde = prefix(c_sde), o_srow = prefix(c_srow),
+             o_exp = prefix(c_exp), o_pow = prefix(c_pow), o_pse = prefix(c_pse);
+  std::vector<int> nn_pos(o_nn[B]), socd_off(osoc[B]), socd_pos(2 * o_sde[B]),
+      socs_diag(o_srow[B]), socs_uv(4 * o_srow[B]), socs_D(2 * osoc[B]), exp_pos(o_exp[B]),
+      pow_pos(o_pow[B]), psdo(opsd[B]), psd_pos(2 * o_pse[B]);
+  par_for(B, nth, [&](int i) {
+    auto &p = prep[i];
+    const int kb = Kp[poff[i]];
+    auto addk = [&](int v) { return v < 0 ? -1 : v + kb; };
+    for (long long t = 0; t < c_nn[i]; ++t) nn_pos[o_nn[i] + t] = addk(p.nn_pos[t]);
+    long long sc_g = osoc[i], de = o_sde[i];
+    size_t sc = 0;
+    for (size_t k = 0; k < p.ctype.size(); ++k) {
+      if (p.ctype[k] != CLGPU_CONE_SOC) continue;
+      const int st0 = p.socd_start[sc];
+      if (st0 < 0) {
+        socd_off[sc_g] = 0;
+      } else {
+        socd_off[sc_g] = (int)de;
+        const int dim = p.cdim[k], t = dim * (dim + 1) / 2;
+        for (int e2 = 0; e2 < t; ++e2) {
+          socd_pos[2 * (de + e2)] = addk(p.socd_pos[2 * (st0 + e2)]);
+          socd_pos[2 * (de + e2) + 1] = addk(p.socd_pos[2 * (st0 + e2) + 1]);
+        }
+        de += t;
+      }
+      socs_D[2 * sc_g] = addk(p.socs_D[2 * sc]);
+      socs_D[2 * sc_g + 1] = addk(p.socs_D[2 * sc + 1]);
+      ++sc;
+      ++sc_g;
+    }
+    for (long long t = 0; t < c_srow[i]; ++t) socs_diag[o_srow[i] + t] = addk(p.socs_diag[t]);
+    for (long long t = 0; t < 4 * c_srow[i]; ++t)
+      socs_uv[4 * o_srow[i] + t] = addk(p.socs_uv[t]);
+    for (long long t = 0; t < c_exp[i]; ++t) exp_pos[o_exp[i] + t] = addk(p.exp_pos[t]);
+    for (long long t = 0; t < c_pow[i]; ++t) pow_pos[o_pow[i] + t] = addk(p.pow_pos[t]);
+    long long pe = o_pse[i], pc_g = opsd[i];
+    size_t pc = 0;
+    for (size_t k = 0; k < p.ctype.size(); ++k) {
+      if (p.ctype[k] != CLGPU_CONE_PSD) continue;
+      const int st0 = p.psd_start[pc++];
+      const long long t = (long long)p.cdim[k] * (p.cdim[k] + 1) / 2, tt = t * (t + 1) / 2;
+      psdo[pc_g++] = (int)pe;
+      for (long long e2 = 0; e2 < tt; ++e2) {
+        psd_pos[2 * (pe + e2)] = addk(p.psd_pos[2 * (st0 + e2)]);
+        psd_pos[2 * (pe + e2) + 1] = addk(p.psd_pos[2 * (st0 + e2) + 1]);
+      }
+      pe += tt;
+    }
+  });
+  mark("kkt concat + maps");
   KKTMapDev &mp = h->map;
   mp.nn_pos = A.upload(nn_pos);
   mp.socd_off = A.upload(socd_off);
@@ -1205,6 +1274,8 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   mp.psd_pos = A.upload(psd_pos);
   KKTDev &kk = h->kk;
   kk.B = B;
+  kk.prof_bytes = nullptr;
+  h->d_prof_bytes = A.alloc<double>(2 * (size_t)B);
   kk.N = A.upload(N);
   kk.voff = A.upload(voff);
   kk.poff = A.upload(poff);
@@ -1223,119 +1294,131 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   kk.nlev = A.upload(nlev);
   kk.lvl_ptr = A.upload(lvl_ptr);
   kk.lvl_nodes = A.upload(lvl_nodes);
-  {
+  mark("kkt upload");
+  // ---------------- substitution schedules (block instances) and streams
+  // (single-warp instances)
+  kk.fsched = kk.bsched = nullptr;
+  if (has_large) {
     std::vector<int4> fsched(VT), bsched(VT);
-    for (int i = 0; i < B; ++i) {
-      const int nl = nlev[i];
+    par_for(B, nth, [&](int i) {
       const int *lp = lvl_ptr.data() + lvl_off[i];
       const int *nodes = lvl_nodes.data() + voff[i];
-      for (int l = 0; l < nl; ++l)
+      for (int l = 0; l < nlev[i]; ++l)
         for (int t = lp[l]; t < lp[l + 1]; ++t) {
           const int j = nodes[t];
           fsched[voff[i] + t] = make_int4(j, Rp[poff[i] + j], Rp[poff[i] + j + 1], 0);
           const int bp = N[i] - lp[l + 1] + (t - lp[l]);
           bsched[voff[i] + bp] = make_int4(j, Lp[poff[i] + j], Lp[poff[i] + j + 1], 0);
         }
-    }
+    });
     kk.fsched = A.upload(fsched);
     kk.bsched = A.upload(bsched);
-    // level-ordered nonzero streams (single-warp substitution) and K rows
-    std::vector<int2> fent((size_t)lnz), bent((size_t)lnz);
-    std::vector<int> fpos((size_t)lnz), bpos((size_t)lnz), flev(lvl_ptr.size()),
-        blev(lvl_ptr.size());
-    std::vector<int2> kent((size_t)knz);
-    for (int i = 0; i < B; ++i) {
-      const auto &p = prep[i];
-      const int nl = nlev[i];
-      const int *lp = p.lvl_ptr.data();
-      const long long base = Lp[poff[i]];
-      long long f = base;
-      for (int l = 0; l < nl; ++l) {
-        flev[lvl_off[i] + l] = (int)f;
-        for (int t = lp[l]; t < lp[l + 1]; ++t) {
-          const int node = p.lvl_nodes[t];
-          for (int r = p.Rp[node]; r < p.Rp[node + 1]; ++r) {
-            fent[f] = make_int2(node, p.Rk[r]);
-            fpos[f] = (int)(base + p.Rpos[r]);
-            ++f;
-          }
-        }
+  }
+  hvec<int2> fent((size_t)lnz), bent((size_t)lnz), kent((size_t)knz);
+  hvec<int> fpos((size_t)lnz), bpos((size_t)lnz), flev(lvl_ptr.size()), blev(lvl_ptr.size());
+  std::vector<int> nchf(B, 0), nchb(B, 0), nchk(B, 0);
+  // encode segment positions: .x = seg | min(pos, 31) << 16 | last << 21
+  auto encode = [](int2 *e, long long n) {
+    long long q = 0;
+    while (q < n) {
+      long long r = q;
+      while (r + 1 < n && e[r + 1].x == e[q].x) ++r;
+      for (long long t = q; t <= r; ++t) {
+        const int pos = (int)std::min<long long>(t - q, 31);
+        e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << 21);
       }
-      flev[lvl_off[i] + nl] = (int)f;
-      long long g = base;
-      for (int l = nl - 1, t2 = 0; l >= 0; --l, ++t2) {
-        blev[lvl_off[i] + t2] = (int)g;
-        for (int t = lp[l]; t < lp[l + 1]; ++t) {
-          const int node = p.lvl_nodes[t];
-          for (int q = p.Lp[node]; q < p.Lp[node + 1]; ++q) {
-            bent[g] = make_int2(node, p.Li[q]);
-            bpos[g] = (int)(base + q);
-            ++g;
-          }
-        }
-      }
-      blev[lvl_off[i] + nl] = (int)g;
-      const long long kbase = Kp[poff[i]];
-      for (int r = 0; r < N[i]; ++r)
-        for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) kent[kbase + q] = make_int2(r, p.Kj[q]);
+      q = r + 1;
     }
-    // encode segment positions and build the chunk tables (entries of one
-    // level at most 32 per chunk; the residual stream is a single level)
-    std::vector<int> fch, bch, kch, fch_off(B + 1, 0), bch_off(B + 1, 0), kch_off(B + 1, 0);
-    auto encode = [](int2 *e, long long n) {
-      long long q = 0;
-      while (q < n) {
-        long long r = q;
-        while (r + 1 < n && e[r + 1].x == e[q].x) ++r;
-        for (long long t = q; t <= r; ++t) {
-          const int pos = (int)std::min<long long>(t - q, 31);
-          e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << 21);
+  };
+  auto nchunks = [](const int *lev, int nl) {
+    int n = 0;
+    for (int l = 0; l < nl; ++l) n += (lev[l + 1] - lev[l] + 31) / 32;
+    return n;
+  };
+  par_for(B, nth, [&](int i) {
+    const auto &p = prep[i];
+    const int nl = nlev[i];
+    const int *lp = p.lvl_ptr.data();
+    const long long base = Lp[poff[i]];
+    long long f = base;
+    for (int l = 0; l < nl; ++l) {
+      flev[lvl_off[i] + l] = (int)f;
+      for (int t = lp[l]; t < lp[l + 1]; ++t) {
+        const int node = p.lvl_nodes[t];
+        for (int r = p.Rp[node]; r < p.Rp[node + 1]; ++r) {
+          fent[f] = make_int2(node, p.Rk[r]);
+          fpos[f] = (int)(base + p.Rpos[r]);
+          ++f;
         }
-        q = r + 1;
       }
-    };
-    auto chunks = [](std::vector<int> &out, const int *lev, int nl, long long base) {
+    }
+    flev[lvl_off[i] + nl] = (int)f;
+    long long g = base;
+    for (int l = nl - 1, t2 = 0; l >= 0; --l, ++t2) {
+      blev[lvl_off[i] + t2] = (int)g;
+      for (int t = lp[l]; t < lp[l + 1]; ++t) {
+        const int node = p.lvl_nodes[t];
+        for (int q = p.Lp[node]; q < p.Lp[node + 1]; ++q) {
+          bent[g] = make_int2(node, p.Li[q]);
+          bpos[g] = (int)(base + q);
+          ++g;
+        }
+      }
+    }
+    blev[lvl_off[i] + nl] = (int)g;
+    const long long kbase = Kp[poff[i]];
+    for (int r = 0; r < N[i]; ++r)
+      for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) kent[kbase + q] = make_int2(r, p.Kj[q]);
+    if ((long long)N[i] * tsize <= 48 * 1024) {
+      encode(fent.data() + base, f - base);
+      encode(bent.data() + base, g - base);
+      encode(kent.data() + kbase, (long long)p.Kj.size());
+      nchf[i] = nchunks(flev.data() + lvl_off[i], nl);
+      nchb[i] = nchunks(blev.data() + lvl_off[i], nl);
+      nchk[i] = ((int)p.Kj.size() + 31) / 32;
+    }
+  });
+  // chunk tables: start relative to the stream base (bits 0..25) | (count - 1) << 26
+  const auto ofch = prefix(nchf), obch = prefix(nchb), okch = prefix(nchk);
+  hvec<int> fch(ofch[B]), bch(obch[B]), kch(okch[B]);
+  std::vector<int> fch_off(B + 1), bch_off(B + 1), kch_off(B + 1);
+  for (int i = 0; i <= B; ++i) {
+    fch_off[i] = (int)ofch[i];
+    bch_off[i] = (int)obch[i];
+    kch_off[i] = (int)okch[i];
+  }
+  par_for(B, nth, [&](int i) {
+    auto put = [](int *out, const int *lev, int nl, long long base) {
       for (int l = 0; l < nl; ++l)
         for (long long c = lev[l]; c < lev[l + 1]; c += 32) {
           const long long cnt = std::min<long long>(32, lev[l + 1] - c);
-          out.push_back((int)((c - base) | ((cnt - 1) << 26)));
+          *out++ = (int)((c - base) | ((cnt - 1) << 26));
         }
     };
-    for (int i = 0; i < B; ++i) {
-      const long long base = Lp[poff[i]], n_l = Lp[poff[i] + N[i]] - base;
-      const long long kbase = Kp[poff[i]], n_k = Kp[poff[i] + N[i]] - kbase;
-      const bool small = (long long)N[i] * tsize <= 48 * 1024;
-      if (small) {
-        encode(fent.data() + base, n_l);
-        encode(bent.data() + base, n_l);
-        encode(kent.data() + kbase, n_k);
-        chunks(fch, flev.data() + lvl_off[i], nlev[i], base);
-        chunks(bch, blev.data() + lvl_off[i], nlev[i], base);
-        const int klev[2] = {(int)kbase, (int)(kbase + n_k)};
-        chunks(kch, klev, 1, kbase);
-      }
-      fch_off[i + 1] = (int)fch.size();
-      bch_off[i + 1] = (int)bch.size();
-      kch_off[i + 1] = (int)kch.size();
-    }
-    kk.fch = A.upload(fch);
-    kk.bch = A.upload(bch);
-    kk.kch = A.upload(kch);
-    kk.fch_off = A.upload(fch_off);
-    kk.bch_off = A.upload(bch_off);
-    kk.kch_off = A.upload(kch_off);
-    kk.fent = A.upload(fent);
-    kk.bent = A.upload(bent);
-    kk.fpos = A.upload(fpos);
-    kk.bpos = A.upload(bpos);
-    kk.flev = A.upload(flev);
-    kk.blev = A.upload(blev);
-    kk.kent = A.upload(kent);
-  }
+    if (!nchf[i] && !nchb[i] && !nchk[i]) return;
+    const long long base = Lp[poff[i]], kbase = Kp[poff[i]];
+    put(fch.data() + ofch[i], flev.data() + lvl_off[i], nlev[i], base);
+    put(bch.data() + obch[i], blev.data() + lvl_off[i], nlev[i], base);
+    const int klev[2] = {(int)kbase, (int)(kbase + prep[i].Kj.size())};
+    put(kch.data() + okch[i], klev, 1, kbase);
+  });
+  kk.fch = A.upload(fch);
+  kk.bch = A.upload(bch);
+  kk.kch = A.upload(kch);
+  kk.fch_off = A.upload(fch_off);
+  kk.bch_off = A.upload(bch_off);
+  kk.kch_off = A.upload(kch_off);
+  kk.fent = A.upload(fent);
+  kk.bent = A.upload(bent);
+  kk.fpos = A.upload(fpos);
+  kk.bpos = A.upload(bpos);
+  kk.flev = A.upload(flev);
+  kk.blev = A.upload(blev);
+  kk.kent = A.upload(kent);
   if (h->mixed) {
     kk.LxF = A.alloc<float>((size_t)lnz);
     kk.LxB = A.alloc<float>((size_t)lnz);
-    kk.LxR = A.alloc<float>((size_t)lnz);
+    kk.LxR = has_large ? A.alloc<float>((size_t)lnz) : nullptr;
     kk.Lx = A.alloc<float>((size_t)lnz);
     kk.D = A.alloc<float>(VT);
     kk.Dinv = A.alloc<float>(VT);
@@ -1344,13 +1427,14 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   } else {
     kk.LxF = A.alloc<double>((size_t)lnz);
     kk.LxB = A.alloc<double>((size_t)lnz);
-    kk.LxR = A.alloc<double>((size_t)lnz);
+    kk.LxR = has_large ? A.alloc<double>((size_t)lnz) : nullptr;
     kk.Lx = A.alloc<double>((size_t)lnz);
     kk.D = A.alloc<double>(VT);
     kk.Dinv = A.alloc<double>(VT);
     kk.Lacc = nullptr;
     kk.Dacc = nullptr;
   }
+  mark("schedules + streams");
   kk.yf = A.alloc<double>(VT);
   kk.w = A.alloc<double>(VT);
   kk.max_small_N = max_small;
@@ -1439,6 +1523,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep) {
   if (A.err != cudaSuccess) return -1000 - (int)A.err;
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return -1000 - (int)e;
+  mark("scratch + tail");
   return 0;
 }
 
@@ -1463,6 +1548,7 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
   int nth = h->st.setup_threads > 0 ? h->st.setup_threads
                                     : (int)std::max(1u, std::thread::hardware_concurrency());
   nth = std::min(nth, nprob);
+  auto t_prep = std::chrono::steady_clock::now();
   {
     std::vector<std::thread> th;
     std::atomic<int> next{0};
@@ -1483,7 +1569,11 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
       delete h;
       return -2;
     }
-  int rc = build_batch(h, prep);
+  if (h->st.verbose)
+    std::fprintf(stderr, "clgpu setup: %-22s %8.1f ms (%d threads)\n", "prepare instances",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                           t_prep).count(), nth);
+  int rc = build_batch(h, prep, nth);
   if (rc != 0) {
     delete h;
     return rc;
@@ -1591,6 +1681,9 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
   Dev &dv = h->dv;
   const int B = h->B;
   h->launches = 0;
+  if (h->profiling && h->d_prof_bytes)
+    cudaMemsetAsync(h->d_prof_bytes, 0, 2 * (size_t)B * sizeof(double), st);
+  h->kk.prof_bytes = h->profiling ? h->d_prof_bytes : nullptr;
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
@@ -1823,6 +1916,12 @@ extern "C" int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms, l
     if (ms) ms[c] = h->prof[c];
     if (calls) calls[c] = h->prof_calls[c];
   }
+  return 0;
+}
+extern "C" int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes) {
+  if (!h || !bytes) return -1;
+  bytes[0] = h->prof_bytes[0];
+  bytes[1] = h->prof_bytes[1];
   return 0;
 }
 extern "C" int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,

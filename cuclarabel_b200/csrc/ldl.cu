@@ -264,6 +264,13 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
     for (int r = rbeg + tid; r < rend; r += NT) LxR[r] = Lx[k.Rpos[r]];
   }
   double bad = block_max<NT>(finite ? 0.0 : 1.0, red);
+  if (k.prof_bytes && tid == 0) {
+    // algorithmic bytes: K (indices + values) and the symbolic structure read
+    // once, L, D, D^-1 and the substitution copies of L written once
+    const double nl = Lp[N] - Lp[0], nk = Kp[N] - Kp[0], ts = sizeof(T);
+    k.prof_bytes[inst] += 12.0 * nk + 16.0 * N + 12.0 * nl + ts * (nl + 2.0 * N) +
+                          (SMEM ? nl * (8.0 + 2.0 * ts) : nl * (4.0 + ts));
+  }
   if (tid == 0) {
     if (bad > 0) ok[inst] = 0;
     if (eps_out) eps_out[inst] = eps;
@@ -631,7 +638,9 @@ __global__ void __launch_bounds__(32, 16)
   const double normb = warp_max(nb);
   __syncwarp();
   double tv[kVecU];
+  int ntri = 0, nres = 0, nir = 0;
   auto trisolve = [&]() {
+    ++ntri;
     ring_pass<T, false>(fch, nfch, lbase, k.fent, LxF, y, y, re, rv, lane);
     VEC_LOOP(i, N, tv[u] = double(Dinv[i]);, y[i] *= tv[u];)
     __syncwarp();
@@ -639,6 +648,7 @@ __global__ void __launch_bounds__(32, 16)
   };
   // e = b - K y, returns ||e||_inf (+inf when not finite)
   auto residual = [&]() {
+    ++nres;
     ring_pass<double, true>(kch, nkch, kbase, k.kent, k.Kx, y, e, re,
                             reinterpret_cast<double *>(rv), lane);
     __syncwarp();
@@ -666,6 +676,7 @@ __global__ void __launch_bounds__(32, 16)
     for (int it = 0; good && it < prm.ir_maxiter; ++it) {
       if (norme <= prm.ir_abstol + prm.ir_reltol * normb) break;
       const double last = norme;
+      ++nir;
       VEC_LOOP(i, N, tv[u] = e[i];, y[i] = tv[u];)
       __syncwarp();
       trisolve();
@@ -692,6 +703,17 @@ __global__ void __launch_bounds__(32, 16)
     }
     if (__any_sync(0xffffffffu, bad)) good = false;
     __syncwarp();
+  }
+  if (k.prof_bytes && lane == 0) {
+    // algorithmic bytes: every stream pass reads its entries, values and
+    // chunk words once; vectors are read / written once per use
+    const double nl = k.Lp[po + N] - lbase, nk = k.Kp[po + N] - kbase, ts = sizeof(T);
+    k.prof_bytes[k.B + inst] +=
+        20.0 * N                                                   // rhs gather, b
+        + ntri * (2.0 * nl * (8 + ts) + 4.0 * (nfch + nbch) + ts * N)  // substitutions
+        + nres * (16.0 * nk + 4.0 * nkch + 24.0 * N)                // residuals
+        + nir * 24.0 * N + 8.0 * N                                  // refinement vectors
+        + 20.0 * N;                                                 // result scatter
   }
   if (!good) {
     if (lane == 0) ok[inst] = 0;

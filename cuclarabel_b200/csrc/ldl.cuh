@@ -60,6 +60,9 @@ struct KKTDev {
   // (bits 0..25) | (count - 1) << 26.  Instance i's chunks of the forward,
   // backward and residual passes are fch[fch_off[i] .. fch_off[i+1]) etc.
   const int *fch, *bch, *kch, *fch_off, *bch_off, *kch_off;
+  // profiling only (else null): per instance, algorithmic bytes moved by the
+  // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
+  double *prof_bytes;
   int max_small_N;       // largest N among single-warp (shared memory) instances
   int has_small, has_large;
   // scratch (global, per instance, sum N each)

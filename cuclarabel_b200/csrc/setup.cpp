@@ -105,28 +105,96 @@ std::vector<int> amd_order(int n, std::vector<std::vector<int>> &adj) {
 // height near (separator size) x log2(N), which is what bounds the
 // level-scheduled factorisation and substitutions.  Dense vertices (degree
 // above max(16, 10 sqrt(n))) are ordered last, as in amd_order.
-std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
-  constexpr int kNdLeaf = 8;
-  for (auto &a : adj) {
-    std::sort(a.begin(), a.end());
-    a.erase(std::unique(a.begin(), a.end()), a.end());
+// Minimum degree on at most 32 vertices (adjacency as bit masks); ties go
+// to the lower local index, as in amd_order.
+static void md_small(const int *S, int k, const uint32_t *mask_in, std::vector<int> &order) {
+  uint32_t m[32];
+  for (int a = 0; a < k; ++a) m[a] = mask_in[a];
+  uint32_t alive = k == 32 ? 0xffffffffu : ((1u << k) - 1u);
+  for (int step = 0; step < k; ++step) {
+    int best = -1, bd = 64;
+    for (uint32_t w = alive; w; w &= w - 1) {
+      const int a = __builtin_ctz(w);
+      const int d = __builtin_popcount(m[a] & alive);
+      if (d < bd) {
+        bd = d;
+        best = a;
+      }
+    }
+    alive &= ~(1u << best);
+    const uint32_t nb = m[best] & alive;
+    for (uint32_t w = nb; w; w &= w - 1) {
+      const int u = __builtin_ctz(w);
+      m[u] |= nb;
+      m[u] &= ~(1u << u);
+    }
+    order.push_back(S[best]);
   }
+}
+
+std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
+  std::vector<int> xadj(n + 1, 0), adjncy;
+  for (int i = 0; i < n; ++i) xadj[i + 1] = xadj[i] + (int)adj[i].size();
+  adjncy.reserve(xadj[n]);
+  for (auto &a : adj) adjncy.insert(adjncy.end(), a.begin(), a.end());
+  return nd_order_csr(n, xadj, adjncy);
+}
+
+// Nested dissection (George's level-structure bisection).  A connected
+// vertex set larger than kNdLeaf is split by a middle level of a breadth-first
+// level structure rooted at a pseudo-peripheral vertex; only the vertices of
+// that level with a neighbour in the next level form the separator.  The two
+// halves are ordered first (recursively), the separator last, so the halves
+// become independent subtrees of the elimination tree.  Small sets are
+// ordered by minimum degree.  The KKT graphs of stage-structured problems
+// are long and thin: minimum degree eliminates them from both ends inward
+// and leaves an elimination tree of height ~N/2, while dissection keeps the
+// height near (separator size) x log2(N), which is what bounds the
+// level-scheduled factorisation and substitutions.  Dense vertices (degree
+// above max(16, 10 sqrt(n))) are ordered last, as in amd_order.  The input
+// CSR may hold repeated neighbours; it is deduplicated in place.
+std::vector<int> nd_order_csr(int n, std::vector<int> &xadj0, std::vector<int> &adj0) {
+  constexpr int kNdLeaf = 8;
+  // sort + deduplicate every row, compacting
+  {
+    int w = 0;
+    for (int i = 0; i < n; ++i) {
+      const int b0 = xadj0[i], b1 = xadj0[i + 1];
+      std::sort(adj0.begin() + b0, adj0.begin() + b1);
+      const int start = w;
+      for (int p = b0; p < b1; ++p)
+        if (p == b0 || adj0[p] != adj0[p - 1]) adj0[w++] = adj0[p];
+      xadj0[i] = start;
+    }
+    xadj0[n] = w;
+    // xadj0[i] now holds row starts; shift into a proper pointer array
+  }
+  std::vector<int> rowend(n);
+  for (int i = 0; i < n; ++i) rowend[i] = i + 1 < n ? xadj0[i + 1] : xadj0[n];
   const double dense_thr = std::max(16.0, 10.0 * std::sqrt((double)n));
   std::vector<char> dense(n, 0);
-  for (int i = 0; i < n; ++i) dense[i] = (double)adj[i].size() > dense_thr;
-  // CSR of the graph without dense vertices
+  bool any_dense = false;
+  for (int i = 0; i < n; ++i) {
+    dense[i] = (double)(rowend[i] - xadj0[i]) > dense_thr;
+    any_dense |= dense[i] != 0;
+  }
   std::vector<int> xadj(n + 1, 0), adjncy;
+  adjncy.reserve(xadj0[n]);
   for (int i = 0; i < n; ++i) {
     if (!dense[i])
-      for (int u : adj[i])
-        if (!dense[u]) adjncy.push_back(u);
+      for (int p = xadj0[i]; p < rowend[i]; ++p)
+        if (!any_dense || !dense[adj0[p]]) adjncy.push_back(adj0[p]);
     xadj[i + 1] = (int)adjncy.size();
   }
   std::vector<int> order;
   order.reserve(n);
-  std::vector<int> mark(n, -1), level(n, -1), queue(n);
+  std::vector<int> mark(n, -1), lidx(n, -1), indeg(n, 0);
+  // two level structures (the current best and a candidate); queue[s] lists
+  // structure s's vertices in visiting order
+  std::vector<int> level_buf[2] = {std::vector<int>(n, -1), std::vector<int>(n, -1)};
+  std::vector<int> queue_buf[2] = {std::vector<int>(n), std::vector<int>(n)};
+  int cnt_buf[2] = {0, 0};
   int stamp = 0;
-  // task: a vertex set and whether it is emitted as is (a separator)
   struct Task {
     std::vector<int> v;
     bool emit;
@@ -139,46 +207,60 @@ std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
       if (!dense[i]) t.v.push_back(i);
     if (!t.v.empty()) stack.push_back(std::move(t));
   }
-  auto deg_in = [&](int v, int sid) {
-    int d = 0;
-    for (int p = xadj[v]; p < xadj[v + 1]; ++p) d += mark[adjncy[p]] == sid;
-    return d;
-  };
-  // breadth-first levels of the set marked sid from src; returns the depth
-  // and fills queue[0..cnt) in visiting order
-  auto bfs = [&](int src, int sid, int &cnt) {
-    for (int i = 0; i < cnt; ++i) level[queue[i]] = -1;
+  // breadth-first levels of the set marked sid from src into structure b
+  // (clearing b's previous visit); also records every visited vertex's
+  // degree inside the set.  Returns the depth.
+  auto bfs = [&](int src, int sid, int b) {
+    std::vector<int> &level = level_buf[b], &queue = queue_buf[b];
+    for (int i = 0; i < cnt_buf[b]; ++i) level[queue[i]] = -1;
     int head = 0, tail = 0, depth = 0;
     queue[tail++] = src;
     level[src] = 0;
     while (head < tail) {
-      int v = queue[head++];
+      const int v = queue[head++];
       depth = std::max(depth, level[v] + 1);
+      int d = 0;
       for (int p = xadj[v]; p < xadj[v + 1]; ++p) {
-        int u = adjncy[p];
-        if (mark[u] == sid && level[u] < 0) {
+        const int u = adjncy[p];
+        if (mark[u] != sid) continue;
+        ++d;
+        if (level[u] < 0) {
           level[u] = level[v] + 1;
           queue[tail++] = u;
         }
       }
+      indeg[v] = d;
     }
-    cnt = tail;
+    cnt_buf[b] = tail;
     return depth;
+  };
+  auto clear_levels = [&](int b) {
+    for (int i = 0; i < cnt_buf[b]; ++i) level_buf[b][queue_buf[b][i]] = -1;
+    cnt_buf[b] = 0;
   };
   auto md_leaf = [&](const std::vector<int> &S) {
     const int k = (int)S.size();
     const int sid = ++stamp;
     for (int a = 0; a < k; ++a) {
       mark[S[a]] = sid;
-      level[S[a]] = a;  // local index
+      lidx[S[a]] = a;
     }
-    std::vector<std::vector<int>> la(k);
-    for (int a = 0; a < k; ++a)
-      for (int p = xadj[S[a]]; p < xadj[S[a] + 1]; ++p)
-        if (mark[adjncy[p]] == sid) la[a].push_back(level[adjncy[p]]);
-    for (int a = 0; a < k; ++a) level[S[a]] = -1;
-    std::vector<int> lp = amd_order(k, la);
-    for (int a : lp) order.push_back(S[a]);
+    if (k <= 32) {
+      uint32_t masks[32];
+      for (int a = 0; a < k; ++a) {
+        uint32_t mk = 0;
+        for (int p = xadj[S[a]]; p < xadj[S[a] + 1]; ++p)
+          if (mark[adjncy[p]] == sid) mk |= 1u << lidx[adjncy[p]];
+        masks[a] = mk;
+      }
+      md_small(S.data(), k, masks, order);
+    } else {
+      std::vector<std::vector<int>> la(k);
+      for (int a = 0; a < k; ++a)
+        for (int p = xadj[S[a]]; p < xadj[S[a] + 1]; ++p)
+          if (mark[adjncy[p]] == sid) la[a].push_back(lidx[adjncy[p]]);
+      for (int a : amd_order(k, la)) order.push_back(S[a]);
+    }
   };
   while (!stack.empty()) {
     Task t = std::move(stack.back());
@@ -193,64 +275,46 @@ std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
       continue;
     }
     const int sid = ++stamp;
-    for (int v : S) {
-      mark[v] = sid;
-      level[v] = -1;
-    }
-    // connected components: dissect each on its own
-    int cnt = 0;
-    bfs(S[0], sid, cnt);
-    if (cnt < (int)S.size()) {
-      for (int i = 0; i < cnt; ++i) level[queue[i]] = -1;
+    for (int v : S) mark[v] = sid;
+    clear_levels(0);
+    clear_levels(1);
+    // connected components (dissect each on its own); the first search also
+    // gives every vertex's degree inside the set
+    bfs(S[0], sid, 0);
+    if (cnt_buf[0] < (int)S.size()) {
       std::vector<std::vector<int>> comps;
-      int comp_id = ++stamp;  // vertices already assigned get mark comp_id
+      const int comp_id = ++stamp;  // vertices already assigned get mark comp_id
       for (int v : S) {
         if (mark[v] == comp_id) continue;
-        int c = 0;
-        // restrict the BFS to unassigned vertices of S
-        bfs(v, sid, c);
-        comps.emplace_back(queue.begin(), queue.begin() + c);
-        for (int i = 0; i < c; ++i) {
-          mark[queue[i]] = comp_id;
-          level[queue[i]] = -1;
-        }
+        bfs(v, sid, 1);
+        comps.emplace_back(queue_buf[1].begin(), queue_buf[1].begin() + cnt_buf[1]);
+        for (int u : comps.back()) mark[u] = comp_id;
       }
-      for (auto it = comps.rbegin(); it != comps.rend(); ++it) stack.push_back({std::move(*it), false});
+      clear_levels(0);
+      clear_levels(1);
+      for (auto it = comps.rbegin(); it != comps.rend(); ++it)
+        stack.push_back({std::move(*it), false});
       continue;
     }
-    // pseudo-peripheral root
-    int root = S[0], best = INT32_MAX;
-    for (int v : S) {
-      int d = deg_in(v, sid);
-      if (d < best) {
-        best = d;
-        root = v;
-      }
+    // pseudo-peripheral root: a vertex of least degree in the set, then a
+    // least-degree vertex of the deepest level while that deepens the
+    // structure (three moves at most)
+    int root = S[0];
+    for (int v : S)
+      if (indeg[v] < indeg[root]) root = v;
+    int cur = 0;
+    int depth = bfs(root, sid, cur);
+    for (int it = 0; it < 3; ++it) {
+      const std::vector<int> &lv = level_buf[cur], &qu = queue_buf[cur];
+      int cand = -1;
+      for (int i = cnt_buf[cur] - 1; i >= 0 && lv[qu[i]] == depth - 1; --i)
+        if (cand < 0 || indeg[qu[i]] < indeg[cand]) cand = qu[i];
+      const int d2 = bfs(cand, sid, 1 - cur);
+      if (d2 <= depth) break;
+      depth = d2;
+      cur = 1 - cur;
     }
-    int depth = bfs(root, sid, cnt);
-    for (int it = 0; it < 5; ++it) {
-      int cand = -1, cd = INT32_MAX;
-      for (int i = 0; i < cnt; ++i) {
-        int v = queue[i];
-        if (level[v] == depth - 1) {
-          int d = deg_in(v, sid);
-          if (d < cd) {
-            cd = d;
-            cand = v;
-          }
-        }
-      }
-      int c2 = cnt;  // the set is connected: every call visits all of it
-      int d2 = bfs(cand, sid, c2);
-      if (d2 > depth) {
-        depth = d2;
-        root = cand;
-        cnt = c2;
-      } else {
-        bfs(root, sid, cnt);  // restore the levels of the deeper structure
-        break;
-      }
-    }
+    const std::vector<int> &level = level_buf[cur];
     if (depth < 3) {
       md_leaf(S);
       continue;
@@ -268,6 +332,8 @@ std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
     Task A, B, sep;
     A.emit = B.emit = false;
     sep.emit = true;
+    A.v.reserve(S.size());
+    B.v.reserve(S.size());
     for (int v : S) {
       const int lv = level[v];
       if (lv < ell) {
@@ -277,13 +343,12 @@ std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
       } else {
         bool touches_next = false;
         for (int p = xadj[v]; p < xadj[v + 1] && !touches_next; ++p) {
-          int u = adjncy[p];
+          const int u = adjncy[p];
           touches_next = mark[u] == sid && level[u] == ell + 1;
         }
         (touches_next ? sep.v : A.v).push_back(v);
       }
     }
-    for (int v : S) level[v] = -1;
     stack.push_back(std::move(sep));
     if (!B.v.empty()) stack.push_back(std::move(B));
     if (!A.v.empty()) stack.push_back(std::move(A));
@@ -563,45 +628,71 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
       ents.push_back({pc + 1, pc + 1, 0.0});
     }
   }
-  // ---- ordering
+  // ---- ordering (graph of the off-diagonal pattern, CSR with repeats)
   {
-    std::vector<std::vector<int>> adj(N);
+    std::vector<int> xadj(N + 1, 0);
     for (auto &en : ents)
       if (en.r != en.c) {
-        adj[en.r].push_back(en.c);
-        adj[en.c].push_back(en.r);
+        xadj[en.r + 1]++;
+        xadj[en.c + 1]++;
       }
-    out.perm = nd_order(N, adj);
+    for (int i = 0; i < N; ++i) xadj[i + 1] += xadj[i];
+    std::vector<int> adjncy(xadj[N]), cur(xadj.begin(), xadj.end() - 1);
+    for (auto &en : ents)
+      if (en.r != en.c) {
+        adjncy[cur[en.r]++] = en.c;
+        adjncy[cur[en.c]++] = en.r;
+      }
+    out.perm = nd_order_csr(N, xadj, adjncy);
   }
   out.iperm.assign(N, 0);
   for (int k = 0; k < N; ++k) out.iperm[out.perm[k]] = k;
   // ---- permuted full CSR (sorted columns, duplicates summed)
-  std::vector<std::vector<std::pair<int, double>>> rowsv(N);
-  for (auto &en : ents) {
-    int a = out.iperm[en.r], bb = out.iperm[en.c];
-    rowsv[a].push_back({bb, en.v});
-    if (a != bb) rowsv[bb].push_back({a, en.v});
-  }
-  out.Kp.assign(N + 1, 0);
-  out.Kdiag.assign(N, -1);
-  for (int r = 0; r < N; ++r) {
-    auto &rv = rowsv[r];
-    std::sort(rv.begin(), rv.end(),
-              [](const std::pair<int, double> &x, const std::pair<int, double> &y) {
-                return x.first < y.first;
-              });
-    int start = (int)out.Kj.size();
-    for (size_t t = 0; t < rv.size(); ++t) {
-      if (!out.Kj.empty() && (int)out.Kj.size() > start && out.Kj.back() == rv[t].first) {
-        out.Kx.back() += rv[t].second;
-        continue;
-      }
-      out.Kj.push_back(rv[t].first);
-      out.Kx.push_back(rv[t].second);
-      if (rv[t].first == r) out.Kdiag[r] = (int)out.Kj.size() - 1;
+  {
+    std::vector<int> rs(N + 1, 0);
+    for (auto &en : ents) {
+      const int a = out.iperm[en.r], bb = out.iperm[en.c];
+      rs[a + 1]++;
+      if (a != bb) rs[bb + 1]++;
     }
-    out.Kp[r + 1] = (int)out.Kj.size();
-    std::vector<std::pair<int, double>>().swap(rv);
+    for (int r = 0; r < N; ++r) rs[r + 1] += rs[r];
+    std::vector<std::pair<int, double>> rv(rs[N]);
+    {
+      std::vector<int> cur(rs.begin(), rs.end() - 1);
+      for (auto &en : ents) {
+        const int a = out.iperm[en.r], bb = out.iperm[en.c];
+        rv[cur[a]++] = {bb, en.v};
+        if (a != bb) rv[cur[bb]++] = {a, en.v};
+      }
+    }
+    out.Kp.assign(N + 1, 0);
+    out.Kdiag.assign(N, -1);
+    out.Kj.reserve(rs[N]);
+    out.Kx.reserve(rs[N]);
+    for (int r = 0; r < N; ++r) {
+      auto *b0 = rv.data() + rs[r], *b1 = rv.data() + rs[r + 1];
+      // rows are short: insertion sort by column (stable)
+      for (auto *x = b0 + 1; x < b1; ++x) {
+        auto v = *x;
+        auto *y = x;
+        while (y > b0 && (y - 1)->first > v.first) {
+          *y = *(y - 1);
+          --y;
+        }
+        *y = v;
+      }
+      const int start = (int)out.Kj.size();
+      for (auto *x = b0; x < b1; ++x) {
+        if ((int)out.Kj.size() > start && out.Kj.back() == x->first) {
+          out.Kx.back() += x->second;
+          continue;
+        }
+        out.Kj.push_back(x->first);
+        out.Kx.push_back(x->second);
+        if (x->first == r) out.Kdiag[r] = (int)out.Kj.size() - 1;
+      }
+      out.Kp[r + 1] = (int)out.Kj.size();
+    }
   }
   auto pos_of = [&](int lr, int lc) -> int {  // local unpermuted (lr, lc)
     int a = out.iperm[lr], bb = out.iperm[lc];

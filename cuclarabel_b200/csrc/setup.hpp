@@ -74,5 +74,8 @@ std::vector<int> amd_order(int n, std::vector<std::vector<int>> &adj);
 // nested-dissection ordering (minimum degree on the small parts); same
 // contract as amd_order
 std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj);
+// the same on a CSR graph (repeated neighbours allowed; rows are sorted and
+// deduplicated in place)
+std::vector<int> nd_order_csr(int n, std::vector<int> &xadj, std::vector<int> &adjncy);
 
 }  // namespace clgpu

@@ -148,6 +148,12 @@ int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
  * counterpart (the reference times host phases with TimerOutputs). */
 int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms,
                                  long long *calls);
+/* algorithmic bytes of the last profiled solve: bytes[0] all LDL
+ * factorisations, bytes[1] all LDL solves with refinement (each stream pass
+ * reads its entries, values and chunk words once; vectors once per use).
+ * Divided by the phase times this gives the achieved bandwidth.  No
+ * reference counterpart. */
+int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes);
 int clgpu_solver_destroy(clgpu_solver *h);
 
 /* --------------------------------------------------------------- cones */
