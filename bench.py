@@ -16,6 +16,7 @@ collective on the data path; NCCL only for the barrier and the max-time
 reduction).
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -119,22 +120,28 @@ def problem_bytes(pbs):
 
 
 def _ref_worker(w, nworkers, count, conn):
-    """One CPU worker: owns instances w, w + nworkers, ... of the workload,
-    generates them once, then solves its slice with the oracle each time the
-    parent says go; reports (solved, seconds)."""
+    """One CPU worker: owns instances w, w + nworkers, ... of the workload and
+    sets each up once (Solver(...): equilibration, KKT assembly, ordering,
+    symbolic factorisation).  On "go" it runs solve! on its slice; on "cold"
+    it solves its slice from scratch (setup included).  Reports (solved,
+    seconds)."""
     os.environ["OMP_NUM_THREADS"] = "1"
     sys.path.insert(0, ROOT)
     import oracle
     from cuclarabel_b200 import problems
     mine = [problems.mpc_qp(i) for i in range(w, count, nworkers)]
+    objs = [oracle.SolverObject(*pb, gpu_equilibration=1) for pb in mine]
     conn.send("ready")
     while True:
         msg = conn.recv()
-        if msg != "go":
+        if msg not in ("go", "cold"):
             break
         t0 = time.perf_counter()
-        solved = sum(1 for pb in mine
-                     if oracle.solve(*pb, gpu_equilibration=1)["status_name"] == "SOLVED")
+        if msg == "go":
+            solved = sum(1 for o in objs if o.run()["status_name"] == "SOLVED")
+        else:
+            solved = sum(1 for pb in mine
+                         if oracle.solve(*pb, gpu_equilibration=1)["status_name"] == "SOLVED")
         conn.send((solved, time.perf_counter() - t0))
 
 
@@ -159,10 +166,10 @@ class RefPool:
         for c in self.conns:
             assert c.recv() == "ready"
 
-    def step(self):
+    def step(self, cold=False):
         t0 = time.perf_counter()
         for c in self.conns:
-            c.send("go")
+            c.send("cold" if cold else "go")
         solved = 0
         for c in self.conns:
             s, _ = c.recv()
@@ -190,6 +197,7 @@ def run_reference(args, rank, world):
         if step >= args.warmup:
             times.append(dt)
             solved += s
+    cold_solved, cold_dt = pool.step(cold=True)
     pool.close()
     total = sum(times)
     val = solved / total
@@ -199,25 +207,34 @@ def run_reference(args, rank, world):
         "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded PCG64, MPC batch shapes)",
-        "config": workload_config(B, "reference CPU path (oracle port)"),
+        "config": workload_config(B, args.method),
         "cpu_baseline": {"value": val, "unit": "solves/s", "cores": pool.cores, "kind": "port",
-                         "sample": "the full %d-instance workload per step, one process per "
+                         "sample": "the full %d-instance workload per step: solve! of every "
+                                   "instance on solvers set up beforehand, one process per "
                                    "core, each owning a fixed slice" % B},
         "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "cold": {"value": cold_solved / cold_dt, "unit": "solves/s",
+                 "note": "one pass with setup included (Solver(...) + solve! per instance)"},
     }
     print(json.dumps(line), flush=True)
 
 
 def cpu_baseline_sample(count):
-    """One step of the CPU reference path over `count` instances (the GPU
-    arm's cpu_baseline field; ~5 ms of CPU per instance)."""
+    """The CPU reference path over `count` instances (the GPU arm's
+    cpu_baseline field): solve! on solvers set up beforehand, three passes
+    (~2 ms of CPU per instance and pass)."""
     pool = RefPool(count)
-    solved, dt = pool.step()
+    solved, dt = 0, 0.0
+    for _ in range(3):
+        s_, d_ = pool.step()
+        solved += s_
+        dt += d_
     pool.close()
     return {"value": solved / dt, "unit": "solves/s", "cores": pool.cores, "kind": "port",
-            "sample": "%d MPC QP/SOCP instances (the workload's first %d), one process per "
-                      "core, %.1f s wall" % (count, count, dt)}
+            "sample": "%d MPC QP/SOCP instances (the workload's first %d) x 3 passes of solve! "
+                      "on solvers set up beforehand, one process per core, %.1f s wall"
+                      % (count, count, dt)}
 
 
 METRIC = "solves/s at 1e-8 (batched MPC QP/SOCP)"
@@ -269,7 +286,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from cuclarabel_b200 import BatchSolver, Solver, SolverStatus
+    from cuclarabel_b200 import BatchSolver, Solver, SolverStatus, _lib
 
     B = args.instances
     seed0 = rank * B
@@ -305,11 +322,13 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        sols = solver.solve(sh)
+        solver.solve_only(sh)
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1) / 1000.0)
-        solved_total += sum(1 for s in sols if s.status == SolverStatus.SOLVED)
+        res = solver.results()
+        solved_total += int(np.sum(res["status"] == int(SolverStatus.SOLVED)))
+    sols = solver.solutions()
     clocks = sampler.stop()
     elapsed = sum(times)
     if dist:
@@ -327,26 +346,63 @@ def main():
         status_counts[s.status.name] = status_counts.get(s.status.name, 0) + 1
     iters = [s.iterations for s in sols]
 
-    # ---- e2e through the public API (host data -> device -> host)
-    e2e_steps = max(1, min(args.steps, 3))
+    # ---- e2e through the public API with host buffers: every step copies the
+    # whole batch's problem values from pinned host memory (update_data!,
+    # the reference's data-update path on solvers set up beforehand), solves,
+    # and reads every solution and info record back to the host
+    from cuclarabel_b200.api import _as_csc
+    Pv = np.concatenate([_as_csc(pb[0], pb[0].shape).data for pb in pbs])
+    Av = np.concatenate([_as_csc(pb[2], pb[2].shape).data for pb in pbs])
+    qv = np.concatenate([np.asarray(pb[1], np.float64) for pb in pbs])
+    bv = np.concatenate([np.asarray(pb[3], np.float64) for pb in pbs])
+    pinned = []
+    for v in (Pv, qv, Av, bv):
+        t = torch.empty(len(v), dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = v
+        pinned.append(t)
+    Pp_, qp_, Ap_, bp_ = [t.numpy() for t in pinned]
+    s2 = BatchSolver(pbs, direct_solve_method=args.method)  # setup outside the timed region
+    for _ in range(2):
+        s2.update_data(P=Pp_, q=qp_, A=Ap_, b=bp_, stream=sh)
+        s2.solve_only(sh)
+        s2.results()
+    e2e_steps = max(1, args.steps)
     e2e_t = 0.0
     e2e_solved = 0
     for _ in range(e2e_steps):
+        flush_l2()
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        s2 = BatchSolver(pbs, direct_solve_method=args.method)
-        out = s2.solve(sh)
-        torch.cuda.synchronize()
+        s2.update_data(P=Pp_, q=qp_, A=Ap_, b=bp_, stream=sh)
+        s2.solve_only(sh)
+        res = s2.results()
         e2e_t += time.perf_counter() - t0
-        e2e_solved += sum(1 for s in out if s.status == SolverStatus.SOLVED)
-        del s2
-    h2d = problem_bytes(pbs)
-    d2h = sum((p[1].nbytes + 2 * p[3].nbytes) for p in pbs) + B * 136
+        e2e_solved += int(np.sum(res["status"] == int(SolverStatus.SOLVED)))
+    h2d = 8 * (len(Pv) + len(qv) + len(Av) + len(bv))
+    d2h = 8 * (s2.nx + 2 * s2.mz) + B * ctypes.sizeof(_lib.ClgpuInfo)
+    del s2
     e2e_val = e2e_solved / e2e_t
     if dist:
-        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = e2e_solved * world / t.item()
+        t = torch.tensor([e2e_t, float(e2e_solved)], device="cuda", dtype=torch.float64)
+        tm = t.clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ts = t.clone()
+        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+        e2e_val = ts[1].item() / tm[0].item()
+    # cold path for reference: Solver(...) setup from host CSC data + solve +
+    # solutions, one pass
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s3 = BatchSolver(pbs, direct_solve_method=args.method)
+    s3.solve_only(sh)
+    res3 = s3.results()
+    cold_t = time.perf_counter() - t0
+    cold = {"value": float(np.sum(res3["status"] == int(SolverStatus.SOLVED))) / cold_t,
+            "unit": "solves/s", "note": "one pass: Solver(...) setup from host CSC data "
+                                        "(equilibration, ordering, symbolic LDL) + solve!"}
+    del s3
 
     # ---- plain path: one instance at a time on the same GPU (FP64, B = 1)
     plain = None
@@ -411,7 +467,10 @@ def main():
                            device_bytes=dev_bytes),
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "note": "includes host setup (Ruiz, ordering, symbolic LDL)"},
+                    "note": "update_data! of every value (P, q, A, b) from pinned host "
+                            "memory + solve! + all solutions and infos to the host, per "
+                            "step; solvers set up beforehand, as on the reference arm"},
+            "e2e_cold": cold,
             "gpu_launches": launches_per_solve * args.steps,
             "roofline": roof,
             "roofline_other": {

@@ -74,7 +74,8 @@ class ClgpuProblem(ctypes.Structure):
 EXPORTED = [
     "clgpu_default_settings", "clgpu_solver_create", "clgpu_solver_solve",
     "clgpu_solver_get_info", "clgpu_solver_get_solution", "clgpu_solver_get_solutions",
-    "clgpu_solver_update_qb", "clgpu_solver_device_bytes", "clgpu_solver_launch_count",
+    "clgpu_solver_update_qb", "clgpu_solver_update_data", "clgpu_solver_device_bytes",
+    "clgpu_solver_launch_count",
     "clgpu_solver_set_profiling", "clgpu_solver_get_profile", "clgpu_solver_get_phase_times",
     "clgpu_solver_get_phase_bytes",
     "clgpu_solver_destroy",
@@ -96,6 +97,7 @@ def _declare(L):
     L.clgpu_solver_get_solution.argtypes = [c_void_p, c_int, dp, dp, dp]
     L.clgpu_solver_get_solutions.argtypes = [c_void_p, dp, dp, dp, ctypes.POINTER(ClgpuInfo)]
     L.clgpu_solver_update_qb.argtypes = [c_void_p, c_int, dp, dp]
+    L.clgpu_solver_update_data.argtypes = [c_void_p, dp, dp, dp, dp, c_void_p]
     L.clgpu_solver_device_bytes.argtypes = [c_void_p]
     L.clgpu_solver_device_bytes.restype = c_ll
     L.clgpu_solver_launch_count.argtypes = [c_void_p]

@@ -328,7 +328,8 @@ def _pack_batch(problems):
         field = {"ct": "cone_types", "cd": "cone_dims", "cp": "cone_params"}.get(f, f)
         arr[field] = np.uint64(flat.ctypes.data) + offs.astype(np.uint64)
     keep["arr"] = arr
-    return arr, keep, [(int(n), int(m)) for n, m, _ in nm]
+    counts = (len(keep["Px"]) - 1, len(keep["Ax"]) - 1)
+    return arr, keep, [(int(n), int(m)) for n, m, _ in nm], counts
 
 
 def _nvars(spec):
@@ -342,7 +343,7 @@ class BatchSolver:
     def __init__(self, problems, settings=None, **kwargs):
         self.settings = settings_from(settings, **kwargs)
         L = _lib.load()
-        arr, keep, self.dims = _pack_batch(problems)
+        arr, keep, self.dims, (self._np, self._na) = _pack_batch(problems)
         cs = self.settings.to_c()
         h = ctypes.c_void_p()
         rc = L.clgpu_solver_create(arr.ctypes.data_as(ctypes.POINTER(_lib.ClgpuProblem)),
@@ -362,12 +363,68 @@ class BatchSolver:
             destroy(h)
             self._h = None
 
+    def update_data(self, P=None, q=None, A=None, b=None, stream=0):
+        """update_data!(solver, P, q, A, b) for every instance
+        (src/data_updating.jl).  Each argument is a concatenated 1-D array of
+        new values -- for P and A the nonzeros in the CSC order given at setup,
+        instance by instance -- or a list with one entry per instance (sparse
+        matrices with the setup sparsity, or value arrays); None leaves that
+        part unchanged.  The equilibration computed at setup is reused, as in
+        the reference."""
+        def cat(v, kind):
+            if v is None:
+                return None
+            if isinstance(v, (list, tuple)):
+                parts = []
+                for k, x in enumerate(v):
+                    if kind in ("P", "A") and sp.issparse(x):
+                        x = _as_csc(x, x.shape).data
+                    parts.append(np.asarray(x, np.float64).ravel())
+                v = np.concatenate(parts) if parts else np.zeros(0)
+            return _f64(np.asarray(v, np.float64).ravel())
+        Pv, qv, Av, bv = cat(P, "P"), cat(q, "q"), cat(A, "A"), cat(b, "b")
+        for v, n, name in ((Pv, self._np, "P"), (qv, self.nx, "q"), (Av, self._na, "A"),
+                           (bv, self.mz, "b")):
+            if v is not None and len(v) != n:
+                raise ValueError("%s: expected %d values, got %d" % (name, n, len(v)))
+        ptr = lambda v: None if v is None else v.ctypes.data_as(_lib.dp)  # noqa: E731
+        rc = _lib.load().clgpu_solver_update_data(self._h, ptr(Pv), ptr(qv), ptr(Av), ptr(bv),
+                                                   ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_update_data failed with code %d" % rc)
+
+    def solve_only(self, stream=0):
+        """solve! without building per-instance solution objects (read the
+        results with results() or solutions())."""
+        rc = _lib.load().clgpu_solver_solve(self._h, ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_solve failed with code %d" % rc)
+
     def solve(self, stream=0):
         L = _lib.load()
         rc = L.clgpu_solver_solve(self._h, ctypes.c_void_p(stream))
         if rc != 0:
             raise RuntimeError("clgpu_solver_solve failed with code %d" % rc)
         return self.solutions()
+
+    def results(self):
+        """The last solve's results as arrays (no per-instance objects): x, s,
+        z concatenated over instances (offsets xoff / moff) and a structured
+        array of the DefaultInfo fields, one row per instance."""
+        L = _lib.load()
+        B = len(self.dims)
+        x = np.empty(max(self.nx, 1))
+        s = np.empty(max(self.mz, 1))
+        z = np.empty(max(self.mz, 1))
+        infos = (_lib.ClgpuInfo * B)()
+        rc = L.clgpu_solver_get_solutions(self._h, x.ctypes.data_as(_lib.dp),
+                                          s.ctypes.data_as(_lib.dp), z.ctypes.data_as(_lib.dp),
+                                          infos)
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_get_solutions failed with code %d" % rc)
+        info = np.ctypeslib.as_array(infos)
+        return {"x": x[:self.nx], "s": s[:self.mz], "z": z[:self.mz], "info": info,
+                "status": info["status"].copy()}
 
     def solutions(self):
         L = _lib.load()
@@ -433,6 +490,19 @@ class Solver(BatchSolver):
     def solve(self, stream=0):
         self.solution = super().solve(stream)[0]
         return self.solution
+
+    # update_P! / update_q! / update_A! / update_b! (src/data_updating.jl)
+    def update_P(self, P):
+        self.update_data(P=[P])
+
+    def update_q(self, q):
+        self.update_data(q=q)
+
+    def update_A(self, A):
+        self.update_data(A=[A])
+
+    def update_b(self, b):
+        self.update_data(b=b)
 
     @property
     def info(self):

@@ -379,6 +379,82 @@ __global__ void k_after_scaling(Dev d) {
   IF(d, I_KKT_OK, i) = 1;
 }
 
+// ======================================================== update_data!
+// New problem values scaled with the equilibration computed at setup (d, e,
+// c), as _update_matrix / _update_vector do (data_updating.jl:185-300), and
+// written into every device copy: the full P, A, A^T and the KKT matrix.
+__global__ void k_update_P(Dev d, const int4 *__restrict__ map, const int2 *__restrict__ xy,
+                           const double *__restrict__ in, long long n, const double *c,
+                           double *Kx) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int2 rc = xy[t];
+  if (rc.x < 0) return;  // below the diagonal: ignored, as at setup
+  const int4 m = map[t];
+  const double v = in[t] * d.d[rc.x] * d.d[rc.y] * c[d.col_inst[rc.x]];
+  double *Px = const_cast<double *>(d.Px);
+  if (m.x >= 0) Px[m.x] = v;
+  if (m.y >= 0) Px[m.y] = v;
+  if (m.z >= 0) Kx[m.z] = v;
+  if (m.w >= 0) Kx[m.w] = v;
+}
+__global__ void k_update_A(Dev d, const int4 *__restrict__ map, const int2 *__restrict__ xy,
+                           const double *__restrict__ in, long long n, double *Kx) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int4 m = map[t];
+  const int2 rc = xy[t];  // global row, global column
+  const double v = in[t] * d.e[rc.x] * d.d[rc.y];
+  const_cast<double *>(d.Atx)[m.x] = v;
+  const_cast<double *>(d.Ax)[m.y] = v;
+  if (m.z >= 0) Kx[m.z] = v;
+  if (m.w >= 0) Kx[m.w] = v;
+}
+__global__ void k_update_q(Dev d, const double *__restrict__ in, int lo, int hi,
+                           const double *c) {
+  const int j = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= hi) return;
+  const double v = in[j] * d.d[j] * c[d.col_inst[j]];
+  const_cast<double *>(d.q)[j] = v;
+  const_cast<double *>(d.negq)[j] = -v;
+}
+__global__ void k_update_b(Dev d, const double *__restrict__ in, int lo, int hi,
+                           const int *zmap) {
+  const int u = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= hi) return;
+  const int g = zmap[u];
+  const_cast<double *>(d.b)[g] = in[u] * d.e[g];
+}
+// unscaled infinity norms of the new q / b of instances [lo, hi) (the
+// reference flushes them on update and recomputes them in solve!)
+template <int NTH>
+__global__ void __launch_bounds__(NTH)
+    k_update_norms(const double *__restrict__ inq, const double *__restrict__ inb,
+                   const int *xoff, const int *moff, int lo, double *normq, double *normb) {
+  const int i = lo + blockIdx.x;
+  __shared__ double red[2][NTH / 32];
+  double mq = 0, mb = 0;
+  if (inq)
+    for (int j = xoff[i] + threadIdx.x; j < xoff[i + 1]; j += NTH) mq = fmax(mq, fabs(inq[j]));
+  if (inb)
+    for (int u = moff[i] + threadIdx.x; u < moff[i + 1]; u += NTH) mb = fmax(mb, fabs(inb[u]));
+  mq = warp_max(mq);
+  mb = warp_max(mb);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = mq;
+    red[1][threadIdx.x >> 5] = mb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < NTH / 32; ++w) {
+      mq = fmax(mq, red[0][w]);
+      mb = fmax(mb, red[1][w]);
+    }
+    if (inq) normq[i] = mq;
+    if (inb) normb[i] = mb;
+  }
+}
+
 // ============================================================ KKT glue
 // workz = dsc - rhs_z (kktsystem_gpu.jl:168)
 __global__ void k_workz(Dev d, const double *dsc) {
@@ -723,7 +799,7 @@ struct clgpu_solver {
   int *d_reset = nullptr;
   double *d_c = nullptr, *d_normq = nullptr, *d_normb = nullptr;
   int *d_pnnz = nullptr;
-  int *d_zmap = nullptr, *d_zinst = nullptr;
+  int *d_zmap = nullptr, *d_zinst = nullptr, *d_moff = nullptr;
   double *d_out = nullptr;  // nx + 2*mz
   int *h_counter = nullptr;  // pinned
   std::vector<int> h_n, h_m, h_xoff, h_moff;
@@ -744,6 +820,14 @@ struct clgpu_solver {
   int passes = 0;
   double last_ms = 0;
   double *d_prof_bytes = nullptr;  // [2B] algorithmic bytes (profiling)
+  // update_data!: maps from the caller's value arrays to the device copies,
+  // and staging buffers for the new values
+  bool upd_ok = false;
+  long long upd_np = 0, upd_na = 0;
+  std::vector<long long> h_pu_off;
+  int4 *d_upd_pmap = nullptr, *d_upd_amap = nullptr;
+  int2 *d_upd_pxy = nullptr, *d_upd_axy = nullptr;
+  double *d_in_P = nullptr, *d_in_A = nullptr, *d_in_q = nullptr, *d_in_b = nullptr;
   double prof_bytes[2] = {0, 0};   // factor, solve: sums of the last profiled solve
   ~clgpu_solver() {
     if (h_counter) cudaFreeHost(h_counter);
@@ -990,6 +1074,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   });
   // A rows (global, type-major order) from A^T, columns ascending per row
   for (int g = 0; g < mz; ++g) Ap[g + 1] = Ap[g] + arow_cnt[g];
+  hvec<int> acsr(aoffs[B]);  // A CSR position of every A^T (= caller CSC) entry
   {
     std::vector<int> next(Ap.begin(), Ap.end() - 1);
     par_for(B, nth, [&](int i) {  // an instance touches only its own rows
@@ -998,6 +1083,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
           const int qd = next[Atj[k]]++;
           Aj[qd] = j;
           Axv[qd] = Atxv[k];
+          acsr[k] = qd;
         }
     });
   }
@@ -1260,6 +1346,47 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       pe += tt;
     }
   });
+  // value-update maps (update_data!): global positions
+  {
+    std::vector<long long> pu(B);
+    bool upd = true;
+    for (int i = 0; i < B; ++i) {
+      pu[i] = prep[i].p_user_nnz;
+      upd = upd && prep[i].updatable;
+    }
+    const auto opu = prefix(pu);
+    hvec<int4> pmap(opu[B]), amap(aoffs[B]);
+    hvec<int2> pxy(opu[B]), axy(aoffs[B]);
+    par_for(B, nth, [&](int i) {
+      const auto &p = prep[i];
+      const int pb = (int)poffs[i], kb = (int)kof[i];
+      auto g = [](int v, int base) { return v < 0 ? -1 : v + base; };
+      for (long long t = 0; t < pu[i]; ++t) {
+        const int *m4 = p.pmap.data() + 4 * t;
+        pmap[opu[i] + t] = make_int4(g(m4[0], pb), g(m4[1], pb), g(m4[2], kb), g(m4[3], kb));
+        const int r = p.pxy[2 * t], c = p.pxy[2 * t + 1];
+        pxy[opu[i] + t] = r < 0 ? make_int2(-1, -1) : make_int2(xoff[i] + r, xoff[i] + c);
+      }
+      for (int j = 0; j < p.n; ++j)
+        for (int k = p.A.p[j]; k < p.A.p[j + 1]; ++k) {
+          const long long t = aoffs[i] + k;
+          amap[t] = make_int4((int)t, acsr[t], g(p.amapk[2 * k], kb), g(p.amapk[2 * k + 1], kb));
+          axy[t] = make_int2(Atj[t], xoff[i] + j);
+        }
+    });
+    h->upd_ok = upd;
+    h->upd_np = opu[B];
+    h->upd_na = aoffs[B];
+    h->h_pu_off.assign(opu.begin(), opu.end());
+    h->d_upd_pmap = A.upload(pmap);
+    h->d_upd_pxy = A.upload(pxy);
+    h->d_upd_amap = A.upload(amap);
+    h->d_upd_axy = A.upload(axy);
+    h->d_in_P = A.alloc<double>(std::max<long long>(opu[B], 1), false);
+    h->d_in_A = A.alloc<double>(std::max<long long>(aoffs[B], 1), false);
+    h->d_in_q = A.alloc<double>(std::max(nx, 1), false);
+    h->d_in_b = A.alloc<double>(std::max(mz, 1), false);
+  }
   mark("kkt concat + maps");
   KKTMapDev &mp = h->map;
   mp.nn_pos = A.upload(nn_pos);
@@ -1511,6 +1638,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       zinst[moff[i] + ur] = i;
     }
   h->d_zmap = A.upload(zmap);
+  h->d_moff = A.upload(moff);
   h->d_zinst = A.upload(zinst);
   h->d_out = A.alloc<double>((size_t)nx + 2 * (size_t)mz);
   h->h_n.resize(B);
@@ -1924,13 +2052,60 @@ extern "C" int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes
   bytes[1] = h->prof_bytes[1];
   return 0;
 }
+extern "C" int clgpu_solver_update_data(clgpu_solver *h, const double *Px, const double *q,
+                                        const double *Ax, const double *b,
+                                        clgpu_stream_t stream) {
+  if (!h) return -1;
+  if ((Px || Ax) && !h->upd_ok) return -11;  // repeated matrix entries at setup
+  cudaStream_t st = (cudaStream_t)stream;
+  Dev &dv = h->dv;
+  if (Px && h->upd_np > 0) {
+    cudaMemcpyAsync(h->d_in_P, Px, (size_t)h->upd_np * sizeof(double), cudaMemcpyHostToDevice,
+                    st);
+    k_update_P<<<nblk(h->upd_np), TB, 0, st>>>(dv, h->d_upd_pmap, h->d_upd_pxy, h->d_in_P,
+                                                h->upd_np, h->d_c, h->kk.Kx);
+  }
+  if (Ax && h->upd_na > 0) {
+    cudaMemcpyAsync(h->d_in_A, Ax, (size_t)h->upd_na * sizeof(double), cudaMemcpyHostToDevice,
+                    st);
+    k_update_A<<<nblk(h->upd_na), TB, 0, st>>>(dv, h->d_upd_amap, h->d_upd_axy, h->d_in_A,
+                                                h->upd_na, h->kk.Kx);
+  }
+  if (q && dv.nx > 0) {
+    cudaMemcpyAsync(h->d_in_q, q, (size_t)dv.nx * sizeof(double), cudaMemcpyHostToDevice, st);
+    k_update_q<<<nblk(dv.nx), TB, 0, st>>>(dv, h->d_in_q, 0, dv.nx, h->d_c);
+  }
+  if (b && dv.mz > 0) {
+    cudaMemcpyAsync(h->d_in_b, b, (size_t)dv.mz * sizeof(double), cudaMemcpyHostToDevice, st);
+    k_update_b<<<nblk(dv.mz), TB, 0, st>>>(dv, h->d_in_b, 0, dv.mz, h->d_zmap);
+  }
+  if (q || b)
+    k_update_norms<128><<<h->B, 128, 0, st>>>(q ? h->d_in_q : nullptr, b ? h->d_in_b : nullptr,
+                                              dv.xoff, h->d_moff, 0, h->d_normq, h->d_normb);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // caller buffers consumed
+  return e == cudaSuccess ? 0 : -1000 - (int)e;
+}
 extern "C" int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,
                                       const double *b) {
-  (void)h;
-  (void)inst;
-  (void)q;
-  (void)b;
-  return -10;  // not implemented yet
+  if (!h || inst < 0 || inst >= h->B) return -1;
+  Dev &dv = h->dv;
+  const int x0 = h->h_xoff[inst], x1 = h->h_xoff[inst + 1];
+  const int m0 = h->h_moff[inst], m1 = h->h_moff[inst + 1];
+  if (q && x1 > x0) {
+    cudaMemcpy(h->d_in_q + x0, q, (size_t)(x1 - x0) * sizeof(double), cudaMemcpyHostToDevice);
+    k_update_q<<<nblk(x1 - x0), TB>>>(dv, h->d_in_q, x0, x1, h->d_c);
+  }
+  if (b && m1 > m0) {
+    cudaMemcpy(h->d_in_b + m0, b, (size_t)(m1 - m0) * sizeof(double), cudaMemcpyHostToDevice);
+    k_update_b<<<nblk(m1 - m0), TB>>>(dv, h->d_in_b, m0, m1, h->d_zmap);
+  }
+  if (q || b)
+    k_update_norms<128><<<1, 128>>>(q ? h->d_in_q : nullptr, b ? h->d_in_b : nullptr, dv.xoff,
+                                    h->d_moff, inst, h->d_normq, h->d_normb);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? 0 : -1000 - (int)e;
 }
 extern "C" int clgpu_solver_destroy(clgpu_solver *h) {
   if (!h) return -1;

@@ -769,6 +769,40 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     std::vector<int> cur(out.lvl_ptr.begin(), out.lvl_ptr.end() - 1);
     for (int j = 0; j < N; ++j) out.lvl_nodes[cur[lev[j]]++] = j;
   }
+  // ---- value-update maps
+  {
+    const int pnz = pb.Pp[n];
+    out.p_user_nnz = pnz;
+    out.pmap.assign(4 * (size_t)pnz, -1);
+    out.pxy.assign(2 * (size_t)pnz, -1);
+    const HostCSC &F = out.Pfull;
+    auto fpos = [&](int r, int c) -> int {  // position of (r, c) in the full CSC
+      auto beg = F.i.begin() + F.p[c], end = F.i.begin() + F.p[c + 1];
+      auto it = std::lower_bound(beg, end, r);
+      return (it != end && *it == r) ? (int)(it - F.i.begin()) : -1;
+    };
+    for (int j = 0; j < n; ++j)
+      for (int k = pb.Pp[j]; k < pb.Pp[j + 1]; ++k) {
+        const int i = pb.Pi[k];
+        if (i > j) continue;
+        if (k > pb.Pp[j] && pb.Pi[k - 1] >= i) out.updatable = false;  // repeats / unsorted
+        out.pmap[4 * (size_t)k] = fpos(i, j);
+        out.pmap[4 * (size_t)k + 1] = i != j ? fpos(j, i) : -1;
+        out.pmap[4 * (size_t)k + 2] = pos_of(i, j);
+        out.pmap[4 * (size_t)k + 3] = i != j ? pos_of(j, i) : -1;
+        out.pxy[2 * (size_t)k] = i;
+        out.pxy[2 * (size_t)k + 1] = j;
+      }
+    const int anz = A.p[n];
+    out.amapk.assign(2 * (size_t)anz, -1);
+    for (int j = 0; j < n; ++j)
+      for (int k = A.p[j]; k < A.p[j + 1]; ++k) {
+        if (k > A.p[j] && A.i[k - 1] >= A.i[k]) out.updatable = false;
+        const int zr = n + local_of_user[A.i[k]];
+        out.amapk[2 * (size_t)k] = pos_of(j, zr);
+        out.amapk[2 * (size_t)k + 1] = pos_of(zr, j);
+      }
+  }
   // ---- refresh positions
   for (size_t c = 0; c < out.ctype.size(); ++c) {
     int t = out.ctype[c], st = n + out.cstart[c];

@@ -55,6 +55,17 @@ struct Prepared {
   std::vector<int> socs_D;                   // per SOC cone 2 (or -1)
   std::vector<int> exp_pos, pow_pos;         // 12 per cone
   std::vector<int> psd_pos, psd_start;       // pairs per triu entry, start per cone
+  // value updates (update_data!): for every entry of the caller's P (CSC
+  // order, entries below the diagonal included and ignored), the positions
+  // of the value in the full symmetric P (two for off-diagonals, else -1) and
+  // in the KKT matrix (two / one, -1 when ignored); for every entry of A its
+  // two KKT positions.  updatable is false when the caller's matrices held
+  // repeated entries (their values were summed at setup).
+  std::vector<int> pmap;   // 4 per caller P entry: pfull1, pfull2, kkt1, kkt2
+  std::vector<int> pxy;    // 2 per caller P entry: local (row, col), -1 if ignored
+  std::vector<int> amapk;  // 2 per A entry: kkt1, kkt2
+  int p_user_nnz = 0;
+  bool updatable = true;
   // for gathering rhs / scattering solution: permuted k -> local original idx
   // (0..n-1 x, n..n+m-1 z type-major local row, >= n+m extra)
 };

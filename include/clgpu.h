@@ -126,8 +126,19 @@ int clgpu_solver_get_solution(clgpu_solver *h, int inst, double *x, double *s,
  * info array of nprob entries; any pointer may be NULL */
 int clgpu_solver_get_solutions(clgpu_solver *h, double *x, double *s,
                                double *z, clgpu_info *info);
-/* replace q and b of one instance (same sizes) before the next solve;
- * the equilibration computed at setup is reused (src/data_updating.jl) */
+/* update_data! for every instance (src/data_updating.jl:26-120): new values
+ * with the sparsity given at setup, concatenated over the instances in
+ * instance order, HOST pointers -- Px: the entries of each instance's P in
+ * the CSC order given at setup (entries below the diagonal are read and
+ * ignored), q, Ax: A's entries in CSC order, b: rows in the caller's order.
+ * A NULL pointer leaves that part unchanged.  The equilibration computed at
+ * setup is reused, as in the reference; the unscaled norms of q and b are
+ * recomputed.  Returns after the values are on the device; -11 when the
+ * setup matrices held repeated entries (their values were summed). */
+int clgpu_solver_update_data(clgpu_solver *h, const double *Px, const double *q,
+                             const double *Ax, const double *b, clgpu_stream_t st);
+/* update_q! / update_b! of one instance (same sizes) before the next solve
+ * (src/data_updating.jl:155-185); NULL leaves that vector unchanged */
 int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,
                            const double *b);
 /* device-memory footprint of the handle in bytes */

@@ -101,6 +101,13 @@ def lib():
             ctypes.c_int, ip, ip, dp, ctypes.POINTER(OracleSettings), dp, dp,
             dp, ctypes.POINTER(OracleInfo)]
         L.oracle_solve.restype = ctypes.c_int
+        L.oracle_solver_create.argtypes = [
+            ctypes.c_int, ctypes.c_int, ip, ip, dp, dp, ip, ip, dp, dp,
+            ctypes.c_int, ip, ip, dp, ctypes.POINTER(OracleSettings)]
+        L.oracle_solver_create.restype = vp
+        L.oracle_solver_run.argtypes = [vp, dp, dp, dp, ctypes.POINTER(OracleInfo)]
+        L.oracle_solver_run.restype = ctypes.c_int
+        L.oracle_solver_destroy.argtypes = [vp]
         L.oracle_cones_create.argtypes = [ctypes.c_int, ip, ip, dp]
         L.oracle_cones_create.restype = vp
         L.oracle_cones_destroy.argtypes = [vp]
@@ -150,6 +157,56 @@ def default_settings(**kw):
     for k, v in kw.items():
         setattr(st, k, v)
     return st
+
+
+def _arrays(P, q, A, b, cones):
+    n = len(q)
+    m = len(b)
+    P = sp.csc_matrix(P, shape=(n, n))
+    P = sp.triu(P, format="csc")
+    P.sort_indices()
+    A = sp.csc_matrix(A, shape=(m, n))
+    A.sort_indices()
+    t, d, p = cone_arrays(cones)
+    return (n, m, np.ascontiguousarray(P.indptr, np.int32),
+            np.ascontiguousarray(P.indices, np.int32), np.ascontiguousarray(P.data, np.float64),
+            np.ascontiguousarray(q, np.float64), np.ascontiguousarray(A.indptr, np.int32),
+            np.ascontiguousarray(A.indices, np.int32), np.ascontiguousarray(A.data, np.float64),
+            np.ascontiguousarray(b, np.float64), t, d, p)
+
+
+class SolverObject:
+    """Setup once, solve repeatedly (Solver(...) then solve!, the CPU path of
+    src/solver.jl); each run starts from the default initial point."""
+
+    def __init__(self, P, q, A, b, cones, **settings):
+        self._a = _arrays(P, q, A, b, cones)
+        n, m, Pp, Pi, Px, q, Ap, Ai, Ax, b, t, d, p = self._a
+        self.n, self.m = n, m
+        st = default_settings(**settings)
+        self.h = lib().oracle_solver_create(n, m, _ip(Pp), _ip(Pi), _dp(Px), _dp(q), _ip(Ap),
+                                            _ip(Ai), _dp(Ax), _dp(b), len(t), _ip(t), _ip(d),
+                                            _dp(p), ctypes.byref(st))
+        if not self.h:
+            raise RuntimeError("oracle_solver_create failed")
+        self._x, self._s, self._z = np.zeros(n), np.zeros(m), np.zeros(m)
+
+    def run(self):
+        info = OracleInfo()
+        rc = lib().oracle_solver_run(self.h, _dp(self._x), _dp(self._s), _dp(self._z),
+                                     ctypes.byref(info))
+        if rc != 0:
+            raise RuntimeError("oracle_solver_run failed with code %d" % rc)
+        out = {f: getattr(info, f) for f, _ in OracleInfo._fields_}
+        out.update(x=self._x.copy(), s=self._s.copy(), z=self._z.copy(),
+                   status_name=STATUS_NAMES[info.status])
+        return out
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().oracle_solver_destroy(h)
+            self.h = None
 
 
 def solve(P, q, A, b, cones, **settings):

@@ -101,6 +101,19 @@ int oracle_solve(int n, int m, const int *Pp, const int *Pi, const double *Px,
                  const double *cone_params, const oracle_settings *settings,
                  double *x, double *s, double *z, oracle_info *info);
 
+/* Solver object: setup once (equilibration, KKT assembly, ordering,
+ * symbolic factorisation), then run the interior-point solve any number of
+ * times, each from the default start (src/solver.jl:5-17, :231-422). */
+typedef struct oracle_solver oracle_solver;
+oracle_solver *oracle_solver_create(int n, int m, const int *Pp, const int *Pi,
+                                    const double *Px, const double *q, const int *Ap,
+                                    const int *Ai, const double *Ax, const double *b,
+                                    int ncones, const int *cone_types, const int *cone_dims,
+                                    const double *cone_params,
+                                    const oracle_settings *settings);
+int oracle_solver_run(oracle_solver *h, double *x, double *s, double *z, oracle_info *info);
+void oracle_solver_destroy(oracle_solver *h);
+
 /* ---- per-cone-operation entry points for kernel-level parity tests ---- */
 typedef struct oracle_cones oracle_cones;
 oracle_cones *oracle_cones_create(int ncones, const int *types,

@@ -677,6 +677,11 @@ struct Solver {
     int iter = 0;
     double sigma = 1.0, alpha = 0.0, mu = kMax;
     t0 = std::chrono::steady_clock::now();
+    // a solver object may be solved repeatedly (solve! after setup!): every
+    // piece of per-solve state starts afresh
+    info = oracle_info{};
+    prev_cost_primal = prev_cost_dual = prev_res_primal = prev_res_dual = kInf;
+    prev_gap_abs = prev_gap_rel = kInf;
     info.status = 0;
     default_start();
     int scaling = cones.allows_primal_dual_scaling() ? PrimalDual : Dual;
@@ -918,6 +923,49 @@ int oracle_solve(int n, int m, const int *Pp, const int *Pi, const double *Px,
   }
   return 0;
 }
+
+// Solver(P,q,A,b,cones,settings) once, then solve! any number of times
+// (src/solver.jl:5-17 and :231-422): setup work (equilibration, KKT
+// assembly, ordering, symbolic factorisation) stays outside the solves.
+struct oracle_solver {
+  Solver S;
+};
+
+oracle_solver *oracle_solver_create(int n, int m, const int *Pp, const int *Pi,
+                                    const double *Px, const double *q, const int *Ap,
+                                    const int *Ai, const double *Ax, const double *b,
+                                    int ncones, const int *cone_types, const int *cone_dims,
+                                    const double *cone_params,
+                                    const oracle_settings *settings) {
+  if (n < 0 || m < 0) return nullptr;
+  auto *h = new oracle_solver;
+  try {
+    if (settings)
+      h->S.st = *settings;
+    else
+      oracle_default_settings(&h->S.st);
+    h->S.setup(n, m, Pp, Pi, Px, q, Ap, Ai, Ax, b, ncones, cone_types, cone_dims,
+               cone_params);
+  } catch (std::exception &e) {
+    std::fprintf(stderr, "oracle_solver_create: %s\n", e.what());
+    delete h;
+    return nullptr;
+  }
+  return h;
+}
+int oracle_solver_run(oracle_solver *h, double *x, double *s, double *z, oracle_info *info) {
+  if (!h) return -1;
+  try {
+    h->S.solve_loop();
+    h->S.finish(x, s, z);
+    *info = h->S.info;
+  } catch (std::exception &e) {
+    std::fprintf(stderr, "oracle_solver_run: %s\n", e.what());
+    return -2;
+  }
+  return 0;
+}
+void oracle_solver_destroy(oracle_solver *h) { delete h; }
 
 struct oracle_cones {
   CompositeCone C;

@@ -1,0 +1,110 @@
+"""update_data! / update_q! / update_b! on the device (src/data_updating.jl):
+new values with the setup sparsity, scaled with the setup equilibration.
+
+A re-solve after an update must agree with a fresh CPU-oracle solve of the
+updated problem: same status and objective to 1e-6 relative (the two runs
+equilibrate differently -- the reference keeps the setup scaling on update --
+so their iterates differ while the optimum does not)."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle
+from cuclarabel_b200 import BatchSolver, Solver, SolverStatus, problems
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _perturb(pb, rng, scale_p=1.0, noise_a=0.0):
+    P, q, A, b, cones = pb
+    q2 = q + 0.1 * rng.standard_normal(len(q))
+    b2 = b.copy()
+    b2 += 0.05 * np.abs(rng.standard_normal(len(b)))  # keeps the interior point feasible
+    P2 = (P * scale_p).tocsc()
+    A2 = A.copy().tocsc()
+    if noise_a:
+        A2.data = A2.data * (1 + noise_a * rng.standard_normal(A2.nnz))
+    return P2, q2, A2, b2, cones
+
+
+def test_update_with_same_data_reproduces_the_solve(cuda_device):
+    """Re-scaling the same values with the final equilibration (one product
+    d_i d_j c) rounds differently from the setup's ten in-place Ruiz sweeps,
+    so the re-solve matches to rounding, not bitwise."""
+    pbs = problems.mpc_batch(24, seed0=500)
+    s = BatchSolver(pbs)
+    a = s.solve()
+    s.update_data(P=[pb[0] for pb in pbs], q=[pb[1] for pb in pbs], A=[pb[2] for pb in pbs],
+                  b=[pb[3] for pb in pbs])
+    c = s.solve()
+    near = {"SOLVED", "ALMOST_SOLVED"}
+    for k, (x, y) in enumerate(zip(a, c)):
+        assert x.status == y.status or {x.status.name, y.status.name} <= near, k
+        assert abs(x.iterations - y.iterations) <= 2, k
+        if x.status == y.status == SolverStatus.SOLVED:
+            assert rel_err(x.obj_val, y.obj_val) < 1e-9, k
+            assert np.linalg.norm(x.x - y.x) <= 1e-5 * max(1.0, np.linalg.norm(x.x)), k
+
+
+def test_update_q_b_matches_fresh_oracle(cuda_device):
+    rng = np.random.default_rng(7)
+    pbs = problems.mpc_batch(24, seed0=600)
+    s = BatchSolver(pbs)
+    s.solve()
+    new = [_perturb(pb, rng) for pb in pbs]
+    s.update_data(q=np.concatenate([p[1] for p in new]), b=np.concatenate([p[3] for p in new]))
+    sols = s.solve()
+    n_ok = 0
+    for k, (pb, sol) in enumerate(zip(new, sols)):
+        ref = oracle.solve(*pb, gpu_equilibration=1)
+        if ref["status_name"] != "SOLVED":
+            continue
+        n_ok += 1
+        assert sol.status.name in ("SOLVED", "ALMOST_SOLVED"), (k, sol.status)
+        assert rel_err(sol.obj_val, ref["obj_val"]) < 1e-6, (k, sol.obj_val, ref["obj_val"])
+    assert n_ok >= 20
+
+
+def test_update_P_A_matches_fresh_oracle(cuda_device):
+    rng = np.random.default_rng(8)
+    pbs = problems.mpc_batch(16, seed0=700)
+    s = BatchSolver(pbs)
+    s.solve()
+    new = [_perturb(pb, rng, scale_p=1.3, noise_a=0.05) for pb in pbs]
+    s.update_data(P=[p[0] for p in new], q=[p[1] for p in new], A=[p[2] for p in new],
+                  b=[p[3] for p in new])
+    sols = s.solve()
+    n_ok = 0
+    for k, (pb, sol) in enumerate(zip(new, sols)):
+        ref = oracle.solve(*pb, gpu_equilibration=1)
+        if ref["status_name"] != "SOLVED":
+            continue
+        n_ok += 1
+        assert sol.status.name in ("SOLVED", "ALMOST_SOLVED"), (k, sol.status)
+        assert rel_err(sol.obj_val, ref["obj_val"]) < 1e-6, (k, sol.obj_val, ref["obj_val"])
+    assert n_ok >= 12
+
+
+def test_single_instance_update_q_b(cuda_device):
+    rng = np.random.default_rng(9)
+    pb = problems.portfolio(seed=1)
+    s = Solver(*pb)
+    s.solve()
+    P, q, A, b, cones = pb
+    q2 = q * (1 + 0.2 * rng.standard_normal(len(q)))
+    s.update_q(q2)
+    s.update_b(b)
+    sol = s.solve()
+    ref = oracle.solve(P, q2, A, b, cones, gpu_equilibration=1)
+    assert sol.status.name == ref["status_name"] == "SOLVED"
+    assert rel_err(sol.obj_val, ref["obj_val"]) < 1e-6
+
+
+def test_update_rejects_wrong_lengths(cuda_device):
+    pbs = problems.mpc_batch(2, seed0=800)
+    s = BatchSolver(pbs)
+    with pytest.raises(ValueError):
+        s.update_data(q=np.zeros(3))
+    with pytest.raises(ValueError):
+        s.update_data(A=np.zeros(5))
