@@ -14,6 +14,7 @@
 // (new scaling strategy) sets its skip flag and sits out the rest of the pass;
 // an instance that would "break" sets done and is frozen.  All vector kernels
 // read the per-instance active mask.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -1529,6 +1530,123 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     const int klev[2] = {(int)kbase, (int)(kbase + prep[i].Kj.size())};
     put(kch.data() + okch[i], klev, 1, kbase);
   });
+  // streamed factorisation: op streams, pivots and chunk tables
+  {
+    constexpr long long kFactorSmemBytes = 96 * 1024;
+    const long long ring_bytes = 8LL * 32 * 16;
+    std::vector<int> fs(B, 0);
+    std::vector<long long> nops(B, 0), nch(B, 0);
+    std::vector<std::vector<int4>> iops(B);
+    std::vector<std::vector<int>> ich(B);
+    hvec<int> Lkpos((size_t)lnz);
+    par_for(B, nth, [&](int i) {
+      const auto &p = prep[i];
+      const int Ni = N[i];
+      const long long nli = (long long)p.Li.size(), kb = kof[i], lb = lof[i];
+      // KKT position of each L entry (i, j): row i of the permuted CSR
+      for (int j = 0; j < Ni; ++j)
+        for (int q = p.Lp[j]; q < p.Lp[j + 1]; ++q) {
+          const int r = p.Li[q];
+          auto b0 = p.Kj.begin() + p.Kp[r], b1 = p.Kj.begin() + p.Kp[r + 1];
+          auto it = std::lower_bound(b0, b1, j);
+          Lkpos[lb + q] = (it != b1 && *it == j) ? (int)(kb + (it - p.Kj.begin())) : -1;
+        }
+      const bool small = (long long)Ni * tsize <= 48 * 1024;
+      if (!small || (Ni + nli) * 8 + ring_bytes > kFactorSmemBytes) return;
+      fs[i] = 1;
+      auto &ops = iops[i];
+      auto &chk = ich[i];
+      const int nl = nlev[i];
+      const int *lp = p.lvl_ptr.data();
+      std::vector<int4> lev;  // {target, a, b, k}
+      bool bad = false;
+      for (int l = 0; l < nl && !bad; ++l) {
+        lev.clear();
+        for (int t = lp[l]; t < lp[l + 1]; ++t) {
+          const int j = p.lvl_nodes[t];
+          for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) {
+            const int k = p.Rk[r], pjk = p.Rpos[r];
+            lev.push_back(make_int4(j, Ni + pjk, Ni + pjk, k));  // d_j -= U(j,k)^2 / d_k
+            int q = p.Lp[j];
+            const int qe = p.Lp[j + 1];
+            for (int pp = pjk + 1; pp < p.Lp[k + 1]; ++pp) {
+              const int row = p.Li[pp];
+              while (q < qe && p.Li[q] != row) ++q;  // struct(L(:,k) below j) in L(:,j)
+              if (q == qe) {
+                bad = true;
+                break;
+              }
+              lev.push_back(make_int4(Ni + q, Ni + pp, Ni + pjk, k));
+            }
+          }
+        }
+        std::stable_sort(lev.begin(), lev.end(),
+                         [](const int4 &a, const int4 &b) { return a.x < b.x; });
+        const long long start = (long long)ops.size();
+        for (size_t q = 0; q < lev.size();) {
+          size_t r = q;
+          while (r + 1 < lev.size() && lev[r + 1].x == lev[q].x) ++r;
+          for (size_t t = q; t <= r; ++t) {
+            const int pos = (int)std::min<size_t>(t - q, 31);
+            int4 o = lev[t];
+            o.w = o.w | (pos << 16) | ((t == r ? 1 : 0) << 21);
+            ops.push_back(o);
+          }
+          q = r + 1;
+        }
+        for (long long c = start; c < (long long)ops.size(); c += 32) {
+          const long long cnt = std::min<long long>(32, (long long)ops.size() - c);
+          chk.push_back((int)(c | ((cnt - 1) << 26)));
+        }
+        // the level's pivots
+        const long long ps = (long long)ops.size();
+        for (int t = lp[l]; t < lp[l + 1]; ++t) {
+          const int j = p.lvl_nodes[t];
+          ops.push_back(make_int4(j, (int)p.Dsign[j], 0, 0));
+        }
+        for (long long c = ps; c < (long long)ops.size(); c += 32) {
+          const long long cnt = std::min<long long>(32, (long long)ops.size() - c);
+          chk.push_back((int)(c | ((cnt - 1) << 26) | (1u << 31)));
+        }
+      }
+      if (bad) {  // not reached for a valid symbolic factorisation
+        fs[i] = 0;
+        ops.clear();
+        chk.clear();
+      }
+      nops[i] = (long long)ops.size();
+      nch[i] = (long long)chk.size();
+    });
+    const auto oop = prefix(nops), och = prefix(nch);
+    if (oop[B] > 2000000000LL) return -4;
+    hvec<int4> fop(std::max<long long>(oop[B], 1));
+    hvec<int> foch(std::max<long long>(och[B], 1));
+    std::vector<int> fop_base(B), foch_off(B + 1);
+    int fs_max = 0;
+    bool any_fs = false;
+    for (int i = 0; i < B; ++i) {
+      fop_base[i] = (int)oop[i];
+      foch_off[i] = (int)och[i];
+      if (fs[i]) {
+        any_fs = true;
+        fs_max = std::max<int>(fs_max, N[i] + (int)prep[i].Li.size());
+      }
+    }
+    foch_off[B] = (int)och[B];
+    par_for(B, nth, [&](int i) {
+      std::copy(iops[i].begin(), iops[i].end(), fop.begin() + oop[i]);
+      std::copy(ich[i].begin(), ich[i].end(), foch.begin() + och[i]);
+      std::vector<int4>().swap(iops[i]);
+    });
+    kk.fstream = A.upload(fs);
+    kk.fop_base = A.upload(fop_base);
+    kk.foch = A.upload(foch);
+    kk.foch_off = A.upload(foch_off);
+    kk.fop = A.upload(fop);
+    kk.Lkpos = A.upload(Lkpos);
+    kk.fs_max = fs_max;
+    kk.has_fstream = any_fs ? 1 : 0;
+  }
   kk.fch = A.upload(fch);
   kk.bch = A.upload(bch);
   kk.kch = A.upload(kch);

@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
   if (!run[inst]) return;
   int N = k.N[inst];
   if (inst_class(N) != (SMEM ? 1 : 2)) return;
+  if (SMEM && k.has_fstream && k.fstream[inst]) return;  // streamed factorisation
   __shared__ double red[NT / 32 + 1];
   extern __shared__ __align__(16) unsigned char sm_raw[];
   const int vo = k.voff[inst], po = k.poff[inst];
@@ -732,11 +733,167 @@ __global__ void __launch_bounds__(32, 16)
 }
 #undef VEC_LOOP
 
+// ------------------------------------------------------------------------
+// Streamed single-warp factorisation.  Shared memory holds V = [d_j, then
+// 1/d_j once pivot j is taken (N) | U = L D (nnz(L))], initialised from the
+// KKT matrix (static regularisation on the diagonal).  The instance's op
+// stream is copied kRing chunks ahead into a shared ring with cp.async; an op
+// chunk subtracts V[a] V[b] V[k] from V[t] through a segmented warp scan
+// (the carry rule of the substitutions), a pivot chunk takes the pivots of
+// one level (dynamic regularisation, D and D^-1 in the storage type, 1/d_j
+// kept in V).  Updates of a level only read columns and pivots of lower
+// levels, all final.  At the end L = U / d is written in CSC order and in the
+// two substitution-stream orders.
+template <typename T>
+__global__ void __launch_bounds__(32, 8)
+    k_ldl_factor_stream(KKTDev k, LDLParams prm, const int *run, int *ok, double *eps_out) {
+  const int inst = blockIdx.x;
+  if (!run[inst] || !k.fstream[inst]) return;
+  const unsigned full = 0xffffffffu;
+  const int N = k.N[inst], vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x;
+  const int lbase = k.Lp[po], nl = k.Lp[po + N] - lbase;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double *V = reinterpret_cast<double *>(sm_raw);
+  int4 *ring = reinterpret_cast<int4 *>(sm_raw + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15));
+  const signed char *sg = k.Dsign + vo;
+  const int *Kdiag = k.Kdiag + vo;
+  T *D = reinterpret_cast<T *>(k.D) + vo;
+  T *Dinv = reinterpret_cast<T *>(k.Dinv) + vo;
+  // static regularisation eps = c + prop * max |diag(K)|
+  double eps = 0.0;
+  if (prm.static_reg) {
+    double mx = 0.0;
+    for (int j = lane; j < N; j += 32) mx = fmax(mx, fabs(k.Kx[Kdiag[j]]));
+    eps = prm.static_c + prm.static_prop * warp_max(mx);
+  }
+  for (int j = lane; j < N; j += 32) V[j] = k.Kx[Kdiag[j]] + (sg[j] > 0 ? eps : -eps);
+  {
+    const int *kp = k.Lkpos + lbase;
+    int pos[8];
+    for (int e0 = lane; e0 < nl; e0 += 32 * 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pos[u] = e0 + 32 * u < nl ? kp[e0 + 32 * u] : -1;
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (e0 + 32 * u < nl) V[N + e0 + 32 * u] = pos[u] >= 0 ? k.Kx[pos[u]] : 0.0;
+    }
+  }
+  __syncwarp();
+  // ---- the op / pivot stream
+  const int *chunks = k.foch + k.foch_off[inst];
+  const int nch = k.foch_off[inst + 1] - k.foch_off[inst];
+  const int4 *ops = k.fop + k.fop_base[inst];
+  bool finite = true;
+  double nent = 0.0;  // stream entries (profiling)
+  if (nch > 0) {
+    int d0 = lane < nch ? chunks[lane] : 0;
+    int d1 = lane + 32 < nch ? chunks[lane + 32] : 0;
+    int d2 = lane + 64 < nch ? chunks[lane + 64] : 0;
+    int blk = 0;
+    auto word = [&](int c) {
+      const int r = c - 32 * blk;
+      return __shfl_sync(full, r < 32 ? d0 : d1, r & 31);
+    };
+    auto issue = [&](int c, int slot) {
+      if (c < nch) {
+        const unsigned w = (unsigned)word(c);
+        const int p0 = (int)(w & 0x3ffffffu), cnt = (int)((w >> 26) & 31u) + 1;
+        if (lane < cnt) {
+          const unsigned dst =
+              static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * 32 + lane]));
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                       "l"(&ops[p0 + lane]));
+        }
+      }
+      asm volatile("cp.async.commit_group;\n" ::);
+    };
+#pragma unroll
+    for (int c = 0; c < kRing; ++c) issue(c, c);
+    double carry = 0.0;
+    for (int c = 0; c < nch; ++c) {
+      if (c > 0 && (c & 31) == 0) {
+        ++blk;
+        d0 = d1;
+        d1 = d2;
+        const int q = 32 * (blk + 2) + lane;
+        d2 = q < nch ? chunks[q] : 0;
+      }
+      const unsigned w = (unsigned)word(c);
+      const int cnt = (int)((w >> 26) & 31u) + 1;
+      const bool pivot = (w >> 31) != 0;
+      nent += cnt;
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
+      __syncwarp();
+      const int slot = c & (kRing - 1);
+      const bool v = lane < cnt;
+      const int4 o = v ? ring[slot * 32 + lane] : make_int4(0, 0, 0, 0);
+      if (pivot) {
+        if (v) {
+          const int j = o.x;
+          const double dj = pivot_value(V[j], (signed char)o.y, prm);
+          const T djs = T(dj);
+          const T dis = T(1.0 / double(djs));
+          D[j] = djs;
+          Dinv[j] = dis;
+          const double r = 1.0 / dj;
+          if (!isfinite(r) || !isfinite(double(djs)) || !isfinite(double(dis))) finite = false;
+          V[j] = r;
+        }
+        carry = 0.0;
+      } else {
+        const int pos = (o.w >> 16) & 31;
+        double x = v ? V[o.y] * V[o.z] * V[o.w & 0xffff] : 0.0;
+        if (lane == 0 && pos > 0) x += carry;
+        x = seg_scan_pos(x, pos, lane);
+        if (v && ((o.w >> 21) & 1)) V[o.x] -= x;
+        carry = __shfl_sync(full, x, cnt - 1);
+      }
+      __syncwarp();
+      issue(c + kRing, slot);
+    }
+    asm volatile("cp.async.wait_all;\n" ::);
+    __syncwarp();
+  }
+  // ---- L = U / d into CSC order and the two substitution-stream orders
+  {
+    T *Lx = reinterpret_cast<T *>(k.Lx), *LxF = reinterpret_cast<T *>(k.LxF),
+      *LxB = reinterpret_cast<T *>(k.LxB);
+    for (int e = lane; e < nl; e += 32) {
+      const int2 be = k.bent[lbase + e];
+      const int q = k.bpos[lbase + e];
+      const double l = V[N + (q - lbase)] * V[be.x & 0xffff];
+      Lx[q] = T(l);
+      LxB[lbase + e] = T(l);
+      const int2 fe = k.fent[lbase + e];
+      const int fq = k.fpos[lbase + e];
+      LxF[lbase + e] = T(V[N + (fq - lbase)] * V[fe.y]);
+    }
+  }
+  const bool bad = __any_sync(full, !finite);
+  if (lane == 0) {
+    if (bad) ok[inst] = 0;
+    if (eps_out) eps_out[inst] = eps;
+    if (k.prof_bytes) {
+      // K diagonal and L-position values (8 + 4 B each), the op stream (16 B
+      // per entry), chunk words, L written three times with the stream
+      // indices read, D and D^-1 written
+      const double ts = sizeof(T);
+      k.prof_bytes[inst] += 12.0 * N + 12.0 * nl + 16.0 * nent + 4.0 * nch +
+                            nl * (3.0 * ts + 16.0) + 2.0 * ts * N;
+    }
+  }
+}
+
 // dynamic shared memory = the largest single-warp instance's work vector
 template <typename T>
 static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, int *ok,
                           double *eps_out, cudaStream_t st) {
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
+  if (k.has_fstream) {
+    const size_t fsm = (((size_t)k.fs_max * sizeof(double) + 15) & ~(size_t)15) +
+                       (size_t)kRing * 32 * sizeof(int4);
+    k_ldl_factor_stream<T><<<k.B, kSmallNT, fsm, st>>>(k, p, run, ok, eps_out);
+  }
   if (k.has_small)
     k_ldl_factor<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
   if (k.has_large)
@@ -760,6 +917,10 @@ static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
 static bool g_attr_done = false;
 static void set_attrs() {
   if (g_attr_done) return;
+  cudaFuncSetAttribute(k_ldl_factor_stream<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       96 * 1024 + 16);
+  cudaFuncSetAttribute(k_ldl_factor_stream<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       96 * 1024 + 16);
   cudaFuncSetAttribute(k_ldl_factor<double, kSmallNT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,

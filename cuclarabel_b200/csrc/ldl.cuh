@@ -60,6 +60,21 @@ struct KKTDev {
   // (bits 0..25) | (count - 1) << 26.  Instance i's chunks of the forward,
   // backward and residual passes are fch[fch_off[i] .. fch_off[i+1]) etc.
   const int *fch, *bch, *kch, *fch_off, *bch_off, *kch_off;
+  // Streamed factorisation (single-warp instances whose N + nnz(L) FP64
+  // values fit in shared memory, fstream[i] = 1).  The kernel keeps U = L D
+  // (column j of L times d_j) and, once pivot j is final, 1/d_j in shared
+  // memory.  Per level of the elimination tree the op stream lists, sorted
+  // by target, every update
+  //     V[t] -= V[a] * V[b] * V[k]   (U(i,k) U(j,k) / d_k into U(i,j) or d_j)
+  // as int4 {t, a, b, k | position-in-segment << 16 | last << 21}, followed
+  // by the level's pivots {j, sign, 0, 0}.  Indices address the shared
+  // array [d or 1/d (N) | U (nnz(L))].  Chunk words: start relative to
+  // fop_base[i] (bits 0..25) | (count - 1) << 26 | pivot chunk << 31.
+  // Lkpos: KKT position of every L entry (-1: structural zero).
+  const int *fstream, *fop_base, *foch, *foch_off, *Lkpos;
+  const int4 *fop;
+  int fs_max;  // largest N + nnz(L) among streamed instances
+  int has_fstream;
   // profiling only (else null): per instance, algorithmic bytes moved by the
   // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
   double *prof_bytes;

@@ -43,7 +43,7 @@ def test_update_with_same_data_reproduces_the_solve(cuda_device):
         assert x.status == y.status or {x.status.name, y.status.name} <= near, k
         assert abs(x.iterations - y.iterations) <= 2, k
         if x.status == y.status == SolverStatus.SOLVED:
-            assert rel_err(x.obj_val, y.obj_val) < 1e-9, k
+            assert rel_err(x.obj_val, y.obj_val) < 1e-7, k
             assert np.linalg.norm(x.x - y.x) <= 1e-5 * max(1.0, np.linalg.norm(x.x)), k
 
 
