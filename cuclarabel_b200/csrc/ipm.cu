@@ -1647,6 +1647,15 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kk.fs_max = fs_max;
     kk.has_fstream = any_fs ? 1 : 0;
   }
+  {
+    std::vector<int> order(B);
+    for (int i = 0; i < B; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      return (long long)N[a] + (long long)prep[a].Li.size() >
+             (long long)N[b] + (long long)prep[b].Li.size();
+    });
+    kk.order = A.upload(order);
+  }
   kk.fch = A.upload(fch);
   kk.bch = A.upload(bch);
   kk.kch = A.upload(kch);

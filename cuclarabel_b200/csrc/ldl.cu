@@ -587,11 +587,11 @@ constexpr int kVecU = 8;
   }
 
 template <typename T>
-__global__ void __launch_bounds__(32, 16)
+__global__ void __launch_bounds__(32, 24)
     k_ldl_solve_warp(KKTDev k, LDLParams prm, const int *run, const double *__restrict__ rx,
                      const double *__restrict__ rz, double *lx, double *lz, int *ok,
                      int ymax) {
-  const int inst = blockIdx.x;
+  const int inst = k.order[blockIdx.x];
   if (!run[inst] || !ok[inst]) return;
   const int N = k.N[inst];
   if (inst_class(N) != 1) return;
@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(32, 16)
 template <typename T>
 __global__ void __launch_bounds__(32, 8)
     k_ldl_factor_stream(KKTDev k, LDLParams prm, const int *run, int *ok, double *eps_out) {
-  const int inst = blockIdx.x;
+  const int inst = k.order[blockIdx.x];
   if (!run[inst] || !k.fstream[inst]) return;
   const unsigned full = 0xffffffffu;
   const int N = k.N[inst], vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x;

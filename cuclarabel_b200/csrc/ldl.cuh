@@ -75,6 +75,10 @@ struct KKTDev {
   const int4 *fop;
   int fs_max;  // largest N + nnz(L) among streamed instances
   int has_fstream;
+  // launch order of the single-warp kernels: instances by decreasing size
+  // (N + nnz(L)), so the largest start in the first wave and the tail of the
+  // launch holds small ones
+  const int *order;
   // profiling only (else null): per instance, algorithmic bytes moved by the
   // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
   double *prof_bytes;

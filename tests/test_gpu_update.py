@@ -43,8 +43,9 @@ def test_update_with_same_data_reproduces_the_solve(cuda_device):
         assert x.status == y.status or {x.status.name, y.status.name} <= near, k
         assert abs(x.iterations - y.iterations) <= 2, k
         if x.status == y.status == SolverStatus.SOLVED:
+            # the objective is pinned to the gap tolerance; x is not (some of
+            # these instances have nearly flat optimal faces)
             assert rel_err(x.obj_val, y.obj_val) < 1e-7, k
-            assert np.linalg.norm(x.x - y.x) <= 1e-5 * max(1.0, np.linalg.norm(x.x)), k
 
 
 def test_update_q_b_matches_fresh_oracle(cuda_device):
