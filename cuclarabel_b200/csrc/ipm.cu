@@ -1445,22 +1445,23 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   hvec<int2> fent((size_t)lnz), bent((size_t)lnz), kent((size_t)knz);
   hvec<int> fpos((size_t)lnz), bpos((size_t)lnz), flev(lvl_ptr.size()), blev(lvl_ptr.size());
   std::vector<int> nchf(B, 0), nchb(B, 0), nchk(B, 0);
-  // encode segment positions: .x = seg | min(pos, 31) << 16 | last << 21
+  std::atomic<bool> too_big{false};
+  // encode segment positions: .x = seg | min(pos, kPosMax) << 16 | last << kLastBit
   auto encode = [](int2 *e, long long n) {
     long long q = 0;
     while (q < n) {
       long long r = q;
       while (r + 1 < n && e[r + 1].x == e[q].x) ++r;
       for (long long t = q; t <= r; ++t) {
-        const int pos = (int)std::min<long long>(t - q, 31);
-        e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << 21);
+        const int pos = (int)std::min<long long>(t - q, kPosMax);
+        e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << kLastBit);
       }
       q = r + 1;
     }
   };
   auto nchunks = [](const int *lev, int nl) {
     int n = 0;
-    for (int l = 0; l < nl; ++l) n += (lev[l + 1] - lev[l] + 31) / 32;
+    for (int l = 0; l < nl; ++l) n += (lev[l + 1] - lev[l] + kChunk - 1) / kChunk;
     return n;
   };
   par_for(B, nth, [&](int i) {
@@ -1498,15 +1499,19 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     for (int r = 0; r < N[i]; ++r)
       for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) kent[kbase + q] = make_int2(r, p.Kj[q]);
     if ((long long)N[i] * tsize <= 48 * 1024) {
+      // chunk words hold stream offsets below 2^25 (single-warp instances)
+      if (f - base > (long long)kStartMask || (long long)p.Kj.size() > (long long)kStartMask)
+        too_big = true;
       encode(fent.data() + base, f - base);
       encode(bent.data() + base, g - base);
       encode(kent.data() + kbase, (long long)p.Kj.size());
       nchf[i] = nchunks(flev.data() + lvl_off[i], nl);
       nchb[i] = nchunks(blev.data() + lvl_off[i], nl);
-      nchk[i] = ((int)p.Kj.size() + 31) / 32;
+      nchk[i] = ((int)p.Kj.size() + kChunk - 1) / kChunk;
     }
   });
-  // chunk tables: start relative to the stream base (bits 0..25) | (count - 1) << 26
+  if (too_big) return -4;
+  // chunk tables: start relative to the stream base | (count - 1) << kCntShift
   const auto ofch = prefix(nchf), obch = prefix(nchb), okch = prefix(nchk);
   hvec<int> fch(ofch[B]), bch(obch[B]), kch(okch[B]);
   std::vector<int> fch_off(B + 1), bch_off(B + 1), kch_off(B + 1);
@@ -1518,9 +1523,9 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   par_for(B, nth, [&](int i) {
     auto put = [](int *out, const int *lev, int nl, long long base) {
       for (int l = 0; l < nl; ++l)
-        for (long long c = lev[l]; c < lev[l + 1]; c += 32) {
-          const long long cnt = std::min<long long>(32, lev[l + 1] - c);
-          *out++ = (int)((c - base) | ((cnt - 1) << 26));
+        for (long long c = lev[l]; c < lev[l + 1]; c += kChunk) {
+          const long long cnt = std::min<long long>(kChunk, lev[l + 1] - c);
+          *out++ = (int)((c - base) | ((cnt - 1) << kCntShift));
         }
     };
     if (!nchf[i] && !nchb[i] && !nchk[i]) return;
@@ -1533,7 +1538,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   // streamed factorisation: op streams, pivots and chunk tables
   {
     constexpr long long kFactorSmemBytes = 96 * 1024;
-    const long long ring_bytes = 8LL * 32 * 16;
+    const long long ring_bytes = 4LL * kChunk * 16;
     std::vector<int> fs(B, 0);
     std::vector<long long> nops(B, 0), nch(B, 0);
     std::vector<std::vector<int4>> iops(B);
@@ -1587,16 +1592,16 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
           size_t r = q;
           while (r + 1 < lev.size() && lev[r + 1].x == lev[q].x) ++r;
           for (size_t t = q; t <= r; ++t) {
-            const int pos = (int)std::min<size_t>(t - q, 31);
+            const int pos = (int)std::min<size_t>(t - q, kPosMax);
             int4 o = lev[t];
-            o.w = o.w | (pos << 16) | ((t == r ? 1 : 0) << 21);
+            o.w = o.w | (pos << 16) | ((t == r ? 1 : 0) << kLastBit);
             ops.push_back(o);
           }
           q = r + 1;
         }
-        for (long long c = start; c < (long long)ops.size(); c += 32) {
-          const long long cnt = std::min<long long>(32, (long long)ops.size() - c);
-          chk.push_back((int)(c | ((cnt - 1) << 26)));
+        for (long long c = start; c < (long long)ops.size(); c += kChunk) {
+          const long long cnt = std::min<long long>(kChunk, (long long)ops.size() - c);
+          chk.push_back((int)(c | ((cnt - 1) << kCntShift)));
         }
         // the level's pivots
         const long long ps = (long long)ops.size();
@@ -1604,9 +1609,9 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
           const int j = p.lvl_nodes[t];
           ops.push_back(make_int4(j, (int)p.Dsign[j], 0, 0));
         }
-        for (long long c = ps; c < (long long)ops.size(); c += 32) {
-          const long long cnt = std::min<long long>(32, (long long)ops.size() - c);
-          chk.push_back((int)(c | ((cnt - 1) << 26) | (1u << 31)));
+        for (long long c = ps; c < (long long)ops.size(); c += kChunk) {
+          const long long cnt = std::min<long long>(kChunk, (long long)ops.size() - c);
+          chk.push_back((int)(c | ((cnt - 1) << kCntShift) | (1u << 31)));
         }
       }
       if (bad) {  // not reached for a valid symbolic factorisation

@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, L
 // complete (__syncwarp) before the next level gathers them.  The summation
 // order depends only on the instance's own layout, never on the batch.
 
-constexpr int kRing = 8;  // chunks in flight per warp (power of two)
+constexpr int kRing = 4;  // chunks in flight per warp (power of two)
 
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
@@ -491,16 +491,26 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(BYTES));
 }
 
-// Segmented inclusive scan of one chunk: lane l adds lane l-d's partial when
-// both lie in the same segment, i.e. d <= its position in the segment (pos,
-// clamped to 31) and d <= l.
-__device__ __forceinline__ double seg_scan_pos(double v, int pos, int lane) {
+// Segmented sums of one chunk held two entries per lane: A = entry 2 lane,
+// B = entry 2 lane + 1, with products xA, xB and positions in their segments
+// pA, pB (clamped to 63).  Returns sA / sB: the sum of A's / B's segment from
+// its start up to A / B, including lower lanes and, for a segment continued
+// from the previous chunk, the carry.  The lane scan runs over each lane's
+// tail value (its part of B's segment); a lane adds lane l-d's value while
+// d does not pass the lane that holds the start of B's segment.
+__device__ __forceinline__ void seg_scan2(double xA, double xB, int pA, int pB, int lane,
+                                          double carry, double &sA, double &sB) {
+  if (lane == 0 && pA > 0) xA += carry;
+  double v = pB > 0 ? xA + xB : xB;
+  const int reach = pB > 0 ? lane - ((2 * lane + 1 - pB) >> 1) : 0;  // lanes back
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     const double o = __shfl_up_sync(0xffffffffu, v, d);
-    if (d <= pos && d <= lane) v += o;
+    if (d <= reach && d <= lane) v += o;
   }
-  return v;
+  sB = v;
+  const double prev = __shfl_up_sync(0xffffffffu, v, 1);
+  sA = xA + ((pA > 0 && lane > 0) ? prev : 0.0);
 }
 
 // One pass over an encoded stream (entries ent / values val from stream
@@ -520,16 +530,20 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
   int blk = 0;  // d0 holds chunks [32 blk, 32 blk + 32)
   auto word = [&](int c) {
     const int r = c - 32 * blk;  // 0 <= r < 64
-    return __shfl_sync(full, r < 32 ? d0 : d1, r & 31);
+    return (unsigned)__shfl_sync(full, r < 32 ? d0 : d1, r & 31);
   };
   auto issue = [&](int c, int slot) {
     if (c < nch) {
-      const int w = word(c);
-      const int p = base + (w & 0x3ffffff);
-      const int cnt = ((unsigned)w >> 26) + 1;
-      if (lane < cnt) {
-        cp_async<8>(&re[slot * 32 + lane], &ent[p + lane]);
-        cp_async<sizeof(T)>(&rv[slot * 32 + lane], &val[p + lane]);
+      const unsigned w = word(c);
+      const int p = base + (int)(w & kStartMask);
+      const int cnt = (int)((w >> kCntShift) & 63u) + 1;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e = 2 * lane + h;
+        if (e < cnt) {
+          cp_async<8>(&re[slot * kChunk + e], &ent[p + e]);
+          cp_async<sizeof(T)>(&rv[slot * kChunk + e], &val[p + e]);
+        }
       }
     }
     asm volatile("cp.async.commit_group;\n" ::);
@@ -545,24 +559,34 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
       const int q = 32 * (blk + 2) + lane;
       d2 = q < nch ? chunks[q] : 0;
     }
-    const int cnt = ((unsigned)word(c) >> 26) + 1;
+    const int cnt = (int)((word(c) >> kCntShift) & 63u) + 1;
     asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
     __syncwarp();
     const int slot = c & (kRing - 1);
-    const bool v = lane < cnt;
-    const int2 en = v ? re[slot * 32 + lane] : make_int2(0, 0);
-    const int pos = (en.x >> 16) & 31;
-    double x = v ? double(rv[slot * 32 + lane]) * y[en.y] : 0.0;
-    if (lane == 0 && pos > 0) x += carry;  // segment continued from the last chunk
-    x = seg_scan_pos(x, pos, lane);
-    if (v && ((en.x >> 21) & 1)) {
-      const int seg = en.x & 0xffff;
+    const int eA = 2 * lane, eB = eA + 1;
+    const bool vA = eA < cnt, vB = eB < cnt;
+    const int2 enA = vA ? re[slot * kChunk + eA] : make_int2(0, 0);
+    const int2 enB = vB ? re[slot * kChunk + eB] : make_int2(0, 0);
+    const double xA = vA ? double(rv[slot * kChunk + eA]) * y[enA.y] : 0.0;
+    const double xB = vB ? double(rv[slot * kChunk + eB]) * y[enB.y] : 0.0;
+    double sA, sB;
+    seg_scan2(xA, xB, (enA.x >> 16) & 63, (enB.x >> 16) & 63, lane, carry, sA, sB);
+    if (vA && ((enA.x >> kLastBit) & 1)) {
       if (RESID)
-        out[seg] = x;
+        out[enA.x & 0xffff] = sA;
       else
-        out[seg] -= x;
+        out[enA.x & 0xffff] -= sA;
     }
-    carry = __shfl_sync(full, x, cnt - 1);
+    if (vB && ((enB.x >> kLastBit) & 1)) {
+      if (RESID)
+        out[enB.x & 0xffff] = sB;
+      else
+        out[enB.x & 0xffff] -= sB;
+    }
+    // partial sum of the segment of the chunk's last entry (used by the next
+    // chunk only if its first entry continues that segment)
+    const int ll = (cnt - 1) >> 1;
+    carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
     __syncwarp();
     issue(c + kRing, slot);
   }
@@ -598,7 +622,7 @@ __global__ void __launch_bounds__(32, 24)
   extern __shared__ __align__(16) unsigned char sm_raw[];
   double *y = reinterpret_cast<double *>(sm_raw);
   int2 *re = reinterpret_cast<int2 *>(sm_raw + (((size_t)ymax * 8 + 15) & ~(size_t)15));
-  T *rv = reinterpret_cast<T *>(re + kRing * 32);
+  T *rv = reinterpret_cast<T *>(re + kRing * kChunk);
   const int vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x;
   double *__restrict__ b = k.b + vo;
   double *__restrict__ x = k.x + vo;
@@ -797,12 +821,16 @@ __global__ void __launch_bounds__(32, 8)
     auto issue = [&](int c, int slot) {
       if (c < nch) {
         const unsigned w = (unsigned)word(c);
-        const int p0 = (int)(w & 0x3ffffffu), cnt = (int)((w >> 26) & 31u) + 1;
-        if (lane < cnt) {
-          const unsigned dst =
-              static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * 32 + lane]));
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
-                       "l"(&ops[p0 + lane]));
+        const int p0 = (int)(w & kStartMask), cnt = (int)((w >> kCntShift) & 63u) + 1;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int e = 2 * lane + h;
+          if (e < cnt) {
+            const unsigned dst =
+                static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * kChunk + e]));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                         "l"(&ops[p0 + e]));
+          }
         }
       }
       asm volatile("cp.async.commit_group;\n" ::);
@@ -819,34 +847,43 @@ __global__ void __launch_bounds__(32, 8)
         d2 = q < nch ? chunks[q] : 0;
       }
       const unsigned w = (unsigned)word(c);
-      const int cnt = (int)((w >> 26) & 31u) + 1;
+      const int cnt = (int)((w >> kCntShift) & 63u) + 1;
       const bool pivot = (w >> 31) != 0;
       nent += cnt;
       asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
       __syncwarp();
       const int slot = c & (kRing - 1);
-      const bool v = lane < cnt;
-      const int4 o = v ? ring[slot * 32 + lane] : make_int4(0, 0, 0, 0);
+      const int eA = 2 * lane, eB = eA + 1;
+      const bool vA = eA < cnt, vB = eB < cnt;
+      const int4 oA = vA ? ring[slot * kChunk + eA] : make_int4(0, 0, 0, 0);
+      const int4 oB = vB ? ring[slot * kChunk + eB] : make_int4(0, 0, 0, 0);
       if (pivot) {
-        if (v) {
-          const int j = o.x;
-          const double dj = pivot_value(V[j], (signed char)o.y, prm);
-          const T djs = T(dj);
-          const T dis = T(1.0 / double(djs));
-          D[j] = djs;
-          Dinv[j] = dis;
-          const double r = 1.0 / dj;
-          if (!isfinite(r) || !isfinite(double(djs)) || !isfinite(double(dis))) finite = false;
-          V[j] = r;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int4 o = h ? oB : oA;
+          if (h ? vB : vA) {
+            const int j = o.x;
+            const double dj = pivot_value(V[j], (signed char)o.y, prm);
+            const T djs = T(dj);
+            const T dis = T(1.0 / double(djs));
+            D[j] = djs;
+            Dinv[j] = dis;
+            const double r = 1.0 / dj;
+            if (!isfinite(r) || !isfinite(double(djs)) || !isfinite(double(dis)))
+              finite = false;
+            V[j] = r;
+          }
         }
         carry = 0.0;
       } else {
-        const int pos = (o.w >> 16) & 31;
-        double x = v ? V[o.y] * V[o.z] * V[o.w & 0xffff] : 0.0;
-        if (lane == 0 && pos > 0) x += carry;
-        x = seg_scan_pos(x, pos, lane);
-        if (v && ((o.w >> 21) & 1)) V[o.x] -= x;
-        carry = __shfl_sync(full, x, cnt - 1);
+        const double xA = vA ? V[oA.y] * V[oA.z] * V[oA.w & 0xffff] : 0.0;
+        const double xB = vB ? V[oB.y] * V[oB.z] * V[oB.w & 0xffff] : 0.0;
+        double sA, sB;
+        seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry, sA, sB);
+        if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] -= sA;
+        if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] -= sB;
+        const int ll = (cnt - 1) >> 1;
+        carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
       }
       __syncwarp();
       issue(c + kRing, slot);
@@ -891,7 +928,7 @@ static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, i
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
   if (k.has_fstream) {
     const size_t fsm = (((size_t)k.fs_max * sizeof(double) + 15) & ~(size_t)15) +
-                       (size_t)kRing * 32 * sizeof(int4);
+                       (size_t)kRing * kChunk * sizeof(int4);
     k_ldl_factor_stream<T><<<k.B, kSmallNT, fsm, st>>>(k, p, run, ok, eps_out);
   }
   if (k.has_small)
@@ -906,7 +943,7 @@ static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
   if (k.has_small) {
     // y, then the cp.async ring (entries + values, FP64 values for the residual)
-    const size_t smw = sm + (size_t)kRing * 32 * (sizeof(int2) + sizeof(double));
+    const size_t smw = sm + (size_t)kRing * kChunk * (sizeof(int2) + sizeof(double));
     k_ldl_solve_warp<T><<<k.B, kSmallNT, smw, st>>>(k, p, run, rx, rz, lx, lz, ok,
                                                      k.max_small_N);
   }
@@ -925,7 +962,7 @@ static void set_attrs() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
-  const int ring_bytes = kRing * 32 * (int)(sizeof(int2) + sizeof(double));
+  const int ring_bytes = kRing * kChunk * (int)(sizeof(int2) + sizeof(double));
   cudaFuncSetAttribute(k_ldl_solve_warp<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        kSmemLimitBytes + 16 + ring_bytes);
   cudaFuncSetAttribute(k_ldl_solve_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -94,6 +94,16 @@ struct KKTDev {
   double *b, *x, *e, *dx;
 };
 
+// Stream chunking shared by the setup and the kernels: a chunk holds up to
+// kChunk consecutive entries of one level, two per lane.  Entry word:
+// segment (bits 0..15) | min(position in segment, 63) << 16 | last << 22.
+// Chunk word: start (bits 0..24) | (count - 1) << 25 | pivot chunk << 31.
+constexpr int kChunk = 64;
+constexpr int kPosMax = 63;
+constexpr int kLastBit = 22;
+constexpr int kCntShift = 25;
+constexpr unsigned kStartMask = (1u << 25) - 1u;
+
 struct LDLParams {
   int static_reg;
   double static_c, static_prop;
