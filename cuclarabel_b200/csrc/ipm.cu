@@ -1651,6 +1651,46 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kk.Lkpos = A.upload(Lkpos);
     kk.fs_max = fs_max;
     kk.has_fstream = any_fs ? 1 : 0;
+    // pack streamed instances into blocks of kFactorWarps warps: first fit by
+    // decreasing shared-memory need, bins as large as the largest need
+    {
+      auto need = [&](int i) {
+        return ((((long long)N[i] + (long long)prep[i].Li.size()) * 8 + 15) & ~15LL) +
+               (long long)kRingSlots * kChunk * 16;
+      };
+      std::vector<int> items;
+      for (int i = 0; i < B; ++i)
+        if (fs[i]) items.push_back(i);
+      std::stable_sort(items.begin(), items.end(), [&](int a, int b) { return need(a) > need(b); });
+      const long long cap = items.empty() ? 0 : need(items[0]);
+      std::vector<long long> used;
+      std::vector<int> cnt, pinst, poffv;
+      size_t first_open = 0;
+      for (int i : items) {
+        const long long s_i = need(i);
+        size_t b = first_open;
+        while (b < used.size() && (cnt[b] == kFactorWarps || used[b] + s_i > cap)) ++b;
+        if (b == used.size()) {
+          used.push_back(0);
+          cnt.push_back(0);
+          for (int w = 0; w < kFactorWarps; ++w) {
+            pinst.push_back(-1);
+            poffv.push_back(0);
+          }
+        }
+        pinst[kFactorWarps * b + cnt[b]] = i;
+        poffv[kFactorWarps * b + cnt[b]] = (int)used[b];
+        used[b] += s_i;
+        ++cnt[b];
+        while (first_open < used.size() &&
+               (cnt[first_open] == kFactorWarps || used[first_open] + need(items.back()) > cap))
+          ++first_open;
+      }
+      kk.fpack_inst = A.upload(pinst);
+      kk.fpack_off = A.upload(poffv);
+      kk.fpack_blocks = (int)used.size();
+      kk.fpack_smem = (int)cap;
+    }
   }
   {
     std::vector<int> order(B);

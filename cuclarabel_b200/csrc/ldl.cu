@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, L
 // complete (__syncwarp) before the next level gathers them.  The summation
 // order depends only on the instance's own layout, never on the batch.
 
-constexpr int kRing = 4;  // chunks in flight per warp (power of two)
+constexpr int kRing = kRingSlots;
 
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
@@ -769,16 +769,20 @@ __global__ void __launch_bounds__(32, 24)
 // levels, all final.  At the end L = U / d is written in CSC order and in the
 // two substitution-stream orders.
 template <typename T>
-__global__ void __launch_bounds__(32, 8)
+__global__ void __launch_bounds__(32 * kFactorWarps, 4)
     k_ldl_factor_stream(KKTDev k, LDLParams prm, const int *run, int *ok, double *eps_out) {
-  const int inst = k.order[blockIdx.x];
-  if (!run[inst] || !k.fstream[inst]) return;
+  // warps of a block factor different instances; they share nothing but the
+  // block's shared memory, each in its own slice, and never synchronise
+  const int slot = blockIdx.x * kFactorWarps + (threadIdx.x >> 5);
+  const int inst = k.fpack_inst[slot];
+  if (inst < 0 || !run[inst]) return;
   const unsigned full = 0xffffffffu;
-  const int N = k.N[inst], vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x;
+  const int N = k.N[inst], vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x & 31;
   const int lbase = k.Lp[po], nl = k.Lp[po + N] - lbase;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  double *V = reinterpret_cast<double *>(sm_raw);
-  int4 *ring = reinterpret_cast<int4 *>(sm_raw + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15));
+  unsigned char *sm = sm_raw + k.fpack_off[slot];
+  double *V = reinterpret_cast<double *>(sm);
+  int4 *ring = reinterpret_cast<int4 *>(sm + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15));
   const signed char *sg = k.Dsign + vo;
   const int *Kdiag = k.Kdiag + vo;
   T *D = reinterpret_cast<T *>(k.D) + vo;
@@ -926,11 +930,9 @@ template <typename T>
 static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, int *ok,
                           double *eps_out, cudaStream_t st) {
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
-  if (k.has_fstream) {
-    const size_t fsm = (((size_t)k.fs_max * sizeof(double) + 15) & ~(size_t)15) +
-                       (size_t)kRing * kChunk * sizeof(int4);
-    k_ldl_factor_stream<T><<<k.B, kSmallNT, fsm, st>>>(k, p, run, ok, eps_out);
-  }
+  if (k.has_fstream)
+    k_ldl_factor_stream<T><<<k.fpack_blocks, 32 * kFactorWarps, k.fpack_smem, st>>>(
+        k, p, run, ok, eps_out);
   if (k.has_small)
     k_ldl_factor<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
   if (k.has_large)
@@ -955,9 +957,9 @@ static bool g_attr_done = false;
 static void set_attrs() {
   if (g_attr_done) return;
   cudaFuncSetAttribute(k_ldl_factor_stream<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       96 * 1024 + 16);
+                       96 * 1024 + 64);
   cudaFuncSetAttribute(k_ldl_factor_stream<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       96 * 1024 + 16);
+                       96 * 1024 + 64);
   cudaFuncSetAttribute(k_ldl_factor<double, kSmallNT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,

@@ -75,6 +75,12 @@ struct KKTDev {
   const int4 *fop;
   int fs_max;  // largest N + nnz(L) among streamed instances
   int has_fstream;
+  // Packing of streamed instances into blocks of kFactorWarps warps (first
+  // fit by decreasing shared-memory need): warp w of block b factors
+  // fpack_inst[kFactorWarps b + w] (-1: idle) with its shared memory at byte
+  // fpack_off[...]; fpack_smem bytes per block.
+  const int *fpack_inst, *fpack_off;
+  int fpack_blocks, fpack_smem;
   // launch order of the single-warp kernels: instances by decreasing size
   // (N + nnz(L)), so the largest start in the first wave and the tail of the
   // launch holds small ones
@@ -99,6 +105,8 @@ struct KKTDev {
 // segment (bits 0..15) | min(position in segment, 63) << 16 | last << 22.
 // Chunk word: start (bits 0..24) | (count - 1) << 25 | pivot chunk << 31.
 constexpr int kChunk = 64;
+constexpr int kRingSlots = 4;          // chunks in flight per warp (power of two)
+constexpr int kFactorWarps = 4;        // instances per streamed-factorisation block
 constexpr int kPosMax = 63;
 constexpr int kLastBit = 22;
 constexpr int kCntShift = 25;
