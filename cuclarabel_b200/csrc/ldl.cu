@@ -787,14 +787,28 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 4)
   const int *Kdiag = k.Kdiag + vo;
   T *D = reinterpret_cast<T *>(k.D) + vo;
   T *Dinv = reinterpret_cast<T *>(k.Dinv) + vo;
-  // static regularisation eps = c + prop * max |diag(K)|
-  double eps = 0.0;
-  if (prm.static_reg) {
-    double mx = 0.0;
-    for (int j = lane; j < N; j += 32) mx = fmax(mx, fabs(k.Kx[Kdiag[j]]));
-    eps = prm.static_c + prm.static_prop * warp_max(mx);
+  // diagonal of K into V (loads of kU elements in flight per lane), then the
+  // static regularisation eps = c + prop * max |diag(K)| on it
+  constexpr int kU = 8;
+  double mx = 0.0;
+  for (int j0 = lane; j0 < N; j0 += 32 * kU) {
+    int kd[kU];
+    double kv[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) kd[u] = j0 + 32 * u < N ? Kdiag[j0 + 32 * u] : -1;
+#pragma unroll
+    for (int u = 0; u < kU; ++u) kv[u] = kd[u] >= 0 ? k.Kx[kd[u]] : 0.0;
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+      if (kd[u] >= 0) {
+        V[j0 + 32 * u] = kv[u];
+        mx = fmax(mx, fabs(kv[u]));
+      }
   }
-  for (int j = lane; j < N; j += 32) V[j] = k.Kx[Kdiag[j]] + (sg[j] > 0 ? eps : -eps);
+  double eps = 0.0;
+  if (prm.static_reg) eps = prm.static_c + prm.static_prop * warp_max(mx);
+  __syncwarp();
+  for (int j = lane; j < N; j += 32) V[j] += sg[j] > 0 ? eps : -eps;
   {
     const int *kp = k.Lkpos + lbase;
     int pos[8];
@@ -899,15 +913,29 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 4)
   {
     T *Lx = reinterpret_cast<T *>(k.Lx), *LxF = reinterpret_cast<T *>(k.LxF),
       *LxB = reinterpret_cast<T *>(k.LxB);
-    for (int e = lane; e < nl; e += 32) {
-      const int2 be = k.bent[lbase + e];
-      const int q = k.bpos[lbase + e];
-      const double l = V[N + (q - lbase)] * V[be.x & 0xffff];
-      Lx[q] = T(l);
-      LxB[lbase + e] = T(l);
-      const int2 fe = k.fent[lbase + e];
-      const int fq = k.fpos[lbase + e];
-      LxF[lbase + e] = T(V[N + (fq - lbase)] * V[fe.y]);
+    for (int e0 = lane; e0 < nl; e0 += 32 * kU) {
+      int2 be[kU], fe[kU];
+      int bq[kU], fq[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int e = e0 + 32 * u;
+        if (e < nl) {
+          be[u] = k.bent[lbase + e];
+          bq[u] = k.bpos[lbase + e];
+          fe[u] = k.fent[lbase + e];
+          fq[u] = k.fpos[lbase + e];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int e = e0 + 32 * u;
+        if (e < nl) {
+          const double l = V[N + (bq[u] - lbase)] * V[be[u].x & 0xffff];
+          Lx[bq[u]] = T(l);
+          LxB[lbase + e] = T(l);
+          LxF[lbase + e] = T(V[N + (fq[u] - lbase)] * V[fe[u].y]);
+        }
+      }
     }
   }
   const bool bad = __any_sync(full, !finite);
