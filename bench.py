@@ -245,10 +245,10 @@ def workload_config(B, method):
                         % B, "instances_per_gpu": B, "method": method}
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the single-warp LDL solve from the committed
-    ncu summary (profiles/ldl_solve_mpc4096.md), or None."""
-    p = os.path.join(ROOT, "profiles", "ldl_solve_mpc4096.md")
+def ncu_traffic(summary):
+    """DRAM bytes (read + write) of one launch from a committed ncu summary
+    under profiles/ (its dram_bytes_per_launch line), or None."""
+    p = os.path.join(ROOT, "profiles", summary)
     try:
         with open(p) as f:
             for line in f:
@@ -433,7 +433,8 @@ def main():
     phases = prof["phases"]
     dom = max(phases.items(), key=lambda kv: kv[1][0])
     kernels = {"ldl_solve": "k_ldl_solve_warp (single-warp LDL solve + refinement)",
-               "ldl_factor": "k_ldl_factor (single-warp LDL factorisation)"}
+               "ldl_factor": "k_ldl_factor_stream (streamed single-warp LDL factorisation)"}
+    summaries = {"ldl_solve": "ldl_solve_mpc4096.md", "ldl_factor": "ldl_factor_stream_mpc4096.md"}
 
     def roofline(name):
         ms, calls = phases[name]
@@ -441,7 +442,10 @@ def main():
         ach = by / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
         return {"bound": "hbm", "kernel": kernels.get(name, name), "achieved": ach,
                 "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": ncu_traffic() if name == "ldl_solve" else None,
+                "traffic": ncu_traffic(summaries[name]) if name in summaries else None,
+                "traffic_source": ("profiles/" + summaries[name] + " (one captured launch; "
+                                   "dram__bytes_read.sum + dram__bytes_write.sum)")
+                if name in summaries else None,
                 "peak_kind": peak_note,
                 "algorithmic_bytes_per_launch": by / max(calls, 1),
                 "avg_launch_ms": ms / max(calls, 1), "launches": calls}
