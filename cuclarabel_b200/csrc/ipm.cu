@@ -1243,8 +1243,15 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   const int tsize = 8;  // work vectors are FP64 in both precision forms
   int max_small = 0;
   bool has_small = false, has_large = false;
+  // kernel class: single warp when the work vector fits the shared-memory
+  // budget and the streams fit the chunk-word offsets
+  std::vector<int> cls(B);
   for (int i = 0; i < B; ++i) {
-    if ((long long)N[i] * tsize <= 48 * 1024) {
+    const bool fits = (long long)N[i] * tsize <= 48 * 1024 &&
+                      (long long)prep[i].Li.size() <= (long long)kStartMask &&
+                      (long long)prep[i].Kj.size() <= (long long)kStartMask;
+    cls[i] = fits ? 1 : 2;
+    if (fits) {
       has_small = true;
       max_small = std::max(max_small, N[i]);
     } else {
@@ -1445,7 +1452,6 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   hvec<int2> fent((size_t)lnz), bent((size_t)lnz), kent((size_t)knz);
   hvec<int> fpos((size_t)lnz), bpos((size_t)lnz), flev(lvl_ptr.size()), blev(lvl_ptr.size());
   std::vector<int> nchf(B, 0), nchb(B, 0), nchk(B, 0);
-  std::atomic<bool> too_big{false};
   // encode segment positions: .x = seg | min(pos, kPosMax) << 16 | last << kLastBit
   auto encode = [](int2 *e, long long n) {
     long long q = 0;
@@ -1498,10 +1504,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     const long long kbase = Kp[poff[i]];
     for (int r = 0; r < N[i]; ++r)
       for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) kent[kbase + q] = make_int2(r, p.Kj[q]);
-    if ((long long)N[i] * tsize <= 48 * 1024) {
-      // chunk words hold stream offsets below 2^25 (single-warp instances)
-      if (f - base > (long long)kStartMask || (long long)p.Kj.size() > (long long)kStartMask)
-        too_big = true;
+    if (cls[i] == 1) {
       encode(fent.data() + base, f - base);
       encode(bent.data() + base, g - base);
       encode(kent.data() + kbase, (long long)p.Kj.size());
@@ -1510,8 +1513,8 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       nchk[i] = ((int)p.Kj.size() + kChunk - 1) / kChunk;
     }
   });
-  if (too_big) return -4;
-  // chunk tables: start relative to the stream base | (count - 1) << kCntShift
+  // chunk tables: start relative to the stream base | scan steps <<
+  // kStepShift | (count - 1) << kCntShift
   const auto ofch = prefix(nchf), obch = prefix(nchb), okch = prefix(nchk);
   hvec<int> fch(ofch[B]), bch(obch[B]), kch(okch[B]);
   std::vector<int> fch_off(B + 1), bch_off(B + 1), kch_off(B + 1);
@@ -1521,20 +1524,44 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kch_off[i] = (int)okch[i];
   }
   par_for(B, nth, [&](int i) {
-    auto put = [](int *out, const int *lev, int nl, long long base) {
+    auto put = [](int *out, const int *lev, int nl, long long base, const int2 *ent) {
       for (int l = 0; l < nl; ++l)
         for (long long c = lev[l]; c < lev[l + 1]; c += kChunk) {
-          const long long cnt = std::min<long long>(kChunk, lev[l + 1] - c);
-          *out++ = (int)((c - base) | ((cnt - 1) << kCntShift));
+          const int cnt = (int)std::min<long long>(kChunk, lev[l + 1] - c);
+          const int steps =
+              chunk_scan_steps(cnt, [&](int e) { return (ent[c + e].x >> 16) & kPosMax; });
+          *out++ = (int)((c - base) | ((long long)steps << kStepShift) |
+                         ((long long)(cnt - 1) << kCntShift));
         }
     };
-    if (!nchf[i] && !nchb[i] && !nchk[i]) return;
+    if (cls[i] != 1) return;
     const long long base = Lp[poff[i]], kbase = Kp[poff[i]];
-    put(fch.data() + ofch[i], flev.data() + lvl_off[i], nlev[i], base);
-    put(bch.data() + obch[i], blev.data() + lvl_off[i], nlev[i], base);
+    put(fch.data() + ofch[i], flev.data() + lvl_off[i], nlev[i], base, fent.data());
+    put(bch.data() + obch[i], blev.data() + lvl_off[i], nlev[i], base, bent.data());
     const int klev[2] = {(int)kbase, (int)(kbase + prep[i].Kj.size())};
-    put(kch.data() + okch[i], klev, 1, kbase);
+    put(kch.data() + okch[i], klev, 1, kbase, kent.data());
   });
+  // setup statistics (verbose): scan steps per chunk of each stream kind
+  auto step_stats = [&](const char *name, const int *w, size_t n) {
+    if (!h->st.verbose) return;
+    long long hist[8] = {0, 0, 0, 0, 0, 0, 0, 0}, nc = 0, ne = 0;
+    for (size_t c = 0; c < n; ++c) {
+      if ((unsigned)w[c] >> 31) continue;  // pivot chunks take no scan
+      ++hist[((unsigned)w[c] >> kStepShift) & 7u];
+      ++nc;
+      ne += (((unsigned)w[c] >> kCntShift) & 63u) + 1;
+    }
+    double mean = 0;
+    for (int q = 0; q < 8; ++q) mean += q * (double)hist[q];
+    std::fprintf(stderr,
+                 "clgpu setup: %-6s chunks %lld, entries/chunk %.1f, scan steps mean %.2f "
+                 "[%lld %lld %lld %lld %lld %lld]\n",
+                 name, nc, nc ? (double)ne / nc : 0.0, nc ? mean / nc : 0.0, hist[0], hist[1],
+                 hist[2], hist[3], hist[4], hist[5]);
+  };
+  step_stats("fwd", fch.data(), fch.size());
+  step_stats("bwd", bch.data(), bch.size());
+  step_stats("resid", kch.data(), kch.size());
   // streamed factorisation: op streams, pivots and chunk tables
   {
     constexpr long long kFactorSmemBytes = 96 * 1024;
@@ -1556,8 +1583,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
           auto it = std::lower_bound(b0, b1, j);
           Lkpos[lb + q] = (it != b1 && *it == j) ? (int)(kb + (it - p.Kj.begin())) : -1;
         }
-      const bool small = (long long)Ni * tsize <= 48 * 1024;
-      if (!small || (Ni + nli) * 8 + ring_bytes > kFactorSmemBytes) return;
+      if (cls[i] != 1 || (Ni + nli) * 8 + ring_bytes > kFactorSmemBytes) return;
       fs[i] = 1;
       auto &ops = iops[i];
       auto &chk = ich[i];
@@ -1600,8 +1626,11 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
           q = r + 1;
         }
         for (long long c = start; c < (long long)ops.size(); c += kChunk) {
-          const long long cnt = std::min<long long>(kChunk, (long long)ops.size() - c);
-          chk.push_back((int)(c | ((cnt - 1) << kCntShift)));
+          const int cnt = (int)std::min<long long>(kChunk, (long long)ops.size() - c);
+          const int steps =
+              chunk_scan_steps(cnt, [&](int e) { return (ops[c + e].w >> 16) & kPosMax; });
+          chk.push_back((int)(c | ((long long)steps << kStepShift) |
+                              ((long long)(cnt - 1) << kCntShift)));
         }
         // the level's pivots
         const long long ps = (long long)ops.size();
@@ -1614,7 +1643,11 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
           chk.push_back((int)(c | ((cnt - 1) << kCntShift) | (1u << 31)));
         }
       }
-      if (bad) {  // not reached for a valid symbolic factorisation
+      // a pattern mismatch is not reached for a valid symbolic factorisation;
+      // an op stream longer than the chunk words address is; both fall back
+      // to the level-scheduled single-warp factorisation
+      if ((long long)ops.size() > (long long)kStartMask) bad = true;
+      if (bad) {
         fs[i] = 0;
         ops.clear();
         chk.clear();
@@ -1643,6 +1676,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       std::copy(ich[i].begin(), ich[i].end(), foch.begin() + och[i]);
       std::vector<int4>().swap(iops[i]);
     });
+    step_stats("factor", foch.data(), foch.size());
     kk.fstream = A.upload(fs);
     kk.fop_base = A.upload(fop_base);
     kk.foch = A.upload(foch);
@@ -1651,6 +1685,9 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kk.Lkpos = A.upload(Lkpos);
     kk.fs_max = fs_max;
     kk.has_fstream = any_fs ? 1 : 0;
+    kk.has_small_legacy = 0;
+    for (int i = 0; i < B; ++i)
+      if (cls[i] == 1 && !fs[i]) kk.has_small_legacy = 1;
     // pack streamed instances into blocks of kFactorWarps warps: first fit by
     // decreasing shared-memory need, bins as large as the largest need
     {
@@ -1701,6 +1738,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     });
     kk.order = A.upload(order);
   }
+  kk.cls = A.upload(cls);
   kk.fch = A.upload(fch);
   kk.bch = A.upload(bch);
   kk.kch = A.upload(kch);

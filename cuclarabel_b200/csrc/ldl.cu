@@ -85,11 +85,6 @@ __device__ __forceinline__ double block_max(double v, double *red) {
   return red[NT / 32];
 }
 
-// class of an instance: 1 = small (single warp, smem), 2 = large
-__device__ __forceinline__ int inst_class(int N) {
-  return (long long)N * (long long)sizeof(double) <= kSmemLimitBytes ? 1 : 2;
-}
-
 // Dynamic regularisation of pivot dj (kktsolver_directldl.jl:224-229 via
 // QDLDL's Dsigns check): the FP64 pivot the elimination continues with.
 __device__ __forceinline__ double pivot_value(double dj, signed char sg, const LDLParams &prm) {
@@ -126,7 +121,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
   int inst = blockIdx.x;
   if (!run[inst]) return;
   int N = k.N[inst];
-  if (inst_class(N) != (SMEM ? 1 : 2)) return;
+  if (k.cls[inst] != (SMEM ? 1 : 2)) return;
   if (SMEM && k.has_fstream && k.fstream[inst]) return;  // streamed factorisation
   __shared__ double red[NT / 32 + 1];
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -399,7 +394,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, L
   int inst = blockIdx.x;
   if (!run[inst] || !ok[inst]) return;
   int N = k.N[inst];
-  if (inst_class(N) != (SMEM ? 1 : 2)) return;
+  if (k.cls[inst] != (SMEM ? 1 : 2)) return;
   __shared__ double red[NT / 32 + 1];
   extern __shared__ __align__(16) unsigned char sm_raw[];
   int vo = k.voff[inst], po = k.poff[inst];
@@ -497,14 +492,19 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
 // its start up to A / B, including lower lanes and, for a segment continued
 // from the previous chunk, the carry.  The lane scan runs over each lane's
 // tail value (its part of B's segment); a lane adds lane l-d's value while
-// d does not pass the lane that holds the start of B's segment.
+// d does not pass the lane that holds the start of B's segment.  After the
+// steps d = 1 .. 2^(s-1) a lane has summed min(reach, 2^s - 1) lanes back, so
+// the chunk's nsteps (from its chunk word, the same on every lane) steps
+// complete every segment and the remaining steps are skipped.
 __device__ __forceinline__ void seg_scan2(double xA, double xB, int pA, int pB, int lane,
-                                          double carry, double &sA, double &sB) {
+                                          double carry, int nsteps, double &sA, double &sB) {
   if (lane == 0 && pA > 0) xA += carry;
   double v = pB > 0 ? xA + xB : xB;
   const int reach = pB > 0 ? lane - ((2 * lane + 1 - pB) >> 1) : 0;  // lanes back
 #pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
+  for (int s = 0; s < 5; ++s) {
+    if (s >= nsteps) break;
+    const int d = 1 << s;
     const double o = __shfl_up_sync(0xffffffffu, v, d);
     if (d <= reach && d <= lane) v += o;
   }
@@ -559,7 +559,9 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
       const int q = 32 * (blk + 2) + lane;
       d2 = q < nch ? chunks[q] : 0;
     }
-    const int cnt = (int)((word(c) >> kCntShift) & 63u) + 1;
+    const unsigned wc = word(c);
+    const int cnt = (int)((wc >> kCntShift) & 63u) + 1;
+    const int nsteps = (int)((wc >> kStepShift) & 7u);
     asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
     __syncwarp();
     const int slot = c & (kRing - 1);
@@ -570,7 +572,7 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
     const double xA = vA ? double(rv[slot * kChunk + eA]) * y[enA.y] : 0.0;
     const double xB = vB ? double(rv[slot * kChunk + eB]) * y[enB.y] : 0.0;
     double sA, sB;
-    seg_scan2(xA, xB, (enA.x >> 16) & 63, (enB.x >> 16) & 63, lane, carry, sA, sB);
+    seg_scan2(xA, xB, (enA.x >> 16) & 63, (enB.x >> 16) & 63, lane, carry, nsteps, sA, sB);
     if (vA && ((enA.x >> kLastBit) & 1)) {
       if (RESID)
         out[enA.x & 0xffff] = sA;
@@ -617,8 +619,8 @@ __global__ void __launch_bounds__(32, 24)
                      int ymax) {
   const int inst = k.order[blockIdx.x];
   if (!run[inst] || !ok[inst]) return;
+  if (k.cls[inst] != 1) return;
   const int N = k.N[inst];
-  if (inst_class(N) != 1) return;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   double *y = reinterpret_cast<double *>(sm_raw);
   int2 *re = reinterpret_cast<int2 *>(sm_raw + (((size_t)ymax * 8 + 15) & ~(size_t)15));
@@ -897,7 +899,8 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 4)
         const double xA = vA ? V[oA.y] * V[oA.z] * V[oA.w & 0xffff] : 0.0;
         const double xB = vB ? V[oB.y] * V[oB.z] * V[oB.w & 0xffff] : 0.0;
         double sA, sB;
-        seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry, sA, sB);
+        seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
+                  (int)((w >> kStepShift) & 7u), sA, sB);
         if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] -= sA;
         if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] -= sB;
         const int ll = (cnt - 1) >> 1;
@@ -961,7 +964,7 @@ static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, i
   if (k.has_fstream)
     k_ldl_factor_stream<T><<<k.fpack_blocks, 32 * kFactorWarps, k.fpack_smem, st>>>(
         k, p, run, ok, eps_out);
-  if (k.has_small)
+  if (k.has_small_legacy)
     k_ldl_factor<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
   if (k.has_large)
     k_ldl_factor<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, ok, eps_out);

@@ -53,12 +53,12 @@ struct KKTDev {
   const int *fpos, *bpos, *flev, *blev;
   void *LxF, *LxB;
   // Entry encoding of the three streams (single-warp instances only):
-  //   .x = segment | min(position in segment, 31) << 16 | last-of-segment << 21
+  //   .x = segment | min(position in segment, 63) << 16 | last-of-segment << 22
   //   .y = gathered index
-  // Chunk tables: a pass is a list of chunks of <= 32 consecutive entries of
-  // one level; chunk word = start relative to the instance's stream base
-  // (bits 0..25) | (count - 1) << 26.  Instance i's chunks of the forward,
-  // backward and residual passes are fch[fch_off[i] .. fch_off[i+1]) etc.
+  // Chunk tables: a pass is a list of chunks of <= kChunk consecutive entries
+  // of one level, encoded as described below.  Instance i's chunks of the
+  // forward, backward and residual passes are fch[fch_off[i] .. fch_off[i+1])
+  // etc.
   const int *fch, *bch, *kch, *fch_off, *bch_off, *kch_off;
   // Streamed factorisation (single-warp instances whose N + nnz(L) FP64
   // values fit in shared memory, fstream[i] = 1).  The kernel keeps U = L D
@@ -66,10 +66,10 @@ struct KKTDev {
   // memory.  Per level of the elimination tree the op stream lists, sorted
   // by target, every update
   //     V[t] -= V[a] * V[b] * V[k]   (U(i,k) U(j,k) / d_k into U(i,j) or d_j)
-  // as int4 {t, a, b, k | position-in-segment << 16 | last << 21}, followed
+  // as int4 {t, a, b, k | position-in-segment << 16 | last << 22}, followed
   // by the level's pivots {j, sign, 0, 0}.  Indices address the shared
-  // array [d or 1/d (N) | U (nnz(L))].  Chunk words: start relative to
-  // fop_base[i] (bits 0..25) | (count - 1) << 26 | pivot chunk << 31.
+  // array [d or 1/d (N) | U (nnz(L))].  Chunk words as below, start relative
+  // to fop_base[i], with the pivot-chunk bit.
   // Lkpos: KKT position of every L entry (-1: structural zero).
   const int *fstream, *fop_base, *foch, *foch_off, *Lkpos;
   const int4 *fop;
@@ -88,8 +88,12 @@ struct KKTDev {
   // profiling only (else null): per instance, algorithmic bytes moved by the
   // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
   double *prof_bytes;
+  // [B] kernel class: 1 = single warp (work vector in shared memory, the
+  // streams above), 2 = block kernels with global scratch
+  const int *cls;
   int max_small_N;       // largest N among single-warp (shared memory) instances
   int has_small, has_large;
+  int has_small_legacy;  // single-warp instances without a streamed factorisation
   // scratch (global, per instance, sum N each)
   double *w;       // dense factor accumulator (large instances)
   double *yf;      // substitution work vector (large instances)
@@ -103,14 +107,39 @@ struct KKTDev {
 // Stream chunking shared by the setup and the kernels: a chunk holds up to
 // kChunk consecutive entries of one level, two per lane.  Entry word:
 // segment (bits 0..15) | min(position in segment, 63) << 16 | last << 22.
-// Chunk word: start (bits 0..24) | (count - 1) << 25 | pivot chunk << 31.
+// Chunk word: start (bits 0..21) | scan steps << 22 | (count - 1) << 25 |
+// pivot chunk << 31.  "Scan steps" (0..5) is how many doubling steps of the
+// segmented warp scan the chunk needs: the steps d = 1, 2, 4, ... up to the
+// farthest any lane reaches back to the start of its segment; later steps
+// would add nothing.  Streams of a single-warp instance are therefore at
+// most kStartMask entries long (longer ones take the block kernels).
 constexpr int kChunk = 64;
 constexpr int kRingSlots = 4;          // chunks in flight per warp (power of two)
 constexpr int kFactorWarps = 4;        // instances per streamed-factorisation block
 constexpr int kPosMax = 63;
 constexpr int kLastBit = 22;
+constexpr int kStepShift = 22;
 constexpr int kCntShift = 25;
-constexpr unsigned kStartMask = (1u << 25) - 1u;
+constexpr unsigned kStartMask = (1u << 22) - 1u;
+
+// Scan steps of a chunk whose cnt entries have segment positions pos(e)
+// (clamped to kPosMax): lane l holds entries 2l and 2l + 1 and reaches back
+// min(l, l - ((2l + 1 - pos(2l + 1)) >> 1)) lanes when pos(2l + 1) > 0.
+template <typename PosOf>
+inline int chunk_scan_steps(int cnt, PosOf pos) {
+  int reach = 0;
+  for (int l = 0; 2 * l + 1 < cnt; ++l) {
+    const int pB = pos(2 * l + 1);
+    if (pB > 0) {
+      int r = l - ((2 * l + 1 - pB) >> 1);
+      if (r > l) r = l;
+      if (r > reach) reach = r;
+    }
+  }
+  int steps = 0;
+  for (int d = 1; d <= 16 && d <= reach; d <<= 1) ++steps;
+  return steps;
+}
 
 struct LDLParams {
   int static_reg;
