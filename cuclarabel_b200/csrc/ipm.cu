@@ -976,6 +976,43 @@ static std::vector<long long> prefix(const std::vector<T> &counts) {
 // Concatenates the prepared instances into the batch layout and uploads it.
 // Every per-instance copy runs on nth host threads: offsets first (prefix
 // sums over instances), then each instance fills its own disjoint slices.
+// First-fit-decreasing packing of instances into blocks of `slots` warps:
+// items in decreasing order of need (stable), each placed in the first block
+// with a free slot and room for it; a block's needs sum to at most cap.
+// pinst / poff receive per slot the instance (-1: idle) and its byte offset in
+// the block's shared memory.  Returns the number of blocks.
+template <typename Need>
+static int ffd_pack(std::vector<int> items, Need need, long long cap, int slots,
+                    std::vector<int> &pinst, std::vector<int> &poff) {
+  std::stable_sort(items.begin(), items.end(), [&](int a, int b) { return need(a) > need(b); });
+  std::vector<long long> used;
+  std::vector<int> cnt;
+  pinst.clear();
+  poff.clear();
+  size_t first_open = 0;
+  for (int i : items) {
+    const long long s_i = need(i);
+    size_t b = first_open;
+    while (b < used.size() && (cnt[b] == slots || used[b] + s_i > cap)) ++b;
+    if (b == used.size()) {
+      used.push_back(0);
+      cnt.push_back(0);
+      for (int w = 0; w < slots; ++w) {
+        pinst.push_back(-1);
+        poff.push_back(0);
+      }
+    }
+    pinst[(size_t)slots * b + cnt[b]] = i;
+    poff[(size_t)slots * b + cnt[b]] = (int)used[b];
+    used[b] += s_i;
+    ++cnt[b];
+    while (first_open < used.size() &&
+           (cnt[first_open] == slots || used[first_open] + need(items.back()) > cap))
+      ++first_open;
+  }
+  return (int)used.size();
+}
+
 static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   DevArena &A = h->arena;
   const int B = (int)prep.size();
@@ -1452,22 +1489,22 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   hvec<int2> fent((size_t)lnz), bent((size_t)lnz), kent((size_t)knz);
   hvec<int> fpos((size_t)lnz), bpos((size_t)lnz), flev(lvl_ptr.size()), blev(lvl_ptr.size());
   std::vector<int> nchf(B, 0), nchb(B, 0), nchk(B, 0);
-  // encode segment positions: .x = seg | min(pos, kPosMax) << 16 | last << kLastBit
+  // encode segment positions: .x = seg | min(pos, kSPosMax) << 16 | last << kSLastBit
   auto encode = [](int2 *e, long long n) {
     long long q = 0;
     while (q < n) {
       long long r = q;
       while (r + 1 < n && e[r + 1].x == e[q].x) ++r;
       for (long long t = q; t <= r; ++t) {
-        const int pos = (int)std::min<long long>(t - q, kPosMax);
-        e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << kLastBit);
+        const int pos = (int)std::min<long long>(t - q, kSPosMax);
+        e[t].x = (e[t].x & 0xffff) | (pos << 16) | ((t == r ? 1 : 0) << kSLastBit);
       }
       q = r + 1;
     }
   };
   auto nchunks = [](const int *lev, int nl) {
     int n = 0;
-    for (int l = 0; l < nl; ++l) n += (lev[l + 1] - lev[l] + kChunk - 1) / kChunk;
+    for (int l = 0; l < nl; ++l) n += (lev[l + 1] - lev[l] + kSChunk - 1) / kSChunk;
     return n;
   };
   par_for(B, nth, [&](int i) {
@@ -1510,7 +1547,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       encode(kent.data() + kbase, (long long)p.Kj.size());
       nchf[i] = nchunks(flev.data() + lvl_off[i], nl);
       nchb[i] = nchunks(blev.data() + lvl_off[i], nl);
-      nchk[i] = ((int)p.Kj.size() + kChunk - 1) / kChunk;
+      nchk[i] = ((int)p.Kj.size() + kSChunk - 1) / kSChunk;
     }
   });
   // chunk tables: start relative to the stream base | scan steps <<
@@ -1526,10 +1563,10 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   par_for(B, nth, [&](int i) {
     auto put = [](int *out, const int *lev, int nl, long long base, const int2 *ent) {
       for (int l = 0; l < nl; ++l)
-        for (long long c = lev[l]; c < lev[l + 1]; c += kChunk) {
-          const int cnt = (int)std::min<long long>(kChunk, lev[l + 1] - c);
-          const int steps =
-              chunk_scan_steps(cnt, [&](int e) { return (ent[c + e].x >> 16) & kPosMax; });
+        for (long long c = lev[l]; c < lev[l + 1]; c += kSChunk) {
+          const int cnt = (int)std::min<long long>(kSChunk, lev[l + 1] - c);
+          const int steps = chunk_scan_steps<kSK>(
+              cnt, [&](int e) { return (ent[c + e].x >> 16) & kSPosMax; });
           *out++ = (int)((c - base) | ((long long)steps << kStepShift) |
                          ((long long)(cnt - 1) << kCntShift));
         }
@@ -1542,14 +1579,14 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     put(kch.data() + okch[i], klev, 1, kbase, kent.data());
   });
   // setup statistics (verbose): scan steps per chunk of each stream kind
-  auto step_stats = [&](const char *name, const int *w, size_t n) {
+  auto step_stats = [&](const char *name, const int *w, size_t n, bool factor) {
     if (!h->st.verbose) return;
     long long hist[8] = {0, 0, 0, 0, 0, 0, 0, 0}, nc = 0, ne = 0;
     for (size_t c = 0; c < n; ++c) {
-      if ((unsigned)w[c] >> 31) continue;  // pivot chunks take no scan
+      if (factor && ((unsigned)w[c] >> 31)) continue;  // pivot chunks take no scan
       ++hist[((unsigned)w[c] >> kStepShift) & 7u];
       ++nc;
-      ne += (((unsigned)w[c] >> kCntShift) & 63u) + 1;
+      ne += (((unsigned)w[c] >> kCntShift) & (factor ? 63u : 127u)) + 1;
     }
     double mean = 0;
     for (int q = 0; q < 8; ++q) mean += q * (double)hist[q];
@@ -1559,9 +1596,9 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
                  name, nc, nc ? (double)ne / nc : 0.0, nc ? mean / nc : 0.0, hist[0], hist[1],
                  hist[2], hist[3], hist[4], hist[5]);
   };
-  step_stats("fwd", fch.data(), fch.size());
-  step_stats("bwd", bch.data(), bch.size());
-  step_stats("resid", kch.data(), kch.size());
+  step_stats("fwd", fch.data(), fch.size(), false);
+  step_stats("bwd", bch.data(), bch.size(), false);
+  step_stats("resid", kch.data(), kch.size(), false);
   // streamed factorisation: op streams, pivots and chunk tables
   {
     constexpr long long kFactorSmemBytes = 96 * 1024;
@@ -1628,7 +1665,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
         for (long long c = start; c < (long long)ops.size(); c += kChunk) {
           const int cnt = (int)std::min<long long>(kChunk, (long long)ops.size() - c);
           const int steps =
-              chunk_scan_steps(cnt, [&](int e) { return (ops[c + e].w >> 16) & kPosMax; });
+              chunk_scan_steps<2>(cnt, [&](int e) { return (ops[c + e].w >> 16) & kPosMax; });
           chk.push_back((int)(c | ((long long)steps << kStepShift) |
                               ((long long)(cnt - 1) << kCntShift)));
         }
@@ -1676,7 +1713,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       std::copy(ich[i].begin(), ich[i].end(), foch.begin() + och[i]);
       std::vector<int4>().swap(iops[i]);
     });
-    step_stats("factor", foch.data(), foch.size());
+    step_stats("factor", foch.data(), foch.size(), true);
     kk.fstream = A.upload(fs);
     kk.fop_base = A.upload(fop_base);
     kk.foch = A.upload(foch);
@@ -1688,57 +1725,43 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kk.has_small_legacy = 0;
     for (int i = 0; i < B; ++i)
       if (cls[i] == 1 && !fs[i]) kk.has_small_legacy = 1;
-    // pack streamed instances into blocks of kFactorWarps warps: first fit by
-    // decreasing shared-memory need, bins as large as the largest need
+    // pack streamed instances into blocks of kFactorWarps warps, bins as
+    // large as the largest need
     {
       auto need = [&](int i) {
         return ((((long long)N[i] + (long long)prep[i].Li.size()) * 8 + 15) & ~15LL) +
                (long long)kRingSlots * kChunk * 16;
       };
-      std::vector<int> items;
+      std::vector<int> items, pinst, poffv;
       for (int i = 0; i < B; ++i)
         if (fs[i]) items.push_back(i);
-      std::stable_sort(items.begin(), items.end(), [&](int a, int b) { return need(a) > need(b); });
-      const long long cap = items.empty() ? 0 : need(items[0]);
-      std::vector<long long> used;
-      std::vector<int> cnt, pinst, poffv;
-      size_t first_open = 0;
-      for (int i : items) {
-        const long long s_i = need(i);
-        size_t b = first_open;
-        while (b < used.size() && (cnt[b] == kFactorWarps || used[b] + s_i > cap)) ++b;
-        if (b == used.size()) {
-          used.push_back(0);
-          cnt.push_back(0);
-          for (int w = 0; w < kFactorWarps; ++w) {
-            pinst.push_back(-1);
-            poffv.push_back(0);
-          }
-        }
-        pinst[kFactorWarps * b + cnt[b]] = i;
-        poffv[kFactorWarps * b + cnt[b]] = (int)used[b];
-        used[b] += s_i;
-        ++cnt[b];
-        while (first_open < used.size() &&
-               (cnt[first_open] == kFactorWarps || used[first_open] + need(items.back()) > cap))
-          ++first_open;
-      }
+      long long cap = 0;
+      for (int i : items) cap = std::max(cap, need(i));
+      kk.fpack_blocks = ffd_pack(items, need, cap, kFactorWarps, pinst, poffv);
       kk.fpack_inst = A.upload(pinst);
       kk.fpack_off = A.upload(poffv);
-      kk.fpack_blocks = (int)used.size();
       kk.fpack_smem = (int)cap;
     }
   }
-  {
-    std::vector<int> order(B);
-    for (int i = 0; i < B; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-      return (long long)N[a] + (long long)prep[a].Li.size() >
-             (long long)N[b] + (long long)prep[b].Li.size();
-    });
-    kk.order = A.upload(order);
-  }
   kk.cls = A.upload(cls);
+  // pack single-warp solves into blocks of kSolveWarps warps: each warp needs
+  // its work vector (N FP64 values) and its ring (entries + FP64 values);
+  // bins sized so kSolveBlocksPerSM blocks fit an SM's shared memory
+  {
+    auto need = [&](int i) {
+      return (((long long)N[i] * 8 + 15) & ~15LL) +
+             (long long)kSRingSlots * kSChunk * (long long)(sizeof(int2) + sizeof(double));
+    };
+    std::vector<int> items, pinst, poffv;
+    for (int i = 0; i < B; ++i)
+      if (cls[i] == 1) items.push_back(i);
+    long long cap = ((228LL * 1024) / kSolveBlocksPerSM - 1024) & ~15LL;
+    for (int i : items) cap = std::max(cap, need(i));
+    kk.spack_blocks = ffd_pack(items, need, cap, kSolveWarps, pinst, poffv);
+    kk.spack_inst = A.upload(pinst);
+    kk.spack_off = A.upload(poffv);
+    kk.spack_smem = (int)cap;
+  }
   kk.fch = A.upload(fch);
   kk.bch = A.upload(bch);
   kk.kch = A.upload(kch);

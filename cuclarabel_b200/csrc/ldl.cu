@@ -467,9 +467,9 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, L
 
 // ------------------------------------------------------------------------
 // Single-warp solve.  Each substitution pass, and the refinement residual,
-// streams its nonzeros in chunks of at most 32 entries of one level.  None
-// of a chunk's entries or values depends on earlier results, so they are
-// copied into a shared-memory ring kRing chunks ahead with cp.async: the
+// streams its nonzeros in chunks of at most kSChunk entries of one level.
+// None of a chunk's entries or values depends on earlier results, so they
+// are copied into a shared-memory ring kSRing chunks ahead with cp.async: the
 // warp's global-memory latency overlaps the reduction of the chunks before.
 // Within a chunk the products are summed per segment (a node of the pass,
 // or a KKT row) by a segmented warp scan; a segment running into the next
@@ -479,6 +479,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, L
 // order depends only on the instance's own layout, never on the batch.
 
 constexpr int kRing = kRingSlots;
+constexpr int kSRing = kSRingSlots;
 
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
@@ -513,15 +514,69 @@ __device__ __forceinline__ void seg_scan2(double xA, double xB, int pA, int pB, 
   sA = xA + ((pA > 0 && lane > 0) ? prev : 0.0);
 }
 
+// Segmented sums of one solve chunk held kSK consecutive entries per lane
+// (entries kSK lane .. kSK lane + kSK - 1), with products x and positions in
+// their segments p (clamped to kSPosMax, zero for entries past the chunk).
+// Returns s: for every entry the sum of its segment from the segment's start
+// up to the entry, including lower lanes and, for a segment continued from
+// the previous chunk, the carry.  Each lane first sums its own entries
+// (a segment restarts where p = 0), the lane scan then runs over each lane's
+// tail value with the reach rule of seg_scan2, and an entry whose segment
+// began below its lane (p > its index in the lane) adds the lower lane's
+// total.  nsteps doubling steps complete every segment of the chunk.
+__device__ __forceinline__ void seg_scan4(double (&x)[kSK], const int (&p)[kSK], int lane,
+                                          double carry, int nsteps, double (&s)[kSK]) {
+  if (lane == 0 && p[0] > 0) x[0] += carry;
+  s[0] = x[0];
+#pragma unroll
+  for (int j = 1; j < kSK; ++j) s[j] = p[j] > 0 ? s[j - 1] + x[j] : x[j];
+  double v = s[kSK - 1];
+  const int pt = p[kSK - 1];
+  const int reach = pt > 0 ? lane - ((kSK * lane + kSK - 1 - pt) >> kSKShift) : 0;
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    if (t >= nsteps) break;
+    const int d = 1 << t;
+    const double o = __shfl_up_sync(0xffffffffu, v, d);
+    if (d <= reach && d <= lane) v += o;
+  }
+  const double prev = __shfl_up_sync(0xffffffffu, v, 1);
+#pragma unroll
+  for (int j = 0; j < kSK - 1; ++j)
+    if (p[j] > j && lane > 0) s[j] += prev;
+  s[kSK - 1] = v;
+}
+
+// kSK consecutive values of the ring as FP64 (two 16-byte or one 16-byte
+// shared load)
+__device__ __forceinline__ void ring_vals(const double *rv, double (&v)[kSK]) {
+  const double2 a = reinterpret_cast<const double2 *>(rv)[0];
+  const double2 b = reinterpret_cast<const double2 *>(rv)[1];
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+__device__ __forceinline__ void ring_vals(const float *rv, double (&v)[kSK]) {
+  const float4 a = *reinterpret_cast<const float4 *>(rv);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+
 // One pass over an encoded stream (entries ent / values val from stream
 // position base), chunk by chunk as listed in chunks[0..nch):
 //   RESID = false:  y[seg] -= sum val * y[idx]     (out == y)
 //   RESID = true:   out[seg] = sum val * y[idx]
 // Chunk words are read 32 at a time, one per lane, two blocks ahead of use.
+// The ring copies are coalesced (lane l copies entries l, l + 32, ...); each
+// lane then reads its kSK consecutive entries with 16-byte shared loads.
 template <typename T, bool RESID>
 __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
                           const int2 *__restrict__ ent, const T *__restrict__ val,
                           const double *y, double *out, int2 *re, T *rv, int lane) {
+  static_assert(kSK == 4, "ring_pass reads four entries per lane");
   const unsigned full = 0xffffffffu;
   if (nch == 0) return;
   int d0 = lane < nch ? chunks[lane] : 0;
@@ -536,20 +591,22 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
     if (c < nch) {
       const unsigned w = word(c);
       const int p = base + (int)(w & kStartMask);
-      const int cnt = (int)((w >> kCntShift) & 63u) + 1;
+      const int cnt = (int)((w >> kCntShift) & 127u) + 1;
+      int2 *rd = re + slot * kSChunk;
+      T *vd = rv + slot * kSChunk;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int e = 2 * lane + h;
+      for (int h = 0; h < kSK; ++h) {
+        const int e = lane + 32 * h;
         if (e < cnt) {
-          cp_async<8>(&re[slot * kChunk + e], &ent[p + e]);
-          cp_async<sizeof(T)>(&rv[slot * kChunk + e], &val[p + e]);
+          cp_async<8>(&rd[e], &ent[p + e]);
+          cp_async<sizeof(T)>(&vd[e], &val[p + e]);
         }
       }
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
 #pragma unroll
-  for (int c = 0; c < kRing; ++c) issue(c, c);
+  for (int c = 0; c < kSRing; ++c) issue(c, c);
   double carry = 0.0;
   for (int c = 0; c < nch; ++c) {
     if (c > 0 && (c & 31) == 0) {
@@ -560,37 +617,42 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
       d2 = q < nch ? chunks[q] : 0;
     }
     const unsigned wc = word(c);
-    const int cnt = (int)((wc >> kCntShift) & 63u) + 1;
+    const int cnt = (int)((wc >> kCntShift) & 127u) + 1;
     const int nsteps = (int)((wc >> kStepShift) & 7u);
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kSRing - 1));
     __syncwarp();
-    const int slot = c & (kRing - 1);
-    const int eA = 2 * lane, eB = eA + 1;
-    const bool vA = eA < cnt, vB = eB < cnt;
-    const int2 enA = vA ? re[slot * kChunk + eA] : make_int2(0, 0);
-    const int2 enB = vB ? re[slot * kChunk + eB] : make_int2(0, 0);
-    const double xA = vA ? double(rv[slot * kChunk + eA]) * y[enA.y] : 0.0;
-    const double xB = vB ? double(rv[slot * kChunk + eB]) * y[enB.y] : 0.0;
-    double sA, sB;
-    seg_scan2(xA, xB, (enA.x >> 16) & 63, (enB.x >> 16) & 63, lane, carry, nsteps, sA, sB);
-    if (vA && ((enA.x >> kLastBit) & 1)) {
-      if (RESID)
-        out[enA.x & 0xffff] = sA;
-      else
-        out[enA.x & 0xffff] -= sA;
+    const int slot = c & (kSRing - 1);
+    const int4 *r4 = reinterpret_cast<const int4 *>(re + slot * kSChunk + kSK * lane);
+    const int4 ea = r4[0], eb = r4[1];
+    const int sg[kSK] = {ea.x, ea.z, eb.x, eb.z};
+    const int ix[kSK] = {ea.y, ea.w, eb.y, eb.w};
+    double vv[kSK];
+    ring_vals(rv + slot * kSChunk + kSK * lane, vv);
+    double x[kSK], sm[kSK];
+    int p[kSK];
+#pragma unroll
+    for (int j = 0; j < kSK; ++j) {
+      const bool ok = kSK * lane + j < cnt;
+      p[j] = ok ? (sg[j] >> 16) & kSPosMax : 0;
+      const double yv = y[ok ? ix[j] : 0];
+      x[j] = ok ? vv[j] * yv : 0.0;
     }
-    if (vB && ((enB.x >> kLastBit) & 1)) {
-      if (RESID)
-        out[enB.x & 0xffff] = sB;
-      else
-        out[enB.x & 0xffff] -= sB;
-    }
+    seg_scan4(x, p, lane, carry, nsteps, sm);
+#pragma unroll
+    for (int j = 0; j < kSK; ++j)
+      if (kSK * lane + j < cnt && ((sg[j] >> kSLastBit) & 1)) {
+        if (RESID)
+          out[sg[j] & 0xffff] = sm[j];
+        else
+          out[sg[j] & 0xffff] -= sm[j];
+      }
     // partial sum of the segment of the chunk's last entry (used by the next
     // chunk only if its first entry continues that segment)
-    const int ll = (cnt - 1) >> 1;
-    carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
+    const int jl = (cnt - 1) & (kSK - 1);
+    const double cs = jl == 0 ? sm[0] : jl == 1 ? sm[1] : jl == 2 ? sm[2] : sm[3];
+    carry = __shfl_sync(full, cs, (cnt - 1) >> kSKShift);
     __syncwarp();
-    issue(c + kRing, slot);
+    issue(c + kSRing, slot);
   }
   asm volatile("cp.async.wait_all;\n" ::);
   __syncwarp();
@@ -612,20 +674,23 @@ constexpr int kVecU = 8;
     }                                                             \
   }
 
+// Warps of a block solve different instances (the packing tables); they
+// share nothing but the block's shared memory, each in its own slice, and
+// never synchronise with one another.
 template <typename T>
-__global__ void __launch_bounds__(32, 24)
+__global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
     k_ldl_solve_warp(KKTDev k, LDLParams prm, const int *run, const double *__restrict__ rx,
-                     const double *__restrict__ rz, double *lx, double *lz, int *ok,
-                     int ymax) {
-  const int inst = k.order[blockIdx.x];
-  if (!run[inst] || !ok[inst]) return;
-  if (k.cls[inst] != 1) return;
+                     const double *__restrict__ rz, double *lx, double *lz, int *ok) {
+  const int slot = blockIdx.x * kSolveWarps + (threadIdx.x >> 5);
+  const int inst = k.spack_inst[slot];
+  if (inst < 0 || !run[inst] || !ok[inst]) return;
   const int N = k.N[inst];
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  double *y = reinterpret_cast<double *>(sm_raw);
-  int2 *re = reinterpret_cast<int2 *>(sm_raw + (((size_t)ymax * 8 + 15) & ~(size_t)15));
-  T *rv = reinterpret_cast<T *>(re + kRing * kChunk);
-  const int vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x;
+  unsigned char *smw = sm_raw + k.spack_off[slot];
+  double *y = reinterpret_cast<double *>(smw);
+  int2 *re = reinterpret_cast<int2 *>(smw + (((size_t)N * 8 + 15) & ~(size_t)15));
+  T *rv = reinterpret_cast<T *>(re + kSRing * kSChunk);
+  const int vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x & 31;
   double *__restrict__ b = k.b + vo;
   double *__restrict__ x = k.x + vo;
   double *__restrict__ e = k.e + vo;
@@ -973,13 +1038,9 @@ template <typename T>
 static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
                          const double *rx, const double *rz, double *lx, double *lz, int *ok,
                          cudaStream_t st) {
-  size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
-  if (k.has_small) {
-    // y, then the cp.async ring (entries + values, FP64 values for the residual)
-    const size_t smw = sm + (size_t)kRing * kChunk * (sizeof(int2) + sizeof(double));
-    k_ldl_solve_warp<T><<<k.B, kSmallNT, smw, st>>>(k, p, run, rx, rz, lx, lz, ok,
-                                                     k.max_small_N);
-  }
+  if (k.has_small)
+    k_ldl_solve_warp<T><<<k.spack_blocks, 32 * kSolveWarps, k.spack_smem, st>>>(
+        k, p, run, rx, rz, lx, lz, ok);
   if (k.has_large)
     k_ldl_solve<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, rx, rz, lx, lz, ok);
 }
@@ -995,11 +1056,21 @@ static void set_attrs() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
-  const int ring_bytes = kRing * kChunk * (int)(sizeof(int2) + sizeof(double));
   cudaFuncSetAttribute(k_ldl_solve_warp<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSmemLimitBytes + 16 + ring_bytes);
+                       kSolveSmemMax);
   cudaFuncSetAttribute(k_ldl_solve_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSmemLimitBytes + 16 + ring_bytes);
+                       kSolveSmemMax);
+  // the packed kernels size their blocks for the SM's full shared memory
+  cudaFuncSetAttribute(k_ldl_solve_warp<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_ldl_solve_warp<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_ldl_factor_stream<double>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_ldl_factor_stream<float>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
   g_attr_done = true;
 }
 

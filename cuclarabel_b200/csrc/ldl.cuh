@@ -53,12 +53,12 @@ struct KKTDev {
   const int *fpos, *bpos, *flev, *blev;
   void *LxF, *LxB;
   // Entry encoding of the three streams (single-warp instances only):
-  //   .x = segment | min(position in segment, 63) << 16 | last-of-segment << 22
+  //   .x = segment | min(position in segment, kSPosMax) << 16 | last << kSLastBit
   //   .y = gathered index
-  // Chunk tables: a pass is a list of chunks of <= kChunk consecutive entries
-  // of one level, encoded as described below.  Instance i's chunks of the
-  // forward, backward and residual passes are fch[fch_off[i] .. fch_off[i+1])
-  // etc.
+  // Chunk tables: a pass is a list of chunks of <= kSChunk consecutive
+  // entries of one level, encoded as described below.  Instance i's chunks of
+  // the forward, backward and residual passes are fch[fch_off[i] ..
+  // fch_off[i+1]) etc.
   const int *fch, *bch, *kch, *fch_off, *bch_off, *kch_off;
   // Streamed factorisation (single-warp instances whose N + nnz(L) FP64
   // values fit in shared memory, fstream[i] = 1).  The kernel keeps U = L D
@@ -81,10 +81,13 @@ struct KKTDev {
   // fpack_off[...]; fpack_smem bytes per block.
   const int *fpack_inst, *fpack_off;
   int fpack_blocks, fpack_smem;
-  // launch order of the single-warp kernels: instances by decreasing size
-  // (N + nnz(L)), so the largest start in the first wave and the tail of the
-  // launch holds small ones
-  const int *order;
+  // Packing of single-warp solves into blocks of kSolveWarps warps (first fit
+  // by decreasing shared-memory need: the work vector y, N FP64 values, plus
+  // the warp's ring): warp w of block b solves spack_inst[kSolveWarps b + w]
+  // (-1: idle) with its shared memory at byte spack_off[...]; spack_smem
+  // bytes per block.
+  const int *spack_inst, *spack_off;
+  int spack_blocks, spack_smem;
   // profiling only (else null): per instance, algorithmic bytes moved by the
   // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
   double *prof_bytes;
@@ -104,34 +107,52 @@ struct KKTDev {
   double *b, *x, *e, *dx;
 };
 
-// Stream chunking shared by the setup and the kernels: a chunk holds up to
-// kChunk consecutive entries of one level, two per lane.  Entry word:
-// segment (bits 0..15) | min(position in segment, 63) << 16 | last << 22.
-// Chunk word: start (bits 0..21) | scan steps << 22 | (count - 1) << 25 |
-// pivot chunk << 31.  "Scan steps" (0..5) is how many doubling steps of the
-// segmented warp scan the chunk needs: the steps d = 1, 2, 4, ... up to the
-// farthest any lane reaches back to the start of its segment; later steps
-// would add nothing.  Streams of a single-warp instance are therefore at
-// most kStartMask entries long (longer ones take the block kernels).
-constexpr int kChunk = 64;
-constexpr int kRingSlots = 4;          // chunks in flight per warp (power of two)
-constexpr int kFactorWarps = 4;        // instances per streamed-factorisation block
-constexpr int kPosMax = 63;
-constexpr int kLastBit = 22;
+// Stream chunking shared by the setup and the kernels.  A chunk is a run of
+// consecutive entries of one level; lane l of the warp holds K consecutive
+// entries K l .. K l + K - 1 of it.  Chunk words carry the chunk's start
+// relative to the instance's stream base (bits 0..21), its "scan steps"
+// (bits 22..24) and its count - 1 (from bit 25).  Scan steps (0..5) is how
+// many doubling steps of the segmented warp scan the chunk needs: the steps
+// d = 1, 2, 4, ... up to the farthest any lane reaches back to the lane that
+// holds the start of its last entry's segment; later steps would add
+// nothing.  Streams of a single-warp instance are therefore at most
+// kStartMask entries long (longer ones take the block kernels).
+constexpr int kRingSlots = 4;          // factorisation chunks in flight per warp (power of two)
+constexpr int kSRingSlots = 2;         // solve chunks in flight per warp (power of two)
+constexpr int kSolveWarps = 4;         // instances per single-warp-solve block
+constexpr int kSolveBlocksPerSM = 5;   // solve blocks resident per SM (register budget)
+constexpr int kSolveSmemMax = 200 * 1024;  // dynamic shared memory cap of a solve block
 constexpr int kStepShift = 22;
 constexpr int kCntShift = 25;
 constexpr unsigned kStartMask = (1u << 22) - 1u;
+// Substitution and residual streams (single-warp solve): K = kSK entries per
+// lane; entry word segment (bits 0..15) | min(position in segment, kSPosMax)
+// << 16 | last-of-segment << kSLastBit; count - 1 in 7 bits.
+constexpr int kSK = 4;
+constexpr int kSKShift = 2;
+constexpr int kSChunk = 32 * kSK;
+constexpr int kSPosMax = 127;
+constexpr int kSLastBit = 23;
+static_assert((1 << kSKShift) == kSK && kSPosMax + 1 >= kSChunk, "solve chunk layout");
+// Factorisation op streams: K = 2 entries per lane; op word .w = k |
+// min(position in segment, kPosMax) << 16 | last << kLastBit; count - 1 in
+// 6 bits; bit 31 marks a pivot chunk.
+constexpr int kChunk = 64;
+constexpr int kFactorWarps = 4;        // instances per streamed-factorisation block
+constexpr int kPosMax = 63;
+constexpr int kLastBit = 22;
 
-// Scan steps of a chunk whose cnt entries have segment positions pos(e)
-// (clamped to kPosMax): lane l holds entries 2l and 2l + 1 and reaches back
-// min(l, l - ((2l + 1 - pos(2l + 1)) >> 1)) lanes when pos(2l + 1) > 0.
-template <typename PosOf>
+// Scan steps of a chunk of cnt entries, K per lane, whose segment positions
+// are pos(e) (clamped at or above the chunk length): lane l reaches back
+// min(l, l - floor((K l + K - 1 - p) / K)) lanes, p = pos(K l + K - 1) > 0.
+template <int K, typename PosOf>
 inline int chunk_scan_steps(int cnt, PosOf pos) {
   int reach = 0;
-  for (int l = 0; 2 * l + 1 < cnt; ++l) {
-    const int pB = pos(2 * l + 1);
-    if (pB > 0) {
-      int r = l - ((2 * l + 1 - pB) >> 1);
+  for (int l = 0; K * l + K - 1 < cnt; ++l) {
+    const int p = pos(K * l + K - 1);
+    if (p > 0) {
+      const int a = K * l + K - 1 - p;
+      int r = l - (a >= 0 ? a / K : -((-a + K - 1) / K));
       if (r > l) r = l;
       if (r > reach) reach = r;
     }
