@@ -15,6 +15,7 @@
 // an instance that would "break" sets done and is frozen.  All vector kernels
 // read the per-instance active mask.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -1599,14 +1600,18 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   step_stats("fwd", fch.data(), fch.size(), false);
   step_stats("bwd", bch.data(), bch.size(), false);
   step_stats("resid", kch.data(), kch.size(), false);
-  // streamed factorisation: op streams, pivots and chunk tables
+  // streamed factorisation: op streams, pivots and chunk tables, split over
+  // the kFactorWarps warps of the instance's block level by level
   {
     constexpr long long kFactorSmemBytes = 96 * 1024;
-    const long long ring_bytes = 4LL * kChunk * 16;
+    constexpr int W = kFactorWarps;
+    const long long ring_bytes = (long long)W * kFRingSlots * kChunk * 16;
     std::vector<int> fs(B, 0);
     std::vector<long long> nops(B, 0), nch(B, 0);
     std::vector<std::vector<int4>> iops(B);
     std::vector<std::vector<int>> ich(B);
+    std::vector<std::array<int, W + 1>> iwoff(B);
+    hvec<int> flcnt((size_t)lvof[B] * W);
     hvec<int> Lkpos((size_t)lnz);
     par_for(B, nth, [&](int i) {
       const auto &p = prep[i];
@@ -1623,11 +1628,26 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       if (cls[i] != 1 || (Ni + nli) * 8 + ring_bytes > kFactorSmemBytes) return;
       fs[i] = 1;
       auto &ops = iops[i];
-      auto &chk = ich[i];
       const int nl = nlev[i];
       const int *lp = p.lvl_ptr.data();
       std::vector<int4> lev;  // {target, a, b, k}
+      std::vector<std::vector<int>> wch(W);
+      std::vector<size_t> segs;
       bool bad = false;
+      // chunk ops[c0, c1) (all of one part) into warp w's list
+      auto put_chunks = [&](int w, long long c0, long long c1, bool pivot) {
+        int n = 0;
+        for (long long c = c0; c < c1; c += kChunk, ++n) {
+          const int cnt = (int)std::min<long long>(kChunk, c1 - c);
+          const int steps = pivot ? 0 : chunk_scan_steps<2>(cnt, [&](int e) {
+            return (ops[c + e].w >> 16) & kPosMax;
+          });
+          wch[w].push_back((int)(c | ((long long)steps << kStepShift) |
+                                 ((long long)(cnt - 1) << kCntShift) |
+                                 (pivot ? (long long)1 << 31 : 0LL)));
+        }
+        return n;
+      };
       for (int l = 0; l < nl && !bad; ++l) {
         lev.clear();
         for (int t = lp[l]; t < lp[l + 1]; ++t) {
@@ -1650,64 +1670,81 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
         }
         std::stable_sort(lev.begin(), lev.end(),
                          [](const int4 &a, const int4 &b) { return a.x < b.x; });
-        const long long start = (long long)ops.size();
-        for (size_t q = 0; q < lev.size();) {
-          size_t r = q;
-          while (r + 1 < lev.size() && lev[r + 1].x == lev[q].x) ++r;
-          for (size_t t = q; t <= r; ++t) {
-            const int pos = (int)std::min<size_t>(t - q, kPosMax);
-            int4 o = lev[t];
-            o.w = o.w | (pos << 16) | ((t == r ? 1 : 0) << kLastBit);
-            ops.push_back(o);
+        // segment starts (one segment per target), then W parts of about
+        // equal length whose boundaries are segment starts
+        segs.clear();
+        for (size_t q = 0; q < lev.size(); ++q)
+          if (q == 0 || lev[q].x != lev[q - 1].x) segs.push_back(q);
+        segs.push_back(lev.size());
+        size_t pb[W + 1];
+        pb[0] = 0;
+        pb[W] = lev.size();
+        for (int w = 1; w < W; ++w) {
+          const size_t ideal = lev.size() * (size_t)w / W;
+          const size_t s0 = *std::lower_bound(segs.begin(), segs.end(), ideal);
+          pb[w] = std::max(pb[w - 1], s0);
+        }
+        int nop[W], npv[W];
+        for (int w = 0; w < W; ++w) {
+          const long long start = (long long)ops.size();
+          for (size_t q = pb[w]; q < pb[w + 1];) {
+            size_t r = q;
+            while (r + 1 < pb[w + 1] && lev[r + 1].x == lev[q].x) ++r;
+            for (size_t t = q; t <= r; ++t) {
+              const int pos = (int)std::min<size_t>(t - q, kPosMax);
+              int4 o = lev[t];
+              o.w = o.w | (pos << 16) | ((t == r ? 1 : 0) << kLastBit);
+              ops.push_back(o);
+            }
+            q = r + 1;
           }
-          q = r + 1;
+          nop[w] = put_chunks(w, start, (long long)ops.size(), false);
         }
-        for (long long c = start; c < (long long)ops.size(); c += kChunk) {
-          const int cnt = (int)std::min<long long>(kChunk, (long long)ops.size() - c);
-          const int steps =
-              chunk_scan_steps<2>(cnt, [&](int e) { return (ops[c + e].w >> 16) & kPosMax; });
-          chk.push_back((int)(c | ((long long)steps << kStepShift) |
-                              ((long long)(cnt - 1) << kCntShift)));
+        // the level's pivots, in W contiguous parts
+        const int np = lp[l + 1] - lp[l];
+        for (int w = 0; w < W; ++w) {
+          const long long start = (long long)ops.size();
+          for (int t = lp[l] + np * w / W; t < lp[l] + np * (w + 1) / W; ++t) {
+            const int j = p.lvl_nodes[t];
+            ops.push_back(make_int4(j, (int)p.Dsign[j], 0, 0));
+          }
+          npv[w] = put_chunks(w, start, (long long)ops.size(), true);
         }
-        // the level's pivots
-        const long long ps = (long long)ops.size();
-        for (int t = lp[l]; t < lp[l + 1]; ++t) {
-          const int j = p.lvl_nodes[t];
-          ops.push_back(make_int4(j, (int)p.Dsign[j], 0, 0));
-        }
-        for (long long c = ps; c < (long long)ops.size(); c += kChunk) {
-          const long long cnt = std::min<long long>(kChunk, (long long)ops.size() - c);
-          chk.push_back((int)(c | ((cnt - 1) << kCntShift) | (1u << 31)));
+        for (int w = 0; w < W; ++w) {
+          if (nop[w] > 0xffff || npv[w] > 0xffff) bad = true;
+          flcnt[((size_t)lvl_off[i] + l) * W + w] = nop[w] | (npv[w] << 16);
         }
       }
       // a pattern mismatch is not reached for a valid symbolic factorisation;
       // an op stream longer than the chunk words address is; both fall back
       // to the level-scheduled single-warp factorisation
       if ((long long)ops.size() > (long long)kStartMask) bad = true;
+      auto &chk = ich[i];
+      iwoff[i][0] = 0;
+      for (int w = 0; w < W; ++w) {
+        chk.insert(chk.end(), wch[w].begin(), wch[w].end());
+        iwoff[i][w + 1] = (int)chk.size();
+      }
       if (bad) {
         fs[i] = 0;
         ops.clear();
         chk.clear();
+        for (int w = 0; w <= W; ++w) iwoff[i][w] = 0;
       }
       nops[i] = (long long)ops.size();
       nch[i] = (long long)chk.size();
     });
     const auto oop = prefix(nops), och = prefix(nch);
-    if (oop[B] > 2000000000LL) return -4;
+    if (oop[B] > 2000000000LL || och[B] > 2000000000LL) return -4;
     hvec<int4> fop(std::max<long long>(oop[B], 1));
     hvec<int> foch(std::max<long long>(och[B], 1));
-    std::vector<int> fop_base(B), foch_off(B + 1);
-    int fs_max = 0;
+    std::vector<int> fop_base(B), fwoff((size_t)B * (W + 1));
     bool any_fs = false;
     for (int i = 0; i < B; ++i) {
       fop_base[i] = (int)oop[i];
-      foch_off[i] = (int)och[i];
-      if (fs[i]) {
-        any_fs = true;
-        fs_max = std::max<int>(fs_max, N[i] + (int)prep[i].Li.size());
-      }
+      for (int w = 0; w <= W; ++w) fwoff[(size_t)i * (W + 1) + w] = (int)(och[i] + iwoff[i][w]);
+      if (fs[i]) any_fs = true;
     }
-    foch_off[B] = (int)och[B];
     par_for(B, nth, [&](int i) {
       std::copy(iops[i].begin(), iops[i].end(), fop.begin() + oop[i]);
       std::copy(ich[i].begin(), ich[i].end(), foch.begin() + och[i]);
@@ -1717,30 +1754,29 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kk.fstream = A.upload(fs);
     kk.fop_base = A.upload(fop_base);
     kk.foch = A.upload(foch);
-    kk.foch_off = A.upload(foch_off);
+    kk.fwoff = A.upload(fwoff);
+    kk.flcnt = A.upload(flcnt);
     kk.fop = A.upload(fop);
     kk.Lkpos = A.upload(Lkpos);
-    kk.fs_max = fs_max;
     kk.has_fstream = any_fs ? 1 : 0;
     kk.has_small_legacy = 0;
     for (int i = 0; i < B; ++i)
       if (cls[i] == 1 && !fs[i]) kk.has_small_legacy = 1;
-    // pack streamed instances into blocks of kFactorWarps warps, bins as
-    // large as the largest need
+    // launch list: streamed instances by decreasing shared-memory need (the
+    // largest start first); one block each, sized for the largest
     {
       auto need = [&](int i) {
         return ((((long long)N[i] + (long long)prep[i].Li.size()) * 8 + 15) & ~15LL) +
-               (long long)kRingSlots * kChunk * 16;
+               ring_bytes;
       };
-      std::vector<int> items, pinst, poffv;
+      std::vector<int> items;
       for (int i = 0; i < B; ++i)
         if (fs[i]) items.push_back(i);
-      long long cap = 0;
-      for (int i : items) cap = std::max(cap, need(i));
-      kk.fpack_blocks = ffd_pack(items, need, cap, kFactorWarps, pinst, poffv);
-      kk.fpack_inst = A.upload(pinst);
-      kk.fpack_off = A.upload(poffv);
-      kk.fpack_smem = (int)cap;
+      std::stable_sort(items.begin(), items.end(),
+                       [&](int a, int b) { return need(a) > need(b); });
+      kk.fs_count = (int)items.size();
+      kk.fs_smem = items.empty() ? 0 : (int)need(items[0]);
+      kk.fs_inst = A.upload(items);
     }
   }
   kk.cls = A.upload(cls);

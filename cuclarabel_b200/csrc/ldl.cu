@@ -478,7 +478,6 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_solve(KKTDev k, L
 // complete (__syncwarp) before the next level gathers them.  The summation
 // order depends only on the instance's own layout, never on the batch.
 
-constexpr int kRing = kRingSlots;
 constexpr int kSRing = kSRingSlots;
 
 template <int BYTES>
@@ -825,168 +824,185 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
 #undef VEC_LOOP
 
 // ------------------------------------------------------------------------
-// Streamed single-warp factorisation.  Shared memory holds V = [d_j, then
-// 1/d_j once pivot j is taken (N) | U = L D (nnz(L))], initialised from the
-// KKT matrix (static regularisation on the diagonal).  The instance's op
-// stream is copied kRing chunks ahead into a shared ring with cp.async; an op
-// chunk subtracts V[a] V[b] V[k] from V[t] through a segmented warp scan
-// (the carry rule of the substitutions), a pivot chunk takes the pivots of
-// one level (dynamic regularisation, D and D^-1 in the storage type, 1/d_j
-// kept in V).  Updates of a level only read columns and pivots of lower
-// levels, all final.  At the end L = U / d is written in CSC order and in the
-// two substitution-stream orders.
+// Streamed factorisation, one instance per block of kFactorWarps warps.
+// Shared memory holds V = [d_j, then 1/d_j once pivot j is taken (N) | U = L D
+// (nnz(L))], initialised from the KKT matrix (static regularisation on the
+// diagonal), and one cp.async ring per warp.  Each warp streams its own part
+// of every level: op chunks subtract V[a] V[b] V[k] from V[t] through a
+// segmented warp scan (the carry rule of the substitutions; a part never
+// splits a target's updates, so each V[t] has one writer), pivot chunks take
+// the warp's pivots of the level (dynamic regularisation, D and D^-1 in the
+// storage type, 1/d_j kept in V).  The block synchronises after a level's
+// updates (its pivots read them) and after its pivots (the next level's
+// updates read them).  Updates of a level only read columns and pivots of
+// lower levels, all final.  At the end L = U / d is written in CSC order and
+// in the two substitution-stream orders.
+constexpr int kFRing = kFRingSlots;
+
 template <typename T>
-__global__ void __launch_bounds__(32 * kFactorWarps, 4)
+__global__ void __launch_bounds__(32 * kFactorWarps, 6)
     k_ldl_factor_stream(KKTDev k, LDLParams prm, const int *run, int *ok, double *eps_out) {
-  // warps of a block factor different instances; they share nothing but the
-  // block's shared memory, each in its own slice, and never synchronise
-  const int slot = blockIdx.x * kFactorWarps + (threadIdx.x >> 5);
-  const int inst = k.fpack_inst[slot];
-  if (inst < 0 || !run[inst]) return;
+  constexpr int NT = 32 * kFactorWarps;
+  const int inst = k.fs_inst[blockIdx.x];
+  if (!run[inst]) return;  // the whole block
+  __shared__ double red[kFactorWarps + 1];
   const unsigned full = 0xffffffffu;
-  const int N = k.N[inst], vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = k.N[inst], vo = k.voff[inst], po = k.poff[inst];
   const int lbase = k.Lp[po], nl = k.Lp[po + N] - lbase;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  unsigned char *sm = sm_raw + k.fpack_off[slot];
-  double *V = reinterpret_cast<double *>(sm);
-  int4 *ring = reinterpret_cast<int4 *>(sm + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15));
+  double *V = reinterpret_cast<double *>(sm_raw);
+  int4 *ring = reinterpret_cast<int4 *>(sm_raw + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15)) +
+               warp * kFRing * kChunk;
   const signed char *sg = k.Dsign + vo;
   const int *Kdiag = k.Kdiag + vo;
   T *D = reinterpret_cast<T *>(k.D) + vo;
   T *Dinv = reinterpret_cast<T *>(k.Dinv) + vo;
-  // diagonal of K into V (loads of kU elements in flight per lane), then the
-  // static regularisation eps = c + prop * max |diag(K)| on it
+  // diagonal of K into V (loads of kU elements in flight per thread), then
+  // the static regularisation eps = c + prop * max |diag(K)| on it
   constexpr int kU = 8;
   double mx = 0.0;
-  for (int j0 = lane; j0 < N; j0 += 32 * kU) {
+  for (int j0 = tid; j0 < N; j0 += NT * kU) {
     int kd[kU];
     double kv[kU];
 #pragma unroll
-    for (int u = 0; u < kU; ++u) kd[u] = j0 + 32 * u < N ? Kdiag[j0 + 32 * u] : -1;
+    for (int u = 0; u < kU; ++u) kd[u] = j0 + NT * u < N ? Kdiag[j0 + NT * u] : -1;
 #pragma unroll
     for (int u = 0; u < kU; ++u) kv[u] = kd[u] >= 0 ? k.Kx[kd[u]] : 0.0;
 #pragma unroll
     for (int u = 0; u < kU; ++u)
       if (kd[u] >= 0) {
-        V[j0 + 32 * u] = kv[u];
+        V[j0 + NT * u] = kv[u];
         mx = fmax(mx, fabs(kv[u]));
       }
   }
   double eps = 0.0;
-  if (prm.static_reg) eps = prm.static_c + prm.static_prop * warp_max(mx);
-  __syncwarp();
-  for (int j = lane; j < N; j += 32) V[j] += sg[j] > 0 ? eps : -eps;
+  mx = block_max<NT>(mx, red);  // synchronises the block
+  if (prm.static_reg) eps = prm.static_c + prm.static_prop * mx;
+  for (int j = tid; j < N; j += NT) V[j] += sg[j] > 0 ? eps : -eps;
   {
     const int *kp = k.Lkpos + lbase;
     int pos[8];
-    for (int e0 = lane; e0 < nl; e0 += 32 * 8) {
+    for (int e0 = tid; e0 < nl; e0 += NT * 8) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) pos[u] = e0 + 32 * u < nl ? kp[e0 + 32 * u] : -1;
+      for (int u = 0; u < 8; ++u) pos[u] = e0 + NT * u < nl ? kp[e0 + NT * u] : -1;
 #pragma unroll
       for (int u = 0; u < 8; ++u)
-        if (e0 + 32 * u < nl) V[N + e0 + 32 * u] = pos[u] >= 0 ? k.Kx[pos[u]] : 0.0;
+        if (e0 + NT * u < nl) V[N + e0 + NT * u] = pos[u] >= 0 ? k.Kx[pos[u]] : 0.0;
     }
   }
-  __syncwarp();
-  // ---- the op / pivot stream
-  const int *chunks = k.foch + k.foch_off[inst];
-  const int nch = k.foch_off[inst + 1] - k.foch_off[inst];
+  __syncthreads();
+  // ---- this warp's op / pivot stream, level by level
+  const int *wo = k.fwoff + (size_t)inst * (kFactorWarps + 1);
+  const int *chunks = k.foch + wo[warp];
+  const int nch = wo[warp + 1] - wo[warp];
   const int4 *ops = k.fop + k.fop_base[inst];
+  const int *lc = k.flcnt + (size_t)k.lvl_off[inst] * kFactorWarps + warp;
+  const int nlev = k.nlev[inst];
   bool finite = true;
   double nent = 0.0;  // stream entries (profiling)
-  if (nch > 0) {
-    int d0 = lane < nch ? chunks[lane] : 0;
-    int d1 = lane + 32 < nch ? chunks[lane + 32] : 0;
-    int d2 = lane + 64 < nch ? chunks[lane + 64] : 0;
-    int blk = 0;
-    auto word = [&](int c) {
-      const int r = c - 32 * blk;
-      return __shfl_sync(full, r < 32 ? d0 : d1, r & 31);
-    };
-    auto issue = [&](int c, int slot) {
-      if (c < nch) {
-        const unsigned w = (unsigned)word(c);
-        const int p0 = (int)(w & kStartMask), cnt = (int)((w >> kCntShift) & 63u) + 1;
+  int d0 = lane < nch ? chunks[lane] : 0;
+  int d1 = lane + 32 < nch ? chunks[lane + 32] : 0;
+  int d2 = lane + 64 < nch ? chunks[lane + 64] : 0;
+  int blk = 0;
+  auto word = [&](int c) {
+    const int r = c - 32 * blk;
+    return (unsigned)__shfl_sync(full, r < 32 ? d0 : d1, r & 31);
+  };
+  auto issue = [&](int c, int slot) {
+    if (c < nch) {
+      const unsigned w = word(c);
+      const int p0 = (int)(w & kStartMask), cnt = (int)((w >> kCntShift) & 63u) + 1;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int e = 2 * lane + h;
-          if (e < cnt) {
-            const unsigned dst =
-                static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * kChunk + e]));
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
-                         "l"(&ops[p0 + e]));
-          }
+      for (int h = 0; h < 2; ++h) {
+        const int e = 2 * lane + h;
+        if (e < cnt) {
+          const unsigned dst =
+              static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * kChunk + e]));
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                       "l"(&ops[p0 + e]));
         }
       }
-      asm volatile("cp.async.commit_group;\n" ::);
-    };
-#pragma unroll
-    for (int c = 0; c < kRing; ++c) issue(c, c);
-    double carry = 0.0;
-    for (int c = 0; c < nch; ++c) {
-      if (c > 0 && (c & 31) == 0) {
-        ++blk;
-        d0 = d1;
-        d1 = d2;
-        const int q = 32 * (blk + 2) + lane;
-        d2 = q < nch ? chunks[q] : 0;
-      }
-      const unsigned w = (unsigned)word(c);
-      const int cnt = (int)((w >> kCntShift) & 63u) + 1;
-      const bool pivot = (w >> 31) != 0;
-      nent += cnt;
-      asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
-      __syncwarp();
-      const int slot = c & (kRing - 1);
-      const int eA = 2 * lane, eB = eA + 1;
-      const bool vA = eA < cnt, vB = eB < cnt;
-      const int4 oA = vA ? ring[slot * kChunk + eA] : make_int4(0, 0, 0, 0);
-      const int4 oB = vB ? ring[slot * kChunk + eB] : make_int4(0, 0, 0, 0);
-      if (pivot) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int4 o = h ? oB : oA;
-          if (h ? vB : vA) {
-            const int j = o.x;
-            const double dj = pivot_value(V[j], (signed char)o.y, prm);
-            const T djs = T(dj);
-            const T dis = T(1.0 / double(djs));
-            D[j] = djs;
-            Dinv[j] = dis;
-            const double r = 1.0 / dj;
-            if (!isfinite(r) || !isfinite(double(djs)) || !isfinite(double(dis)))
-              finite = false;
-            V[j] = r;
-          }
-        }
-        carry = 0.0;
-      } else {
-        const double xA = vA ? V[oA.y] * V[oA.z] * V[oA.w & 0xffff] : 0.0;
-        const double xB = vB ? V[oB.y] * V[oB.z] * V[oB.w & 0xffff] : 0.0;
-        double sA, sB;
-        seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
-                  (int)((w >> kStepShift) & 7u), sA, sB);
-        if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] -= sA;
-        if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] -= sB;
-        const int ll = (cnt - 1) >> 1;
-        carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
-      }
-      __syncwarp();
-      issue(c + kRing, slot);
     }
-    asm volatile("cp.async.wait_all;\n" ::);
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+#pragma unroll
+  for (int c = 0; c < kFRing; ++c) issue(c, c);
+  int c = 0;
+  double carry = 0.0;
+  // one chunk of the stream: updates (segmented scan, one write per target)
+  // or pivots
+  auto step = [&]() {
+    if (c >= nch) return;  // the level counts and the chunk list agree; never taken
+    if (c > 0 && (c & 31) == 0) {
+      ++blk;
+      d0 = d1;
+      d1 = d2;
+      const int q = 32 * (blk + 2) + lane;
+      d2 = q < nch ? chunks[q] : 0;
+    }
+    const unsigned w = word(c);
+    const int cnt = (int)((w >> kCntShift) & 63u) + 1;
+    const bool pivot = (w >> 31) != 0;
+    nent += cnt;
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kFRing - 1));
     __syncwarp();
+    const int slot = c & (kFRing - 1);
+    const int eA = 2 * lane, eB = eA + 1;
+    const bool vA = eA < cnt, vB = eB < cnt;
+    const int4 oA = vA ? ring[slot * kChunk + eA] : make_int4(0, 0, 0, 0);
+    const int4 oB = vB ? ring[slot * kChunk + eB] : make_int4(0, 0, 0, 0);
+    if (pivot) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int4 o = h ? oB : oA;
+        if (h ? vB : vA) {
+          const int j = o.x;
+          const double dj = pivot_value(V[j], (signed char)o.y, prm);
+          const T djs = T(dj);
+          const T dis = T(1.0 / double(djs));
+          D[j] = djs;
+          Dinv[j] = dis;
+          const double r = 1.0 / dj;
+          if (!isfinite(r) || !isfinite(double(djs)) || !isfinite(double(dis))) finite = false;
+          V[j] = r;
+        }
+      }
+      carry = 0.0;
+    } else {
+      const double xA = vA ? V[oA.y] * V[oA.z] * V[oA.w & 0xffff] : 0.0;
+      const double xB = vB ? V[oB.y] * V[oB.z] * V[oB.w & 0xffff] : 0.0;
+      double sA, sB;
+      seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
+                (int)((w >> kStepShift) & 7u), sA, sB);
+      if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] -= sA;
+      if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] -= sB;
+      const int ll = (cnt - 1) >> 1;
+      carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
+    }
+    __syncwarp();
+    issue(c + kFRing, slot);
+    ++c;
+  };
+  for (int l = 0; l < nlev; ++l) {
+    const int cw = lc[(size_t)l * kFactorWarps];
+    const int nop = cw & 0xffff, npv = (cw >> 16) & 0xffff;
+    for (int q = 0; q < nop; ++q) step();
+    __syncthreads();  // the level's updates before its pivots
+    for (int q = 0; q < npv; ++q) step();
+    __syncthreads();  // the level's pivots before the next level's updates
   }
+  asm volatile("cp.async.wait_all;\n" ::);
   // ---- L = U / d into CSC order and the two substitution-stream orders
   {
     T *Lx = reinterpret_cast<T *>(k.Lx), *LxF = reinterpret_cast<T *>(k.LxF),
       *LxB = reinterpret_cast<T *>(k.LxB);
-    for (int e0 = lane; e0 < nl; e0 += 32 * kU) {
+    for (int e0 = tid; e0 < nl; e0 += NT * kU) {
       int2 be[kU], fe[kU];
       int bq[kU], fq[kU];
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
-        const int e = e0 + 32 * u;
+        const int e = e0 + NT * u;
         if (e < nl) {
           be[u] = k.bent[lbase + e];
           bq[u] = k.bpos[lbase + e];
@@ -996,7 +1012,7 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 4)
       }
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
-        const int e = e0 + 32 * u;
+        const int e = e0 + NT * u;
         if (e < nl) {
           const double l = V[N + (bq[u] - lbase)] * V[be[u].x & 0xffff];
           Lx[bq[u]] = T(l);
@@ -1006,18 +1022,19 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 4)
       }
     }
   }
-  const bool bad = __any_sync(full, !finite);
-  if (lane == 0) {
+  const int bad = __syncthreads_or(finite ? 0 : 1);
+  if (k.prof_bytes && lane == 0) {
+    // the op stream (16 B per entry) and chunk words of this warp; thread 0
+    // adds the K diagonal and L-position values (8 + 4 B each), L written
+    // three times with the stream indices read, D and D^-1 written
+    const double ts = sizeof(T);
+    double by = 16.0 * nent + 4.0 * nch;
+    if (tid == 0) by += 12.0 * N + 12.0 * nl + nl * (3.0 * ts + 16.0) + 2.0 * ts * N;
+    atomicAdd(&k.prof_bytes[inst], by);
+  }
+  if (tid == 0) {
     if (bad) ok[inst] = 0;
     if (eps_out) eps_out[inst] = eps;
-    if (k.prof_bytes) {
-      // K diagonal and L-position values (8 + 4 B each), the op stream (16 B
-      // per entry), chunk words, L written three times with the stream
-      // indices read, D and D^-1 written
-      const double ts = sizeof(T);
-      k.prof_bytes[inst] += 12.0 * N + 12.0 * nl + 16.0 * nent + 4.0 * nch +
-                            nl * (3.0 * ts + 16.0) + 2.0 * ts * N;
-    }
   }
 }
 
@@ -1027,8 +1044,8 @@ static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, i
                           double *eps_out, cudaStream_t st) {
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
   if (k.has_fstream)
-    k_ldl_factor_stream<T><<<k.fpack_blocks, 32 * kFactorWarps, k.fpack_smem, st>>>(
-        k, p, run, ok, eps_out);
+    k_ldl_factor_stream<T><<<k.fs_count, 32 * kFactorWarps, k.fs_smem, st>>>(k, p, run, ok,
+                                                                           eps_out);
   if (k.has_small_legacy)
     k_ldl_factor<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
   if (k.has_large)

@@ -61,26 +61,26 @@ struct KKTDev {
   // fch_off[i+1]) etc.
   const int *fch, *bch, *kch, *fch_off, *bch_off, *kch_off;
   // Streamed factorisation (single-warp instances whose N + nnz(L) FP64
-  // values fit in shared memory, fstream[i] = 1).  The kernel keeps U = L D
-  // (column j of L times d_j) and, once pivot j is final, 1/d_j in shared
-  // memory.  Per level of the elimination tree the op stream lists, sorted
-  // by target, every update
+  // values fit in shared memory, fstream[i] = 1), one block of kFactorWarps
+  // warps per instance.  The block keeps U = L D (column j of L times d_j)
+  // and, once pivot j is final, 1/d_j in shared memory.  Per level of the
+  // elimination tree the op stream lists, sorted by target, every update
   //     V[t] -= V[a] * V[b] * V[k]   (U(i,k) U(j,k) / d_k into U(i,j) or d_j)
-  // as int4 {t, a, b, k | position-in-segment << 16 | last << 22}, followed
-  // by the level's pivots {j, sign, 0, 0}.  Indices address the shared
-  // array [d or 1/d (N) | U (nnz(L))].  Chunk words as below, start relative
-  // to fop_base[i], with the pivot-chunk bit.
-  // Lkpos: KKT position of every L entry (-1: structural zero).
-  const int *fstream, *fop_base, *foch, *foch_off, *Lkpos;
+  // as int4 {t, a, b, k | position-in-segment << 16 | last << 22}, split into
+  // kFactorWarps parts at target boundaries (part w for warp w), followed by
+  // the level's pivots {j, sign, 0, 0}, also in kFactorWarps parts.
+  // Indices address the shared array [d or 1/d (N) | U (nnz(L))].  Warp w of
+  // instance i reads its chunk words foch[fwoff[(kFactorWarps+1) i + w] ..
+  // fwoff[(kFactorWarps+1) i + w + 1]) (start relative to fop_base[i], pivot
+  // chunks flagged); flcnt[(lvl_off[i] + l) kFactorWarps + w] = its number of
+  // op chunks | pivot chunks << 16 at level l.  The block synchronises after
+  // each level's updates and after its pivots.  Lkpos: KKT position of every
+  // L entry (-1: structural zero).  fs_inst lists the fs_count streamed
+  // instances by decreasing shared-memory need (block b factors fs_inst[b]);
+  // fs_smem bytes per block.
+  const int *fstream, *fop_base, *foch, *fwoff, *flcnt, *Lkpos, *fs_inst;
   const int4 *fop;
-  int fs_max;  // largest N + nnz(L) among streamed instances
-  int has_fstream;
-  // Packing of streamed instances into blocks of kFactorWarps warps (first
-  // fit by decreasing shared-memory need): warp w of block b factors
-  // fpack_inst[kFactorWarps b + w] (-1: idle) with its shared memory at byte
-  // fpack_off[...]; fpack_smem bytes per block.
-  const int *fpack_inst, *fpack_off;
-  int fpack_blocks, fpack_smem;
+  int has_fstream, fs_count, fs_smem;
   // Packing of single-warp solves into blocks of kSolveWarps warps (first fit
   // by decreasing shared-memory need: the work vector y, N FP64 values, plus
   // the warp's ring): warp w of block b solves spack_inst[kSolveWarps b + w]
@@ -117,7 +117,7 @@ struct KKTDev {
 // holds the start of its last entry's segment; later steps would add
 // nothing.  Streams of a single-warp instance are therefore at most
 // kStartMask entries long (longer ones take the block kernels).
-constexpr int kRingSlots = 4;          // factorisation chunks in flight per warp (power of two)
+constexpr int kFRingSlots = 2;         // factorisation chunks in flight per warp (power of two)
 constexpr int kSRingSlots = 2;         // solve chunks in flight per warp (power of two)
 constexpr int kSolveWarps = 4;         // instances per single-warp-solve block
 constexpr int kSolveBlocksPerSM = 5;   // solve blocks resident per SM (register budget)
@@ -138,7 +138,7 @@ static_assert((1 << kSKShift) == kSK && kSPosMax + 1 >= kSChunk, "solve chunk la
 // min(position in segment, kPosMax) << 16 | last << kLastBit; count - 1 in
 // 6 bits; bit 31 marks a pivot chunk.
 constexpr int kChunk = 64;
-constexpr int kFactorWarps = 4;        // instances per streamed-factorisation block
+constexpr int kFactorWarps = 4;        // warps per streamed-factorisation block (one instance)
 constexpr int kPosMax = 63;
 constexpr int kLastBit = 22;
 
