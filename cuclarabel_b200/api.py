@@ -180,6 +180,7 @@ class Settings:
     chordal_decomposition_enable: bool = True
     soc_threshold: int = 5
     setup_threads: int = 0
+    fused_solves: bool = True
 
     def to_c(self):
         if self.direct_solve_method not in _METHODS:

@@ -945,6 +945,7 @@ extern "C" int clgpu_default_settings(clgpu_settings *s) {
   s->soc_threshold = 5;
   s->verbose = 0;
   s->setup_threads = 0;
+  s->fused_solves = 1;
   return 0;
 }
 
@@ -1783,9 +1784,10 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   // pack single-warp solves into blocks of kSolveWarps warps: each warp needs
   // its work vector (N FP64 values) and its ring (entries + FP64 values);
   // bins sized so kSolveBlocksPerSM blocks fit an SM's shared memory
-  {
+  // (two-side solves: two work vectors per warp)
+  for (int nr = 1; nr <= 2; ++nr) {
     auto need = [&](int i) {
-      return (((long long)N[i] * 8 + 15) & ~15LL) +
+      return nr * (((long long)N[i] * 8 + 15) & ~15LL) +
              (long long)kSRingSlots * kSChunk * (long long)(sizeof(int2) + sizeof(double));
     };
     std::vector<int> items, pinst, poffv;
@@ -1793,10 +1795,18 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       if (cls[i] == 1) items.push_back(i);
     long long cap = ((228LL * 1024) / kSolveBlocksPerSM - 1024) & ~15LL;
     for (int i : items) cap = std::max(cap, need(i));
-    kk.spack_blocks = ffd_pack(items, need, cap, kSolveWarps, pinst, poffv);
-    kk.spack_inst = A.upload(pinst);
-    kk.spack_off = A.upload(poffv);
-    kk.spack_smem = (int)cap;
+    const int nb = ffd_pack(items, need, cap, kSolveWarps, pinst, poffv);
+    if (nr == 1) {
+      kk.spack_blocks = nb;
+      kk.spack_inst = A.upload(pinst);
+      kk.spack_off = A.upload(poffv);
+      kk.spack_smem = (int)cap;
+    } else {
+      kk.spack2_blocks = nb;
+      kk.spack2_inst = A.upload(pinst);
+      kk.spack2_off = A.upload(poffv);
+      kk.spack2_smem = (int)cap;
+    }
   }
   kk.fch = A.upload(fch);
   kk.bch = A.upload(bch);
@@ -1839,6 +1849,9 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   kk.b = A.alloc<double>(VT);
   kk.x = A.alloc<double>(VT);
   kk.e = A.alloc<double>(VT);
+  kk.b2 = A.alloc<double>(VT);
+  kk.x2 = A.alloc<double>(VT);
+  kk.e2 = A.alloc<double>(VT);
   kk.dx = A.alloc<double>(VT);
   // ---------------- vectors and scalars
   Dev &dv = h->dv;
@@ -2005,8 +2018,9 @@ struct Phase {
     k_zero_fields<<<nblk((long long)nf * h->B), TB, 0, st>>>(h->dv, f0, nf, v);
     h->launches++;
   }
-  // kkt_update!: Hs refresh, regularise + refactor, constant rhs solve
-  void kkt_update() {
+  // kkt_update! without its constant-rhs solve: Hs refresh, regularise +
+  // refactor
+  void kkt_refactor() {
     h->prof_begin(2, st);
     cones_refresh_kkt(h->cs, h->map, h->kk.Kx, st);
     h->prof_end(st);
@@ -2014,14 +2028,22 @@ struct Phase {
     h->prof_begin(0, st);
     ldl_factor(h->kk, h->mixed, h->lp, h->dv.active, ok, h->dv.S + F_KKT_EPS * h->B, st);
     h->prof_end(st);
+    h->launches += 8;
+  }
+  // kkt_update!: refresh, refactor, constant rhs solve [x2; z2] = K \ [-q; b]
+  void kkt_update() {
+    kkt_refactor();
+    int *ok = h->dv.I + I_KKT_OK * h->B;
     h->prof_begin(1, st);
     ldl_solve(h->kk, h->mixed, h->lp, h->dv.active, h->dv.negq, h->dv.b, h->dv.x2, h->dv.z2,
               ok, st);
     h->prof_end(st);
-    h->launches += 12;
+    h->launches += 4;
   }
-  // kkt_solve! (kktsystem_gpu.jl:139-227)
-  void kkt_solve(bool affine) {
+  // kkt_solve! (kktsystem_gpu.jl:139-227).  with_constant: also solve the
+  // constant rhs of kkt_update! in the same launch (it depends on neither
+  // side's result, and each side's result is exactly that of its own solve)
+  void kkt_solve(bool affine, bool with_constant = false) {
     Dev &dv = h->dv;
     const double *dsc;
     if (affine) {
@@ -2033,7 +2055,11 @@ struct Phase {
     k_workz<<<nblk(dv.mz), TB, 0, st>>>(dv, dsc);
     int *ok = dv.I + I_KKT_OK * h->B;
     h->prof_begin(1, st);
-    ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.rhs_x, dv.workz, dv.x1, dv.z1, ok, st);
+    if (with_constant)
+      ldl_solve2(h->kk, h->mixed, h->lp, dv.active, dv.negq, dv.b, dv.x2, dv.z2, dv.rhs_x,
+                 dv.workz, dv.x1, dv.z1, ok, st);
+    else
+      ldl_solve(h->kk, h->mixed, h->lp, dv.active, dv.rhs_x, dv.workz, dv.x1, dv.z1, ok, st);
     h->prof_end(st);
     k_tau_dots<kRedThreads><<<h->B, kRedThreads, 0, st>>>(dv);
     k_tau_solve<<<nblk(h->B), TB, 0, st>>>(dv);
@@ -2144,11 +2170,16 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     h->prof_end(st);
     k_after_scaling<<<nblk(B), TB, 0, st>>>(dv);
     P.mask(M_PASS);
-    // KKT update and affine step
-    P.kkt_update();
+    // KKT update and affine step; the affine rhs needs nothing from the new
+    // factor, so kkt_update!'s constant solve runs with the affine solve
+    const bool fused = h->st.fused_solves != 0;
+    if (fused)
+      P.kkt_refactor();
+    else
+      P.kkt_update();
     k_affine_rhs<<<nblk(std::max(std::max(dv.nx, dv.mz), B)), TB, 0, st>>>(dv);
     cones_affine_ds(h->cs, dv.rhs_s, dv.s, st);
-    P.kkt_solve(true);
+    P.kkt_solve(true, fused);
     P.step_length(false, F_ALPHA_AFF);
     k_combined_scalars<<<nblk(B), TB, 0, st>>>(dv);
     k_combined_pre<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);

@@ -486,6 +486,11 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(BYTES));
 }
 
+// The stream kernels spell their products and sums with __dmul_rn /
+// __dadd_rn / __dsub_rn: the compiler never fuses those into FMAs, so every
+// value is rounded the same way whatever the surrounding code (one or two
+// right-hand sides, unrolling), and results do not depend on code shape.
+
 // Segmented sums of one chunk held two entries per lane: A = entry 2 lane,
 // B = entry 2 lane + 1, with products xA, xB and positions in their segments
 // pA, pB (clamped to 63).  Returns sA / sB: the sum of A's / B's segment from
@@ -498,19 +503,19 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc) {
 // complete every segment and the remaining steps are skipped.
 __device__ __forceinline__ void seg_scan2(double xA, double xB, int pA, int pB, int lane,
                                           double carry, int nsteps, double &sA, double &sB) {
-  if (lane == 0 && pA > 0) xA += carry;
-  double v = pB > 0 ? xA + xB : xB;
+  if (lane == 0 && pA > 0) xA = __dadd_rn(xA, carry);
+  double v = pB > 0 ? __dadd_rn(xA, xB) : xB;
   const int reach = pB > 0 ? lane - ((2 * lane + 1 - pB) >> 1) : 0;  // lanes back
 #pragma unroll
   for (int s = 0; s < 5; ++s) {
     if (s >= nsteps) break;
     const int d = 1 << s;
     const double o = __shfl_up_sync(0xffffffffu, v, d);
-    if (d <= reach && d <= lane) v += o;
+    if (d <= reach && d <= lane) v = __dadd_rn(v, o);
   }
   sB = v;
   const double prev = __shfl_up_sync(0xffffffffu, v, 1);
-  sA = xA + ((pA > 0 && lane > 0) ? prev : 0.0);
+  sA = (pA > 0 && lane > 0) ? __dadd_rn(xA, prev) : xA;
 }
 
 // Segmented sums of one solve chunk held kSK consecutive entries per lane
@@ -525,10 +530,10 @@ __device__ __forceinline__ void seg_scan2(double xA, double xB, int pA, int pB, 
 // total.  nsteps doubling steps complete every segment of the chunk.
 __device__ __forceinline__ void seg_scan4(double (&x)[kSK], const int (&p)[kSK], int lane,
                                           double carry, int nsteps, double (&s)[kSK]) {
-  if (lane == 0 && p[0] > 0) x[0] += carry;
+  if (lane == 0 && p[0] > 0) x[0] = __dadd_rn(x[0], carry);
   s[0] = x[0];
 #pragma unroll
-  for (int j = 1; j < kSK; ++j) s[j] = p[j] > 0 ? s[j - 1] + x[j] : x[j];
+  for (int j = 1; j < kSK; ++j) s[j] = p[j] > 0 ? __dadd_rn(s[j - 1], x[j]) : x[j];
   double v = s[kSK - 1];
   const int pt = p[kSK - 1];
   const int reach = pt > 0 ? lane - ((kSK * lane + kSK - 1 - pt) >> kSKShift) : 0;
@@ -537,12 +542,12 @@ __device__ __forceinline__ void seg_scan4(double (&x)[kSK], const int (&p)[kSK],
     if (t >= nsteps) break;
     const int d = 1 << t;
     const double o = __shfl_up_sync(0xffffffffu, v, d);
-    if (d <= reach && d <= lane) v += o;
+    if (d <= reach && d <= lane) v = __dadd_rn(v, o);
   }
   const double prev = __shfl_up_sync(0xffffffffu, v, 1);
 #pragma unroll
   for (int j = 0; j < kSK - 1; ++j)
-    if (p[j] > j && lane > 0) s[j] += prev;
+    if (p[j] > j && lane > 0) s[j] = __dadd_rn(s[j], prev);
   s[kSK - 1] = v;
 }
 
@@ -565,19 +570,33 @@ __device__ __forceinline__ void ring_vals(const float *rv, double (&v)[kSK]) {
 }
 
 // One pass over an encoded stream (entries ent / values val from stream
-// position base), chunk by chunk as listed in chunks[0..nch):
-//   RESID = false:  y[seg] -= sum val * y[idx]     (out == y)
-//   RESID = true:   out[seg] = sum val * y[idx]
-// Chunk words are read 32 at a time, one per lane, two blocks ahead of use.
-// The ring copies are coalesced (lane l copies entries l, l + 32, ...); each
-// lane then reads its kSK consecutive entries with 16-byte shared loads.
-template <typename T, bool RESID>
+// position base), chunk by chunk as listed in chunks[0..nch), for each
+// right-hand side r < NR whose bit is set in act:
+//   RESID = false:  y_r[seg] -= sum val * y_r[idx]     (out_r == y_r)
+//   RESID = true:   out_r[seg] = sum val * y_r[idx]
+// A chunk's entries and values are read once for all right-hand sides; each
+// side's arithmetic is exactly that of a single-side pass.  Chunk words are
+// read 32 at a time, one per lane, two blocks ahead of use.  The ring copies
+// are coalesced (lane l copies entries l, l + 32, ...); each lane then reads
+// its kSK consecutive entries with 16-byte shared loads.
+template <typename T, bool RESID, int NR>
 __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
                           const int2 *__restrict__ ent, const T *__restrict__ val,
-                          const double *y, double *out, int2 *re, T *rv, int lane) {
+                          double *const (&yin)[NR], double *const (&outin)[NR], int2 *re, T *rv,
+                          int lane, unsigned act) {
   static_assert(kSK == 4, "ring_pass reads four entries per lane");
   const unsigned full = 0xffffffffu;
   if (nch == 0) return;
+  // register copies of the side pointers (the caller's arrays may live in
+  // local memory; every index below is a compile-time constant)
+  double *y[NR], *out[NR];
+  bool on[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    y[r] = yin[r];
+    out[r] = outin[r];
+    on[r] = (act >> r) & 1u;
+  }
   int d0 = lane < nch ? chunks[lane] : 0;
   int d1 = lane + 32 < nch ? chunks[lane + 32] : 0;
   int d2 = lane + 64 < nch ? chunks[lane + 64] : 0;
@@ -606,7 +625,9 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
   };
 #pragma unroll
   for (int c = 0; c < kSRing; ++c) issue(c, c);
-  double carry = 0.0;
+  double carry[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) carry[r] = 0.0;
   for (int c = 0; c < nch; ++c) {
     if (c > 0 && (c & 31) == 0) {
       ++blk;
@@ -627,29 +648,39 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
     const int ix[kSK] = {ea.y, ea.w, eb.y, eb.w};
     double vv[kSK];
     ring_vals(rv + slot * kSChunk + kSK * lane, vv);
-    double x[kSK], sm[kSK];
-    int p[kSK];
+    int p[kSK], gi[kSK];
+    bool ok[kSK], wr[kSK];
 #pragma unroll
     for (int j = 0; j < kSK; ++j) {
-      const bool ok = kSK * lane + j < cnt;
-      p[j] = ok ? (sg[j] >> 16) & kSPosMax : 0;
-      const double yv = y[ok ? ix[j] : 0];
-      x[j] = ok ? vv[j] * yv : 0.0;
+      ok[j] = kSK * lane + j < cnt;
+      p[j] = ok[j] ? (sg[j] >> 16) & kSPosMax : 0;
+      gi[j] = ok[j] ? ix[j] : 0;
+      wr[j] = ok[j] && ((sg[j] >> kSLastBit) & 1);
     }
-    seg_scan4(x, p, lane, carry, nsteps, sm);
+    const int jl = (cnt - 1) & (kSK - 1), ll = (cnt - 1) >> kSKShift;
 #pragma unroll
-    for (int j = 0; j < kSK; ++j)
-      if (kSK * lane + j < cnt && ((sg[j] >> kSLastBit) & 1)) {
-        if (RESID)
-          out[sg[j] & 0xffff] = sm[j];
-        else
-          out[sg[j] & 0xffff] -= sm[j];
+    for (int r = 0; r < NR; ++r) {
+      if (!on[r]) continue;
+      double x[kSK], sm[kSK];
+#pragma unroll
+      for (int j = 0; j < kSK; ++j) {
+        const double yv = y[r][gi[j]];
+        x[j] = ok[j] ? __dmul_rn(vv[j], yv) : 0.0;
       }
-    // partial sum of the segment of the chunk's last entry (used by the next
-    // chunk only if its first entry continues that segment)
-    const int jl = (cnt - 1) & (kSK - 1);
-    const double cs = jl == 0 ? sm[0] : jl == 1 ? sm[1] : jl == 2 ? sm[2] : sm[3];
-    carry = __shfl_sync(full, cs, (cnt - 1) >> kSKShift);
+      seg_scan4(x, p, lane, carry[r], nsteps, sm);
+#pragma unroll
+      for (int j = 0; j < kSK; ++j)
+        if (wr[j]) {
+          if (RESID)
+            out[r][sg[j] & 0xffff] = sm[j];
+          else
+            out[r][sg[j] & 0xffff] = __dsub_rn(out[r][sg[j] & 0xffff], sm[j]);
+        }
+      // partial sum of the segment of the chunk's last entry (used by the
+      // next chunk only if its first entry continues that segment)
+      const double cs = jl == 0 ? sm[0] : jl == 1 ? sm[1] : jl == 2 ? sm[2] : sm[3];
+      carry[r] = __shfl_sync(full, cs, ll);
+    }
     __syncwarp();
     issue(c + kSRing, slot);
   }
@@ -673,26 +704,43 @@ constexpr int kVecU = 8;
     }                                                             \
   }
 
+// Right-hand sides of one solve launch: side r gathers its rhs from rx[r] /
+// rz[r] and scatters its solution to lx[r] / lz[r] (either may be null).
+template <int NR>
+struct SolveIO {
+  const double *rx[NR], *rz[NR];
+  double *lx[NR], *lz[NR];
+};
+
 // Warps of a block solve different instances (the packing tables); they
 // share nothing but the block's shared memory, each in its own slice, and
-// never synchronise with one another.
-template <typename T>
+// never synchronise with one another.  A warp solves NR right-hand sides with
+// one factor: every stream pass serves all sides still refining, and each
+// side follows the refinement rules on its own, so its result is exactly
+// that of a single-side solve.
+template <typename T, int NR>
 __global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
-    k_ldl_solve_warp(KKTDev k, LDLParams prm, const int *run, const double *__restrict__ rx,
-                     const double *__restrict__ rz, double *lx, double *lz, int *ok) {
+    k_ldl_solve_warp(KKTDev k, LDLParams prm, const int *run, SolveIO<NR> io, int *ok) {
   const int slot = blockIdx.x * kSolveWarps + (threadIdx.x >> 5);
-  const int inst = k.spack_inst[slot];
+  const int inst = NR == 1 ? k.spack_inst[slot] : k.spack2_inst[slot];
   if (inst < 0 || !run[inst] || !ok[inst]) return;
   const int N = k.N[inst];
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  unsigned char *smw = sm_raw + k.spack_off[slot];
-  double *y = reinterpret_cast<double *>(smw);
-  int2 *re = reinterpret_cast<int2 *>(smw + (((size_t)N * 8 + 15) & ~(size_t)15));
+  unsigned char *smw = sm_raw + (NR == 1 ? k.spack_off[slot] : k.spack2_off[slot]);
+  const size_t ybytes = ((size_t)N * 8 + 15) & ~(size_t)15;
+  double *y[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) y[r] = reinterpret_cast<double *>(smw + r * ybytes);
+  int2 *re = reinterpret_cast<int2 *>(smw + NR * ybytes);
   T *rv = reinterpret_cast<T *>(re + kSRing * kSChunk);
   const int vo = k.voff[inst], po = k.poff[inst], lane = threadIdx.x & 31;
-  double *__restrict__ b = k.b + vo;
-  double *__restrict__ x = k.x + vo;
-  double *__restrict__ e = k.e + vo;
+  double *b[NR], *x[NR], *e[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    b[r] = (r == 0 ? k.b : k.b2) + vo;
+    x[r] = (r == 0 ? k.x : k.x2) + vo;
+    e[r] = (r == 0 ? k.e : k.e2) + vo;
+  }
   const int *__restrict__ gs = k.gsrc + vo;
   const int lbase = k.Lp[po], kbase = k.Kp[po];
   const int *fch = k.fch + k.fch_off[inst], *bch = k.bch + k.bch_off[inst],
@@ -702,8 +750,11 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
   const int nkch = k.kch_off[inst + 1] - k.kch_off[inst];
   const T *LxF = reinterpret_cast<const T *>(k.LxF), *LxB = reinterpret_cast<const T *>(k.LxB);
   const T *__restrict__ Dinv = reinterpret_cast<const T *>(k.Dinv) + vo;
-  double nb = 0;
-  {
+  double normb[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const double *__restrict__ rx = io.rx[r], *__restrict__ rz = io.rz[r];
+    double nb = 0;
     int g[kVecU];
     double v[kVecU];
     for (int i0 = lane; i0 < N; i0 += 32 * kVecU) {
@@ -719,100 +770,150 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
       for (int u = 0; u < kVecU; ++u) {
         const int i = i0 + 32 * u;
         if (i < N) {
-          b[i] = v[u];
-          y[i] = v[u];
+          b[r][i] = v[u];
+          y[r][i] = v[u];
           nb = fmax(nb, fabs(v[u]));
         }
       }
     }
+    normb[r] = warp_max(nb);
   }
-  const double normb = warp_max(nb);
   __syncwarp();
   double tv[kVecU];
-  int ntri = 0, nres = 0, nir = 0;
-  auto trisolve = [&]() {
-    ++ntri;
-    ring_pass<T, false>(fch, nfch, lbase, k.fent, LxF, y, y, re, rv, lane);
-    VEC_LOOP(i, N, tv[u] = double(Dinv[i]);, y[i] *= tv[u];)
+  int ntri = 0, nres = 0, nir = 0;  // side-passes (profiling)
+  auto popc = [](unsigned m) { return __popc(m); };
+  auto trisolve = [&](unsigned m) {
+    ntri += popc(m);
+    ring_pass<T, false, NR>(fch, nfch, lbase, k.fent, LxF, y, y, re, rv, lane, m);
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if ((m >> r) & 1u) {
+        double *yr = y[r];
+        VEC_LOOP(i, N, tv[u] = double(Dinv[i]);, yr[i] *= tv[u];)
+      }
     __syncwarp();
-    ring_pass<T, false>(bch, nbch, lbase, k.bent, LxB, y, y, re, rv, lane);
+    ring_pass<T, false, NR>(bch, nbch, lbase, k.bent, LxB, y, y, re, rv, lane, m);
   };
-  // e = b - K y, returns ||e||_inf (+inf when not finite)
-  auto residual = [&]() {
-    ++nres;
-    ring_pass<double, true>(kch, nkch, kbase, k.kent, k.Kx, y, e, re,
-                            reinterpret_cast<double *>(rv), lane);
+  // e_r = b_r - K y_r; norme[r] = ||e_r||_inf (+inf when not finite)
+  auto residual = [&](unsigned m, double (&norme)[NR]) {
+    nres += popc(m);
+    ring_pass<double, true, NR>(kch, nkch, kbase, k.kent, k.Kx, y, e, re,
+                                reinterpret_cast<double *>(rv), lane, m);
     __syncwarp();
-    double mx = 0.0;
-    bool bad = false;
-    double tb[kVecU];
-    VEC_LOOP(i, N, tb[u] = b[i]; tv[u] = e[i];, {
-      const double er = tb[u] - tv[u];
-      e[i] = er;
-      if (!isfinite(er)) bad = true;
-      mx = fmax(mx, fabs(er));
-    })
-    __syncwarp();
-    mx = warp_max(mx);
-    return __any_sync(0xffffffffu, bad) ? CUDART_INF : mx;
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if ((m >> r) & 1u) {
+        double mx = 0.0;
+        bool bad = false;
+        double tb[kVecU];
+        double *br = b[r], *er = e[r];
+        VEC_LOOP(i, N, tb[u] = br[i]; tv[u] = er[i];, {
+          const double ev = tb[u] - tv[u];
+          er[i] = ev;
+          if (!isfinite(ev)) bad = true;
+          mx = fmax(mx, fabs(ev));
+        })
+        __syncwarp();
+        mx = warp_max(mx);
+        norme[r] = __any_sync(0xffffffffu, bad) ? CUDART_INF : mx;
+      }
   };
-  trisolve();
+  // The per-side loops of the refinement stay rolled (unroll 1): with them
+  // unrolled, the two-side build skipped every refinement sweep (its results
+  // then differed from the one-side solve's); rolled, each side's result is
+  // bitwise that of the one-side kernel, which the two-side parity test checks.
+  const unsigned all = (1u << NR) - 1u;
+  trisolve(all);
   bool good = true;
   if (prm.ir_enable) {
     // x keeps the accepted iterate; y holds the candidate the residual reads
-    double norme = residual();
-    for (int i = lane; i < N; i += 32) x[i] = y[i];
-    __syncwarp();
-    if (!isfinite(norme)) good = false;
-    for (int it = 0; good && it < prm.ir_maxiter; ++it) {
-      if (norme <= prm.ir_abstol + prm.ir_reltol * normb) break;
-      const double last = norme;
-      ++nir;
-      VEC_LOOP(i, N, tv[u] = e[i];, y[i] = tv[u];)
-      __syncwarp();
-      trisolve();
-      VEC_LOOP(i, N, tv[u] = x[i];, y[i] += tv[u];)
-      __syncwarp();
-      norme = residual();
-      if (!isfinite(norme)) {
+    double norme[NR], last[NR];
+    residual(all, norme);
+    unsigned m = 0;
+#pragma unroll 1
+    for (int r = 0; r < NR; ++r) {
+      for (int i = lane; i < N; i += 32) x[r][i] = y[r][i];
+      if (!isfinite(norme[r]))
         good = false;
-        break;
-      }
-      // kktsolver_directldl_gpu.jl:390-400: keep the candidate if it improved
-      // on the last error; stop when the improvement ratio is below stopratio
-      const double ratio = last / norme;
-      if (ratio > 1.0 || ratio >= prm.ir_stopratio)
-        for (int i = lane; i < N; i += 32) x[i] = y[i];
+      else
+        m |= 1u << r;
+    }
+    __syncwarp();
+    if (!good) m = 0;
+    for (int it = 0; m && it < prm.ir_maxiter; ++it) {
+#pragma unroll 1
+      for (int r = 0; r < NR; ++r)
+        if (((m >> r) & 1u) && norme[r] <= prm.ir_abstol + prm.ir_reltol * normb[r])
+          m &= ~(1u << r);
+      if (!m) break;
+#pragma unroll 1
+      for (int r = 0; r < NR; ++r)
+        if ((m >> r) & 1u) {
+          last[r] = norme[r];
+          ++nir;
+          double *yr = y[r], *er = e[r];
+          VEC_LOOP(i, N, tv[u] = er[i];, yr[i] = tv[u];)
+        }
       __syncwarp();
-      if (ratio < prm.ir_stopratio) break;
+      trisolve(m);
+#pragma unroll 1
+      for (int r = 0; r < NR; ++r)
+        if ((m >> r) & 1u) {
+          double *yr = y[r], *xr = x[r];
+          VEC_LOOP(i, N, tv[u] = xr[i];, yr[i] += tv[u];)
+        }
+      __syncwarp();
+      residual(m, norme);
+#pragma unroll 1
+      for (int r = 0; r < NR; ++r)
+        if ((m >> r) & 1u) {
+          if (!isfinite(norme[r])) {
+            good = false;
+            m &= ~(1u << r);
+            continue;
+          }
+          // kktsolver_directldl_gpu.jl:390-400: keep the candidate if it
+          // improved on the last error; stop when the improvement ratio is
+          // below stopratio
+          const double ratio = last[r] / norme[r];
+          if (ratio > 1.0 || ratio >= prm.ir_stopratio)
+            for (int i = lane; i < N; i += 32) x[r][i] = y[r][i];
+          if (ratio < prm.ir_stopratio) m &= ~(1u << r);
+        }
+      __syncwarp();
+      if (!good) break;
     }
   } else {
     bool bad = false;
-    for (int i = lane; i < N; i += 32) {
-      x[i] = y[i];
-      if (!isfinite(y[i])) bad = true;
-    }
+#pragma unroll 1
+    for (int r = 0; r < NR; ++r)
+      for (int i = lane; i < N; i += 32) {
+        x[r][i] = y[r][i];
+        if (!isfinite(y[r][i])) bad = true;
+      }
     if (__any_sync(0xffffffffu, bad)) good = false;
     __syncwarp();
   }
   if (k.prof_bytes && lane == 0) {
     // algorithmic bytes: every stream pass reads its entries, values and
-    // chunk words once; vectors are read / written once per use
+    // chunk words once per side-pass; vectors are read / written once per use
     const double nl = k.Lp[po + N] - lbase, nk = k.Kp[po + N] - kbase, ts = sizeof(T);
     k.prof_bytes[k.B + inst] +=
-        20.0 * N                                                   // rhs gather, b
+        NR * 20.0 * N                                               // rhs gather, b
         + ntri * (2.0 * nl * (8 + ts) + 4.0 * (nfch + nbch) + ts * N)  // substitutions
         + nres * (16.0 * nk + 4.0 * nkch + 24.0 * N)                // residuals
-        + nir * 24.0 * N + 8.0 * N                                  // refinement vectors
-        + 20.0 * N;                                                 // result scatter
+        + nir * 24.0 * N + NR * 8.0 * N                             // refinement vectors
+        + NR * 20.0 * N;                                            // result scatter
   }
   if (!good) {
     if (lane == 0) ok[inst] = 0;
     return;
   }
-  {
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    double *lx = io.lx[r], *lz = io.lz[r], *xr = x[r];
     int g[kVecU];
-    VEC_LOOP(i, N, g[u] = gs[i]; tv[u] = x[i];, {
+    VEC_LOOP(i, N, g[u] = gs[i]; tv[u] = xr[i];, {
       if (g[u] >= 0) {
         if (lx) lx[g[u]] = tv[u];
       } else if (g[u] <= -2) {
@@ -970,13 +1071,13 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
       }
       carry = 0.0;
     } else {
-      const double xA = vA ? V[oA.y] * V[oA.z] * V[oA.w & 0xffff] : 0.0;
-      const double xB = vB ? V[oB.y] * V[oB.z] * V[oB.w & 0xffff] : 0.0;
+      const double xA = vA ? __dmul_rn(__dmul_rn(V[oA.y], V[oA.z]), V[oA.w & 0xffff]) : 0.0;
+      const double xB = vB ? __dmul_rn(__dmul_rn(V[oB.y], V[oB.z]), V[oB.w & 0xffff]) : 0.0;
       double sA, sB;
       seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
                 (int)((w >> kStepShift) & 7u), sA, sB);
-      if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] -= sA;
-      if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] -= sB;
+      if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] = __dsub_rn(V[oA.x], sA);
+      if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] = __dsub_rn(V[oB.x], sB);
       const int ll = (cnt - 1) >> 1;
       carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
     }
@@ -1055,11 +1156,28 @@ template <typename T>
 static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
                          const double *rx, const double *rz, double *lx, double *lz, int *ok,
                          cudaStream_t st) {
-  if (k.has_small)
-    k_ldl_solve_warp<T><<<k.spack_blocks, 32 * kSolveWarps, k.spack_smem, st>>>(
-        k, p, run, rx, rz, lx, lz, ok);
+  if (k.has_small) {
+    SolveIO<1> io{{rx}, {rz}, {lx}, {lz}};
+    k_ldl_solve_warp<T, 1><<<k.spack_blocks, 32 * kSolveWarps, k.spack_smem, st>>>(k, p, run,
+                                                                                 io, ok);
+  }
   if (k.has_large)
     k_ldl_solve<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, rx, rz, lx, lz, ok);
+}
+template <typename T>
+static void launch_solve2(const KKTDev &k, const LDLParams &p, const int *run,
+                          const double *rx0, const double *rz0, double *lx0, double *lz0,
+                          const double *rx1, const double *rz1, double *lx1, double *lz1,
+                          int *ok, cudaStream_t st) {
+  if (k.has_small) {
+    SolveIO<2> io{{rx0, rx1}, {rz0, rz1}, {lx0, lx1}, {lz0, lz1}};
+    k_ldl_solve_warp<T, 2><<<k.spack2_blocks, 32 * kSolveWarps, k.spack2_smem, st>>>(k, p, run,
+                                                                                   io, ok);
+  }
+  if (k.has_large) {
+    k_ldl_solve<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, rx0, rz0, lx0, lz0, ok);
+    k_ldl_solve<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, rx1, rz1, lx1, lz1, ok);
+  }
 }
 
 static bool g_attr_done = false;
@@ -1073,15 +1191,16 @@ static void set_attrs() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
-  cudaFuncSetAttribute(k_ldl_solve_warp<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSolveSmemMax);
-  cudaFuncSetAttribute(k_ldl_solve_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSolveSmemMax);
   // the packed kernels size their blocks for the SM's full shared memory
-  cudaFuncSetAttribute(k_ldl_solve_warp<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
-  cudaFuncSetAttribute(k_ldl_solve_warp<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
+  auto solve_attrs = [](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmemMax);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+  };
+  solve_attrs(k_ldl_solve_warp<double, 1>);
+  solve_attrs(k_ldl_solve_warp<float, 1>);
+  solve_attrs(k_ldl_solve_warp<double, 2>);
+  solve_attrs(k_ldl_solve_warp<float, 2>);
   cudaFuncSetAttribute(k_ldl_factor_stream<double>,
                        cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
@@ -1108,6 +1227,17 @@ void ldl_solve(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
     launch_solve<float>(k, p, run, rx, rz, lx, lz, ok, st);
   else
     launch_solve<double>(k, p, run, rx, rz, lx, lz, ok, st);
+}
+
+void ldl_solve2(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
+                const double *rx0, const double *rz0, double *lx0, double *lz0,
+                const double *rx1, const double *rz1, double *lx1, double *lz1, int *ok,
+                cudaStream_t st) {
+  set_attrs();
+  if (fp32)
+    launch_solve2<float>(k, p, run, rx0, rz0, lx0, lz0, rx1, rz1, lx1, lz1, ok, st);
+  else
+    launch_solve2<double>(k, p, run, rx0, rz0, lx0, lz0, rx1, rz1, lx1, lz1, ok, st);
 }
 
 }  // namespace clgpu

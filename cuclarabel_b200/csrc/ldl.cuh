@@ -88,6 +88,9 @@ struct KKTDev {
   // bytes per block.
   const int *spack_inst, *spack_off;
   int spack_blocks, spack_smem;
+  // the same for solves of two right-hand sides at once (two work vectors)
+  const int *spack2_inst, *spack2_off;
+  int spack2_blocks, spack2_smem;
   // profiling only (else null): per instance, algorithmic bytes moved by the
   // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
   double *prof_bytes;
@@ -104,7 +107,10 @@ struct KKTDev {
   // pivots the factorisation itself runs on; the solves read the FP32 copy
   double *Lacc;
   double *Dacc;
-  double *b, *x, *e, *dx;
+  // single-warp solve scratch per instance (sum N each): right-hand side b,
+  // accepted iterate x and residual e of the first and the second side
+  double *b, *x, *e, *b2, *x2, *e2;
+  double *dx;
 };
 
 // Stream chunking shared by the setup and the kernels.  A chunk is a run of
@@ -120,7 +126,7 @@ struct KKTDev {
 constexpr int kFRingSlots = 2;         // factorisation chunks in flight per warp (power of two)
 constexpr int kSRingSlots = 2;         // solve chunks in flight per warp (power of two)
 constexpr int kSolveWarps = 4;         // instances per single-warp-solve block
-constexpr int kSolveBlocksPerSM = 5;   // solve blocks resident per SM (register budget)
+constexpr int kSolveBlocksPerSM = 4;   // solve blocks resident per SM (register budget)
 constexpr int kSolveSmemMax = 200 * 1024;  // dynamic shared memory cap of a solve block
 constexpr int kStepShift = 22;
 constexpr int kCntShift = 25;
@@ -182,5 +188,11 @@ void ldl_factor(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
 void ldl_solve(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
                const double *rx, const double *rz, double *lx, double *lz,
                int *ok, cudaStream_t st);
+// two right-hand sides with the same factor in one launch: side 0 (rx0, rz0)
+// -> (lx0, lz0), side 1 likewise; each result is exactly that of ldl_solve
+void ldl_solve2(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
+                const double *rx0, const double *rz0, double *lx0, double *lz0,
+                const double *rx1, const double *rz1, double *lx1, double *lz1, int *ok,
+                cudaStream_t st);
 
 }  // namespace clgpu

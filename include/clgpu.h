@@ -74,6 +74,8 @@ typedef struct {
   int soc_threshold;       /* src/settings.jl:147 */
   int verbose;
   int setup_threads;       /* host threads for per-instance setup; 0 = all */
+  int fused_solves;        /* 1: kkt_update!'s constant-rhs solve shares the
+                              affine solve's launch (same results); 0: its own */
 } clgpu_settings;
 
 /* mirrors DefaultInfo (src/types.jl:227-255) plus solution scalars */

@@ -132,6 +132,20 @@ def test_batch_equals_single(cuda_device):
         assert np.allclose(s1.x, sb.x, rtol=1e-6, atol=1e-6)
 
 
+@pytest.mark.parametrize("method", ["cudss", "cudssmixed"])
+def test_fused_constant_and_affine_solves_are_bitwise_separate_solves(cuda_device, method):
+    """kkt_update!'s constant-rhs solve runs in the affine solve's launch (two
+    right-hand sides per warp).  Each side's arithmetic is that of its own
+    solve, so the whole IPM must reproduce the unfused run bit for bit."""
+    pbs = problems.mpc_batch(24, seed0=300) + [problems.mixed_socp(scale=0.02, seed=4)]
+    a = BatchSolver(pbs, direct_solve_method=method).solve()
+    b = BatchSolver(pbs, direct_solve_method=method, fused_solves=False).solve()
+    for k, (x, y) in enumerate(zip(a, b)):
+        assert x.status == y.status and x.iterations == y.iterations, k
+        assert np.array_equal(x.x, y.x) and np.array_equal(x.z, y.z), k
+        assert x.obj_val == y.obj_val, k
+
+
 def test_mixed_socp_scaled(cuda_device):
     pb = problems.mixed_socp(scale=0.02, seed=2)
     sol = Solver(*pb).solve()
