@@ -432,9 +432,13 @@ def main():
                  else "fallback 6.65 TB/s")
     phases = prof["phases"]
     dom = max(phases.items(), key=lambda kv: kv[1][0])
-    kernels = {"ldl_solve": "k_ldl_solve_warp (single-warp LDL solve + refinement)",
-               "ldl_factor": "k_ldl_factor_stream (streamed single-warp LDL factorisation)"}
-    summaries = {"ldl_solve": "ldl_solve_mpc4096.md", "ldl_factor": "ldl_factor_stream_mpc4096.md"}
+    kernels = {"ldl_solve": "k_ldl_solve_warp<double, 1> (single-warp LDL solve + refinement)",
+               "ldl_solve2": "k_ldl_solve_warp<double, 2> (single-warp LDL solve of the "
+                             "constant and affine right-hand sides + refinement)",
+               "ldl_factor": "k_ldl_factor_stream (streamed LDL factorisation, 4 warps per "
+                             "instance)"}
+    summaries = {"ldl_solve": "ldl_solve_mpc4096.md", "ldl_solve2": "ldl_solve2_mpc4096.md",
+                 "ldl_factor": "ldl_factor_stream_mpc4096.md"}
 
     def roofline(name):
         ms, calls = phases[name]
@@ -458,7 +462,8 @@ def main():
         cpu = cpu_baseline_sample(args.ref_sample)
 
     if rank == 0:
-        roof = roofline(dom[0] if dom[0] in kernels else "ldl_solve")
+        roof_name = dom[0] if dom[0] in kernels else "ldl_solve"
+        roof = roofline(roof_name)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -477,13 +482,12 @@ def main():
             "e2e_cold": cold,
             "gpu_launches": launches_per_solve * args.steps,
             "roofline": roof,
-            "roofline_other": {
-                "ldl_factor" if roof["kernel"] == kernels["ldl_solve"] else "ldl_solve":
-                    roofline("ldl_factor" if roof["kernel"] == kernels["ldl_solve"]
-                             else "ldl_solve"),
-                "update_scaling": {"achieved": us_ach, "frac": us_ach / hbm, "unit": "GB/s",
-                                   "algorithmic_bytes_per_launch": us_bytes,
-                                   "avg_launch_ms": us_ms / max(us_calls, 1)}},
+            "roofline_other": dict(
+                {nm: roofline(nm) for nm in kernels
+                 if nm != roof_name and phases.get(nm, (0.0, 0))[1] > 0},
+                update_scaling={"achieved": us_ach, "frac": us_ach / hbm, "unit": "GB/s",
+                                "algorithmic_bytes_per_launch": us_bytes,
+                                "avg_launch_ms": us_ms / max(us_calls, 1)}),
             "phases_ms": {k: round(v[0], 3) for k, v in phases.items()},
             "dominant_phase": {"name": dom[0], "ms": dom[1][0], "calls": dom[1][1]},
             "batch": {"status": status_counts, "iters_mean": float(np.mean(iters)),

@@ -470,15 +470,16 @@ class BatchSolver:
         passes = ctypes.c_int()
         L.clgpu_solver_get_profile(self._h, *[ctypes.byref(v) for v in vals],
                                    ctypes.byref(passes))
-        ms = (ctypes.c_double * 5)()
-        calls = (ctypes.c_longlong * 5)()
+        ms = (ctypes.c_double * 6)()
+        calls = (ctypes.c_longlong * 6)()
         L.clgpu_solver_get_phase_times(self._h, ms, calls)
-        names = ["ldl_factor", "ldl_solve", "kkt_refresh", "residual", "update_scaling"]
-        by = (ctypes.c_double * 2)()
+        names = ["ldl_factor", "ldl_solve", "kkt_refresh", "residual", "update_scaling",
+                 "ldl_solve2"]
+        by = (ctypes.c_double * 3)()
         L.clgpu_solver_get_phase_bytes(self._h, by)
         return dict(ms_total=vals[0].value, passes=passes.value,
                     phases={n: (ms[i], calls[i]) for i, n in enumerate(names)},
-                    bytes={"ldl_factor": by[0], "ldl_solve": by[1]})
+                    bytes={"ldl_factor": by[0], "ldl_solve": by[1], "ldl_solve2": by[2]})
 
 
 class Solver(BatchSolver):

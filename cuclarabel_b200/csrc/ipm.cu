@@ -811,17 +811,19 @@ struct clgpu_solver {
   bool solved = false;
   long long launches = 0;
   bool profiling = false;
-  // per-phase device time of the last solve (ms): factor, ldl solve, cone
-  // kernels, residual/vector kernels, update_scaling alone
-  double prof[5] = {0, 0, 0, 0, 0};
-  long long prof_calls[5] = {0, 0, 0, 0, 0};
+  // per-phase device time of the last solve (ms): factor, one-side ldl
+  // solves, KKT refresh, residual kernels, update_scaling alone, two-side ldl
+  // solves
+  static constexpr int kPhases = 6;
+  double prof[kPhases] = {0, 0, 0, 0, 0, 0};
+  long long prof_calls[kPhases] = {0, 0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<int, int>>> ev_marks;  // class, (ev begin, ev end)
   size_t ev_next = 0;
   int prof_open = -1, prof_open_ev = -1;
   int passes = 0;
   double last_ms = 0;
-  double *d_prof_bytes = nullptr;  // [2B] algorithmic bytes (profiling)
+  double *d_prof_bytes = nullptr;  // [3B] algorithmic bytes (profiling)
   // update_data!: maps from the caller's value arrays to the device copies,
   // and staging buffers for the new values
   bool upd_ok = false;
@@ -830,7 +832,7 @@ struct clgpu_solver {
   int4 *d_upd_pmap = nullptr, *d_upd_amap = nullptr;
   int2 *d_upd_pxy = nullptr, *d_upd_axy = nullptr;
   double *d_in_P = nullptr, *d_in_A = nullptr, *d_in_q = nullptr, *d_in_b = nullptr;
-  double prof_bytes[2] = {0, 0};   // factor, solve: sums of the last profiled solve
+  double prof_bytes[3] = {0, 0, 0};  // factor, one-side, two-side solves (last profiled solve)
   ~clgpu_solver() {
     if (h_counter) cudaFreeHost(h_counter);
     for (auto e : ev_pool) cudaEventDestroy(e);
@@ -859,15 +861,14 @@ struct clgpu_solver {
   }
   void prof_collect() {
     if (d_prof_bytes) {
-      std::vector<double> hb(2 * (size_t)B);
+      std::vector<double> hb(3 * (size_t)B);
       cudaMemcpy(hb.data(), d_prof_bytes, hb.size() * sizeof(double), cudaMemcpyDeviceToHost);
-      prof_bytes[0] = prof_bytes[1] = 0;
-      for (int i = 0; i < B; ++i) {
-        prof_bytes[0] += hb[i];
-        prof_bytes[1] += hb[(size_t)B + i];
+      for (int c = 0; c < 3; ++c) {
+        prof_bytes[c] = 0;
+        for (int i = 0; i < B; ++i) prof_bytes[c] += hb[(size_t)c * B + i];
       }
     }
-    for (int c = 0; c < 5; ++c) {
+    for (int c = 0; c < kPhases; ++c) {
       prof[c] = 0;
       prof_calls[c] = 0;
     }
@@ -1449,7 +1450,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   KKTDev &kk = h->kk;
   kk.B = B;
   kk.prof_bytes = nullptr;
-  h->d_prof_bytes = A.alloc<double>(2 * (size_t)B);
+  h->d_prof_bytes = A.alloc<double>(3 * (size_t)B);
   kk.N = A.upload(N);
   kk.voff = A.upload(voff);
   kk.poff = A.upload(poff);
@@ -2054,7 +2055,7 @@ struct Phase {
     }
     k_workz<<<nblk(dv.mz), TB, 0, st>>>(dv, dsc);
     int *ok = dv.I + I_KKT_OK * h->B;
-    h->prof_begin(1, st);
+    h->prof_begin(with_constant ? 5 : 1, st);
     if (with_constant)
       ldl_solve2(h->kk, h->mixed, h->lp, dv.active, dv.negq, dv.b, dv.x2, dv.z2, dv.rhs_x,
                  dv.workz, dv.x1, dv.z1, ok, st);
@@ -2105,7 +2106,7 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
   const int B = h->B;
   h->launches = 0;
   if (h->profiling && h->d_prof_bytes)
-    cudaMemsetAsync(h->d_prof_bytes, 0, 2 * (size_t)B * sizeof(double), st);
+    cudaMemsetAsync(h->d_prof_bytes, 0, 3 * (size_t)B * sizeof(double), st);
   h->kk.prof_bytes = h->profiling ? h->d_prof_bytes : nullptr;
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
@@ -2340,7 +2341,7 @@ extern "C" int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
 }
 extern "C" int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms, long long *calls) {
   if (!h) return -1;
-  for (int c = 0; c < 5; ++c) {
+  for (int c = 0; c < clgpu_solver::kPhases; ++c) {
     if (ms) ms[c] = h->prof[c];
     if (calls) calls[c] = h->prof_calls[c];
   }
@@ -2348,8 +2349,7 @@ extern "C" int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms, l
 }
 extern "C" int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes) {
   if (!h || !bytes) return -1;
-  bytes[0] = h->prof_bytes[0];
-  bytes[1] = h->prof_bytes[1];
+  for (int c = 0; c < 3; ++c) bytes[c] = h->prof_bytes[c];
   return 0;
 }
 extern "C" int clgpu_solver_update_data(clgpu_solver *h, const double *Px, const double *q,

@@ -898,7 +898,7 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
     // algorithmic bytes: every stream pass reads its entries, values and
     // chunk words once per side-pass; vectors are read / written once per use
     const double nl = k.Lp[po + N] - lbase, nk = k.Kp[po + N] - kbase, ts = sizeof(T);
-    k.prof_bytes[k.B + inst] +=
+    k.prof_bytes[(NR == 1 ? 1 : 2) * (size_t)k.B + inst] +=
         NR * 20.0 * N                                               // rhs gather, b
         + ntri * (2.0 * nl * (8 + ts) + 4.0 * (nfch + nbch) + ts * N)  // substitutions
         + nres * (16.0 * nk + 4.0 * nkch + 24.0 * N)                // residuals

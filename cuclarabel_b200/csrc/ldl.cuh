@@ -92,7 +92,8 @@ struct KKTDev {
   const int *spack2_inst, *spack2_off;
   int spack2_blocks, spack2_smem;
   // profiling only (else null): per instance, algorithmic bytes moved by the
-  // factorisations [0, B) and by the solves [B, 2B) of the profiled solve
+  // factorisations [0, B), the one-side solves [B, 2B) and the two-side
+  // solves [2B, 3B) of the profiled solve
   double *prof_bytes;
   // [B] kernel class: 1 = single warp (work vector in shared memory, the
   // streams above), 2 = block kernels with global scratch

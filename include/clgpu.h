@@ -155,17 +155,19 @@ int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,
                              double *ms_cones, double *ms_residual,
                              int *passes);
 /* per-phase device time of the last profiled solve (CUDA events on the solve
- * stream): ms[0] LDL factorisation, ms[1] LDL solves + refinement, ms[2] KKT
- * refresh (Hs scatter), ms[3] residual kernels, ms[4] update_scaling; calls
- * receives the number of timed launches of each phase.  No reference
- * counterpart (the reference times host phases with TimerOutputs). */
+ * stream), ms[6]: ms[0] LDL factorisation, ms[1] one-side LDL solves +
+ * refinement, ms[2] KKT refresh (Hs scatter), ms[3] residual kernels, ms[4]
+ * update_scaling, ms[5] two-side LDL solves (constant + affine rhs, see
+ * fused_solves); calls[6] receives the number of timed launches of each
+ * phase.  No reference counterpart (the reference times host phases with
+ * TimerOutputs). */
 int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms,
                                  long long *calls);
-/* algorithmic bytes of the last profiled solve: bytes[0] all LDL
- * factorisations, bytes[1] all LDL solves with refinement (each stream pass
- * reads its entries, values and chunk words once; vectors once per use).
- * Divided by the phase times this gives the achieved bandwidth.  No
- * reference counterpart. */
+/* algorithmic bytes of the last profiled solve, bytes[3]: bytes[0] all LDL
+ * factorisations, bytes[1] all one-side LDL solves, bytes[2] all two-side
+ * solves, with refinement (each stream pass reads its entries, values and
+ * chunk words once per side; vectors once per use).  Divided by the phase
+ * times this gives the achieved bandwidth.  No reference counterpart. */
 int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes);
 int clgpu_solver_destroy(clgpu_solver *h);
 
