@@ -78,7 +78,7 @@ EXPORTED = [
     "clgpu_solver_launch_count",
     "clgpu_solver_set_profiling", "clgpu_solver_get_profile", "clgpu_solver_get_phase_times",
     "clgpu_solver_get_phase_bytes",
-    "clgpu_solver_destroy",
+    "clgpu_solver_destroy", "clgpu_serve_admit", "clgpu_serve_step", "clgpu_serve_collect",
     "clgpu_cones_create", "clgpu_cones_destroy", "clgpu_cones_numel", "clgpu_cones_degree",
     "clgpu_cones_hs_len", "clgpu_update_scaling", "clgpu_set_identity_scaling",
     "clgpu_get_Hs", "clgpu_mul_Hs", "clgpu_affine_ds", "clgpu_combined_ds_shift",
@@ -107,6 +107,10 @@ def _declare(L):
     L.clgpu_solver_get_phase_times.argtypes = [c_void_p, dp, ctypes.POINTER(c_ll)]
     L.clgpu_solver_get_phase_bytes.argtypes = [c_void_p, dp]
     L.clgpu_solver_destroy.argtypes = [c_void_p]
+    L.clgpu_serve_admit.argtypes = [c_void_p, ip, c_int, dp, dp, c_void_p]
+    L.clgpu_serve_step.argtypes = [c_void_p, c_void_p, ip, ip, ip]
+    L.clgpu_serve_collect.argtypes = [c_void_p, ip, c_int, dp, dp, dp,
+                                      ctypes.POINTER(ClgpuInfo), c_void_p]
     L.clgpu_cones_create.argtypes = [c_int, ip, ip, dp, c_int, ctypes.POINTER(c_void_p)]
     L.clgpu_cones_destroy.argtypes = [c_void_p]
     for f in ("clgpu_cones_numel", "clgpu_cones_degree", "clgpu_cones_hs_len"):

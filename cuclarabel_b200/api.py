@@ -454,6 +454,77 @@ class BatchSolver:
             mo += m
         return out
 
+    # ------------------------------------------------------------ serving
+    # Continuous batching: the instances are slots.  serve_admit starts new
+    # solves in idle slots (optionally with new q / b, one array per slot)
+    # while others are mid-solve; serve_step runs one IPM iteration of every
+    # running slot and returns the slots that finished in it; serve_collect
+    # returns their solutions and frees the slots.
+
+    def serve_admit(self, slots, q=None, b=None, stream=0):
+        slots = np.ascontiguousarray(np.asarray(slots, dtype=np.int32))
+        if slots.size == 0:
+            return
+        def packed(vals, which):
+            if vals is None:
+                return None
+            if len(vals) != slots.size:
+                raise ValueError("one %s array per admitted slot" % which)
+            parts = []
+            for k, v in zip(slots, vals):
+                v = np.asarray(v, np.float64).ravel()
+                want = self.dims[k][0] if which == "q" else self.dims[k][1]
+                if v.size != want:
+                    raise ValueError("slot %d: %s needs %d values" % (k, which, want))
+                parts.append(v)
+            return _f64(np.concatenate(parts))
+        qv, bv = packed(q, "q"), packed(b, "b")
+        ptr = lambda v: None if v is None else v.ctypes.data_as(_lib.dp)  # noqa: E731
+        rc = _lib.load().clgpu_serve_admit(self._h, slots.ctypes.data_as(_lib.ip), slots.size,
+                                           ptr(qv), ptr(bv), ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError("clgpu_serve_admit failed with code %d" % rc)
+
+    def serve_step(self, stream=0):
+        """One IPM iteration of every running slot: (finished slots, running)."""
+        fin = np.empty(len(self.dims), np.int32)
+        nf, nr = ctypes.c_int(), ctypes.c_int()
+        rc = _lib.load().clgpu_serve_step(self._h, ctypes.c_void_p(stream),
+                                          fin.ctypes.data_as(_lib.ip), ctypes.byref(nf),
+                                          ctypes.byref(nr))
+        if rc != 0:
+            raise RuntimeError("clgpu_serve_step failed with code %d" % rc)
+        return fin[:nf.value].tolist(), nr.value
+
+    def serve_collect(self, slots, stream=0):
+        slots = np.ascontiguousarray(np.asarray(slots, dtype=np.int32))
+        n = slots.size
+        if n == 0:
+            return []
+        nx = sum(self.dims[k][0] for k in slots)
+        mz = sum(self.dims[k][1] for k in slots)
+        x, s, z = np.empty(max(nx, 1)), np.empty(max(mz, 1)), np.empty(max(mz, 1))
+        infos = (_lib.ClgpuInfo * n)()
+        rc = _lib.load().clgpu_serve_collect(self._h, slots.ctypes.data_as(_lib.ip), n,
+                                             x.ctypes.data_as(_lib.dp), s.ctypes.data_as(_lib.dp),
+                                             z.ctypes.data_as(_lib.dp), infos,
+                                             ctypes.c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError("clgpu_serve_collect failed with code %d" % rc)
+        out, xo, mo = [], 0, 0
+        for k, slot in enumerate(slots):
+            n_i, m_i = self.dims[slot]
+            inf = infos[k]
+            d = {f: getattr(inf, f) for f, _ in _lib.ClgpuInfo._fields_}
+            out.append(DefaultSolution(
+                x=x[xo:xo + n_i].copy(), z=z[mo:mo + m_i].copy(), s=s[mo:mo + m_i].copy(),
+                status=SolverStatus(inf.status), obj_val=inf.obj_val,
+                obj_val_dual=inf.obj_val_dual, solve_time=inf.solve_time,
+                iterations=inf.iterations, r_prim=inf.res_primal, r_dual=inf.res_dual, info=d))
+            xo += n_i
+            mo += m_i
+        return out
+
     def device_bytes(self):
         return _lib.load().clgpu_solver_device_bytes(self._h)
 

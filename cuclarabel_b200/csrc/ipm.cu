@@ -74,7 +74,9 @@ struct SettingsDev {
 };
 
 // =============================================================== masks
-__global__ void k_set_mask(Dev d, InstConst ic, int mode) {
+// sel (optional): only instances with sel[i] != 0 can be active (serving
+// admits a subset while other instances are mid-solve)
+__global__ void k_set_mask(Dev d, InstConst ic, int mode, const int *sel) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.B) return;
   bool undone = IF(d, I_DONE, i) == 0;
@@ -88,6 +90,7 @@ __global__ void k_set_mask(Dev d, InstConst ic, int mode) {
     case M_BT: v = undone && IF(d, I_SKIP, i) == 0 && IF(d, I_BT_ACTIVE, i); break;
     case M_ALL_UNDONE: v = undone; break;
   }
+  if (sel && !sel[i]) v = false;
   d.active[i] = v ? 1 : 0;
 }
 
@@ -99,9 +102,9 @@ __global__ void k_zero_fields(Dev d, int f0, int nf, double v) {
 
 // =============================================================== init
 __global__ void k_init_state(Dev d, const double *c, const double *normq,
-                             const double *normb, const int *pnnz) {
+                             const double *normb, const int *pnnz, const int *sel) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.B) return;
+  if (i >= d.B || (sel && !sel[i])) return;
   for (int f = 0; f < NUM_SCALARS; ++f) SF(d, f, i) = 0.0;
   for (int f = 0; f < NUM_INTS; ++f) IF(d, f, i) = 0;
   SF(d, F_TAU, i) = 1.0;
@@ -745,9 +748,9 @@ __global__ void k_count_running(Dev d) {
 // ============================================================ post-process
 // info_post_process! + solution_post_process! + variables_unscale!
 // (info.jl:275-291, solution.jl:2-50, variables.jl:373-403)
-__global__ void k_post_status(Dev d, SettingsDev st) {
+__global__ void k_post_status(Dev d, SettingsDev st, const int *sel) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.B) return;
+  if (i >= d.B || (sel && !sel[i])) return;
   int s = IF(d, I_STATUS, i);
   if (s == ST_NUMERICAL_ERROR || s == ST_INSUFFICIENT_PROGRESS || s == ST_MAX_ITERATIONS ||
       s == ST_MAX_TIME)
@@ -762,15 +765,15 @@ __device__ __forceinline__ bool status_infeasible(int s) {
 // out_x: instance-concatenated; out_s/out_z: instance-concatenated in user row
 // order, zmap[k] = global type-major row of output slot k
 __global__ void k_unscale(Dev d, const int *zmap, const int *zinst, double *ox, double *os,
-                          double *oz) {
+                          double *oz, const int *sel) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < d.nx) {
+  if (t < d.nx && !(sel && !sel[d.col_inst[t]])) {
     int inst = d.col_inst[t];
     int s = IF(d, I_STATUS, inst);
     double sinv = status_infeasible(s) ? 1.0 / SF(d, F_KAPPA, inst) : 1.0 / SF(d, F_TAU, inst);
     ox[t] = d.x[t] * d.d[t] * sinv;
   }
-  if (t < d.mz) {
+  if (t < d.mz && !(sel && !sel[zinst[t]])) {
     int g = zmap[t];
     int inst = zinst[t];
     int s = IF(d, I_STATUS, inst);
@@ -833,8 +836,20 @@ struct clgpu_solver {
   int2 *d_upd_pxy = nullptr, *d_upd_axy = nullptr;
   double *d_in_P = nullptr, *d_in_A = nullptr, *d_in_q = nullptr, *d_in_b = nullptr;
   double prof_bytes[3] = {0, 0, 0};  // factor, one-side, two-side solves (last profiled solve)
+  // serving (continuous batching): instances are slots; mask_sel restricts
+  // the masks to the slots being started; d_run flags the running slots;
+  // d_list / h_list carry slot lists; slot_state: 0 idle, 1 running, 2
+  // finished (awaiting collect)
+  const int *mask_sel = nullptr;
+  int *d_sel = nullptr, *d_run = nullptr, *d_list = nullptr, *h_list = nullptr;
+  double *d_info = nullptr, *h_info = nullptr;
+  bool serving = false;
+  std::vector<int> slot_state;
+  std::vector<std::chrono::steady_clock::time_point> slot_t0;
   ~clgpu_solver() {
     if (h_counter) cudaFreeHost(h_counter);
+    if (h_list) cudaFreeHost(h_list);
+    if (h_info) cudaFreeHost(h_info);
     for (auto e : ev_pool) cudaEventDestroy(e);
   }
   int next_event() {
@@ -1931,6 +1946,15 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     h->h_m[i] = prep[i].m;
   }
   cudaMallocHost(&h->h_counter, 4 * sizeof(int));
+  // serving buffers
+  h->d_sel = A.alloc<int>(B);
+  h->d_run = A.alloc<int>(B);
+  h->d_list = A.alloc<int>(B);
+  h->d_info = A.alloc<double>((size_t)B * (NUM_SCALARS + NUM_INTS));
+  cudaMallocHost(&h->h_list, (size_t)B * sizeof(int));
+  cudaMallocHost(&h->h_info, (size_t)B * (NUM_SCALARS + NUM_INTS) * sizeof(double));
+  h->slot_state.assign(B, 0);
+  h->slot_t0.assign(B, std::chrono::steady_clock::now());
   if (A.err != cudaSuccess) return -1000 - (int)A.err;
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return -1000 - (int)e;
@@ -2012,7 +2036,7 @@ struct Phase {
   cudaStream_t st;
   Dev &d() { return h->dv; }
   void mask(int mode) {
-    k_set_mask<<<nblk(h->B), TB, 0, st>>>(h->dv, h->ic, mode);
+    k_set_mask<<<nblk(h->B), TB, 0, st>>>(h->dv, h->ic, mode, h->mask_sel);
     h->launches++;
   }
   void zero(int f0, int nf, double v = 0.0) {
@@ -2097,25 +2121,15 @@ struct Phase {
   }
 };
 
-extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
-  if (!h) return -1;
-  cudaStream_t st = (cudaStream_t)stream;
-  auto t0 = std::chrono::steady_clock::now();
-  Phase P{h, st};
+// solver_default_start! (solver.jl:425-446) for every instance, or with
+// h->mask_sel set only for the selected ones (the others are untouched)
+static void ipm_start(clgpu_solver *h, Phase &P, cudaStream_t st) {
   Dev &dv = h->dv;
   const int B = h->B;
-  h->launches = 0;
-  if (h->profiling && h->d_prof_bytes)
-    cudaMemsetAsync(h->d_prof_bytes, 0, 3 * (size_t)B * sizeof(double), st);
-  h->kk.prof_bytes = h->profiling ? h->d_prof_bytes : nullptr;
-  cudaEvent_t ev0, ev1;
-  cudaEventCreate(&ev0);
-  cudaEventCreate(&ev1);
-  cudaEventRecord(ev0, st);
   // (re)initialise every per-instance scalar; solve! may be called repeatedly
-  k_init_state<<<nblk(B), TB, 0, st>>>(dv, h->d_c, h->d_normq, h->d_normb, h->d_pnnz);
-  k_set_mask<<<nblk(B), TB, 0, st>>>(dv, h->ic, M_ALL_UNDONE);
-  // solver_default_start! (solver.jl:425-446)
+  k_init_state<<<nblk(B), TB, 0, st>>>(dv, h->d_c, h->d_normq, h->d_normb, h->d_pnnz,
+                                        h->mask_sel);
+  P.mask(M_ALL_UNDONE);
   if (h->any_sym) {
     P.mask(M_SYM);
     cones_set_identity_scaling(h->cs, st);
@@ -2152,6 +2166,154 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     k_zero_x_masked<<<nblk(dv.nx), TB, 0, st>>>(dv);
     k_set_tau_kappa_one<<<nblk(B), TB, 0, st>>>(dv);
   }
+}
+
+// slots that finished in the pass just run: flagged running, now done
+__global__ void k_serve_finished(Dev d, int *run, int *list, int *count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  if (run[i] && IF(d, I_DONE, i)) {
+    run[i] = 0;
+    list[atomicAdd(count, 1)] = i;
+  }
+}
+
+// one pass of the IPM loop (solver.jl:265-393) over every running instance;
+// returns how many are still running.  serve: also list the slots that
+// finished in this pass into h->h_list (count in *nfin).
+static int ipm_pass(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed, bool serve,
+                    int *nfin) {
+  Dev &dv = h->dv;
+  const int B = h->B;
+  P.mask(M_PASS);
+  P.residuals();
+  k_info_termination<<<nblk(B), TB, 0, st>>>(dv, h->ic, h->sd, elapsed, h->d_reset);
+  k_reset_vars<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_reset);
+  P.mask(M_PASS);
+  // update_scaling
+  h->prof_begin(4, st);
+  cones_update_scaling(h->cs, dv.s, dv.z, dv.S + F_MU * B, dv.I + I_SCALING * B,
+                       dv.I + I_SCALE_OK * B, st);
+  h->prof_end(st);
+  k_after_scaling<<<nblk(B), TB, 0, st>>>(dv);
+  P.mask(M_PASS);
+  // KKT update and affine step; the affine rhs needs nothing from the new
+  // factor, so kkt_update!'s constant solve runs with the affine solve
+  const bool fused = h->st.fused_solves != 0;
+  if (fused)
+    P.kkt_refactor();
+  else
+    P.kkt_update();
+  k_affine_rhs<<<nblk(std::max(std::max(dv.nx, dv.mz), B)), TB, 0, st>>>(dv);
+  cones_affine_ds(h->cs, dv.rhs_s, dv.s, st);
+  P.kkt_solve(true, fused);
+  P.step_length(false, F_ALPHA_AFF);
+  k_combined_scalars<<<nblk(B), TB, 0, st>>>(dv);
+  k_combined_pre<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
+  cones_combined_ds_shift(h->cs, dv.rhs_z, dv.dz, dv.ds, dv.S + F_SIGMA_MU * B, st);
+  k_combined_post<<<nblk(dv.mz), TB, 0, st>>>(dv);
+  P.kkt_solve(false);
+  k_check_numerical<<<nblk(B), TB, 0, st>>>(dv, h->ic);
+  P.mask(M_PASS);
+  P.step_length(true, F_ALPHA);
+  if (h->any_asym) {
+    cudaMemsetAsync(dv.counter + 1, 0, sizeof(int), st);
+    k_bt_setup<<<nblk(B), TB, 0, st>>>(dv, h->ic);
+    if (P.read_counter(1) > 0) {
+      P.mask(M_BT);
+      for (int j = 0; j < 50; ++j) {
+        P.zero(F_BARRIER, 1);
+        k_dot_shifted<kRedThreads><<<B, kRedThreads, 0, st>>>(dv);
+        k_bt_central<<<nblk(B), TB, 0, st>>>(dv, h->ic);
+        cones_barrier(h->cs, dv.z, dv.s, dv.dz, dv.ds, dv.S + F_ALPHA * B,
+                      dv.I + I_BT_ACTIVE * B, dv.S + F_BARRIER * B, st);
+        cudaMemsetAsync(dv.counter + 1, 0, sizeof(int), st);
+        k_bt_check<<<nblk(B), TB, 0, st>>>(dv, h->st.linesearch_backtrack_step);
+        P.mask(M_BT);
+        if (P.read_counter(1) == 0) break;
+      }
+      P.mask(M_PASS);
+    }
+  }
+  k_check_small_step<<<nblk(B), TB, 0, st>>>(dv, h->ic, h->sd);
+  P.mask(M_PASS);
+  k_add_step<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
+  k_add_step_scalars<<<nblk(B), TB, 0, st>>>(dv);
+  cudaMemsetAsync(dv.counter, 0, 3 * sizeof(int), st);
+  k_count_running<<<nblk(B), TB, 0, st>>>(dv);
+  if (serve) k_serve_finished<<<nblk(B), TB, 0, st>>>(dv, h->d_run, h->d_list, dv.counter + 2);
+  h->launches += 25;
+  const int running = P.read_counter(0);
+  if (serve) {
+    *nfin = h->h_counter[2];
+    if (*nfin > 0) {
+      cudaMemcpyAsync(h->h_list, h->d_list, (size_t)*nfin * sizeof(int),
+                      cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      std::sort(h->h_list, h->h_list + *nfin);
+    }
+  }
+  if (h->st.verbose) {
+    // per-pass trace of instance 0 (same columns as the CPU oracle's)
+    double sv[NUM_SCALARS];
+    int iv[NUM_INTS];
+    for (int f = 0; f < NUM_SCALARS; ++f)
+      cudaMemcpy(&sv[f], dv.S + (size_t)f * B, sizeof(double), cudaMemcpyDeviceToHost);
+    for (int f = 0; f < NUM_INTS; ++f)
+      cudaMemcpy(&iv[f], dv.I + (size_t)f * B, sizeof(int), cudaMemcpyDeviceToHost);
+    std::fprintf(stderr,
+                 "%3d  %+.8e  %+.8e  %.2e %.2e %.2e %.2e %.2e  a=%.3e st=%d sc=%d ok=%d\n",
+                 iv[I_ITER], sv[F_COST_P], sv[F_COST_D], sv[F_GAP_REL], sv[F_RES_P],
+                 sv[F_RES_D], sv[F_KTRATIO], sv[F_MU], sv[F_ALPHA], iv[I_STATUS],
+                 iv[I_SCALING], iv[I_KKT_OK]);
+  }
+  return running;
+}
+
+// DefaultInfo of instance i from its scalar / integer fields
+template <typename SF_, typename IF_>
+static void fill_info(clgpu_info &inf, SF_ s, IF_ iv, double solve_time) {
+  inf.status = iv(I_STATUS);
+  inf.iterations = iv(I_ITER);
+  inf.cost_primal = s(F_COST_P);
+  inf.cost_dual = s(F_COST_D);
+  bool infeas = inf.status == ST_PRIMAL_INFEASIBLE || inf.status == ST_DUAL_INFEASIBLE ||
+                inf.status == ST_ALMOST_PRIMAL_INFEASIBLE ||
+                inf.status == ST_ALMOST_DUAL_INFEASIBLE;
+  inf.obj_val = infeas ? NAN : inf.cost_primal;
+  inf.obj_val_dual = infeas ? NAN : inf.cost_dual;
+  inf.res_primal = s(F_RES_P);
+  inf.res_dual = s(F_RES_D);
+  inf.res_primal_inf = s(F_RES_PINF);
+  inf.res_dual_inf = s(F_RES_DINF);
+  inf.gap_abs = s(F_GAP_ABS);
+  inf.gap_rel = s(F_GAP_REL);
+  inf.ktratio = s(F_KTRATIO);
+  inf.mu = s(F_MU);
+  inf.sigma = s(F_SIGMA);
+  inf.step_length = s(F_ALPHA);
+  inf.solve_time = solve_time;
+}
+
+extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
+  if (!h) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto t0 = std::chrono::steady_clock::now();
+  Phase P{h, st};
+  Dev &dv = h->dv;
+  const int B = h->B;
+  h->launches = 0;
+  h->serving = false;
+  h->mask_sel = nullptr;
+  std::fill(h->slot_state.begin(), h->slot_state.end(), 0);
+  if (h->profiling && h->d_prof_bytes)
+    cudaMemsetAsync(h->d_prof_bytes, 0, 3 * (size_t)B * sizeof(double), st);
+  h->kk.prof_bytes = h->profiling ? h->d_prof_bytes : nullptr;
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0, st);
+  ipm_start(h, P, st);
   // ----------------------------------------------------------- main loop
   int passes = 0;
   const int max_passes = 4 * (h->st.max_iter + 5);
@@ -2159,79 +2321,7 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     ++passes;
     double elapsed =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    P.mask(M_PASS);
-    P.residuals();
-    k_info_termination<<<nblk(B), TB, 0, st>>>(dv, h->ic, h->sd, elapsed, h->d_reset);
-    k_reset_vars<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_reset);
-    P.mask(M_PASS);
-    // update_scaling
-    h->prof_begin(4, st);
-    cones_update_scaling(h->cs, dv.s, dv.z, dv.S + F_MU * B, dv.I + I_SCALING * B,
-                         dv.I + I_SCALE_OK * B, st);
-    h->prof_end(st);
-    k_after_scaling<<<nblk(B), TB, 0, st>>>(dv);
-    P.mask(M_PASS);
-    // KKT update and affine step; the affine rhs needs nothing from the new
-    // factor, so kkt_update!'s constant solve runs with the affine solve
-    const bool fused = h->st.fused_solves != 0;
-    if (fused)
-      P.kkt_refactor();
-    else
-      P.kkt_update();
-    k_affine_rhs<<<nblk(std::max(std::max(dv.nx, dv.mz), B)), TB, 0, st>>>(dv);
-    cones_affine_ds(h->cs, dv.rhs_s, dv.s, st);
-    P.kkt_solve(true, fused);
-    P.step_length(false, F_ALPHA_AFF);
-    k_combined_scalars<<<nblk(B), TB, 0, st>>>(dv);
-    k_combined_pre<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
-    cones_combined_ds_shift(h->cs, dv.rhs_z, dv.dz, dv.ds, dv.S + F_SIGMA_MU * B, st);
-    k_combined_post<<<nblk(dv.mz), TB, 0, st>>>(dv);
-    P.kkt_solve(false);
-    k_check_numerical<<<nblk(B), TB, 0, st>>>(dv, h->ic);
-    P.mask(M_PASS);
-    P.step_length(true, F_ALPHA);
-    if (h->any_asym) {
-      cudaMemsetAsync(dv.counter + 1, 0, sizeof(int), st);
-      k_bt_setup<<<nblk(B), TB, 0, st>>>(dv, h->ic);
-      if (P.read_counter(1) > 0) {
-        P.mask(M_BT);
-        for (int j = 0; j < 50; ++j) {
-          P.zero(F_BARRIER, 1);
-          k_dot_shifted<kRedThreads><<<B, kRedThreads, 0, st>>>(dv);
-          k_bt_central<<<nblk(B), TB, 0, st>>>(dv, h->ic);
-          cones_barrier(h->cs, dv.z, dv.s, dv.dz, dv.ds, dv.S + F_ALPHA * B,
-                        dv.I + I_BT_ACTIVE * B, dv.S + F_BARRIER * B, st);
-          cudaMemsetAsync(dv.counter + 1, 0, sizeof(int), st);
-          k_bt_check<<<nblk(B), TB, 0, st>>>(dv, h->st.linesearch_backtrack_step);
-          P.mask(M_BT);
-          if (P.read_counter(1) == 0) break;
-        }
-        P.mask(M_PASS);
-      }
-    }
-    k_check_small_step<<<nblk(B), TB, 0, st>>>(dv, h->ic, h->sd);
-    P.mask(M_PASS);
-    k_add_step<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv);
-    k_add_step_scalars<<<nblk(B), TB, 0, st>>>(dv);
-    cudaMemsetAsync(dv.counter, 0, sizeof(int), st);
-    k_count_running<<<nblk(B), TB, 0, st>>>(dv);
-    h->launches += 25;
-    int running = P.read_counter(0);
-    if (h->st.verbose) {
-      // per-pass trace of instance 0 (same columns as the CPU oracle's)
-      double sv[NUM_SCALARS];
-      int iv[NUM_INTS];
-      for (int f = 0; f < NUM_SCALARS; ++f)
-        cudaMemcpy(&sv[f], dv.S + (size_t)f * B, sizeof(double), cudaMemcpyDeviceToHost);
-      for (int f = 0; f < NUM_INTS; ++f)
-        cudaMemcpy(&iv[f], dv.I + (size_t)f * B, sizeof(int), cudaMemcpyDeviceToHost);
-      std::fprintf(stderr,
-                   "%3d  %+.8e  %+.8e  %.2e %.2e %.2e %.2e %.2e  a=%.3e st=%d sc=%d ok=%d\n",
-                   iv[I_ITER], sv[F_COST_P], sv[F_COST_D], sv[F_GAP_REL], sv[F_RES_P],
-                   sv[F_RES_D], sv[F_KTRATIO], sv[F_MU], sv[F_ALPHA], iv[I_STATUS],
-                   iv[I_SCALING], iv[I_KKT_OK]);
-    }
-    if (running == 0) break;
+    if (ipm_pass(h, P, st, elapsed, false, nullptr) == 0) break;
   }
   h->passes = passes;
   if (h->profiling) {
@@ -2239,9 +2329,10 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     h->prof_collect();
   }
   // post-process
-  k_post_status<<<nblk(B), TB, 0, st>>>(dv, h->sd);
+  k_post_status<<<nblk(B), TB, 0, st>>>(dv, h->sd, nullptr);
   double *ox = h->d_out, *os = ox + dv.nx, *oz = os + dv.mz;
-  k_unscale<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_zmap, h->d_zinst, ox, os, oz);
+  k_unscale<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_zmap, h->d_zinst, ox, os, oz,
+                                                        nullptr);
   cudaEventRecord(ev1, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return -1000 - (int)e;
@@ -2260,31 +2351,171 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
   h->sol.resize((size_t)dv.nx + 2 * (size_t)dv.mz);
   cudaMemcpy(h->sol.data(), h->d_out, h->sol.size() * sizeof(double), cudaMemcpyDeviceToHost);
   double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  for (int i = 0; i < B; ++i) {
-    clgpu_info &inf = h->info[i];
-    auto s = [&](int f) { return S[(size_t)f * B + i]; };
-    inf.status = I[(size_t)I_STATUS * B + i];
-    inf.iterations = I[(size_t)I_ITER * B + i];
-    inf.cost_primal = s(F_COST_P);
-    inf.cost_dual = s(F_COST_D);
-    bool infeas = inf.status == ST_PRIMAL_INFEASIBLE || inf.status == ST_DUAL_INFEASIBLE ||
-                  inf.status == ST_ALMOST_PRIMAL_INFEASIBLE ||
-                  inf.status == ST_ALMOST_DUAL_INFEASIBLE;
-    inf.obj_val = infeas ? NAN : inf.cost_primal;
-    inf.obj_val_dual = infeas ? NAN : inf.cost_dual;
-    inf.res_primal = s(F_RES_P);
-    inf.res_dual = s(F_RES_D);
-    inf.res_primal_inf = s(F_RES_PINF);
-    inf.res_dual_inf = s(F_RES_DINF);
-    inf.gap_abs = s(F_GAP_ABS);
-    inf.gap_rel = s(F_GAP_REL);
-    inf.ktratio = s(F_KTRATIO);
-    inf.mu = s(F_MU);
-    inf.sigma = s(F_SIGMA);
-    inf.step_length = s(F_ALPHA);
-    inf.solve_time = elapsed;
-  }
+  for (int i = 0; i < B; ++i)
+    fill_info(
+        h->info[i], [&](int f) { return S[(size_t)f * B + i]; },
+        [&](int f) { return I[(size_t)f * B + i]; }, elapsed);
   h->solved = true;
+  return 0;
+}
+
+// ------------------------------------------------------------- serving
+__global__ void k_serve_mark_idle(Dev d, int *run) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.B) return;
+  IF(d, I_DONE, i) = 1;
+  run[i] = 0;
+}
+// sel[i] = 1 for the listed slots (sel zeroed before); run[i] = 1 too if given
+__global__ void k_serve_set(const int *list, int n, int *sel, int *run) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  sel[list[t]] = 1;
+  if (run) run[list[t]] = 1;
+}
+// scalar and integer fields of the listed slots, packed slot by slot
+__global__ void k_serve_gather_info(Dev d, const int *list, int n, double *out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = list[t];
+  double *o = out + (size_t)t * (NUM_SCALARS + NUM_INTS);
+  for (int f = 0; f < NUM_SCALARS; ++f) o[f] = SF(d, f, i);
+  for (int f = 0; f < NUM_INTS; ++f) o[NUM_SCALARS + f] = (double)IF(d, f, i);
+}
+
+static int serve_upload_list(clgpu_solver *h, const int *slots, int n, int *run,
+                             cudaStream_t st) {
+  std::memcpy(h->h_list, slots, (size_t)n * sizeof(int));
+  cudaMemcpyAsync(h->d_list, h->h_list, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(h->d_sel, 0, (size_t)h->B * sizeof(int), st);
+  k_serve_set<<<nblk(n), TB, 0, st>>>(h->d_list, n, h->d_sel, run);
+  return 0;
+}
+
+extern "C" int clgpu_serve_admit(clgpu_solver *h, const int *slots, int n, const double *q,
+                                 const double *b, clgpu_stream_t stream) {
+  if (!h || n < 0 || (n > 0 && !slots)) return -1;
+  if (n == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  Dev &dv = h->dv;
+  std::vector<char> seen(h->B, 0);
+  for (int k = 0; k < n; ++k) {
+    const int i = slots[k];
+    if (i < 0 || i >= h->B || seen[i]) return -2;
+    if (h->serving && h->slot_state[i] != 0) return -3;  // slot busy or not collected
+    seen[i] = 1;
+  }
+  if (!h->serving) {
+    k_serve_mark_idle<<<nblk(h->B), TB, 0, st>>>(dv, h->d_run);
+    std::fill(h->slot_state.begin(), h->slot_state.end(), 0);
+    h->serving = true;
+    h->kk.prof_bytes = nullptr;
+  }
+  // new q / b values (packed slot by slot), scaled with the setup equilibration
+  long long qo = 0, bo = 0;
+  for (int k = 0; k < n; ++k) {
+    const int i = slots[k];
+    const int x0 = h->h_xoff[i], x1 = h->h_xoff[i + 1];
+    const int m0 = h->h_moff[i], m1 = h->h_moff[i + 1];
+    if (q && x1 > x0) {
+      cudaMemcpyAsync(h->d_in_q + x0, q + qo, (size_t)(x1 - x0) * sizeof(double),
+                      cudaMemcpyHostToDevice, st);
+      k_update_q<<<nblk(x1 - x0), TB, 0, st>>>(dv, h->d_in_q, x0, x1, h->d_c);
+    }
+    if (b && m1 > m0) {
+      cudaMemcpyAsync(h->d_in_b + m0, b + bo, (size_t)(m1 - m0) * sizeof(double),
+                      cudaMemcpyHostToDevice, st);
+      k_update_b<<<nblk(m1 - m0), TB, 0, st>>>(dv, h->d_in_b, m0, m1, h->d_zmap);
+    }
+    if (q || b)
+      k_update_norms<128><<<1, 128, 0, st>>>(q ? h->d_in_q : nullptr, b ? h->d_in_b : nullptr,
+                                             dv.xoff, h->d_moff, i, h->d_normq, h->d_normb);
+    qo += x1 - x0;
+    bo += m1 - m0;
+  }
+  // the starting point of the admitted slots only; they join the next step
+  serve_upload_list(h, slots, n, h->d_run, st);
+  Phase P{h, st};
+  h->mask_sel = h->d_sel;
+  ipm_start(h, P, st);
+  h->mask_sel = nullptr;
+  const auto now = std::chrono::steady_clock::now();
+  for (int k = 0; k < n; ++k) {
+    h->slot_state[slots[k]] = 1;
+    h->slot_t0[slots[k]] = now;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // caller buffers consumed
+  return e == cudaSuccess ? 0 : -1000 - (int)e;
+}
+
+extern "C" int clgpu_serve_step(clgpu_solver *h, clgpu_stream_t stream, int *finished,
+                                int *nfinished, int *nrunning) {
+  if (!h || !h->serving) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  Phase P{h, st};
+  int nfin = 0;
+  const int running = ipm_pass(h, P, st, 0.0, true, &nfin);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return -1000 - (int)e;
+  for (int k = 0; k < nfin; ++k) {
+    h->slot_state[h->h_list[k]] = 2;
+    if (finished) finished[k] = h->h_list[k];
+  }
+  if (nfinished) *nfinished = nfin;
+  if (nrunning) *nrunning = running;
+  return 0;
+}
+
+extern "C" int clgpu_serve_collect(clgpu_solver *h, const int *slots, int n, double *x,
+                                   double *s, double *z, clgpu_info *info,
+                                   clgpu_stream_t stream) {
+  if (!h || !h->serving || n < 0 || (n > 0 && !slots)) return -1;
+  if (n == 0) return 0;
+  for (int k = 0; k < n; ++k)
+    if (slots[k] < 0 || slots[k] >= h->B || h->slot_state[slots[k]] != 2) return -2;
+  cudaStream_t st = (cudaStream_t)stream;
+  Dev &dv = h->dv;
+  serve_upload_list(h, slots, n, nullptr, st);
+  k_post_status<<<nblk(h->B), TB, 0, st>>>(dv, h->sd, h->d_sel);
+  double *ox = h->d_out, *os = ox + dv.nx, *oz = os + dv.mz;
+  k_unscale<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_zmap, h->d_zinst, ox, os, oz,
+                                                        h->d_sel);
+  k_serve_gather_info<<<nblk(n), TB, 0, st>>>(dv, h->d_list, n, h->d_info);
+  constexpr int NF = NUM_SCALARS + NUM_INTS;
+  cudaMemcpyAsync(h->h_info, h->d_info, (size_t)n * NF * sizeof(double),
+                  cudaMemcpyDeviceToHost, st);
+  long long xo = 0, mo = 0;
+  for (int k = 0; k < n; ++k) {
+    const int i = slots[k];
+    const int nx_i = h->h_n[i], m_i = h->h_m[i];
+    if (x && nx_i)
+      cudaMemcpyAsync(x + xo, ox + h->h_xoff[i], (size_t)nx_i * sizeof(double),
+                      cudaMemcpyDeviceToHost, st);
+    if (s && m_i)
+      cudaMemcpyAsync(s + mo, os + h->h_moff[i], (size_t)m_i * sizeof(double),
+                      cudaMemcpyDeviceToHost, st);
+    if (z && m_i)
+      cudaMemcpyAsync(z + mo, oz + h->h_moff[i], (size_t)m_i * sizeof(double),
+                      cudaMemcpyDeviceToHost, st);
+    xo += nx_i;
+    mo += m_i;
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return -1000 - (int)e;
+  const auto now = std::chrono::steady_clock::now();
+  for (int k = 0; k < n; ++k) {
+    const int i = slots[k];
+    const double *o = h->h_info + (size_t)k * NF;
+    const double t = std::chrono::duration<double>(now - h->slot_t0[i]).count();
+    clgpu_info inf{};
+    fill_info(
+        inf, [&](int f) { return o[f]; }, [&](int f) { return (int)o[NUM_SCALARS + f]; }, t);
+    if (info) info[k] = inf;
+    h->info[i] = inf;
+    h->slot_state[i] = 0;
+  }
   return 0;
 }
 

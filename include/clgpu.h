@@ -171,6 +171,26 @@ int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms,
 int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes);
 int clgpu_solver_destroy(clgpu_solver *h);
 
+/* ------------------------------------------------ serving (continuous batching)
+ * The instances of a solver are slots with fixed structure (P, A sparsity,
+ * cones).  admit starts new solves in idle slots, with new q / b values when
+ * given (packed slot by slot in the order of `slots`; NULL keeps the current
+ * values), while other slots are mid-solve; step runs one IPM iteration of
+ * every running slot and lists the slots that finished in it (ascending);
+ * collect post-processes finished slots, copies their x / s / z (packed slot
+ * by slot in user order) and infos to the host, and makes them idle again.
+ * A slot's result is exactly that of solving it alone.  The first admit
+ * makes every slot idle; clgpu_solver_solve leaves serving.  Returns 0, -1 on
+ * a bad argument, -2 on a bad or repeated slot, -3 when admitting a slot that
+ * is running or not yet collected.  No reference counterpart (the reference
+ * has no serving loop; config 5 of the benchmark plan). */
+int clgpu_serve_admit(clgpu_solver *h, const int *slots, int n, const double *q,
+                      const double *b, clgpu_stream_t stream);
+int clgpu_serve_step(clgpu_solver *h, clgpu_stream_t stream, int *finished,
+                     int *nfinished, int *nrunning);
+int clgpu_serve_collect(clgpu_solver *h, const int *slots, int n, double *x, double *s,
+                        double *z, clgpu_info *info, clgpu_stream_t stream);
+
 /* --------------------------------------------------------------- cones */
 /* CompositeConeGPU{T}(cones, soc_threshold)
  * (src/gpucones/compositecone_type_gpu.jl:72-216).  Cones must be sorted
