@@ -259,6 +259,87 @@ def ncu_traffic(summary):
     return None
 
 
+def serve_run(solver, pbs, lam, seconds, seed, stream):
+    """Continuous batching under a Poisson request stream (config 5 shape,
+    its config-4 part): `lam` requests/s for `seconds`, each for a uniformly
+    drawn slot (one of the resident MPC structures) with new q / b (the
+    structure's values plus noise, as a new MPC state would give).  Requests
+    are admitted at IPM-step boundaries as their slot frees up, run one IPM
+    iteration per step together with every other running request, and are
+    collected when done.  Latency = arrival to result on the host."""
+    import collections
+    rng = np.random.default_rng(seed)
+    B = len(pbs)
+    n = int(rng.poisson(lam * seconds))
+    arrive = np.sort(rng.uniform(0.0, seconds, n))
+    slot_of = rng.integers(0, B, n)
+    queues = collections.defaultdict(collections.deque)
+    busy = {}          # slot -> request
+    lat, statuses, iters = [], collections.Counter(), []
+    nxt, running, steps, occupancy = 0, 0, 0, 0
+    t_admit = t_step = t_collect = 0.0
+    n_admit = 0
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < n and arrive[nxt] <= now:
+            queues[int(slot_of[nxt])].append(nxt)
+            nxt += 1
+        adm, qv, bv = [], [], []
+        for slot in list(queues):
+            if slot in busy or not queues[slot]:
+                continue
+            r = queues[slot].popleft()
+            if not queues[slot]:
+                del queues[slot]
+            P, q, A, b, cones = pbs[slot]
+            qv.append(q + 0.05 * rng.standard_normal(len(q)))
+            bv.append(b + 0.02 * np.abs(rng.standard_normal(len(b))))
+            adm.append(slot)
+            busy[slot] = r
+        if adm:
+            ta = time.perf_counter()
+            solver.serve_admit(adm, q=qv, b=bv, stream=stream)
+            t_admit += time.perf_counter() - ta
+            n_admit += 1
+            running += len(adm)
+        if running:
+            ta = time.perf_counter()
+            fin, running = solver.serve_step(stream)
+            t_step += time.perf_counter() - ta
+            steps += 1
+            occupancy += running + len(fin)
+            if fin:
+                ta = time.perf_counter()
+                sols = solver.serve_collect(fin, stream)
+                t_collect += time.perf_counter() - ta
+                done = time.perf_counter() - t0
+                for slot, sol in zip(fin, sols):
+                    r = busy.pop(slot)
+                    lat.append(done - arrive[r])
+                    statuses[sol.status.name] += 1
+                    iters.append(sol.iterations)
+        elif nxt < n:
+            time.sleep(max(0.0, arrive[nxt] - (time.perf_counter() - t0)))
+        elif not queues:
+            break
+    wall = time.perf_counter() - t0
+    solved = statuses.get("SOLVED", 0)
+    return {"lambda_per_s": lam, "seconds": seconds, "requests": n, "completed": len(lat),
+            "value": solved / wall, "unit": "solves/s", "wall_s": wall,
+            "p50_ms": 1000 * float(np.percentile(lat, 50)),
+            "p99_ms": 1000 * float(np.percentile(lat, 99)),
+            "steps": steps, "mean_running": occupancy / max(steps, 1),
+            "ms_per_step": {"admit": 1000 * t_admit / max(n_admit, 1),
+                            "admissions": n_admit,
+                            "iterate": 1000 * t_step / max(steps, 1),
+                            "collect": 1000 * t_collect / max(steps, 1),
+                            "wall": 1000 * wall / max(steps, 1)},
+            "iters_mean": float(np.mean(iters)), "status": dict(statuses),
+            "mix": "config-4-like requests only (the 5 % config-2-like large requests of the "
+                   "serving config are not in this run)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -270,6 +351,9 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=5.0,
+                    help="length of the served (continuous batching) run; 0 skips it")
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -424,6 +508,15 @@ def main():
                  "p50_ms": 1000 * float(np.percentile(lat, 50)),
                  "p99_ms": 1000 * float(np.percentile(lat, 99)), "method": "cudss"}
 
+    # ---- served: continuous batching under a Poisson request stream
+    served = None
+    if rank == 0 and args.serve_seconds > 0:
+        srv = BatchSolver(pbs, direct_solve_method=args.method)
+        served = serve_run(srv, pbs, args.serve_rate, args.serve_seconds, 12345 + rank, sh)
+        del srv
+        if plain:
+            served["vs_plain_solves"] = served["value"] / plain["value"]
+
     # ---- roofline: the dominant device phase (an LDL kernel), plus the
     # update_scaling cone kernels for reference
     peaks, peak_kind = load_peaks()
@@ -495,6 +588,7 @@ def main():
                       "batch_latency_ms": 1000 * elapsed / args.steps},
             "plain_gpu": plain,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
+            "served": served,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

@@ -79,7 +79,9 @@ struct SettingsDev {
 __global__ void k_set_mask(Dev d, InstConst ic, int mode, const int *sel) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.B) return;
-  bool undone = IF(d, I_DONE, i) == 0;
+  // with sel (admitting), the selected slots stay marked done until they are
+  // activated at a step boundary, so they count as undone here
+  bool undone = sel ? true : IF(d, I_DONE, i) == 0;
   bool v = false;
   switch (mode) {
     case M_PASS: v = undone && IF(d, I_SKIP, i) == 0; break;
@@ -125,6 +127,8 @@ __global__ void k_init_state(Dev d, const double *c, const double *normq,
   IF(d, I_SCALING, i) = 0;  // PrimalDual (every supported cone allows it)
   IF(d, I_KKT_OK, i) = 1;
   IF(d, I_SCALE_OK, i) = 1;
+  // an admitted slot (sel) stays out of the running passes until activated
+  if (sel) IF(d, I_DONE, i) = 1;
 }
 
 // x = 0 for the asymmetric (unit) start, tau = kappa = 1
@@ -840,16 +844,38 @@ struct clgpu_solver {
   // the masks to the slots being started; d_run flags the running slots;
   // d_list / h_list carry slot lists; slot_state: 0 idle, 1 running, 2
   // finished (awaiting collect)
+  // Admissions run on their own stream (st_admit) through views (dv_admit,
+  // cs_admit) whose active mask is separate, overlapping the running pass;
+  // an admitted batch joins at the step after the one it was admitted
+  // before (fresh -> aged -> activated), so it never joins a pass midway.
   const int *mask_sel = nullptr;
-  int *d_sel = nullptr, *d_run = nullptr, *d_list = nullptr, *h_list = nullptr;
-  double *d_info = nullptr, *h_info = nullptr;
+  int *d_sel = nullptr, *d_sel_admit = nullptr, *d_run = nullptr, *d_active_admit = nullptr;
+  int *d_list = nullptr, *d_list_admit = nullptr, *d_list_collect = nullptr,
+      *d_list_act = nullptr;
+  int *h_list = nullptr, *h_list_admit = nullptr, *h_list_collect = nullptr,
+      *h_list_act = nullptr;
+  double *d_info = nullptr, *h_info = nullptr, *h_stage = nullptr;
   bool serving = false;
-  std::vector<int> slot_state;
+  Dev dv_admit{};
+  ConeSet cs_admit{};
+  cudaStream_t st_admit = nullptr;
+  cudaEvent_t ev_admit[2] = {nullptr, nullptr};  // alternate between admissions
+  int ev_fresh = 0, ev_aged = 0;                 // event of the fresh / aged batch
+  std::vector<int> fresh, aged;  // admitted slots awaiting activation
+  std::vector<int> slot_state;   // 0 idle, 1 running, 2 finished, 3 admitted
   std::vector<std::chrono::steady_clock::time_point> slot_t0;
   ~clgpu_solver() {
     if (h_counter) cudaFreeHost(h_counter);
-    if (h_list) cudaFreeHost(h_list);
+    if (st_admit) {
+      cudaStreamSynchronize(st_admit);
+      cudaStreamDestroy(st_admit);
+    }
+    for (auto ev : ev_admit)
+      if (ev) cudaEventDestroy(ev);
+    for (int *p : {h_list, h_list_admit, h_list_collect, h_list_act})
+      if (p) cudaFreeHost(p);
     if (h_info) cudaFreeHost(h_info);
+    if (h_stage) cudaFreeHost(h_stage);
     for (auto e : ev_pool) cudaEventDestroy(e);
   }
   int next_event() {
@@ -1948,11 +1974,20 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   cudaMallocHost(&h->h_counter, 4 * sizeof(int));
   // serving buffers
   h->d_sel = A.alloc<int>(B);
+  h->d_sel_admit = A.alloc<int>(B);
   h->d_run = A.alloc<int>(B);
+  h->d_active_admit = A.alloc<int>(B);
   h->d_list = A.alloc<int>(B);
+  h->d_list_admit = A.alloc<int>(B);
+  h->d_list_collect = A.alloc<int>(B);
+  h->d_list_act = A.alloc<int>(B);
   h->d_info = A.alloc<double>((size_t)B * (NUM_SCALARS + NUM_INTS));
   cudaMallocHost(&h->h_list, (size_t)B * sizeof(int));
+  cudaMallocHost(&h->h_list_admit, (size_t)B * sizeof(int));
+  cudaMallocHost(&h->h_list_collect, (size_t)B * sizeof(int));
+  cudaMallocHost(&h->h_list_act, (size_t)B * sizeof(int));
   cudaMallocHost(&h->h_info, (size_t)B * (NUM_SCALARS + NUM_INTS) * sizeof(double));
+  cudaMallocHost(&h->h_stage, ((size_t)nx + (size_t)mz) * sizeof(double));
   h->slot_state.assign(B, 0);
   h->slot_t0.assign(B, std::chrono::steady_clock::now());
   if (A.err != cudaSuccess) return -1000 - (int)A.err;
@@ -2034,34 +2069,38 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
 struct Phase {
   clgpu_solver *h;
   cudaStream_t st;
-  Dev &d() { return h->dv; }
+  // the views the kernels run on (default: the solver's own); serving admits
+  // through views whose active mask is separate from the running passes'
+  Dev *dp = nullptr;
+  ConeSet *cp = nullptr;
+  Dev &D() { return dp ? *dp : h->dv; }
+  ConeSet &C() { return cp ? *cp : h->cs; }
   void mask(int mode) {
-    k_set_mask<<<nblk(h->B), TB, 0, st>>>(h->dv, h->ic, mode, h->mask_sel);
+    k_set_mask<<<nblk(h->B), TB, 0, st>>>(D(), h->ic, mode, h->mask_sel);
     h->launches++;
   }
   void zero(int f0, int nf, double v = 0.0) {
-    k_zero_fields<<<nblk((long long)nf * h->B), TB, 0, st>>>(h->dv, f0, nf, v);
+    k_zero_fields<<<nblk((long long)nf * h->B), TB, 0, st>>>(D(), f0, nf, v);
     h->launches++;
   }
   // kkt_update! without its constant-rhs solve: Hs refresh, regularise +
   // refactor
   void kkt_refactor() {
     h->prof_begin(2, st);
-    cones_refresh_kkt(h->cs, h->map, h->kk.Kx, st);
+    cones_refresh_kkt(C(), h->map, h->kk.Kx, st);
     h->prof_end(st);
-    int *ok = h->dv.I + I_KKT_OK * h->B;
+    int *ok = D().I + I_KKT_OK * h->B;
     h->prof_begin(0, st);
-    ldl_factor(h->kk, h->mixed, h->lp, h->dv.active, ok, h->dv.S + F_KKT_EPS * h->B, st);
+    ldl_factor(h->kk, h->mixed, h->lp, D().active, ok, D().S + F_KKT_EPS * h->B, st);
     h->prof_end(st);
     h->launches += 8;
   }
   // kkt_update!: refresh, refactor, constant rhs solve [x2; z2] = K \ [-q; b]
   void kkt_update() {
     kkt_refactor();
-    int *ok = h->dv.I + I_KKT_OK * h->B;
+    int *ok = D().I + I_KKT_OK * h->B;
     h->prof_begin(1, st);
-    ldl_solve(h->kk, h->mixed, h->lp, h->dv.active, h->dv.negq, h->dv.b, h->dv.x2, h->dv.z2,
-              ok, st);
+    ldl_solve(h->kk, h->mixed, h->lp, D().active, D().negq, D().b, D().x2, D().z2, ok, st);
     h->prof_end(st);
     h->launches += 4;
   }
@@ -2124,7 +2163,8 @@ struct Phase {
 // solver_default_start! (solver.jl:425-446) for every instance, or with
 // h->mask_sel set only for the selected ones (the others are untouched)
 static void ipm_start(clgpu_solver *h, Phase &P, cudaStream_t st) {
-  Dev &dv = h->dv;
+  Dev &dv = P.D();
+  ConeSet &cs = P.C();
   const int B = h->B;
   // (re)initialise every per-instance scalar; solve! may be called repeatedly
   k_init_state<<<nblk(B), TB, 0, st>>>(dv, h->d_c, h->d_normq, h->d_normb, h->d_pnnz,
@@ -2132,7 +2172,7 @@ static void ipm_start(clgpu_solver *h, Phase &P, cudaStream_t st) {
   P.mask(M_ALL_UNDONE);
   if (h->any_sym) {
     P.mask(M_SYM);
-    cones_set_identity_scaling(h->cs, st);
+    cones_set_identity_scaling(cs, st);
     P.kkt_update();
     // QP instances: [x; z] = K \ [-q; b], s = -z
     P.mask(M_SYM_QP);
@@ -2152,17 +2192,17 @@ static void ipm_start(clgpu_solver *h, Phase &P, cudaStream_t st) {
       double *v = pd == 0 ? dv.s : dv.z;
       k_zero_fields<<<nblk(B), TB, 0, st>>>(dv, F_MARGIN_MIN, 1, kDMax);
       P.zero(F_MARGIN_SUM, 1);
-      cones_margins(h->cs, v, pd, dv.S + F_MARGIN_MIN * B, dv.S + F_MARGIN_SUM * B, st);
+      cones_margins(cs, v, pd, dv.S + F_MARGIN_MIN * B, dv.S + F_MARGIN_SUM * B, st);
       k_shift_amounts<<<nblk(B), TB, 0, st>>>(dv, h->ic, F_MARGIN_MIN, F_MARGIN_SUM, F_TAU_NUM,
                                               F_TAU_DEN);
-      cones_scaled_unit_shift(h->cs, v, dv.S + F_TAU_NUM * B, pd, st);
-      cones_scaled_unit_shift(h->cs, v, dv.S + F_TAU_DEN * B, pd, st);
+      cones_scaled_unit_shift(cs, v, dv.S + F_TAU_NUM * B, pd, st);
+      cones_scaled_unit_shift(cs, v, dv.S + F_TAU_DEN * B, pd, st);
     }
     k_set_tau_kappa_one<<<nblk(B), TB, 0, st>>>(dv);
   }
   if (h->any_asym) {
     P.mask(M_ASYM);
-    cones_unit_initialization(h->cs, dv.z, dv.s, st);
+    cones_unit_initialization(cs, dv.z, dv.s, st);
     k_zero_x_masked<<<nblk(dv.nx), TB, 0, st>>>(dv);
     k_set_tau_kappa_one<<<nblk(B), TB, 0, st>>>(dv);
   }
@@ -2303,7 +2343,10 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
   Dev &dv = h->dv;
   const int B = h->B;
   h->launches = 0;
+  if (h->st_admit) cudaStreamSynchronize(h->st_admit);  // no admission in flight
   h->serving = false;
+  h->fresh.clear();
+  h->aged.clear();
   h->mask_sel = nullptr;
   std::fill(h->slot_state.begin(), h->slot_state.end(), 0);
   if (h->profiling && h->d_prof_bytes)
@@ -2366,12 +2409,17 @@ __global__ void k_serve_mark_idle(Dev d, int *run) {
   IF(d, I_DONE, i) = 1;
   run[i] = 0;
 }
-// sel[i] = 1 for the listed slots (sel zeroed before); run[i] = 1 too if given
-__global__ void k_serve_set(const int *list, int n, int *sel, int *run) {
+// sel[i] = 1 for the listed slots (sel zeroed before)
+__global__ void k_serve_set(const int *list, int n, int *sel) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) sel[list[t]] = 1;
+}
+// the listed (admitted, started) slots join the running passes
+__global__ void k_serve_activate(Dev d, const int *list, int n, int *run) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  sel[list[t]] = 1;
-  if (run) run[list[t]] = 1;
+  IF(d, I_DONE, list[t]) = 0;
+  run[list[t]] = 1;
 }
 // scalar and integer fields of the listed slots, packed slot by slot
 __global__ void k_serve_gather_info(Dev d, const int *list, int n, double *out) {
@@ -2383,47 +2431,68 @@ __global__ void k_serve_gather_info(Dev d, const int *list, int n, double *out) 
   for (int f = 0; f < NUM_INTS; ++f) o[NUM_SCALARS + f] = (double)IF(d, f, i);
 }
 
-static int serve_upload_list(clgpu_solver *h, const int *slots, int n, int *run,
-                             cudaStream_t st) {
-  std::memcpy(h->h_list, slots, (size_t)n * sizeof(int));
-  cudaMemcpyAsync(h->d_list, h->h_list, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(h->d_sel, 0, (size_t)h->B * sizeof(int), st);
-  k_serve_set<<<nblk(n), TB, 0, st>>>(h->d_list, n, h->d_sel, run);
-  return 0;
+// list -> device (through pinned host memory) and sel = its indicator
+static void serve_upload_list(const int *slots, int n, int *h_buf, int *d_buf, int *d_sel,
+                              int B, cudaStream_t st) {
+  std::memcpy(h_buf, slots, (size_t)n * sizeof(int));
+  cudaMemcpyAsync(d_buf, h_buf, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_sel, 0, (size_t)B * sizeof(int), st);
+  k_serve_set<<<nblk(n), TB, 0, st>>>(d_buf, n, d_sel);
 }
 
 extern "C" int clgpu_serve_admit(clgpu_solver *h, const int *slots, int n, const double *q,
                                  const double *b, clgpu_stream_t stream) {
   if (!h || n < 0 || (n > 0 && !slots)) return -1;
   if (n == 0) return 0;
-  cudaStream_t st = (cudaStream_t)stream;
   Dev &dv = h->dv;
   std::vector<char> seen(h->B, 0);
   for (int k = 0; k < n; ++k) {
     const int i = slots[k];
     if (i < 0 || i >= h->B || seen[i]) return -2;
-    if (h->serving && h->slot_state[i] != 0) return -3;  // slot busy or not collected
+    if (h->serving && h->slot_state[i] != 0) return -3;  // running, pending or not collected
     seen[i] = 1;
   }
+  if (h->serving && !h->fresh.empty()) return -4;  // one admission per step
   if (!h->serving) {
-    k_serve_mark_idle<<<nblk(h->B), TB, 0, st>>>(dv, h->d_run);
+    cudaStream_t cst = (cudaStream_t)stream;
+    k_serve_mark_idle<<<nblk(h->B), TB, 0, cst>>>(dv, h->d_run);
+    if (!h->st_admit) {
+      cudaStreamCreateWithFlags(&h->st_admit, cudaStreamNonBlocking);
+      for (auto &ev : h->ev_admit) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    }
+    h->dv_admit = dv;
+    h->dv_admit.active = h->d_active_admit;
+    h->cs_admit = h->cs;
+    h->cs_admit.inst_active = h->d_active_admit;
     std::fill(h->slot_state.begin(), h->slot_state.end(), 0);
+    h->fresh.clear();
+    h->aged.clear();
     h->serving = true;
     h->kk.prof_bytes = nullptr;
+    cudaError_t e = cudaStreamSynchronize(cst);
+    if (e != cudaSuccess) return -1000 - (int)e;
   }
-  // new q / b values (packed slot by slot), scaled with the setup equilibration
+  cudaStream_t st = h->st_admit;
+  // the previous admission's buffers are free once it completed
+  const int ev = h->ev_fresh ^ 1;
+  cudaEventSynchronize(h->ev_admit[h->ev_fresh]);
+  // new q / b values (packed slot by slot, staged in pinned memory), scaled
+  // with the setup equilibration
   long long qo = 0, bo = 0;
+  double *hq = h->h_stage, *hb = h->h_stage + dv.nx;
   for (int k = 0; k < n; ++k) {
     const int i = slots[k];
     const int x0 = h->h_xoff[i], x1 = h->h_xoff[i + 1];
     const int m0 = h->h_moff[i], m1 = h->h_moff[i + 1];
     if (q && x1 > x0) {
-      cudaMemcpyAsync(h->d_in_q + x0, q + qo, (size_t)(x1 - x0) * sizeof(double),
+      std::memcpy(hq + x0, q + qo, (size_t)(x1 - x0) * sizeof(double));
+      cudaMemcpyAsync(h->d_in_q + x0, hq + x0, (size_t)(x1 - x0) * sizeof(double),
                       cudaMemcpyHostToDevice, st);
       k_update_q<<<nblk(x1 - x0), TB, 0, st>>>(dv, h->d_in_q, x0, x1, h->d_c);
     }
     if (b && m1 > m0) {
-      cudaMemcpyAsync(h->d_in_b + m0, b + bo, (size_t)(m1 - m0) * sizeof(double),
+      std::memcpy(hb + m0, b + bo, (size_t)(m1 - m0) * sizeof(double));
+      cudaMemcpyAsync(h->d_in_b + m0, hb + m0, (size_t)(m1 - m0) * sizeof(double),
                       cudaMemcpyHostToDevice, st);
       k_update_b<<<nblk(m1 - m0), TB, 0, st>>>(dv, h->d_in_b, m0, m1, h->d_zmap);
     }
@@ -2433,19 +2502,21 @@ extern "C" int clgpu_serve_admit(clgpu_solver *h, const int *slots, int n, const
     qo += x1 - x0;
     bo += m1 - m0;
   }
-  // the starting point of the admitted slots only; they join the next step
-  serve_upload_list(h, slots, n, h->d_run, st);
-  Phase P{h, st};
-  h->mask_sel = h->d_sel;
+  // the starting point of the admitted slots, through the admission views
+  serve_upload_list(slots, n, h->h_list_admit, h->d_list_admit, h->d_sel_admit, h->B, st);
+  Phase P{h, st, &h->dv_admit, &h->cs_admit};
+  h->mask_sel = h->d_sel_admit;
   ipm_start(h, P, st);
   h->mask_sel = nullptr;
+  cudaEventRecord(h->ev_admit[ev], st);
+  h->ev_fresh = ev;
   const auto now = std::chrono::steady_clock::now();
   for (int k = 0; k < n; ++k) {
-    h->slot_state[slots[k]] = 1;
+    h->slot_state[slots[k]] = 3;
     h->slot_t0[slots[k]] = now;
+    h->fresh.push_back(slots[k]);
   }
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // caller buffers consumed
   return e == cudaSuccess ? 0 : -1000 - (int)e;
 }
 
@@ -2453,6 +2524,26 @@ extern "C" int clgpu_serve_step(clgpu_solver *h, clgpu_stream_t stream, int *fin
                                 int *nfinished, int *nrunning) {
   if (!h || !h->serving) return -1;
   cudaStream_t st = (cudaStream_t)stream;
+  int active = 0;
+  for (int v : h->slot_state) active += v == 1;
+  // the batch admitted before the previous step joins now; so does a fresh
+  // one when nothing else runs (there is no pass for it to overlap)
+  std::vector<int> join = h->aged;
+  int wait_ev = h->ev_aged;
+  h->aged.clear();
+  if (active == 0 && join.empty() && !h->fresh.empty()) {
+    join.swap(h->fresh);
+    wait_ev = h->ev_fresh;
+  }
+  if (!join.empty()) {
+    cudaStreamWaitEvent(st, h->ev_admit[wait_ev], 0);
+    std::memcpy(h->h_list_act, join.data(), join.size() * sizeof(int));
+    cudaMemcpyAsync(h->d_list_act, h->h_list_act, join.size() * sizeof(int),
+                    cudaMemcpyHostToDevice, st);
+    k_serve_activate<<<nblk((int)join.size()), TB, 0, st>>>(h->dv, h->d_list_act,
+                                                           (int)join.size(), h->d_run);
+    for (int i : join) h->slot_state[i] = 1;
+  }
   Phase P{h, st};
   int nfin = 0;
   const int running = ipm_pass(h, P, st, 0.0, true, &nfin);
@@ -2462,8 +2553,12 @@ extern "C" int clgpu_serve_step(clgpu_solver *h, clgpu_stream_t stream, int *fin
     h->slot_state[h->h_list[k]] = 2;
     if (finished) finished[k] = h->h_list[k];
   }
+  // the fresh batch has overlapped this pass; it joins the next one
+  h->aged.swap(h->fresh);
+  h->fresh.clear();
+  h->ev_aged = h->ev_fresh;
   if (nfinished) *nfinished = nfin;
-  if (nrunning) *nrunning = running;
+  if (nrunning) *nrunning = running + (int)h->aged.size();
   return 0;
 }
 
@@ -2476,12 +2571,12 @@ extern "C" int clgpu_serve_collect(clgpu_solver *h, const int *slots, int n, dou
     if (slots[k] < 0 || slots[k] >= h->B || h->slot_state[slots[k]] != 2) return -2;
   cudaStream_t st = (cudaStream_t)stream;
   Dev &dv = h->dv;
-  serve_upload_list(h, slots, n, nullptr, st);
+  serve_upload_list(slots, n, h->h_list_collect, h->d_list_collect, h->d_sel, h->B, st);
   k_post_status<<<nblk(h->B), TB, 0, st>>>(dv, h->sd, h->d_sel);
   double *ox = h->d_out, *os = ox + dv.nx, *oz = os + dv.mz;
   k_unscale<<<nblk(std::max(dv.nx, dv.mz)), TB, 0, st>>>(dv, h->d_zmap, h->d_zinst, ox, os, oz,
                                                         h->d_sel);
-  k_serve_gather_info<<<nblk(n), TB, 0, st>>>(dv, h->d_list, n, h->d_info);
+  k_serve_gather_info<<<nblk(n), TB, 0, st>>>(dv, h->d_list_collect, n, h->d_info);
   constexpr int NF = NUM_SCALARS + NUM_INTS;
   cudaMemcpyAsync(h->h_info, h->d_info, (size_t)n * NF * sizeof(double),
                   cudaMemcpyDeviceToHost, st);

@@ -175,15 +175,20 @@ int clgpu_solver_destroy(clgpu_solver *h);
  * The instances of a solver are slots with fixed structure (P, A sparsity,
  * cones).  admit starts new solves in idle slots, with new q / b values when
  * given (packed slot by slot in the order of `slots`; NULL keeps the current
- * values), while other slots are mid-solve; step runs one IPM iteration of
- * every running slot and lists the slots that finished in it (ascending);
- * collect post-processes finished slots, copies their x / s / z (packed slot
- * by slot in user order) and infos to the host, and makes them idle again.
- * A slot's result is exactly that of solving it alone.  The first admit
- * makes every slot idle; clgpu_solver_solve leaves serving.  Returns 0, -1 on
- * a bad argument, -2 on a bad or repeated slot, -3 when admitting a slot that
- * is running or not yet collected.  No reference counterpart (the reference
- * has no serving loop; config 5 of the benchmark plan). */
+ * values; copied before return), while other slots are mid-solve: the
+ * starting points are computed on a stream of the library's own, overlapping
+ * the next step, and the slots join the step after it (at once when nothing
+ * else runs).  step runs one IPM iteration of every running slot and lists
+ * the slots that finished in it (ascending); *nrunning counts running and
+ * admitted slots.  collect post-processes finished slots, copies their
+ * x / s / z (packed slot by slot in user order) and infos to the host, and
+ * makes them idle again.  At most one admit between two steps.  A slot's
+ * result is exactly that of solving it alone.  The first admit makes every
+ * slot idle; clgpu_solver_solve leaves serving.  Returns 0, -1 on a bad
+ * argument, -2 on a bad or repeated slot, -3 when admitting a slot that is
+ * running, admitted or not yet collected, -4 on a second admit before a
+ * step.  No reference counterpart (the reference has no serving loop;
+ * config 5 of the benchmark plan). */
 int clgpu_serve_admit(clgpu_solver *h, const int *slots, int n, const double *q,
                       const double *b, clgpu_stream_t stream);
 int clgpu_serve_step(clgpu_solver *h, clgpu_stream_t stream, int *finished,

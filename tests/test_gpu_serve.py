@@ -68,9 +68,11 @@ def test_slot_reuse_and_errors(cuda_device):
     s = BatchSolver(pbs)
     s.serve_admit([0, 1])
     with pytest.raises(RuntimeError):
-        s.serve_admit([1])          # still running
+        s.serve_admit([1])          # already admitted
     with pytest.raises(RuntimeError):
         s.serve_admit([2, 2])       # repeated slot
+    with pytest.raises(RuntimeError):
+        s.serve_admit([2])          # a second admission before a step
     got = {}
     for _ in range(1000):
         fin, running = s.serve_step()
