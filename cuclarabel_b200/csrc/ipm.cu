@@ -856,6 +856,10 @@ struct clgpu_solver {
       *h_list_act = nullptr;
   double *d_info = nullptr, *h_info = nullptr, *h_stage = nullptr;
   bool serving = false;
+  // the pass as a CUDA graph (index 1: with the serving finished-list)
+  bool use_graphs = true;
+  cudaGraphExec_t pass_exec[2] = {nullptr, nullptr};
+  long long pass_launches = 0;
   Dev dv_admit{};
   ConeSet cs_admit{};
   cudaStream_t st_admit = nullptr;
@@ -865,6 +869,8 @@ struct clgpu_solver {
   std::vector<int> slot_state;   // 0 idle, 1 running, 2 finished, 3 admitted
   std::vector<std::chrono::steady_clock::time_point> slot_t0;
   ~clgpu_solver() {
+    for (auto ex : pass_exec)
+      if (ex) cudaGraphExecDestroy(ex);
     if (h_counter) cudaFreeHost(h_counter);
     if (st_admit) {
       cudaStreamSynchronize(st_admit);
@@ -2218,11 +2224,11 @@ __global__ void k_serve_finished(Dev d, int *run, int *list, int *count) {
   }
 }
 
-// one pass of the IPM loop (solver.jl:265-393) over every running instance;
-// returns how many are still running.  serve: also list the slots that
-// finished in this pass into h->h_list (count in *nfin).
-static int ipm_pass(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed, bool serve,
-                    int *nfin) {
+// the kernels of one pass of the IPM loop (solver.jl:265-393) over every
+// running instance, up to the running count (dv.counter[0]) and, serving,
+// the list of slots that finished in it (dv.counter[2], h->d_list)
+static void ipm_pass_kernels(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed,
+                             bool serve) {
   Dev &dv = h->dv;
   const int B = h->B;
   P.mask(M_PASS);
@@ -2283,6 +2289,47 @@ static int ipm_pass(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed, 
   k_count_running<<<nblk(B), TB, 0, st>>>(dv);
   if (serve) k_serve_finished<<<nblk(B), TB, 0, st>>>(dv, h->d_run, h->d_list, dv.counter + 2);
   h->launches += 25;
+}
+
+// One pass of the IPM loop over every running instance; returns how many are
+// still running.  serve: also lists the slots that finished in this pass in
+// h->h_list (count in *nfin).  Without host decisions inside the pass (no
+// asymmetric-cone backtracking, no profiling or tracing, no time limit) the
+// pass is captured once as a CUDA graph and replayed: one launch instead of
+// ~60.
+static int ipm_pass(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed, bool serve,
+                    int *nfin) {
+  Dev &dv = h->dv;
+  const int B = h->B;
+  const bool graph = h->use_graphs && !h->any_asym && !h->profiling && !h->st.verbose &&
+                     !std::isfinite(h->st.time_limit) && h->mask_sel == nullptr;
+  bool done = false;
+  if (graph) {
+    cudaGraphExec_t &ex = h->pass_exec[serve ? 1 : 0];
+    if (!ex) {
+      cudaGraph_t g = nullptr;
+      const long long l0 = h->launches;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        ipm_pass_kernels(h, P, st, 0.0, serve);
+        if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
+          if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) ex = nullptr;
+          cudaGraphDestroy(g);
+        }
+      }
+      h->pass_launches = h->launches - l0;
+      h->launches = l0;
+      if (!ex) {
+        cudaGetLastError();     // clear the failed capture's error
+        h->use_graphs = false;  // and launch kernel by kernel from now on
+      }
+    }
+    if (ex) {
+      cudaGraphLaunch(ex, st);
+      h->launches += h->pass_launches;
+      done = true;
+    }
+  }
+  if (!done) ipm_pass_kernels(h, P, st, elapsed, serve);
   const int running = P.read_counter(0);
   if (serve) {
     *nfin = h->h_counter[2];

@@ -146,6 +146,22 @@ def test_fused_constant_and_affine_solves_are_bitwise_separate_solves(cuda_devic
         assert x.obj_val == y.obj_val, k
 
 
+def test_graph_replayed_pass_equals_direct_launches(cuda_device):
+    """The IPM pass is captured once as a CUDA graph and replayed; a profiled
+    solve launches the same kernels one by one.  Results must agree bitwise."""
+    pbs = problems.mpc_batch(16, seed0=400)
+    s = BatchSolver(pbs)
+    a = s.solve()                 # captured and replayed
+    s.set_profiling(True)
+    b = s.solve()                 # launched kernel by kernel
+    s.set_profiling(False)
+    c = s.solve()                 # replayed again
+    for x, y, z in zip(a, b, c):
+        assert x.status == y.status == z.status and x.iterations == y.iterations
+        assert np.array_equal(x.x, y.x) and np.array_equal(x.x, z.x)
+        assert np.array_equal(x.z, y.z) and x.obj_val == y.obj_val
+
+
 def test_mixed_socp_scaled(cuda_device):
     pb = problems.mixed_socp(scale=0.02, seed=2)
     sol = Solver(*pb).solve()
