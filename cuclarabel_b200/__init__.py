@@ -6,7 +6,9 @@ from .api import (BatchSolver, DefaultSolution, ExponentialConeT,  # noqa: F401
                   NonnegativeConeT, PowerConeT, PSDTriangleConeT, SecondOrderConeT,
                   Settings, Solver, SolverStatus, SupportedCone, ZeroConeT,
                   cones_from_dict)
+from .json_io import read_from_file, write_to_file  # noqa: F401
 
 __all__ = ["BatchSolver", "DefaultSolution", "ExponentialConeT", "NonnegativeConeT",
            "PowerConeT", "PSDTriangleConeT", "SecondOrderConeT", "Settings", "Solver",
-           "SolverStatus", "SupportedCone", "ZeroConeT", "cones_from_dict"]
+           "SolverStatus", "SupportedCone", "ZeroConeT", "cones_from_dict", "read_from_file",
+           "write_to_file"]

@@ -559,6 +559,12 @@ class Solver(BatchSolver):
     def __init__(self, P, q, A, b, cones, settings=None, **kwargs):
         super().__init__([(P, q, A, b, cones)], settings, **kwargs)
         self.solution = None
+        # the problem as given (for write_to_file), kept current by update_*
+        n, m = len(np.ravel(q)), len(np.ravel(b))
+        if isinstance(cones, dict):
+            cones = cones_from_dict(cones)
+        self.problem = (_as_csc(P, (n, n)).copy(), np.array(q, np.float64).ravel(),
+                        _as_csc(A, (m, n)).copy(), np.array(b, np.float64).ravel(), list(cones))
 
     def solve(self, stream=0):
         self.solution = super().solve(stream)[0]
@@ -567,15 +573,29 @@ class Solver(BatchSolver):
     # update_P! / update_q! / update_A! / update_b! (src/data_updating.jl)
     def update_P(self, P):
         self.update_data(P=[P])
+        P0, q, A, b, c = self.problem
+        P1 = P0.copy()
+        P1.data = (_as_csc(P, P0.shape).data if sp.issparse(P)
+                   else np.asarray(P, np.float64).ravel()).copy()
+        self.problem = (P1, q, A, b, c)
 
     def update_q(self, q):
         self.update_data(q=q)
+        P, _, A, b, c = self.problem
+        self.problem = (P, np.array(q, np.float64).ravel(), A, b, c)
 
     def update_A(self, A):
         self.update_data(A=[A])
+        P, q, A0, b, c = self.problem
+        A1 = A0.copy()
+        A1.data = (_as_csc(A, A0.shape).data if sp.issparse(A)
+                   else np.asarray(A, np.float64).ravel()).copy()
+        self.problem = (P, q, A1, b, c)
 
     def update_b(self, b):
         self.update_data(b=b)
+        P, q, A, _, c = self.problem
+        self.problem = (P, q, A, np.array(b, np.float64).ravel(), c)
 
     @property
     def info(self):
