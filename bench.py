@@ -259,6 +259,26 @@ def ncu_traffic(summary):
     return None
 
 
+def rank_seed0(rank, instances):
+    """First instance seed of a rank: rank r owns instances [r B, (r+1) B),
+    so ranks share no instance (weak scaling, no data-path collective)."""
+    return rank * instances
+
+
+def aggregate_over_ranks(elapsed, solved, dist, device):
+    """Whole-job figures: the slowest rank's time and every rank's solves
+    (the only collectives of the multi-GPU run)."""
+    if dist is None:
+        return elapsed, solved
+    import torch
+    t = torch.tensor([elapsed, float(solved)], device=device, dtype=torch.float64)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return tmax[0].item(), int(round(tsum[1].item()))
+
+
 def serve_run(solver, pbs, lam, seconds, seed, stream):
     """Continuous batching under a Poisson request stream (config 5 shape,
     its config-4 part): `lam` requests/s for `seconds`, each for a uniformly
@@ -373,7 +393,7 @@ def main():
     from cuclarabel_b200 import BatchSolver, Solver, SolverStatus, _lib
 
     B = args.instances
-    seed0 = rank * B
+    seed0 = rank_seed0(rank, B)
     pbs = gen_problems(B, seed0)
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
@@ -414,15 +434,7 @@ def main():
         solved_total += int(np.sum(res["status"] == int(SolverStatus.SOLVED)))
     sols = solver.solutions()
     clocks = sampler.stop()
-    elapsed = sum(times)
-    if dist:
-        t = torch.tensor([elapsed, float(solved_total)], device="cuda", dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        elapsed = tmax[0].item()
-        solved_total = int(tsum[1].item())
+    elapsed, solved_total = aggregate_over_ranks(sum(times), solved_total, dist, "cuda")
     value = solved_total / elapsed
     n_solved_last = sum(1 for s in sols if s.status == SolverStatus.SOLVED)
     status_counts = {}
@@ -467,14 +479,8 @@ def main():
     h2d = 8 * (len(Pv) + len(qv) + len(Av) + len(bv))
     d2h = 8 * (s2.nx + 2 * s2.mz) + B * ctypes.sizeof(_lib.ClgpuInfo)
     del s2
+    e2e_t, e2e_solved = aggregate_over_ranks(e2e_t, e2e_solved, dist, "cuda")
     e2e_val = e2e_solved / e2e_t
-    if dist:
-        t = torch.tensor([e2e_t, float(e2e_solved)], device="cuda", dtype=torch.float64)
-        tm = t.clone()
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ts = t.clone()
-        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
-        e2e_val = ts[1].item() / tm[0].item()
     # cold path for reference: Solver(...) setup from host CSC data + solve +
     # solutions, one pass
     torch.cuda.synchronize()

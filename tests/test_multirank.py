@@ -1,0 +1,47 @@
+"""The multi-GPU bench path on CPU ranks (gloo, world size 2): instance
+shards do not overlap, and the whole-job figures are the slowest rank's time
+and the sum of every rank's solves."""
+import datetime
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    import bench
+    t, s = bench.aggregate_over_ranks(1.5 + rank, 7 * (rank + 1), dist, "cpu")
+    out.put((rank, t, s, bench.rank_seed0(rank, 4096)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_cpu_ranks_aggregate_and_shard():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[0] for r in res] == [0, 1]
+    for _, t, s, _ in res:
+        assert t == 2.5 and s == 21          # max over ranks, sum over ranks
+    assert [r[3] for r in res] == [0, 4096]  # disjoint instance ranges
