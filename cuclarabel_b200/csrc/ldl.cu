@@ -661,7 +661,13 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       if (!on[r]) continue;
-      double x[kSK], sm[kSK];
+      double x[kSK], sm[kSK], yo[kSK];
+      // a segment's target is written once per pass, by its last entry, so
+      // its old value can be read before the scan, off the dependent chain
+      if (!RESID) {
+#pragma unroll
+        for (int j = 0; j < kSK; ++j) yo[j] = wr[j] ? out[r][sg[j] & 0xffff] : 0.0;
+      }
 #pragma unroll
       for (int j = 0; j < kSK; ++j) {
         const double yv = y[r][gi[j]];
@@ -674,7 +680,7 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
           if (RESID)
             out[r][sg[j] & 0xffff] = sm[j];
           else
-            out[r][sg[j] & 0xffff] = __dsub_rn(out[r][sg[j] & 0xffff], sm[j]);
+            out[r][sg[j] & 0xffff] = __dsub_rn(yo[j], sm[j]);
         }
       // partial sum of the segment of the chunk's last entry (used by the
       // next chunk only if its first entry continues that segment)
@@ -1071,13 +1077,17 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
       }
       carry = 0.0;
     } else {
+      // each target is written once per level (by its last update), so its
+      // old value is read before the scan, off the dependent chain
+      const bool wA = vA && ((oA.w >> kLastBit) & 1), wB = vB && ((oB.w >> kLastBit) & 1);
+      const double tA = wA ? V[oA.x] : 0.0, tB = wB ? V[oB.x] : 0.0;
       const double xA = vA ? __dmul_rn(__dmul_rn(V[oA.y], V[oA.z]), V[oA.w & 0xffff]) : 0.0;
       const double xB = vB ? __dmul_rn(__dmul_rn(V[oB.y], V[oB.z]), V[oB.w & 0xffff]) : 0.0;
       double sA, sB;
       seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
                 (int)((w >> kStepShift) & 7u), sA, sB);
-      if (vA && ((oA.w >> kLastBit) & 1)) V[oA.x] = __dsub_rn(V[oA.x], sA);
-      if (vB && ((oB.w >> kLastBit) & 1)) V[oB.x] = __dsub_rn(V[oB.x], sB);
+      if (wA) V[oA.x] = __dsub_rn(tA, sA);
+      if (wB) V[oB.x] = __dsub_rn(tB, sB);
       const int ll = (cnt - 1) >> 1;
       carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
     }
