@@ -628,6 +628,7 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
   double carry[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) carry[r] = 0.0;
+  unsigned wnext = word(0);  // each chunk's word is read one chunk ahead
   for (int c = 0; c < nch; ++c) {
     if (c > 0 && (c & 31) == 0) {
       ++blk;
@@ -636,7 +637,7 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
       const int q = 32 * (blk + 2) + lane;
       d2 = q < nch ? chunks[q] : 0;
     }
-    const unsigned wc = word(c);
+    const unsigned wc = wnext;
     const int cnt = (int)((wc >> kCntShift) & 127u) + 1;
     const int nsteps = (int)((wc >> kStepShift) & 7u);
     asm volatile("cp.async.wait_group %0;\n" ::"n"(kSRing - 1));
@@ -689,6 +690,7 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
     }
     __syncwarp();
     issue(c + kSRing, slot);
+    if (c + 1 < nch) wnext = word(c + 1);  // before the block rotation: c + 1 - 32 blk <= 32
   }
   asm volatile("cp.async.wait_all;\n" ::);
   __syncwarp();
