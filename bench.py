@@ -111,6 +111,176 @@ def algorithmic_bytes_update_scaling(pbs, soc_threshold=5):
     return total
 
 
+# ---------------------------------------------------------------- cone kernels
+# Cone-kernel roofline workload: the cone types of the large single-problem
+# configurations (nonnegative rows and SOC(10) of the mixed QP/SOCP; exp, pow
+# and PSD(10) of the exp/pow/PSD LP), one cone-level handle per type (the
+# plain B = 1 path through the CompositeConeGPU method table of the C ABI),
+# at counts where every vector an operation streams exceeds L2 (126 MB).
+CONE_WORKLOAD = {  # name: (type code, dim, cones at scale 1)
+    "nn": (1, 16_000_000, 1),
+    "soc10": (2, 10, 1_600_000),
+    "exp": (3, 3, 4_000_000),
+    "pow": (4, 3, 4_000_000),
+    "psd10": (5, 10, 400_000),
+}
+CONE_OPS = ("update_scaling", "mul_Hs", "affine_ds", "combined_ds_shift",
+            "ds_from_dz_offset", "step_length")
+
+
+def cone_op_bytes(op, code, dim, count, soc_threshold=5):
+    """Algorithmic bytes of one cone operation over `count` cones of one type:
+    every input the operation needs read once and every output written once
+    (FP64 values, 8 B).  Per-row state (w, lambda; sparse SOC u, v), per-cone
+    state (SOC eta, d; exp/pow gradient, H_dual, Hs and the stored z; PSD
+    R, R^-1, lambda) as the kernels of this library keep it."""
+    if code == 1:
+        per = {"update_scaling": 32, "mul_Hs": 24, "affine_ds": 16,
+               "combined_ds_shift": 32, "ds_from_dz_offset": 24, "step_length": 32}
+        return per[op] * dim * count
+    if code == 2:
+        rows = dim * count
+        sparse = dim > soc_threshold
+        per = {"update_scaling": 32 * rows + 8 * count + ((16 * rows + 8 * count) if sparse else 0),
+               "mul_Hs": 24 * rows + 8 * count, "affine_ds": 16 * rows,
+               "combined_ds_shift": 32 * rows + 8 * count,
+               "ds_from_dz_offset": 40 * rows + 8 * count, "step_length": 32 * rows}
+        return per[op]
+    if code in (3, 4):
+        a = 8 if code == 4 else 0  # the power cone's alpha
+        per = {"update_scaling": 240 + a, "mul_Hs": 120, "affine_ds": 48,
+               "combined_ds_shift": 192 + a, "ds_from_dz_offset": 48, "step_length": 96 + a}
+        return per[op] * count
+    n = dim
+    t = n * (n + 1) // 2
+    per = {"update_scaling": 16 * t + 16 * n * n + 8 * n, "mul_Hs": 8 * n * n + 16 * t,
+           "affine_ds": 8 * n + 8 * t, "combined_ds_shift": 24 * t + 16 * n * n,
+           "ds_from_dz_offset": 16 * t + 8 * n * n + 8 * n,
+           "step_length": 16 * t + 16 * n * n + 8 * n}
+    return per[op] * count
+
+
+def cone_points(code, dim, count, rng, alpha=None):
+    """Strictly interior points of `count` cones of one type, concatenated in
+    the cone-level row layout, and the power cones' alphas (drawn unless
+    given)."""
+    if code == 1:
+        v = rng.uniform(0.5, 2.0, dim * count)
+    elif code == 2:
+        tail = rng.standard_normal((count, dim - 1))
+        head = 1.0 + np.linalg.norm(tail, axis=1) * rng.uniform(1.05, 2.0, count)
+        v = np.concatenate([head[:, None], tail], axis=1).ravel()
+    elif code == 3:
+        base = np.array([-1.051383945322714, 0.556409619469370, 1.258967884768947])
+        v = (base[None, :] * rng.uniform(0.5, 2.0, (count, 1))
+             + rng.normal(0, 0.02, (count, 3))).ravel()
+    elif code == 4:
+        if alpha is None:
+            alpha = rng.uniform(0.2, 0.8, count)
+        v = np.stack([np.sqrt(1 + alpha), np.sqrt(2 - alpha), np.zeros(count)], axis=1)
+        v = v * rng.uniform(0.5, 2.0, (count, 1))
+        v[:, 2] = rng.normal(0, 0.1, count)
+        v = v.ravel()
+    else:
+        n = dim
+        E = rng.standard_normal((count, n, n)) * 0.1
+        M = np.eye(n)[None] + (E + E.transpose(0, 2, 1)) / 2
+        ii, jj = [], []
+        for j in range(n):
+            for i in range(j + 1):
+                ii.append(i)
+                jj.append(j)
+        ii, jj = np.array(ii), np.array(jj)
+        scale = np.where(ii == jj, 1.0, np.sqrt(2.0))
+        v = (M[:, ii, jj] * scale[None, :]).ravel()
+    return v, alpha
+
+
+def cone_kernel_roofline(hbm, scale=1.0, reps=5, seed=7):
+    """Per-kernel device time and HBM throughput of every per-iteration cone
+    operation on the cone roofline workload (CUDA events around each
+    operation's kernels inside the library, median of `reps` after warm-up,
+    L2 flushed before each timed call)."""
+    import torch
+    from cuclarabel_b200 import _lib
+    L = _lib.load()
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    rng = np.random.default_rng(seed)
+    out = {}
+    for name, (code, dim, count) in CONE_WORKLOAD.items():
+        if code == 1:
+            dim = max(1, int(dim * scale))
+        else:
+            count = max(1, int(count * scale))
+        types = np.full(count, code, np.int32)
+        dims = np.full(count, dim, np.int32)
+        s_h, alpha = cone_points(code, dim, count, rng)
+        z_h, _ = cone_points(code, dim, count, rng, alpha)
+        params = np.ascontiguousarray(alpha if alpha is not None else np.zeros(count),
+                                      np.float64)
+        h = ctypes.c_void_p()
+        rc = L.clgpu_cones_create(count, types.ctypes.data_as(_lib.ip),
+                                  dims.ctypes.data_as(_lib.ip), params.ctypes.data_as(_lib.dp),
+                                  5, ctypes.byref(h))
+        assert rc == 0, (name, rc)
+        try:
+            assert L.clgpu_cones_set_profiling(h, 1) == 0
+            m = L.clgpu_cones_numel(h)
+
+            def dev(a):
+                return torch.tensor(np.asarray(a, np.float64), device="cuda")
+
+            s, z = dev(s_h), dev(z_h)
+            dz = dev(0.05 * rng.standard_normal(m))
+            ds = dev(0.05 * rng.standard_normal(m))
+            x = dev(rng.standard_normal(m))
+            y = torch.empty(m, dtype=torch.float64, device="cuda")
+
+            def P(t):
+                return ctypes.c_void_p(t.data_ptr())
+
+            a_out = ctypes.c_double()
+            calls = {
+                "update_scaling": lambda: L.clgpu_update_scaling(h, P(s), P(z), 1.0, 0, sh),
+                "mul_Hs": lambda: L.clgpu_mul_Hs(h, P(y), P(x), sh),
+                "affine_ds": lambda: L.clgpu_affine_ds(h, P(y), P(s), sh),
+                "combined_ds_shift": lambda: L.clgpu_combined_ds_shift(
+                    h, P(y), P(dz), P(ds), P(z), 0.1, sh),
+                "ds_from_dz_offset": lambda: L.clgpu_ds_from_dz_offset(h, P(y), P(ds), P(z), sh),
+                "step_length": lambda: L.clgpu_step_length(
+                    h, P(dz), P(ds), P(z), P(s), 1.0, 0.99, 0.8, 1e-4, ctypes.byref(a_out), sh),
+            }
+            res = {}
+            for op in CONE_OPS:
+                fn = calls[op]
+                for _ in range(1 if reps <= 1 else 2):
+                    rc = fn()
+                    assert rc == 0, (name, op, rc)
+                ts = []
+                for _ in range(reps):
+                    flush.add_(1.0)
+                    torch.cuda.synchronize()
+                    rc = fn()
+                    assert rc == 0, (name, op, rc)
+                    ms = ctypes.c_double()
+                    L.clgpu_cones_last_kernel_ms(h, ctypes.byref(ms))
+                    ts.append(ms.value)
+                ms = float(np.median(ts))
+                by = cone_op_bytes(op, code, dim, count)
+                gbs = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+                res[op] = {"us": round(1000 * ms, 2), "bytes": int(by),
+                           "GB/s": round(gbs, 1), "frac": round(gbs / hbm, 3)}
+            out[name] = {"cones": count, "dim": dim, "rows": m, "ops": res}
+            del s, z, dz, ds, x, y
+        finally:
+            L.clgpu_cones_destroy(h)
+    del flush
+    torch.cuda.synchronize()
+    return out
+
+
 def problem_bytes(pbs):
     b = 0
     for P, q, A, bb, c in pbs:
@@ -374,6 +544,13 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0,
                     help="length of the served (continuous batching) run; 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--cone-scale", type=float, default=1.0,
+                    help="size of the cone-kernel roofline workload (1.0: every streamed "
+                         "vector larger than L2); 0 skips it")
+    ap.add_argument("--cone-reps", type=int, default=5,
+                    help="timed calls per cone operation (median reported)")
+    ap.add_argument("--cone-kernels-only", action="store_true",
+                    help="run only the cone-kernel roofline workload and print its JSON")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -385,6 +562,13 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.cone_kernels_only:
+        peaks, _ = load_peaks()
+        hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+        print(json.dumps({"cone_kernels": cone_kernel_roofline(hbm, args.cone_scale,
+                                                               args.cone_reps),
+                          "peak_gbs": hbm}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -560,6 +744,18 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(args.ref_sample)
 
+    cones = None
+    if rank == 0 and args.cone_scale > 0:
+        ck = cone_kernel_roofline(hbm, args.cone_scale, args.cone_reps)
+        fr = sorted(v["frac"] for t in ck.values() for v in t["ops"].values())
+        cones = {"workload": "one cone-level handle per type (plain path, B = 1): "
+                             + ", ".join("%s %d cones x dim %d" % (k, v["cones"], v["dim"])
+                                         for k, v in ck.items()),
+                 "peak_gbs": hbm, "peak_kind": peak_note,
+                 "timing": "CUDA events around each operation's kernels, median of %d, "
+                           "L2 flushed before each call" % args.cone_reps,
+                 "frac_median": fr[len(fr) // 2], "types": ck}
+
     if rank == 0:
         roof_name = dom[0] if dom[0] in kernels else "ldl_solve"
         roof = roofline(roof_name)
@@ -596,6 +792,7 @@ def main():
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "served": served,
             "cpu_baseline": cpu,
+            "cone_kernels": cones,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

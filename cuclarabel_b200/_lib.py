@@ -85,6 +85,7 @@ EXPORTED = [
     "clgpu_ds_from_dz_offset", "clgpu_step_length", "clgpu_compute_barrier",
     "clgpu_margins", "clgpu_scaled_unit_shift", "clgpu_unit_initialization",
     "clgpu_debug_check_instance", "clgpu_margins_static",
+    "clgpu_cones_set_profiling", "clgpu_cones_last_kernel_ms",
 ]
 
 
@@ -115,6 +116,8 @@ def _declare(L):
     L.clgpu_cones_destroy.argtypes = [c_void_p]
     for f in ("clgpu_cones_numel", "clgpu_cones_degree", "clgpu_cones_hs_len"):
         getattr(L, f).argtypes = [c_void_p]
+    L.clgpu_cones_set_profiling.argtypes = [c_void_p, c_int]
+    L.clgpu_cones_last_kernel_ms.argtypes = [c_void_p, dp]
     V = c_void_p  # device pointers are passed as integers
     L.clgpu_update_scaling.argtypes = [c_void_p, V, V, c_double, c_int, c_void_p]
     L.clgpu_set_identity_scaling.argtypes = [c_void_p, c_void_p]

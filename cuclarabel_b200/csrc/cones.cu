@@ -32,6 +32,15 @@ static constexpr int kPsdWarps = 2;  // warps (cones) per PSD block
 __device__ __forceinline__ bool active_inst(const ConeSet &cs, int inst) {
   return cs.inst_active == nullptr || cs.inst_active[inst] != 0;
 }
+// Instance of row g: a single problem streams no row-to-instance index.
+__device__ __forceinline__ int row_instance(const ConeSet &cs, int g) {
+  return cs.B == 1 ? 0 : cs.row_inst[g];
+}
+// Row g belongs to a running instance; the row's instance is looked up only
+// when there is an active mask.
+__device__ __forceinline__ bool active_row(const ConeSet &cs, int g) {
+  return cs.inst_active == nullptr || cs.inst_active[row_instance(cs, g)] != 0;
+}
 
 // =================================================================== NN
 __global__ void k_nn_update_scaling(ConeSet cs, const double *__restrict__ s,
@@ -39,7 +48,7 @@ __global__ void k_nn_update_scaling(ConeSet cs, const double *__restrict__ s,
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
   int g = cs.nn_begin + e;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   double si = s[g], zi = z[g];
   cs.nn_lambda[e] = sqrt(si * zi);
   cs.nn_w[e] = sqrt(si / zi);
@@ -812,7 +821,7 @@ __device__ __forceinline__ void tri_coord(int k, int &row, int &col) {
 __global__ void k_nn_refresh(ConeSet cs, const int *__restrict__ pos, double *kv) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
-  if (!active_inst(cs, cs.row_inst[cs.nn_begin + e])) return;
+  if (!active_row(cs, cs.nn_begin + e)) return;
   double w = cs.nn_w[e];
   kv[pos[e]] = -(w * w);
 }
@@ -951,14 +960,14 @@ __global__ void k_zero_fill(ConeSet cs, double *y) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_zero) return;
   int g = cs.zero_begin + e;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   y[g] = 0.0;
 }
 __global__ void k_nn_mul_hs(ConeSet cs, double *y, const double *__restrict__ x) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
   int g = cs.nn_begin + e;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   double w = cs.nn_w[e];
   y[g] = w * (w * x[g]);
 }
@@ -1011,7 +1020,7 @@ __global__ void k_nn_affine_ds(ConeSet cs, double *ds) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
   int g = cs.nn_begin + e;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   double l = cs.nn_lambda[e];
   ds[g] = l * l;
 }
@@ -1054,7 +1063,7 @@ __global__ void k_nn_combined(ConeSet cs, double *shift, const double *__restric
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
   int g = cs.nn_begin + e;
-  int inst = cs.row_inst[g];
+  int inst = row_instance(cs, g);
   if (!active_inst(cs, inst)) return;
   double w = cs.nn_w[e];
   double wz = dz[g] * w, ws = ds[g] / w;
@@ -1164,7 +1173,7 @@ __global__ void k_nn_ds_offset(ConeSet cs, double *out, const double *__restrict
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
   int g = cs.nn_begin + e;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   out[g] = ds[g] / z[g];
 }
 // coneops_socone.jl:539-566
@@ -1227,7 +1236,7 @@ __global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
   double a = CUDART_INF;
   if (e < cs.n_nn) {
     int g = cs.nn_begin + e;
-    inst = cs.row_inst[g];
+    inst = row_instance(cs, g);
     if (active_inst(cs, inst)) {
       double dzi = dz[g], dsi = ds[g];
       if (dzi < 0) a = fmin(a, -z[g] / dzi);
@@ -1519,14 +1528,14 @@ __global__ void k_zero_shift(ConeSet cs, double *z, int pd) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_zero) return;
   int g = cs.zero_begin + e;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   if (pd == 0) z[g] = 0.0;
 }
 __global__ void k_nn_shift(ConeSet cs, double *z, const double *alpha) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= cs.n_nn) return;
   int g = cs.nn_begin + e;
-  int inst = cs.row_inst[g];
+  int inst = row_instance(cs, g);
   if (!active_inst(cs, inst)) return;
   z[g] += alpha[inst];
 }
@@ -1548,7 +1557,7 @@ __global__ void k_psd_shift(ConeSet cs, double *z, const double *alpha) {
 __global__ void k_unit_init(ConeSet cs, double *z, double *s) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= cs.m_total) return;
-  if (!active_inst(cs, cs.row_inst[g])) return;
+  if (!active_row(cs, g)) return;
   double v = 0.0;
   if (g >= cs.nn_begin && g < cs.nn_begin + cs.n_nn) v = 1.0;
   s[g] = v;
@@ -1595,11 +1604,11 @@ __global__ void k_unit_init_cones(ConeSet cs, double *z, double *s) {
 __global__ void k_identity(ConeSet cs) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < cs.n_nn) {
-    if (active_inst(cs, cs.row_inst[cs.nn_begin + t])) cs.nn_w[t] = 1.0;
+    if (active_row(cs, cs.nn_begin + t)) cs.nn_w[t] = 1.0;
   }
   if (t < cs.soc_rows) {
     int g = cs.soc_begin + t;
-    if (active_inst(cs, cs.row_inst[g])) {
+    if (active_row(cs, g)) {
       // first element of its cone?  soc rows are contiguous per cone; a row is
       // a head iff it equals the cone's offset -- found by the cone loop below
       cs.soc_w[t] = 0.0;

@@ -20,7 +20,31 @@ struct clgpu_cones {
       *d_psd_blk = nullptr;
   double *d_scal = nullptr;  // small scalar workspace [8]
   int *d_iscal = nullptr;    // [4]
+  // kernel-time profiling: events around an operation's launches only
+  bool prof = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double last_ms = 0.0;
+  ~clgpu_cones() {
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+  }
 };
+
+// Marks the start (k even) or end (k odd) of an operation's launch group
+// when profiling is on; step_length has two groups (k = 0..3).
+static void prof_mark(clgpu_cones *h, int k, cudaStream_t st) {
+  if (h->prof) cudaEventRecord(h->ev[k], st);
+}
+// After the stream has been synchronised: the operation's kernel time.
+static void prof_collect(clgpu_cones *h, int groups) {
+  if (!h->prof) return;
+  double ms = 0.0;
+  for (int p = 0; p < groups; ++p) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, h->ev[2 * p], h->ev[2 * p + 1]) == cudaSuccess) ms += t;
+  }
+  h->last_ms = ms;
+}
 
 extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
                                   const double *params, int soc_threshold,
@@ -184,12 +208,32 @@ extern "C" int clgpu_cones_numel(const clgpu_cones *h) { return h ? h->numel : -
 extern "C" int clgpu_cones_degree(const clgpu_cones *h) { return h ? h->degree : -1; }
 extern "C" int clgpu_cones_hs_len(const clgpu_cones *h) { return h ? h->hs_len : -1; }
 
+extern "C" int clgpu_cones_set_profiling(clgpu_cones *h, int enable) {
+  if (!h) return -1;
+  if (enable && !h->ev[0])
+    for (auto &e : h->ev)
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+  h->prof = enable != 0;
+  h->last_ms = 0.0;
+  return 0;
+}
+extern "C" int clgpu_cones_last_kernel_ms(const clgpu_cones *h, double *ms) {
+  if (!h || !ms) return -1;
+  *ms = h->last_ms;
+  return 0;
+}
+
 static int finish(cudaStream_t st) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return -1000 - (int)e;
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return -1000 - (int)e;
   return 0;
+}
+static int finish_prof(clgpu_cones *h, cudaStream_t st) {
+  int rc = finish(st);
+  if (rc == 0) prof_collect(h, 1);
+  return rc;
 }
 
 extern "C" int clgpu_update_scaling(clgpu_cones *h, const double *s, const double *z,
@@ -199,11 +243,14 @@ extern "C" int clgpu_update_scaling(clgpu_cones *h, const double *s, const doubl
   int iv[2] = {strategy, 1};
   cudaMemcpyAsync(h->d_scal, &mu, sizeof(double), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(h->d_iscal, iv, 2 * sizeof(int), cudaMemcpyHostToDevice, st);
+  prof_mark(h, 0, st);
   cones_update_scaling(h->cs, s, z, h->d_scal, h->d_iscal, h->d_iscal + 1, st);
+  prof_mark(h, 1, st);
   int ok = 0;
   cudaMemcpyAsync(&ok, h->d_iscal + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
   int rc = finish(st);
   if (rc) return rc;
+  prof_collect(h, 1);
   return ok ? 0 : 1;
 }
 extern "C" int clgpu_set_identity_scaling(clgpu_cones *h, clgpu_stream_t stream) {
@@ -215,20 +262,28 @@ extern "C" int clgpu_get_Hs(clgpu_cones *h, double *Hs, clgpu_stream_t stream) {
   if (!h) return -1;
   cudaStream_t st = (cudaStream_t)stream;
   cudaMemsetAsync(Hs, 0, (size_t)std::max(h->hs_len, 1) * sizeof(double), st);
+  prof_mark(h, 0, st);
   cones_get_Hs(h->cs, h->d_nn_blk, h->d_soc_blk, h->d_exp_blk, h->d_pow_blk, h->d_psd_blk, Hs,
                st);
-  return finish(st);
+  prof_mark(h, 1, st);
+  return finish_prof(h, st);
 }
 extern "C" int clgpu_mul_Hs(clgpu_cones *h, double *y, const double *x, clgpu_stream_t stream) {
   if (!h) return -1;
-  cones_mul_Hs(h->cs, y, x, (cudaStream_t)stream);
-  return finish((cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  prof_mark(h, 0, st);
+  cones_mul_Hs(h->cs, y, x, st);
+  prof_mark(h, 1, st);
+  return finish_prof(h, st);
 }
 extern "C" int clgpu_affine_ds(clgpu_cones *h, double *ds, const double *s,
                                clgpu_stream_t stream) {
   if (!h) return -1;
-  cones_affine_ds(h->cs, ds, s, (cudaStream_t)stream);
-  return finish((cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  prof_mark(h, 0, st);
+  cones_affine_ds(h->cs, ds, s, st);
+  prof_mark(h, 1, st);
+  return finish_prof(h, st);
 }
 extern "C" int clgpu_combined_ds_shift(clgpu_cones *h, double *shift, const double *step_z,
                                        const double *step_s, const double *z, double sigma_mu,
@@ -237,14 +292,19 @@ extern "C" int clgpu_combined_ds_shift(clgpu_cones *h, double *shift, const doub
   (void)z;
   cudaStream_t st = (cudaStream_t)stream;
   cudaMemcpyAsync(h->d_scal + 1, &sigma_mu, sizeof(double), cudaMemcpyHostToDevice, st);
+  prof_mark(h, 0, st);
   cones_combined_ds_shift(h->cs, shift, step_z, step_s, h->d_scal + 1, st);
-  return finish(st);
+  prof_mark(h, 1, st);
+  return finish_prof(h, st);
 }
 extern "C" int clgpu_ds_from_dz_offset(clgpu_cones *h, double *out, const double *ds,
                                        const double *z, clgpu_stream_t stream) {
   if (!h) return -1;
-  cones_ds_from_dz_offset(h->cs, out, ds, z, (cudaStream_t)stream);
-  return finish((cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  prof_mark(h, 0, st);
+  cones_ds_from_dz_offset(h->cs, out, ds, z, st);
+  prof_mark(h, 1, st);
+  return finish_prof(h, st);
 }
 extern "C" int clgpu_step_length(clgpu_cones *h, const double *dz, const double *ds,
                                  const double *z, const double *s, double alpha_max,
@@ -253,21 +313,28 @@ extern "C" int clgpu_step_length(clgpu_cones *h, const double *dz, const double 
   if (!h || !alpha) return -1;
   cudaStream_t st = (cudaStream_t)stream;
   cudaMemcpyAsync(h->d_scal + 2, &alpha_max, sizeof(double), cudaMemcpyHostToDevice, st);
+  prof_mark(h, 0, st);
   cones_step_length_sym(h->cs, dz, ds, z, s, h->d_scal + 2, st);
+  prof_mark(h, 1, st);
   double a = 0;
   cudaMemcpyAsync(&a, h->d_scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
   int rc = finish(st);
   if (rc) return rc;
+  int groups = 1;
   if (!h->symmetric) {
     a = std::min(a, max_step_fraction);
     cudaMemcpyAsync(h->d_scal + 2, &a, sizeof(double), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(h->d_scal + 3, &a, sizeof(double), cudaMemcpyHostToDevice, st);
+    prof_mark(h, 2, st);
     cones_step_length_asym(h->cs, dz, ds, z, s, h->d_scal + 2, h->d_scal + 3, backtrack_step,
                            alpha_min, st);
+    prof_mark(h, 3, st);
     cudaMemcpyAsync(&a, h->d_scal + 3, sizeof(double), cudaMemcpyDeviceToHost, st);
     rc = finish(st);
     if (rc) return rc;
+    groups = 2;
   }
+  prof_collect(h, groups);
   *alpha = a;
   return 0;
 }

@@ -208,6 +208,14 @@ int clgpu_cones_numel(const clgpu_cones *h);
 int clgpu_cones_degree(const clgpu_cones *h);
 /* length of the packed Hsblocks vector (rng_blocks, compositecone_type.jl:251) */
 int clgpu_cones_hs_len(const clgpu_cones *h);
+/* Kernel-time profiling of the cone operations: a profiling hook with no
+ * counterpart in the reference.  With profiling on, each operation below
+ * brackets its own kernel launches (not its scalar copies or its final
+ * synchronisation) with CUDA events, and clgpu_cones_last_kernel_ms returns
+ * the device time of the last completed operation in milliseconds
+ * (step_length: both launch groups summed). */
+int clgpu_cones_set_profiling(clgpu_cones *h, int enable);
+int clgpu_cones_last_kernel_ms(const clgpu_cones *h, double *ms);
 /* update_scaling! (coneops_compositecone_gpu.jl:185); strategy 0 PrimalDual,
  * 1 Dual; returns 1 if a cone is not strictly interior */
 int clgpu_update_scaling(clgpu_cones *h, const double *s, const double *z,

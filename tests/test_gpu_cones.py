@@ -187,3 +187,23 @@ def test_scaling_failure_reported(cuda_device):
     z = np.array([2.0, 0.1, 0.1, 0.1])
     d_s, d_z = G.dev(s), G.dev(z)
     assert G.L.clgpu_update_scaling(G.h, d_s.data_ptr(), d_z.data_ptr(), 1.0, 0, None) == 1
+
+
+def test_kernel_time_profiling_leaves_results_unchanged(cuda_device):
+    """With profiling on, an operation reports a positive kernel time and
+    writes the same values as without profiling."""
+    specs, rng, s, z = setup("mixed", seed=11)
+    G = GPUCones(specs)
+    d_s, d_z = G.dev(s), G.dev(z)
+    x = G.dev(rng.standard_normal(G.numel))
+    outs = []
+    for prof in (0, 1):
+        assert G.L.clgpu_cones_set_profiling(G.h, prof) == 0
+        assert G.L.clgpu_update_scaling(G.h, d_s.data_ptr(), d_z.data_ptr(), 1.0, 0, None) == 0
+        y = G.empty(G.numel)
+        assert G.L.clgpu_mul_Hs(G.h, y.data_ptr(), x.data_ptr(), None) == 0
+        ms = ctypes.c_double(-1.0)
+        assert G.L.clgpu_cones_last_kernel_ms(G.h, ctypes.byref(ms)) == 0
+        assert (ms.value > 0) if prof else (ms.value == 0.0)
+        outs.append(y.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
