@@ -201,6 +201,58 @@ __device__ __forceinline__ void seg_atomic_min_nonneg(double *base, int inst,
     atomic_min_nonneg(base + inst, v);
   }
 }
+// Atomic min of a non-negative value that skips the atomic when the stored
+// value is already no larger.  The stored value only decreases, so a stale
+// read can only let an unneeded atomic through; the result is the same.
+// Thousands of blocks folding into one instance's step length would
+// otherwise queue on a single address.
+__device__ __forceinline__ void atomic_min_nonneg_filtered(double *addr, double v) {
+  if (!(v >= 0)) v = 0;
+  if (v < __ldcg(addr)) atomic_min_nonneg(addr, v);
+}
+
+// Block-aggregated per-instance min: every thread of the block must call it
+// (threads without a value pass inst = -1); blockDim.x is a multiple of 32.
+// Warps whose contributing lanes share one instance are reduced in the warp,
+// then runs of equal instances across the block's warps in one thread, so a
+// block whose rows all belong to one instance issues one filtered atomic.
+__device__ __forceinline__ void block_seg_min_nonneg(double *base, int inst, double v) {
+  __shared__ int s_inst[32];
+  __shared__ double s_val[32];
+  const unsigned full = 0xffffffffu;
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (inst < 0) v = CUDART_INF;
+  else if (!(v >= 0)) v = 0;  // NaN or negative -> 0, as atomic_min_nonneg
+  int lead = inst;
+  for (int o = 16; o > 0; o >>= 1) lead = max(lead, __shfl_xor_sync(full, lead, o));
+  bool uniform = __all_sync(full, inst < 0 || inst == lead);
+  if (!uniform) {
+    if (inst >= 0) atomic_min_nonneg_filtered(base + inst, v);
+    lead = -1;
+  }
+  double m = warp_min(v);
+  if (lane == 0) {
+    s_inst[wid] = lead;
+    s_val[wid] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int cur = -1;
+    double cm = CUDART_INF;
+    for (int w = 0; w < nw; ++w) {
+      int iw = s_inst[w];
+      if (iw < 0) continue;
+      if (iw != cur) {
+        if (cur >= 0) atomic_min_nonneg_filtered(base + cur, cm);
+        cur = iw;
+        cm = s_val[w];
+      } else {
+        cm = fmin(cm, s_val[w]);
+      }
+    }
+    if (cur >= 0) atomic_min_nonneg_filtered(base + cur, cm);
+  }
+}
 __device__ __forceinline__ void seg_atomic_max_nonneg(double *base, int inst,
                                                       double v) {
   unsigned full = 0xffffffffu;

@@ -1246,7 +1246,7 @@ __global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
       inst = -1;
     }
   }
-  seg_atomic_min_nonneg(alpha, inst, a);
+  block_seg_min_nonneg(alpha, inst, a);
 }
 
 // coneops_socone.jl:745-814 with group reductions
@@ -1279,7 +1279,7 @@ __global__ void k_soc_step(ConeSet cs, const double *__restrict__ dz,
   double amax = alpha[ctx.inst];  // upper bound already there (atomic min target)
   double az = soc_step_component<G>(z + ctx.off, dz + ctx.off, amax, ctx);
   double as = soc_step_component<G>(s + ctx.off, ds + ctx.off, amax, ctx);
-  if (ctx.valid && ctx.lane == 0) atomic_min_nonneg(alpha + ctx.inst, fmin(az, as));
+  block_seg_min_nonneg(alpha, (ctx.valid && ctx.lane == 0) ? ctx.inst : -1, fmin(az, as));
 }
 __global__ void k_psd_step(ConeSet cs, const double *__restrict__ dz,
                            const double *__restrict__ ds, double *alpha) {
@@ -1312,7 +1312,7 @@ __global__ void k_psd_step(ConeSet cs, const double *__restrict__ dz,
     double a = gmin < 0 ? fmin(1.0 / (-gmin), amax) : amax;
     res = fmin(res, a);
   }
-  if (p.lane == 0) atomic_min_nonneg(alpha + p.inst, res);
+  if (p.lane == 0) atomic_min_nonneg_filtered(alpha + p.inst, res);
 }
 // coneops_nonsymmetric_common.jl:5-34 backtracking, per cone
 template <class Ops>
@@ -1321,29 +1321,31 @@ __global__ void k_nonsym_step(ConeSet cs, NonsymArgs<Ops> a, const double *__res
                               const double *__restrict__ s, const double *astart,
                               double *alpha, double step, double amin) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.n) return;
-  int inst = a.inst[c];
-  if (!active_inst(cs, inst)) return;
-  double pa = a.alpha ? a.alpha[c] : 0.0;
-  int b = a.begin + 3 * c;
-  double a0 = astart[inst];
-  double res = a0;
-  for (int side = 0; side < 2; ++side) {
-    const double *q = side == 0 ? z : s;
-    const double *dq = side == 0 ? dz : ds;
-    double al = a0, wq[3];
-    while (true) {
-      for (int i = 0; i < 3; ++i) wq[i] = q[b + i] + al * dq[b + i];
-      bool ok = side == 0 ? Ops::dual_feasible(wq, pa) : Ops::primal_feasible(wq, pa);
-      if (ok) break;
-      if ((al *= step) < amin) {
-        al = 0;
-        break;
+  int inst = c < a.n ? a.inst[c] : -1;
+  if (inst >= 0 && !active_inst(cs, inst)) inst = -1;
+  double res = CUDART_INF;
+  if (inst >= 0) {
+    double pa = a.alpha ? a.alpha[c] : 0.0;
+    int b = a.begin + 3 * c;
+    double a0 = astart[inst];
+    res = a0;
+    for (int side = 0; side < 2; ++side) {
+      const double *q = side == 0 ? z : s;
+      const double *dq = side == 0 ? dz : ds;
+      double al = a0, wq[3];
+      while (true) {
+        for (int i = 0; i < 3; ++i) wq[i] = q[b + i] + al * dq[b + i];
+        bool ok = side == 0 ? Ops::dual_feasible(wq, pa) : Ops::primal_feasible(wq, pa);
+        if (ok) break;
+        if ((al *= step) < amin) {
+          al = 0;
+          break;
+        }
       }
+      res = fmin(res, al);
     }
-    res = fmin(res, al);
   }
-  atomic_min_nonneg(alpha + inst, res);
+  block_seg_min_nonneg(alpha, inst, res);
 }
 
 // ================================================================ barrier
