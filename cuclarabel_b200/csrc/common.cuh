@@ -47,6 +47,9 @@ struct ConeSet {
   const int *soc_dim;   // [n_soc]
   const int *soc_inst;  // [n_soc]
   const int *soc_sparse;// [n_soc] 1 if dim > soc_threshold
+  int soc_ntiles;       // shared-memory tiles of consecutive small cones
+  int soc_skip_small;   // lane-group kernels leave tiled cones alone
+  const int *soc_tile;  // [2*soc_ntiles] first and one-past-last cone of each
   // exponential / power cones (3 rows each, contiguous)
   int n_exp, exp_begin;
   int n_pow, pow_begin;

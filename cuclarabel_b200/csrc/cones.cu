@@ -69,6 +69,7 @@ struct SocCtx {
     dim = cs.soc_dim[c];
     inst = cs.soc_inst[c];
     if (valid && !active_inst(cs, inst)) valid = false;
+    if (valid && cs.soc_skip_small && dim <= kSocTileMaxDim) valid = false;
   }
 };
 #define SOC_FOR(i) for (int i = ctx.lane; i < ctx.dim; i += G)
@@ -1645,6 +1646,354 @@ __global__ void k_identity_cones(ConeSet cs) {
   }
 }
 
+// ======================================================== SOC tile kernels
+// One block per tile of consecutive small cones (dim <= kSocTileMaxDim), one
+// thread per cone.  The tile's rows are staged in shared memory by coalesced
+// loads, each thread runs its cone's formulas sequentially over its own rows
+// (same formulas as the lane-group kernels above, sums in element order), and
+// results leave through coalesced stores of the rows whose cone is active.
+// Shared rows are skewed by one word every 16 so that threads walking their
+// cones at a stride of 3..16 words meet few bank conflicts.
+__device__ __forceinline__ int tsk(int i) { return i + (i >> 4); }
+static constexpr int kTileWords = kSocTileRows + kSocTileRows / 16 + 1;
+
+struct SocTileCtx {
+  int c0, nc, r0, nrows;  // tile: cones [c0, c0+nc), global rows [r0, r0+nrows)
+  int k, c, off, dim, inst;  // this thread's cone (k < nc) and its rows in the tile
+  bool valid;
+  unsigned short *rcone;  // [kSocTileRows] local cone of each tile row
+  unsigned char *ok;      // [kSocTileCones] cone's rows are written back
+};
+
+// Shared layout: `narr` staged arrays of kTileWords doubles, then rcone, ok.
+__device__ __forceinline__ double *tile_arr(int a) {
+  extern __shared__ __align__(16) double tile_smem[];
+  return tile_smem + (size_t)a * kTileWords;
+}
+__device__ __forceinline__ SocTileCtx soc_tile_ctx(const ConeSet &cs, int narr) {
+  SocTileCtx t;
+  int b = blockIdx.x;
+  t.c0 = cs.soc_tile[2 * b];
+  int c1 = cs.soc_tile[2 * b + 1];
+  t.nc = c1 - t.c0;
+  t.r0 = cs.soc_off[t.c0];
+  t.nrows = cs.soc_off[c1 - 1] + cs.soc_dim[c1 - 1] - t.r0;
+  t.rcone = reinterpret_cast<unsigned short *>(tile_arr(narr));
+  t.ok = reinterpret_cast<unsigned char *>(t.rcone + kSocTileRows);
+  t.k = threadIdx.x;
+  t.valid = t.k < t.nc;
+  t.c = t.valid ? t.c0 + t.k : t.c0;
+  t.off = cs.soc_off[t.c] - t.r0;
+  t.dim = cs.soc_dim[t.c];
+  t.inst = cs.soc_inst[t.c];
+  if (t.valid) {
+    for (int i = 0; i < t.dim; ++i) t.rcone[t.off + i] = (unsigned short)t.k;
+    t.ok[t.k] = 0;
+    if (!active_inst(cs, t.inst)) t.valid = false;
+  }
+  return t;
+}
+__device__ __forceinline__ void tile_load(double *dst, const double *__restrict__ src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[tsk(i)] = src[i];
+}
+__device__ __forceinline__ void tile_store(double *dst, const double *src, int n,
+                                           const SocTileCtx &t) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (t.ok[t.rcone[i]]) dst[i] = src[tsk(i)];
+}
+
+// update_scaling! for tiled cones (coneops_socone.jl:372-451; sparse d/u/v of
+// coneops_socone_gpu.jl:338-470).  w and lambda overwrite the staged s and z
+// rows in place (each thread only reads its own rows).
+__global__ void k_soc_tile_update_scaling(ConeSet cs, const double *__restrict__ s_,
+                                          const double *__restrict__ z_, int *scale_ok) {
+  SocTileCtx t = soc_tile_ctx(cs, 4);
+  double *S = tile_arr(0), *Z = tile_arr(1), *U = tile_arr(2), *V = tile_arr(3);
+  tile_load(S, s_ + t.r0, t.nrows);
+  tile_load(Z, z_ + t.r0, t.nrows);
+  __syncthreads();
+  bool sparse_tile = false;
+  if (t.valid) {
+    const int o = t.off, d = t.dim;
+    double s0 = S[tsk(o)], z0 = Z[tsk(o)];
+    double z1sq = 0, s1sq = 0;
+    for (int i = 1; i < d; ++i) {
+      double zi = Z[tsk(o + i)], si = S[tsk(o + i)];
+      z1sq += zi * zi;
+      s1sq += si * si;
+    }
+    double zs = soc_res(z0, z1sq), ss = soc_res(s0, s1sq);
+    double zscale = zs > 0.0 ? sqrt(zs) : 0.0;
+    double sscale = ss > 0.0 ? sqrt(ss) : 0.0;
+    bool fail = (zscale == 0.0 || sscale == 0.0);
+    if (fail) zscale = sscale = 1.0;
+    double eta = sqrt(sscale / zscale);
+    double w1sq_a = 0;
+    for (int i = 1; i < d; ++i) {
+      double wi = S[tsk(o + i)] / sscale + (-Z[tsk(o + i)]) / zscale;
+      w1sq_a += wi * wi;
+    }
+    double w0pre = s0 / sscale + z0 / zscale;
+    double wres = soc_res(w0pre, w1sq_a);
+    double wscale = wres > 0.0 ? sqrt(wres) : 0.0;
+    if (wscale == 0.0) {
+      fail = true;
+      wscale = 1.0;
+    }
+    double w1sq = 0;
+    for (int i = 1; i < d; ++i) {
+      double wi = (S[tsk(o + i)] / sscale + (-Z[tsk(o + i)]) / zscale) / wscale;
+      w1sq += wi * wi;
+    }
+    double w0 = sqrt(1 + w1sq);
+    double gamma = 0.5 * wscale;
+    double c1 = (gamma + z0 / zscale) / sscale;
+    double c2 = (gamma + s0 / sscale) / zscale;
+    double inv = 1.0 / (s0 / sscale + z0 / zscale + 2 * gamma);
+    double sc = sqrt(sscale * zscale);
+    bool sparse = cs.soc_sparse[t.c] != 0;
+    double u0 = 0, u1 = 0, v1 = 0, dd = 0;
+    if (sparse) {
+      double wsq = w0 * w0 + w1sq;
+      double wsqinv = 1 / wsq;
+      dd = wsqinv / 2;
+      u0 = sqrt(wsq - dd);
+      u1 = 2 * w0 / u0;
+      v1 = sqrt(2 * (2 + wsqinv) / (2 * wsq - wsqinv));
+    }
+    if (fail) {
+      scale_ok[t.inst] = 0;
+    } else {
+      for (int i = 1; i < d; ++i) {
+        double si = S[tsk(o + i)], zi = Z[tsk(o + i)];
+        double wi = (si / sscale + (-zi) / zscale) / wscale;
+        S[tsk(o + i)] = wi;
+        Z[tsk(o + i)] = ((c1 * si + c2 * zi) * inv) * sc;
+        if (sparse) {
+          U[tsk(o + i)] = u1 * wi;
+          V[tsk(o + i)] = v1 * wi;
+        }
+      }
+      S[tsk(o)] = w0;
+      Z[tsk(o)] = gamma * sc;
+      if (sparse) {
+        U[tsk(o)] = u0;
+        V[tsk(o)] = 0.0;
+      }
+      cs.soc_eta[t.c] = eta;
+      if (sparse) cs.soc_d[t.c] = dd;
+      t.ok[t.k] = sparse ? 2 : 1;
+    }
+    sparse_tile = sparse;
+  }
+  sparse_tile = __syncthreads_or(sparse_tile);
+  const int r = t.r0 - cs.soc_begin;
+  tile_store(cs.soc_w + r, S, t.nrows, t);
+  tile_store(cs.soc_lambda + r, Z, t.nrows, t);
+  if (sparse_tile) {
+    for (int i = threadIdx.x; i < t.nrows; i += blockDim.x)
+      if (t.ok[t.rcone[i]] == 2) {
+        cs.soc_u[r + i] = U[tsk(i)];
+        cs.soc_v[r + i] = V[tsk(i)];
+      }
+  }
+}
+
+// mul_Hs for tiled cones: y = eta^2 (J x + 2 (w'x) w), J = diag(-1, 1, ...)
+__global__ void k_soc_tile_mul_hs(ConeSet cs, double *y_, const double *__restrict__ x_) {
+  SocTileCtx t = soc_tile_ctx(cs, 2);
+  double *W = tile_arr(0), *X = tile_arr(1);
+  tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
+  tile_load(X, x_ + t.r0, t.nrows);
+  __syncthreads();
+  if (t.valid) {
+    const int o = t.off, d = t.dim;
+    double tt = 0;
+    for (int i = 0; i < d; ++i) tt += W[tsk(o + i)] * X[tsk(o + i)];
+    double c = 2 * tt;
+    double eta = cs.soc_eta[t.c], e2 = eta * eta;
+    for (int i = 0; i < d; ++i) {
+      double xi = X[tsk(o + i)];
+      double v = (i == 0) ? -xi : xi;
+      X[tsk(o + i)] = (v + c * W[tsk(o + i)]) * e2;
+    }
+    t.ok[t.k] = 1;
+  }
+  __syncthreads();
+  tile_store(y_ + t.r0, X, t.nrows, t);
+}
+
+// affine_ds! for tiled cones: ds = lambda o lambda
+__global__ void k_soc_tile_affine_ds(ConeSet cs, double *ds_) {
+  SocTileCtx t = soc_tile_ctx(cs, 1);
+  double *L = tile_arr(0);
+  tile_load(L, cs.soc_lambda + (t.r0 - cs.soc_begin), t.nrows);
+  __syncthreads();
+  if (t.valid) {
+    const int o = t.off, d = t.dim;
+    double tt = 0;
+    for (int i = 0; i < d; ++i) tt += L[tsk(o + i)] * L[tsk(o + i)];
+    double l0 = L[tsk(o)];
+    for (int i = 1; i < d; ++i) {
+      double li = L[tsk(o + i)];
+      L[tsk(o + i)] = l0 * li + l0 * li;
+    }
+    L[tsk(o)] = tt;
+    t.ok[t.k] = 1;
+  }
+  __syncthreads();
+  tile_store(ds_ + t.r0, L, t.nrows, t);
+}
+
+// combined_ds_shift! for tiled cones (coneops_defaults.jl:335-368): the
+// shift overwrites the staged dz rows in place.
+__global__ void k_soc_tile_combined(ConeSet cs, double *shift_, const double *__restrict__ dz_,
+                                    const double *__restrict__ ds_, const double *sm) {
+  SocTileCtx t = soc_tile_ctx(cs, 3);
+  double *W = tile_arr(0), *DZ = tile_arr(1), *DS = tile_arr(2);
+  tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
+  tile_load(DZ, dz_ + t.r0, t.nrows);
+  tile_load(DS, ds_ + t.r0, t.nrows);
+  __syncthreads();
+  if (t.valid) {
+    const int o = t.off, d = t.dim;
+    double eta = cs.soc_eta[t.c], w0 = W[tsk(o)];
+    double zz = 0, zs = 0;
+    for (int i = 1; i < d; ++i) {
+      double wi = W[tsk(o + i)];
+      zz += wi * DZ[tsk(o + i)];
+      zs += wi * DS[tsk(o + i)];
+    }
+    double dz0 = DZ[tsk(o)], ds0 = DS[tsk(o)];
+    double cz = dz0 + zz / (1 + w0);
+    double csn = -ds0 + zs / (1 + w0);
+    double wz0 = eta * (w0 * dz0 + zz);
+    double ws0 = (1 / eta) * (w0 * ds0 - zs);
+    double dot = wz0 * ws0;
+    for (int i = 1; i < d; ++i) {
+      double wi = W[tsk(o + i)];
+      double a = eta * (DZ[tsk(o + i)] + cz * wi);
+      double b = (1 / eta) * (DS[tsk(o + i)] + csn * wi);
+      dot += a * b;
+    }
+    for (int i = 1; i < d; ++i) {
+      double wi = W[tsk(o + i)];
+      double a = eta * (DZ[tsk(o + i)] + cz * wi);
+      double b = (1 / eta) * (DS[tsk(o + i)] + csn * wi);
+      DZ[tsk(o + i)] = ws0 * a + wz0 * b;
+    }
+    DZ[tsk(o)] = dot - sm[t.inst];
+    t.ok[t.k] = 1;
+  }
+  __syncthreads();
+  tile_store(shift_ + t.r0, DZ, t.nrows, t);
+}
+
+// Δs_from_Δz_offset! for tiled cones (coneops_socone.jl:539-566): the output
+// overwrites the staged ds rows in place.
+__global__ void k_soc_tile_ds_offset(ConeSet cs, double *out_, const double *__restrict__ ds_,
+                                     const double *__restrict__ z_) {
+  SocTileCtx t = soc_tile_ctx(cs, 4);
+  double *W = tile_arr(0), *L = tile_arr(1), *DS = tile_arr(2), *Z = tile_arr(3);
+  const int r = t.r0 - cs.soc_begin;
+  tile_load(W, cs.soc_w + r, t.nrows);
+  tile_load(L, cs.soc_lambda + r, t.nrows);
+  tile_load(DS, ds_ + t.r0, t.nrows);
+  tile_load(Z, z_ + t.r0, t.nrows);
+  __syncthreads();
+  if (t.valid) {
+    const int o = t.off, d = t.dim;
+    double z1sq = 0, l1ds1 = 0, w1ds1 = 0;
+    for (int i = 1; i < d; ++i) {
+      double zi = Z[tsk(o + i)], dsi = DS[tsk(o + i)];
+      z1sq += zi * zi;
+      l1ds1 += L[tsk(o + i)] * dsi;
+      w1ds1 += W[tsk(o + i)] * dsi;
+    }
+    double z0 = Z[tsk(o)], l0 = L[tsk(o)], w0 = W[tsk(o)];
+    double resz = soc_res(z0, z1sq);
+    double eta = cs.soc_eta[t.c];
+    double c = l0 * DS[tsk(o)] - l1ds1;
+    double il = 1 / l0;
+    for (int i = 1; i < d; ++i) {
+      double o_i = -Z[tsk(o + i)] * (c / resz);
+      o_i += eta * (DS[tsk(o + i)] + w1ds1 / (1 + w0) * W[tsk(o + i)]);
+      DS[tsk(o + i)] = o_i * il;
+    }
+    double o0 = z0 * (c / resz);
+    o0 += eta * w1ds1;
+    DS[tsk(o)] = o0 * il;
+    t.ok[t.k] = 1;
+  }
+  __syncthreads();
+  tile_store(out_ + t.r0, DS, t.nrows, t);
+}
+
+// step_length for tiled cones (coneops_socone.jl:745-814), sequential sums
+__device__ double soc_tile_step_component(const double *X, const double *Y, int o, int d,
+                                          double amax) {
+  double x0 = X[tsk(o)], y0 = Y[tsk(o)];
+  double ysq = 0, xsq = 0, xy = 0;
+  for (int i = 1; i < d; ++i) {
+    double xi = X[tsk(o + i)], yi = Y[tsk(o + i)];
+    ysq += yi * yi;
+    xsq += xi * xi;
+    xy += xi * yi;
+  }
+  if (x0 >= 0 && y0 < 0) amax = fmin(amax, -x0 / y0);
+  double a = soc_res(y0, ysq);
+  double b = 2 * (x0 * y0 - xy);
+  double c = fmax(0.0, soc_res(x0, xsq));
+  double dd = b * b - 4 * a * c;
+  if ((a > 0 && b > 0) || dd < 0) return amax;
+  if (a == 0) return amax;
+  if (c == 0) return a >= 0 ? amax : 0.0;
+  double tq = (b >= 0) ? (-b - sqrt(dd)) : (-b + sqrt(dd));
+  double r1 = (2 * c) / tq, r2 = tq / (2 * a);
+  r1 = r1 < 0 ? kDMax : r1;
+  r2 = r2 < 0 ? kDMax : r2;
+  return fmin(amax, fmin(r1, r2));
+}
+__global__ void k_soc_tile_step(ConeSet cs, const double *__restrict__ dz_,
+                                const double *__restrict__ ds_, const double *__restrict__ z_,
+                                const double *__restrict__ s_, double *alpha) {
+  SocTileCtx t = soc_tile_ctx(cs, 4);
+  double *DZ = tile_arr(0), *DS = tile_arr(1), *Z = tile_arr(2), *S = tile_arr(3);
+  tile_load(DZ, dz_ + t.r0, t.nrows);
+  tile_load(DS, ds_ + t.r0, t.nrows);
+  tile_load(Z, z_ + t.r0, t.nrows);
+  tile_load(S, s_ + t.r0, t.nrows);
+  __syncthreads();
+  double a = CUDART_INF;
+  if (t.valid) {
+    double amax = alpha[t.inst];
+    double az = soc_tile_step_component(Z, DZ, t.off, t.dim, amax);
+    double as = soc_tile_step_component(S, DS, t.off, t.dim, amax);
+    a = fmin(az, as);
+  }
+  block_seg_min_nonneg(alpha, t.valid ? t.inst : -1, a);
+}
+
+std::vector<int> soc_tiles(const int *off, const int *dim, int n) {
+  std::vector<int> t;
+  int k = 0;
+  while (k < n) {
+    if (dim[k] > kSocTileMaxDim || dim[k] < 1) {
+      ++k;
+      continue;
+    }
+    int start = k, rows = 0;
+    while (k < n && dim[k] >= 1 && dim[k] <= kSocTileMaxDim && k - start < kSocTileCones &&
+           rows + dim[k] <= kSocTileRows && (k == start || off[k] == off[k - 1] + dim[k - 1])) {
+      rows += dim[k];
+      ++k;
+    }
+    t.push_back(start);
+    t.push_back(k);
+  }
+  return t;
+}
+
 // =============================================================== launchers
 static inline int blocks_for(long long n, int b = kBlock) {
   return n <= 0 ? 0 : ceil_div(n, b);
@@ -1661,6 +2010,24 @@ static inline int blocks_for(long long n, int b = kBlock) {
         case 16: KERNEL<16><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                \
         default: KERNEL<32><<<nb, kBlock, 0, st>>>(__VA_ARGS__); break;                \
       }                                                                                \
+    }                                                                                  \
+  } while (0)
+
+// Tiled small cones, then (when some cone is larger than the tile limit) the
+// lane-group kernel for the large cones only.
+static inline size_t soc_tile_smem(int narr) {
+  return (size_t)narr * kTileWords * sizeof(double) + kSocTileRows * sizeof(unsigned short) +
+         kSocTileCones;
+}
+#define LAUNCH_SOC_TILED(TILE_KERNEL, NARR, GROUP_KERNEL, ...)                         \
+  do {                                                                                 \
+    if (cs.soc_ntiles > 0)                                                             \
+      TILE_KERNEL<<<cs.soc_ntiles, kSocTileCones, soc_tile_smem(NARR), st>>>(          \
+          cs, __VA_ARGS__);                                                            \
+    if (cs.n_soc > 0 && cs.soc_group == 32) {                                          \
+      ConeSet csl = cs;                                                                \
+      csl.soc_skip_small = 1;                                                          \
+      LAUNCH_SOC(GROUP_KERNEL, csl, __VA_ARGS__);                                      \
     }                                                                                  \
   } while (0)
 
@@ -1693,7 +2060,7 @@ void cones_update_scaling(const ConeSet &cs, const double *s, const double *z,
                           const double *mu, const int *scaling, int *scale_ok,
                           cudaStream_t st) {
   if (cs.n_nn) k_nn_update_scaling<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, s, z);
-  LAUNCH_SOC(k_soc_update_scaling, cs, s, z, scale_ok);
+  LAUNCH_SOC_TILED(k_soc_tile_update_scaling, 4, k_soc_update_scaling, s, z, scale_ok);
   if (cs.n_exp)
     k_nonsym_update_scaling<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
         cs, exp_args(cs), s, z, mu, scaling);
@@ -1731,7 +2098,7 @@ void cones_get_Hs(const ConeSet &cs, const int *nn_blk, const int *soc_blk,
 void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, y);
   if (cs.n_nn) k_nn_mul_hs<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, y, x);
-  LAUNCH_SOC(k_soc_mul_hs, cs, y, x);
+  LAUNCH_SOC_TILED(k_soc_tile_mul_hs, 2, k_soc_mul_hs, y, x);
   if (cs.n_exp)
     k_nonsym_mul_hs<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                             cs.exp_inst, cs.exp_Hs, y, x);
@@ -1744,7 +2111,7 @@ void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st
 void cones_affine_ds(const ConeSet &cs, double *ds, const double *s, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, ds);
   if (cs.n_nn) k_nn_affine_ds<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, ds);
-  LAUNCH_SOC(k_soc_affine_ds, cs, ds);
+  LAUNCH_SOC_TILED(k_soc_tile_affine_ds, 1, k_soc_affine_ds, ds);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                               cs.exp_inst, ds, s);
@@ -1758,7 +2125,7 @@ void cones_combined_ds_shift(const ConeSet &cs, double *shift, const double *dz,
                              const double *ds, const double *sm, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, shift);
   if (cs.n_nn) k_nn_combined<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, shift, dz, ds, sm);
-  LAUNCH_SOC(k_soc_combined, cs, shift, dz, ds, sm);
+  LAUNCH_SOC_TILED(k_soc_tile_combined, 3, k_soc_combined, shift, dz, ds, sm);
   if (cs.n_exp)
     k_nonsym_combined<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
         cs, exp_args(cs), shift, dz, ds, sm);
@@ -1772,7 +2139,7 @@ void cones_ds_from_dz_offset(const ConeSet &cs, double *out, const double *ds,
                              const double *z, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, out);
   if (cs.n_nn) k_nn_ds_offset<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, out, ds, z);
-  LAUNCH_SOC(k_soc_ds_offset, cs, out, ds, z);
+  LAUNCH_SOC_TILED(k_soc_tile_ds_offset, 4, k_soc_ds_offset, out, ds, z);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                               cs.exp_inst, out, ds);
@@ -1786,7 +2153,7 @@ void cones_step_length_sym(const ConeSet &cs, const double *dz, const double *ds
                            const double *z, const double *s, double *alpha,
                            cudaStream_t st) {
   if (cs.n_nn) k_nn_step<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, dz, ds, z, s, alpha);
-  LAUNCH_SOC(k_soc_step, cs, dz, ds, z, s, alpha);
+  LAUNCH_SOC_TILED(k_soc_tile_step, 4, k_soc_step, dz, ds, z, s, alpha);
   LAUNCH_PSD(k_psd_step, 4, cs, dz, ds, alpha);
 }
 

@@ -7,7 +7,23 @@
 #pragma once
 #include "common.cuh"
 
+#include <vector>
+
 namespace clgpu {
+
+// Second-order cones of dimension <= kSocTileMaxDim are processed in tiles by
+// the per-iteration kernels (update_scaling, mul_Hs, affine_ds,
+// combined_ds_shift, ds_from_dz_offset, step_length): a tile is a run of
+// consecutive cones with contiguous rows, at most kSocTileCones cones and
+// kSocTileRows rows, staged through shared memory with coalesced loads and
+// stores, one thread per cone.  Larger cones keep the lane-group kernels.
+// A cone's arithmetic depends only on its own dimension either way, so an
+// instance computes the same bits alone or in any batch.
+constexpr int kSocTileMaxDim = 16;
+constexpr int kSocTileCones = 128;
+constexpr int kSocTileRows = 1024;
+// Tile list [c0, c1, c0, c1, ...] over n cones (rows off[k] .. off[k]+dim[k]).
+std::vector<int> soc_tiles(const int *off, const int *dim, int n);
 
 // update_scaling!  (coneops_compositecone_gpu.jl:185).  mu/scaling are
 // per-instance device arrays; scale_ok[i] is cleared to 0 on failure.

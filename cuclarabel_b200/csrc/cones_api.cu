@@ -143,6 +143,12 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
   cs.soc_dim = A.upload(soc_dim);
   cs.soc_inst = A.upload(soc_inst);
   cs.soc_sparse = A.upload(soc_sparse);
+  {
+    std::vector<int> tiles = soc_tiles(soc_off.data(), soc_dim.data(), (int)soc_off.size());
+    cs.soc_ntiles = (int)tiles.size() / 2;
+    cs.soc_tile = A.upload(tiles);
+    cs.soc_skip_small = 0;
+  }
   cs.exp_inst = A.upload(exp_inst);
   cs.pow_inst = A.upload(pow_inst);
   cs.pow_alpha = A.upload(pow_alpha);

@@ -45,6 +45,13 @@ SPECS = {
     "psd": [(5, 3, 0.0), (5, 10, 0.0)],
     "mixed": [(0, 2, 0.0), (1, 4, 0.0), (2, 3, 0.0), (2, 8, 0.0), (3, 3, 0.0), (4, 3, 0.4),
               (5, 4, 0.0)],
+    # several shared-memory tiles of small cones (at most 128 cones or 1024
+    # rows each), broken by cones above the tile limit (dim > 16)
+    "soc_tiles": [(2, int(d), 0.0) for d in
+                  np.random.default_rng(42).choice([2, 3, 5, 8, 10, 13, 16, 17, 24, 33],
+                                                   size=300,
+                                                   p=[.1, .15, .15, .15, .1, .1, .1, .05,
+                                                      .05, .05])],
 }
 
 
