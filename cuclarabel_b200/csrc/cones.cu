@@ -1649,12 +1649,33 @@ __global__ void k_identity_cones(ConeSet cs) {
 // ======================================================== SOC tile kernels
 // One block per tile of consecutive small cones (dim <= kSocTileMaxDim), one
 // thread per cone.  The tile's rows are staged in shared memory by coalesced
-// loads, each thread runs its cone's formulas sequentially over its own rows
-// (same formulas as the lane-group kernels above, sums in element order), and
-// results leave through coalesced stores of the rows whose cone is active.
+// loads, each thread runs its cone's formulas over its own rows (the
+// formulas of the lane-group kernels above, with their sums in the same
+// butterfly order, tree16), and results leave through coalesced stores of
+// the rows whose cone is active.
 // Shared rows are skewed by one word every 16 so that threads walking their
 // cones at a stride of 3..16 words meet few bank conflicts.
 __device__ __forceinline__ int tsk(int i) { return i + (i >> 4); }
+// Sum of a cone's per-element terms in the order of the lane-group kernels'
+// butterfly reduction (pairs at distance 8, 4, 2, 1 over 16 leaves, leaves
+// from the cone's dimension on are +0): for dim <= 16 this is the same
+// result, bit for bit, as group_sum<G> for every G >= dim.  leaf(l) is the
+// partial a group lane l would hold (0.0 + its term).
+template <class F>
+__device__ __forceinline__ double tree16(int d, F leaf) {
+  double p[8];
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    double a = l < d ? leaf(l) : 0.0;
+    double b = l + 8 < d ? leaf(l + 8) : 0.0;
+    p[l] = a + b;
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+    for (int l = 0; l < o; ++l) p[l] = p[l] + p[l + o];
+  return p[0];
+}
 static constexpr int kTileWords = kSocTileRows + kSocTileRows / 16 + 1;
 
 struct SocTileCtx {
@@ -1716,23 +1737,24 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const double *__restrict__
   if (t.valid) {
     const int o = t.off, d = t.dim;
     double s0 = S[tsk(o)], z0 = Z[tsk(o)];
-    double z1sq = 0, s1sq = 0;
-    for (int i = 1; i < d; ++i) {
-      double zi = Z[tsk(o + i)], si = S[tsk(o + i)];
-      z1sq += zi * zi;
-      s1sq += si * si;
-    }
+    double z1sq = tree16(d, [&](int l) {
+      double zl = Z[tsk(o + l)];
+      return l > 0 ? 0.0 + zl * zl : 0.0;
+    });
+    double s1sq = tree16(d, [&](int l) {
+      double sl = S[tsk(o + l)];
+      return l > 0 ? 0.0 + sl * sl : 0.0;
+    });
     double zs = soc_res(z0, z1sq), ss = soc_res(s0, s1sq);
     double zscale = zs > 0.0 ? sqrt(zs) : 0.0;
     double sscale = ss > 0.0 ? sqrt(ss) : 0.0;
     bool fail = (zscale == 0.0 || sscale == 0.0);
     if (fail) zscale = sscale = 1.0;
     double eta = sqrt(sscale / zscale);
-    double w1sq_a = 0;
-    for (int i = 1; i < d; ++i) {
-      double wi = S[tsk(o + i)] / sscale + (-Z[tsk(o + i)]) / zscale;
-      w1sq_a += wi * wi;
-    }
+    double w1sq_a = tree16(d, [&](int l) {
+      double wl = S[tsk(o + l)] / sscale + (-Z[tsk(o + l)]) / zscale;
+      return l > 0 ? 0.0 + wl * wl : 0.0;
+    });
     double w0pre = s0 / sscale + z0 / zscale;
     double wres = soc_res(w0pre, w1sq_a);
     double wscale = wres > 0.0 ? sqrt(wres) : 0.0;
@@ -1740,11 +1762,10 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const double *__restrict__
       fail = true;
       wscale = 1.0;
     }
-    double w1sq = 0;
-    for (int i = 1; i < d; ++i) {
-      double wi = (S[tsk(o + i)] / sscale + (-Z[tsk(o + i)]) / zscale) / wscale;
-      w1sq += wi * wi;
-    }
+    double w1sq = tree16(d, [&](int l) {
+      double wl = (S[tsk(o + l)] / sscale + (-Z[tsk(o + l)]) / zscale) / wscale;
+      return l > 0 ? 0.0 + wl * wl : 0.0;
+    });
     double w0 = sqrt(1 + w1sq);
     double gamma = 0.5 * wscale;
     double c1 = (gamma + z0 / zscale) / sscale;
@@ -1808,8 +1829,7 @@ __global__ void k_soc_tile_mul_hs(ConeSet cs, double *y_, const double *__restri
   __syncthreads();
   if (t.valid) {
     const int o = t.off, d = t.dim;
-    double tt = 0;
-    for (int i = 0; i < d; ++i) tt += W[tsk(o + i)] * X[tsk(o + i)];
+    double tt = tree16(d, [&](int l) { return 0.0 + W[tsk(o + l)] * X[tsk(o + l)]; });
     double c = 2 * tt;
     double eta = cs.soc_eta[t.c], e2 = eta * eta;
     for (int i = 0; i < d; ++i) {
@@ -1831,8 +1851,10 @@ __global__ void k_soc_tile_affine_ds(ConeSet cs, double *ds_) {
   __syncthreads();
   if (t.valid) {
     const int o = t.off, d = t.dim;
-    double tt = 0;
-    for (int i = 0; i < d; ++i) tt += L[tsk(o + i)] * L[tsk(o + i)];
+    double tt = tree16(d, [&](int l) {
+      double ll = L[tsk(o + l)];
+      return 0.0 + ll * ll;
+    });
     double l0 = L[tsk(o)];
     for (int i = 1; i < d; ++i) {
       double li = L[tsk(o + i)];
@@ -1858,24 +1880,23 @@ __global__ void k_soc_tile_combined(ConeSet cs, double *shift_, const double *__
   if (t.valid) {
     const int o = t.off, d = t.dim;
     double eta = cs.soc_eta[t.c], w0 = W[tsk(o)];
-    double zz = 0, zs = 0;
-    for (int i = 1; i < d; ++i) {
-      double wi = W[tsk(o + i)];
-      zz += wi * DZ[tsk(o + i)];
-      zs += wi * DS[tsk(o + i)];
-    }
+    double zz = tree16(d, [&](int l) {
+      return l > 0 ? 0.0 + W[tsk(o + l)] * DZ[tsk(o + l)] : 0.0;
+    });
+    double zs = tree16(d, [&](int l) {
+      return l > 0 ? 0.0 + W[tsk(o + l)] * DS[tsk(o + l)] : 0.0;
+    });
     double dz0 = DZ[tsk(o)], ds0 = DS[tsk(o)];
     double cz = dz0 + zz / (1 + w0);
     double csn = -ds0 + zs / (1 + w0);
     double wz0 = eta * (w0 * dz0 + zz);
     double ws0 = (1 / eta) * (w0 * ds0 - zs);
-    double dot = wz0 * ws0;
-    for (int i = 1; i < d; ++i) {
-      double wi = W[tsk(o + i)];
-      double a = eta * (DZ[tsk(o + i)] + cz * wi);
-      double b = (1 / eta) * (DS[tsk(o + i)] + csn * wi);
-      dot += a * b;
-    }
+    double dot = tree16(d, [&](int l) {
+      double wl = W[tsk(o + l)];
+      double a = (l == 0) ? wz0 : eta * (DZ[tsk(o + l)] + cz * wl);
+      double b = (l == 0) ? ws0 : (1 / eta) * (DS[tsk(o + l)] + csn * wl);
+      return 0.0 + a * b;
+    });
     for (int i = 1; i < d; ++i) {
       double wi = W[tsk(o + i)];
       double a = eta * (DZ[tsk(o + i)] + cz * wi);
@@ -1903,13 +1924,16 @@ __global__ void k_soc_tile_ds_offset(ConeSet cs, double *out_, const double *__r
   __syncthreads();
   if (t.valid) {
     const int o = t.off, d = t.dim;
-    double z1sq = 0, l1ds1 = 0, w1ds1 = 0;
-    for (int i = 1; i < d; ++i) {
-      double zi = Z[tsk(o + i)], dsi = DS[tsk(o + i)];
-      z1sq += zi * zi;
-      l1ds1 += L[tsk(o + i)] * dsi;
-      w1ds1 += W[tsk(o + i)] * dsi;
-    }
+    double z1sq = tree16(d, [&](int l) {
+      double zl = Z[tsk(o + l)];
+      return l > 0 ? 0.0 + zl * zl : 0.0;
+    });
+    double l1ds1 = tree16(d, [&](int l) {
+      return l > 0 ? 0.0 + L[tsk(o + l)] * DS[tsk(o + l)] : 0.0;
+    });
+    double w1ds1 = tree16(d, [&](int l) {
+      return l > 0 ? 0.0 + W[tsk(o + l)] * DS[tsk(o + l)] : 0.0;
+    });
     double z0 = Z[tsk(o)], l0 = L[tsk(o)], w0 = W[tsk(o)];
     double resz = soc_res(z0, z1sq);
     double eta = cs.soc_eta[t.c];
@@ -1933,13 +1957,17 @@ __global__ void k_soc_tile_ds_offset(ConeSet cs, double *out_, const double *__r
 __device__ double soc_tile_step_component(const double *X, const double *Y, int o, int d,
                                           double amax) {
   double x0 = X[tsk(o)], y0 = Y[tsk(o)];
-  double ysq = 0, xsq = 0, xy = 0;
-  for (int i = 1; i < d; ++i) {
-    double xi = X[tsk(o + i)], yi = Y[tsk(o + i)];
-    ysq += yi * yi;
-    xsq += xi * xi;
-    xy += xi * yi;
-  }
+  double ysq = tree16(d, [&](int l) {
+    double yl = Y[tsk(o + l)];
+    return l > 0 ? 0.0 + yl * yl : 0.0;
+  });
+  double xsq = tree16(d, [&](int l) {
+    double xl = X[tsk(o + l)];
+    return l > 0 ? 0.0 + xl * xl : 0.0;
+  });
+  double xy = tree16(d, [&](int l) {
+    return l > 0 ? 0.0 + X[tsk(o + l)] * Y[tsk(o + l)] : 0.0;
+  });
   if (x0 >= 0 && y0 < 0) amax = fmin(amax, -x0 / y0);
   double a = soc_res(y0, ysq);
   double b = 2 * (x0 * y0 - xy);
