@@ -47,9 +47,13 @@ struct ConeSet {
   const int *soc_dim;   // [n_soc]
   const int *soc_inst;  // [n_soc]
   const int *soc_sparse;// [n_soc] 1 if dim > soc_threshold
-  int soc_ntiles;       // shared-memory tiles of consecutive small cones
-  int soc_skip_small;   // lane-group kernels leave tiled cones alone
-  const int *soc_tile;  // [2*soc_ntiles] first and one-past-last cone of each
+  // shared-memory tiles of consecutive cones, [c0, c1) pairs: soc_tile over
+  // cones of dim 1..16 (update_scaling), soc_tile_mid over dim 9..16 (the
+  // other per-iteration operations; smaller cones fill their lane groups)
+  int soc_ntiles, soc_ntiles_mid;
+  const int *soc_tile, *soc_tile_mid;
+  int soc_outside_mid;  // some cone has dim < 9 or > 16
+  int soc_skip_lo, soc_skip_hi;  // lane-group kernels leave these dims alone
   // exponential / power cones (3 rows each, contiguous)
   int n_exp, exp_begin;
   int n_pow, pow_begin;

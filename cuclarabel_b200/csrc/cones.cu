@@ -20,6 +20,7 @@
 //     (Cholesky, one-sided Jacobi SVD, Jacobi eigenvalues, small GEMMs).  The
 //     t x t Hs block is never stored: the KKT refresh evaluates the symmetric
 //     Kronecker product entries from R R^T on the fly.
+#include <algorithm>
 #include <cstdio>
 
 #include "cones.cuh"
@@ -69,7 +70,7 @@ struct SocCtx {
     dim = cs.soc_dim[c];
     inst = cs.soc_inst[c];
     if (valid && !active_inst(cs, inst)) valid = false;
-    if (valid && cs.soc_skip_small && dim <= kSocTileMaxDim) valid = false;
+    if (valid && dim >= cs.soc_skip_lo && dim <= cs.soc_skip_hi) valid = false;
   }
 };
 #define SOC_FOR(i) for (int i = ctx.lane; i < ctx.dim; i += G)
@@ -1247,7 +1248,10 @@ __global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
       inst = -1;
     }
   }
-  block_seg_min_nonneg(alpha, inst, a);
+  if (cs.B == 1)
+    block_seg_min_nonneg(alpha, inst, a);  // one problem: one atomic per block
+  else
+    seg_atomic_min_nonneg(alpha, inst, a);  // short per-instance segments
 }
 
 // coneops_socone.jl:745-814 with group reductions
@@ -1280,7 +1284,10 @@ __global__ void k_soc_step(ConeSet cs, const double *__restrict__ dz,
   double amax = alpha[ctx.inst];  // upper bound already there (atomic min target)
   double az = soc_step_component<G>(z + ctx.off, dz + ctx.off, amax, ctx);
   double as = soc_step_component<G>(s + ctx.off, ds + ctx.off, amax, ctx);
-  block_seg_min_nonneg(alpha, (ctx.valid && ctx.lane == 0) ? ctx.inst : -1, fmin(az, as));
+  if (cs.B == 1)
+    block_seg_min_nonneg(alpha, (ctx.valid && ctx.lane == 0) ? ctx.inst : -1, fmin(az, as));
+  else if (ctx.valid && ctx.lane == 0)
+    atomic_min_nonneg(alpha + ctx.inst, fmin(az, as));
 }
 __global__ void k_psd_step(ConeSet cs, const double *__restrict__ dz,
                            const double *__restrict__ ds, double *alpha) {
@@ -1346,7 +1353,10 @@ __global__ void k_nonsym_step(ConeSet cs, NonsymArgs<Ops> a, const double *__res
       res = fmin(res, al);
     }
   }
-  block_seg_min_nonneg(alpha, inst, res);
+  if (cs.B == 1)
+    block_seg_min_nonneg(alpha, inst, res);
+  else if (inst >= 0)
+    atomic_min_nonneg(alpha + inst, res);
 }
 
 // ================================================================ barrier
@@ -1691,11 +1701,12 @@ __device__ __forceinline__ double *tile_arr(int a) {
   extern __shared__ __align__(16) double tile_smem[];
   return tile_smem + (size_t)a * kTileWords;
 }
-__device__ __forceinline__ SocTileCtx soc_tile_ctx(const ConeSet &cs, int narr) {
+__device__ __forceinline__ SocTileCtx soc_tile_ctx(const ConeSet &cs, const int *tiles,
+                                                   int narr) {
   SocTileCtx t;
   int b = blockIdx.x;
-  t.c0 = cs.soc_tile[2 * b];
-  int c1 = cs.soc_tile[2 * b + 1];
+  t.c0 = tiles[2 * b];
+  int c1 = tiles[2 * b + 1];
   t.nc = c1 - t.c0;
   t.r0 = cs.soc_off[t.c0];
   t.nrows = cs.soc_off[c1 - 1] + cs.soc_dim[c1 - 1] - t.r0;
@@ -1726,9 +1737,9 @@ __device__ __forceinline__ void tile_store(double *dst, const double *src, int n
 // update_scaling! for tiled cones (coneops_socone.jl:372-451; sparse d/u/v of
 // coneops_socone_gpu.jl:338-470).  w and lambda overwrite the staged s and z
 // rows in place (each thread only reads its own rows).
-__global__ void k_soc_tile_update_scaling(ConeSet cs, const double *__restrict__ s_,
+__global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, const double *__restrict__ s_,
                                           const double *__restrict__ z_, int *scale_ok) {
-  SocTileCtx t = soc_tile_ctx(cs, 4);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, 4);
   double *S = tile_arr(0), *Z = tile_arr(1), *U = tile_arr(2), *V = tile_arr(3);
   tile_load(S, s_ + t.r0, t.nrows);
   tile_load(Z, z_ + t.r0, t.nrows);
@@ -1820,32 +1831,9 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const double *__restrict__
   }
 }
 
-// mul_Hs for tiled cones: y = eta^2 (J x + 2 (w'x) w), J = diag(-1, 1, ...)
-__global__ void k_soc_tile_mul_hs(ConeSet cs, double *y_, const double *__restrict__ x_) {
-  SocTileCtx t = soc_tile_ctx(cs, 2);
-  double *W = tile_arr(0), *X = tile_arr(1);
-  tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
-  tile_load(X, x_ + t.r0, t.nrows);
-  __syncthreads();
-  if (t.valid) {
-    const int o = t.off, d = t.dim;
-    double tt = tree16(d, [&](int l) { return 0.0 + W[tsk(o + l)] * X[tsk(o + l)]; });
-    double c = 2 * tt;
-    double eta = cs.soc_eta[t.c], e2 = eta * eta;
-    for (int i = 0; i < d; ++i) {
-      double xi = X[tsk(o + i)];
-      double v = (i == 0) ? -xi : xi;
-      X[tsk(o + i)] = (v + c * W[tsk(o + i)]) * e2;
-    }
-    t.ok[t.k] = 1;
-  }
-  __syncthreads();
-  tile_store(y_ + t.r0, X, t.nrows, t);
-}
-
 // affine_ds! for tiled cones: ds = lambda o lambda
-__global__ void k_soc_tile_affine_ds(ConeSet cs, double *ds_) {
-  SocTileCtx t = soc_tile_ctx(cs, 1);
+__global__ void k_soc_tile_affine_ds(ConeSet cs, const int *tiles, double *ds_) {
+  SocTileCtx t = soc_tile_ctx(cs, tiles, 1);
   double *L = tile_arr(0);
   tile_load(L, cs.soc_lambda + (t.r0 - cs.soc_begin), t.nrows);
   __syncthreads();
@@ -1869,9 +1857,9 @@ __global__ void k_soc_tile_affine_ds(ConeSet cs, double *ds_) {
 
 // combined_ds_shift! for tiled cones (coneops_defaults.jl:335-368): the
 // shift overwrites the staged dz rows in place.
-__global__ void k_soc_tile_combined(ConeSet cs, double *shift_, const double *__restrict__ dz_,
+__global__ void k_soc_tile_combined(ConeSet cs, const int *tiles, double *shift_, const double *__restrict__ dz_,
                                     const double *__restrict__ ds_, const double *sm) {
-  SocTileCtx t = soc_tile_ctx(cs, 3);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, 3);
   double *W = tile_arr(0), *DZ = tile_arr(1), *DS = tile_arr(2);
   tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
   tile_load(DZ, dz_ + t.r0, t.nrows);
@@ -1912,9 +1900,9 @@ __global__ void k_soc_tile_combined(ConeSet cs, double *shift_, const double *__
 
 // Δs_from_Δz_offset! for tiled cones (coneops_socone.jl:539-566): the output
 // overwrites the staged ds rows in place.
-__global__ void k_soc_tile_ds_offset(ConeSet cs, double *out_, const double *__restrict__ ds_,
+__global__ void k_soc_tile_ds_offset(ConeSet cs, const int *tiles, double *out_, const double *__restrict__ ds_,
                                      const double *__restrict__ z_) {
-  SocTileCtx t = soc_tile_ctx(cs, 4);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, 4);
   double *W = tile_arr(0), *L = tile_arr(1), *DS = tile_arr(2), *Z = tile_arr(3);
   const int r = t.r0 - cs.soc_begin;
   tile_load(W, cs.soc_w + r, t.nrows);
@@ -1982,10 +1970,10 @@ __device__ double soc_tile_step_component(const double *X, const double *Y, int 
   r2 = r2 < 0 ? kDMax : r2;
   return fmin(amax, fmin(r1, r2));
 }
-__global__ void k_soc_tile_step(ConeSet cs, const double *__restrict__ dz_,
+__global__ void k_soc_tile_step(ConeSet cs, const int *tiles, const double *__restrict__ dz_,
                                 const double *__restrict__ ds_, const double *__restrict__ z_,
                                 const double *__restrict__ s_, double *alpha) {
-  SocTileCtx t = soc_tile_ctx(cs, 4);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, 4);
   double *DZ = tile_arr(0), *DS = tile_arr(1), *Z = tile_arr(2), *S = tile_arr(3);
   tile_load(DZ, dz_ + t.r0, t.nrows);
   tile_load(DS, ds_ + t.r0, t.nrows);
@@ -2002,16 +1990,18 @@ __global__ void k_soc_tile_step(ConeSet cs, const double *__restrict__ dz_,
   block_seg_min_nonneg(alpha, t.valid ? t.inst : -1, a);
 }
 
-std::vector<int> soc_tiles(const int *off, const int *dim, int n) {
+std::vector<int> soc_tiles(const int *off, const int *dim, int n, int lo, int hi) {
   std::vector<int> t;
+  lo = std::max(lo, 1);
+  hi = std::min(hi, kSocTileMaxDim);
   int k = 0;
   while (k < n) {
-    if (dim[k] > kSocTileMaxDim || dim[k] < 1) {
+    if (dim[k] > hi || dim[k] < lo) {
       ++k;
       continue;
     }
     int start = k, rows = 0;
-    while (k < n && dim[k] >= 1 && dim[k] <= kSocTileMaxDim && k - start < kSocTileCones &&
+    while (k < n && dim[k] >= lo && dim[k] <= hi && k - start < kSocTileCones &&
            rows + dim[k] <= kSocTileRows && (k == start || off[k] == off[k - 1] + dim[k - 1])) {
       rows += dim[k];
       ++k;
@@ -2047,15 +2037,25 @@ static inline size_t soc_tile_smem(int narr) {
   return (size_t)narr * kTileWords * sizeof(double) + kSocTileRows * sizeof(unsigned short) +
          kSocTileCones;
 }
-#define LAUNCH_SOC_TILED(TILE_KERNEL, NARR, GROUP_KERNEL, ...)                         \
+// ALL: tiles over every cone of dim <= 16 (update_scaling); otherwise tiles
+// over dims 9..16.  The lane-group kernel takes the remaining cones.
+#define LAUNCH_SOC_TILED(ALL, TILE_KERNEL, NARR, GROUP_KERNEL, ...)                    \
   do {                                                                                 \
-    if (cs.soc_ntiles > 0)                                                             \
-      TILE_KERNEL<<<cs.soc_ntiles, kSocTileCones, soc_tile_smem(NARR), st>>>(          \
-          cs, __VA_ARGS__);                                                            \
-    if (cs.n_soc > 0 && cs.soc_group == 32) {                                          \
-      ConeSet csl = cs;                                                                \
-      csl.soc_skip_small = 1;                                                          \
-      LAUNCH_SOC(GROUP_KERNEL, csl, __VA_ARGS__);                                      \
+    if (cs.n_soc > 0) {                                                                \
+      const int _nt = (ALL) ? cs.soc_ntiles : cs.soc_ntiles_mid;                       \
+      const int *_tl = (ALL) ? cs.soc_tile : cs.soc_tile_mid;                          \
+      if (_nt > 0)                                                                     \
+        TILE_KERNEL<<<_nt, kSocTileCones, soc_tile_smem(NARR), st>>>(cs, _tl,          \
+                                                                      __VA_ARGS__);    \
+      bool _rest = (ALL) ? cs.soc_group == 32 : (_nt == 0 || cs.soc_outside_mid != 0); \
+      if (_rest) {                                                                     \
+        ConeSet csl = cs;                                                              \
+        if (_nt > 0) {                                                                 \
+          csl.soc_skip_lo = (ALL) ? 1 : kSocTileMidDim;                                \
+          csl.soc_skip_hi = kSocTileMaxDim;                                            \
+        }                                                                              \
+        LAUNCH_SOC(GROUP_KERNEL, csl, __VA_ARGS__);                                    \
+      }                                                                                \
     }                                                                                  \
   } while (0)
 
@@ -2088,7 +2088,7 @@ void cones_update_scaling(const ConeSet &cs, const double *s, const double *z,
                           const double *mu, const int *scaling, int *scale_ok,
                           cudaStream_t st) {
   if (cs.n_nn) k_nn_update_scaling<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, s, z);
-  LAUNCH_SOC_TILED(k_soc_tile_update_scaling, 4, k_soc_update_scaling, s, z, scale_ok);
+  LAUNCH_SOC_TILED(true, k_soc_tile_update_scaling, 4, k_soc_update_scaling, s, z, scale_ok);
   if (cs.n_exp)
     k_nonsym_update_scaling<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
         cs, exp_args(cs), s, z, mu, scaling);
@@ -2126,7 +2126,7 @@ void cones_get_Hs(const ConeSet &cs, const int *nn_blk, const int *soc_blk,
 void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, y);
   if (cs.n_nn) k_nn_mul_hs<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, y, x);
-  LAUNCH_SOC_TILED(k_soc_tile_mul_hs, 2, k_soc_mul_hs, y, x);
+  LAUNCH_SOC(k_soc_mul_hs, cs, y, x);
   if (cs.n_exp)
     k_nonsym_mul_hs<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                             cs.exp_inst, cs.exp_Hs, y, x);
@@ -2139,7 +2139,7 @@ void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st
 void cones_affine_ds(const ConeSet &cs, double *ds, const double *s, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, ds);
   if (cs.n_nn) k_nn_affine_ds<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, ds);
-  LAUNCH_SOC_TILED(k_soc_tile_affine_ds, 1, k_soc_affine_ds, ds);
+  LAUNCH_SOC_TILED(false, k_soc_tile_affine_ds, 1, k_soc_affine_ds, ds);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                               cs.exp_inst, ds, s);
@@ -2153,7 +2153,7 @@ void cones_combined_ds_shift(const ConeSet &cs, double *shift, const double *dz,
                              const double *ds, const double *sm, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, shift);
   if (cs.n_nn) k_nn_combined<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, shift, dz, ds, sm);
-  LAUNCH_SOC_TILED(k_soc_tile_combined, 3, k_soc_combined, shift, dz, ds, sm);
+  LAUNCH_SOC_TILED(false, k_soc_tile_combined, 3, k_soc_combined, shift, dz, ds, sm);
   if (cs.n_exp)
     k_nonsym_combined<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
         cs, exp_args(cs), shift, dz, ds, sm);
@@ -2167,7 +2167,7 @@ void cones_ds_from_dz_offset(const ConeSet &cs, double *out, const double *ds,
                              const double *z, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, out);
   if (cs.n_nn) k_nn_ds_offset<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, out, ds, z);
-  LAUNCH_SOC_TILED(k_soc_tile_ds_offset, 4, k_soc_ds_offset, out, ds, z);
+  LAUNCH_SOC_TILED(false, k_soc_tile_ds_offset, 4, k_soc_ds_offset, out, ds, z);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                               cs.exp_inst, out, ds);
@@ -2181,7 +2181,7 @@ void cones_step_length_sym(const ConeSet &cs, const double *dz, const double *ds
                            const double *z, const double *s, double *alpha,
                            cudaStream_t st) {
   if (cs.n_nn) k_nn_step<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, dz, ds, z, s, alpha);
-  LAUNCH_SOC_TILED(k_soc_tile_step, 4, k_soc_step, dz, ds, z, s, alpha);
+  LAUNCH_SOC_TILED(false, k_soc_tile_step, 4, k_soc_step, dz, ds, z, s, alpha);
   LAUNCH_PSD(k_psd_step, 4, cs, dz, ds, alpha);
 }
 

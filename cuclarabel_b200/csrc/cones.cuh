@@ -11,19 +11,23 @@
 
 namespace clgpu {
 
-// Second-order cones of dimension <= kSocTileMaxDim are processed in tiles by
-// the per-iteration kernels (update_scaling, mul_Hs, affine_ds,
-// combined_ds_shift, ds_from_dz_offset, step_length): a tile is a run of
-// consecutive cones with contiguous rows, at most kSocTileCones cones and
-// kSocTileRows rows, staged through shared memory with coalesced loads and
-// stores, one thread per cone.  Larger cones keep the lane-group kernels.
-// A cone's arithmetic depends only on its own dimension either way, so an
-// instance computes the same bits alone or in any batch.
+// Second-order cones are processed in shared-memory tiles by some
+// per-iteration kernels: a tile is a run of consecutive cones with contiguous
+// rows, at most kSocTileCones cones and kSocTileRows rows, staged with
+// coalesced loads and stores, one thread per cone.  update_scaling tiles
+// every cone of dim <= kSocTileMaxDim; affine_ds, combined_ds_shift,
+// ds_from_dz_offset and step_length tile dims kSocTileMidDim..kSocTileMaxDim
+// (smaller cones keep most lanes of their lane groups busy); mul_Hs and the
+// rest use lane groups.  Which kernel handles a cone depends only on the
+// cone's own dimension, so an instance computes the same bits alone or in
+// any batch.
 constexpr int kSocTileMaxDim = 16;
+constexpr int kSocTileMidDim = 9;
 constexpr int kSocTileCones = 128;
 constexpr int kSocTileRows = 1024;
-// Tile list [c0, c1, c0, c1, ...] over n cones (rows off[k] .. off[k]+dim[k]).
-std::vector<int> soc_tiles(const int *off, const int *dim, int n);
+// Tile list [c0, c1, c0, c1, ...] over the cones of dim in [lo, hi] among n
+// cones (rows off[k] .. off[k]+dim[k]).
+std::vector<int> soc_tiles(const int *off, const int *dim, int n, int lo, int hi);
 
 // update_scaling!  (coneops_compositecone_gpu.jl:185).  mu/scaling are
 // per-instance device arrays; scale_ok[i] is cleared to 0 on failure.

@@ -144,10 +144,19 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
   cs.soc_inst = A.upload(soc_inst);
   cs.soc_sparse = A.upload(soc_sparse);
   {
-    std::vector<int> tiles = soc_tiles(soc_off.data(), soc_dim.data(), (int)soc_off.size());
+    const int nsc = (int)soc_off.size();
+    std::vector<int> tiles = soc_tiles(soc_off.data(), soc_dim.data(), nsc, 1, kSocTileMaxDim);
+    std::vector<int> mid =
+        soc_tiles(soc_off.data(), soc_dim.data(), nsc, kSocTileMidDim, kSocTileMaxDim);
     cs.soc_ntiles = (int)tiles.size() / 2;
     cs.soc_tile = A.upload(tiles);
-    cs.soc_skip_small = 0;
+    cs.soc_ntiles_mid = (int)mid.size() / 2;
+    cs.soc_tile_mid = A.upload(mid);
+    cs.soc_outside_mid = 0;
+    for (int k = 0; k < nsc; ++k)
+      if (soc_dim[k] < kSocTileMidDim || soc_dim[k] > kSocTileMaxDim) cs.soc_outside_mid = 1;
+    cs.soc_skip_lo = 1;
+    cs.soc_skip_hi = 0;  // empty range: lane-group kernels take every cone
   }
   cs.exp_inst = A.upload(exp_inst);
   cs.pow_inst = A.upload(pow_inst);

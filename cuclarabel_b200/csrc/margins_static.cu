@@ -116,6 +116,8 @@ extern "C" int clgpu_margins_static(int ncones, const int *types, const int *dim
   int *ints = reinterpret_cast<int *>(base + kDblWords);
   ConeSet cs{};
   cs.B = 1;
+  cs.soc_skip_lo = 1;  // empty skip range: the lane-group kernels take every cone
+  cs.soc_skip_hi = 0;
   cs.m_total = row;
   cs.nn_begin = nn_begin < 0 ? 0 : nn_begin;
   cs.n_nn = n_nn;
