@@ -642,10 +642,11 @@ def main():
         pinned.append(t)
     Pp_, qp_, Ap_, bp_ = [t.numpy() for t in pinned]
     s2 = BatchSolver(pbs, direct_solve_method=args.method)  # setup outside the timed region
+    res_buf = None
     for _ in range(2):
         s2.update_data(P=Pp_, q=qp_, A=Ap_, b=bp_, stream=sh)
         s2.solve_only(sh)
-        s2.results()
+        res_buf = s2.results(res_buf)  # result arrays allocated once, then refilled
     e2e_steps = max(1, args.steps)
     e2e_t = 0.0
     e2e_solved = 0
@@ -657,7 +658,7 @@ def main():
         t0 = time.perf_counter()
         s2.update_data(P=Pp_, q=qp_, A=Ap_, b=bp_, stream=sh)
         s2.solve_only(sh)
-        res = s2.results()
+        res = s2.results(res_buf)
         e2e_t += time.perf_counter() - t0
         e2e_solved += int(np.sum(res["status"] == int(SolverStatus.SOLVED)))
     h2d = 8 * (len(Pv) + len(qv) + len(Av) + len(bv))

@@ -408,16 +408,25 @@ class BatchSolver:
             raise RuntimeError("clgpu_solver_solve failed with code %d" % rc)
         return self.solutions()
 
-    def results(self):
+    def results(self, out=None):
         """The last solve's results as arrays (no per-instance objects): x, s,
         z concatenated over instances (offsets xoff / moff) and a structured
-        array of the DefaultInfo fields, one row per instance."""
+        array of the DefaultInfo fields, one row per instance.  `out` may be
+        a previous return value of results(): its arrays are filled in place
+        (no new host allocation for repeated solves)."""
         L = _lib.load()
         B = len(self.dims)
-        x = np.empty(max(self.nx, 1))
-        s = np.empty(max(self.mz, 1))
-        z = np.empty(max(self.mz, 1))
-        infos = (_lib.ClgpuInfo * B)()
+        if out is not None:
+            x, s, z = out["x"], out["s"], out["z"]
+            for a, n in ((x, self.nx), (s, self.mz), (z, self.mz)):
+                if a.dtype != np.float64 or not a.flags.c_contiguous or len(a) < n:
+                    raise ValueError("results(out=...): arrays of the last results() needed")
+            infos = out["_infos"]
+        else:
+            x = np.empty(max(self.nx, 1))
+            s = np.empty(max(self.mz, 1))
+            z = np.empty(max(self.mz, 1))
+            infos = (_lib.ClgpuInfo * B)()
         rc = L.clgpu_solver_get_solutions(self._h, x.ctypes.data_as(_lib.dp),
                                           s.ctypes.data_as(_lib.dp), z.ctypes.data_as(_lib.dp),
                                           infos)
@@ -425,7 +434,7 @@ class BatchSolver:
             raise RuntimeError("clgpu_solver_get_solutions failed with code %d" % rc)
         info = np.ctypeslib.as_array(infos)
         return {"x": x[:self.nx], "s": s[:self.mz], "z": z[:self.mz], "info": info,
-                "status": info["status"].copy()}
+                "status": info["status"].copy(), "_infos": infos}
 
     def solutions(self):
         L = _lib.load()

@@ -814,7 +814,7 @@ struct clgpu_solver {
   std::vector<int> h_n, h_m, h_xoff, h_moff;
   bool any_asym = false, any_sym = false;
   std::vector<clgpu_info> info;
-  std::vector<double> sol;  // host copy of x, s, z (concatenated)
+  double *h_sol = nullptr;  // pinned host copy of x, s, z (concatenated), nx + 2*mz
   bool solved = false;
   long long launches = 0;
   bool profiling = false;
@@ -882,6 +882,7 @@ struct clgpu_solver {
       if (p) cudaFreeHost(p);
     if (h_info) cudaFreeHost(h_info);
     if (h_stage) cudaFreeHost(h_stage);
+    if (h_sol) cudaFreeHost(h_sol);
     for (auto e : ev_pool) cudaEventDestroy(e);
   }
   int next_event() {
@@ -2009,6 +2010,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   cudaMallocHost(&h->h_list_act, (size_t)B * sizeof(int));
   cudaMallocHost(&h->h_info, (size_t)B * (NUM_SCALARS + NUM_INTS) * sizeof(double));
   cudaMallocHost(&h->h_stage, ((size_t)nx + (size_t)mz) * sizeof(double));
+  cudaMallocHost(&h->h_sol, ((size_t)nx + 2 * (size_t)mz) * sizeof(double));
   h->slot_state.assign(B, 0);
   h->slot_t0.assign(B, std::chrono::steady_clock::now());
   if (A.err != cudaSuccess) return -1000 - (int)A.err;
@@ -2448,13 +2450,16 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
   h->last_ms = ms;
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  // copy results back
-  std::vector<double> S((size_t)NUM_SCALARS * B);
-  std::vector<int> I((size_t)NUM_INTS * B);
-  cudaMemcpy(S.data(), dv.S, S.size() * sizeof(double), cudaMemcpyDeviceToHost);
-  cudaMemcpy(I.data(), dv.I, I.size() * sizeof(int), cudaMemcpyDeviceToHost);
-  h->sol.resize((size_t)dv.nx + 2 * (size_t)dv.mz);
-  cudaMemcpy(h->sol.data(), h->d_out, h->sol.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  // copy results back into pinned staging (the info scalars reuse the
+  // serving info buffer: a solve ends serving)
+  double *S = h->h_info;
+  int *I = reinterpret_cast<int *>(h->h_info + (size_t)NUM_SCALARS * B);
+  cudaMemcpyAsync(S, dv.S, (size_t)NUM_SCALARS * B * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(I, dv.I, (size_t)NUM_INTS * B * sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(h->h_sol, h->d_out, ((size_t)dv.nx + 2 * (size_t)dv.mz) * sizeof(double),
+                  cudaMemcpyDeviceToHost, st);
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return -1000 - (int)e;
   double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   for (int i = 0; i < B; ++i)
     fill_info(
@@ -2685,7 +2690,7 @@ extern "C" int clgpu_solver_get_info(clgpu_solver *h, int inst, clgpu_info *info
 extern "C" int clgpu_solver_get_solution(clgpu_solver *h, int inst, double *x, double *s,
                                          double *z) {
   if (!h || inst < 0 || inst >= h->B || !h->solved) return -1;
-  const double *ox = h->sol.data(), *os = ox + h->nx, *oz = os + h->mz;
+  const double *ox = h->h_sol, *os = ox + h->nx, *oz = os + h->mz;
   int n = h->h_n[inst], m = h->h_m[inst];
   if (x) std::memcpy(x, ox + h->h_xoff[inst], n * sizeof(double));
   if (s) std::memcpy(s, os + h->h_moff[inst], m * sizeof(double));
@@ -2696,10 +2701,33 @@ extern "C" int clgpu_solver_get_solution(clgpu_solver *h, int inst, double *x, d
 extern "C" int clgpu_solver_get_solutions(clgpu_solver *h, double *x, double *s, double *z,
                                           clgpu_info *info) {
   if (!h || !h->solved) return -1;
-  const double *ox = h->sol.data(), *os = ox + h->nx, *oz = os + h->mz;
-  if (x) std::memcpy(x, ox, h->nx * sizeof(double));
-  if (s) std::memcpy(s, os, h->mz * sizeof(double));
-  if (z) std::memcpy(z, oz, h->mz * sizeof(double));
+  const double *ox = h->h_sol, *os = ox + h->nx, *oz = os + h->mz;
+  // large batches: the three copies split over a few host threads
+  struct Part {
+    double *dst;
+    const double *src;
+    size_t n;
+  };
+  std::vector<Part> parts;
+  const size_t chunk = (size_t)1 << 18;  // 2 MB
+  for (auto pr : {Part{x, ox, (size_t)h->nx}, Part{s, os, (size_t)h->mz},
+                  Part{z, oz, (size_t)h->mz}})
+    if (pr.dst)
+      for (size_t o = 0; o < pr.n; o += chunk)
+        parts.push_back({pr.dst + o, pr.src + o, std::min(chunk, pr.n - o)});
+  const int np = (int)parts.size(), nth = std::min(8, np);
+  if (nth <= 1) {
+    for (auto &pr : parts) std::memcpy(pr.dst, pr.src, pr.n * sizeof(double));
+  } else {
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; ++t)
+      th.emplace_back([&]() {
+        for (int k; (k = next.fetch_add(1)) < np;)
+          std::memcpy(parts[k].dst, parts[k].src, parts[k].n * sizeof(double));
+      });
+    for (auto &t : th) t.join();
+  }
   if (info) std::memcpy(info, h->info.data(), h->B * sizeof(clgpu_info));
   return 0;
 }

@@ -181,3 +181,20 @@ def test_repeat_solve_is_identical(cuda_device):
     b = s.solve()
     assert a.status == b.status and a.iterations == b.iterations
     assert rel_err(a.obj_val, b.obj_val) < 1e-12
+
+
+def test_results_refill_in_place_matches_fresh_arrays(cuda_device):
+    """results(out=...) refills the arrays of an earlier call with the same
+    values a fresh call returns."""
+    pbs = problems.mpc_batch(6, seed0=20)
+    solver = BatchSolver(pbs)
+    solver.solve_only()
+    buf = solver.results()
+    buf["x"][:] = np.nan
+    solver.solve_only()
+    fresh = solver.results()
+    again = solver.results(buf)
+    assert again["x"] is buf["x"]
+    for k in ("x", "s", "z", "status"):
+        assert np.array_equal(again[k], fresh[k])
+    assert np.array_equal(again["info"]["obj_val"], fresh["info"]["obj_val"])
