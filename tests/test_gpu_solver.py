@@ -194,7 +194,7 @@ def test_results_refill_in_place_matches_fresh_arrays(cuda_device):
     solver.solve_only()
     fresh = solver.results()
     again = solver.results(buf)
-    assert again["x"] is buf["x"]
+    assert np.shares_memory(again["x"], buf["x"])
     for k in ("x", "s", "z", "status"):
         assert np.array_equal(again[k], fresh[k])
     assert np.array_equal(again["info"]["obj_val"], fresh["info"]["obj_val"])
