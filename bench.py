@@ -530,6 +530,30 @@ def serve_run(solver, pbs, lam, seconds, seed, stream):
                    "serving config are not in this run)"}
 
 
+def plain_under_load(service_s, lam, seconds, seed):
+    """Response times of the plain one-at-a-time GPU path under the served
+    run's request stream: the same Poisson arrivals (same seed, rate and
+    length) into one FIFO server whose per-request service times cycle
+    through the plain path's measured per-solve latencies.  Arithmetic on
+    measured times, no GPU work: the plain path serves one request at a
+    time, so this is its latency under that load."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.poisson(lam * seconds))
+    arrive = np.sort(rng.uniform(0.0, seconds, n))
+    svc = np.resize(np.asarray(service_s, np.float64), n)
+    finish = np.empty(n)
+    t = 0.0
+    for i in range(n):
+        t = max(t, arrive[i]) + svc[i]
+        finish[i] = t
+    resp = finish - arrive
+    return {"requests": n, "p50_ms": 1000 * float(np.percentile(resp, 50)),
+            "p99_ms": 1000 * float(np.percentile(resp, 99)),
+            "value": n / float(finish[-1]) if n else 0.0, "unit": "solves/s",
+            "note": "FIFO queue of the plain path's measured per-solve times under the "
+                    "served run's arrivals (same seed, rate and length)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -697,7 +721,9 @@ def main():
         dt = time.perf_counter() - t0
         plain = {"value": nsol / dt, "unit": "solves/s", "sample": args.plain_sample,
                  "p50_ms": 1000 * float(np.percentile(lat, 50)),
-                 "p99_ms": 1000 * float(np.percentile(lat, 99)), "method": "cudss"}
+                 "p99_ms": 1000 * float(np.percentile(lat, 99)), "method": "cudss",
+                 "note": "per-solve latency back to back, no queue"}
+        plain_lat = lat
 
     # ---- served: continuous batching under a Poisson request stream
     served = None
@@ -707,6 +733,8 @@ def main():
         del srv
         if plain:
             served["vs_plain_solves"] = served["value"] / plain["value"]
+            served["plain_under_same_load"] = plain_under_load(
+                plain_lat, args.serve_rate, args.serve_seconds, 12345 + rank)
 
     # ---- roofline: the dominant device phase (an LDL kernel), plus the
     # update_scaling cone kernels for reference
