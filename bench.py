@@ -252,6 +252,10 @@ def cone_kernel_roofline(hbm, scale=1.0, reps=5, seed=7):
                 "step_length": lambda: L.clgpu_step_length(
                     h, P(dz), P(ds), P(z), P(s), 1.0, 0.99, 0.8, 1e-4, ctypes.byref(a_out), sh),
             }
+            nb, sv = ctypes.c_int(), (ctypes.c_int * 5)()
+            L.clgpu_cones_get_launch_shapes(h, ctypes.byref(nb), sv)
+            shapes = {"nn_block": nb.value,
+                      "soc": ["groups" if x == 0 else "tiles%d" % (32 << (x - 1)) for x in sv]}
             res = {}
             for op in CONE_OPS:
                 fn = calls[op]
@@ -272,7 +276,8 @@ def cone_kernel_roofline(hbm, scale=1.0, reps=5, seed=7):
                 gbs = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
                 res[op] = {"us": round(1000 * ms, 2), "bytes": int(by),
                            "GB/s": round(gbs, 1), "frac": round(gbs / hbm, 3)}
-            out[name] = {"cones": count, "dim": dim, "rows": m, "ops": res}
+            out[name] = {"cones": count, "dim": dim, "rows": m, "ops": res,
+                         "launch_shapes": shapes if code in (1, 2) else None}
             del s, z, dz, ds, x, y
         finally:
             L.clgpu_cones_destroy(h)
@@ -607,6 +612,7 @@ def main():
     sh = stream.cuda_stream
     solver = BatchSolver(pbs, direct_solve_method=args.method)
     dev_bytes = solver.device_bytes()
+    launch_shapes = solver.launch_shapes()  # chosen by the setup autotuner
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
 
     def flush_l2():
@@ -797,7 +803,7 @@ def main():
             "data": "synthetic (seeded PCG64, MPC batch shapes)",
             "config": dict(workload_config(B, args.method),
                            l2="flushed (256 MB write) between timed steps",
-                           device_bytes=dev_bytes),
+                           device_bytes=dev_bytes, launch_shapes=launch_shapes),
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "note": "update_data! of every value (P, q, A, b) from pinned host "

@@ -86,6 +86,8 @@ EXPORTED = [
     "clgpu_margins", "clgpu_scaled_unit_shift", "clgpu_unit_initialization",
     "clgpu_debug_check_instance", "clgpu_margins_static",
     "clgpu_cones_set_profiling", "clgpu_cones_last_kernel_ms",
+    "clgpu_cones_get_launch_shapes", "clgpu_cones_set_launch_shapes",
+    "clgpu_solver_get_launch_shapes",
 ]
 
 
@@ -117,6 +119,9 @@ def _declare(L):
     for f in ("clgpu_cones_numel", "clgpu_cones_degree", "clgpu_cones_hs_len"):
         getattr(L, f).argtypes = [c_void_p]
     L.clgpu_cones_set_profiling.argtypes = [c_void_p, c_int]
+    L.clgpu_cones_get_launch_shapes.argtypes = [c_void_p, ip, ip]
+    L.clgpu_cones_set_launch_shapes.argtypes = [c_void_p, c_int, ip]
+    L.clgpu_solver_get_launch_shapes.argtypes = [c_void_p, ip, ip]
     L.clgpu_cones_last_kernel_ms.argtypes = [c_void_p, dp]
     V = c_void_p  # device pointers are passed as integers
     L.clgpu_update_scaling.argtypes = [c_void_p, V, V, c_double, c_int, c_void_p]

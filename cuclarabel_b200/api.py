@@ -540,6 +540,21 @@ class BatchSolver:
     def launch_count(self):
         return _lib.load().clgpu_solver_launch_count(self._h)
 
+    SOC_OPS = ("update_scaling", "affine_ds", "combined_ds_shift", "ds_from_dz_offset",
+               "step_length")
+
+    def launch_shapes(self):
+        """Launch shapes the setup autotuner chose for this batch: threads per
+        block of the nonnegative kernels, and per SOC operation "groups" (one
+        lane group per cone) or "tiles<C>" (shared-memory tiles of C cones)."""
+        nb, v = ctypes.c_int(), (ctypes.c_int * 5)()
+        rc = _lib.load().clgpu_solver_get_launch_shapes(self._h, ctypes.byref(nb), v)
+        if rc != 0:
+            raise RuntimeError("clgpu_solver_get_launch_shapes failed with code %d" % rc)
+        return {"nn_block": nb.value,
+                "soc": {op: ("groups" if x == 0 else "tiles%d" % (32 << (x - 1)))
+                        for op, x in zip(self.SOC_OPS, v)}}
+
     def set_profiling(self, enable=True):
         _lib.load().clgpu_solver_set_profiling(self._h, 1 if enable else 0)
 

@@ -47,12 +47,14 @@ struct ConeSet {
   const int *soc_dim;   // [n_soc]
   const int *soc_inst;  // [n_soc]
   const int *soc_sparse;// [n_soc] 1 if dim > soc_threshold
-  // shared-memory tiles of consecutive cones, [c0, c1) pairs: soc_tile over
-  // cones of dim 1..16 (update_scaling), soc_tile_mid over dim 9..16 (the
-  // other per-iteration operations; smaller cones fill their lane groups)
-  int soc_ntiles, soc_ntiles_mid;
-  const int *soc_tile, *soc_tile_mid;
-  int soc_outside_mid;  // some cone has dim < 9 or > 16
+  // Launch shapes, chosen per cone set by cones_autotune: threads per block
+  // of the nonnegative kernels, and for each tiled SOC operation its
+  // variant, 0 = lane groups, v = 1..3 = shared-memory tiles of 32 << (v-1)
+  // cones (8 rows per cone) over the cones of dim <= 16.
+  int nn_block;
+  int soc_variant[5];
+  int soc_ntiles[4];         // tiles per shape v = 1..3 ([0] unused)
+  const int *soc_tile[4];    // [2*soc_ntiles[v]] first and one-past-last cone
   int soc_skip_lo, soc_skip_hi;  // lane-group kernels leave these dims alone
   // exponential / power cones (3 rows each, contiguous)
   int n_exp, exp_begin;

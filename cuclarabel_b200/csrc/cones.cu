@@ -1666,6 +1666,8 @@ __global__ void k_identity_cones(ConeSet cs) {
 // Shared rows are skewed by one word every 16 so that threads walking their
 // cones at a stride of 3..16 words meet few bank conflicts.
 __device__ __forceinline__ int tsk(int i) { return i + (i >> 4); }
+// words of one staged array for a tile of `rows` rows (skew included)
+__host__ __device__ __forceinline__ int tile_words(int rows) { return rows + rows / 16 + 1; }
 // Sum of a cone's per-element terms in the order of the lane-group kernels'
 // butterfly reduction (pairs at distance 8, 4, 2, 1 over 16 leaves, leaves
 // from the cone's dimension on are +0): for dim <= 16 this is the same
@@ -1686,32 +1688,33 @@ __device__ __forceinline__ double tree16(int d, F leaf) {
     for (int l = 0; l < o; ++l) p[l] = p[l] + p[l + o];
   return p[0];
 }
-static constexpr int kTileWords = kSocTileRows + kSocTileRows / 16 + 1;
-
 struct SocTileCtx {
   int c0, nc, r0, nrows;  // tile: cones [c0, c0+nc), global rows [r0, r0+nrows)
   int k, c, off, dim, inst;  // this thread's cone (k < nc) and its rows in the tile
   bool valid;
-  unsigned short *rcone;  // [kSocTileRows] local cone of each tile row
-  unsigned char *ok;      // [kSocTileCones] cone's rows are written back
+  int words;              // words of one staged array
+  unsigned short *rcone;  // [rows per tile] local cone of each tile row
+  unsigned char *ok;      // [cones per tile] cone's rows are written back
 };
 
-// Shared layout: `narr` staged arrays of kTileWords doubles, then rcone, ok.
-__device__ __forceinline__ double *tile_arr(int a) {
+// Shared layout: `narr` staged arrays of tile_words(rows) doubles, then
+// rcone, ok.
+__device__ __forceinline__ double *tile_arr(int a, int words) {
   extern __shared__ __align__(16) double tile_smem[];
-  return tile_smem + (size_t)a * kTileWords;
+  return tile_smem + (size_t)a * words;
 }
 __device__ __forceinline__ SocTileCtx soc_tile_ctx(const ConeSet &cs, const int *tiles,
-                                                   int narr) {
+                                                   int trows, int narr) {
   SocTileCtx t;
+  t.words = tile_words(trows);
   int b = blockIdx.x;
   t.c0 = tiles[2 * b];
   int c1 = tiles[2 * b + 1];
   t.nc = c1 - t.c0;
   t.r0 = cs.soc_off[t.c0];
   t.nrows = cs.soc_off[c1 - 1] + cs.soc_dim[c1 - 1] - t.r0;
-  t.rcone = reinterpret_cast<unsigned short *>(tile_arr(narr));
-  t.ok = reinterpret_cast<unsigned char *>(t.rcone + kSocTileRows);
+  t.rcone = reinterpret_cast<unsigned short *>(tile_arr(narr, t.words));
+  t.ok = reinterpret_cast<unsigned char *>(t.rcone + trows);
   t.k = threadIdx.x;
   t.valid = t.k < t.nc;
   t.c = t.valid ? t.c0 + t.k : t.c0;
@@ -1737,10 +1740,10 @@ __device__ __forceinline__ void tile_store(double *dst, const double *src, int n
 // update_scaling! for tiled cones (coneops_socone.jl:372-451; sparse d/u/v of
 // coneops_socone_gpu.jl:338-470).  w and lambda overwrite the staged s and z
 // rows in place (each thread only reads its own rows).
-__global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, const double *__restrict__ s_,
+__global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, int trows, const double *__restrict__ s_,
                                           const double *__restrict__ z_, int *scale_ok) {
-  SocTileCtx t = soc_tile_ctx(cs, tiles, 4);
-  double *S = tile_arr(0), *Z = tile_arr(1), *U = tile_arr(2), *V = tile_arr(3);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 4);
+  double *S = tile_arr(0, t.words), *Z = tile_arr(1, t.words), *U = tile_arr(2, t.words), *V = tile_arr(3, t.words);
   tile_load(S, s_ + t.r0, t.nrows);
   tile_load(Z, z_ + t.r0, t.nrows);
   __syncthreads();
@@ -1832,9 +1835,9 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, const do
 }
 
 // affine_ds! for tiled cones: ds = lambda o lambda
-__global__ void k_soc_tile_affine_ds(ConeSet cs, const int *tiles, double *ds_) {
-  SocTileCtx t = soc_tile_ctx(cs, tiles, 1);
-  double *L = tile_arr(0);
+__global__ void k_soc_tile_affine_ds(ConeSet cs, const int *tiles, int trows, double *ds_) {
+  SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 1);
+  double *L = tile_arr(0, t.words);
   tile_load(L, cs.soc_lambda + (t.r0 - cs.soc_begin), t.nrows);
   __syncthreads();
   if (t.valid) {
@@ -1857,10 +1860,10 @@ __global__ void k_soc_tile_affine_ds(ConeSet cs, const int *tiles, double *ds_) 
 
 // combined_ds_shift! for tiled cones (coneops_defaults.jl:335-368): the
 // shift overwrites the staged dz rows in place.
-__global__ void k_soc_tile_combined(ConeSet cs, const int *tiles, double *shift_, const double *__restrict__ dz_,
+__global__ void k_soc_tile_combined(ConeSet cs, const int *tiles, int trows, double *shift_, const double *__restrict__ dz_,
                                     const double *__restrict__ ds_, const double *sm) {
-  SocTileCtx t = soc_tile_ctx(cs, tiles, 3);
-  double *W = tile_arr(0), *DZ = tile_arr(1), *DS = tile_arr(2);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 3);
+  double *W = tile_arr(0, t.words), *DZ = tile_arr(1, t.words), *DS = tile_arr(2, t.words);
   tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
   tile_load(DZ, dz_ + t.r0, t.nrows);
   tile_load(DS, ds_ + t.r0, t.nrows);
@@ -1900,10 +1903,10 @@ __global__ void k_soc_tile_combined(ConeSet cs, const int *tiles, double *shift_
 
 // Δs_from_Δz_offset! for tiled cones (coneops_socone.jl:539-566): the output
 // overwrites the staged ds rows in place.
-__global__ void k_soc_tile_ds_offset(ConeSet cs, const int *tiles, double *out_, const double *__restrict__ ds_,
+__global__ void k_soc_tile_ds_offset(ConeSet cs, const int *tiles, int trows, double *out_, const double *__restrict__ ds_,
                                      const double *__restrict__ z_) {
-  SocTileCtx t = soc_tile_ctx(cs, tiles, 4);
-  double *W = tile_arr(0), *L = tile_arr(1), *DS = tile_arr(2), *Z = tile_arr(3);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 4);
+  double *W = tile_arr(0, t.words), *L = tile_arr(1, t.words), *DS = tile_arr(2, t.words), *Z = tile_arr(3, t.words);
   const int r = t.r0 - cs.soc_begin;
   tile_load(W, cs.soc_w + r, t.nrows);
   tile_load(L, cs.soc_lambda + r, t.nrows);
@@ -1970,11 +1973,11 @@ __device__ double soc_tile_step_component(const double *X, const double *Y, int 
   r2 = r2 < 0 ? kDMax : r2;
   return fmin(amax, fmin(r1, r2));
 }
-__global__ void k_soc_tile_step(ConeSet cs, const int *tiles, const double *__restrict__ dz_,
+__global__ void k_soc_tile_step(ConeSet cs, const int *tiles, int trows, const double *__restrict__ dz_,
                                 const double *__restrict__ ds_, const double *__restrict__ z_,
                                 const double *__restrict__ s_, double *alpha) {
-  SocTileCtx t = soc_tile_ctx(cs, tiles, 4);
-  double *DZ = tile_arr(0), *DS = tile_arr(1), *Z = tile_arr(2), *S = tile_arr(3);
+  SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 4);
+  double *DZ = tile_arr(0, t.words), *DS = tile_arr(1, t.words), *Z = tile_arr(2, t.words), *S = tile_arr(3, t.words);
   tile_load(DZ, dz_ + t.r0, t.nrows);
   tile_load(DS, ds_ + t.r0, t.nrows);
   tile_load(Z, z_ + t.r0, t.nrows);
@@ -1990,10 +1993,9 @@ __global__ void k_soc_tile_step(ConeSet cs, const int *tiles, const double *__re
   block_seg_min_nonneg(alpha, t.valid ? t.inst : -1, a);
 }
 
-std::vector<int> soc_tiles(const int *off, const int *dim, int n, int lo, int hi) {
+std::vector<int> soc_tiles(const int *off, const int *dim, int n, int max_cones, int max_rows) {
   std::vector<int> t;
-  lo = std::max(lo, 1);
-  hi = std::min(hi, kSocTileMaxDim);
+  const int lo = 1, hi = kSocTileMaxDim;
   int k = 0;
   while (k < n) {
     if (dim[k] > hi || dim[k] < lo) {
@@ -2001,8 +2003,8 @@ std::vector<int> soc_tiles(const int *off, const int *dim, int n, int lo, int hi
       continue;
     }
     int start = k, rows = 0;
-    while (k < n && dim[k] >= lo && dim[k] <= hi && k - start < kSocTileCones &&
-           rows + dim[k] <= kSocTileRows && (k == start || off[k] == off[k - 1] + dim[k - 1])) {
+    while (k < n && dim[k] >= lo && dim[k] <= hi && k - start < max_cones &&
+           rows + dim[k] <= max_rows && (k == start || off[k] == off[k - 1] + dim[k - 1])) {
       rows += dim[k];
       ++k;
     }
@@ -2031,33 +2033,34 @@ static inline int blocks_for(long long n, int b = kBlock) {
     }                                                                                  \
   } while (0)
 
-// Tiled small cones, then (when some cone is larger than the tile limit) the
-// lane-group kernel for the large cones only.
-static inline size_t soc_tile_smem(int narr) {
-  return (size_t)narr * kTileWords * sizeof(double) + kSocTileRows * sizeof(unsigned short) +
-         kSocTileCones;
+// Shared memory of a tile kernel staging `narr` arrays of `rows` rows.
+static inline size_t soc_tile_smem(int narr, int rows) {
+  return (size_t)narr * tile_words(rows) * sizeof(double) + rows * sizeof(unsigned short) +
+         rows / 8;
 }
-// ALL: tiles over every cone of dim <= 16 (update_scaling); otherwise tiles
-// over dims 9..16.  The lane-group kernel takes the remaining cones.
-#define LAUNCH_SOC_TILED(ALL, TILE_KERNEL, NARR, GROUP_KERNEL, ...)                    \
+// One SOC operation with the cone set's launch shape: tiles of the chosen
+// size over the cones of dim <= 16 and the lane-group kernel for the larger
+// ones, or lane groups for every cone.
+#define LAUNCH_SOC_SHAPED(OP, TILE_KERNEL, NARR, GROUP_KERNEL, ...)                    \
   do {                                                                                 \
     if (cs.n_soc > 0) {                                                                \
-      const int _nt = (ALL) ? cs.soc_ntiles : cs.soc_ntiles_mid;                       \
-      const int *_tl = (ALL) ? cs.soc_tile : cs.soc_tile_mid;                          \
-      if (_nt > 0)                                                                     \
-        TILE_KERNEL<<<_nt, kSocTileCones, soc_tile_smem(NARR), st>>>(cs, _tl,          \
-                                                                      __VA_ARGS__);    \
-      bool _rest = (ALL) ? cs.soc_group == 32 : (_nt == 0 || cs.soc_outside_mid != 0); \
-      if (_rest) {                                                                     \
-        ConeSet csl = cs;                                                              \
-        if (_nt > 0) {                                                                 \
-          csl.soc_skip_lo = (ALL) ? 1 : kSocTileMidDim;                                \
+      const int _v = cs.soc_variant[OP];                                               \
+      if (_v >= 1 && _v <= kSocTileShapes && cs.soc_ntiles[_v] > 0) {                  \
+        const int _rows = soc_tile_rows(_v);                                           \
+        TILE_KERNEL<<<cs.soc_ntiles[_v], soc_tile_cones(_v), soc_tile_smem(NARR, _rows), \
+                      st>>>(cs, cs.soc_tile[_v], _rows, __VA_ARGS__);                  \
+        if (cs.soc_group == 32) {                                                      \
+          ConeSet csl = cs;                                                            \
+          csl.soc_skip_lo = 1;                                                         \
           csl.soc_skip_hi = kSocTileMaxDim;                                            \
+          LAUNCH_SOC(GROUP_KERNEL, csl, __VA_ARGS__);                                  \
         }                                                                              \
-        LAUNCH_SOC(GROUP_KERNEL, csl, __VA_ARGS__);                                    \
+      } else {                                                                         \
+        LAUNCH_SOC(GROUP_KERNEL, cs, __VA_ARGS__);                                     \
       }                                                                                \
     }                                                                                  \
   } while (0)
+static inline int nn_block(const ConeSet &cs) { return cs.nn_block > 0 ? cs.nn_block : kBlock; }
 
 static inline void psd_launch_dims(const ConeSet &cs, int nmats, int &nb, int &nt,
                                    size_t &smem) {
@@ -2087,8 +2090,9 @@ static NonsymArgs<PowOps> pow_args(const ConeSet &cs) {
 void cones_update_scaling(const ConeSet &cs, const double *s, const double *z,
                           const double *mu, const int *scaling, int *scale_ok,
                           cudaStream_t st) {
-  if (cs.n_nn) k_nn_update_scaling<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, s, z);
-  LAUNCH_SOC_TILED(true, k_soc_tile_update_scaling, 4, k_soc_update_scaling, s, z, scale_ok);
+  if (cs.n_nn) k_nn_update_scaling<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, s, z);
+  LAUNCH_SOC_SHAPED(kSocUpdateScaling, k_soc_tile_update_scaling, 4, k_soc_update_scaling, s, z,
+                    scale_ok);
   if (cs.n_exp)
     k_nonsym_update_scaling<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
         cs, exp_args(cs), s, z, mu, scaling);
@@ -2125,7 +2129,7 @@ void cones_get_Hs(const ConeSet &cs, const int *nn_blk, const int *soc_blk,
 
 void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, y);
-  if (cs.n_nn) k_nn_mul_hs<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, y, x);
+  if (cs.n_nn) k_nn_mul_hs<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, y, x);
   LAUNCH_SOC(k_soc_mul_hs, cs, y, x);
   if (cs.n_exp)
     k_nonsym_mul_hs<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
@@ -2138,8 +2142,8 @@ void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st
 
 void cones_affine_ds(const ConeSet &cs, double *ds, const double *s, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, ds);
-  if (cs.n_nn) k_nn_affine_ds<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, ds);
-  LAUNCH_SOC_TILED(false, k_soc_tile_affine_ds, 1, k_soc_affine_ds, ds);
+  if (cs.n_nn) k_nn_affine_ds<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, ds);
+  LAUNCH_SOC_SHAPED(kSocAffineDs, k_soc_tile_affine_ds, 1, k_soc_affine_ds, ds);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                               cs.exp_inst, ds, s);
@@ -2152,8 +2156,8 @@ void cones_affine_ds(const ConeSet &cs, double *ds, const double *s, cudaStream_
 void cones_combined_ds_shift(const ConeSet &cs, double *shift, const double *dz,
                              const double *ds, const double *sm, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, shift);
-  if (cs.n_nn) k_nn_combined<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, shift, dz, ds, sm);
-  LAUNCH_SOC_TILED(false, k_soc_tile_combined, 3, k_soc_combined, shift, dz, ds, sm);
+  if (cs.n_nn) k_nn_combined<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, shift, dz, ds, sm);
+  LAUNCH_SOC_SHAPED(kSocCombined, k_soc_tile_combined, 3, k_soc_combined, shift, dz, ds, sm);
   if (cs.n_exp)
     k_nonsym_combined<ExpOps><<<blocks_for(cs.n_exp, 128), 128, 0, st>>>(
         cs, exp_args(cs), shift, dz, ds, sm);
@@ -2166,8 +2170,8 @@ void cones_combined_ds_shift(const ConeSet &cs, double *shift, const double *dz,
 void cones_ds_from_dz_offset(const ConeSet &cs, double *out, const double *ds,
                              const double *z, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, out);
-  if (cs.n_nn) k_nn_ds_offset<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, out, ds, z);
-  LAUNCH_SOC_TILED(false, k_soc_tile_ds_offset, 4, k_soc_ds_offset, out, ds, z);
+  if (cs.n_nn) k_nn_ds_offset<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, out, ds, z);
+  LAUNCH_SOC_SHAPED(kSocDsOffset, k_soc_tile_ds_offset, 4, k_soc_ds_offset, out, ds, z);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                               cs.exp_inst, out, ds);
@@ -2180,8 +2184,8 @@ void cones_ds_from_dz_offset(const ConeSet &cs, double *out, const double *ds,
 void cones_step_length_sym(const ConeSet &cs, const double *dz, const double *ds,
                            const double *z, const double *s, double *alpha,
                            cudaStream_t st) {
-  if (cs.n_nn) k_nn_step<<<blocks_for(cs.n_nn), kBlock, 0, st>>>(cs, dz, ds, z, s, alpha);
-  LAUNCH_SOC_TILED(false, k_soc_tile_step, 4, k_soc_step, dz, ds, z, s, alpha);
+  if (cs.n_nn) k_nn_step<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, dz, ds, z, s, alpha);
+  LAUNCH_SOC_SHAPED(kSocStep, k_soc_tile_step, 4, k_soc_step, dz, ds, z, s, alpha);
   LAUNCH_PSD(k_psd_step, 4, cs, dz, ds, alpha);
 }
 
@@ -2237,6 +2241,114 @@ void cones_set_identity_scaling(const ConeSet &cs, cudaStream_t st) {
   if (t) k_identity<<<blocks_for(t), kBlock, 0, st>>>(cs);
   int c = cs.n_soc + cs.n_psd;
   if (c) k_identity_cones<<<blocks_for(c), kBlock, 0, st>>>(cs);
+}
+
+
+// ============================================================ autotuning
+void cones_default_shapes(ConeSet &cs) {
+  cs.nn_block = kBlock;
+  cs.soc_variant[kSocUpdateScaling] = kSocTileShapes;
+  for (int op = 1; op < kSocOps; ++op) cs.soc_variant[op] = 0;
+  cs.soc_skip_lo = 1;  // empty skip range: lane groups take every cone
+  cs.soc_skip_hi = 0;
+}
+
+int cones_autotune(ConeSet &cs, cudaStream_t st) {
+  if (cs.n_nn == 0 && cs.n_soc == 0) return 0;
+  const size_t m = std::max(cs.m_total, 1), B = std::max(cs.B, 1), nn = cs.n_nn,
+               sr = cs.soc_rows, nsoc = cs.n_soc;
+  // scratch: five vectors, the NN / SOC state, per-instance scalars
+  const size_t words = 5 * m + 2 * nn + 4 * sr + 2 * nsoc + 4 * B + 8;
+  double *buf = nullptr;
+  cudaError_t e = cudaMalloc(&buf, words * sizeof(double));
+  if (e != cudaSuccess) return -1000 - (int)e;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  ConeSet t = cs;
+  t.inst_active = nullptr;  // every instance runs while timing
+  double *s = buf, *z = s + m, *dz = z + m, *ds = dz + m, *y = ds + m, *p = y + m;
+  t.nn_w = p, p += nn;
+  t.nn_lambda = p, p += nn;
+  t.soc_w = p, p += sr;
+  t.soc_lambda = p, p += sr;
+  t.soc_u = p, p += sr;
+  t.soc_v = p, p += sr;
+  t.soc_eta = p, p += nsoc;
+  t.soc_d = p, p += nsoc;
+  double *mu = p, *sm = p + B, *alpha = p + 2 * B;
+  int *scaling = reinterpret_cast<int *>(p + 3 * B), *scale_ok = scaling + B;
+  cudaMemsetAsync(buf, 0, words * sizeof(double), st);
+  cones_unit_initialization(t, z, s, st);
+  {
+    std::vector<double> sc(3 * B);
+    for (size_t i = 0; i < B; ++i) sc[i] = 1.0, sc[B + i] = 0.1, sc[2 * B + i] = 1.0;
+    std::vector<int> ok(B, 1);
+    cudaMemcpyAsync(mu, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(scale_ok, ok.data(), B * sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);  // host vectors leave scope
+  }
+  auto timed = [&](auto launch) {
+    launch();
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 3; ++r) launch();
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  auto run = [&](const ConeSet &c, int op) {
+    switch (op) {
+      case kSocUpdateScaling: cones_update_scaling(c, s, z, mu, scaling, scale_ok, st); break;
+      case kSocAffineDs: cones_affine_ds(c, y, s, st); break;
+      case kSocCombined: cones_combined_ds_shift(c, y, dz, ds, sm, st); break;
+      case kSocDsOffset: cones_ds_from_dz_offset(c, y, ds, z, st); break;
+      default: cones_step_length_sym(c, dz, ds, z, s, alpha, st); break;
+    }
+  };
+  // only the cone type being tuned launches
+  ConeSet only = t;
+  only.n_zero = 0, only.n_exp = 0, only.n_pow = 0, only.n_psd = 0;
+  run(only, kSocUpdateScaling);  // fills the scratch state the other operations read
+  if (cs.n_nn > 0) {
+    ConeSet c = only;
+    c.n_soc = 0;
+    int best = cs.nn_block;
+    float best_ms = 1e30f;
+    for (int b : {128, 256, 512}) {
+      c.nn_block = b;
+      float ms = timed([&]() {
+        run(c, kSocUpdateScaling);
+        run(c, kSocCombined);
+        run(c, kSocStep);
+      });
+      if (ms < best_ms) best_ms = ms, best = b;
+    }
+    cs.nn_block = best;
+  }
+  if (cs.n_soc > 0) {
+    ConeSet c = only;
+    c.n_nn = 0;
+    for (int op = 0; op < kSocOps; ++op) {
+      int best = cs.soc_variant[op];
+      float best_ms = 1e30f;
+      for (int v = 0; v <= kSocTileShapes; ++v) {
+        if (v > 0 && cs.soc_ntiles[v] == 0) continue;
+        c.soc_variant[op] = v;
+        float ms = timed([&]() { run(c, op); });
+        if (ms < best_ms) best_ms = ms, best = v;
+      }
+      c.soc_variant[op] = best;
+      cs.soc_variant[op] = best;
+    }
+  }
+  e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  return e == cudaSuccess ? 0 : -1000 - (int)e;
 }
 
 }  // namespace clgpu

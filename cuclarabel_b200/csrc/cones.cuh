@@ -11,23 +11,28 @@
 
 namespace clgpu {
 
-// Second-order cones are processed in shared-memory tiles by some
-// per-iteration kernels: a tile is a run of consecutive cones with contiguous
-// rows, at most kSocTileCones cones and kSocTileRows rows, staged with
-// coalesced loads and stores, one thread per cone.  update_scaling tiles
-// every cone of dim <= kSocTileMaxDim; affine_ds, combined_ds_shift,
-// ds_from_dz_offset and step_length tile dims kSocTileMidDim..kSocTileMaxDim
-// (smaller cones keep most lanes of their lane groups busy); mul_Hs and the
-// rest use lane groups.  Which kernel handles a cone depends only on the
-// cone's own dimension, so an instance computes the same bits alone or in
-// any batch.
+// Second-order cones of dim <= kSocTileMaxDim can be processed in
+// shared-memory tiles by the per-iteration operations below: a tile is a run
+// of consecutive cones with contiguous rows (at most C cones and 8*C rows,
+// C = 32, 64 or 128 = the block size), staged with coalesced loads and
+// stores, one thread per cone.  The alternative is a lane group per cone.
+// Both evaluate the same formulas with sums in the same butterfly order, so
+// the choice (made per cone set by cones_autotune) does not change results.
 constexpr int kSocTileMaxDim = 16;
-constexpr int kSocTileMidDim = 9;
-constexpr int kSocTileCones = 128;
-constexpr int kSocTileRows = 1024;
-// Tile list [c0, c1, c0, c1, ...] over the cones of dim in [lo, hi] among n
-// cones (rows off[k] .. off[k]+dim[k]).
-std::vector<int> soc_tiles(const int *off, const int *dim, int n, int lo, int hi);
+constexpr int kSocTileShapes = 3;  // v = 1..3: 32, 64, 128 cones per tile
+__host__ __device__ constexpr int soc_tile_cones(int v) { return 32 << (v - 1); }
+__host__ __device__ constexpr int soc_tile_rows(int v) { return 8 * soc_tile_cones(v); }
+enum SocOp { kSocUpdateScaling = 0, kSocAffineDs, kSocCombined, kSocDsOffset, kSocStep, kSocOps };
+// Tile list [c0, c1, c0, c1, ...] over the cones of dim <= kSocTileMaxDim
+// among n cones (rows off[k] .. off[k]+dim[k]), at most max_cones cones and
+// max_rows rows per tile.
+std::vector<int> soc_tiles(const int *off, const int *dim, int n, int max_cones, int max_rows);
+// Default launch shapes of a cone set (before or without tuning).
+void cones_default_shapes(ConeSet &cs);
+// Times the candidate launch shapes of the nonnegative and SOC kernels on
+// this cone set (scratch state and vectors, nothing of cs is written but
+// its shape fields) and keeps the fastest.  Returns 0 or -1000 - cudaError.
+int cones_autotune(ConeSet &cs, cudaStream_t st);
 
 // update_scaling!  (coneops_compositecone_gpu.jl:185).  mu/scaling are
 // per-instance device arrays; scale_ok[i] is cleared to 0 on failure.

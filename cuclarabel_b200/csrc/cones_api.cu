@@ -145,18 +145,15 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
   cs.soc_sparse = A.upload(soc_sparse);
   {
     const int nsc = (int)soc_off.size();
-    std::vector<int> tiles = soc_tiles(soc_off.data(), soc_dim.data(), nsc, 1, kSocTileMaxDim);
-    std::vector<int> mid =
-        soc_tiles(soc_off.data(), soc_dim.data(), nsc, kSocTileMidDim, kSocTileMaxDim);
-    cs.soc_ntiles = (int)tiles.size() / 2;
-    cs.soc_tile = A.upload(tiles);
-    cs.soc_ntiles_mid = (int)mid.size() / 2;
-    cs.soc_tile_mid = A.upload(mid);
-    cs.soc_outside_mid = 0;
-    for (int k = 0; k < nsc; ++k)
-      if (soc_dim[k] < kSocTileMidDim || soc_dim[k] > kSocTileMaxDim) cs.soc_outside_mid = 1;
-    cs.soc_skip_lo = 1;
-    cs.soc_skip_hi = 0;  // empty range: lane-group kernels take every cone
+    for (int v = 1; v <= kSocTileShapes; ++v) {
+      std::vector<int> tiles =
+          soc_tiles(soc_off.data(), soc_dim.data(), nsc, soc_tile_cones(v), soc_tile_rows(v));
+      cs.soc_ntiles[v] = (int)tiles.size() / 2;
+      cs.soc_tile[v] = A.upload(tiles);
+    }
+    cs.soc_ntiles[0] = 0;
+    cs.soc_tile[0] = nullptr;
+    cones_default_shapes(cs);
   }
   cs.exp_inst = A.upload(exp_inst);
   cs.pow_inst = A.upload(pow_inst);
@@ -210,6 +207,11 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
     delete h;
     return e;
   }
+  int rc = cones_autotune(cs, 0);  // launch shapes timed on this cone set
+  if (rc != 0) {
+    delete h;
+    return rc;
+  }
   *out = h;
   return 0;
 }
@@ -223,6 +225,26 @@ extern "C" int clgpu_cones_numel(const clgpu_cones *h) { return h ? h->numel : -
 extern "C" int clgpu_cones_degree(const clgpu_cones *h) { return h ? h->degree : -1; }
 extern "C" int clgpu_cones_hs_len(const clgpu_cones *h) { return h ? h->hs_len : -1; }
 
+extern "C" int clgpu_cones_get_launch_shapes(const clgpu_cones *h, int *nn_block,
+                                             int *soc_variants) {
+  if (!h) return -1;
+  if (nn_block) *nn_block = h->cs.nn_block;
+  if (soc_variants)
+    for (int op = 0; op < kSocOps; ++op) soc_variants[op] = h->cs.soc_variant[op];
+  return 0;
+}
+extern "C" int clgpu_cones_set_launch_shapes(clgpu_cones *h, int nn_block,
+                                             const int *soc_variants) {
+  if (!h) return -1;
+  if (nn_block != 0 && (nn_block < 32 || nn_block > 1024 || nn_block % 32 != 0)) return -1;
+  if (soc_variants)
+    for (int op = 0; op < kSocOps; ++op)
+      if (soc_variants[op] < 0 || soc_variants[op] > kSocTileShapes) return -1;
+  if (nn_block) h->cs.nn_block = nn_block;
+  if (soc_variants)
+    for (int op = 0; op < kSocOps; ++op) h->cs.soc_variant[op] = soc_variants[op];
+  return 0;
+}
 extern "C" int clgpu_cones_set_profiling(clgpu_cones *h, int enable) {
   if (!h) return -1;
   if (enable && !h->ev[0])

@@ -1279,18 +1279,15 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   cs.soc_sparse = A.upload(soc_sparse);
   {
     const int nsc = (int)soc_off.size();
-    std::vector<int> tiles = soc_tiles(soc_off.data(), soc_dim.data(), nsc, 1, kSocTileMaxDim);
-    std::vector<int> mid =
-        soc_tiles(soc_off.data(), soc_dim.data(), nsc, kSocTileMidDim, kSocTileMaxDim);
-    cs.soc_ntiles = (int)tiles.size() / 2;
-    cs.soc_tile = A.upload(tiles);
-    cs.soc_ntiles_mid = (int)mid.size() / 2;
-    cs.soc_tile_mid = A.upload(mid);
-    cs.soc_outside_mid = 0;
-    for (int k = 0; k < nsc; ++k)
-      if (soc_dim[k] < kSocTileMidDim || soc_dim[k] > kSocTileMaxDim) cs.soc_outside_mid = 1;
-    cs.soc_skip_lo = 1;
-    cs.soc_skip_hi = 0;  // empty range: lane-group kernels take every cone
+    for (int v = 1; v <= kSocTileShapes; ++v) {
+      std::vector<int> tiles =
+          soc_tiles(soc_off.data(), soc_dim.data(), nsc, soc_tile_cones(v), soc_tile_rows(v));
+      cs.soc_ntiles[v] = (int)tiles.size() / 2;
+      cs.soc_tile[v] = A.upload(tiles);
+    }
+    cs.soc_ntiles[0] = 0;
+    cs.soc_tile[0] = nullptr;
+    cones_default_shapes(cs);
   }
   cs.exp_inst = A.upload(exp_inst);
   cs.pow_inst = A.upload(pow_inst);
@@ -2084,6 +2081,12 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
   h->lp.ir_stopratio = h->st.iterative_refinement_stop_ratio;
   h->sd = make_sd(h->st);
   h->info.assign(nprob, clgpu_info{});
+  // launch shapes of the nonnegative and SOC kernels, timed on this batch
+  rc = cones_autotune(h->cs, 0);
+  if (rc != 0) {
+    delete h;
+    return rc;
+  }
   *out = h;
   return 0;
 }
@@ -2732,6 +2735,14 @@ extern "C" int clgpu_solver_get_solutions(clgpu_solver *h, double *x, double *s,
   return 0;
 }
 
+extern "C" int clgpu_solver_get_launch_shapes(const clgpu_solver *h, int *nn_block,
+                                              int *soc_variants) {
+  if (!h) return -1;
+  if (nn_block) *nn_block = h->cs.nn_block;
+  if (soc_variants)
+    for (int op = 0; op < kSocOps; ++op) soc_variants[op] = h->cs.soc_variant[op];
+  return 0;
+}
 extern "C" long long clgpu_solver_device_bytes(const clgpu_solver *h) {
   return h ? h->arena.bytes : -1;
 }

@@ -145,6 +145,9 @@ int clgpu_solver_update_qb(clgpu_solver *h, int inst, const double *q,
                            const double *b);
 /* device-memory footprint of the handle in bytes */
 long long clgpu_solver_device_bytes(const clgpu_solver *h);
+/* The launch shapes the setup autotuner chose for this batch (see
+ * clgpu_cones_get_launch_shapes); tuning hook, no reference counterpart. */
+int clgpu_solver_get_launch_shapes(const clgpu_solver *h, int *nn_block, int *soc_variants);
 /* number of kernel launches issued by the last solve */
 long long clgpu_solver_launch_count(const clgpu_solver *h);
 /* timing of the last solve: total ms and the per-kernel-class ms measured
@@ -215,6 +218,17 @@ int clgpu_cones_hs_len(const clgpu_cones *h);
  * the device time of the last completed operation in milliseconds
  * (step_length: both launch groups summed). */
 int clgpu_cones_set_profiling(clgpu_cones *h, int enable);
+/* Launch shapes (a tuning hook with no counterpart in the reference): the
+ * threads per block of the nonnegative-cone kernels and, for the SOC
+ * operations update_scaling, affine_ds, combined_ds_shift,
+ * Δs_from_Δz_offset and step_length (in that order), 0 = one lane group per
+ * cone or v = 1..3 = shared-memory tiles of 32, 64 or 128 cones of
+ * dim <= 16.  clgpu_cones_create and clgpu_solver_create time the
+ * candidates on their own cone layout and keep the fastest; every shape
+ * gives the same results.  set: nn_block 0 keeps the current block size,
+ * soc_variants NULL keeps the SOC variants; -1 on an invalid shape. */
+int clgpu_cones_get_launch_shapes(const clgpu_cones *h, int *nn_block, int *soc_variants);
+int clgpu_cones_set_launch_shapes(clgpu_cones *h, int nn_block, const int *soc_variants);
 int clgpu_cones_last_kernel_ms(const clgpu_cones *h, double *ms);
 /* update_scaling! (coneops_compositecone_gpu.jl:185); strategy 0 PrimalDual,
  * 1 Dual; returns 1 if a cone is not strictly interior */

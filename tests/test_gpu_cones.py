@@ -214,3 +214,49 @@ def test_kernel_time_profiling_leaves_results_unchanged(cuda_device):
         assert (ms.value > 0) if prof else (ms.value == 0.0)
         outs.append(y.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("name", ["soc_tiles", "soc_sparse", "mixed", "nn"])
+def test_launch_shapes_give_identical_results(cuda_device, name):
+    """Every launch shape the autotuner may pick (lane groups or tiles of
+    32 / 64 / 128 cones for the SOC operations, 64..512 threads per block for
+    the nonnegative kernels) returns the same bits."""
+    specs, rng, s, z = setup(name, seed=7)
+    G = GPUCones(specs)
+    m = G.numel
+    d_s, d_z = G.dev(s), G.dev(z)
+    dz, ds = G.dev(rng.standard_normal(m) * 0.3), G.dev(rng.standard_normal(m) * 0.3)
+    x = G.dev(rng.standard_normal(m))
+    runs = []
+    for v, nb in [(0, 128), (1, 256), (2, 512), (3, 64)]:
+        assert G.L.clgpu_cones_set_launch_shapes(G.h, nb, (ctypes.c_int * 5)(*[v] * 5)) == 0
+        nbo, vo = ctypes.c_int(), (ctypes.c_int * 5)()
+        assert G.L.clgpu_cones_get_launch_shapes(G.h, ctypes.byref(nbo), vo) == 0
+        assert nbo.value == nb and list(vo) == [v] * 5
+        out = {}
+        assert G.L.clgpu_update_scaling(G.h, d_s.data_ptr(), d_z.data_ptr(), 1.0, 0, None) == 0
+        hs = G.empty(G.hs_len)
+        assert G.L.clgpu_get_Hs(G.h, hs.data_ptr(), None) == 0
+        out["Hs"] = hs.cpu().numpy()
+        for key, call in (
+                ("mul_Hs", lambda y: G.L.clgpu_mul_Hs(G.h, y.data_ptr(), x.data_ptr(), None)),
+                ("affine_ds", lambda y: G.L.clgpu_affine_ds(G.h, y.data_ptr(), d_s.data_ptr(),
+                                                            None)),
+                ("combined", lambda y: G.L.clgpu_combined_ds_shift(
+                    G.h, y.data_ptr(), dz.data_ptr(), ds.data_ptr(), d_z.data_ptr(), 0.05, None)),
+                ("ds_offset", lambda y: G.L.clgpu_ds_from_dz_offset(
+                    G.h, y.data_ptr(), ds.data_ptr(), d_z.data_ptr(), None))):
+            y = G.empty(m)
+            assert call(y) == 0
+            out[key] = y.cpu().numpy()
+        a = ctypes.c_double()
+        assert G.L.clgpu_step_length(G.h, dz.data_ptr(), ds.data_ptr(), d_z.data_ptr(),
+                                     d_s.data_ptr(), 1.0, 0.99, 0.8, 1e-4, ctypes.byref(a),
+                                     None) == 0
+        out["alpha"] = np.array([a.value])
+        runs.append(out)
+    for r in runs[1:]:
+        for k, v in r.items():
+            assert np.array_equal(v.view(np.uint64), runs[0][k].view(np.uint64)), k
+    assert G.L.clgpu_cones_set_launch_shapes(G.h, 48, None) == -1
+    assert G.L.clgpu_cones_set_launch_shapes(G.h, 0, (ctypes.c_int * 5)(0, 0, 4, 0, 0)) == -1

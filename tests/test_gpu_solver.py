@@ -198,3 +198,15 @@ def test_results_refill_in_place_matches_fresh_arrays(cuda_device):
     for k in ("x", "s", "z", "status"):
         assert np.array_equal(again[k], fresh[k])
     assert np.array_equal(again["info"]["obj_val"], fresh["info"]["obj_val"])
+
+
+def test_setup_autotuner_picks_valid_launch_shapes(cuda_device):
+    """The batch solver's setup times the cone kernels' launch shapes on its
+    own cone layout and keeps valid ones."""
+    import ctypes
+    from cuclarabel_b200 import _lib
+    solver = BatchSolver(problems.mpc_batch(8, seed0=30))
+    nb, v = ctypes.c_int(), (ctypes.c_int * 5)()
+    assert _lib.load().clgpu_solver_get_launch_shapes(solver._h, ctypes.byref(nb), v) == 0
+    assert nb.value in (128, 256, 512)
+    assert all(0 <= x <= 3 for x in v)
