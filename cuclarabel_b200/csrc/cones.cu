@@ -1728,8 +1728,19 @@ __device__ __forceinline__ SocTileCtx soc_tile_ctx(const ConeSet &cs, const int 
   }
   return t;
 }
+// Staging copies go global -> shared with cp.async (no register round trip),
+// so every thread has all of its copies in flight at once; tile_loaded()
+// waits for this thread's copies and the block barrier that follows makes
+// them visible to the block.
 __device__ __forceinline__ void tile_load(double *dst, const double *__restrict__ src, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[tsk(i)] = src[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + tsk(i)));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src + i)
+                 : "memory");
+  }
+}
+__device__ __forceinline__ void tile_loaded() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 __device__ __forceinline__ void tile_store(double *dst, const double *src, int n,
                                            const SocTileCtx &t) {
@@ -1746,6 +1757,7 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, int trow
   double *S = tile_arr(0, t.words), *Z = tile_arr(1, t.words), *U = tile_arr(2, t.words), *V = tile_arr(3, t.words);
   tile_load(S, s_ + t.r0, t.nrows);
   tile_load(Z, z_ + t.r0, t.nrows);
+  tile_loaded();
   __syncthreads();
   bool sparse_tile = false;
   if (t.valid) {
@@ -1839,6 +1851,7 @@ __global__ void k_soc_tile_affine_ds(ConeSet cs, const int *tiles, int trows, do
   SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 1);
   double *L = tile_arr(0, t.words);
   tile_load(L, cs.soc_lambda + (t.r0 - cs.soc_begin), t.nrows);
+  tile_loaded();
   __syncthreads();
   if (t.valid) {
     const int o = t.off, d = t.dim;
@@ -1867,6 +1880,7 @@ __global__ void k_soc_tile_combined(ConeSet cs, const int *tiles, int trows, dou
   tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
   tile_load(DZ, dz_ + t.r0, t.nrows);
   tile_load(DS, ds_ + t.r0, t.nrows);
+  tile_loaded();
   __syncthreads();
   if (t.valid) {
     const int o = t.off, d = t.dim;
@@ -1912,6 +1926,7 @@ __global__ void k_soc_tile_ds_offset(ConeSet cs, const int *tiles, int trows, do
   tile_load(L, cs.soc_lambda + r, t.nrows);
   tile_load(DS, ds_ + t.r0, t.nrows);
   tile_load(Z, z_ + t.r0, t.nrows);
+  tile_loaded();
   __syncthreads();
   if (t.valid) {
     const int o = t.off, d = t.dim;
@@ -1982,6 +1997,7 @@ __global__ void k_soc_tile_step(ConeSet cs, const int *tiles, int trows, const d
   tile_load(DS, ds_ + t.r0, t.nrows);
   tile_load(Z, z_ + t.r0, t.nrows);
   tile_load(S, s_ + t.r0, t.nrows);
+  tile_loaded();
   __syncthreads();
   double a = CUDART_INF;
   if (t.valid) {
