@@ -1663,11 +1663,14 @@ __global__ void k_identity_cones(ConeSet cs) {
 // formulas of the lane-group kernels above, with their sums in the same
 // butterfly order, tree16), and results leave through coalesced stores of
 // the rows whose cone is active.
-// Shared rows are skewed by one word every 16 so that threads walking their
-// cones at a stride of 3..16 words meet few bank conflicts.
-__device__ __forceinline__ int tsk(int i) { return i + (i >> 4); }
-// words of one staged array for a tile of `rows` rows (skew included)
-__host__ __device__ __forceinline__ int tile_words(int rows) { return rows + rows / 16 + 1; }
+// Shared rows keep their global order (tsk is the identity): with the mixed
+// cone dimensions of real tiles the threads' strides are irregular and no
+// fixed skew spreads the banks better (about 2.2 wavefronts per access
+// either way), while one word per 16 rows made uniform dim-10 tiles 5-way
+// conflicted.
+__device__ __forceinline__ int tsk(int i) { return i; }
+// words of one staged array for a tile of `rows` rows
+__host__ __device__ __forceinline__ int tile_words(int rows) { return rows; }
 // Sum of a cone's per-element terms in the order of the lane-group kernels'
 // butterfly reduction (pairs at distance 8, 4, 2, 1 over 16 leaves, leaves
 // from the cone's dimension on are +0): for dim <= 16 this is the same
