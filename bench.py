@@ -252,7 +252,7 @@ def cone_kernel_roofline(hbm, scale=1.0, reps=5, seed=7):
                 "step_length": lambda: L.clgpu_step_length(
                     h, P(dz), P(ds), P(z), P(s), 1.0, 0.99, 0.8, 1e-4, ctypes.byref(a_out), sh),
             }
-            nb, sv = ctypes.c_int(), (ctypes.c_int * 5)()
+            nb, sv = ctypes.c_int(), (ctypes.c_int * 6)()
             L.clgpu_cones_get_launch_shapes(h, ctypes.byref(nb), sv)
             shapes = {"nn_block": nb.value,
                       "soc": ["groups" if x == 0 else "tiles%d" % (32 << (x - 1)) for x in sv]}

@@ -541,13 +541,13 @@ class BatchSolver:
         return _lib.load().clgpu_solver_launch_count(self._h)
 
     SOC_OPS = ("update_scaling", "affine_ds", "combined_ds_shift", "ds_from_dz_offset",
-               "step_length")
+               "step_length", "mul_Hs")
 
     def launch_shapes(self):
         """Launch shapes the setup autotuner chose for this batch: threads per
         block of the nonnegative kernels, and per SOC operation "groups" (one
         lane group per cone) or "tiles<C>" (shared-memory tiles of C cones)."""
-        nb, v = ctypes.c_int(), (ctypes.c_int * 5)()
+        nb, v = ctypes.c_int(), (ctypes.c_int * len(self.SOC_OPS))()
         rc = _lib.load().clgpu_solver_get_launch_shapes(self._h, ctypes.byref(nb), v)
         if rc != 0:
             raise RuntimeError("clgpu_solver_get_launch_shapes failed with code %d" % rc)

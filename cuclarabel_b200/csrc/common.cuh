@@ -52,7 +52,7 @@ struct ConeSet {
   // variant, 0 = lane groups, v = 1..3 = shared-memory tiles of 32 << (v-1)
   // cones (8 rows per cone) over the cones of dim <= 16.
   int nn_block;
-  int soc_variant[5];
+  int soc_variant[6];  // indexed by SocOp (cones.cuh)
   int soc_ntiles[4];         // tiles per shape v = 1..3 ([0] unused)
   const int *soc_tile[4];    // [2*soc_ntiles[v]] first and one-past-last cone
   int soc_skip_lo, soc_skip_hi;  // lane-group kernels leave these dims alone

@@ -1849,6 +1849,32 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, int trow
   }
 }
 
+// mul_Hs for tiled cones: y = eta^2 (J x + 2 (w'x) w), J = diag(-1, 1, ...);
+// y overwrites the staged x rows in place.
+__global__ void k_soc_tile_mul_hs(ConeSet cs, const int *tiles, int trows, double *y_,
+                                  const double *__restrict__ x_) {
+  SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 2);
+  double *W = tile_arr(0, t.words), *X = tile_arr(1, t.words);
+  tile_load(W, cs.soc_w + (t.r0 - cs.soc_begin), t.nrows);
+  tile_load(X, x_ + t.r0, t.nrows);
+  tile_loaded();
+  __syncthreads();
+  if (t.valid) {
+    const int o = t.off, d = t.dim;
+    double tt = tree16(d, [&](int l) { return 0.0 + W[tsk(o + l)] * X[tsk(o + l)]; });
+    double c = 2 * tt;
+    double eta = cs.soc_eta[t.c], e2 = eta * eta;
+    for (int i = 0; i < d; ++i) {
+      double xi = X[tsk(o + i)];
+      double v = (i == 0) ? -xi : xi;
+      X[tsk(o + i)] = (v + c * W[tsk(o + i)]) * e2;
+    }
+    t.ok[t.k] = 1;
+  }
+  __syncthreads();
+  tile_store(y_ + t.r0, X, t.nrows, t);
+}
+
 // affine_ds! for tiled cones: ds = lambda o lambda
 __global__ void k_soc_tile_affine_ds(ConeSet cs, const int *tiles, int trows, double *ds_) {
   SocTileCtx t = soc_tile_ctx(cs, tiles, trows, 1);
@@ -2149,7 +2175,7 @@ void cones_get_Hs(const ConeSet &cs, const int *nn_blk, const int *soc_blk,
 void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, y);
   if (cs.n_nn) k_nn_mul_hs<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, y, x);
-  LAUNCH_SOC(k_soc_mul_hs, cs, y, x);
+  LAUNCH_SOC_SHAPED(kSocMulHs, k_soc_tile_mul_hs, 2, k_soc_mul_hs, y, x);
   if (cs.n_exp)
     k_nonsym_mul_hs<<<blocks_for(cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
                                                             cs.exp_inst, cs.exp_Hs, y, x);
@@ -2339,7 +2365,9 @@ int cones_autotune(ConeSet &cs, cudaStream_t st) {
       case kSocAffineDs: cones_affine_ds(c, y, s, st); break;
       case kSocCombined: cones_combined_ds_shift(c, y, dz, ds, sm, st); break;
       case kSocDsOffset: cones_ds_from_dz_offset(c, y, ds, z, st); break;
-      default: cones_step_length_sym(c, dz, ds, z, s, alpha, st); break;
+      case kSocMulHs: cones_mul_Hs(c, y, dz, st); break;
+      case kSocStep: cones_step_length_sym(c, dz, ds, z, s, alpha, st); break;
+      default: break;
     }
   };
   // only the cone type being tuned launches

@@ -22,7 +22,15 @@ constexpr int kSocTileMaxDim = 16;
 constexpr int kSocTileShapes = 3;  // v = 1..3: 32, 64, 128 cones per tile
 __host__ __device__ constexpr int soc_tile_cones(int v) { return 32 << (v - 1); }
 __host__ __device__ constexpr int soc_tile_rows(int v) { return 8 * soc_tile_cones(v); }
-enum SocOp { kSocUpdateScaling = 0, kSocAffineDs, kSocCombined, kSocDsOffset, kSocStep, kSocOps };
+enum SocOp {
+  kSocUpdateScaling = 0,
+  kSocAffineDs,
+  kSocCombined,
+  kSocDsOffset,
+  kSocStep,
+  kSocMulHs,
+  kSocOps
+};
 // Tile list [c0, c1, c0, c1, ...] over the cones of dim <= kSocTileMaxDim
 // among n cones (rows off[k] .. off[k]+dim[k]), at most max_cones cones and
 // max_rows rows per tile.

@@ -229,10 +229,10 @@ def test_launch_shapes_give_identical_results(cuda_device, name):
     x = G.dev(rng.standard_normal(m))
     runs = []
     for v, nb in [(0, 128), (1, 256), (2, 512), (3, 64)]:
-        assert G.L.clgpu_cones_set_launch_shapes(G.h, nb, (ctypes.c_int * 5)(*[v] * 5)) == 0
-        nbo, vo = ctypes.c_int(), (ctypes.c_int * 5)()
+        assert G.L.clgpu_cones_set_launch_shapes(G.h, nb, (ctypes.c_int * 6)(*[v] * 6)) == 0
+        nbo, vo = ctypes.c_int(), (ctypes.c_int * 6)()
         assert G.L.clgpu_cones_get_launch_shapes(G.h, ctypes.byref(nbo), vo) == 0
-        assert nbo.value == nb and list(vo) == [v] * 5
+        assert nbo.value == nb and list(vo) == [v] * 6
         out = {}
         assert G.L.clgpu_update_scaling(G.h, d_s.data_ptr(), d_z.data_ptr(), 1.0, 0, None) == 0
         hs = G.empty(G.hs_len)
@@ -259,4 +259,4 @@ def test_launch_shapes_give_identical_results(cuda_device, name):
         for k, v in r.items():
             assert np.array_equal(v.view(np.uint64), runs[0][k].view(np.uint64)), k
     assert G.L.clgpu_cones_set_launch_shapes(G.h, 48, None) == -1
-    assert G.L.clgpu_cones_set_launch_shapes(G.h, 0, (ctypes.c_int * 5)(0, 0, 4, 0, 0)) == -1
+    assert G.L.clgpu_cones_set_launch_shapes(G.h, 0, (ctypes.c_int * 6)(0, 0, 4, 0, 0, 0)) == -1

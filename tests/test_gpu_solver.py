@@ -206,7 +206,7 @@ def test_setup_autotuner_picks_valid_launch_shapes(cuda_device):
     import ctypes
     from cuclarabel_b200 import _lib
     solver = BatchSolver(problems.mpc_batch(8, seed0=30))
-    nb, v = ctypes.c_int(), (ctypes.c_int * 5)()
+    nb, v = ctypes.c_int(), (ctypes.c_int * 6)()
     assert _lib.load().clgpu_solver_get_launch_shapes(solver._h, ctypes.byref(nb), v) == 0
     assert nb.value in (128, 256, 512)
     assert all(0 <= x <= 3 for x in v)
