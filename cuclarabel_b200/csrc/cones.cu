@@ -2306,7 +2306,10 @@ int cones_autotune(ConeSet &cs, cudaStream_t st) {
   const size_t words = 5 * m + 2 * nn + 4 * sr + 2 * nsoc + 4 * B + 8;
   double *buf = nullptr;
   cudaError_t e = cudaMalloc(&buf, words * sizeof(double));
-  if (e != cudaSuccess) return -1000 - (int)e;
+  if (e != cudaSuccess) {  // no room for scratch: keep the default shapes
+    cudaGetLastError();
+    return 0;
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

@@ -39,7 +39,8 @@ std::vector<int> soc_tiles(const int *off, const int *dim, int n, int max_cones,
 void cones_default_shapes(ConeSet &cs);
 // Times the candidate launch shapes of the nonnegative and SOC kernels on
 // this cone set (scratch state and vectors, nothing of cs is written but
-// its shape fields) and keeps the fastest.  Returns 0 or -1000 - cudaError.
+// its shape fields) and keeps the fastest; without room for the scratch it
+// keeps the default shapes.  Returns 0 or -1000 - cudaError.
 int cones_autotune(ConeSet &cs, cudaStream_t st);
 
 // update_scaling!  (coneops_compositecone_gpu.jl:185).  mu/scaling are
