@@ -28,6 +28,7 @@
 namespace clgpu {
 
 static constexpr int kBlock = 256;
+static constexpr int kNNRows = 4;  // rows per thread of k_nn_affine_ds, single-problem k_nn_step
 static constexpr int kPsdWarps = 2;  // warps (cones) per PSD block
 
 __device__ __forceinline__ bool active_inst(const ConeSet &cs, int inst) {
@@ -1023,13 +1024,22 @@ __global__ void k_psd_mul_hs(ConeSet cs, double *y, const double *__restrict__ x
 }
 
 // ============================================================== affine_ds
+// kNNRows rows per thread (a block covers kNNRows * blockDim consecutive
+// rows, row k * blockDim + threadIdx of its range): the loads of all of a
+// thread's rows are issued before the first store.
 __global__ void k_nn_affine_ds(ConeSet cs, double *ds) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= cs.n_nn) return;
-  int g = cs.nn_begin + e;
-  if (!active_row(cs, g)) return;
-  double l = cs.nn_lambda[e];
-  ds[g] = l * l;
+  const int base = blockIdx.x * blockDim.x * kNNRows + threadIdx.x;
+  double l[kNNRows];
+  bool on[kNNRows];
+#pragma unroll
+  for (int k = 0; k < kNNRows; ++k) {
+    const int e = base + k * blockDim.x;
+    on[k] = e < cs.n_nn && active_row(cs, cs.nn_begin + e);
+    l[k] = on[k] ? cs.nn_lambda[e] : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < kNNRows; ++k)
+    if (on[k]) ds[cs.nn_begin + base + k * blockDim.x] = l[k] * l[k];
 }
 template <int G>
 __global__ void k_soc_affine_ds(ConeSet cs, double *ds_) {
@@ -1238,6 +1248,30 @@ __global__ void k_psd_ds_offset(ConeSet cs, double *out, const double *__restric
 __global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
                           const double *__restrict__ ds, const double *__restrict__ z,
                           const double *__restrict__ s, double *alpha) {
+  if (cs.B == 1) {
+    // one problem: kNNRows rows per thread (as k_nn_affine_ds), one
+    // block-level reduction per kNNRows * blockDim rows
+    const int base = blockIdx.x * blockDim.x * kNNRows + threadIdx.x;
+    double a = CUDART_INF;
+    if (active_inst(cs, 0)) {
+      double dzv[kNNRows], dsv[kNNRows];
+#pragma unroll
+      for (int k = 0; k < kNNRows; ++k) {
+        const int e = base + k * blockDim.x;
+        const bool in = e < cs.n_nn;
+        dzv[k] = in ? dz[cs.nn_begin + e] : 0.0;
+        dsv[k] = in ? ds[cs.nn_begin + e] : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < kNNRows; ++k) {
+        const int g = cs.nn_begin + base + k * blockDim.x;
+        if (dzv[k] < 0) a = fmin(a, -z[g] / dzv[k]);
+        if (dsv[k] < 0) a = fmin(a, -s[g] / dsv[k]);
+      }
+    }
+    block_seg_min_nonneg(alpha, a == CUDART_INF ? -1 : 0, a);
+    return;
+  }
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   int inst = -1;
   double a = CUDART_INF;
@@ -1253,10 +1287,7 @@ __global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
       inst = -1;
     }
   }
-  if (cs.B == 1)
-    block_seg_min_nonneg(alpha, inst, a);  // one problem: one atomic per block
-  else
-    seg_atomic_min_nonneg(alpha, inst, a);  // short per-instance segments
+  seg_atomic_min_nonneg(alpha, inst, a);  // short per-instance segments
 }
 
 // coneops_socone.jl:745-814 with group reductions
@@ -2192,7 +2223,8 @@ void cones_mul_Hs(const ConeSet &cs, double *y, const double *x, cudaStream_t st
 
 void cones_affine_ds(const ConeSet &cs, double *ds, const double *s, cudaStream_t st) {
   if (cs.n_zero) k_zero_fill<<<blocks_for(cs.n_zero), kBlock, 0, st>>>(cs, ds);
-  if (cs.n_nn) k_nn_affine_ds<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, ds);
+  if (cs.n_nn)
+    k_nn_affine_ds<<<blocks_for(cs.n_nn, nn_block(cs) * kNNRows), nn_block(cs), 0, st>>>(cs, ds);
   LAUNCH_SOC_SHAPED(kSocAffineDs, k_soc_tile_affine_ds, 1, k_soc_affine_ds, ds);
   if (cs.n_exp)
     k_nonsym_copy<<<blocks_for(3 * cs.n_exp), kBlock, 0, st>>>(cs, cs.n_exp, cs.exp_begin,
@@ -2234,7 +2266,9 @@ void cones_ds_from_dz_offset(const ConeSet &cs, double *out, const double *ds,
 void cones_step_length_sym(const ConeSet &cs, const double *dz, const double *ds,
                            const double *z, const double *s, double *alpha,
                            cudaStream_t st) {
-  if (cs.n_nn) k_nn_step<<<blocks_for(cs.n_nn, nn_block(cs)), nn_block(cs), 0, st>>>(cs, dz, ds, z, s, alpha);
+  if (cs.n_nn)
+    k_nn_step<<<blocks_for(cs.n_nn, nn_block(cs) * (cs.B == 1 ? kNNRows : 1)), nn_block(cs), 0,
+                st>>>(cs, dz, ds, z, s, alpha);
   LAUNCH_SOC_SHAPED(kSocStep, k_soc_tile_step, 4, k_soc_step, dz, ds, z, s, alpha);
   LAUNCH_PSD(k_psd_step, 4, cs, dz, ds, alpha);
 }
