@@ -413,3 +413,15 @@ extern "C" int clgpu_unit_initialization(clgpu_cones *h, double *z, double *s,
   cones_unit_initialization(h->cs, z, s, (cudaStream_t)stream);
   return finish((cudaStream_t)stream);
 }
+
+extern "C" int clgpu_debug_soc_tiles(const int *off, const int *dim, int n, int max_cones,
+                                     int max_rows, int *tiles, int cap) {
+  if (n < 0 || (n > 0 && (!off || !dim)) || max_cones < 1 || max_rows < 1 || cap < 0 ||
+      (cap > 0 && !tiles))
+    return -1;
+  std::vector<int> t = soc_tiles(off, dim, n, max_cones, max_rows);
+  const int nt = (int)t.size() / 2;
+  if (nt > cap) return -1;
+  for (size_t i = 0; i < t.size(); ++i) tiles[i] = t[i];
+  return nt;
+}

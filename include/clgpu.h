@@ -292,6 +292,14 @@ int clgpu_unit_initialization(clgpu_cones *h, double *z, double *s,
  * every index map, then factors a quasi-definite test matrix on the KKT
  * pattern and returns the solve residual.  No reference counterpart
  * (diagnostic); needs no GPU. */
+/* Host-only view of the SOC tiling (diagnostic, no reference counterpart):
+ * for n second-order cones with first rows off[k] and dimensions dim[k],
+ * writes the tiles the kernels would use for tiles of at most max_cones
+ * cones and max_rows rows as [c0, c1) pairs into tiles (room for cap
+ * pairs) and returns the number of tiles, or -1 on bad arguments or too
+ * little room.  Needs no GPU. */
+int clgpu_debug_soc_tiles(const int *off, const int *dim, int n, int max_cones,
+                          int max_rows, int *tiles, int cap);
 int clgpu_debug_check_instance(const clgpu_problem *prob,
                                const clgpu_settings *settings, double *resid);
 
