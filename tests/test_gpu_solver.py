@@ -7,6 +7,7 @@ import pytest
 
 import oracle
 from cuclarabel_b200 import BatchSolver, Solver, SolverStatus, problems
+from cuclarabel_b200.api import NonnegativeConeT, SecondOrderConeT, ZeroConeT
 from helpers import ITER_TOL, OBJ_RTOL, golden_cases, rel_err, to_cone_objects
 
 pytestmark = pytest.mark.gpu
@@ -210,3 +211,47 @@ def test_setup_autotuner_picks_valid_launch_shapes(cuda_device):
     assert _lib.load().clgpu_solver_get_launch_shapes(solver._h, ctypes.byref(nb), v) == 0
     assert nb.value in (128, 256, 512)
     assert all(0 <= x <= 3 for x in v)
+
+
+def test_full_mpc_batch_solutions_satisfy_kkt_on_the_host(cuda_device):
+    """Size-independent check at the benchmark's full size (4096 MPC
+    instances, seeds 0..4095): every instance the batch reports SOLVED has,
+    recomputed on the host from its returned x, s, z, small primal and dual
+    residuals and duality gap, s in the cone and z in the dual cone."""
+    import scipy.sparse as sp
+    pbs = problems.mpc_batch(4096, seed0=0)
+    solver = BatchSolver(pbs)
+    solver.solve_only()
+    res = solver.results()
+    xo = np.concatenate([[0], np.cumsum([pb[1].shape[0] for pb in pbs])])
+    mo = np.concatenate([[0], np.cumsum([pb[3].shape[0] for pb in pbs])])
+    solved = 0
+    for i, (P, q, A, b, cones) in enumerate(pbs):
+        if res["status"][i] != int(SolverStatus.SOLVED):
+            continue
+        solved += 1
+        x = res["x"][xo[i]:xo[i + 1]]
+        s = res["s"][mo[i]:mo[i + 1]]
+        z = res["z"][mo[i]:mo[i + 1]]
+        Pf = P + sp.triu(P, 1).T
+        Px, Ax = Pf @ x, A @ x
+        rp = np.abs(Ax + s - b).max() / (1 + max(np.abs(b).max(), np.abs(Ax).max(),
+                                                  np.abs(s).max()))
+        rd = np.abs(Px + q + A.T @ z).max() / (1 + max(np.abs(q).max(), np.abs(Px).max()))
+        pobj = 0.5 * x @ Px + q @ x
+        gap = abs(x @ Px + q @ x + b @ z) / (1 + abs(pobj))
+        assert rp < 1e-6 and rd < 1e-6 and gap < 1e-6, (i, rp, rd, gap)
+        r = 0
+        for c in cones:
+            d = c.nvars()
+            sc, zc = s[r:r + d], z[r:r + d]
+            scale = 1 + np.abs(sc).max() + np.abs(zc).max()
+            if isinstance(c, SecondOrderConeT):
+                assert sc[0] - np.linalg.norm(sc[1:]) >= -1e-8 * scale, (i, "s soc")
+                assert zc[0] - np.linalg.norm(zc[1:]) >= -1e-8 * scale, (i, "z soc")
+            elif isinstance(c, NonnegativeConeT):
+                assert sc.min() >= -1e-8 * scale and zc.min() >= -1e-8 * scale, (i, "nn")
+            elif isinstance(c, ZeroConeT):
+                assert np.abs(sc).max() <= 1e-8 * scale, (i, "zero")
+            r += d
+    assert solved >= 0.97 * len(pbs)
