@@ -223,10 +223,13 @@ int clgpu_cones_set_profiling(clgpu_cones *h, int enable);
  * CLGPU_SOC_SHAPED_OPS SOC operations update_scaling, affine_ds,
  * combined_ds_shift, Δs_from_Δz_offset, step_length and mul_Hs (in that
  * order), 0 = one lane group per cone or v = 1..3 = shared-memory tiles of
- * 32, 64 or 128 cones of dim <= 16.  clgpu_cones_create and clgpu_solver_create time the
- * candidates on their own cone layout and keep the fastest; every shape
- * gives the same results.  set: nn_block 0 keeps the current block size,
- * soc_variants NULL keeps the SOC variants; -1 on an invalid shape. */
+ * 32, 64 or 128 cones of dim <= 16.  clgpu_cones_create and
+ * clgpu_solver_create time the candidates on their own cone layout and keep
+ * the fastest (a few ms, with temporary device scratch of up to 160 MB plus
+ * five vectors of the cone rows, freed before they return; like the rest of
+ * set-up, call them outside stream capture); every shape gives the same
+ * results.  set: nn_block 0 keeps the current block size, soc_variants NULL
+ * keeps the SOC variants; -1 on an invalid shape. */
 #define CLGPU_SOC_SHAPED_OPS 6
 int clgpu_cones_get_launch_shapes(const clgpu_cones *h, int *nn_block, int *soc_variants);
 int clgpu_cones_set_launch_shapes(clgpu_cones *h, int nn_block, const int *soc_variants);
