@@ -88,6 +88,7 @@ EXPORTED = [
     "clgpu_cones_set_profiling", "clgpu_cones_last_kernel_ms",
     "clgpu_cones_get_launch_shapes", "clgpu_cones_set_launch_shapes",
     "clgpu_solver_get_launch_shapes", "clgpu_debug_soc_tiles",
+    "clgpu_solver_get_solution_views",
 ]
 
 
@@ -123,6 +124,8 @@ def _declare(L):
     L.clgpu_cones_set_launch_shapes.argtypes = [c_void_p, c_int, ip]
     L.clgpu_solver_get_launch_shapes.argtypes = [c_void_p, ip, ip]
     L.clgpu_debug_soc_tiles.argtypes = [ip, ip, c_int, c_int, c_int, ip, c_int]
+    L.clgpu_solver_get_solution_views.argtypes = [c_void_p, ctypes.POINTER(dp),
+                                                  ctypes.POINTER(dp), ctypes.POINTER(dp)]
     L.clgpu_cones_last_kernel_ms.argtypes = [c_void_p, dp]
     V = c_void_p  # device pointers are passed as integers
     L.clgpu_update_scaling.argtypes = [c_void_p, V, V, c_double, c_int, c_void_p]

@@ -408,14 +408,34 @@ class BatchSolver:
             raise RuntimeError("clgpu_solver_solve failed with code %d" % rc)
         return self.solutions()
 
-    def results(self, out=None):
+    def results(self, out=None, view=False):
         """The last solve's results as arrays (no per-instance objects): x, s,
         z concatenated over instances (offsets xoff / moff) and a structured
         array of the DefaultInfo fields, one row per instance.  `out` may be
         a previous return value of results(): its arrays are filled in place
-        (no new host allocation for repeated solves)."""
+        (no new host allocation for repeated solves).  view=True returns x,
+        s, z as read-only arrays over the library's pinned result staging,
+        without a copy; the next solve overwrites them."""
         L = _lib.load()
         B = len(self.dims)
+        if view:
+            px, ps, pz = _lib.dp(), _lib.dp(), _lib.dp()
+            rc = L.clgpu_solver_get_solution_views(self._h, ctypes.byref(px), ctypes.byref(ps),
+                                                   ctypes.byref(pz))
+            if rc != 0:
+                raise RuntimeError("clgpu_solver_get_solution_views failed with code %d" % rc)
+            infos = out["_infos"] if out is not None else (_lib.ClgpuInfo * B)()
+            rc = L.clgpu_solver_get_solutions(self._h, None, None, None, infos)
+            if rc != 0:
+                raise RuntimeError("clgpu_solver_get_solutions failed with code %d" % rc)
+            arrs = []
+            for p, n in ((px, self.nx), (ps, self.mz), (pz, self.mz)):
+                a = np.ctypeslib.as_array(p, shape=(max(n, 1),))[:n]
+                a.flags.writeable = False
+                arrs.append(a)
+            info = np.ctypeslib.as_array(infos)
+            return {"x": arrs[0], "s": arrs[1], "z": arrs[2], "info": info,
+                    "status": info["status"].copy(), "_infos": infos}
         if out is not None:
             x, s, z = out["x"], out["s"], out["z"]
             for a, n in ((x, self.nx), (s, self.mz), (z, self.mz)):

@@ -2743,6 +2743,14 @@ extern "C" int clgpu_solver_get_launch_shapes(const clgpu_solver *h, int *nn_blo
     for (int op = 0; op < kSocOps; ++op) soc_variants[op] = h->cs.soc_variant[op];
   return 0;
 }
+extern "C" int clgpu_solver_get_solution_views(const clgpu_solver *h, const double **x,
+                                               const double **s, const double **z) {
+  if (!h || !h->solved || !h->h_sol) return -1;
+  if (x) *x = h->h_sol;
+  if (s) *s = h->h_sol + h->nx;
+  if (z) *z = h->h_sol + h->nx + h->mz;
+  return 0;
+}
 extern "C" long long clgpu_solver_device_bytes(const clgpu_solver *h) {
   return h ? h->arena.bytes : -1;
 }

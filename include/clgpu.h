@@ -128,6 +128,12 @@ int clgpu_solver_get_solution(clgpu_solver *h, int inst, double *x, double *s,
  * info array of nprob entries; any pointer may be NULL */
 int clgpu_solver_get_solutions(clgpu_solver *h, double *x, double *s,
                                double *z, clgpu_info *info);
+/* The same x / s / z without a copy: pointers into the handle's pinned host
+ * staging, which the next solve overwrites (no reference counterpart; the
+ * reference's solver.solution is likewise refilled by every solve!).  Any
+ * pointer may be NULL; -1 before the first solve. */
+int clgpu_solver_get_solution_views(const clgpu_solver *h, const double **x,
+                                    const double **s, const double **z);
 /* update_data! for every instance (src/data_updating.jl:26-120): new values
  * with the sparsity given at setup, concatenated over the instances in
  * instance order, HOST pointers -- Px: the entries of each instance's P in

@@ -255,3 +255,16 @@ def test_full_mpc_batch_solutions_satisfy_kkt_on_the_host(cuda_device):
                 assert np.abs(sc).max() <= 1e-8 * scale, (i, "zero")
             r += d
     assert solved >= 0.97 * len(pbs)
+
+
+def test_result_views_match_copies(cuda_device):
+    """results(view=True) shows the same x, s, z as the copying form,
+    read-only, over the library's pinned staging."""
+    solver = BatchSolver(problems.mpc_batch(6, seed0=40))
+    solver.solve_only()
+    v = solver.results(view=True)
+    c = solver.results()
+    for k in ("x", "s", "z", "status"):
+        assert np.array_equal(v[k], c[k])
+    assert not v["x"].flags.writeable
+    assert np.array_equal(v["info"]["obj_val"], c["info"]["obj_val"])
