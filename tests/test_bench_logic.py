@@ -40,3 +40,33 @@ def test_cone_op_bytes_per_element_and_cone():
     assert bench.cone_op_bytes("step_length", 4, 3, 2) == 2 * 104
     # PSD(10): svec 55 entries, R and R^-1 100 entries each, lambda 10
     assert bench.cone_op_bytes("update_scaling", 5, 10, 1) == 16 * 55 + 16 * 100 + 8 * 10
+
+
+def test_cone_roofline_points_are_interior():
+    """The cone-kernel workload's s and z are strictly inside their cones
+    (and the power cones' z inside the dual cone for the same alphas)."""
+    rng = np.random.default_rng(3)
+    v, _ = bench.cone_points(1, 1000, 1, rng)
+    assert v.min() > 0
+    v, _ = bench.cone_points(2, 10, 500, rng)
+    V = v.reshape(-1, 10)
+    assert np.all(V[:, 0] > np.linalg.norm(V[:, 1:], axis=1))
+    v, _ = bench.cone_points(3, 3, 500, rng)
+    x, y, z = v.reshape(-1, 3).T
+    assert np.all(y > 0) and np.all(y * np.exp(x / y) < z)            # primal exp cone
+    assert np.all(x < 0) and np.all(-x * np.exp(y / x) < np.e * z)     # dual exp cone
+    s, a = bench.cone_points(4, 3, 500, rng)
+    zz, _ = bench.cone_points(4, 3, 500, rng, a)
+    S, Z = s.reshape(-1, 3), zz.reshape(-1, 3)
+    assert np.all(S[:, 0] ** a * S[:, 1] ** (1 - a) > np.abs(S[:, 2]))
+    assert np.all((Z[:, 0] / a) ** a * (Z[:, 1] / (1 - a)) ** (1 - a) > np.abs(Z[:, 2]))
+    v, _ = bench.cone_points(5, 10, 50, rng)
+    n, t = 10, 55
+    ii, jj = np.triu_indices(n)
+    order = np.lexsort((ii, jj))  # svec: column by column, upper triangle
+    for x in v.reshape(-1, t):
+        M = np.zeros((n, n))
+        vals = x / np.where(ii[order] == jj[order], 1.0, np.sqrt(2.0))
+        M[ii[order], jj[order]] = vals
+        M = M + np.triu(M, 1).T
+        assert np.linalg.eigvalsh(M).min() > 0
