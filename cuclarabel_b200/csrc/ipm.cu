@@ -25,6 +25,7 @@
 #include "cones.cuh"
 #include "devbuf.hpp"
 #include "ldl.cuh"
+#include "sn_exec.cuh"
 #include "setup.hpp"
 
 namespace clgpu {
@@ -813,6 +814,8 @@ struct clgpu_solver {
   int *h_counter = nullptr;  // pinned
   std::vector<int> h_n, h_m, h_xoff, h_moff;
   bool any_asym = false, any_sym = false;
+  bool any_sn = false;                // class-3 (supernodal) instances present
+  std::unique_ptr<SnExec> sn;         // their factorisation
   std::vector<clgpu_info> info;
   double *h_sol = nullptr;  // pinned host copy of x, s, z (concatenated), nx + 2*mz
   bool solved = false;
@@ -1350,8 +1353,10 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     const bool fits = (long long)N[i] * tsize <= 48 * 1024 &&
                       (long long)prep[i].Li.size() <= (long long)kStartMask &&
                       (long long)prep[i].Kj.size() <= (long long)kStartMask;
-    cls[i] = fits ? 1 : 2;
-    if (fits) {
+    cls[i] = prep[i].supernodal ? 3 : (fits ? 1 : 2);
+    if (cls[i] == 3) {
+      h->any_sn = true;
+    } else if (fits) {
       has_small = true;
       max_small = std::max(max_small, N[i]);
     } else {
@@ -1842,6 +1847,29 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     }
   }
   kk.cls = A.upload(cls);
+  // ---------------- supernodal instances: plan and numeric storage
+  kk.sn = nullptr;
+  if (h->any_sn) {
+    std::vector<SnInstance> sin;
+    int vlo = VT, vhi = 0;
+    for (int i = 0; i < B; ++i)
+      if (cls[i] == 3) {
+        sin.push_back({&prep[i].sym, prep[i].Kp.data(), prep[i].Kj.data(), kof[i], voff[i], i});
+        vlo = std::min(vlo, voff[i]);
+        vhi = std::max(vhi, voff[i + 1]);
+      }
+    SnPlan plan;
+    std::string err;
+    if (!sn_build_plan(sin, plan, &err)) return -4;
+    std::vector<int> vinst(vhi - vlo, -1);
+    for (int i = 0; i < B; ++i)
+      if (cls[i] == 3)
+        for (int v = voff[i]; v < voff[i + 1]; ++v) vinst[v - vlo] = i;
+    h->sn.reset(new SnExec());
+    if (!sn_exec_create(plan, h->mixed, B, vlo, vhi - vlo, vinst, A, *h->sn)) return -5;
+    kk.sn = h->sn.get();
+    mark("supernodal plan");
+  }
   // pack single-warp solves into blocks of kSolveWarps warps: each warp needs
   // its work vector (N FP64 values) and its ring (entries + FP64 values);
   // bins sized so kSolveBlocksPerSM blocks fit an SM's shared memory
@@ -2321,7 +2349,7 @@ static int ipm_pass(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed, 
                     int *nfin) {
   Dev &dv = h->dv;
   const int B = h->B;
-  const bool graph = h->use_graphs && !h->any_asym && !h->profiling && !h->st.verbose &&
+  const bool graph = h->use_graphs && !h->any_asym && !h->any_sn && !h->profiling && !h->st.verbose &&
                      !std::isfinite(h->st.time_limit) && h->mask_sel == nullptr;
   bool done = false;
   if (graph) {

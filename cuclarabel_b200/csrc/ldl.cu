@@ -37,6 +37,7 @@
 // substitution arithmetic, the refinement residual and the iterate are FP64.
 #include <type_traits>
 #include "ldl.cuh"
+#include "sn_exec.cuh"
 
 namespace clgpu {
 
@@ -1229,6 +1230,7 @@ void ldl_factor(const KKTDev &k, bool fp32, const LDLParams &p, const int *run, 
     launch_factor<float>(k, p, run, ok, eps_out, st);
   else
     launch_factor<double>(k, p, run, ok, eps_out, st);
+  if (k.sn) sn_factor(*k.sn, k, p, run, ok, eps_out, st);
 }
 
 void ldl_solve(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
@@ -1239,6 +1241,7 @@ void ldl_solve(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
     launch_solve<float>(k, p, run, rx, rz, lx, lz, ok, st);
   else
     launch_solve<double>(k, p, run, rx, rz, lx, lz, ok, st);
+  if (k.sn) sn_solve(*k.sn, k, p, run, rx, rz, lx, lz, ok, st);
 }
 
 void ldl_solve2(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
@@ -1250,6 +1253,10 @@ void ldl_solve2(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
     launch_solve2<float>(k, p, run, rx0, rz0, lx0, lz0, rx1, rz1, lx1, lz1, ok, st);
   else
     launch_solve2<double>(k, p, run, rx0, rz0, lx0, lz0, rx1, rz1, lx1, lz1, ok, st);
+  if (k.sn) {
+    sn_solve(*k.sn, k, p, run, rx0, rz0, lx0, lz0, ok, st);
+    sn_solve(*k.sn, k, p, run, rx1, rz1, lx1, lz1, ok, st);
+  }
 }
 
 }  // namespace clgpu

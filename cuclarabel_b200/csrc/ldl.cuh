@@ -11,6 +11,8 @@
 
 namespace clgpu {
 
+struct SnExec;
+
 struct KKTDev {
   int B;
   const int *N;     // [B] KKT dimension of each instance
@@ -96,8 +98,12 @@ struct KKTDev {
   // solves [2B, 3B) of the profiled solve
   double *prof_bytes;
   // [B] kernel class: 1 = single warp (work vector in shared memory, the
-  // streams above), 2 = block kernels with global scratch
+  // streams above), 2 = block kernels with global scratch, 3 = supernodal
+  // (sn below; no scalar factor structures)
   const int *cls;
+  // supernodal factorisation of the class-3 instances (host object; null
+  // when there are none)
+  SnExec *sn;
   int max_small_N;       // largest N among single-warp (shared memory) instances
   int has_small, has_large;
   int has_small_legacy;  // single-warp instances without a streamed factorisation

@@ -643,7 +643,14 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
         adjncy[cur[en.r]++] = en.c;
         adjncy[cur[en.c]++] = en.r;
       }
-    out.perm = nd_order_csr(N, xadj, adjncy);
+    // instances whose work vector exceeds the single-warp kernels' budget
+    // (48 KB of FP64) take the supernodal factorisation
+    out.supernodal = (long long)N * 8 > 48 * 1024;
+    if (out.supernodal) {
+      if (!sn_analyse(N, xadj, adjncy, out.perm, out.sym, &out.error)) return false;
+    } else {
+      out.perm = nd_order_csr(N, xadj, adjncy);
+    }
   }
   out.iperm.assign(N, 0);
   for (int k = 0; k < N; ++k) out.iperm[out.perm[k]] = k;
@@ -708,8 +715,13 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     if (o >= n + m) sgn = ((o - n - m) % 2 == 0) ? -1 : 1;
     out.Dsign[out.iperm[o]] = sgn;
   }
-  // ---- symbolic LDL^T on the permuted matrix
-  {
+  // ---- symbolic LDL^T on the permuted matrix (scalar structures; the
+  // supernodal instances have theirs from sn_analyse)
+  if (out.supernodal) {
+    out.Lp.assign(N + 1, 0);
+    out.Rp.assign(N + 1, 0);
+    out.lvl_ptr.assign(1, 0);
+  } else {
     std::vector<int> parent(N, -1), Lnz(N, 0), work(N, -1);
     for (int k = 0; k < N; ++k) {
       work[k] = k;
@@ -885,6 +897,82 @@ extern "C" int clgpu_debug_check_instance(const clgpu_problem *pb, const clgpu_s
     if (p.Kdiag[r] < p.Kp[r] || p.Kdiag[r] >= p.Kp[r + 1]) return -11;
     for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q)
       if (p.Kj[q] < 0 || p.Kj[q] >= N || (q > p.Kp[r] && p.Kj[q] <= p.Kj[q - 1])) return -12;
+  }
+  if (p.supernodal) {
+    // supernodal instance: build its device plan and replay the multifrontal
+    // factorisation and solve on a quasi-definite test matrix
+    auto inK0 = [&](int v) { return v == -1 || (v >= 0 && v < knz); };
+    for (int v : p.nn_pos) if (!inK0(v) || v < 0) return -16;
+    for (int v : p.socd_pos) if (!inK0(v)) return -17;
+    for (int v : p.socs_uv) if (!inK0(v)) return -19;
+    SnPlan plan;
+    std::string err;
+    std::vector<SnInstance> in{{&p.sym, p.Kp.data(), p.Kj.data(), 0, 0, 0}};
+    if (!sn_build_plan(in, plan, &err)) return -30;
+    for (size_t q = 0; q < plan.amap.size(); ++q) {
+      const SnPair a = plan.amap[q];
+      if (a.x < 0 || a.x >= knz) return -31;
+    }
+    for (int s = 0; s < plan.ns; ++s) {
+      const long long ld = plan.ld[s];
+      for (int q = plan.acol[plan.cbase[s]]; q < plan.acol[plan.cbase[s] + plan.ncol[s]]; ++q) {
+        const int off = plan.amap[q].y, r = off % (int)ld, c = off / (int)ld;
+        if (c >= plan.ncol[s] || r < c || r >= ld) return -32;
+      }
+      for (int k = 0; k < plan.nrow[s]; ++k) {
+        const int* fi = plan.fidx.data() + plan.fix_off[s];
+        if (fi[plan.u0[s] + k] < 0 || fi[plan.u0[s] + k] >= N) return -33;
+      }
+    }
+    // children: relative indices strictly increasing, inside the parent's
+    // front and never on its dummy or padding positions
+    for (int s = 0; s < plan.ns; ++s)
+      for (int a = plan.ch_ptr[s]; a < plan.ch_ptr[s + 1]; ++a) {
+        const int c = plan.ch[a];
+        const int *rel = plan.rel.data() + plan.rel_off[c];
+        const int *fi = plan.fidx.data() + plan.fix_off[s];
+        for (int k = 0; k < plan.nrow[c]; ++k) {
+          if (rel[k] < 0 || rel[k] >= plan.ld[s] || fi[rel[k]] < 0) return -34;
+          if (k > 0 && rel[k] <= rel[k - 1]) return -35;
+        }
+      }
+    // every launch's tasks inside the task list, tiles inside their fronts
+    for (auto *sched : {&plan.fact, &plan.fwd, &plan.bwd})
+      for (const SnLaunch &L : *sched) {
+        if (L.begin < 0 || L.count <= 0 || (size_t)L.begin + L.count > plan.tasks.size()) return -36;
+        for (int q = L.begin; q < L.begin + L.count; ++q) {
+          const SnQuad t = plan.tasks[q];
+          if (t.x < 0 || t.x >= plan.ns) return -37;
+          const int ld = plan.ld[t.x], k0 = t.y & 0xffff, K = t.y >> 16;
+          if (L.kind == SN_DIAG || L.kind == SN_TRSM || L.kind == SN_UPDATE ||
+              L.kind == SN_FWD_DIAG || L.kind == SN_FWD_GEMV || L.kind == SN_BWD_PARTIAL ||
+              L.kind == SN_BWD_DIAG) {
+            if (!plan.large[t.x] || K <= 0 || K > kSnNB || K % kSnKPad || k0 + K > plan.u0[t.x])
+              return -38;
+            if ((L.kind == SN_TRSM || L.kind == SN_UPDATE || L.kind == SN_FWD_GEMV ||
+                 L.kind == SN_BWD_PARTIAL) &&
+                (t.z < k0 + K || t.z + kSnNB > ld || (t.z - k0 - K) % kSnNB))
+              return -39;
+            if (L.kind == SN_UPDATE && (t.w < k0 + K || t.w > t.z || (t.w - k0 - K) % kSnNB))
+              return -40;
+          }
+          if (L.kind == SN_ASSEMBLE && (t.y < 0 || t.z > ld || t.y >= t.z)) return -41;
+          if ((L.kind == SN_SMALL_FACTOR || L.kind == SN_FWD_SMALL || L.kind == SN_BWD_SMALL) &&
+              (plan.large[t.x] || ld > kSnSmallMax))
+            return -42;
+        }
+      }
+    std::vector<double> Kx(knz, 0.0);
+    for (int r = 0; r < N; ++r)
+      for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) {
+        int c = p.Kj[q];
+        if (c != r) Kx[q] = 0.01 * std::sin(1.0 + r + 7.0 * c) * std::sin(1.0 + c + 7.0 * r);
+      }
+    for (int r = 0; r < N; ++r) Kx[p.Kdiag[r]] = p.Dsign[r] * 2.0;
+    std::vector<int> voff{0, N};
+    const double res = sn_host_check(plan, p.Kp, p.Kj, Kx, p.Dsign, voff, 1e-7);
+    if (resid) *resid = res;
+    return 0;
   }
   if ((int)p.Lp.size() != N + 1 || p.Lp[N] != lnz || (int)p.Rp.size() != N + 1) return -13;
   for (int j = 0; j < N; ++j)

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/clgpu.h"
+#include "supernodal.hpp"
 
 namespace clgpu {
 
@@ -47,6 +48,12 @@ struct Prepared {
   std::vector<signed char> Dsign;  // permuted
   std::vector<int> Lp, Li, Rp, Rk, Rpos;
   std::vector<int> lvl_ptr, lvl_nodes;  // elimination-tree levels (leaves first)
+  // Large instances (work vector beyond the single-warp kernels' budget)
+  // take the supernodal factorisation: AMD ordering, supernodal symbolic
+  // structure in sym, and no scalar structures (Lp, Rp zero, Li, Rk, Rpos
+  // and the levels empty).
+  bool supernodal = false;
+  SnSymbolic sym;
   // refresh positions (local CSR positions)
   std::vector<int> nn_pos;                   // per NN row (type-major order)
   std::vector<int> socd_pos;                 // dense SOC triu pairs (concat over cones)
@@ -88,5 +95,9 @@ std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj);
 // the same on a CSR graph (repeated neighbours allowed; rows are sorted and
 // deduplicated in place)
 std::vector<int> nd_order_csr(int n, std::vector<int> &xadj, std::vector<int> &adjncy);
+// approximate minimum degree on the quotient graph (amd.cpp): the
+// fill-reducing ordering of the supernodal factorisation; CSR graph,
+// repeated neighbours and self loops allowed; same contract as amd_order
+std::vector<int> amd_order_qg(int n, const std::vector<int> &xadj, const std::vector<int> &adj);
 
 }  // namespace clgpu

@@ -1,0 +1,63 @@
+"""The large single problems (configurations 2 and 3) on the supernodal
+LDL^T: instances whose KKT work vector exceeds the single-warp kernels'
+budget (N > 6144) are factored by dense fronts, level by level.
+
+Parity with the CPU oracle at the largest scales the oracle finishes in
+about a minute: same status, objective within 1e-7 relative, residuals
+below tol_feas, iterations within +-2 (the bar of test_gpu_solver.py)."""
+import numpy as np
+import pytest
+
+import oracle
+from cuclarabel_b200 import Solver, SolverStatus, problems
+from helpers import ITER_TOL, OBJ_RTOL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def check_parity(sol, ref, name=""):
+    assert sol.status.name == ref["status_name"], (name, sol.status.name, ref["status_name"])
+    assert abs(sol.iterations - ref["iterations"]) <= ITER_TOL, (name, sol.iterations,
+                                                                 ref["iterations"])
+    if sol.status == SolverStatus.SOLVED:
+        assert rel_err(sol.obj_val, ref["obj_val"]) < OBJ_RTOL, (name, sol.obj_val,
+                                                                ref["obj_val"])
+        assert sol.r_prim < 1e-8 and sol.r_dual < 1e-8
+    else:
+        assert rel_err(sol.obj_val, ref["obj_val"]) < 1e-5, (name, sol.obj_val, ref["obj_val"])
+
+
+def test_mixed_socp_supernodal(cuda_device):
+    """Configuration 2 at 10 % (KKT dimension 8600)."""
+    pb = problems.mixed_socp(scale=0.1, seed=2)
+    sol = Solver(*pb).solve()
+    check_parity(sol, oracle.solve(*pb, gpu_equilibration=1), "mixed_socp 10%")
+
+
+def test_exp_pow_psd_supernodal(cuda_device):
+    """Configuration 3 at 5 % (KKT dimension 6300: exp, pow, PSD(10), nonneg)."""
+    pb = problems.exp_pow_psd(scale=0.05, seed=3)
+    sol = Solver(*pb).solve()
+    check_parity(sol, oracle.solve(*pb, gpu_equilibration=1), "exp_pow_psd 5%")
+
+
+def test_supernodal_repeat_solve_is_identical(cuda_device):
+    """Every reduction runs in a fixed order: a second solve repeats the
+    first bit for bit."""
+    pb = problems.mixed_socp(scale=0.08, seed=5)
+    s = Solver(*pb)
+    a = s.solve()
+    b = s.solve()
+    assert a.status == b.status and a.iterations == b.iterations
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.z, b.z)
+
+
+def test_supernodal_mixed_precision(cuda_device):
+    """:cudssmixed on the supernodal path: FP32 fronts (factorisation and
+    substitutions read FP32), FP64 iterative refinement; the error against
+    the FP64 oracle is reported by the objective."""
+    pb = problems.mixed_socp(scale=0.1, seed=2)
+    ref = oracle.solve(*pb, gpu_equilibration=1)
+    sol = Solver(*pb, direct_solve_method="cudssmixed").solve()
+    assert sol.status in (SolverStatus.SOLVED, SolverStatus.ALMOST_SOLVED), sol.status
+    assert rel_err(sol.obj_val, ref["obj_val"]) < 1e-6, (sol.obj_val, ref["obj_val"])
