@@ -338,6 +338,17 @@ def _nvars(spec):
     return 3 if t in (3, 4) else (d * (d + 1) // 2 if t == 5 else d)
 
 
+class _StagingView:
+    """Read-only array interface over n doubles of a solver's pinned result
+    staging.  numpy keeps this object as the array's base, and it keeps the
+    solver: the staging (freed by clgpu_solver_destroy) outlives every view."""
+
+    def __init__(self, addr, n, owner):
+        self._owner = owner
+        self.__array_interface__ = {"shape": (n,), "typestr": "<f8", "version": 3,
+                                    "data": (addr, True)}
+
+
 class BatchSolver:
     """Many independent problems solved in one lock-step device loop."""
 
@@ -415,7 +426,8 @@ class BatchSolver:
         a previous return value of results(): its arrays are filled in place
         (no new host allocation for repeated solves).  view=True returns x,
         s, z as read-only arrays over the library's pinned result staging,
-        without a copy; the next solve overwrites them."""
+        without a copy; the next solve overwrites them, and each array keeps
+        the solver (and so the staging) alive while it exists."""
         L = _lib.load()
         B = len(self.dims)
         if view:
@@ -430,9 +442,13 @@ class BatchSolver:
                 raise RuntimeError("clgpu_solver_get_solutions failed with code %d" % rc)
             arrs = []
             for p, n in ((px, self.nx), (ps, self.mz), (pz, self.mz)):
-                a = np.ctypeslib.as_array(p, shape=(max(n, 1),))[:n]
-                a.flags.writeable = False
-                arrs.append(a)
+                if n == 0:
+                    a = np.empty(0)
+                    a.flags.writeable = False
+                    arrs.append(a)
+                    continue
+                addr = ctypes.cast(p, ctypes.c_void_p).value
+                arrs.append(np.asarray(_StagingView(addr, n, self)))
             info = np.ctypeslib.as_array(infos)
             return {"x": arrs[0], "s": arrs[1], "z": arrs[2], "info": info,
                     "status": info["status"].copy(), "_infos": infos}

@@ -1516,14 +1516,21 @@ __global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z) {
   if (!p.valid) return;
   int n = p.n, nm = cs.psd_nmax;
   double *Z = psd_smem(nm, 2), *ev = Z + nm * nm;
-  if (n == 0) return;
+  const int slot = cs.n_soc + cs.n_exp + cs.n_pow + p.c;
+  if (n == 0) {
+    // an empty cone: (floatmax, 0), coneops_psdtrianglecone.jl:16-19
+    if (p.lane == 0) {
+      cs.cone_tmp[slot] = kDMax;
+      cs.cone_tmp2[slot] = 0.0;
+    }
+    return;
+  }
   svec_to_mat(n, z + p.off, Z, p.lane);
   __syncwarp();
   double mn = warp_eig_min(n, Z, ev, p.lane);
   double pos = (p.lane < n && ev[p.lane] > 0) ? ev[p.lane] : 0.0;
   pos = warp_sum(pos);
   if (p.lane == 0) {
-    const int slot = cs.n_soc + cs.n_exp + cs.n_pow + p.c;
     cs.cone_tmp[slot] = mn;
     cs.cone_tmp2[slot] = pos;
   }

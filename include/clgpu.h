@@ -282,7 +282,9 @@ int clgpu_margins(clgpu_cones *h, const double *z, int pd, double *alpha,
  * most CLGPU_MARGINS_STATIC_MAX_CONES second-order plus PSD cones are
  * accepted (CLGPU_ERR_STATIC_TOO_LARGE above that).  The first call on each
  * device looks up that array's address and should come before any stream
- * capture.  The array is shared per device: overlapping calls race. */
+ * capture.  Every call is synchronous: it copies the layout through host
+ * staging, synchronises the stream and reads the two results back before it
+ * returns.  The array is shared per device: overlapping calls race. */
 #define CLGPU_MARGINS_STATIC_MAX_CONES 32768
 #define CLGPU_ERR_STATIC_TOO_LARGE (-20)
 int clgpu_margins_static(int ncones, const int *types, const int *dims,

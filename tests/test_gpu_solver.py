@@ -268,3 +268,23 @@ def test_result_views_match_copies(cuda_device):
         assert np.array_equal(v[k], c[k])
     assert not v["x"].flags.writeable
     assert np.array_equal(v["info"]["obj_val"], c["info"]["obj_val"])
+
+
+def test_result_views_keep_the_solver_alive(cuda_device):
+    """A view outlives the last user reference to its solver: the solver (and
+    with it the pinned staging the view reads) is released only after every
+    view is gone."""
+    import gc
+    import weakref
+    solver = BatchSolver(problems.mpc_batch(4, seed0=44))
+    solver.solve_only()
+    expect = solver.results()["x"].copy()
+    v = solver.results(view=True)
+    ref = weakref.ref(solver)
+    del solver
+    gc.collect()
+    assert ref() is not None
+    assert np.array_equal(v["x"], expect)
+    del v
+    gc.collect()
+    assert ref() is None

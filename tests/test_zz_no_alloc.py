@@ -19,7 +19,7 @@ ERR_TOO_LARGE = -20      # CLGPU_ERR_STATIC_TOO_LARGE
 
 LAYOUTS = {
     "mixed": [(0, 2, 0.0), (1, 5, 0.0), (2, 3, 0.0), (2, 8, 0.0), (3, 3, 0.0), (4, 3, 0.4),
-              (5, 4, 0.0), (5, 3, 0.0)],
+              (5, 4, 0.0), (5, 0, 0.0), (5, 3, 0.0)],
     "many_soc": [(1, 40, 0.0)] + [(2, 3 + (k % 9), 0.0) for k in range(300)],
     "psd_only": [(5, 10, 0.0), (5, 2, 0.0), (5, 16, 0.0)],
     "nn_only": [(1, 1000, 0.0)],
@@ -116,3 +116,25 @@ def test_static_margins_rejects_oversize_layout(cuda_device):
                                 zt.data_ptr(), 0, ctypes.byref(a), ctypes.byref(b), None)
     assert rc == 0
     assert a.value == 0.0 and b.value == 0.0  # z = 0: every SOC margin is 0
+
+
+def test_empty_psd_cone_leaves_margins_unchanged(cuda_device):
+    """An empty PSD cone contributes (floatmax, 0) (the reference's
+    coneops_psdtrianglecone.jl:16-19), so inserting one changes neither
+    margin -- also right after a call that left other values in the shared
+    scratch slot the empty cone occupies."""
+    import torch
+    L = _lib.load()
+    with_empty = [(1, 3, 0.0), (5, 3, 0.0), (5, 0, 0.0), (5, 2, 0.0)]
+    without = [(1, 3, 0.0), (5, 3, 0.0), (5, 2, 0.0)]
+    rng = np.random.default_rng(9)
+    z = torch.tensor(rng.standard_normal(sum(_rows(s) for s in without)), dtype=torch.float64,
+                     device="cuda")
+    zp = torch.tensor(rng.standard_normal(sum(_rows(s) for s in LAYOUTS["psd_only"])),
+                      dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for pd in (0, 1):
+        _static_margins(L, LAYOUTS["psd_only"], zp, pd, stream)  # leaves PSD values behind
+        ref = _handle_margins(L, without, z, pd)
+        assert _static_margins(L, with_empty, z, pd, stream) == ref
+        assert _handle_margins(L, with_empty, z, pd) == ref
