@@ -89,6 +89,9 @@ EXPORTED = [
     "clgpu_cones_get_launch_shapes", "clgpu_cones_set_launch_shapes",
     "clgpu_solver_get_launch_shapes", "clgpu_debug_soc_tiles",
     "clgpu_solver_get_solution_views",
+    "clgpu_mul_Hs_diag", "clgpu_rectify_equilibration", "clgpu_refresh_kkt",
+    "clgpu_step_length_device", "clgpu_ldl_create", "clgpu_ldl_refactor", "clgpu_ldl_solve",
+    "clgpu_ldl_destroy", "clgpu_residuals", "clgpu_residuals_work_len", "clgpu_add_step",
 ]
 
 
@@ -144,6 +147,20 @@ def _declare(L):
     L.clgpu_unit_initialization.argtypes = [c_void_p, V, V, c_void_p]
     L.clgpu_debug_check_instance.argtypes = [ctypes.POINTER(ClgpuProblem),
                                              ctypes.POINTER(ClgpuSettings), dp]
+    # KKT-level boundary (device pointers as integers)
+    L.clgpu_mul_Hs_diag.argtypes = [c_void_p, V, V, c_void_p]
+    L.clgpu_rectify_equilibration.argtypes = [c_void_p, V, V, ip, c_void_p]
+    L.clgpu_refresh_kkt.argtypes = [c_void_p, V, V, V, V, V, V, c_void_p]
+    L.clgpu_step_length_device.argtypes = [c_void_p, V, V, V, V, V, c_double, c_double,
+                                           c_double, V, c_void_p]
+    L.clgpu_ldl_create.argtypes = [c_int, ip, ip, ctypes.POINTER(ctypes.c_byte),
+                                   ctypes.POINTER(ClgpuSettings), ctypes.POINTER(c_void_p)]
+    L.clgpu_ldl_refactor.argtypes = [c_void_p, V, dp, c_void_p]
+    L.clgpu_ldl_solve.argtypes = [c_void_p, V, V, c_void_p]
+    L.clgpu_ldl_destroy.argtypes = [c_void_p]
+    L.clgpu_residuals.argtypes = [c_int, c_int] + [V] * 9 + [V] * 7 + [V] * 7 + [c_void_p]
+    L.clgpu_residuals_work_len.argtypes = []
+    L.clgpu_add_step.argtypes = [c_int, c_int] + [V] * 11 + [c_void_p]
 
 
 def load():

@@ -20,6 +20,9 @@ struct clgpu_cones {
       *d_psd_blk = nullptr;
   double *d_scal = nullptr;  // small scalar workspace [8]
   int *d_iscal = nullptr;    // [4]
+  double *d_save = nullptr;  // [soc_rows] rows kept by mul_Hs_diag
+  double *d_hs = nullptr;    // [hs_len] Hs blocks for refresh_kkt
+  int n_sparse = 0, sparse_rows = 0;
   // kernel-time profiling: events around an operation's launches only
   bool prof = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -200,6 +203,13 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
   h->d_psd_blk = A.upload(psd_blk);
   h->d_scal = A.alloc<double>(8);
   h->d_iscal = A.alloc<int>(4);
+  h->d_save = A.alloc<double>(cs.soc_rows);
+  h->d_hs = A.alloc<double>(blk);
+  for (size_t c = 0; c < soc_sparse.size(); ++c)
+    if (soc_sparse[c]) {
+      h->n_sparse++;
+      h->sparse_rows += soc_dim[c];
+    }
   int one = 1;
   cudaMemcpy(h->d_iscal + 2, &one, sizeof(int), cudaMemcpyHostToDevice);  // bt active
   if (A.err != cudaSuccess) {
@@ -258,6 +268,11 @@ extern "C" int clgpu_cones_last_kernel_ms(const clgpu_cones *h, double *ms) {
   if (!h || !ms) return -1;
   *ms = h->last_ms;
   return 0;
+}
+
+__global__ void k_fill(double *v, int n, double a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = a;
 }
 
 static int finish(cudaStream_t st) {
@@ -412,6 +427,154 @@ extern "C" int clgpu_unit_initialization(clgpu_cones *h, double *z, double *s,
   if (!h) return -1;
   cones_unit_initialization(h->cs, z, s, (cudaStream_t)stream);
   return finish((cudaStream_t)stream);
+}
+
+// ------------------------------------------------ KKT-level cone operations
+// Rows of the sparse (expanded) second-order cones: dir 0 saves y there,
+// dir 1 puts the saved values back.
+__global__ void k_sparse_soc_rows(ConeSet cs, double *y, double *save, int dir) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cs.n_soc || !cs.soc_sparse[c]) return;
+  const int off = cs.soc_off[c], d = cs.soc_dim[c];
+  for (int i = 0; i < d; ++i) {
+    if (dir == 0)
+      save[off + i - cs.soc_begin] = y[off + i];
+    else
+      y[off + i] = save[off + i - cs.soc_begin];
+  }
+}
+
+extern "C" int clgpu_mul_Hs_diag(clgpu_cones *h, double *y, const double *x,
+                                 clgpu_stream_t stream) {
+  if (!h || (h->numel > 0 && (!y || !x))) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (h->cs.n_soc + 127) / 128;
+  if (h->n_sparse) k_sparse_soc_rows<<<nb, 128, 0, st>>>(h->cs, y, h->d_save, 0);
+  cones_mul_Hs(h->cs, y, x, st);
+  if (h->n_sparse) k_sparse_soc_rows<<<nb, 128, 0, st>>>(h->cs, y, h->d_save, 1);
+  return finish(st);
+}
+
+// delta = mean(e over the cone) / e for every cone without elementwise
+// scaling (second-order, exponential, power, PSD), 1 elsewhere
+// (rectify_equilibration!, coneops_compositecone_gpu.jl:21-39 and
+// mathutils_gpu.jl:41-55)
+__global__ void k_rectify(ConeSet cs, double *delta, const double *e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nrec = cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd;
+  if (c >= nrec) return;
+  int off, len;
+  if (c < cs.n_soc) {
+    off = cs.soc_off[c];
+    len = cs.soc_dim[c];
+  } else if (c < cs.n_soc + cs.n_exp) {
+    off = cs.exp_begin + 3 * (c - cs.n_soc);
+    len = 3;
+  } else if (c < cs.n_soc + cs.n_exp + cs.n_pow) {
+    off = cs.pow_begin + 3 * (c - cs.n_soc - cs.n_exp);
+    len = 3;
+  } else {
+    const int k = c - cs.n_soc - cs.n_exp - cs.n_pow;
+    off = cs.psd_off[k];
+    len = cs.psd_n[k] * (cs.psd_n[k] + 1) / 2;
+  }
+  if (len == 0) return;
+  double mean = 0;
+  for (int i = 0; i < len; ++i) mean += e[off + i];
+  mean /= len;
+  for (int i = 0; i < len; ++i) delta[off + i] = mean / e[off + i];
+}
+
+extern "C" int clgpu_rectify_equilibration(clgpu_cones *h, double *delta, const double *e,
+                                           int *any_changed, clgpu_stream_t stream) {
+  if (!h || (h->numel > 0 && (!delta || !e))) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  const ConeSet &cs = h->cs;
+  const int nrec = cs.n_soc + cs.n_exp + cs.n_pow + cs.n_psd;
+  if (h->numel > 0) {
+    k_fill<<<(h->numel + 255) / 256, 256, 0, st>>>(delta, h->numel, 1.0);
+    if (nrec > 0) k_rectify<<<(nrec + 127) / 128, 128, 0, st>>>(cs, delta, e);
+  }
+  if (any_changed) *any_changed = nrec > 0 ? 1 : 0;
+  return finish(st);
+}
+
+// -Hs into the caller's KKT values, and the sparse-SOC expansion entries
+// (the reference's vut values [-eta^2 v; -eta^2 u] per cone and -/+ eta^2 on
+// the two extra diagonals)
+__global__ void k_scatter_neg(const double *hs, const int *map, int n, double *kv, float *kv32) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double v = -hs[k];
+  kv[map[k]] = v;
+  if (kv32) kv32[map[k]] = float(v);
+}
+__global__ void k_sparse_soc_kkt(ConeSet cs, const int *vu, const int *vut, const int *D,
+                                 double *kv, float *kv32) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cs.n_soc || !cs.soc_sparse[c]) return;
+  // position of this cone among the sparse ones and its first expansion entry
+  int sidx = 0, base = 0;
+  for (int q = 0; q < c; ++q)
+    if (cs.soc_sparse[q]) {
+      ++sidx;
+      base += 2 * cs.soc_dim[q];
+    }
+  const int off = cs.soc_off[c] - cs.soc_begin, d = cs.soc_dim[c];
+  const double eta = cs.soc_eta[c], e2 = eta * eta;
+  auto put = [&](int pos, double v) {
+    kv[pos] = v;
+    if (kv32) kv32[pos] = float(v);
+  };
+  for (int i = 0; i < d; ++i) {
+    const double vv = -e2 * cs.soc_v[off + i], uu = -e2 * cs.soc_u[off + i];
+    put(vu[base + i], vv);
+    put(vut[base + i], vv);
+    put(vu[base + d + i], uu);
+    put(vut[base + d + i], uu);
+  }
+  put(D[2 * sidx], -e2);
+  put(D[2 * sidx + 1], e2);
+}
+
+extern "C" int clgpu_refresh_kkt(clgpu_cones *h, double *kkt_vals, const int *hs_map,
+                                 const int *vu_map, const int *vut_map, const int *D_map,
+                                 float *kkt_vals32, clgpu_stream_t stream) {
+  if (!h || !kkt_vals || (h->hs_len > 0 && !hs_map)) return -1;
+  if (h->n_sparse > 0 && (!vu_map || !vut_map || !D_map)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h->hs_len > 0) {
+    cudaMemsetAsync(h->d_hs, 0, (size_t)h->hs_len * sizeof(double), st);
+    cones_get_Hs(h->cs, h->d_nn_blk, h->d_soc_blk, h->d_exp_blk, h->d_pow_blk, h->d_psd_blk,
+                 h->d_hs, st);
+    k_scatter_neg<<<(h->hs_len + 255) / 256, 256, 0, st>>>(h->d_hs, hs_map, h->hs_len, kkt_vals,
+                                                          kkt_vals32);
+  }
+  if (h->n_sparse > 0)
+    k_sparse_soc_kkt<<<(h->cs.n_soc + 127) / 128, 128, 0, st>>>(h->cs, vu_map, vut_map, D_map,
+                                                               kkt_vals, kkt_vals32);
+  return finish(st);
+}
+
+__global__ void k_min_scalar(double *a, double cap) { *a = fmin(*a, cap); }
+
+extern "C" int clgpu_step_length_device(clgpu_cones *h, const double *dz, const double *ds,
+                                        const double *z, const double *s,
+                                        const double *alpha_max, double max_step_fraction,
+                                        double backtrack_step, double alpha_min, double *alpha,
+                                        clgpu_stream_t stream) {
+  if (!h || !alpha_max || !alpha) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemcpyAsync(alpha, alpha_max, sizeof(double), cudaMemcpyDeviceToDevice, st);
+  cones_step_length_sym(h->cs, dz, ds, z, s, alpha, st);
+  if (!h->symmetric) {
+    k_min_scalar<<<1, 1, 0, st>>>(alpha, max_step_fraction);
+    cudaMemcpyAsync(h->d_scal + 2, alpha, sizeof(double), cudaMemcpyDeviceToDevice, st);
+    cones_step_length_asym(h->cs, dz, ds, z, s, h->d_scal + 2, alpha, backtrack_step, alpha_min,
+                           st);
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : -1000 - (int)e;
 }
 
 extern "C" int clgpu_debug_soc_tiles(const int *off, const int *dim, int n, int max_cones,

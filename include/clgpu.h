@@ -290,12 +290,95 @@ int clgpu_margins(clgpu_cones *h, const double *z, int pd, double *alpha,
 int clgpu_margins_static(int ncones, const int *types, const int *dims,
                          const double *z, int pd, double *alpha, double *beta,
                          clgpu_stream_t st);
+/* mul_Hs_diag! (:365): y = Hs x like clgpu_mul_Hs, except on the rows of
+ * the sparse (expanded, dim > soc_threshold) second-order cones, which are
+ * left as the caller had them: the reference's refinement residual adds
+ * their diagonal and rank-2 parts from the KKT matrix
+ * (kktsolver_directldl_gpu.jl:454-480). */
+int clgpu_mul_Hs_diag(clgpu_cones *h, double *y, const double *x, clgpu_stream_t st);
+/* rectify_equilibration! (:21): delta = 1, and mean(e over the cone) / e on
+ * the rows of every second-order, exponential, power and PSD cone; device
+ * vectors of length numel.  *any_changed (host, may be NULL) = 1 when such
+ * a cone exists, as the reference's return value. */
+int clgpu_rectify_equilibration(clgpu_cones *h, double *delta, const double *e,
+                                int *any_changed, clgpu_stream_t st);
+/* The Hs -> KKT refresh of kktsolver_update! (kktsolver_directldl_gpu.jl:
+ * 181-214 with update_KKT_sparse_soc_parallel!, :490-548): writes -Hs into
+ * the caller's KKT values (device) at hs_map[k] for entry k of the packed
+ * Hsblocks layout (clgpu_cones_hs_len entries), and for the sparse
+ * second-order cones the expansion entries: per cone (in order) its values
+ * [-eta^2 v; -eta^2 u] (2 dim values) at vu_map[j] and vut_map[j], j running
+ * over the concatenated 2 dim slots of the sparse cones, and -eta^2, +eta^2
+ * at D_map[2 i], D_map[2 i + 1] for the i-th sparse cone.  Maps are the
+ * reference's GPUDataMap fields Hsblocks, vu, vut, D made 0-based (device
+ * int32).  kkt_vals32 (may be NULL) receives the same values in FP32 (the
+ * :cudssmixed matrix copy). */
+int clgpu_refresh_kkt(clgpu_cones *h, double *kkt_vals, const int *hs_map, const int *vu_map,
+                      const int *vut_map, const int *D_map, float *kkt_vals32,
+                      clgpu_stream_t st);
+/* step_length (:566) with its scalars in DEVICE memory and no host
+ * synchronisation: *alpha = the common step from the start value
+ * *alpha_max (both device pointers); asymmetric cones cap it at
+ * max_step_fraction and backtrack as clgpu_step_length does.  Returns once
+ * the work is queued. */
+int clgpu_step_length_device(clgpu_cones *h, const double *dz, const double *ds,
+                             const double *z, const double *s, const double *alpha_max,
+                             double max_step_fraction, double backtrack_step, double alpha_min,
+                             double *alpha, clgpu_stream_t st);
 /* scaled_unit_shift! (:81) */
 int clgpu_scaled_unit_shift(clgpu_cones *h, double *z, double alpha, int pd,
                             clgpu_stream_t st);
 /* unit_initialization! (:115) */
 int clgpu_unit_initialization(clgpu_cones *h, double *z, double *s,
                               clgpu_stream_t st);
+
+/* ------------------------------------------------------------ KKT level
+ * The direct LDL solver of a KKT matrix the caller assembles and refreshes
+ * itself: the AbstractDirectLDLSolver protocol (ldlsolver_constructor /
+ * refactor! / solve!, directldl_cudss.jl:30-59) together with
+ * _kktsolver_regularize_and_refactor! and the refined solve of
+ * GPULDLKKTSolver (kktsolver_directldl_gpu.jl:216-260, :300-413).
+ * create: N x N symmetric pattern as a full CSR (both triangles, 0-based,
+ * HOST arrays, every row with its diagonal; -2 otherwise, -4 on a repeated
+ * entry), Dsigns (+1 / -1 per row, host) and the settings'
+ * regularisation, refinement and direct_solve_method (CLGPU_METHOD_MIXED:
+ * FP32 factor and substitutions, FP64 refinement); orders the matrix and
+ * plans the supernodal factorisation.
+ * refactor: Kx (DEVICE, values in the create pattern's CSR order) is
+ * copied, its diagonal shifted by eps Dsigns (eps = static_c + static_prop
+ * max|diag|, returned in *eps when not NULL) and factored; returns 0, or 1
+ * when a pivot is not finite (is_success = false in the reference).
+ * solve: x = K \ b with iterative refinement against the unshifted K (b, x
+ * DEVICE vectors of length N; may not alias); 0, 1 on a non-finite result,
+ * -2 before a successful refactor.  Both synchronise the stream. */
+typedef struct clgpu_ldl clgpu_ldl;
+int clgpu_ldl_create(int N, const int *Kp, const int *Kj, const signed char *Dsigns,
+                     const clgpu_settings *settings, clgpu_ldl **out);
+int clgpu_ldl_refactor(clgpu_ldl *h, const double *Kx, double *eps, clgpu_stream_t st);
+int clgpu_ldl_solve(clgpu_ldl *h, const double *b, double *x, clgpu_stream_t st);
+int clgpu_ldl_destroy(clgpu_ldl *h);
+
+/* residuals_update! (src/residuals.jl:39-75, the GPU form): P full
+ * symmetric n x n, A m x n and At = A' (n x m) as CSR, all DEVICE arrays;
+ * q, b, x, s, z device vectors; tau, kappa device scalars.  Writes Px, rx_inf
+ * = -A' z, rz_inf = A x + s, rx = rx_inf - Px - q tau, rz = rz_inf - b tau
+ * and dots[5] = {q.x, b.z, s.z, x.Px, r_tau = q.x + b.z + kappa + x.Px /
+ * tau} in device memory.  work: device scratch of clgpu_residuals_work_len()
+ * doubles (the per-block partial sums; every reduction runs in a fixed
+ * order).  Returns once the work is queued. */
+int clgpu_residuals(int n, int m, const int *Pp, const int *Pj, const double *Px,
+                    const int *Ap, const int *Aj, const double *Ax, const int *Atp,
+                    const int *Atj, const double *Atx, const double *q, const double *b,
+                    const double *x, const double *s, const double *z, const double *tau,
+                    const double *kappa, double *rx, double *rz, double *rx_inf, double *rz_inf,
+                    double *Px_out, double *dots, double *work, clgpu_stream_t st);
+int clgpu_residuals_work_len(void);
+/* variables_add_step! (src/variables.jl:146-158): x += alpha dx, s += alpha
+ * ds, z += alpha dz, tau += alpha dtau, kappa += alpha dkappa; every
+ * argument in device memory, alpha included.  Returns once queued. */
+int clgpu_add_step(int n, int m, double *x, double *s, double *z, double *tau, double *kappa,
+                   const double *dx, const double *ds, const double *dz, const double *dtau,
+                   const double *dkappa, const double *alpha, clgpu_stream_t st);
 
 /* --------------------------------------------------------------- checks */
 /* Host-only replay of the device factorisation on the structures prepared
