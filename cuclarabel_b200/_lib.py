@@ -92,6 +92,7 @@ EXPORTED = [
     "clgpu_mul_Hs_diag", "clgpu_rectify_equilibration", "clgpu_refresh_kkt",
     "clgpu_step_length_device", "clgpu_ldl_create", "clgpu_ldl_refactor", "clgpu_ldl_solve",
     "clgpu_ldl_destroy", "clgpu_residuals", "clgpu_residuals_work_len", "clgpu_add_step",
+    "clgpu_cones_debug_scaling",
 ]
 
 
@@ -161,6 +162,7 @@ def _declare(L):
     L.clgpu_residuals.argtypes = [c_int, c_int] + [V] * 9 + [V] * 7 + [V] * 7 + [c_void_p]
     L.clgpu_residuals_work_len.argtypes = []
     L.clgpu_add_step.argtypes = [c_int, c_int] + [V] * 11 + [c_void_p]
+    L.clgpu_cones_debug_scaling.argtypes = [c_void_p] + [dp] * 9 + [ip]
 
 
 def load():

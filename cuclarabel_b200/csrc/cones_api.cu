@@ -577,6 +577,33 @@ extern "C" int clgpu_step_length_device(clgpu_cones *h, const double *dz, const 
   return e == cudaSuccess ? 0 : -1000 - (int)e;
 }
 
+extern "C" int clgpu_cones_debug_scaling(const clgpu_cones *h, double *soc_w,
+                                         double *soc_lambda, double *soc_u, double *soc_v,
+                                         double *soc_eta, double *soc_d, double *psd_R,
+                                         double *psd_Rinv, double *psd_lambda, int *psd_nmax) {
+  if (!h) return -1;
+  const ConeSet &cs = h->cs;
+  const size_t nr = (size_t)cs.soc_rows, nc = (size_t)cs.n_soc;
+  const size_t n2 = (size_t)cs.psd_nmax * cs.psd_nmax * cs.n_psd;
+  const size_t nl = (size_t)cs.psd_nmax * cs.n_psd;
+  struct {
+    double *dst;
+    const double *src;
+    size_t n;
+  } copies[] = {{soc_w, cs.soc_w, nr},          {soc_lambda, cs.soc_lambda, nr},
+                {soc_u, cs.soc_u, nr},          {soc_v, cs.soc_v, nr},
+                {soc_eta, cs.soc_eta, nc},      {soc_d, cs.soc_d, nc},
+                {psd_R, cs.psd_R, n2},          {psd_Rinv, cs.psd_Rinv, n2},
+                {psd_lambda, cs.psd_lam, nl}};
+  for (auto &c : copies)
+    if (c.dst && c.n) {
+      cudaError_t e = cudaMemcpy(c.dst, c.src, c.n * sizeof(double), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return -1000 - (int)e;
+    }
+  if (psd_nmax) *psd_nmax = cs.psd_nmax;
+  return 0;
+}
+
 extern "C" int clgpu_debug_soc_tiles(const int *off, const int *dim, int n, int max_cones,
                                      int max_rows, int *tiles, int cap) {
   if (n < 0 || (n > 0 && (!off || !dim)) || max_cones < 1 || max_rows < 1 || cap < 0 ||

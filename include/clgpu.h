@@ -381,6 +381,19 @@ int clgpu_add_step(int n, int m, double *x, double *s, double *z, double *tau, d
                    const double *dkappa, const double *alpha, clgpu_stream_t st);
 
 /* --------------------------------------------------------------- checks */
+/* The scaling state of the last update_scaling, copied to HOST buffers (any
+ * may be NULL); a diagnostic with no reference counterpart, used to check the
+ * reference's cone identities (test/UnitTests/test_coneops_secondordercone.jl,
+ * test_coneops_psdtrianglecone.jl) on the device's numbers.
+ *  second-order cones: w and lambda (one value per SOC row, cones in order),
+ *    u and v of the rank-2 form W'W = eta^2 (D + u u' - v v') (per SOC row,
+ *    zero on dense cones), eta and d = D[0,0] (one per cone);
+ *  PSD cones: R and Rinv (n x n, column-major, cone k from k nmax^2) and
+ *    lambda (cone k from k nmax), nmax = the largest side (returned). */
+int clgpu_cones_debug_scaling(const clgpu_cones *h, double *soc_w, double *soc_lambda,
+                              double *soc_u, double *soc_v, double *soc_eta, double *soc_d,
+                              double *psd_R, double *psd_Rinv, double *psd_lambda,
+                              int *psd_nmax);
 /* Host-only replay of the device factorisation on the structures prepared
  * for one instance: validates the ordering, the symbolic factorisation and
  * every index map, then factors a quasi-definite test matrix on the KKT
