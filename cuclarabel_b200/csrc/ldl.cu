@@ -552,18 +552,26 @@ __device__ __forceinline__ void seg_scan4(double (&x)[kSK], const int (&p)[kSK],
   s[kSK - 1] = v;
 }
 
-// kSK consecutive values of the ring as FP64 (two 16-byte or one 16-byte
-// shared load)
-__device__ __forceinline__ void ring_vals(const double *rv, double (&v)[kSK]) {
-  const double2 a = reinterpret_cast<const double2 *>(rv)[0];
-  const double2 b = reinterpret_cast<const double2 *>(rv)[1];
+// Ring slot layout of the 8-byte items (entries, FP64 values) of a solve
+// chunk: lane l holds entries 4l .. 4l+3, which it reads as two 16-byte
+// pairs; pair (4l, 4l+1) is stored in 16-byte unit l and pair (4l+2, 4l+3)
+// in unit 32 + l, so each of the two reads is contiguous across the warp
+// (conflict-free) instead of striding 32 bytes (two-way conflicts).
+__device__ __forceinline__ int ring_pos8(int e) {
+  return 2 * (((e >> 1) & 1) * 32 + (e >> 2)) + (e & 1);
+}
+// lane's kSK values of the ring as FP64 (two 16-byte or one 16-byte shared
+// load); FP32 values keep the plain order (one contiguous float4 per lane)
+__device__ __forceinline__ void ring_vals(const double *rv, int lane, double (&v)[kSK]) {
+  const double2 a = reinterpret_cast<const double2 *>(rv)[lane];
+  const double2 b = reinterpret_cast<const double2 *>(rv)[32 + lane];
   v[0] = a.x;
   v[1] = a.y;
   v[2] = b.x;
   v[3] = b.y;
 }
-__device__ __forceinline__ void ring_vals(const float *rv, double (&v)[kSK]) {
-  const float4 a = *reinterpret_cast<const float4 *>(rv);
+__device__ __forceinline__ void ring_vals(const float *rv, int lane, double (&v)[kSK]) {
+  const float4 a = reinterpret_cast<const float4 *>(rv)[lane];
   v[0] = a.x;
   v[1] = a.y;
   v[2] = a.z;
@@ -617,8 +625,9 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
       for (int h = 0; h < kSK; ++h) {
         const int e = lane + 32 * h;
         if (e < cnt) {
-          cp_async<8>(&rd[e], &ent[p + e]);
-          cp_async<sizeof(T)>(&vd[e], &val[p + e]);
+          const int pe = ring_pos8(e);
+          cp_async<8>(&rd[pe], &ent[p + e]);
+          cp_async<sizeof(T)>(&vd[sizeof(T) == 8 ? pe : e], &val[p + e]);
         }
       }
     }
@@ -644,12 +653,12 @@ __device__ void ring_pass(const int *__restrict__ chunks, int nch, int base,
     asm volatile("cp.async.wait_group %0;\n" ::"n"(kSRing - 1));
     __syncwarp();
     const int slot = c & (kSRing - 1);
-    const int4 *r4 = reinterpret_cast<const int4 *>(re + slot * kSChunk + kSK * lane);
-    const int4 ea = r4[0], eb = r4[1];
+    const int4 *r4 = reinterpret_cast<const int4 *>(re + slot * kSChunk);
+    const int4 ea = r4[lane], eb = r4[32 + lane];
     const int sg[kSK] = {ea.x, ea.z, eb.x, eb.z};
     const int ix[kSK] = {ea.y, ea.w, eb.y, eb.w};
     double vv[kSK];
-    ring_vals(rv + slot * kSChunk + kSK * lane, vv);
+    ring_vals(rv + slot * kSChunk, lane, vv);
     int p[kSK], gi[kSK];
     bool ok[kSK], wr[kSK];
 #pragma unroll
@@ -1028,7 +1037,7 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
         const int e = 2 * lane + h;
         if (e < cnt) {
           const unsigned dst =
-              static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * kChunk + e]));
+              static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * kChunk + h * 32 + lane]));
           asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
                        "l"(&ops[p0 + e]));
         }
@@ -1060,8 +1069,10 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
     const int slot = c & (kFRing - 1);
     const int eA = 2 * lane, eB = eA + 1;
     const bool vA = eA < cnt, vB = eB < cnt;
-    const int4 oA = vA ? ring[slot * kChunk + eA] : make_int4(0, 0, 0, 0);
-    const int4 oB = vB ? ring[slot * kChunk + eB] : make_int4(0, 0, 0, 0);
+    // entry 2 lane + h sits at h * 32 + lane: both reads contiguous across the warp
+    static_assert(kChunk == 64, "two ring entries per lane");
+    const int4 oA = vA ? ring[slot * kChunk + lane] : make_int4(0, 0, 0, 0);
+    const int4 oB = vB ? ring[slot * kChunk + 32 + lane] : make_int4(0, 0, 0, 0);
     if (pivot) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
