@@ -434,6 +434,145 @@ def ncu_traffic(summary):
     return None
 
 
+def fp64_gemm_peak():
+    """cuBLAS FP64 GEMM throughput on this GPU (torch.matmul, 8192^3, best of
+    10 after warm-up): the denominator of the FP64 tensor-core roofline."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        a @ b
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(10):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        best = t if best is None else min(best, t)
+    del a, b
+    return 2.0 * n ** 3 / (best / 1000.0) / 1e12
+
+
+def _oracle_sample_worker(which, scale, conn):
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    import oracle
+    from cuclarabel_b200 import problems
+    pb = problems.mixed_socp(scale) if which == 2 else problems.exp_pow_psd(scale)
+    obj = oracle.SolverObject(*pb, gpu_equilibration=1)
+    t0 = time.perf_counter()
+    r = obj.run()
+    conn.send((r["status_name"], r["iterations"], time.perf_counter() - t0))
+
+
+def large_single(which, scale, method, sh, fp64_peak, cpu_scale):
+    """One large single problem (configuration 2: mixed SOCP, n = 20000,
+    m = 60000; configuration 3: exp/pow/PSD LP, n = 30000, m = 96000, at
+    `scale`) on the supernodal LDL^T: setup, a warm-up solve, a solve timed
+    with CUDA events (L2 flushed before), a profiled solve for the per-kernel
+    breakdown, and the end-to-end pass (new values from pinned host memory +
+    solve! + solution read back)."""
+    import torch
+    from cuclarabel_b200 import Solver, SolverStatus, problems
+    from cuclarabel_b200.api import _as_csc
+    pb = problems.mixed_socp(scale) if which == 2 else problems.exp_pow_psd(scale)
+    t0 = time.perf_counter()
+    s = Solver(*pb, direct_solve_method=method)
+    setup_s = time.perf_counter() - t0
+    s.solve(sh)
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
+    flush.add_(1.0)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(sh)
+    e0.record(stream)
+    s.solve_only(sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_s = e0.elapsed_time(e1) / 1000.0
+    sol = s.solutions()[0]
+    s.set_profiling(True)
+    s.solve(sh)
+    prof = s.profile()
+    s.set_profiling(False)
+    sn = prof.get("supernodal", {})
+    upd = sn.get("update", {"ms": 0.0, "flops": 0.0, "launches": 0})
+    fact_fl = sum(v["flops"] for v in sn.values())
+    fact_ms = sum(sn[k]["ms"] for k in ("small_fronts", "assemble", "diag", "trsm", "update")
+                  if k in sn)
+    solve_ms = sum(v["ms"] for k, v in sn.items() if k.startswith(("fwd", "bwd")))
+    ach = upd["flops"] / (upd["ms"] / 1000.0) / 1e12 if upd["ms"] > 0 else 0.0
+    # end to end: new P, q, A, b values from pinned host memory, solve!, x/s/z back
+    P, q, A, b, _ = pb
+    vals = [_as_csc(P, P.shape).data, np.asarray(q, np.float64),
+            _as_csc(A, A.shape).data, np.asarray(b, np.float64)]
+    pinned = []
+    for v in vals:
+        t = torch.empty(len(v), dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = v
+        pinned.append(t.numpy())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.update_data(P=pinned[0], q=pinned[1], A=pinned[2], b=pinned[3], stream=sh)
+    s.solve_only(sh)
+    res = s.results()
+    e2e_s = time.perf_counter() - t0
+    ok = res["status"][0] == int(SolverStatus.SOLVED)
+    out = {
+        "workload": ("config 2: mixed-cone QP/SOCP n=%d, m=%d (2000 zero, 28000 nonneg, "
+                     "3000 SOC(10) at scale 1)" if which == 2 else
+                     "config 3: exp/pow/PSD LP n=%d, m=%d (20000 exp, 5000 pow, 200 PSD(10), "
+                     "10000 nonneg at scale 1)") % (A.shape[1], A.shape[0]),
+        "scale": scale, "method": method,
+        "value": (1.0 / dev_s) if sol.status == SolverStatus.SOLVED else 0.0,
+        "unit": "solves/s", "solve_s": dev_s, "setup_s": setup_s,
+        "status": sol.status.name, "iterations": sol.iterations, "obj_val": sol.obj_val,
+        "device_bytes": s.device_bytes(),
+        "e2e": {"value": (1.0 / e2e_s) if ok else 0.0, "unit": "solves/s",
+                "h2d_bytes_per_step": int(sum(v.nbytes for v in vals)),
+                "d2h_bytes_per_step": int(8 * (A.shape[1] + 2 * A.shape[0])),
+                "note": "update_data! of P, q, A, b from pinned host memory + solve! + x, s, "
+                        "z read back; solver set up beforehand"},
+        "factor": {"ms_per_solve": fact_ms, "flops_per_solve": fact_fl,
+                   "tflops": fact_fl / (fact_ms / 1000.0) / 1e12 if fact_ms > 0 else 0.0,
+                   "factorisations": sn.get("diag", {}).get("launches", 0)},
+        "solves_ms_per_solve": solve_ms,
+        "kernels": {k: {"ms": round(v["ms"], 3), "launches": v["launches"]}
+                    for k, v in sn.items() if v["launches"]},
+        "roofline": {"bound": "tensor", "kernel": "k_sn_gemm_f64<UPDATE> (trailing update of "
+                     "the blocked fronts, m8n8k4 FP64 DMMA)" if method == "cudss" else
+                     "k_sn_gemm_f32<UPDATE> (trailing update, FP32 FMA)",
+                     "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": ach / fp64_peak if fp64_peak else None,
+                     "peak_kind": "measured: cuBLAS FP64 GEMM 8192^3 on this GPU in this run",
+                     "flops_per_launch": upd["flops"] / max(upd["launches"], 1),
+                     "avg_launch_ms": upd["ms"] / max(upd["launches"], 1),
+                     "launches": upd["launches"], "traffic": None},
+    }
+    del s
+    if cpu_scale > 0:
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        a, b_ = ctx.Pipe()
+        p = ctx.Process(target=_oracle_sample_worker, args=(which, cpu_scale, b_), daemon=True)
+        p.start()
+        st_, it_, dt_ = a.recv()
+        p.join(timeout=10)
+        out["cpu_baseline"] = {
+            "value": (1.0 / dt_) if st_ == "SOLVED" else 0.0, "unit": "solves/s", "cores": 1,
+            "kind": "port", "status": st_, "iterations": it_, "seconds": dt_,
+            "sample": "the same family at scale %.3f (the oracle's scalar LDL^T of the full "
+                      "size does not finish in minutes), solve! on a solver set up "
+                      "beforehand, one core" % cpu_scale}
+    return out
+
+
 def rank_seed0(rank, instances):
     """First instance seed of a rank: rank r owns instances [r B, (r+1) B),
     so ranks share no instance (weak scaling, no data-path collective)."""
@@ -580,6 +719,13 @@ def main():
                     help="timed calls per cone operation (median reported)")
     ap.add_argument("--cone-kernels-only", action="store_true",
                     help="run only the cone-kernel roofline workload and print its JSON")
+    ap.add_argument("--large-scale", type=float, default=1.0,
+                    help="scale of the large single problems (configurations 2 and 3) run "
+                         "on the supernodal factorisation; 0 skips them")
+    ap.add_argument("--large-cpu-scale", type=float, default=0.05,
+                    help="scale of the CPU oracle's sample of configurations 2 and 3")
+    ap.add_argument("--large-only", action="store_true",
+                    help="run only configurations 2 and 3 and print their JSON")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -597,6 +743,16 @@ def main():
         print(json.dumps({"cone_kernels": cone_kernel_roofline(hbm, args.cone_scale,
                                                                args.cone_reps),
                           "peak_gbs": hbm}), flush=True)
+        return
+    if args.large_only:
+        from cuclarabel_b200 import problems as _p  # noqa: F401
+        st_ = torch.cuda.Stream()
+        pk = fp64_gemm_peak()
+        out = {"fp64_gemm_tflops": pk}
+        for which in (2, 3):
+            out["config%d" % which] = large_single(which, args.large_scale, args.method,
+                                                   st_.cuda_stream, pk, args.large_cpu_scale)
+        print(json.dumps(out), flush=True)
         return
     dist = None
     if world > 1:
@@ -818,6 +974,15 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(args.ref_sample)
 
+    large = None
+    if rank == 0 and args.large_scale > 0:
+        pk = fp64_gemm_peak()
+        large = {"fp64_gemm_tflops": pk,
+                 "config2": large_single(2, args.large_scale, args.method, sh, pk,
+                                         0 if args.no_cpu else args.large_cpu_scale),
+                 "config3": large_single(3, args.large_scale, args.method, sh, pk,
+                                         0 if args.no_cpu else args.large_cpu_scale)}
+
     cones = None
     if rank == 0 and args.cone_scale > 0:
         ck = cone_kernel_roofline(hbm, args.cone_scale, args.cone_reps)
@@ -869,6 +1034,7 @@ def main():
             "served": served,
             "cpu_baseline": cpu,
             "cone_kernels": cones,
+            "large_single": large,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

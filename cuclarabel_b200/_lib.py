@@ -44,7 +44,7 @@ class ClgpuSettings(ctypes.Structure):
         ("iterative_refinement_max_iter", c_int),
         ("iterative_refinement_stop_ratio", c_double),
         ("direct_solve_method", c_int), ("soc_threshold", c_int), ("verbose", c_int),
-        ("setup_threads", c_int), ("fused_solves", c_int),
+        ("setup_threads", c_int), ("fused_solves", c_int), ("device_setup", c_int),
     ]
 
 
@@ -92,7 +92,8 @@ EXPORTED = [
     "clgpu_mul_Hs_diag", "clgpu_rectify_equilibration", "clgpu_refresh_kkt",
     "clgpu_step_length_device", "clgpu_ldl_create", "clgpu_ldl_refactor", "clgpu_ldl_solve",
     "clgpu_ldl_destroy", "clgpu_residuals", "clgpu_residuals_work_len", "clgpu_add_step",
-    "clgpu_cones_debug_scaling",
+    "clgpu_cones_debug_scaling", "clgpu_solver_get_sn_profile", "clgpu_solver_debug_setup",
+    "clgpu_solver_get_sn_refinement",
 ]
 
 
@@ -163,6 +164,10 @@ def _declare(L):
     L.clgpu_residuals_work_len.argtypes = []
     L.clgpu_add_step.argtypes = [c_int, c_int] + [V] * 11 + [c_void_p]
     L.clgpu_cones_debug_scaling.argtypes = [c_void_p] + [dp] * 9 + [ip]
+    L.clgpu_solver_get_sn_profile.argtypes = [c_void_p, dp, dp, ctypes.POINTER(c_ll)]
+    L.clgpu_solver_get_sn_refinement.argtypes = [c_void_p, ctypes.POINTER(c_ll), dp]
+    L.clgpu_solver_debug_setup.argtypes = [c_void_p, dp, dp, dp, dp, dp, dp,
+                                           ctypes.POINTER(c_ll)]
 
 
 def load():

@@ -181,6 +181,7 @@ class Settings:
     soc_threshold: int = 5
     setup_threads: int = 0
     fused_solves: bool = True
+    device_setup: bool = True
 
     def to_c(self):
         if self.direct_solve_method not in _METHODS:
@@ -336,6 +337,13 @@ def _pack_batch(problems):
 def _nvars(spec):
     t, d, _ = spec
     return 3 if t in (3, 4) else (d * (d + 1) // 2 if t == 5 else d)
+
+
+# launch kinds of the supernodal factorisation (CLGPU_SN_KINDS, clgpu.h)
+SN_KIND_NAMES = ["small_fronts", "assemble", "diag", "trsm", "update", "fwd_small",
+                 "fwd_gather", "fwd_diag", "fwd_gemv", "fwd_scatter", "bwd_small", "bwd_gather",
+                 "bwd_partial", "bwd_diag", "bwd_scatter"]
+SN_KINDS = len(SN_KIND_NAMES)
 
 
 class _StagingView:
@@ -608,9 +616,21 @@ class BatchSolver:
                  "ldl_solve2"]
         by = (ctypes.c_double * 3)()
         L.clgpu_solver_get_phase_bytes(self._h, by)
-        return dict(ms_total=vals[0].value, passes=passes.value,
-                    phases={n: (ms[i], calls[i]) for i, n in enumerate(names)},
-                    bytes={"ldl_factor": by[0], "ldl_solve": by[1], "ldl_solve2": by[2]})
+        out = dict(ms_total=vals[0].value, passes=passes.value,
+                   phases={n: (ms[i], calls[i]) for i, n in enumerate(names)},
+                   bytes={"ldl_factor": by[0], "ldl_solve": by[1], "ldl_solve2": by[2]})
+        sms = (ctypes.c_double * SN_KINDS)()
+        sfl = (ctypes.c_double * SN_KINDS)()
+        scl = (ctypes.c_longlong * SN_KINDS)()
+        if L.clgpu_solver_get_sn_profile(self._h, sms, sfl, scl) == 0:
+            out["supernodal"] = {n: {"ms": sms[i], "flops": sfl[i], "launches": scl[i]}
+                                 for i, n in enumerate(SN_KIND_NAMES)}
+            cnt = (ctypes.c_longlong * 3)()
+            worst = ctypes.c_double()
+            L.clgpu_solver_get_sn_refinement(self._h, cnt, ctypes.byref(worst))
+            out["refinement"] = {"solves": cnt[0], "sweeps": cnt[1], "unconverged": cnt[2],
+                                 "worst_ratio": worst.value}
+        return out
 
 
 class Solver(BatchSolver):

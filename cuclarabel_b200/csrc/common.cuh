@@ -25,6 +25,9 @@ enum ConeType { CONE_ZERO = 0, CONE_NONNEG = 1, CONE_SOC = 2, CONE_EXP = 3,
 
 constexpr double kDMax = DBL_MAX;
 constexpr double kDEps = 2.220446049250313e-16;
+// largest PSD side: one warp per cone, its matrices (7 of side n for
+// update_scaling) in shared memory
+constexpr int kPsdMaxSide = 48;
 
 // src/utils/mathutils.jl:12 (logsafe)
 __device__ __forceinline__ double logsafe(double v) {

@@ -620,11 +620,11 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
     for (int p = 0; p < n; ++p)
       for (int q = p + 1; q < n; ++q) {
         double a = 0, b = 0, g = 0;
-        if (lane < n) {
-          double mp = M[lane + n * p], mq = M[lane + n * q];
-          a = mp * mp;
-          b = mq * mq;
-          g = mp * mq;
+        for (int r = lane; r < n; r += 32) {
+          double mp = M[r + n * p], mq = M[r + n * q];
+          a += mp * mp;
+          b += mq * mq;
+          g += mp * mq;
         }
         a = warp_sum(a);
         b = warp_sum(b);
@@ -634,23 +634,23 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
         double zeta = (b - a) / (2 * g);
         double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
         double cs = 1 / sqrt(1 + t * t), sn = cs * t;
-        if (lane < n) {
-          double mp = M[lane + n * p], mq = M[lane + n * q];
-          M[lane + n * p] = cs * mp - sn * mq;
-          M[lane + n * q] = sn * mp + cs * mq;
-          double vp = V[lane + n * p], vq = V[lane + n * q];
-          V[lane + n * p] = cs * vp - sn * vq;
-          V[lane + n * q] = sn * vp + cs * vq;
+        for (int r = lane; r < n; r += 32) {
+          double mp = M[r + n * p], mq = M[r + n * q];
+          M[r + n * p] = cs * mp - sn * mq;
+          M[r + n * q] = sn * mp + cs * mq;
+          double vp = V[r + n * p], vq = V[r + n * q];
+          V[r + n * p] = cs * vp - sn * vq;
+          V[r + n * q] = sn * vp + cs * vq;
         }
         __syncwarp();
       }
     if (!rotated) break;
   }
   // column norms, sort descending (selection on lane 0 into tmp perm)
-  if (lane < n) {
+  for (int c = lane; c < n; c += 32) {
     double t = 0;
-    for (int k = 0; k < n; ++k) t += M[k + n * lane] * M[k + n * lane];
-    S[lane] = sqrt(t);
+    for (int k = 0; k < n; ++k) t += M[k + n * c] * M[k + n * c];
+    S[c] = sqrt(t);
   }
   __syncwarp();
   int *perm = reinterpret_cast<int *>(tmp + n * n);
@@ -678,10 +678,15 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
     int i = e % n, j = e / n;
     tmp[e] = V[i + n * perm[j]];
   }
-  double sl = lane < n ? S[perm[lane]] : 0.0;
+  double sl[kPsdMaxSide / 32];
+#pragma unroll
+  for (int r = 0; r < kPsdMaxSide / 32; ++r)
+    sl[r] = lane + 32 * r < n ? S[perm[lane + 32 * r]] : 0.0;
   __syncwarp();
   for (int e = lane; e < n * n; e += 32) V[e] = tmp[e];
-  if (lane < n) S[lane] = sl;
+#pragma unroll
+  for (int r = 0; r < kPsdMaxSide / 32; ++r)
+    if (lane + 32 * r < n) S[lane + 32 * r] = sl[r];
   __syncwarp();
 }
 // cyclic Jacobi eigenvalues of symmetric A (destroyed); returns min eigenvalue,
@@ -706,22 +711,26 @@ __device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
         double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
         double c = 1 / sqrt(t * t + 1), s = t * c;
         __syncwarp();
-        if (lane < n) {
-          double akp = A[lane + n * p], akq = A[lane + n * q];
-          A[lane + n * p] = c * akp - s * akq;
-          A[lane + n * q] = s * akp + c * akq;
+        for (int r = lane; r < n; r += 32) {
+          double akp = A[r + n * p], akq = A[r + n * q];
+          A[r + n * p] = c * akp - s * akq;
+          A[r + n * q] = s * akp + c * akq;
         }
         __syncwarp();
-        if (lane < n) {
-          double apk = A[p + n * lane], aqk = A[q + n * lane];
-          A[p + n * lane] = c * apk - s * aqk;
-          A[q + n * lane] = s * apk + c * aqk;
+        for (int r = lane; r < n; r += 32) {
+          double apk = A[p + n * r], aqk = A[q + n * r];
+          A[p + n * r] = c * apk - s * aqk;
+          A[q + n * r] = s * apk + c * aqk;
         }
         __syncwarp();
       }
   }
-  double v = lane < n ? A[lane + n * lane] : CUDART_INF;
-  if (ev && lane < n) ev[lane] = v;
+  double v = CUDART_INF;
+  for (int r = lane; r < n; r += 32) {
+    const double a = A[r + n * r];
+    v = fmin(v, a);
+    if (ev) ev[r] = a;
+  }
   __syncwarp();
   return warp_min(v);
 }
@@ -779,7 +788,7 @@ __global__ void k_psd_update_scaling(ConeSet cs, const double *__restrict__ s,
     R[e] = t * (1.0 / sqrt(S[j]));
     Ri[e] = (1.0 / sqrt(S[i])) * u;
   }
-  if (p.lane < n) lam[p.lane] = S[p.lane];
+  for (int r = p.lane; r < n; r += 32) lam[r] = S[r];
 }
 
 // y = a*op(Rx)... helper: Y = Rx' X Rx (trans=false) or Rx X Rx' (trans=true)
@@ -1458,7 +1467,8 @@ __global__ void k_psd_barrier(ConeSet cs, const double *__restrict__ z,
     bool ok = warp_chol(n, Q, p.lane);
     double ld;
     if (ok) {
-      double t = p.lane < n ? log(Q[p.lane + n * p.lane]) : 0.0;
+      double t = 0.0;
+      for (int r = p.lane; r < n; r += 32) t += log(Q[r + n * r]);
       ld = 2 * warp_sum(t);
     } else {
       ld = CUDART_INF;
@@ -1528,7 +1538,8 @@ __global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z) {
   svec_to_mat(n, z + p.off, Z, p.lane);
   __syncwarp();
   double mn = warp_eig_min(n, Z, ev, p.lane);
-  double pos = (p.lane < n && ev[p.lane] > 0) ? ev[p.lane] : 0.0;
+  double pos = 0.0;
+  for (int r = p.lane; r < n; r += 32) pos += ev[r] > 0 ? ev[r] : 0.0;
   pos = warp_sum(pos);
   if (p.lane == 0) {
     cs.cone_tmp[slot] = mn;
@@ -2152,13 +2163,20 @@ static inline int nn_block(const ConeSet &cs) { return cs.nn_block > 0 ? cs.nn_b
 
 static inline void psd_launch_dims(const ConeSet &cs, int nmats, int &nb, int &nt,
                                    size_t &smem) {
-  nt = 32 * kPsdWarps;
+  // warps (cones) per block: kPsdWarps while their matrices fit 200 KB
+  const size_t per = (size_t)nmats * cs.psd_nmax * cs.psd_nmax * sizeof(double);
+  const int warps = (int)std::max<size_t>(1, std::min<size_t>(kPsdWarps, (200 * 1024) / per));
+  nt = 32 * warps;
   nb = blocks_for((long long)cs.n_psd * 32, nt);
-  smem = (size_t)kPsdWarps * nmats * cs.psd_nmax * cs.psd_nmax * sizeof(double) + 256;
+  smem = (size_t)warps * per + 256;
 }
 #define LAUNCH_PSD(KERNEL, NMATS, ...)                                                 \
   do {                                                                                 \
     if (cs.n_psd > 0) {                                                                \
+      static const bool _attr = (cudaFuncSetAttribute(                                  \
+                                     KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     210 * 1024) == cudaSuccess);                      \
+      (void)_attr;                                                                     \
       int _nb, _nt;                                                                    \
       size_t _smem;                                                                    \
       psd_launch_dims(cs, NMATS, _nb, _nt, _smem);                                     \

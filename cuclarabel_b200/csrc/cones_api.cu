@@ -104,7 +104,7 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
         h->symmetric = false;
         break;
       case 5:
-        if (d > 16) {
+        if (d > kPsdMaxSide) {
           delete h;
           return -3;
         }

@@ -25,6 +25,7 @@
 #include "cones.cuh"
 #include "devbuf.hpp"
 #include "ldl.cuh"
+#include "equilibrate.cuh"
 #include "sn_exec.cuh"
 #include "setup.hpp"
 
@@ -814,6 +815,7 @@ struct clgpu_solver {
   int *h_counter = nullptr;  // pinned
   std::vector<int> h_n, h_m, h_xoff, h_moff;
   bool any_asym = false, any_sym = false;
+  long long kkt_nnz = 0;              // stored KKT entries over all instances
   bool any_sn = false;                // class-3 (supernodal) instances present
   std::unique_ptr<SnExec> sn;         // their factorisation
   std::vector<clgpu_info> info;
@@ -998,6 +1000,7 @@ extern "C" int clgpu_default_settings(clgpu_settings *s) {
   s->verbose = 0;
   s->setup_threads = 0;
   s->fused_solves = 1;
+  s->device_setup = 1;
   return 0;
 }
 
@@ -1216,7 +1219,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       if (prep[i].ctype[k] == CLGPU_CONE_PSD) psd_nmax = std::max(psd_nmax, prep[i].cdim[k]);
     }
   }
-  if (psd_nmax > 16) return -3;  // PSD side limited to 16 (warp-per-cone kernels)
+  if (psd_nmax > kPsdMaxSide) return -3;  // warp-per-cone kernels, matrices in shared memory
   const auto osoc = prefix(nsoc), oexp = prefix(nexp), opow = prefix(npow), opsd = prefix(npsd);
   std::vector<int> soc_off(osoc[B]), soc_dim(osoc[B]), soc_inst(osoc[B]), soc_sparse(osoc[B]),
       exp_inst(oexp[B]), pow_inst(opow[B]), psd_off(opsd[B]), psd_n(opsd[B]), psd_inst(opsd[B]);
@@ -1522,6 +1525,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   kk.Kp = A.upload(Kp);
   kk.Kj = A.upload(Kj);
   kk.Kx = A.upload(Kx);
+  h->kkt_nnz = knz;
   kk.Kdiag = A.upload(Kdiag);
   kk.Dsign = A.upload(Dsign);
   kk.gsrc = A.upload(gsrc);
@@ -1997,6 +2001,68 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   h->d_reset = A.alloc<int>(B);
   // per-instance constants for init
   h->d_c = A.upload(c);
+  // ---------------- numeric setup on the device: Ruiz equilibration, the
+  // cost scaling, rectification and the KKT values of the instances whose
+  // equilibration the host left undone (bitwise the host's result)
+  {
+    std::vector<int> on(B, 0);
+    bool any = false;
+    for (int i = 0; i < B; ++i) {
+      on[i] = prep[i].eq_deferred ? 1 : 0;
+      any = any || on[i];
+    }
+    if (any) {
+      std::vector<int2> rc;
+      for (size_t k = 0; k < soc_off.size(); ++k)
+        if (on[soc_inst[k]]) rc.push_back(make_int2(soc_off[k], soc_dim[k]));
+      for (size_t k = 0; k < exp_inst.size(); ++k)
+        if (on[exp_inst[k]]) rc.push_back(make_int2(cs.exp_begin + 3 * (int)k, 3));
+      for (size_t k = 0; k < pow_inst.size(); ++k)
+        if (on[pow_inst[k]]) rc.push_back(make_int2(cs.pow_begin + 3 * (int)k, 3));
+      for (size_t k = 0; k < psd_off.size(); ++k)
+        if (on[psd_inst[k]]) rc.push_back(make_int2(psd_off[k], psd_n[k] * (psd_n[k] + 1) / 2));
+      EqDev q{};
+      q.B = B;
+      q.nx = nx;
+      q.mz = mz;
+      q.xoff = dv.xoff;
+      q.col_inst = dv.col_inst;
+      q.row_inst = dv.row_inst;
+      q.Pp = dv.Pp;
+      q.Pj = dv.Pj;
+      q.Px = const_cast<double *>(dv.Px);
+      q.Ap = dv.Ap;
+      q.Aj = dv.Aj;
+      q.Ax = const_cast<double *>(dv.Ax);
+      q.Atp = dv.Atp;
+      q.Atj = dv.Atj;
+      q.Atx = const_cast<double *>(dv.Atx);
+      q.q = const_cast<double *>(dv.q);
+      q.b = const_cast<double *>(dv.b);
+      q.negq = const_cast<double *>(dv.negq);
+      q.d = const_cast<double *>(dv.d);
+      q.dinv = const_cast<double *>(dv.dinv);
+      q.e = const_cast<double *>(dv.e);
+      q.einv = const_cast<double *>(dv.einv);
+      q.c = h->d_c;
+      q.dw = A.alloc<double>(nx);
+      q.ew = A.alloc<double>(mz);
+      q.ct = A.alloc<double>(B);
+      q.cflag = A.alloc<int>(B);
+      q.on = A.upload(on);
+      q.rcone = A.upload(rc);
+      q.nrc = (int)rc.size();
+      EqParams ep{h->st.equilibrate_enable, h->st.equilibrate_max_iter,
+                  h->st.equilibrate_min_scaling, h->st.equilibrate_max_scaling};
+      if (A.err != cudaSuccess) return -5;
+      equilibrate_on_device(q, ep, h->d_upd_pmap, h->d_upd_pxy, h->upd_np, h->d_upd_amap,
+                            h->d_upd_axy, h->upd_na, h->kk.Kx, 0);
+      cudaError_t e = cudaDeviceSynchronize();
+      if (e == cudaSuccess) e = cudaGetLastError();
+      if (e != cudaSuccess) return -1000 - (int)e;
+    }
+    mark("device equilibration");
+  }
   h->d_normq = A.upload(nq);
   h->d_normb = A.upload(nb);
   h->d_pnnz = A.upload(pnnz);
@@ -2061,6 +2127,7 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
   opt.equilibrate_max_iter = h->st.equilibrate_max_iter;
   opt.equilibrate_min_scaling = h->st.equilibrate_min_scaling;
   opt.equilibrate_max_scaling = h->st.equilibrate_max_scaling;
+  opt.defer_equilibration = h->st.device_setup != 0;
   std::vector<Prepared> prep(nprob);
   std::vector<int> okv(nprob, 0);
   int nth = h->st.setup_threads > 0 ? h->st.setup_threads
@@ -2788,6 +2855,45 @@ extern "C" long long clgpu_solver_launch_count(const clgpu_solver *h) {
 extern "C" int clgpu_solver_set_profiling(clgpu_solver *h, int enable) {
   if (!h) return -1;
   h->profiling = enable != 0;
+  if (h->sn) sn_set_profiling(*h->sn, enable != 0);
+  return 0;
+}
+extern "C" int clgpu_solver_debug_setup(const clgpu_solver *h, double *d, double *e, double *c,
+                                        double *q, double *b, double *Kx, long long *kkt_nnz) {
+  if (!h) return -1;
+  const Dev &dv = h->dv;
+  struct {
+    double *dst;
+    const double *src;
+    size_t n;
+  } cp[] = {{d, dv.d, (size_t)h->nx},       {e, dv.e, (size_t)h->mz},
+            {c, h->d_c, (size_t)h->B},      {q, dv.q, (size_t)h->nx},
+            {b, dv.b, (size_t)h->mz},       {Kx, h->kk.Kx, (size_t)h->kkt_nnz}};
+  for (auto &x : cp)
+    if (x.dst && x.n) {
+      cudaError_t err = cudaMemcpy(x.dst, x.src, x.n * sizeof(double), cudaMemcpyDeviceToHost);
+      if (err != cudaSuccess) return -1000 - (int)err;
+    }
+  if (kkt_nnz) *kkt_nnz = h->kkt_nnz;
+  return 0;
+}
+extern "C" int clgpu_solver_get_sn_refinement(const clgpu_solver *h, long long *counts,
+                                               double *worst) {
+  if (!h) return -1;
+  if (!h->sn) return 1;
+  if (counts) {
+    counts[0] = h->sn->ir_solves;
+    counts[1] = h->sn->ir_sweeps;
+    counts[2] = h->sn->ir_unconverged;
+  }
+  if (worst) *worst = h->sn->ir_worst;
+  return 0;
+}
+extern "C" int clgpu_solver_get_sn_profile(const clgpu_solver *h, double *ms, double *flops,
+                                           long long *calls) {
+  if (!h) return -1;
+  if (!h->sn) return 1;
+  sn_get_profile(*h->sn, ms, flops, calls);
   return 0;
 }
 extern "C" int clgpu_solver_get_profile(const clgpu_solver *h, double *ms_total,

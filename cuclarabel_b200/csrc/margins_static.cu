@@ -75,7 +75,7 @@ extern "C" int clgpu_margins_static(int ncones, const int *types, const int *dim
       soc_max = d > soc_max ? d : soc_max;
     }
     if (t == 5) {
-      if (d > 16) return -3;
+      if (d > kPsdMaxSide) return -3;
       ++n_psd;
       psd_max = d > psd_max ? d : psd_max;
     }

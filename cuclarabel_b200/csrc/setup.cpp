@@ -512,7 +512,19 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     }
     for (int i = 0; i < m; ++i) out.b[i] *= ew[i];
   };
-  if (opt.equilibrate_enable) {
+  // the device can take the numeric part of setup when every value has one
+  // KKT position: P's upper entries and A's entries sorted, none repeated
+  if (opt.defer_equilibration) {
+    bool sorted = true;
+    for (int j = 0; j < n && sorted; ++j)
+      for (int k = pb.Pp[j] + 1; k < pb.Pp[j + 1]; ++k)
+        if (pb.Pi[k] <= j && pb.Pi[k - 1] >= pb.Pi[k]) sorted = false;
+    for (int j = 0; j < n && sorted; ++j)
+      for (int k = pb.Ap[j] + 1; k < pb.Ap[j + 1]; ++k)
+        if (pb.Ai[k - 1] >= pb.Ai[k]) sorted = false;
+    out.eq_deferred = sorted;
+  }
+  if (opt.equilibrate_enable && !out.eq_deferred) {
     double smin = opt.equilibrate_min_scaling, smax = opt.equilibrate_max_scaling;
     std::vector<double> dw(n), ew(m);
     for (int it = 0; it < opt.equilibrate_max_iter; ++it) {
@@ -953,10 +965,27 @@ extern "C" int clgpu_debug_check_instance(const clgpu_problem *pb, const clgpu_s
                  L.kind == SN_BWD_PARTIAL) &&
                 (t.z < k0 + K || t.z + kSnNB > ld || (t.z - k0 - K) % kSnNB))
               return -39;
-            if (L.kind == SN_UPDATE && (t.w < k0 + K || t.w > t.z || (t.w - k0 - K) % kSnNB))
+            if (L.kind == SN_UPDATE &&
+                (t.w < k0 + K || t.w + 64 > ld || (t.w - k0 - K) % 64 || t.z + kSnNB <= t.w))
               return -40;
           }
-          if (L.kind == SN_ASSEMBLE && (t.y < 0 || t.z > ld || t.y >= t.z)) return -41;
+          if ((L.kind == SN_ASSEMBLE || L.kind == SN_FWD_GATHER) &&
+              (t.y < 0 || t.z > ld || t.y >= t.z))
+            return -41;
+          if (L.kind == SN_ASSEMBLE || L.kind == SN_FWD_GATHER) {
+            // the chunk's children: entries q of each map inside [t.y, t.z)
+            if (t.w < plan.chunk_off[t.x] || t.w >= plan.chunk_off[t.x + 1] ||
+                (t.w - plan.chunk_off[t.x]) * kSnAsmCols != t.y)
+              return -44;
+            for (int e = plan.cl_ptr[t.w]; e < plan.cl_ptr[t.w + 1]; ++e) {
+              const SnQuad c = plan.clist[e];
+              bool child = false;
+              for (int a = plan.ch_ptr[t.x]; a < plan.ch_ptr[t.x + 1]; ++a) child |= plan.ch[a] == c.x;
+              if (!child || c.y < 0 || c.y >= c.z || c.z > plan.nrow[c.x]) return -45;
+              const int *rel = plan.rel.data() + plan.rel_off[c.x];
+              if (rel[c.y] < t.y || rel[c.z - 1] >= t.z) return -46;
+            }
+          }
           if ((L.kind == SN_SMALL_FACTOR || L.kind == SN_FWD_SMALL || L.kind == SN_BWD_SMALL) &&
               (plan.large[t.x] || ld > kSnSmallMax))
             return -42;

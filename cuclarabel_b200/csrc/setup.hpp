@@ -73,6 +73,9 @@ struct Prepared {
   std::vector<int> amapk;  // 2 per A entry: kkt1, kkt2
   int p_user_nnz = 0;
   bool updatable = true;
+  // equilibration left to the device (SetupOptions::defer_equilibration):
+  // d, e = 1, c = 1 and the data unscaled here
+  bool eq_deferred = false;
   // for gathering rhs / scattering solution: permuted k -> local original idx
   // (0..n-1 x, n..n+m-1 z type-major local row, >= n+m extra)
 };
@@ -81,6 +84,9 @@ struct SetupOptions {
   int soc_threshold = 5;
   int equilibrate_enable = 1, equilibrate_max_iter = 10;
   double equilibrate_min_scaling = 1e-4, equilibrate_max_scaling = 1e4;
+  // leave the Ruiz equilibration (and so the KKT values) to the device when
+  // the caller's P and A columns are sorted without repeated entries
+  bool defer_equilibration = false;
 };
 
 bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt,

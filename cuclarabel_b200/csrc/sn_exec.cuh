@@ -20,8 +20,10 @@ struct SnDev {
   const long long *foff, *woff, *soff;
   const int2 *amap;
   const int4 *tasks;
+  const int *cl_ptr;   // per chunk of a blocked front: its children in clist
+  const int4 *clist;   // {child, q_begin, q_end}
   void *F;       // fronts (T)
-  void *W;       // factor workspace of blocked fronts (T): Linv, dinv, W
+  void *W;       // factor workspace of blocked fronts (T): dinv, W
   double *S;     // solve workspace of blocked fronts: work vector, partial sums
   double *U;     // forward-substitution contributions, nrow per supernode
   double *Dinv;  // [global vector index] 1 / pivot
@@ -48,8 +50,25 @@ struct SnExec {
   unsigned long long *h_nrm = nullptr;  // pinned [2 B]
   int *d_flags = nullptr;               // [B]
   long long launches = 0;               // kernel launches issued (statistics)
+  // refinement statistics since profiling was switched on: solves, sweeps,
+  // solves that stopped above the tolerance, and the worst such final
+  // |e|_inf / (abstol + reltol |b|_inf)
+  long long ir_solves = 0, ir_sweeps = 0, ir_unconverged = 0;
+  double ir_worst = 0.0;
+  // profiling: every launch bracketed by CUDA events, device time and
+  // algorithmic flops summed per launch kind (SnLaunchKind)
+  struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<int> kinds;  // kind of event pair k (events 2k, 2k + 1)
+    double ms[SN_KINDS] = {}, flops[SN_KINDS] = {};
+    long long calls[SN_KINDS] = {};
+  } prof;
   ~SnExec();
 };
+// profiling on / off (turning it on clears the totals) and the totals
+void sn_set_profiling(SnExec &ex, bool on);
+void sn_get_profile(const SnExec &ex, double *ms, double *flops, long long *calls);
 
 // Uploads the plan and allocates the fronts and workspaces (arena-owned).
 // false when an allocation fails.

@@ -337,7 +337,7 @@ bool sn_build_plan(const std::vector<SnInstance> &in, SnPlan &P, std::string *er
       fo += align32((long long)P.ld[s] * P.ld[s]);
       if (lg) {
         P.woff[s] = wo;
-        wo += align32((long long)kSnNB * kSnNB + kSnNB + (long long)P.ld[s] * kSnNB);
+        wo += align32(kSnNB + (long long)P.ld[s] * kSnNB);
         P.soff[s] = so;
         so += align32(2LL * P.ld[s]);
       }
@@ -426,14 +426,40 @@ bool sn_build_plan(const std::vector<SnInstance> &in, SnPlan &P, std::string *er
     }
     sbase += S.ns();
   }
+  // ---- children per chunk of the blocked fronts (assembly, forward gather)
+  P.chunk_off.assign(ns + 1, 0);
+  for (int s = 0; s < ns; ++s)
+    P.chunk_off[s + 1] = P.chunk_off[s] + (P.large[s] ? (P.ld[s] + kSnAsmCols - 1) / kSnAsmCols : 0);
+  {
+    std::vector<std::vector<SnQuad>> lists(P.chunk_off[ns]);
+    for (int s = 0; s < ns; ++s) {
+      if (!P.large[s]) continue;
+      for (int a = P.ch_ptr[s]; a < P.ch_ptr[s + 1]; ++a) {
+        const int c = P.ch[a], cn = P.nrow[c];
+        const int *rel = P.rel.data() + P.rel_off[c];
+        for (int q = 0; q < cn;) {
+          const int chunk = rel[q] / kSnAsmCols;
+          int qe = q + 1;
+          while (qe < cn && rel[qe] / kSnAsmCols == chunk) ++qe;
+          lists[P.chunk_off[s] + chunk].push_back({c, q, qe, 0});
+          q = qe;
+        }
+      }
+    }
+    P.cl_ptr.assign(P.chunk_off[ns] + 1, 0);
+    for (size_t g = 0; g < lists.size(); ++g) P.cl_ptr[g + 1] = P.cl_ptr[g] + (int)lists[g].size();
+    P.clist.reserve(P.cl_ptr.back());
+    for (auto &l : lists) P.clist.insert(P.clist.end(), l.begin(), l.end());
+  }
   // ---- schedules, level by level
   int H = 0;
   for (int s = 0; s < ns; ++s) H = std::max(H, level[s] + 1);
   std::vector<std::vector<int>> small(H), big(H);
   for (int s = 0; s < ns; ++s) (P.large[s] ? big : small)[level[s]].push_back(s);
-  auto launch = [&](std::vector<SnLaunch> &sched, int kind, int begin, int smem = 0) {
+  auto launch = [&](std::vector<SnLaunch> &sched, int kind, int begin, int smem = 0,
+                    double fl = 0.0) {
     const int count = (int)P.tasks.size() - begin;
-    if (count > 0) sched.push_back({kind, begin, count, smem});
+    if (count > 0) sched.push_back({kind, begin, count, smem, fl});
   };
   auto kK = [](int k, int K) { return k | (K << 16); };
   std::vector<std::pair<int, int>> pan;
@@ -441,21 +467,24 @@ bool sn_build_plan(const std::vector<SnInstance> &in, SnPlan &P, std::string *er
   for (int L = 0; L < H; ++L) {
     // factorisation
     int b0 = (int)P.tasks.size(), smem = 0;
+    double fl = 0;
     for (int s : small[L]) {
       P.tasks.push_back({s, 0, 0, 0});
       smem = std::max(smem, P.ld[s] * P.ld[s]);
       for (int c = 0; c < P.ncol[s]; ++c) {
         const double below = P.ld[s] - 1 - c;
-        flops += below * below;
+        fl += below * below;
       }
     }
+    flops += fl;
     P.small_smem_max = std::max(P.small_smem_max, smem);
-    launch(P.fact, SN_SMALL_FACTOR, b0, smem);
+    launch(P.fact, SN_SMALL_FACTOR, b0, smem, fl);
     if (big[L].empty()) continue;
     b0 = (int)P.tasks.size();
     for (int s : big[L])
       for (int c = 0; c < P.ld[s]; c += kSnAsmCols)
-        P.tasks.push_back({s, c, std::min(P.ld[s], c + kSnAsmCols), 0});
+        P.tasks.push_back({s, c, std::min(P.ld[s], c + kSnAsmCols),
+                           P.chunk_off[s] + c / kSnAsmCols});
     launch(P.fact, SN_ASSEMBLE, b0);
     std::vector<std::vector<std::pair<int, int>>> pl(big[L].size());
     size_t maxp = 0;
@@ -464,27 +493,47 @@ bool sn_build_plan(const std::vector<SnInstance> &in, SnPlan &P, std::string *er
       maxp = std::max(maxp, pl[a].size());
     }
     for (size_t p = 0; p < maxp; ++p) {
+      // flops: 2 K^3 / 3 per diagonal block; K^2 per TRSM row; 2 K per
+      // lower-triangle entry of the update
       b0 = (int)P.tasks.size();
+      fl = 0;
       for (size_t a = 0; a < big[L].size(); ++a)
-        if (p < pl[a].size()) P.tasks.push_back({big[L][a], kK(pl[a][p].first, pl[a][p].second), 0, 0});
-      launch(P.fact, SN_DIAG, b0);
+        if (p < pl[a].size()) {
+          const int K = pl[a][p].second;
+          P.tasks.push_back({big[L][a], kK(pl[a][p].first, K), 0, 0});
+          fl += 2.0 * K * K * K / 3.0;
+        }
+      flops += fl;
+      launch(P.fact, SN_DIAG, b0, 0, fl);
       b0 = (int)P.tasks.size();
+      fl = 0;
       for (size_t a = 0; a < big[L].size(); ++a) {
         if (p >= pl[a].size()) continue;
         const int s = big[L][a], k = pl[a][p].first, K = pl[a][p].second, e = k + K;
-        for (int r0 = e; r0 < P.ld[s]; r0 += kSnNB) P.tasks.push_back({s, kK(k, K), r0, 0});
+        for (int r0 = e; r0 < P.ld[s]; r0 += kSnNB) {
+          P.tasks.push_back({s, kK(k, K), r0, 0});
+          fl += 1.0 * K * K * kSnNB;
+        }
       }
-      launch(P.fact, SN_TRSM, b0);
+      flops += fl;
+      launch(P.fact, SN_TRSM, b0, 0, fl);
       b0 = (int)P.tasks.size();
+      fl = 0;
       for (size_t a = 0; a < big[L].size(); ++a) {
         if (p >= pl[a].size()) continue;
         const int s = big[L][a], k = pl[a][p].first, K = pl[a][p].second, e = k + K;
-        const double T = (P.ld[s] - e) / kSnNB;
-        flops += (double)K * K * K + 2.0 * K * K * kSnNB * T + 2.0 * K * kSnNB * kSnNB * T * (T + 1) / 2;
-        for (int c0 = e; c0 < P.ld[s]; c0 += kSnNB)
-          for (int r0 = c0; r0 < P.ld[s]; r0 += kSnNB) P.tasks.push_back({s, kK(k, K), r0, c0});
+        // 128 x 64 tiles: for every 64-column block, the 128-row tiles from
+        // the one holding its diagonal down
+        for (int c0 = e; c0 < P.ld[s]; c0 += 64)
+          for (int r0 = e + (c0 - e) / kSnNB * kSnNB; r0 < P.ld[s]; r0 += kSnNB) {
+            P.tasks.push_back({s, kK(k, K), r0, c0});
+            double below = 0;  // entries on or below the diagonal
+            for (int n = 0; n < 64; ++n) below += std::max(0, std::min(kSnNB, r0 + kSnNB - c0 - n));
+            fl += 2.0 * below * K;
+          }
       }
-      launch(P.fact, SN_UPDATE, b0);
+      flops += fl;
+      launch(P.fact, SN_UPDATE, b0, 0, fl);
     }
   }
   P.flops = flops;
@@ -495,7 +544,10 @@ bool sn_build_plan(const std::vector<SnInstance> &in, SnPlan &P, std::string *er
     launch(P.fwd, SN_FWD_SMALL, b0);
     if (big[L].empty()) continue;
     b0 = (int)P.tasks.size();
-    for (int s : big[L]) P.tasks.push_back({s, 0, 0, 0});
+    for (int s : big[L])
+      for (int c = 0; c < P.ld[s]; c += kSnAsmCols)
+        P.tasks.push_back({s, c, std::min(P.ld[s], c + kSnAsmCols),
+                           P.chunk_off[s] + c / kSnAsmCols});
     launch(P.fwd, SN_FWD_GATHER, b0);
     std::vector<std::vector<std::pair<int, int>>> pl(big[L].size());
     size_t maxp = 0;

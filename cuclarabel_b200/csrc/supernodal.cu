@@ -14,13 +14,13 @@
 //   blocked       k_sn_assemble zeroes and assembles column ranges of the
 //   fronts        front (a task owns its columns, so children are added in a
 //                 fixed order without atomics), then per panel of K <= 128
-//                 pivots: k_sn_diag factors the K x K diagonal block and
-//                 inverts its unit L, k_sn_gemm<TRSM> forms W = A Linv^T and
-//                 L = W D^-1 for every 128-row tile below, and
-//                 k_sn_gemm<UPDATE> subtracts L W^T from every lower tile of
-//                 the trailing matrix.  FP64 tiles run on the tensor cores
-//                 (DMMA, mma.sync m8n8k4), FP32 tiles (mixed form) on FMA
-//                 units; both stage their operands with cp.async.
+//                 pivots: k_sn_diag factors the K x K diagonal block,
+//                 k_sn_trsm solves every 128-row tile below by triangular
+//                 substitution (W = A L11^-T, L = W D^-1), and
+//                 k_sn_update_* subtracts L W^T from every lower tile of the
+//                 trailing matrix.  FP64 tiles run on the tensor cores (DMMA,
+//                 mma.sync m8n8k4), FP32 tiles (mixed form) on FMA units;
+//                 both stage their operands with cp.async.
 // Solve: forward substitution leaves first (small fronts one warp each,
 // blocked fronts panel by panel: diagonal solve then a matrix-vector
 // update of the rows below), D^-1, backward substitution roots first.
@@ -37,10 +37,15 @@ namespace clgpu {
 
 namespace {
 
-constexpr int kGemmKC = 8;       // k per pipeline stage
-constexpr int kGemmStages = 4;   // cp.async stages
-constexpr int kGemmLd = kSnNB + 4;  // shared row stride (elements): conflict-free fragments
+// trailing update tiles: 128 rows x kUpdCols columns, k in chunks of kUpdKC
+constexpr int kUpdCols = 64;
+constexpr int kUpdKC = 16;
+constexpr int kUpdStages = 3;
+constexpr int kUpdLdA = kSnNB + 4;     // shared row strides (elements): 4 mod 16 (FP64
+constexpr int kUpdLdB = kUpdCols + 4;  // banks), so DMMA fragment loads are conflict-free
+static_assert(kSnKPad % kUpdKC == 0, "panel widths are whole update chunks");
 constexpr int kDiagThreads = 256;
+constexpr int kTrsmThreads = 256;
 constexpr int kAsmThreads = 256;
 constexpr int kSmallThreads = 128;
 constexpr int kVecThreads = 128;
@@ -137,10 +142,14 @@ __global__ void __launch_bounds__(kSmallThreads) k_sn_small(SnDev d, KKTDev k, L
     const T dj = T(sn_pivot(double(f[j * ld + j]), k.Dsign[g], prm));
     for (int i = j + 1 + tid; i < ld; i += kSmallThreads) col[i] = f[j * ld + i];
     __syncthreads();
-    const int rem = ld - j - 1;
-    for (int idx = tid; idx < rem * rem; idx += kSmallThreads) {
-      const int r = j + 1 + idx / rem, i = j + 1 + idx % rem;
-      if (i >= r) f[r * ld + i] -= (col[i] / dj) * col[r];
+    {
+      // rank-1 update of the trailing lower triangle: 16 x 8 threads
+      const int tx = tid & 15, ty = tid >> 4;
+      for (int r = j + 1 + ty; r < ld; r += kSmallThreads / 16) {
+        const T cr = col[r];
+        for (int i = j + 1 + tx; i < ld; i += 16)
+          if (i >= r) f[r * ld + i] -= (col[i] / dj) * cr;
+      }
     }
     for (int i = j + 1 + tid; i < ld; i += kSmallThreads) f[j * ld + i] = col[i] / dj;
     if (tid == 0) {
@@ -162,7 +171,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_sn_small(SnDev d, KKTDev k, L
 // ------------------------------------------------------- blocked fronts
 // Assembly of columns [ca, cb) of a blocked front: zero (rows c..ld), the
 // original entries (+ static regularisation), unit dummy pivots, then the
-// children's Schur complements in order.
+// Schur complements of the children that touch these columns, in child
+// order (the plan lists them per 32-column chunk with their entry ranges).
 template <typename T>
 __global__ void __launch_bounds__(kAsmThreads) k_sn_assemble(SnDev d, KKTDev k, int base,
                                                             const int *run) {
@@ -190,23 +200,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_sn_assemble(SnDev d, KKTDev k, 
   for (int c = max(ca, nc) + tid; c < min(cb, u0); c += kAsmThreads) f[c * ld + c] = T(1);
   __syncthreads();
   const T *F = reinterpret_cast<const T *>(d.F);
-  for (int a = d.ch_ptr[s]; a < d.ch_ptr[s + 1]; ++a) {
-    const int c = d.ch[a], cn = d.nrow[c], cu = d.u0[c];
+  // the children touching columns [ca, cb), in child order (plan)
+  for (int a = d.cl_ptr[t.w]; a < d.cl_ptr[t.w + 1]; ++a) {
+    const int4 cq = d.clist[a];
+    const int c = cq.x, qa = cq.y, qb = cq.z, cn = d.nrow[c], cu = d.u0[c];
     const long long cld = d.ld[c];
     const int *rel = d.rel + d.rel_off[c];
-    // child columns whose parent position lies in [ca, cb): rel is increasing
-    int lo = 0, hi = cn;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (rel[mid] < ca) lo = mid + 1; else hi = mid;
-    }
-    const int qa = lo;
-    hi = cn;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (rel[mid] < cb) lo = mid + 1; else hi = mid;
-    }
-    const int qb = lo;
     const T *cf = F + d.foff[c];
     for (int q = qa; q < qb; ++q) {
       const long long pc = rel[q];
@@ -218,8 +217,8 @@ __global__ void __launch_bounds__(kAsmThreads) k_sn_assemble(SnDev d, KKTDev k, 
 }
 
 // Diagonal block of a panel: factor the K x K block (right-looking, the
-// static shift was applied at assembly), write L11 and D, and the inverse
-// of the unit L11 (zero-padded to kSnNB x kSnNB) and 1/d to the workspace.
+// static shift was applied at assembly), write L11 and D to the front and
+// 1/d to the workspace.
 template <typename T>
 __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDLParams prm,
                                                          int base, const int *run, int *ok) {
@@ -244,10 +243,15 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
     const T dj = T(sn_pivot(double(blk[j * K + j]), pivot_sign(k, fi[k0 + j]), prm));
     for (int i = j + 1 + tid; i < K; i += kDiagThreads) col[i] = blk[j * K + i];
     __syncthreads();
-    const int rem = K - j - 1;
-    for (int idx = tid; idx < rem * rem; idx += kDiagThreads) {
-      const int r = j + 1 + idx / rem, i = j + 1 + idx % rem;
-      if (i >= r) blk[r * K + i] -= (col[i] / dj) * col[r];
+    // rank-1 update of the trailing lower triangle: 16 x 16 threads, thread
+    // (tx, ty) takes columns j+1+ty, +16, ... and rows i >= r, i = j+1+tx, +16, ...
+    {
+      const int tx = tid & 15, ty = tid >> 4;
+      for (int r = j + 1 + ty; r < K; r += 16) {
+        const T cr = col[r];
+        for (int i = j + 1 + tx; i < K; i += 16)
+          if (i >= r) blk[r * K + i] -= (col[i] / dj) * cr;
+      }
     }
     for (int i = j + 1 + tid; i < K; i += kDiagThreads) blk[j * K + i] = col[i] / dj;
     if (tid == 0) {
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
       const double di = 1.0 / double(dj);
       const int g = fi[k0 + j];
       if (g >= 0) d.Dinv[g] = di;
-      ws[kSnNB * kSnNB + j] = T(di);
+      ws[j] = T(di);
       if (!isfinite(di) || !isfinite(double(dj))) bad = true;
     }
     __syncthreads();
@@ -264,50 +268,67 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
     const int c = idx / K, r = idx - c * K;
     if (r >= c) f[(k0 + c) * ld + k0 + r] = blk[idx];
   }
-  for (int j = K + tid; j < kSnNB; j += kDiagThreads) ws[kSnNB * kSnNB + j] = T(0);
-  __syncthreads();
-  // in-place inverse of the unit lower L11: after step t row t of X = L^-1
-  // is final; rows below subtract L(r, t) times it
-  for (int tt = 0; tt + 1 < K; ++tt) {
-    for (int r = tt + 1 + tid; r < K; r += kDiagThreads) col[r] = blk[tt * K + r];
-    __syncthreads();
-    const int w = tt + 1, cnt = (K - 1 - tt) * w;
-    for (int idx = tid; idx < cnt; idx += kDiagThreads) {
-      const int r = tt + 1 + idx / w, c = idx % w;
-      if (c == tt)
-        blk[tt * K + r] = -col[r];
-      else
-        blk[c * K + r] -= col[r] * blk[c * K + tt];
-    }
-    __syncthreads();
-  }
-  for (int idx = tid; idx < kSnNB * kSnNB; idx += kDiagThreads) {
-    const int q = idx / kSnNB, n = idx - q * kSnNB;  // Linv(n, q) at n + q kSnNB
-    T v = T(0);
-    if (n < K && q < K) v = n == q ? T(1) : (n > q ? blk[q * K + n] : T(0));
-    ws[idx] = v;
-  }
+  for (int j = K + tid; j < kSnNB; j += kDiagThreads) ws[j] = T(0);
   if (bad && tid == 0) ok[inst] = 0;
 }
 
-// 128 x 128 tile products of the blocked fronts.
-//   TRSM   (MODE 0): rows r0.. of panel [k, k+K): W = A Linv^T -> workspace,
-//                    L = W diag(1/d) -> front (in place of A)
-//   UPDATE (MODE 1): front tile (r0, c0) -= L(r0.., panel) W(c0.., :)^T,
-//                    lower triangle only on a diagonal tile
-// FP64: 8 warps as 2 (rows) x 4 (columns), warp tile 64 x 32 of m8n8k4 DMMA.
-template <int MODE>
-__global__ void __launch_bounds__(256, 1) k_sn_gemm_f64(SnDev d, int base, const int *run) {
+// TRSM of a panel's row tile: rows r0..r0+127 of panel [k0, k0+K),
+// W = A L11^-T by column-oriented substitution (after step j column j of W
+// is final and is subtracted, times L11(t, j), from every later column t),
+// then L = W D^-1: L overwrites A in the front, W goes to the workspace for
+// the trailing update.  The tile (K x 128) and the strict lower triangle of
+// L11 (packed by columns) sit in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(kTrsmThreads) k_sn_trsm(SnDev d, int base, const int *run) {
+  const int4 t = d.tasks[base + blockIdx.x];
+  const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, r0 = t.z;
+  if (!run[d.inst[s]]) return;
+  extern __shared__ __align__(16) unsigned char sraw[];
+  T *X = reinterpret_cast<T *>(sraw);  // column q of the tile at X + q kSnNB
+  T *Lp = X + K * kSnNB;               // column j of L11 below the diagonal at Lp + cs(j)
+  const long long ld = d.ld[s];
+  T *f = reinterpret_cast<T *>(d.F) + d.foff[s];
+  const T *ws = reinterpret_cast<const T *>(d.W) + d.woff[s];
+  T *wr = reinterpret_cast<T *>(d.W) + d.woff[s] + kSnNB;
+  const int tid = threadIdx.x;
+  auto cs = [K](int j) { return j * (K - 1) - j * (j - 1) / 2; };
+  for (int idx = tid; idx < K * kSnNB; idx += kTrsmThreads) {
+    const int q = idx / kSnNB, m = idx - q * kSnNB;
+    X[idx] = f[(k0 + q) * ld + r0 + m];
+  }
+  for (int j = 0; j < K; ++j)
+    for (int i = j + 1 + tid; i < K; i += kTrsmThreads) Lp[cs(j) + i - j - 1] = f[(k0 + j) * ld + k0 + i];
+  __syncthreads();
+  const int m = tid & (kSnNB - 1), half = tid / kSnNB;
+  for (int j = 0; j + 1 < K; ++j) {
+    const T xj = X[j * kSnNB + m];
+    const T *lc = Lp + cs(j) - j - 1;
+    for (int q = j + 1 + half; q < K; q += kTrsmThreads / kSnNB) X[q * kSnNB + m] -= xj * lc[q];
+    __syncthreads();
+  }
+  for (int idx = tid; idx < K * kSnNB; idx += kTrsmThreads) {
+    const int q = idx / kSnNB, mm = idx - q * kSnNB;
+    const T w = X[idx];
+    wr[(long long)q * ld + r0 + mm] = w;
+    f[(k0 + q) * ld + r0 + mm] = w * ws[q];
+  }
+}
+
+// Trailing update of the blocked fronts, one 128 x 64 tile per block:
+// front tile (r0, c0) -= L(r0.., panel) W(c0.., :)^T, entries on or below
+// the diagonal only (r0 + m >= c0 + n).  K (a multiple of kSnKPad = 16) is
+// streamed in chunks of kUpdKC through a kUpdStages-deep cp.async pipeline;
+// two blocks are resident per SM, so one's prologue and epilogue overlap the
+// other's main loop.
+// FP64: 4 warps as 2 (rows) x 2 (columns), warp tile 64 x 32 of m8n8k4 DMMA.
+__global__ void __launch_bounds__(128, 2) k_sn_update_f64(SnDev d, int base, const int *run) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, r0 = t.z, c0 = t.w;
   if (!run[d.inst[s]]) return;
   const long long ld = d.ld[s];
   double *f = reinterpret_cast<double *>(d.F) + d.foff[s];
-  double *ws = reinterpret_cast<double *>(d.W) + d.woff[s];
-  double *wr = ws + kSnNB * kSnNB + kSnNB;
   const double *Ag = f + k0 * ld + r0;
-  const double *Bg = MODE == 0 ? ws : wr + c0;
-  const long long ldb = MODE == 0 ? kSnNB : ld;
+  const double *Bg = reinterpret_cast<const double *>(d.W) + d.woff[s] + kSnNB + c0;
   extern __shared__ __align__(16) unsigned char sraw[];
   double *sm = reinterpret_cast<double *>(sraw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -317,37 +338,41 @@ __global__ void __launch_bounds__(256, 1) k_sn_gemm_f64(SnDev d, int base, const
   for (int mi = 0; mi < 8; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-  const int nchunks = K / kGemmKC;
+  const int nchunks = K / kUpdKC;
+  constexpr int kStage = kUpdKC * (kUpdLdA + kUpdLdB);
   auto load = [&](int chunk, int stage) {
-    double *As = sm + stage * 2 * kGemmKC * kGemmLd, *Bs = As + kGemmKC * kGemmLd;
-    for (int p = tid; p < kGemmKC * (kSnNB / 2); p += 256) {
-      const int q = p / (kSnNB / 2), m = (p % (kSnNB / 2)) * 2;
-      const long long kq = (long long)chunk * kGemmKC + q;
-      cp_async16(As + q * kGemmLd + m, Ag + kq * ld + m);
-      cp_async16(Bs + q * kGemmLd + m, Bg + kq * ldb + m);
+    double *As = sm + stage * kStage, *Bs = As + kUpdKC * kUpdLdA;
+    // A: kUpdKC columns x 64 pieces of 16 B; B: kUpdKC x 32
+    for (int p = tid; p < kUpdKC * 64; p += 128) {
+      const int q = p >> 6, m = (p & 63) * 2;
+      cp_async16(As + q * kUpdLdA + m, Ag + ((long long)chunk * kUpdKC + q) * ld + m);
+    }
+    for (int p = tid; p < kUpdKC * 32; p += 128) {
+      const int q = p >> 5, n = (p & 31) * 2;
+      cp_async16(Bs + q * kUpdLdB + n, Bg + ((long long)chunk * kUpdKC + q) * ld + n);
     }
   };
 #pragma unroll
-  for (int st = 0; st < kGemmStages - 1; ++st) {
+  for (int st = 0; st < kUpdStages - 1; ++st) {
     if (st < nchunks) load(st, st);
     cp_async_commit();
   }
   for (int c = 0; c < nchunks; ++c) {
-    cp_async_wait<kGemmStages - 2>();
+    cp_async_wait<kUpdStages - 2>();
     __syncthreads();
-    const int nx = c + kGemmStages - 1;
-    if (nx < nchunks) load(nx, nx % kGemmStages);
+    const int nx = c + kUpdStages - 1;
+    if (nx < nchunks) load(nx, nx % kUpdStages);
     cp_async_commit();
-    const double *As = sm + (c % kGemmStages) * 2 * kGemmKC * kGemmLd;
-    const double *Bs = As + kGemmKC * kGemmLd;
+    const double *As = sm + (c % kUpdStages) * kStage;
+    const double *Bs = As + kUpdKC * kUpdLdA;
 #pragma unroll
-    for (int kk = 0; kk < kGemmKC; kk += 4) {
-      const int row = (kk + (lane & 3)) * kGemmLd + (lane >> 2);
+    for (int kk = 0; kk < kUpdKC; kk += 4) {
+      const int q = kk + (lane & 3);
       double a[8], b[4];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi) a[mi] = As[row + wm * 64 + mi * 8];
+      for (int mi = 0; mi < 8; ++mi) a[mi] = As[q * kUpdLdA + wm * 64 + mi * 8 + (lane >> 2)];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[row + wn * 32 + ni * 8];
+      for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[q * kUpdLdB + wn * 32 + ni * 8 + (lane >> 2)];
 #pragma unroll
       for (int mi = 0; mi < 8; ++mi)
 #pragma unroll
@@ -355,8 +380,7 @@ __global__ void __launch_bounds__(256, 1) k_sn_gemm_f64(SnDev d, int base, const
     }
   }
   cp_async_wait<0>();
-  __syncthreads();
-  const double *dinv = ws + kSnNB * kSnNB;
+  const bool diag = r0 < c0 + 64;  // the tile reaches above the diagonal
 #pragma unroll
   for (int mi = 0; mi < 8; ++mi) {
     const int m = wm * 64 + mi * 8 + (lane >> 2);
@@ -365,68 +389,61 @@ __global__ void __launch_bounds__(256, 1) k_sn_gemm_f64(SnDev d, int base, const
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int n = wn * 32 + ni * 8 + 2 * (lane & 3) + h;
-        const double v = acc[mi][ni][h];
-        if (MODE == 0) {
-          if (n < K) {
-            wr[(long long)n * ld + r0 + m] = v;
-            f[(long long)(k0 + n) * ld + r0 + m] = v * dinv[n];
-          }
-        } else {
-          if (r0 != c0 || m >= n) f[(long long)(c0 + n) * ld + r0 + m] -= v;
-        }
+        if (!diag || r0 + m >= c0 + n) f[(long long)(c0 + n) * ld + r0 + m] -= acc[mi][ni][h];
       }
   }
 }
 
-// FP32 form: 16 x 16 threads, each 8 x 8 outputs (rows ty*4 + {0..3} and
-// 64 + ty*4 + {0..3}, columns likewise with tx), FMA units.
-template <int MODE>
-__global__ void __launch_bounds__(256) k_sn_gemm_f32(SnDev d, int base, const int *run) {
+// FP32 form: 16 x 8 threads, each 8 x 8 outputs (rows ty*4 + {0..3} and
+// 64 + ty*4 + {0..3}; columns tx*4 + {0..3} and 32 + tx*4 + {0..3}), FMA units.
+__global__ void __launch_bounds__(128, 2) k_sn_update_f32(SnDev d, int base, const int *run) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, r0 = t.z, c0 = t.w;
   if (!run[d.inst[s]]) return;
   const long long ld = d.ld[s];
   float *f = reinterpret_cast<float *>(d.F) + d.foff[s];
-  float *ws = reinterpret_cast<float *>(d.W) + d.woff[s];
-  float *wr = ws + kSnNB * kSnNB + kSnNB;
   const float *Ag = f + k0 * ld + r0;
-  const float *Bg = MODE == 0 ? ws : wr + c0;
-  const long long ldb = MODE == 0 ? kSnNB : ld;
+  const float *Bg = reinterpret_cast<const float *>(d.W) + d.woff[s] + kSnNB + c0;
   extern __shared__ __align__(16) unsigned char sraw[];
   float *sm = reinterpret_cast<float *>(sraw);
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
   float acc[8][8];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-  const int nchunks = K / kGemmKC;
+  const int nchunks = K / kUpdKC;
+  constexpr int kStage = kUpdKC * (kUpdLdA + kUpdLdB);
   auto load = [&](int chunk, int stage) {
-    float *As = sm + stage * 2 * kGemmKC * kGemmLd, *Bs = As + kGemmKC * kGemmLd;
-    const int q = tid / (kSnNB / 4), m = (tid % (kSnNB / 4)) * 4;  // 8 x 32 pieces
-    const long long kq = (long long)chunk * kGemmKC + q;
-    cp_async16(As + q * kGemmLd + m, Ag + kq * ld + m);
-    cp_async16(Bs + q * kGemmLd + m, Bg + kq * ldb + m);
+    float *As = sm + stage * kStage, *Bs = As + kUpdKC * kUpdLdA;
+    for (int p = tid; p < kUpdKC * 32; p += 128) {  // 16 B = 4 floats
+      const int q = p >> 5, m = (p & 31) * 4;
+      cp_async16(As + q * kUpdLdA + m, Ag + ((long long)chunk * kUpdKC + q) * ld + m);
+    }
+    for (int p = tid; p < kUpdKC * 16; p += 128) {
+      const int q = p >> 4, n = (p & 15) * 4;
+      cp_async16(Bs + q * kUpdLdB + n, Bg + ((long long)chunk * kUpdKC + q) * ld + n);
+    }
   };
 #pragma unroll
-  for (int st = 0; st < kGemmStages - 1; ++st) {
+  for (int st = 0; st < kUpdStages - 1; ++st) {
     if (st < nchunks) load(st, st);
     cp_async_commit();
   }
   for (int c = 0; c < nchunks; ++c) {
-    cp_async_wait<kGemmStages - 2>();
+    cp_async_wait<kUpdStages - 2>();
     __syncthreads();
-    const int nx = c + kGemmStages - 1;
-    if (nx < nchunks) load(nx, nx % kGemmStages);
+    const int nx = c + kUpdStages - 1;
+    if (nx < nchunks) load(nx, nx % kUpdStages);
     cp_async_commit();
-    const float *As = sm + (c % kGemmStages) * 2 * kGemmKC * kGemmLd;
-    const float *Bs = As + kGemmKC * kGemmLd;
+    const float *As = sm + (c % kUpdStages) * kStage;
+    const float *Bs = As + kUpdKC * kUpdLdA;
 #pragma unroll
-    for (int q = 0; q < kGemmKC; ++q) {
-      const float4 a0 = *reinterpret_cast<const float4 *>(As + q * kGemmLd + ty * 4);
-      const float4 a1 = *reinterpret_cast<const float4 *>(As + q * kGemmLd + 64 + ty * 4);
-      const float4 b0 = *reinterpret_cast<const float4 *>(Bs + q * kGemmLd + tx * 4);
-      const float4 b1 = *reinterpret_cast<const float4 *>(Bs + q * kGemmLd + 64 + tx * 4);
+    for (int q = 0; q < kUpdKC; ++q) {
+      const float4 a0 = *reinterpret_cast<const float4 *>(As + q * kUpdLdA + ty * 4);
+      const float4 a1 = *reinterpret_cast<const float4 *>(As + q * kUpdLdA + 64 + ty * 4);
+      const float4 b0 = *reinterpret_cast<const float4 *>(Bs + q * kUpdLdB + tx * 4);
+      const float4 b1 = *reinterpret_cast<const float4 *>(Bs + q * kUpdLdB + 32 + tx * 4);
       const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
       const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
@@ -436,23 +453,14 @@ __global__ void __launch_bounds__(256) k_sn_gemm_f32(SnDev d, int base, const in
     }
   }
   cp_async_wait<0>();
-  __syncthreads();
-  const float *dinv = ws + kSnNB * kSnNB;
+  const bool diag = r0 < c0 + 64;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int m = (i < 4 ? 0 : 64) + ty * 4 + (i & 3);
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const int n = (j < 4 ? 0 : 64) + tx * 4 + (j & 3);
-      const float v = acc[i][j];
-      if (MODE == 0) {
-        if (n < K) {
-          wr[(long long)n * ld + r0 + m] = v;
-          f[(long long)(k0 + n) * ld + r0 + m] = v * dinv[n];
-        }
-      } else {
-        if (r0 != c0 || m >= n) f[(long long)(c0 + n) * ld + r0 + m] -= v;
-      }
+      const int n = (j < 4 ? 0 : 32) + tx * 4 + (j & 3);
+      if (!diag || r0 + m >= c0 + n) f[(long long)(c0 + n) * ld + r0 + m] -= acc[i][j];
     }
   }
 }
@@ -483,9 +491,26 @@ __global__ void __launch_bounds__(256) k_sn_fwd_small(SnDev d, int base, int cou
     __syncwarp();
   }
   const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s];
+  // lane holds rows lane + 32 r (ld <= 128); column j + 1 is loaded while
+  // column j is applied, so the dependent chain waits on shared memory only
+  double cur[4], nxt[4];
+  auto column = [&](int j, double (&o)[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = lane + 32 * r;
+      o[r] = (j < nc && i > j && i < ld) ? double(f[j * ld + i]) : 0.0;
+    }
+  };
+  column(0, cur);
   for (int j = 0; j < nc; ++j) {
+    column(j + 1, nxt);
     const double vj = v[j];
-    for (int i = j + 1 + lane; i < ld; i += 32) v[i] -= double(f[j * ld + i]) * vj;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = lane + 32 * r;
+      if (i > j && i < ld) v[i] -= cur[r] * vj;
+      cur[r] = nxt[r];
+    }
     __syncwarp();
   }
   for (int i = lane; i < nc; i += 32) y[vix(d, d.col0g[s] + i)] = v[i];
@@ -509,9 +534,25 @@ __global__ void __launch_bounds__(256) k_sn_bwd_small(SnDev d, int base, int cou
   for (int i = lane; i < ld; i += 32) v[i] = y[vix(d, fi[i])];
   __syncwarp();
   const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s];
+  // column j - 1 is loaded while column j's dot product runs
+  double cur[4], nxt[4];
+  auto column = [&](int j, double (&o)[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = lane + 32 * r;
+      o[r] = (j >= 0 && i > j && i < ld) ? double(f[j * ld + i]) : 0.0;
+    }
+  };
+  column(nc - 1, cur);
   for (int j = nc - 1; j >= 0; --j) {
+    column(j - 1, nxt);
     double t = 0;
-    for (int i = j + 1 + lane; i < ld; i += 32) t += double(f[j * ld + i]) * v[i];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = lane + 32 * r;
+      if (i > j && i < ld) t += cur[r] * v[i];
+      cur[r] = nxt[r];
+    }
     t = warp_sum(t);
     if (lane == 0) v[j] -= t;
     __syncwarp();
@@ -519,43 +560,57 @@ __global__ void __launch_bounds__(256) k_sn_bwd_small(SnDev d, int base, int cou
   for (int i = lane; i < nc; i += 32) y[vix(d, d.col0g[s] + i)] = v[i];
 }
 
-// blocked fronts: work vector v (ld) from y and the children's contributions
-__global__ void __launch_bounds__(kVecThreads) k_sn_fwd_gather(SnDev d, int base) {
-  const int s = d.tasks[base + blockIdx.x].x;
+// blocked fronts: positions [ca, cb) of the work vector v (ld) from y and
+// the contributions of the children touching them (in child order); one
+// warp per 32-position chunk
+__global__ void __launch_bounds__(256) k_sn_fwd_gather(SnDev d, int base, int count) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ti = blockIdx.x * 8 + w;
+  if (ti >= count) return;
+  const int4 t = d.tasks[base + ti];
+  const int s = t.x, ca = t.y, cb = t.z;
   if (!d.srun[d.inst[s]]) return;
-  const int ld = d.ld[s], nc = d.ncol[s];
+  const int nc = d.ncol[s];
   double *v = d.S + d.soff[s];
-  for (int i = threadIdx.x; i < ld; i += kVecThreads) v[i] = i < nc ? d.y[vix(d, d.col0g[s] + i)] : 0.0;
-  __syncthreads();
-  for (int a = d.ch_ptr[s]; a < d.ch_ptr[s + 1]; ++a) {
-    const int c = d.ch[a], cn = d.nrow[c];
-    const int *rel = d.rel + d.rel_off[c];
-    const double *u = d.U + d.uoff[c];
-    for (int q = threadIdx.x; q < cn; q += kVecThreads) v[rel[q]] += u[q];
-    __syncthreads();
+  const int i = ca + lane;
+  if (i < cb) v[i] = i < nc ? d.y[vix(d, d.col0g[s] + i)] : 0.0;
+  __syncwarp();
+  for (int a = d.cl_ptr[t.w]; a < d.cl_ptr[t.w + 1]; ++a) {
+    const int4 cq = d.clist[a];
+    const int *rel = d.rel + d.rel_off[cq.x];
+    const double *u = d.U + d.uoff[cq.x];
+    for (int q = cq.y + lane; q < cq.z; q += 32) v[rel[q]] += u[q];
+    __syncwarp();
   }
 }
 
-// forward: v[k..k+K) <- L11^-1 v[k..k+K)
+// forward: v[k..k+K) <- L11^-1 v[k..k+K).  L11's strict lower triangle is
+// first copied to shared memory (coalesced), so the K dependent steps read
+// shared memory only.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_sn_fwd_diag(SnDev d, int base) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16;
   if (!d.srun[d.inst[s]]) return;
+  extern __shared__ __align__(16) unsigned char sraw[];
+  T *Ls = reinterpret_cast<T *>(sraw);  // K x K, column-major, stride K
   __shared__ double x[kSnNB];
   const long long ld = d.ld[s];
   double *v = d.S + d.soff[s] + k0;
   const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + k0;
   const int i = threadIdx.x;
+  for (int j = 0; j < K; ++j)
+    if (i < K) Ls[j * K + i] = f[j * ld + i];
   if (i < K) x[i] = v[i];
   __syncthreads();
+  double xi = i < K ? x[i] : 0.0;
   for (int j = 0; j < K; ++j) {
-    if (i > j && i < K) x[i] -= double(f[j * ld + i]) * x[j];
+    if (i == j) x[j] = xi;
     __syncthreads();
+    if (i > j && i < K) xi -= double(Ls[j * K + i]) * x[j];
   }
-  if (i < K) v[i] = x[i];
+  if (i < K) v[i] = xi;
 }
-
 // forward: v[r0..r0+128) -= L(r0.., panel) v[k..k+K)
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_sn_fwd_gemv(SnDev d, int base) {
@@ -619,29 +674,35 @@ __global__ void __launch_bounds__(kVecThreads) k_sn_bwd_partial(SnDev d, int bas
   }
 }
 
-// backward: v[k..k+K) <- L11^-T (v[k..k+K) - sum of the tiles' partials)
+// backward: v[k..k+K) <- L11^-T (v[k..k+K) - sum of the tiles' partials),
+// the partials summed in tile order; L11 staged in shared memory, then one
+// warp runs the K dependent column dot products
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_sn_bwd_diag(SnDev d, int base) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16;
   if (!d.srun[d.inst[s]]) return;
+  extern __shared__ __align__(16) unsigned char sraw[];
+  T *Ls = reinterpret_cast<T *>(sraw);  // K x K, column-major, stride K
   __shared__ double x[kSnNB];
   const long long ld = d.ld[s];
   double *v = d.S + d.soff[s];
   const double *part = v + ld;
   const int q = threadIdx.x, e = k0 + K;
+  const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + k0;
+  for (int j = 0; j < K; ++j)
+    if (q < K) Ls[j * K + q] = f[j * ld + q];
   if (q < K) {
     double a = v[k0 + q];
     for (long long r0 = e; r0 < ld; r0 += kSnNB) a -= part[r0 + q];
     x[q] = a;
   }
   __syncthreads();
-  const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + k0;
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     for (int j = K - 1; j >= 0; --j) {
       double acc = 0;
-      for (int i = j + 1 + lane; i < K; i += 32) acc += double(f[j * ld + i]) * x[i];
+      for (int i = j + 1 + lane; i < K; i += 32) acc += double(Ls[j * K + i]) * x[i];
       acc = warp_sum(acc);
       if (lane == 0) x[j] -= acc;
       __syncwarp();
@@ -753,8 +814,12 @@ size_t diag_smem() {
   return (size_t)kSnNB * kSnNB * sizeof(T) + kSnNB * sizeof(T);
 }
 template <typename T>
+size_t trsm_smem() {  // the tile (kSnNB x kSnNB) and the packed strict lower L11
+  return (size_t)kSnNB * kSnNB * sizeof(T) + (size_t)kSnNB * (kSnNB - 1) / 2 * sizeof(T);
+}
+template <typename T>
 size_t gemm_smem() {
-  return (size_t)kGemmStages * 2 * kGemmKC * kGemmLd * sizeof(T);
+  return (size_t)kUpdStages * kUpdKC * (kUpdLdA + kUpdLdB) * sizeof(T);
 }
 
 template <typename T>
@@ -765,13 +830,54 @@ void set_sn_attrs() {
                        (int)diag_smem<T>());
   cudaFuncSetAttribute(k_sn_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)((kSnSmallMax * kSnSmallMax + kSnSmallMax) * sizeof(T)));
-  if (sizeof(T) == 8) {
-    cudaFuncSetAttribute(k_sn_gemm_f64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_sn_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)trsm_smem<T>());
+  cudaFuncSetAttribute(k_sn_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(kSnNB * kSnNB * sizeof(T)));
+  cudaFuncSetAttribute(k_sn_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(kSnNB * kSnNB * sizeof(T)));
+  if (sizeof(T) == 8)
+    cudaFuncSetAttribute(k_sn_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)gemm_smem<double>());
-    cudaFuncSetAttribute(k_sn_gemm_f64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)gemm_smem<double>());
-  }
+  else
+    cudaFuncSetAttribute(k_sn_update_f32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)gemm_smem<float>());
   done = true;
+}
+
+// profiling: an event pair around one launch
+void prof_begin(SnExec &ex, const SnLaunch &L, cudaStream_t st) {
+  if (!ex.prof.on) return;
+  auto &P = ex.prof;
+  const size_t k = P.kinds.size();
+  while (P.pool.size() < 2 * k + 2) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      P.on = false;
+      return;
+    }
+    P.pool.push_back(e);
+  }
+  P.kinds.push_back(L.kind);
+  P.flops[L.kind] += L.flops;
+  P.calls[L.kind]++;
+  cudaEventRecord(P.pool[2 * k], st);
+}
+void prof_end(SnExec &ex, cudaStream_t st) {
+  if (!ex.prof.on || ex.prof.kinds.empty()) return;
+  cudaEventRecord(ex.prof.pool[2 * ex.prof.kinds.size() - 1], st);
+}
+// sum the recorded pairs (waits for the last one)
+void prof_collect(SnExec &ex) {
+  auto &P = ex.prof;
+  if (!P.on || P.kinds.empty()) return;
+  cudaEventSynchronize(P.pool[2 * P.kinds.size() - 1]);
+  for (size_t k = 0; k < P.kinds.size(); ++k) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, P.pool[2 * k], P.pool[2 * k + 1]) == cudaSuccess)
+      P.ms[P.kinds[k]] += t;
+  }
+  P.kinds.clear();
 }
 
 template <typename T>
@@ -780,6 +886,7 @@ void run_factor(SnExec &ex, const KKTDev &k, const LDLParams &p, const int *run,
   set_sn_attrs<T>();
   const SnDev &d = ex.d;
   for (const SnLaunch &L : ex.fact) {
+    prof_begin(ex, L, st);
     switch (L.kind) {
       case SN_SMALL_FACTOR:
         k_sn_small<T><<<L.count, kSmallThreads, (L.smem + kSnSmallMax) * sizeof(T), st>>>(
@@ -792,57 +899,89 @@ void run_factor(SnExec &ex, const KKTDev &k, const LDLParams &p, const int *run,
         k_sn_diag<T><<<L.count, kDiagThreads, diag_smem<T>(), st>>>(d, k, p, L.begin, run, ok);
         break;
       case SN_TRSM:
-        if (sizeof(T) == 8)
-          k_sn_gemm_f64<0><<<L.count, 256, gemm_smem<double>(), st>>>(d, L.begin, run);
-        else
-          k_sn_gemm_f32<0><<<L.count, 256, gemm_smem<float>(), st>>>(d, L.begin, run);
+        k_sn_trsm<T><<<L.count, kTrsmThreads, trsm_smem<T>(), st>>>(d, L.begin, run);
         break;
       case SN_UPDATE:
         if (sizeof(T) == 8)
-          k_sn_gemm_f64<1><<<L.count, 256, gemm_smem<double>(), st>>>(d, L.begin, run);
+          k_sn_update_f64<<<L.count, 128, gemm_smem<double>(), st>>>(d, L.begin, run);
         else
-          k_sn_gemm_f32<1><<<L.count, 256, gemm_smem<float>(), st>>>(d, L.begin, run);
+          k_sn_update_f32<<<L.count, 128, gemm_smem<float>(), st>>>(d, L.begin, run);
         break;
       default:
         break;
     }
+    prof_end(ex, st);
     ex.launches++;
   }
+  prof_collect(ex);
 }
 
 // one pass y <- K^-1 y for the instances with srun set
 template <typename T>
 void run_solve_pass(SnExec &ex, cudaStream_t st) {
+  set_sn_attrs<T>();
   const SnDev &d = ex.d;
   for (const SnLaunch &L : ex.fwd) {
+    prof_begin(ex, L, st);
     switch (L.kind) {
       case SN_FWD_SMALL: k_sn_fwd_small<T><<<(L.count + 7) / 8, 256, 0, st>>>(d, L.begin, L.count); break;
-      case SN_FWD_GATHER: k_sn_fwd_gather<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
-      case SN_FWD_DIAG: k_sn_fwd_diag<T><<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
+      case SN_FWD_GATHER: k_sn_fwd_gather<<<(L.count + 7) / 8, 256, 0, st>>>(d, L.begin, L.count); break;
+      case SN_FWD_DIAG:
+        k_sn_fwd_diag<T><<<L.count, kVecThreads, kSnNB * kSnNB * sizeof(T), st>>>(d, L.begin);
+        break;
       case SN_FWD_GEMV: k_sn_fwd_gemv<T><<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
       case SN_FWD_SCATTER: k_sn_fwd_scatter<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
       default: break;
     }
+    prof_end(ex, st);
     ex.launches++;
   }
   k_sn_dscale<<<nb256(d.vcount), 256, 0, st>>>(d);
   for (const SnLaunch &L : ex.bwd) {
+    prof_begin(ex, L, st);
     switch (L.kind) {
       case SN_BWD_SMALL: k_sn_bwd_small<T><<<(L.count + 7) / 8, 256, 0, st>>>(d, L.begin, L.count); break;
       case SN_BWD_GATHER: k_sn_bwd_gather<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
       case SN_BWD_PARTIAL: k_sn_bwd_partial<T><<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
-      case SN_BWD_DIAG: k_sn_bwd_diag<T><<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
+      case SN_BWD_DIAG:
+        k_sn_bwd_diag<T><<<L.count, kVecThreads, kSnNB * kSnNB * sizeof(T), st>>>(d, L.begin);
+        break;
       case SN_BWD_SCATTER: k_sn_bwd_scatter<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
       default: break;
     }
+    prof_end(ex, st);
     ex.launches++;
   }
   ex.launches++;
+  prof_collect(ex);
 }
 
 }  // namespace
 
+void sn_set_profiling(SnExec &ex, bool on) {
+  ex.prof.on = on;
+  ex.prof.kinds.clear();
+  if (on) {
+    ex.ir_solves = ex.ir_sweeps = ex.ir_unconverged = 0;
+    ex.ir_worst = 0.0;
+  }
+  if (on)
+    for (int k = 0; k < SN_KINDS; ++k) {
+      ex.prof.ms[k] = ex.prof.flops[k] = 0.0;
+      ex.prof.calls[k] = 0;
+    }
+}
+
+void sn_get_profile(const SnExec &ex, double *ms, double *flops, long long *calls) {
+  for (int k = 0; k < SN_KINDS; ++k) {
+    if (ms) ms[k] = ex.prof.ms[k];
+    if (flops) flops[k] = ex.prof.flops[k];
+    if (calls) calls[k] = ex.prof.calls[k];
+  }
+}
+
 SnExec::~SnExec() {
+  for (cudaEvent_t e : prof.pool) cudaEventDestroy(e);
   if (h_srun) cudaFreeHost(h_srun);
   if (h_flags) cudaFreeHost(h_flags);
   if (h_nrm) cudaFreeHost(h_nrm);
@@ -879,6 +1018,8 @@ bool sn_exec_create(const SnPlan &P, bool fp32, int B, int vbase, int vcount,
   d.soff = A.upload(P.soff);
   d.amap = reinterpret_cast<const int2 *>(A.upload(P.amap));
   d.tasks = reinterpret_cast<const int4 *>(A.upload(P.tasks));
+  d.cl_ptr = A.upload(P.cl_ptr);
+  d.clist = reinterpret_cast<const int4 *>(A.upload(P.clist));
   const size_t ts = fp32 ? 4 : 8;
   d.F = fp32 ? (void *)A.alloc<float>(P.f_elems) : (void *)A.alloc<double>(P.f_elems);
   d.W = fp32 ? (void *)A.alloc<float>(P.w_elems) : (void *)A.alloc<double>(P.w_elems);
@@ -988,6 +1129,7 @@ void sn_solve(SnExec &ex, const KKTDev &k, const LDLParams &p, const int *run, c
       anyc = true;
     }
     if (!anyc) break;
+    ex.ir_sweeps++;
     upload_srun(cont);
     k_sn_vec<<<nb256(d.vcount), 256, 0, st>>>(d, 1);  // y = e
     pass();
@@ -1024,6 +1166,15 @@ void sn_solve(SnExec &ex, const KKTDev &k, const LDLParams &p, const int *run, c
   }
   std::vector<char> good(n);
   for (int a = 0; a < n; ++a) good[a] = act[a] && !bad[a];
+  for (int a = 0; a < n; ++a) {
+    if (!act[a]) continue;
+    ex.ir_solves++;
+    const double tol = p.ir_abstol + p.ir_reltol * normb[a];
+    if (p.ir_enable && !bad[a] && norme[a] > tol) {
+      ex.ir_unconverged++;
+      ex.ir_worst = std::max(ex.ir_worst, norme[a] / tol);
+    }
+  }
   upload_srun(good);
   k_sn_out<<<nb256(d.vcount), 256, 0, st>>>(d, k, lx, lz);
   bool anybad = false;

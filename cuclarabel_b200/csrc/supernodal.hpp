@@ -19,9 +19,9 @@
 // (extend-add), and its pivots are eliminated.  Fronts of at most
 // kSnSmallMax rows are assembled and factored by one block in shared memory;
 // larger fronts are padded to kSnNB-column panels and factored panel by
-// panel: the diagonal block by one block, the rows below it by a product
-// with the inverted diagonal block, and the trailing matrix by a rank-kSnNB
-// update (FP64 tensor-core MMA, or FP32 FMA in the mixed-precision form).
+// panel: the diagonal block by one block, the rows below it by triangular
+// substitution, and the trailing matrix by a rank-kSnNB update (FP64
+// tensor-core MMA, or FP32 FMA in the mixed-precision form).
 #pragma once
 #include <cstdint>
 #include <string>
@@ -58,7 +58,7 @@ bool sn_analyse(int N, const std::vector<int> &xadj, const std::vector<int> &adj
 // multiple of kSnNB, so every trailing region is a whole number of
 // kSnNB x kSnNB tiles: the first panel takes u0 mod kSnNB columns (when
 // nonzero), every later panel kSnNB.
-constexpr int kSnKPad = 8;
+constexpr int kSnKPad = 16;
 constexpr int kSnAsmCols = 32;  // parent columns per assembly task
 
 struct SnPair {
@@ -72,23 +72,26 @@ struct SnQuad {
 // count) are the launch's blocks (or warps, for the small-front solves).
 enum SnLaunchKind : int {
   SN_SMALL_FACTOR = 0,  // {s}: assemble + factor a small front in shared memory
-  SN_ASSEMBLE,          // {s, c_begin, c_end}: zero + assemble parent columns of a blocked front
-  SN_DIAG,              // {s, k | K << 16}: factor the K x K diagonal block, invert its L
-  SN_TRSM,              // {s, k | K << 16, r0}: rows r0..r0+127 of the panel: W = A Linv^T, L = W / d
-  SN_UPDATE,            // {s, k | K << 16, r0, c0}: tile (r0, c0) -= L(r0 rows) W(c0 rows)^T
+  SN_ASSEMBLE,          // {s, c_begin, c_end, chunk}: zero + assemble columns of a blocked front
+  SN_DIAG,              // {s, k | K << 16}: factor the K x K diagonal block
+  SN_TRSM,              // {s, k | K << 16, r0}: rows r0..r0+127 of the panel: W = A L11^-T
+                        //   by substitution, L = W D^-1
+  SN_UPDATE,            // {s, k | K << 16, r0, c0}: 128 x 64 tile (r0, c0) -= L(r0 rows) W(c0 rows)^T
   SN_FWD_SMALL,         // {s}: forward substitution of a small front (one warp)
-  SN_FWD_GATHER,        // {s}: work vector of a blocked front
-  SN_FWD_DIAG,          // {s, k | K << 16}
-  SN_FWD_GEMV,          // {s, k | K << 16, r0}
+  SN_FWD_GATHER,        // {s, c_begin, c_end, chunk}: positions of a blocked front's work vector
+  SN_FWD_DIAG,          // {s, k | K << 16}: v(panel) <- L11^-1 v(panel)
+  SN_FWD_GEMV,          // {s, k | K << 16, r0}: v(r0 rows) -= L(r0 rows, panel) v(panel)
   SN_FWD_SCATTER,       // {s}
   SN_BWD_SMALL,         // {s}
   SN_BWD_GATHER,        // {s}
-  SN_BWD_PARTIAL,       // {s, k | K << 16, r0}
-  SN_BWD_DIAG,          // {s, k | K << 16}
+  SN_BWD_PARTIAL,       // {s, k | K << 16, r0}: L(r0 rows, panel)^T v(r0 rows)
+  SN_BWD_DIAG,          // {s, k | K << 16}: v(panel) <- L11^-T (v(panel) - partial sums)
   SN_BWD_SCATTER,       // {s}
+  SN_KINDS
 };
 struct SnLaunch {
   int kind, begin, count, smem;
+  double flops;  // algorithmic floating-point operations of the launch (factorisation)
 };
 
 // One instance handed to the plan builder.
@@ -112,19 +115,25 @@ struct SnPlan {
   std::vector<int> inst, col0g, ncol, nrow, u0, ld, large, cbase, fix_off, rel_off, ch_ptr,
       uoff;
   std::vector<long long> foff;  // front offsets (elements, multiples of 32)
-  std::vector<long long> woff;  // factor workspace of blocked fronts: Linv (kSnNB^2), dinv (kSnNB), W (ld x kSnNB)
+  std::vector<long long> woff;  // factor workspace of blocked fronts: dinv (kSnNB), W (ld x kSnNB)
   std::vector<long long> soff;  // solve workspace of blocked fronts: v (ld), partial sums (ld)
   std::vector<int> ch;          // children, in order
   std::vector<int> fidx;        // front position -> global vector index (-1 none)
   std::vector<int> rel;         // struct row k of s -> position in the parent's front
   std::vector<int> acol;        // [sum ncol + 1] start of pivot column (cbase[s] + c) in amap
   std::vector<SnPair> amap;     // {global KKT position, front offset} of original entries
+  // children touching each kSnAsmCols-wide chunk of a blocked front's
+  // positions, in child order: {child, q_begin, q_end} (the child's row
+  // structure entries q whose parent positions fall in the chunk); chunk k
+  // of front s is chunk_off[s] + k, its entries clist[cl_ptr[..]..)
+  std::vector<int> chunk_off, cl_ptr;
+  std::vector<SnQuad> clist;
   std::vector<SnQuad> tasks;
   std::vector<SnLaunch> fact, fwd, bwd;
   std::vector<int> insts;       // the instances of the plan
   long long f_elems = 0, w_elems = 0, s_elems = 0, u_elems = 0;
   int small_smem_max = 0;       // largest small front, elements
-  double flops = 0;             // factorisation flops with padding (GEMM tiles counted in full)
+  double flops = 0;             // factorisation flops of the padded fronts (sum over launches)
 };
 
 // Builds the plan; false (with *err) on an index overflow.

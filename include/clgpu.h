@@ -76,6 +76,11 @@ typedef struct {
   int setup_threads;       /* host threads for per-instance setup; 0 = all */
   int fused_solves;        /* 1: kkt_update!'s constant-rhs solve shares the
                               affine solve's launch (same results); 0: its own */
+  int device_setup;        /* 1: Ruiz equilibration and the KKT values computed
+                              on the device at setup (bitwise the host's
+                              result); 0: on the host.  Problems whose
+                              matrices hold repeated or unsorted entries are
+                              equilibrated on the host either way. */
 } clgpu_settings;
 
 /* mirrors DefaultInfo (src/types.jl:227-255) plus solution scalars */
@@ -178,6 +183,33 @@ int clgpu_solver_get_phase_times(const clgpu_solver *h, double *ms,
  * chunk words once per side; vectors once per use).  Divided by the phase
  * times this gives the achieved bandwidth.  No reference counterpart. */
 int clgpu_solver_get_phase_bytes(const clgpu_solver *h, double *bytes);
+/* Supernodal factorisation of the large instances (those whose KKT work
+ * vector exceeds the single-warp kernels' 48 KB), per launch kind, summed
+ * over the solves since profiling was switched on: device ms (each launch
+ * bracketed by CUDA events), algorithmic flops and launches, CLGPU_SN_KINDS
+ * entries each (any pointer may be NULL).  Kinds: 0 small fronts, 1 front
+ * assembly, 2 diagonal blocks, 3 panel TRSM, 4 trailing update (FP64 DMMA /
+ * FP32 FMA tiles), 5-9 forward substitution (small fronts, gather,
+ * diagonal blocks, matrix-vector, scatter), 10-14 backward substitution
+ * (small fronts, gather, partial sums, diagonal blocks, scatter).  Returns 1
+ * when the solver has no such instance.  No reference counterpart. */
+#define CLGPU_SN_KINDS 15
+/* The numeric setup as the solve sees it, copied to HOST buffers (any may
+ * be NULL): equilibration d (sum n), e (sum m, type-major rows), c (one per
+ * instance), the scaled q and b (the same layouts) and the stored KKT values
+ * (*kkt_nnz of them, the library's permuted order); before the first solve.
+ * A diagnostic with no reference counterpart: it lets a test compare the
+ * device equilibration (device_setup = 1) with the host's bit for bit. */
+int clgpu_solver_debug_setup(const clgpu_solver *h, double *d, double *e, double *c, double *q,
+                             double *b, double *Kx, long long *kkt_nnz);
+int clgpu_solver_get_sn_profile(const clgpu_solver *h, double *ms, double *flops,
+                                long long *calls);
+/* Iterative refinement of those instances since profiling was switched on:
+ * counts[3] = {solves, refinement sweeps, solves that stopped above the
+ * tolerance (stop ratio or sweep limit)}, *worst = the largest final
+ * |e|_inf / (abstol + reltol |b|_inf) among the latter.  1 when the solver
+ * has no such instance.  A diagnostic with no reference counterpart. */
+int clgpu_solver_get_sn_refinement(const clgpu_solver *h, long long *counts, double *worst);
 int clgpu_solver_destroy(clgpu_solver *h);
 
 /* ------------------------------------------------ serving (continuous batching)

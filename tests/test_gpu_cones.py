@@ -27,7 +27,9 @@ def interior(rng, spec, scale=1.0):
     if t == 4:
         return np.array([np.sqrt(1 + p), np.sqrt(2 - p), 0.0]) * rng.uniform(0.5, 2) + \
             np.array([0, 0, rng.normal(0, 0.1)])
-    E = rng.standard_normal((d, d)) * 0.2
+    # off-diagonal noise shrinks with the side so the matrix stays positive
+    # definite (semicircle radius about 0.6 at every side)
+    E = rng.standard_normal((d, d)) * (0.2 if d <= 10 else 0.6 / np.sqrt(d))
     M = np.eye(d) + (E + E.T) / 2
     out = []
     for j in range(d):
@@ -43,6 +45,9 @@ SPECS = {
     "exp": [(3, 3, 0.0)] * 5,
     "pow": [(4, 3, 0.3), (4, 3, 0.7), (4, 3, 0.55)],
     "psd": [(5, 3, 0.0), (5, 10, 0.0)],
+    # sides above one warp's 32 lanes (row loops in the warp kernels) and
+    # mixed sides in one launch
+    "psd_large": [(5, 20, 0.0), (5, 33, 0.0), (5, 40, 0.0), (5, 7, 0.0)],
     "mixed": [(0, 2, 0.0), (1, 4, 0.0), (2, 3, 0.0), (2, 8, 0.0), (3, 3, 0.0), (4, 3, 0.4),
               (5, 4, 0.0)],
     # several shared-memory tiles of small cones (at most 128 cones or 1024
@@ -163,7 +168,7 @@ def test_step_length_and_barrier(cuda_device, name):
         assert abs(bar.value - bref) <= 1e-9 * max(1.0, abs(bref))
 
 
-@pytest.mark.parametrize("name", ["nn", "soc_dense", "soc_sparse", "psd"])
+@pytest.mark.parametrize("name", ["nn", "soc_dense", "soc_sparse", "psd", "psd_large"])
 def test_margins_shift_and_init(cuda_device, name):
     specs, rng, s, z = setup(name, seed=5)
     C = oracle.Cones(specs)

@@ -175,6 +175,15 @@ def test_exp_pow_psd_scaled(cuda_device):
     check_parity(sol, oracle.solve(*pb, gpu_equilibration=1), "exp_pow_psd")
 
 
+@pytest.mark.parametrize("psd_n", [24, 40])
+def test_exp_pow_psd_large_side(cuda_device, psd_n):
+    """PSD cones of side 24 and 40 (beyond one warp's lanes) through the
+    whole solve."""
+    pb = problems.exp_pow_psd(scale=0.004, seed=3, psd_n=psd_n)
+    sol = Solver(*pb).solve()
+    check_parity(sol, oracle.solve(*pb, gpu_equilibration=1), f"exp_pow_psd side {psd_n}")
+
+
 def test_repeat_solve_is_identical(cuda_device):
     pb = problems.mpc_qp(3)
     s = Solver(*pb)
