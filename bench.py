@@ -16,6 +16,7 @@ collective on the data path; NCCL only for the barrier and the max-time
 reduction).
 """
 import argparse
+import collections
 import ctypes
 import json
 import os
@@ -473,10 +474,10 @@ def _oracle_sample_worker(which, scale, conn):
 def large_single(which, scale, method, sh, fp64_peak, cpu_scale):
     """One large single problem (configuration 2: mixed SOCP, n = 20000,
     m = 60000; configuration 3: exp/pow/PSD LP, n = 30000, m = 96000, at
-    `scale`) on the supernodal LDL^T: setup, a warm-up solve, a solve timed
-    with CUDA events (L2 flushed before), a profiled solve for the per-kernel
-    breakdown, and the end-to-end pass (new values from pinned host memory +
-    solve! + solution read back)."""
+    `scale`) on the supernodal LDL^T: setup, a profiled solve for the
+    per-kernel breakdown (which also warms up), a solve timed with CUDA
+    events (L2 flushed before), and the end-to-end pass (new values from
+    pinned host memory + solve! + solution read back)."""
     import torch
     from cuclarabel_b200 import Solver, SolverStatus, problems
     from cuclarabel_b200.api import _as_csc
@@ -484,7 +485,10 @@ def large_single(which, scale, method, sh, fp64_peak, cpu_scale):
     t0 = time.perf_counter()
     s = Solver(*pb, direct_solve_method=method)
     setup_s = time.perf_counter() - t0
+    s.set_profiling(True)
     s.solve(sh)
+    prof = s.profile()
+    s.set_profiling(False)
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device="cuda")
     flush.add_(1.0)
     torch.cuda.synchronize()
@@ -497,10 +501,6 @@ def large_single(which, scale, method, sh, fp64_peak, cpu_scale):
     torch.cuda.synchronize()
     dev_s = e0.elapsed_time(e1) / 1000.0
     sol = s.solutions()[0]
-    s.set_profiling(True)
-    s.solve(sh)
-    prof = s.profile()
-    s.set_profiling(False)
     sn = prof.get("supernodal", {})
     upd = sn.get("update", {"ms": 0.0, "flops": 0.0, "launches": 0})
     fact_fl = sum(v["flops"] for v in sn.values())
@@ -531,6 +531,7 @@ def large_single(which, scale, method, sh, fp64_peak, cpu_scale):
                      "10000 nonneg at scale 1)") % (A.shape[1], A.shape[0]),
         "scale": scale, "method": method,
         "value": (1.0 / dev_s) if sol.status == SolverStatus.SOLVED else 0.0,
+        "solve_rate_any_status": 1.0 / dev_s,
         "unit": "solves/s", "solve_s": dev_s, "setup_s": setup_s,
         "status": sol.status.name, "iterations": sol.iterations, "obj_val": sol.obj_val,
         "device_bytes": s.device_bytes(),
@@ -593,109 +594,135 @@ def aggregate_over_ranks(elapsed, solved, dist, device):
     return tmax[0].item(), int(round(tsum[1].item()))
 
 
-def serve_run(solver, pbs, lam, seconds, seed, stream):
-    """Continuous batching under a Poisson request stream (config 5 shape,
-    its config-4 part): `lam` requests/s for `seconds`, each for a uniformly
-    drawn slot (one of the resident MPC structures) with new q / b (the
-    structure's values plus noise, as a new MPC state would give).  Requests
-    are admitted at IPM-step boundaries as their slot frees up, run one IPM
-    iteration per step together with every other running request, and are
-    collected when done.  Latency = arrival to result on the host."""
-    import collections
+# scales of the large (configuration-2-like) request structures of the
+# serving configuration: n = 20000 * scale spans 2000..20000
+SERVE_LARGE_SCALES = (0.1, 0.2, 0.35, 0.5, 0.75, 1.0)
+
+
+def serve_config5(pbs, lam, seconds, seed, method, budget_gb, new_frac, large_frac, grace,
+                  plain_small_pool):
+    """The serving configuration under a Poisson stream of `lam` requests/s
+    for `seconds`: a `large_frac` share of configuration-2-like requests
+    (n from 2000 to 20000, resident structures on the supernodal path, new
+    q / b), a `new_frac` share of MPC requests with structures that are not
+    resident (set up in cohorts under the HBM budget), the rest MPC requests
+    for the resident batch's structures (new q / b).  The served arm runs
+    the three lanes of cuclarabel_b200.serving concurrently; the plain arm
+    then serves the same arrivals one request at a time (FIFO) on
+    single-instance solvers.  Both arms stop at `seconds + grace`; requests
+    still open then are reported as unfinished."""
+    import torch
+    from cuclarabel_b200 import Solver, problems
+    from cuclarabel_b200 import serving
     rng = np.random.default_rng(seed)
     B = len(pbs)
     n = int(rng.poisson(lam * seconds))
     arrive = np.sort(rng.uniform(0.0, seconds, n))
-    slot_of = rng.integers(0, B, n)
-    queues = collections.defaultdict(collections.deque)
-    busy = {}          # slot -> request
-    lat, statuses, iters = [], collections.Counter(), []
-    nxt, running, steps, occupancy = 0, 0, 0, 0
-    t_admit = t_step = t_collect = 0.0
-    n_admit = 0
+    u = rng.uniform(size=n)
+    cls = np.where(u < large_frac, 2, np.where(u < large_frac + new_frac, 1, 0))
+    large_pbs = [problems.mixed_socp(sc, seed=40 + k) for k, sc in enumerate(SERVE_LARGE_SCALES)]
+    which = np.where(cls == 2, rng.integers(0, len(large_pbs), n), rng.integers(0, B, n))
+    qv, bv, newp = [None] * n, [None] * n, {}
+    for r in range(n):
+        if cls[r] == 1:
+            newp[r] = problems.mpc_qp(1000000 + r)
+            continue
+        P, q, A, b, cones = (large_pbs if cls[r] == 2 else pbs)[which[r]]
+        qv[r] = q + 0.05 * rng.standard_normal(len(q))
+        bv[r] = b + 0.02 * np.abs(rng.standard_normal(len(b)))
+    idx = [np.nonzero(cls == c)[0] for c in range(3)]
+    horizon = seconds + grace
+
+    # ---- served arm: three lanes, one thread and stream each
+    budget = serving.Budget(budget_gb * 1e9)
+    streams = [torch.cuda.Stream() for _ in range(3)]
+    t_setup = time.perf_counter()
+    small = serving.SlotLane.build("resident MPC", pbs, streams[0].cuda_stream, budget,
+                                   direct_solve_method=method)
+    large = serving.SlotLane.build("resident config-2-like", large_pbs, streams[1].cuda_stream,
+                                   budget, direct_solve_method=method)
+    cohort = serving.CohortLane("new-structure MPC", streams[2].cuda_stream, budget,
+                                bytes_per_nnz=small.bytes / max(small.kkt_nnz, 1),
+                                direct_solve_method=method)
+    setup_s = time.perf_counter() - t_setup
+    jobs = [(small, (arrive[idx[0]], which[idx[0]], [qv[r] for r in idx[0]],
+                     [bv[r] for r in idx[0]])),
+            (large, (arrive[idx[2]], which[idx[2]], [qv[r] for r in idx[2]],
+                     [bv[r] for r in idx[2]])),
+            (cohort, (arrive[idx[1]], [newp[r] for r in idx[1]]))]
+    wall, left = serving.run_lanes(jobs, horizon)
+    lanes = {}
+    all_lat, solved = [], 0
+    for (lane, _), lf in zip(jobs, left):
+        d = lane.stats.summary(wall)
+        d["requests"] = int(len(_[0]))
+        d["unfinished"] = int(lf)
+        lanes[lane.name] = d
+        all_lat += lane.stats.lat
+        solved += d["solved"]
+    served = {"lambda_per_s": lam, "seconds": seconds, "grace_s": grace, "requests": n,
+              "completed": len(all_lat), "unfinished": int(sum(left)),
+              "value": solved / wall, "unit": "solves/s", "wall_s": wall,
+              "p50_ms": 1000 * float(np.percentile(all_lat, 50)) if all_lat else None,
+              "p99_ms": 1000 * float(np.percentile(all_lat, 99)) if all_lat else None,
+              "lanes": lanes, "setup_s": setup_s,
+              "hbm_budget_gb": budget_gb, "hbm_peak_held_gb": budget.peak / 1e9,
+              "cohorts": cohort.cohorts, "cohort_setup_s": cohort.setup_s,
+              "cohort_budget_waits": cohort.waited_for_budget,
+              "mix": {"resident_mpc": int(len(idx[0])), "new_structure_mpc": int(len(idx[1])),
+                      "config2_like": int(len(idx[2]))}}
+    small.close()
+    large.close()
+    del small, large, cohort
+    torch.cuda.synchronize()
+
+    # ---- plain arm: the same arrivals, one request at a time
+    pool = [Solver(*pbs[k], direct_solve_method=method) for k in range(min(plain_small_pool, B))]
+    lsol = [Solver(*pb, direct_solve_method=method) for pb in large_pbs]
+    solvers, pw = [], np.empty(n, np.int64)
+    for r in range(n):
+        if cls[r] == 0:
+            pw[r] = which[r] % len(pool)
+        elif cls[r] == 2:
+            pw[r] = len(pool) + which[r]
+        else:
+            pw[r] = -1
+    solvers = pool + lsol
+    lat, status = [], collections.Counter()
     t0 = time.perf_counter()
-    while True:
+    unfinished = 0
+    for r in range(n):
         now = time.perf_counter() - t0
-        while nxt < n and arrive[nxt] <= now:
-            queues[int(slot_of[nxt])].append(nxt)
-            nxt += 1
-        adm, qv, bv = [], [], []
-        for slot in list(queues):
-            if slot in busy or not queues[slot]:
-                continue
-            r = queues[slot].popleft()
-            if not queues[slot]:
-                del queues[slot]
-            P, q, A, b, cones = pbs[slot]
-            qv.append(q + 0.05 * rng.standard_normal(len(q)))
-            bv.append(b + 0.02 * np.abs(rng.standard_normal(len(b))))
-            adm.append(slot)
-            busy[slot] = r
-        if adm:
-            ta = time.perf_counter()
-            solver.serve_admit(adm, q=qv, b=bv, stream=stream)
-            t_admit += time.perf_counter() - ta
-            n_admit += 1
-            running += len(adm)
-        if running:
-            ta = time.perf_counter()
-            fin, running = solver.serve_step(stream)
-            t_step += time.perf_counter() - ta
-            steps += 1
-            occupancy += running + len(fin)
-            if fin:
-                ta = time.perf_counter()
-                sols = solver.serve_collect(fin, stream)
-                t_collect += time.perf_counter() - ta
-                done = time.perf_counter() - t0
-                for slot, sol in zip(fin, sols):
-                    r = busy.pop(slot)
-                    lat.append(done - arrive[r])
-                    statuses[sol.status.name] += 1
-                    iters.append(sol.iterations)
-        elif nxt < n:
-            time.sleep(max(0.0, arrive[nxt] - (time.perf_counter() - t0)))
-        elif not queues:
+        if now > horizon:
+            unfinished = n - r
             break
-    wall = time.perf_counter() - t0
-    solved = statuses.get("SOLVED", 0)
-    return {"lambda_per_s": lam, "seconds": seconds, "requests": n, "completed": len(lat),
-            "value": solved / wall, "unit": "solves/s", "wall_s": wall,
-            "p50_ms": 1000 * float(np.percentile(lat, 50)),
-            "p99_ms": 1000 * float(np.percentile(lat, 99)),
-            "steps": steps, "mean_running": occupancy / max(steps, 1),
-            "ms_per_step": {"admit": 1000 * t_admit / max(n_admit, 1),
-                            "admissions": n_admit,
-                            "iterate": 1000 * t_step / max(steps, 1),
-                            "collect": 1000 * t_collect / max(steps, 1),
-                            "wall": 1000 * wall / max(steps, 1)},
-            "iters_mean": float(np.mean(iters)), "status": dict(statuses),
-            "mix": "config-4-like requests only (the 5 % config-2-like large requests of the "
-                   "serving config are not in this run)"}
-
-
-def plain_under_load(service_s, lam, seconds, seed):
-    """Response times of the plain one-at-a-time GPU path under the served
-    run's request stream: the same Poisson arrivals (same seed, rate and
-    length) into one FIFO server whose per-request service times cycle
-    through the plain path's measured per-solve latencies.  Arithmetic on
-    measured times, no GPU work: the plain path serves one request at a
-    time, so this is its latency under that load."""
-    rng = np.random.default_rng(seed)
-    n = int(rng.poisson(lam * seconds))
-    arrive = np.sort(rng.uniform(0.0, seconds, n))
-    svc = np.resize(np.asarray(service_s, np.float64), n)
-    finish = np.empty(n)
-    t = 0.0
-    for i in range(n):
-        t = max(t, arrive[i]) + svc[i]
-        finish[i] = t
-    resp = finish - arrive
-    return {"requests": n, "p50_ms": 1000 * float(np.percentile(resp, 50)),
-            "p99_ms": 1000 * float(np.percentile(resp, 99)),
-            "value": n / float(finish[-1]) if n else 0.0, "unit": "solves/s",
-            "note": "FIFO queue of the plain path's measured per-solve times under the "
-                    "served run's arrivals (same seed, rate and length)"}
+        if arrive[r] > now:
+            time.sleep(arrive[r] - now)
+        if pw[r] >= 0:
+            s_ = solvers[pw[r]]
+            s_.update_data(q=qv[r], b=bv[r])
+            sol = s_.solve()
+        else:
+            s_ = Solver(*newp[r], direct_solve_method=method)
+            sol = s_.solve()
+            del s_
+        lat.append(time.perf_counter() - t0 - arrive[r])
+        status[sol.status.name] += 1
+    pwall = time.perf_counter() - t0
+    plain = {"requests": n, "completed": len(lat), "unfinished": unfinished,
+             "value": status.get("SOLVED", 0) / pwall, "unit": "solves/s", "wall_s": pwall,
+             "p50_ms": 1000 * float(np.percentile(lat, 50)) if lat else None,
+             "p99_ms": 1000 * float(np.percentile(lat, 99)) if lat else None,
+             "status": dict(status),
+             "note": "run, not replayed: the same arrivals served one at a time, first come "
+                     "first served, on single-instance solvers (resident MPC requests on a pool "
+                     "of %d solvers, slot mod pool; config-2-like requests on one solver per "
+                     "structure; new structures set up per request); requests still queued "
+                     "at the horizon are unfinished and not in p50/p99" % len(pool)}
+    del pool, lsol, solvers
+    torch.cuda.synchronize()
+    served["plain_under_same_load"] = plain
+    return served
 
 
 def main():
@@ -712,6 +739,15 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0,
                     help="length of the served (continuous batching) run; 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
+    ap.add_argument("--serve-new-frac", type=float, default=0.05,
+                    help="share of MPC requests whose structure is not resident")
+    ap.add_argument("--serve-large-frac", type=float, default=0.05,
+                    help="share of configuration-2-like requests (n 2000..20000)")
+    ap.add_argument("--serve-grace", type=float, default=10.0,
+                    help="seconds after the last arrival before both arms stop")
+    ap.add_argument("--plain-pool", type=int, default=256,
+                    help="single-instance solvers of the plain arm for resident MPC structures")
     ap.add_argument("--cone-scale", type=float, default=1.0,
                     help="size of the cone-kernel roofline workload (1.0: every streamed "
                          "vector larger than L2); 0 skips it")
@@ -929,13 +965,11 @@ def main():
     # ---- served: continuous batching under a Poisson request stream
     served = None
     if rank == 0 and args.serve_seconds > 0:
-        srv = BatchSolver(pbs, direct_solve_method=args.method)
-        served = serve_run(srv, pbs, args.serve_rate, args.serve_seconds, 12345 + rank, sh)
-        del srv
+        served = serve_config5(pbs, args.serve_rate, args.serve_seconds, 12345 + rank,
+                               args.method, args.serve_budget_gb, args.serve_new_frac,
+                               args.serve_large_frac, args.serve_grace, args.plain_pool)
         if plain:
             served["vs_plain_solves"] = served["value"] / plain["value"]
-            served["plain_under_same_load"] = plain_under_load(
-                plain_lat, args.serve_rate, args.serve_seconds, 12345 + rank)
 
     # ---- roofline: the dominant device phase (an LDL kernel), plus the
     # update_scaling cone kernels for reference

@@ -678,14 +678,15 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
     int i = e % n, j = e / n;
     tmp[e] = V[i + n * perm[j]];
   }
-  double sl[kPsdMaxSide / 32];
+  constexpr int kRows = (kPsdMaxSide + 31) / 32;  // rows per lane
+  double sl[kRows];
 #pragma unroll
-  for (int r = 0; r < kPsdMaxSide / 32; ++r)
+  for (int r = 0; r < kRows; ++r)
     sl[r] = lane + 32 * r < n ? S[perm[lane + 32 * r]] : 0.0;
   __syncwarp();
   for (int e = lane; e < n * n; e += 32) V[e] = tmp[e];
 #pragma unroll
-  for (int r = 0; r < kPsdMaxSide / 32; ++r)
+  for (int r = 0; r < kRows; ++r)
     if (lane + 32 * r < n) S[lane + 32 * r] = sl[r];
   __syncwarp();
 }
@@ -2165,7 +2166,9 @@ static inline void psd_launch_dims(const ConeSet &cs, int nmats, int &nb, int &n
                                    size_t &smem) {
   // warps (cones) per block: kPsdWarps while their matrices fit 200 KB
   const size_t per = (size_t)nmats * cs.psd_nmax * cs.psd_nmax * sizeof(double);
-  const int warps = (int)std::max<size_t>(1, std::min<size_t>(kPsdWarps, (200 * 1024) / per));
+  const int warps =
+      per == 0 ? kPsdWarps
+               : (int)std::max<size_t>(1, std::min<size_t>(kPsdWarps, (200 * 1024) / per));
   nt = 32 * warps;
   nb = blocks_for((long long)cs.n_psd * 32, nt);
   smem = (size_t)warps * per + 256;

@@ -50,6 +50,13 @@ struct SnExec {
   unsigned long long *h_nrm = nullptr;  // pinned [2 B]
   int *d_flags = nullptr;               // [B]
   long long launches = 0;               // kernel launches issued (statistics)
+  // one substitution pass (forward, D^-1, backward) as a CUDA graph,
+  // captured on first use on a private stream and replayed on the caller's
+  // stream (not used while profiling, which brackets every launch)
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t g_pass = nullptr;
+  long long pass_launches = 0;
+  bool graph_failed = false;
   // refinement statistics since profiling was switched on: solves, sweeps,
   // solves that stopped above the tolerance, and the worst such final
   // |e|_inf / (abstol + reltol |b|_inf)

@@ -49,6 +49,28 @@ constexpr int kTrsmThreads = 256;
 constexpr int kAsmThreads = 256;
 constexpr int kSmallThreads = 128;
 constexpr int kVecThreads = 128;
+constexpr int kGemvThreads = 256;
+constexpr int kDiagSolveThreads = 512;
+
+// two consecutive elements of a front (8- or 16-byte aligned pairs)
+template <typename T>
+struct Pair {
+  T x, y;
+};
+__device__ __forceinline__ Pair<double> load_pair(const double *p) {
+  const double2 w = *reinterpret_cast<const double2 *>(p);
+  return {w.x, w.y};
+}
+__device__ __forceinline__ Pair<float> load_pair(const float *p) {
+  const float2 w = *reinterpret_cast<const float2 *>(p);
+  return {w.x, w.y};
+}
+__device__ __forceinline__ void store_pair(double *p, Pair<double> w) {
+  *reinterpret_cast<double2 *>(p) = make_double2(w.x, w.y);
+}
+__device__ __forceinline__ void store_pair(float *p, Pair<float> w) {
+  *reinterpret_cast<float2 *>(p) = make_float2(w.x, w.y);
+}
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -216,9 +238,20 @@ __global__ void __launch_bounds__(kAsmThreads) k_sn_assemble(SnDev d, KKTDev k, 
   }
 }
 
-// Diagonal block of a panel: factor the K x K block (right-looking, the
-// static shift was applied at assembly), write L11 and D to the front and
-// 1/d to the workspace.
+// Diagonal block of a panel: factor the K x K block (the static shift was
+// applied at assembly), write L11 and D to the front and 1/d to the
+// workspace.  Blocked right-looking LDL^T in 32-column blocks, every column
+// kept unscaled until the end (L(:, j) = a(:, j) / d_j is written last):
+//   1. one warp factors the 32 x 32 diagonal block (lane i owns row i; step
+//      j subtracts a(i, j) (a(k, j) / d_j) from a(i, k), j < k <= i), with
+//      the pivot rule applied to each pivot as it becomes final;
+//   2. every row below the block (one thread each, the row in registers)
+//      takes the same 32 steps against the block's columns;
+//   3. the trailing lower triangle -= X D^-1 X^T over the block's 32
+//      columns, 6 x 6 outputs per thread.
+// Three barriers per column block instead of one per pivot.  Pivot signs
+// and D's global positions are staged first.
+constexpr int kDiagNB = 32;
 template <typename T>
 __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDLParams prm,
                                                          int base, const int *run, int *ok) {
@@ -226,8 +259,11 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, inst = d.inst[s];
   if (!run[inst]) return;
   extern __shared__ __align__(16) unsigned char sraw[];
-  T *blk = reinterpret_cast<T *>(sraw);  // K x K, column-major, stride K
-  T *col = blk + K * K;
+  T *blk = reinterpret_cast<T *>(sraw);       // K x K, column-major, stride K
+  T *wsc = blk + kSnNB * kSnNB;               // scaled block columns, [kDiagNB][kSnNB]
+  __shared__ double dinv[kSnNB];
+  __shared__ T dd[kSnNB];
+  __shared__ int gix[kSnNB], sgn[kSnNB];
   const long long ld = d.ld[s];
   T *f = reinterpret_cast<T *>(d.F) + d.foff[s];
   T *ws = reinterpret_cast<T *>(d.W) + d.woff[s];
@@ -237,47 +273,154 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
     const int c = idx / K, r = idx - c * K;
     blk[idx] = r >= c ? f[(k0 + c) * ld + k0 + r] : T(0);
   }
+  for (int j = tid; j < K; j += kDiagThreads) {
+    const int g = fi[k0 + j];
+    gix[j] = g;
+    sgn[j] = pivot_sign(k, g);
+  }
   __syncthreads();
-  bool bad = false;
-  for (int j = 0; j < K; ++j) {
-    const T dj = T(sn_pivot(double(blk[j * K + j]), pivot_sign(k, fi[k0 + j]), prm));
-    for (int i = j + 1 + tid; i < K; i += kDiagThreads) col[i] = blk[j * K + i];
-    __syncthreads();
-    // rank-1 update of the trailing lower triangle: 16 x 16 threads, thread
-    // (tx, ty) takes columns j+1+ty, +16, ... and rows i >= r, i = j+1+tx, +16, ...
-    {
-      const int tx = tid & 15, ty = tid >> 4;
-      for (int r = j + 1 + ty; r < K; r += 16) {
-        const T cr = col[r];
-        for (int i = j + 1 + tx; i < K; i += 16)
-          if (i >= r) blk[r * K + i] -= (col[i] / dj) * cr;
+  for (int b0 = 0; b0 < K; b0 += kDiagNB) {
+    const int nb = min(kDiagNB, K - b0);
+    // 1. the diagonal block, one warp
+    if (tid < 32) {
+      const int i = tid;
+      for (int j = 0; j < nb; ++j) {
+        const T dj = T(sn_pivot(double(blk[(b0 + j) * K + b0 + j]), sgn[b0 + j], prm));
+        const double di = 1.0 / double(dj);
+        if (i == 0) {
+          dd[b0 + j] = dj;
+          dinv[b0 + j] = di;
+        }
+        if (i > j && i < nb) {
+          const T *cj = blk + (b0 + j) * K + b0;
+          const T li = cj[i] * T(di);
+          for (int q = j + 1; q <= i; ++q) blk[(b0 + q) * K + b0 + i] -= li * cj[q];
+        }
+        __syncwarp();
       }
     }
-    for (int i = j + 1 + tid; i < K; i += kDiagThreads) blk[j * K + i] = col[i] / dj;
-    if (tid == 0) {
-      blk[j * K + j] = dj;
-      const double di = 1.0 / double(dj);
-      const int g = fi[k0 + j];
-      if (g >= 0) d.Dinv[g] = di;
-      ws[j] = T(di);
-      if (!isfinite(di) || !isfinite(double(dj))) bad = true;
+    __syncthreads();
+    const int rb = b0 + nb, m = K - rb;  // rows below the block
+    if (m <= 0) break;
+    // 2. the rows below, one thread each
+    if (tid < m) {
+      const int r = rb + tid;
+      T x[kDiagNB];
+#pragma unroll
+      for (int j = 0; j < kDiagNB; ++j) x[j] = j < nb ? blk[(b0 + j) * K + r] : T(0);
+#pragma unroll
+      for (int j = 0; j < kDiagNB; ++j) {
+        if (j < nb) {
+          const T lj = x[j] * T(dinv[b0 + j]);
+#pragma unroll
+          for (int q = j + 1; q < kDiagNB; ++q)
+            if (q < nb) x[q] -= lj * blk[(b0 + j) * K + b0 + q];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kDiagNB; ++j)
+        if (j < nb) {
+          blk[(b0 + j) * K + r] = x[j];
+          wsc[j * kSnNB + tid] = x[j] * T(dinv[b0 + j]);
+        }
+    }
+    __syncthreads();
+    // 3. trailing lower triangle: a(r, c) -= sum_j x(r, j) (x(c, j) / d_j)
+    {
+      const int tx = tid & 15, ty = tid >> 4;
+      T acc[6][6];
+#pragma unroll
+      for (int u = 0; u < 6; ++u)
+#pragma unroll
+        for (int v = 0; v < 6; ++v) acc[u][v] = T(0);
+      for (int j = 0; j < nb; ++j) {
+        T xa[6], wb[6];
+#pragma unroll
+        for (int u = 0; u < 6; ++u) {
+          const int rr = ty + 16 * u, cc = tx + 16 * u;
+          xa[u] = rr < m ? blk[(b0 + j) * K + rb + rr] : T(0);
+          wb[u] = cc < m ? wsc[j * kSnNB + cc] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 6; ++u)
+#pragma unroll
+          for (int v = 0; v < 6; ++v) acc[u][v] += xa[u] * wb[v];
+      }
+#pragma unroll
+      for (int u = 0; u < 6; ++u)
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+          const int rr = ty + 16 * u, cc = tx + 16 * v;
+          if (rr < m && cc <= rr) blk[(rb + cc) * K + rb + rr] -= acc[u][v];
+        }
     }
     __syncthreads();
   }
   for (int idx = tid; idx < K * K; idx += kDiagThreads) {
     const int c = idx / K, r = idx - c * K;
-    if (r >= c) f[(k0 + c) * ld + k0 + r] = blk[idx];
+    if (r > c)
+      f[(k0 + c) * ld + k0 + r] = blk[idx] * T(dinv[c]);
+    else if (r == c)
+      f[(k0 + c) * ld + k0 + r] = dd[c];
   }
-  for (int j = K + tid; j < kSnNB; j += kDiagThreads) ws[j] = T(0);
-  if (bad && tid == 0) ok[inst] = 0;
+  bool bad = false;
+  for (int j = tid; j < kSnNB; j += kDiagThreads) {
+    if (j < K) {
+      const double di = dinv[j];
+      if (gix[j] >= 0) d.Dinv[gix[j]] = di;
+      ws[j] = T(di);
+      if (!isfinite(di) || !isfinite(double(dd[j]))) bad = true;
+    } else {
+      ws[j] = T(0);
+    }
+  }
+  if (bad) ok[inst] = 0;
+}
+
+// one column block of the TRSM below: (a) then (b), NB columns from b0
+template <typename T, int NB>
+__device__ __forceinline__ void trsm_block(T *X, const T *Lr, int b0, int K, int m, int half) {
+  if (half == 0) {
+    T x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) x[j] = X[(b0 + j) * kSnNB + m];
+#pragma unroll
+    for (int q = 1; q < NB; ++q) {
+      const T *lq = Lr + (b0 + q) * (b0 + q - 1) / 2 + b0;
+      T acc = x[q];
+#pragma unroll
+      for (int j = 0; j < q; ++j) acc -= x[j] * lq[j];
+      x[q] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) X[(b0 + j) * kSnNB + m] = x[j];
+  }
+  __syncthreads();
+  if (b0 + NB < K) {
+    T x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) x[j] = X[(b0 + j) * kSnNB + m];
+    for (int q = b0 + NB + half; q < K; q += kTrsmThreads / kSnNB) {
+      const T *lq = Lr + q * (q - 1) / 2 + b0;
+      T acc = T(0);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) acc += x[j] * lq[j];
+      X[q * kSnNB + m] -= acc;
+    }
+  }
+  __syncthreads();
 }
 
 // TRSM of a panel's row tile: rows r0..r0+127 of panel [k0, k0+K),
-// W = A L11^-T by column-oriented substitution (after step j column j of W
-// is final and is subtracted, times L11(t, j), from every later column t),
-// then L = W D^-1: L overwrites A in the front, W goes to the workspace for
-// the trailing update.  The tile (K x 128) and the strict lower triangle of
-// L11 (packed by columns) sit in shared memory.
+// W = A L11^-T by substitution, then L = W D^-1: L overwrites A in the
+// front, W goes to the workspace for the trailing update.  Blocked by 32
+// columns: (a) each row (one thread) solves the block's 32 columns in
+// registers against the block's unit lower triangle (row-oriented: w(m, q)
+// = a(m, q) - sum_{j<q} w(m, j) L11(q, j)); (b) the later columns of the
+// row take the block's contribution, sum_j w(m, j) L11(q, j), the two
+// halves of the thread block splitting the columns.  Two barriers per
+// column block.  The tile (K x 128, column-major) and the strict lower triangle
+// of L11 packed by rows (row q at q (q - 1) / 2) sit in shared memory.
 template <typename T>
 __global__ void __launch_bounds__(kTrsmThreads) k_sn_trsm(SnDev d, int base, const int *run) {
   const int4 t = d.tasks[base + blockIdx.x];
@@ -285,43 +428,55 @@ __global__ void __launch_bounds__(kTrsmThreads) k_sn_trsm(SnDev d, int base, con
   if (!run[d.inst[s]]) return;
   extern __shared__ __align__(16) unsigned char sraw[];
   T *X = reinterpret_cast<T *>(sraw);  // column q of the tile at X + q kSnNB
-  T *Lp = X + K * kSnNB;               // column j of L11 below the diagonal at Lp + cs(j)
+  T *Lr = X + K * kSnNB;               // L11(q, j), j < q, at Lr[q (q - 1) / 2 + j]
   const long long ld = d.ld[s];
   T *f = reinterpret_cast<T *>(d.F) + d.foff[s];
   const T *ws = reinterpret_cast<const T *>(d.W) + d.woff[s];
   T *wr = reinterpret_cast<T *>(d.W) + d.woff[s] + kSnNB;
   const int tid = threadIdx.x;
-  auto cs = [K](int j) { return j * (K - 1) - j * (j - 1) / 2; };
-  for (int idx = tid; idx < K * kSnNB; idx += kTrsmThreads) {
-    const int q = idx / kSnNB, m = idx - q * kSnNB;
-    X[idx] = f[(k0 + q) * ld + r0 + m];
+#pragma unroll 4
+  for (int it = 0; it < kSnNB * kSnNB / kTrsmThreads; ++it) {
+    const int idx = tid + it * kTrsmThreads, q = idx >> 7, m = idx & (kSnNB - 1);
+    if (q < K) X[idx] = f[(k0 + q) * ld + r0 + m];
   }
-  for (int j = 0; j < K; ++j)
-    for (int i = j + 1 + tid; i < K; i += kTrsmThreads) Lp[cs(j) + i - j - 1] = f[(k0 + j) * ld + k0 + i];
+#pragma unroll 4
+  for (int it = 0; it < kSnNB * kSnNB / kTrsmThreads; ++it) {
+    const int idx = tid + it * kTrsmThreads, j = idx >> 7, q = idx & (kSnNB - 1);
+    if (j < q && q < K) Lr[q * (q - 1) / 2 + j] = f[(k0 + j) * ld + k0 + q];
+  }
   __syncthreads();
   const int m = tid & (kSnNB - 1), half = tid / kSnNB;
-  for (int j = 0; j + 1 < K; ++j) {
-    const T xj = X[j * kSnNB + m];
-    const T *lc = Lp + cs(j) - j - 1;
-    for (int q = j + 1 + half; q < K; q += kTrsmThreads / kSnNB) X[q * kSnNB + m] -= xj * lc[q];
-    __syncthreads();
+  for (int b0 = 0; b0 < K; b0 += 32) {
+    // K is a multiple of 16, so a block has 32 or 16 columns
+    if (K - b0 >= 32)
+      trsm_block<T, 32>(X, Lr, b0, K, m, half);
+    else
+      trsm_block<T, 16>(X, Lr, b0, K, m, half);
   }
-  for (int idx = tid; idx < K * kSnNB; idx += kTrsmThreads) {
-    const int q = idx / kSnNB, mm = idx - q * kSnNB;
-    const T w = X[idx];
-    wr[(long long)q * ld + r0 + mm] = w;
-    f[(k0 + q) * ld + r0 + mm] = w * ws[q];
+#pragma unroll 4
+  for (int it = 0; it < kSnNB * kSnNB / kTrsmThreads; ++it) {
+    const int idx = tid + it * kTrsmThreads, q = idx >> 7, mm = idx & (kSnNB - 1);
+    if (q < K) {
+      const T w = X[idx];
+      wr[(long long)q * ld + r0 + mm] = w;
+      f[(k0 + q) * ld + r0 + mm] = w * ws[q];
+    }
   }
 }
 
 // Trailing update of the blocked fronts, one 128 x 64 tile per block:
 // front tile (r0, c0) -= L(r0.., panel) W(c0.., :)^T, entries on or below
 // the diagonal only (r0 + m >= c0 + n).  K (a multiple of kSnKPad = 16) is
-// streamed in chunks of kUpdKC through a kUpdStages-deep cp.async pipeline;
-// two blocks are resident per SM, so one's prologue and epilogue overlap the
-// other's main loop.
-// FP64: 4 warps as 2 (rows) x 2 (columns), warp tile 64 x 32 of m8n8k4 DMMA.
-__global__ void __launch_bounds__(128, 2) k_sn_update_f64(SnDev d, int base, const int *run) {
+// streamed in chunks of kUpdKC through a kUpdStages-deep cp.async pipeline.
+// FP64: 8 warps as 4 (rows) x 2 (columns), warp tile 32 x 32 of m8n8k4
+// DMMA; 120 registers, so two blocks (16 warps) are resident per SM and
+// one block's prologue and epilogue overlap the other's main loop.  The
+// accumulators start from the front tile itself (its loads are issued
+// before the operand pipeline fills, so their latency is hidden) and the
+// products are subtracted as they come (W fragments negated), so the
+// epilogue only stores.
+constexpr int kUpdThreads = 256;
+__global__ void __launch_bounds__(kUpdThreads, 2) k_sn_update_f64(SnDev d, int base, const int *run) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, r0 = t.z, c0 = t.w;
   if (!run[d.inst[s]]) return;
@@ -332,22 +487,29 @@ __global__ void __launch_bounds__(128, 2) k_sn_update_f64(SnDev d, int base, con
   extern __shared__ __align__(16) unsigned char sraw[];
   double *sm = reinterpret_cast<double *>(sraw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp & 1, wn = warp >> 1;
-  double acc[8][4][2];
+  const int wm = warp & 3, wn = warp >> 2;
+  // accumulator (mi, ni, h) is front entry (r0 + m, c0 + n); the whole
+  // tile lies inside the front (entries above the diagonal are read and
+  // left unchanged)
+  double acc[4][4][2];
 #pragma unroll
-  for (int mi = 0; mi < 8; ++mi)
+  for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        acc[mi][ni][h] = f[(long long)(c0 + wn * 32 + ni * 8 + 2 * (lane & 3) + h) * ld + r0 +
+                           wm * 32 + mi * 8 + (lane >> 2)];
   const int nchunks = K / kUpdKC;
   constexpr int kStage = kUpdKC * (kUpdLdA + kUpdLdB);
   auto load = [&](int chunk, int stage) {
     double *As = sm + stage * kStage, *Bs = As + kUpdKC * kUpdLdA;
     // A: kUpdKC columns x 64 pieces of 16 B; B: kUpdKC x 32
-    for (int p = tid; p < kUpdKC * 64; p += 128) {
+    for (int p = tid; p < kUpdKC * 64; p += kUpdThreads) {
       const int q = p >> 6, m = (p & 63) * 2;
       cp_async16(As + q * kUpdLdA + m, Ag + ((long long)chunk * kUpdKC + q) * ld + m);
     }
-    for (int p = tid; p < kUpdKC * 32; p += 128) {
+    for (int p = tid; p < kUpdKC * 32; p += kUpdThreads) {
       const int q = p >> 5, n = (p & 31) * 2;
       cp_async16(Bs + q * kUpdLdB + n, Bg + ((long long)chunk * kUpdKC + q) * ld + n);
     }
@@ -368,13 +530,13 @@ __global__ void __launch_bounds__(128, 2) k_sn_update_f64(SnDev d, int base, con
 #pragma unroll
     for (int kk = 0; kk < kUpdKC; kk += 4) {
       const int q = kk + (lane & 3);
-      double a[8], b[4];
+      double a[4], b[4];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi) a[mi] = As[q * kUpdLdA + wm * 64 + mi * 8 + (lane >> 2)];
+      for (int mi = 0; mi < 4; ++mi) a[mi] = As[q * kUpdLdA + wm * 32 + mi * 8 + (lane >> 2)];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[q * kUpdLdB + wn * 32 + ni * 8 + (lane >> 2)];
+      for (int ni = 0; ni < 4; ++ni) b[ni] = -Bs[q * kUpdLdB + wn * 32 + ni * 8 + (lane >> 2)];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi)
+      for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
     }
@@ -382,14 +544,14 @@ __global__ void __launch_bounds__(128, 2) k_sn_update_f64(SnDev d, int base, con
   cp_async_wait<0>();
   const bool diag = r0 < c0 + 64;  // the tile reaches above the diagonal
 #pragma unroll
-  for (int mi = 0; mi < 8; ++mi) {
-    const int m = wm * 64 + mi * 8 + (lane >> 2);
+  for (int mi = 0; mi < 4; ++mi) {
+    const int m = wm * 32 + mi * 8 + (lane >> 2);
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int n = wn * 32 + ni * 8 + 2 * (lane & 3) + h;
-        if (!diag || r0 + m >= c0 + n) f[(long long)(c0 + n) * ld + r0 + m] -= acc[mi][ni][h];
+        if (!diag || r0 + m >= c0 + n) f[(long long)(c0 + n) * ld + r0 + m] = acc[mi][ni][h];
       }
   }
 }
@@ -407,11 +569,14 @@ __global__ void __launch_bounds__(128, 2) k_sn_update_f32(SnDev d, int base, con
   extern __shared__ __align__(16) unsigned char sraw[];
   float *sm = reinterpret_cast<float *>(sraw);
   const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+  // accumulators start from the front tile (as in the FP64 kernel)
   float acc[8][8];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    for (int j = 0; j < 8; ++j)
+      acc[i][j] = f[(long long)(c0 + (j < 4 ? 0 : 32) + tx * 4 + (j & 3)) * ld + r0 +
+                    (i < 4 ? 0 : 64) + ty * 4 + (i & 3)];
   const int nchunks = K / kUpdKC;
   constexpr int kStage = kUpdKC * (kUpdLdA + kUpdLdB);
   auto load = [&](int chunk, int stage) {
@@ -449,7 +614,7 @@ __global__ void __launch_bounds__(128, 2) k_sn_update_f32(SnDev d, int base, con
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(-a[i], b[j], acc[i][j]);
     }
   }
   cp_async_wait<0>();
@@ -460,7 +625,7 @@ __global__ void __launch_bounds__(128, 2) k_sn_update_f32(SnDev d, int base, con
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int n = (j < 4 ? 0 : 32) + tx * 4 + (j & 3);
-      if (!diag || r0 + m >= c0 + n) f[(long long)(c0 + n) * ld + r0 + m] -= acc[i][j];
+      if (!diag || r0 + m >= c0 + n) f[(long long)(c0 + n) * ld + r0 + m] = acc[i][j];
     }
   }
 }
@@ -584,48 +749,80 @@ __global__ void __launch_bounds__(256) k_sn_fwd_gather(SnDev d, int base, int co
   }
 }
 
-// forward: v[k..k+K) <- L11^-1 v[k..k+K).  L11's strict lower triangle is
-// first copied to shared memory (coalesced), so the K dependent steps read
-// shared memory only.
+// forward: v[k..k+K) <- L11^-1 v[k..k+K).  L11 is first copied to shared
+// memory (coalesced pairs), then one warp runs the K dependent steps with x
+// in registers.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_sn_fwd_diag(SnDev d, int base) {
+__global__ void __launch_bounds__(kDiagSolveThreads) k_sn_fwd_diag(SnDev d, int base) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16;
   if (!d.srun[d.inst[s]]) return;
   extern __shared__ __align__(16) unsigned char sraw[];
-  T *Ls = reinterpret_cast<T *>(sraw);  // K x K, column-major, stride K
-  __shared__ double x[kSnNB];
+  T *Ls = reinterpret_cast<T *>(sraw);  // column j at Ls + j kSnNB
   const long long ld = d.ld[s];
   double *v = d.S + d.soff[s] + k0;
   const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + k0;
-  const int i = threadIdx.x;
-  for (int j = 0; j < K; ++j)
-    if (i < K) Ls[j * K + i] = f[j * ld + i];
-  if (i < K) x[i] = v[i];
-  __syncthreads();
-  double xi = i < K ? x[i] : 0.0;
-  for (int j = 0; j < K; ++j) {
-    if (i == j) x[j] = xi;
-    __syncthreads();
-    if (i > j && i < K) xi -= double(Ls[j * K + i]) * x[j];
+  // stage L11 by pairs of rows (K, ld and the front offsets are even); a
+  // fixed trip count, so the loads are unrolled and many are in flight
+#pragma unroll 8
+  for (int it = 0; it < kSnNB * kSnNB / 2 / kDiagSolveThreads; ++it) {
+    const int p = threadIdx.x + it * kDiagSolveThreads, j = p >> 6, i = (p & 63) * 2;
+    if (j < K && i < K) store_pair(Ls + j * kSnNB + i, load_pair(f + j * ld + i));
   }
-  if (i < K) v[i] = xi;
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  // one warp: lane owns rows lane + 32 r; x_j is final when step j starts
+  // and is broadcast from its owner
+  const int lane = threadIdx.x;
+  double xr[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) xr[r] = lane + 32 * r < K ? v[lane + 32 * r] : 0.0;
+#pragma unroll
+  for (int sb = 0; sb < 4; ++sb) {
+    if (32 * sb >= K) break;
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) {
+      const int j = 32 * sb + jj;
+      const double xj = __shfl_sync(0xffffffffu, xr[sb], jj);
+#pragma unroll
+      for (int r = sb; r < 4; ++r) {
+        const int i = 32 * r + lane;
+        if (i > j && i < K) xr[r] -= double(Ls[j * kSnNB + i]) * xj;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    if (lane + 32 * r < K) v[lane + 32 * r] = xr[r];
 }
-// forward: v[r0..r0+128) -= L(r0.., panel) v[k..k+K)
+
+// forward: v[r0..r0+128) -= L(r0.., panel) v[k..k+K).  Thread (rp, g) takes
+// rows 2 rp, 2 rp + 1 and columns g, g + 4, ...; the four column groups'
+// sums are added in group order.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_sn_fwd_gemv(SnDev d, int base) {
+__global__ void __launch_bounds__(kGemvThreads) k_sn_fwd_gemv(SnDev d, int base) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, r0 = t.z;
   if (!d.srun[d.inst[s]]) return;
   __shared__ double x[kSnNB];
+  __shared__ __align__(16) double acc[4][kSnNB];
   const long long ld = d.ld[s];
   double *v = d.S + d.soff[s];
-  if (threadIdx.x < K) x[threadIdx.x] = v[k0 + threadIdx.x];
+  const int tid = threadIdx.x, rp = tid & 63, g = tid >> 6;
+  if (tid < K) x[tid] = v[k0 + tid];
   __syncthreads();
-  const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + r0 + threadIdx.x;
-  double acc = 0;
-  for (int q = 0; q < K; ++q) acc += double(f[q * ld]) * x[q];
-  v[r0 + threadIdx.x] -= acc;
+  const T *fp = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + r0 + 2 * rp;
+  double a0 = 0.0, a1 = 0.0;
+#pragma unroll 8
+  for (int q = g; q < K; q += 4) {
+    const Pair<T> w = load_pair(fp + q * ld);
+    const double xq = x[q];
+    a0 += double(w.x) * xq;
+    a1 += double(w.y) * xq;
+  }
+  reinterpret_cast<double2 *>(acc[g])[rp] = make_double2(a0, a1);
+  __syncthreads();
+  if (tid < kSnNB) v[r0 + tid] -= (acc[0][tid] + acc[1][tid]) + (acc[2][tid] + acc[3][tid]);
 }
 
 __global__ void __launch_bounds__(kVecThreads) k_sn_fwd_scatter(SnDev d, int base) {
@@ -650,66 +847,119 @@ __global__ void __launch_bounds__(kVecThreads) k_sn_bwd_gather(SnDev d, int base
   }
 }
 
-// backward: partial sums over the row tile r0: p[q] = sum_m L(r0 + m, k + q) v[r0 + m]
+// backward: partial sums over the row tile r0: p[q] = sum_m L(r0 + m, k + q) v[r0 + m].
+// Thread (rp, g) takes rows 2 rp, 2 rp + 1 and columns g, g + 4, ...; each
+// column's 64 products are summed by a fixed butterfly in the two warps of
+// its group, then the two warp sums in order.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_sn_bwd_partial(SnDev d, int base) {
+__global__ void __launch_bounds__(kGemvThreads) k_sn_bwd_partial(SnDev d, int base) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16, r0 = t.z;
   if (!d.srun[d.inst[s]]) return;
+  __shared__ double red[2][kSnNB];
   const long long ld = d.ld[s];
   const double *v = d.S + d.soff[s] + r0;
   double *part = d.S + d.soff[s] + ld + r0;  // tile r0's partials at [r0, r0 + K)
-  const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + r0;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double vm[4];
+  const int tid = threadIdx.x, rp = tid & 63, g = tid >> 6, lane = tid & 31, h = rp >> 5;
+  const double2 vm = reinterpret_cast<const double2 *>(v)[rp];
+  const T *fp = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + r0 + 2 * rp;
+  for (int c0 = 0; 4 * c0 < K; c0 += 8) {
+    double pr[8];
 #pragma unroll
-  for (int e = 0; e < 4; ++e) vm[e] = v[lane * 4 + e];
-  for (int q = w; q < K; q += kVecThreads / 32) {
-    const T *fc = f + q * ld + lane * 4;
-    double acc = 0;
+    for (int u = 0; u < 8; ++u) {
+      const int q = g + 4 * (c0 + u);
+      pr[u] = 0.0;
+      if (q < K) {
+        const Pair<T> w = load_pair(fp + q * ld);
+        pr[u] = double(w.x) * vm.x + double(w.y) * vm.y;
+      }
+    }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) acc += double(fc[e]) * vm[e];
-    acc = warp_sum(acc);
-    if (lane == 0) part[q] = acc;
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pr[u] += __shfl_xor_sync(0xffffffffu, pr[u], off);
+    if (lane == 0)
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int q = g + 4 * (c0 + u);
+        if (q < K) red[h][q] = pr[u];
+      }
   }
+  __syncthreads();
+  if (tid < K) part[tid] = red[0][tid] + red[1][tid];
 }
 
 // backward: v[k..k+K) <- L11^-T (v[k..k+K) - sum of the tiles' partials),
-// the partials summed in tile order; L11 staged in shared memory, then one
-// warp runs the K dependent column dot products
+// the partials summed in a fixed order (kParts interleaved runs of tiles,
+// then the runs in order).  L11 is staged transposed (row i of L11
+// contiguous, stride kSnNB + 1), then one warp runs the chain: lane owns
+// x_j for j = lane + 32 r; x_i is final when step i (descending) starts,
+// is broadcast from its owner, and L(i, j) x_i leaves every x_j, j < i.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_sn_bwd_diag(SnDev d, int base) {
+__global__ void __launch_bounds__(kDiagSolveThreads) k_sn_bwd_diag(SnDev d, int base) {
   const int4 t = d.tasks[base + blockIdx.x];
   const int s = t.x, k0 = t.y & 0xffff, K = t.y >> 16;
   if (!d.srun[d.inst[s]]) return;
   extern __shared__ __align__(16) unsigned char sraw[];
-  T *Ls = reinterpret_cast<T *>(sraw);  // K x K, column-major, stride K
-  __shared__ double x[kSnNB];
+  T *LT = reinterpret_cast<T *>(sraw);  // LT[i (kSnNB + 1) + j] = L(i, j)
+  constexpr int KP = kSnNB + 1;
+  constexpr int kParts = kDiagSolveThreads / kSnNB;  // threads per partial sum
+  __shared__ double a[kParts][kSnNB];
   const long long ld = d.ld[s];
   double *v = d.S + d.soff[s];
   const double *part = v + ld;
-  const int q = threadIdx.x, e = k0 + K;
+  const int e = k0 + K;
   const T *f = reinterpret_cast<const T *>(d.F) + d.foff[s] + k0 * ld + k0;
-  for (int j = 0; j < K; ++j)
-    if (q < K) Ls[j * K + q] = f[j * ld + q];
-  if (q < K) {
-    double a = v[k0 + q];
-    for (long long r0 = e; r0 < ld; r0 += kSnNB) a -= part[r0 + q];
-    x[q] = a;
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    for (int j = K - 1; j >= 0; --j) {
-      double acc = 0;
-      for (int i = j + 1 + lane; i < K; i += 32) acc += double(Ls[j * K + i]) * x[i];
-      acc = warp_sum(acc);
-      if (lane == 0) x[j] -= acc;
-      __syncwarp();
+#pragma unroll 8
+  for (int it = 0; it < kSnNB * kSnNB / 2 / kDiagSolveThreads; ++it) {
+    const int p = threadIdx.x + it * kDiagSolveThreads, j = p >> 6, i = (p & 63) * 2;
+    if (j < K && i < K) {
+      const Pair<T> w = load_pair(f + j * ld + i);
+      LT[i * KP + j] = w.x;
+      LT[(i + 1) * KP + j] = w.y;
     }
   }
+  // the tiles' partials of column q: thread (q, h) sums tiles h, h + kParts,
+  // ... in order; the kParts sums are then added in order
+  {
+    const int q = threadIdx.x & (kSnNB - 1), h = threadIdx.x / kSnNB;
+    double acc = 0.0;
+    if (q < K)
+#pragma unroll 4
+      for (long long r0 = e + (long long)h * kSnNB; r0 < ld; r0 += kParts * kSnNB)
+        acc += part[r0 + q];
+    a[h][q] = acc;
+  }
   __syncthreads();
-  if (q < K) v[k0 + q] = x[q];
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  double xr[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int j = lane + 32 * r;
+    double sum = 0.0;
+#pragma unroll
+    for (int h = 0; h < kParts; ++h) sum += a[h][j];
+    xr[r] = j < K ? v[k0 + j] - sum : 0.0;
+  }
+#pragma unroll
+  for (int sb = 3; sb >= 0; --sb) {
+    if (32 * sb >= K) continue;
+#pragma unroll
+    for (int jj = 31; jj >= 0; --jj) {
+      const int i = 32 * sb + jj;
+      if (i >= K) continue;  // uniform over the warp
+      const double xi = __shfl_sync(0xffffffffu, xr[sb], jj);
+#pragma unroll
+      for (int r = 0; r <= sb; ++r) {
+        const int j = 32 * r + lane;
+        if (j < i) xr[r] -= double(LT[i * KP + j]) * xi;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    if (lane + 32 * r < K) v[k0 + lane + 32 * r] = xr[r];
 }
 
 __global__ void __launch_bounds__(kVecThreads) k_sn_bwd_scatter(SnDev d, int base) {
@@ -810,8 +1060,8 @@ __global__ void k_sn_clear_ok(const int *insts, const int *bad, int n, int *ok) 
 inline int nb256(long long n) { return n <= 0 ? 1 : (int)((n + 255) / 256); }
 
 template <typename T>
-size_t diag_smem() {
-  return (size_t)kSnNB * kSnNB * sizeof(T) + kSnNB * sizeof(T);
+size_t diag_smem() {  // the block and the scaled columns of one column block
+  return (size_t)kSnNB * kSnNB * sizeof(T) + (size_t)kDiagNB * kSnNB * sizeof(T);
 }
 template <typename T>
 size_t trsm_smem() {  // the tile (kSnNB x kSnNB) and the packed strict lower L11
@@ -835,7 +1085,7 @@ void set_sn_attrs() {
   cudaFuncSetAttribute(k_sn_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(kSnNB * kSnNB * sizeof(T)));
   cudaFuncSetAttribute(k_sn_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(kSnNB * kSnNB * sizeof(T)));
+                       (int)(kSnNB * (kSnNB + 1) * sizeof(T)));
   if (sizeof(T) == 8)
     cudaFuncSetAttribute(k_sn_update_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)gemm_smem<double>());
@@ -903,7 +1153,7 @@ void run_factor(SnExec &ex, const KKTDev &k, const LDLParams &p, const int *run,
         break;
       case SN_UPDATE:
         if (sizeof(T) == 8)
-          k_sn_update_f64<<<L.count, 128, gemm_smem<double>(), st>>>(d, L.begin, run);
+          k_sn_update_f64<<<L.count, kUpdThreads, gemm_smem<double>(), st>>>(d, L.begin, run);
         else
           k_sn_update_f32<<<L.count, 128, gemm_smem<float>(), st>>>(d, L.begin, run);
         break;
@@ -927,9 +1177,9 @@ void run_solve_pass(SnExec &ex, cudaStream_t st) {
       case SN_FWD_SMALL: k_sn_fwd_small<T><<<(L.count + 7) / 8, 256, 0, st>>>(d, L.begin, L.count); break;
       case SN_FWD_GATHER: k_sn_fwd_gather<<<(L.count + 7) / 8, 256, 0, st>>>(d, L.begin, L.count); break;
       case SN_FWD_DIAG:
-        k_sn_fwd_diag<T><<<L.count, kVecThreads, kSnNB * kSnNB * sizeof(T), st>>>(d, L.begin);
+        k_sn_fwd_diag<T><<<L.count, kDiagSolveThreads, kSnNB * kSnNB * sizeof(T), st>>>(d, L.begin);
         break;
-      case SN_FWD_GEMV: k_sn_fwd_gemv<T><<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
+      case SN_FWD_GEMV: k_sn_fwd_gemv<T><<<L.count, kGemvThreads, 0, st>>>(d, L.begin); break;
       case SN_FWD_SCATTER: k_sn_fwd_scatter<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
       default: break;
     }
@@ -942,9 +1192,10 @@ void run_solve_pass(SnExec &ex, cudaStream_t st) {
     switch (L.kind) {
       case SN_BWD_SMALL: k_sn_bwd_small<T><<<(L.count + 7) / 8, 256, 0, st>>>(d, L.begin, L.count); break;
       case SN_BWD_GATHER: k_sn_bwd_gather<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
-      case SN_BWD_PARTIAL: k_sn_bwd_partial<T><<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
+      case SN_BWD_PARTIAL: k_sn_bwd_partial<T><<<L.count, kGemvThreads, 0, st>>>(d, L.begin); break;
       case SN_BWD_DIAG:
-        k_sn_bwd_diag<T><<<L.count, kVecThreads, kSnNB * kSnNB * sizeof(T), st>>>(d, L.begin);
+        k_sn_bwd_diag<T><<<L.count, kDiagSolveThreads, kSnNB * (kSnNB + 1) * sizeof(T), st>>>(
+            d, L.begin);
         break;
       case SN_BWD_SCATTER: k_sn_bwd_scatter<<<L.count, kVecThreads, 0, st>>>(d, L.begin); break;
       default: break;
@@ -954,6 +1205,38 @@ void run_solve_pass(SnExec &ex, cudaStream_t st) {
   }
   ex.launches++;
   prof_collect(ex);
+}
+
+// one pass, replayed from a CUDA graph when possible (direct launches while
+// profiling or if capturing failed)
+template <typename T>
+void solve_pass(SnExec &ex, cudaStream_t st) {
+  if (!ex.prof.on && !ex.g_pass && !ex.graph_failed) {
+    set_sn_attrs<T>();
+    bool ok = ex.cap || cudaStreamCreateWithFlags(&ex.cap, cudaStreamNonBlocking) == cudaSuccess;
+    cudaGraph_t g = nullptr;
+    const long long before = ex.launches;
+    if (ok) ok = cudaStreamBeginCapture(ex.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      run_solve_pass<T>(ex, ex.cap);
+      ok = cudaStreamEndCapture(ex.cap, &g) == cudaSuccess && g;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ex.g_pass, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    ex.pass_launches = ex.launches - before;
+    ex.launches = before;
+    if (!ok) {
+      ex.g_pass = nullptr;
+      ex.graph_failed = true;
+      cudaGetLastError();  // clear a capture error; the pass runs directly
+    }
+  }
+  if (!ex.prof.on && ex.g_pass) {
+    cudaGraphLaunch(ex.g_pass, st);
+    ex.launches += ex.pass_launches;
+  } else {
+    run_solve_pass<T>(ex, st);
+  }
 }
 
 }  // namespace
@@ -981,6 +1264,8 @@ void sn_get_profile(const SnExec &ex, double *ms, double *flops, long long *call
 }
 
 SnExec::~SnExec() {
+  if (g_pass) cudaGraphExecDestroy(g_pass);
+  if (cap) cudaStreamDestroy(cap);
   for (cudaEvent_t e : prof.pool) cudaEventDestroy(e);
   if (h_srun) cudaFreeHost(h_srun);
   if (h_flags) cudaFreeHost(h_flags);
@@ -1065,9 +1350,9 @@ void sn_solve(SnExec &ex, const KKTDev &k, const LDLParams &p, const int *run, c
   const int B = ex.B;
   auto pass = [&]() {
     if (ex.fp32)
-      run_solve_pass<float>(ex, st);
+      solve_pass<float>(ex, st);
     else
-      run_solve_pass<double>(ex, st);
+      solve_pass<double>(ex, st);
   };
   auto upload_srun = [&](const std::vector<char> &on) {
     cudaStreamSynchronize(st);  // the previous upload has left the staging

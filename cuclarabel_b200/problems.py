@@ -13,6 +13,7 @@ A CSC and cones as a list of cone objects (cuclarabel_b200.api).
   exp_pow_psd(scale, seed)  conic LP with exp/pow/PSD cones (n=30000 at
                             scale 1): 20000 exp, 5000 pow, 200 PSD(10),
                             10000 nonneg
+  psd_lp(side, ncones, ...) linear SDP over PSD blocks of one side
   mpc_qp(seed)              one MPC-style QP/SOCP, n ~ U{20..400}, m ~ 2n
   mpc_batch(count, seed0)   `count` MPC-style instances, instance i seeded i
 
@@ -176,6 +177,32 @@ def exp_pow_psd(scale=1.0, seed=3, psd_n=10):
     s0, z0 = interior(), interior()
     cones = ([NonnegativeConeT(nnn)] + [ExponentialConeT()] * nexp
              + [PowerConeT(float(a)) for a in alphas] + [PSDTriangleConeT(psd_n)] * npsd)
+    return _finish(sp.csc_matrix((n, n)), A, x0, s0, z0, cones)
+
+
+def psd_lp(side=24, ncones=3, m_eq=None, seed=0):
+    """Linear SDP: ncones PSD blocks of the given side (svec variables x),
+    m_eq random equality rows coupling them, x + b_psd in the PSD cone,
+    cost from an interior dual (same interior-point construction as the
+    other families)."""
+    r = _rng(seed)
+    t = side * (side + 1) // 2
+    n = ncones * t
+    m_eq = m_eq if m_eq is not None else max(1, n // 4)
+    Aeq = sp.random(m_eq, n, density=min(1.0, 8.0 / n), random_state=r,
+                    data_rvs=r.standard_normal, format="csc")
+    A = sp.vstack([Aeq, -sp.identity(n, format="csc")], format="csc")
+
+    def interior():
+        parts = []
+        for _ in range(ncones):
+            E = r.standard_normal((side, side)) * (0.6 / np.sqrt(side))
+            parts.append(_svec_sym(np.eye(side) + (E + E.T) / 2))
+        return np.concatenate(parts)
+    x0 = r.standard_normal(n)
+    s0 = np.concatenate([np.zeros(m_eq), interior()])
+    z0 = np.concatenate([r.standard_normal(m_eq), interior()])
+    cones = [ZeroConeT(m_eq)] + [PSDTriangleConeT(side)] * ncones
     return _finish(sp.csc_matrix((n, n)), A, x0, s0, z0, cones)
 
 

@@ -77,6 +77,8 @@ class OracleInfo(ctypes.Structure):
         ("ktratio", ctypes.c_double), ("mu", ctypes.c_double),
         ("sigma", ctypes.c_double), ("step_length", ctypes.c_double),
         ("solve_time", ctypes.c_double),
+        ("ir_solves", ctypes.c_int), ("ir_sweeps", ctypes.c_int),
+        ("ir_unconverged", ctypes.c_int), ("ir_worst_ratio", ctypes.c_double),
     ]
 
 

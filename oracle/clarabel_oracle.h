@@ -86,6 +86,10 @@ typedef struct {
   double res_primal, res_dual, res_primal_inf, res_dual_inf;
   double gap_abs, gap_rel, ktratio, mu, sigma, step_length;
   double solve_time;
+  /* iterative refinement over the run: solves, refinement sweeps, solves
+   * that ended above abstol + reltol |b|, worst final |e| / that tolerance */
+  int ir_solves, ir_sweeps, ir_unconverged;
+  double ir_worst_ratio;
 } oracle_info;
 
 void oracle_default_settings(oracle_settings *s);

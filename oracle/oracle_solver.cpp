@@ -104,6 +104,10 @@ struct KKTSolver {
   const oracle_settings *st;
   CompositeCone *cones;
   double diag_reg = 0;
+  // refinement statistics of the last solve loop: solves, sweeps, solves
+  // that ended above the tolerance, and the worst final |e| / tolerance
+  int ir_solves = 0, ir_sweeps = 0, ir_unconverged = 0;
+  double ir_worst = 0;
 
   void assemble(const CSC &P, const CSC &A, CompositeCone &C) {
     cones = &C;
@@ -309,22 +313,32 @@ struct KKTSolver {
       double normb = norm_inf(b.data(), N);
       double norme = refine_error(e, xsol);
       if (!std::isfinite(norme)) return false;
+      const double tol = st->iterative_refinement_abstol +
+                         st->iterative_refinement_reltol * normb;
+      double final_e = norme;
       for (int it = 0; it < st->iterative_refinement_max_iter; ++it) {
-        if (norme <= st->iterative_refinement_abstol +
-                         st->iterative_refinement_reltol * normb)
-          break;
+        if (norme <= tol) break;
         double last = norme;
         dx = e;
         ldl.solve(dx.data());
+        ++ir_sweeps;
         for (int i = 0; i < N; ++i) dx[i] += xsol[i];
         norme = refine_error(e, dx);
         if (!std::isfinite(norme)) return false;
         double ratio = last / norme;
         if (ratio < st->iterative_refinement_stop_ratio) {
           if (ratio > 1.0) std::swap(xsol, dx);
+          final_e = ratio > 1.0 ? norme : last;
+          norme = final_e;
           break;
         }
         std::swap(xsol, dx);
+        final_e = norme;
+      }
+      ++ir_solves;
+      if (final_e > tol) {
+        ++ir_unconverged;
+        ir_worst = std::max(ir_worst, final_e / tol);
       }
       ok = true;
     } else {
@@ -674,6 +688,8 @@ struct Solver {
   }
 
   void solve_loop() {
+    kkt.ir_solves = kkt.ir_sweeps = kkt.ir_unconverged = 0;
+    kkt.ir_worst = 0;
     int iter = 0;
     double sigma = 1.0, alpha = 0.0, mu = kMax;
     t0 = std::chrono::steady_clock::now();
@@ -917,6 +933,10 @@ int oracle_solve(int n, int m, const int *Pp, const int *Pi, const double *Px,
     S.solve_loop();
     S.finish(x, s, z);
     *info = S.info;
+    info->ir_solves = S.kkt.ir_solves;
+    info->ir_sweeps = S.kkt.ir_sweeps;
+    info->ir_unconverged = S.kkt.ir_unconverged;
+    info->ir_worst_ratio = S.kkt.ir_worst;
   } catch (std::exception &e) {
     std::fprintf(stderr, "oracle_solve: %s\n", e.what());
     return -2;
@@ -959,6 +979,10 @@ int oracle_solver_run(oracle_solver *h, double *x, double *s, double *z, oracle_
     h->S.solve_loop();
     h->S.finish(x, s, z);
     *info = h->S.info;
+    info->ir_solves = h->S.kkt.ir_solves;
+    info->ir_sweeps = h->S.kkt.ir_sweeps;
+    info->ir_unconverged = h->S.kkt.ir_unconverged;
+    info->ir_worst_ratio = h->S.kkt.ir_worst;
   } catch (std::exception &e) {
     std::fprintf(stderr, "oracle_solver_run: %s\n", e.what());
     return -2;

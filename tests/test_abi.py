@@ -44,3 +44,31 @@ def test_create_rejects_bad_input_without_gpu_work():
         _prep_problem(sp.eye(2), np.zeros(2), sp.eye(3, 2), np.zeros(3), [])
     with pytest.raises(ValueError):
         Settings(direct_solve_method="qdldl").to_c()
+
+
+def test_host_objects_hold_no_compiler_traps():
+    """gcc turns undefined behaviour it can prove (a division by a constant
+    zero, a null dereference on some path) into a trap instruction; the
+    library's own host objects must hold none."""
+    import shutil
+    import subprocess
+    import pytest
+    build = os.path.join(os.path.dirname(_lib.LIB_PATH), "_build")
+    objdump = shutil.which("objdump")
+    if not objdump or not os.path.isdir(build):
+        pytest.skip("objdump or the object directory is missing")
+    bad = []
+    for name in sorted(os.listdir(build)):
+        if not name.endswith(".o"):
+            continue
+        out = subprocess.run([objdump, "-d", "--no-show-raw-insn", "-C",
+                              os.path.join(build, name)],
+                             capture_output=True, text=True).stdout
+        fn = None
+        for line in out.splitlines():
+            m = re.match(r"^[0-9a-f]+ <(.*)>:$", line)
+            if m:
+                fn = m.group(1)
+            elif "\tud2" in line:
+                bad.append((name, fn))
+    assert not bad, bad

@@ -1,5 +1,6 @@
-"""Host-side arithmetic of bench.py (no GPU): the plain path's latency under
-the served run's arrival stream, and the cone operations' byte counts."""
+"""Host-side logic of bench.py and of the serving lanes (no GPU): the lanes'
+slot protocol, budget admission and concurrency on fake solvers, and the
+cone operations' byte counts."""
 import os
 import sys
 
@@ -10,26 +11,106 @@ sys.path.insert(0, ROOT)
 import bench  # noqa: E402
 
 
-def test_plain_under_load_matches_a_hand_computed_fifo_queue():
-    # same arrivals as the served run: replay the generator by hand
-    rng = np.random.default_rng(5)
-    n = int(rng.poisson(50 * 2.0))
-    arrive = np.sort(rng.uniform(0.0, 2.0, n))
-    svc = [0.01, 0.03]
-    t, resp = 0.0, []
-    for i in range(n):
-        t = max(t, arrive[i]) + svc[i % 2]
-        resp.append(t - arrive[i])
-    r = bench.plain_under_load(svc, 50, 2.0, 5)
-    assert r["requests"] == n
-    assert abs(r["p50_ms"] - 1000 * np.percentile(resp, 50)) < 1e-9
-    assert abs(r["p99_ms"] - 1000 * np.percentile(resp, 99)) < 1e-9
+class _Status:
+    name = "SOLVED"
 
 
-def test_plain_under_load_saturates_when_arrivals_outpace_service():
-    r = bench.plain_under_load([0.0075], 2000, 1.0, 1)
-    # ~2000 requests at 133/s: the last waits ~14 s
-    assert r["p99_ms"] > 10000 and r["value"] < 140
+class _Sol:
+    status = _Status()
+
+    def __init__(self, it):
+        self.iterations = it
+
+
+class FakeSlots:
+    """The serve_* protocol of BatchSolver on the host: an admitted slot
+    joins the next step and finishes after `steps[slot]` steps."""
+
+    def __init__(self, steps, nbytes=1000):
+        self.steps, self.left, self.nbytes = steps, {}, nbytes
+        self.admitted = []
+
+    def device_bytes(self):
+        return self.nbytes
+
+    def serve_admit(self, slots, q=None, b=None, stream=0):
+        for k in slots:
+            assert k not in self.left, "slot admitted while running"
+            self.left[k] = self.steps[k]
+            self.admitted.append(k)
+
+    def serve_step(self, stream=0):
+        fin = []
+        for k in list(self.left):
+            self.left[k] -= 1
+            if self.left[k] == 0:
+                fin.append(k)
+                del self.left[k]
+        return sorted(fin), len(self.left)
+
+    def serve_collect(self, slots, stream=0):
+        return [_Sol(self.steps[k]) for k in slots]
+
+
+def test_slot_lane_serves_every_request_in_slot_order():
+    from cuclarabel_b200 import serving
+    budget = serving.Budget(10_000)
+    fake = FakeSlots({0: 3, 1: 5, 2: 2})
+    lane = serving.SlotLane("fake", fake, 0, budget)
+    assert budget.held == 1000
+    arrive = np.zeros(7)
+    slot = np.array([0, 1, 0, 2, 0, 1, 2])
+    left = lane.run(0.0 + __import__("time").perf_counter(), arrive, slot, [None] * 7,
+                    [None] * 7, 30.0)
+    assert left == 0 and len(lane.stats.lat) == 7
+    # a slot's requests run one after another, in arrival order
+    assert [k for k in fake.admitted if k == 0] == [0, 0, 0]
+    assert lane.stats.status["SOLVED"] == 7
+    lane.close()
+    assert budget.held == 0
+
+
+def test_cohort_lane_waits_for_the_budget_and_frees_it():
+    from cuclarabel_b200 import serving
+    import scipy.sparse as sp
+    budget = serving.Budget(5000)
+    budget.hold(4000)  # a resident lane
+    made = []
+
+    def make(pbs):
+        made.append(len(pbs))
+        return FakeSlots({k: 2 for k in range(len(pbs))}, nbytes=800)
+
+    lane = serving.CohortLane("fake", 0, budget, bytes_per_nnz=1.0, make_solver=make)
+    pb = (sp.csc_matrix((3, 3)), np.zeros(3), sp.csc_matrix(np.eye(3)), np.zeros(3), [])
+    import threading
+    import time
+    t0 = time.perf_counter()
+    # 9 nnz per problem: 4 problems need 36 + 4000 <= 5000; then true 800 B
+    th = threading.Thread(target=lambda: lane.run(t0, np.zeros(4), [pb] * 4, 30.0))
+    th.start()
+    th.join(10)
+    assert not th.is_alive()
+    assert made == [4] and lane.cohorts == 1 and len(lane.stats.lat) == 4
+    assert budget.held == 4000 and budget.peak == 4800
+    # a cohort larger than the free budget waits until the horizon
+    budget.hold(950)
+    lane2 = serving.CohortLane("fake", 0, budget, bytes_per_nnz=100.0, make_solver=make)
+    left = lane2.run(time.perf_counter(), np.zeros(2), [pb] * 2, 0.05)
+    assert left == 2 and lane2.waited_for_budget > 0 and lane2.cohorts == 0
+
+
+def test_run_lanes_runs_lanes_concurrently():
+    from cuclarabel_b200 import serving
+
+    class Sleeper:
+        def run(self, t0, d, horizon):
+            import time
+            time.sleep(d)
+            return 0
+
+    wall, left = serving.run_lanes([(Sleeper(), (0.2,)), (Sleeper(), (0.2,))], 5.0)
+    assert left == [0, 0] and wall < 0.35
 
 
 def test_cone_op_bytes_per_element_and_cone():

@@ -96,3 +96,18 @@ def test_slot_reuse_and_errors(cuda_device):
     again = s.solve()
     for k in range(4):
         _same(again[k], ref[k])
+
+
+def test_served_supernodal_slots_equal_their_lone_solves(cuda_device):
+    """Large slots (configuration-2-like structures on the supernodal
+    factorisation, the serving configuration's large requests) admitted
+    while another is mid-solve give exactly their lone results: the
+    supernodal launches cover only running instances and every reduction
+    has a fixed order."""
+    pbs = [problems.mixed_socp(0.08, seed=41), problems.mixed_socp(0.1, seed=42),
+           problems.mixed_socp(0.09, seed=43)]
+    alone = [BatchSolver([pb]).solve()[0] for pb in pbs]
+    s = BatchSolver(pbs)
+    got = _serve_all(s, [[1], [], [0, 2]])
+    for k in range(3):
+        _same(got[k], alone[k])
