@@ -703,11 +703,20 @@ __device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
     off = warp_sum(off);
     tot = warp_sum(tot);
     if (off <= 1e-30 * tot || off == 0) break;
+    // threshold Jacobi: a rotation whose effect on the diagonal is below
+    // the rounding of its entries (apq^2 <= 2^-106 |app aqq|) or of the
+    // matrix (apq^2 <= 1e-30 |A|_F^2 / n^2) is skipped; a sweep without a
+    // rotation ends the iteration
+    const double tiny = 1e-30 * tot / (double(n) * n);
+    bool rotated = false;
     for (int p = 0; p < n; ++p)
       for (int q = p + 1; q < n; ++q) {
         double apq = A[p + n * q];
         if (apq == 0) continue;
         double app = A[p + n * p], aqq = A[q + n * q];
+        const double a2 = apq * apq;
+        if (a2 <= 1.2325951644078310e-32 * fabs(app * aqq) || a2 <= tiny) continue;
+        rotated = true;
         double theta = (aqq - app) / (2 * apq);
         double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
         double c = 1 / sqrt(t * t + 1), s = t * c;
@@ -725,6 +734,7 @@ __device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
         }
         __syncwarp();
       }
+    if (!rotated) break;
   }
   double v = CUDART_INF;
   for (int r = lane; r < n; r += 32) {

@@ -376,6 +376,37 @@ static void csc_transpose(const HostCSC &A, HostCSC &T) {
     }
 }
 
+// entries of the single-warp kernels' encoded streams addressable by a
+// chunk word (ldl.cuh kStartMask)
+constexpr long long kStreamMaxEntries = (1LL << 22) - 1;
+
+// true when the scalar factor of the pattern (CSR graph, repeats allowed,
+// no self loops needed) under perm has more than `limit` entries below the
+// diagonal; elimination-tree path walk (Liu), stopping early
+static bool scalar_fill_exceeds(int N, const std::vector<int> &xadj,
+                                const std::vector<int> &adj, const std::vector<int> &perm,
+                                long long limit) {
+  std::vector<int> iperm(N), parent(N, -1), mark(N, -1);
+  for (int k = 0; k < N; ++k) iperm[perm[k]] = k;
+  long long lnz = 0;
+  for (int k = 0; k < N; ++k) {
+    mark[k] = k;
+    const int o = perm[k];
+    for (int p = xadj[o]; p < xadj[o + 1]; ++p) {
+      int i = iperm[adj[p]];
+      if (i >= k) continue;
+      while (mark[i] != k) {
+        if (parent[i] == -1) parent[i] = k;
+        ++lnz;
+        mark[i] = k;
+        i = parent[i];
+      }
+    }
+    if (lnz > limit) return true;
+  }
+  return false;
+}
+
 bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared &out) {
   const int n = pb.n, m = pb.m;
   out = Prepared();
@@ -656,12 +687,15 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
         adjncy[cur[en.c]++] = en.r;
       }
     // instances whose work vector exceeds the single-warp kernels' budget
-    // (48 KB of FP64) take the supernodal factorisation
-    out.supernodal = (long long)N * 8 > 48 * 1024;
+    // (48 KB of FP64), or whose factor or matrix exceeds the range of their
+    // stream chunk words, take the supernodal factorisation
+    out.supernodal = (long long)N * 8 > 48 * 1024 || (long long)xadj[N] + N > kStreamMaxEntries;
+    if (!out.supernodal) {
+      out.perm = nd_order_csr(N, xadj, adjncy);
+      out.supernodal = scalar_fill_exceeds(N, xadj, adjncy, out.perm, kStreamMaxEntries);
+    }
     if (out.supernodal) {
       if (!sn_analyse(N, xadj, adjncy, out.perm, out.sym, &out.error)) return false;
-    } else {
-      out.perm = nd_order_csr(N, xadj, adjncy);
     }
   }
   out.iperm.assign(N, 0);

@@ -232,7 +232,24 @@ __global__ void __launch_bounds__(kAsmThreads) k_sn_assemble(SnDev d, KKTDev k, 
     for (int q = qa; q < qb; ++q) {
       const long long pc = rel[q];
       const T *src = cf + (cu + q) * cld + cu;
-      for (int r = q + tid; r < cn; r += kAsmThreads) f[pc * ld + rel[r]] += src[r];
+      // four rows per thread per round, their loads issued before any add
+      // (the parent positions of one column are distinct)
+      for (int r0 = q + tid; r0 < cn; r0 += 4 * kAsmThreads) {
+        int rr[4];
+        T sv[4], fv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = r0 + u * kAsmThreads;
+          rr[u] = r < cn ? rel[r] : 0;
+          sv[u] = r < cn ? src[r] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (r0 + u * kAsmThreads < cn) fv[u] = f[pc * ld + rr[u]];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (r0 + u * kAsmThreads < cn) f[pc * ld + rr[u]] = fv[u] + sv[u];
+      }
     }
     __syncthreads();
   }
@@ -269,9 +286,13 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
   T *ws = reinterpret_cast<T *>(d.W) + d.woff[s];
   const int *fi = d.fidx + d.fix_off[s];
   const int tid = threadIdx.x;
-  for (int idx = tid; idx < K * K; idx += kDiagThreads) {
-    const int c = idx / K, r = idx - c * K;
-    blk[idx] = r >= c ? f[(k0 + c) * ld + k0 + r] : T(0);
+  // stage the block by row pairs (16-byte loads for FP64), a fixed trip
+  // count so that many loads are in flight; the strict upper part is not
+  // read by the factorisation below
+#pragma unroll 8
+  for (int it = 0; it < kSnNB * kSnNB / 2 / kDiagThreads; ++it) {
+    const int p = tid + it * kDiagThreads, c = p >> 6, r = (p & 63) * 2;
+    if (c < K && r < K) store_pair(blk + c * K + r, load_pair(f + (k0 + c) * ld + k0 + r));
   }
   for (int j = tid; j < K; j += kDiagThreads) {
     const int g = fi[k0 + j];
@@ -356,12 +377,11 @@ __global__ void __launch_bounds__(kDiagThreads) k_sn_diag(SnDev d, KKTDev k, LDL
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < K * K; idx += kDiagThreads) {
-    const int c = idx / K, r = idx - c * K;
-    if (r > c)
-      f[(k0 + c) * ld + k0 + r] = blk[idx] * T(dinv[c]);
-    else if (r == c)
-      f[(k0 + c) * ld + k0 + r] = dd[c];
+#pragma unroll 8
+  for (int it = 0; it < kSnNB * kSnNB / kDiagThreads; ++it) {
+    const int p = tid + it * kDiagThreads, c = p >> 7, r = p & (kSnNB - 1);
+    if (c < K && r < K && r >= c)
+      f[(k0 + c) * ld + k0 + r] = r > c ? blk[c * K + r] * T(dinv[c]) : dd[c];
   }
   bool bad = false;
   for (int j = tid; j < kSnNB; j += kDiagThreads) {
@@ -434,15 +454,21 @@ __global__ void __launch_bounds__(kTrsmThreads) k_sn_trsm(SnDev d, int base, con
   const T *ws = reinterpret_cast<const T *>(d.W) + d.woff[s];
   T *wr = reinterpret_cast<T *>(d.W) + d.woff[s] + kSnNB;
   const int tid = threadIdx.x;
-#pragma unroll 4
-  for (int it = 0; it < kSnNB * kSnNB / kTrsmThreads; ++it) {
-    const int idx = tid + it * kTrsmThreads, q = idx >> 7, m = idx & (kSnNB - 1);
-    if (q < K) X[idx] = f[(k0 + q) * ld + r0 + m];
+  // stage the tile and L11 by row pairs, fixed trip counts (many 16-byte
+  // loads in flight)
+#pragma unroll 8
+  for (int it = 0; it < kSnNB * kSnNB / 2 / kTrsmThreads; ++it) {
+    const int p = tid + it * kTrsmThreads, q = p >> 6, m = (p & 63) * 2;
+    if (q < K) store_pair(X + q * kSnNB + m, load_pair(f + (k0 + q) * ld + r0 + m));
   }
-#pragma unroll 4
-  for (int it = 0; it < kSnNB * kSnNB / kTrsmThreads; ++it) {
-    const int idx = tid + it * kTrsmThreads, j = idx >> 7, q = idx & (kSnNB - 1);
-    if (j < q && q < K) Lr[q * (q - 1) / 2 + j] = f[(k0 + j) * ld + k0 + q];
+#pragma unroll 8
+  for (int it = 0; it < kSnNB * kSnNB / 2 / kTrsmThreads; ++it) {
+    const int p = tid + it * kTrsmThreads, j = p >> 6, q = (p & 63) * 2;
+    if (j < K && q + 1 > j && q < K) {
+      const Pair<T> w = load_pair(f + (k0 + j) * ld + k0 + q);
+      if (q > j) Lr[q * (q - 1) / 2 + j] = w.x;
+      Lr[(q + 1) * q / 2 + j] = w.y;  // q + 1 > j
+    }
   }
   __syncthreads();
   const int m = tid & (kSnNB - 1), half = tid / kSnNB;
@@ -925,7 +951,7 @@ __global__ void __launch_bounds__(kDiagSolveThreads) k_sn_bwd_diag(SnDev d, int 
     const int q = threadIdx.x & (kSnNB - 1), h = threadIdx.x / kSnNB;
     double acc = 0.0;
     if (q < K)
-#pragma unroll 4
+#pragma unroll 8
       for (long long r0 = e + (long long)h * kSnNB; r0 < ld; r0 += kParts * kSnNB)
         acc += part[r0 + q];
     a[h][q] = acc;

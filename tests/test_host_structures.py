@@ -40,3 +40,11 @@ def test_config_families():
     # dense SOC path (threshold above every cone)
     rc, res = check(problems.mpc_qp(3), soc_threshold=100)
     assert rc == 0 and res < 1e-9
+
+
+@pytest.mark.parametrize("side,ncones", [(24, 3), (40, 2)])
+def test_psd_block_structures(side, ncones):
+    """Dense PSD blocks: side 40 fills the factor beyond the single-warp
+    streams' range and is prepared for the supernodal factorisation."""
+    rc, res = check(problems.psd_lp(side, ncones, seed=0))
+    assert rc == 0 and res < 1e-9
