@@ -546,9 +546,9 @@ def large_single(which, scale, method, sh, fp64_peak, cpu_scale):
         "solves_ms_per_solve": solve_ms,
         "kernels": {k: {"ms": round(v["ms"], 3), "launches": v["launches"]}
                     for k, v in sn.items() if v["launches"]},
-        "roofline": {"bound": "tensor", "kernel": "k_sn_gemm_f64<UPDATE> (trailing update of "
+        "roofline": {"bound": "tensor", "kernel": "k_sn_update_f64 (trailing update of "
                      "the blocked fronts, m8n8k4 FP64 DMMA)" if method == "cudss" else
-                     "k_sn_gemm_f32<UPDATE> (trailing update, FP32 FMA)",
+                     "k_sn_update_f32 (trailing update, FP32 FMA)",
                      "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": ach / fp64_peak if fp64_peak else None,
                      "peak_kind": "measured: cuBLAS FP64 GEMM 8192^3 on this GPU in this run",
@@ -594,6 +594,21 @@ def aggregate_over_ranks(elapsed, solved, dist, device):
     return tmax[0].item(), int(round(tsum[1].item()))
 
 
+def _b_noise(rng, cones, m):
+    """A request's change of b: +0.02 |N(0,1)| on the inequality rows (the
+    slack grows, so the problem stays feasible); equality (zero-cone) rows
+    keep their values, since an empty equality row must keep b = 0."""
+    from cuclarabel_b200.api import ZeroConeT
+    mask = np.ones(m)
+    row = 0
+    for c in cones:
+        d = c.nvars()
+        if isinstance(c, ZeroConeT):
+            mask[row:row + d] = 0.0
+        row += d
+    return 0.02 * np.abs(rng.standard_normal(m)) * mask
+
+
 # scales of the large (configuration-2-like) request structures of the
 # serving configuration: n = 20000 * scale spans 2000..20000
 SERVE_LARGE_SCALES = (0.1, 0.2, 0.35, 0.5, 0.75, 1.0)
@@ -629,13 +644,19 @@ def serve_config5(pbs, lam, seconds, seed, method, budget_gb, new_frac, large_fr
             continue
         P, q, A, b, cones = (large_pbs if cls[r] == 2 else pbs)[which[r]]
         qv[r] = q + 0.05 * rng.standard_normal(len(q))
-        bv[r] = b + 0.02 * np.abs(rng.standard_normal(len(b)))
+        bv[r] = b + _b_noise(rng, cones, len(b))
     idx = [np.nonzero(cls == c)[0] for c in range(3)]
     horizon = seconds + grace
 
     # ---- served arm: three lanes, one thread and stream each
     budget = serving.Budget(budget_gb * 1e9)
-    streams = [torch.cuda.Stream() for _ in range(3)]
+    # the MPC lanes' streams take the highest priority, the large lane's the
+    # lowest: the block scheduler then fills free SMs with MPC work first,
+    # so the large lane's long kernels do not set the MPC requests' latency
+    lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream,
+                                                           "priority_range") else (0, -1)
+    streams = [torch.cuda.Stream(priority=hi), torch.cuda.Stream(priority=lo),
+               torch.cuda.Stream(priority=hi)]
     t_setup = time.perf_counter()
     small = serving.SlotLane.build("resident MPC", pbs, streams[0].cuda_stream, budget,
                                    direct_solve_method=method)
@@ -702,9 +723,9 @@ def serve_config5(pbs, lam, seconds, seed, method, budget_gb, new_frac, large_fr
         if pw[r] >= 0:
             s_ = solvers[pw[r]]
             if cls[r] == 0:  # new q / b for the pool structure that serves it
-                _, q0, _, b0, _ = pbs[pw[r]]
+                _, q0, _, b0, c0_ = pbs[pw[r]]
                 s_.update_data(q=q0 + 0.05 * prng.standard_normal(len(q0)),
-                               b=b0 + 0.02 * np.abs(prng.standard_normal(len(b0))))
+                               b=b0 + _b_noise(prng, c0_, len(b0)))
             else:
                 s_.update_data(q=qv[r], b=bv[r])
             sol = s_.solve()
@@ -752,6 +773,8 @@ def main():
                     help="share of configuration-2-like requests (n 2000..20000)")
     ap.add_argument("--serve-grace", type=float, default=10.0,
                     help="seconds after the last arrival before both arms stop")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving configuration and print its JSON")
     ap.add_argument("--plain-pool", type=int, default=256,
                     help="single-instance solvers of the plain arm for resident MPC structures")
     ap.add_argument("--cone-scale", type=float, default=1.0,
@@ -806,6 +829,12 @@ def main():
     B = args.instances
     seed0 = rank_seed0(rank, B)
     pbs = gen_problems(B, seed0)
+    if args.serve_only:
+        print(json.dumps({"served": serve_config5(
+            pbs, args.serve_rate, args.serve_seconds, 12345 + rank, args.method,
+            args.serve_budget_gb, args.serve_new_frac, args.serve_large_frac,
+            args.serve_grace, args.plain_pool)}), flush=True)
+        return
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     solver = BatchSolver(pbs, direct_solve_method=args.method)

@@ -115,17 +115,20 @@ __global__ void k_soc_update_scaling(ConeSet cs, const double *__restrict__ s_,
     zscale = sscale = 1.0;  // keep lanes in lock step; results discarded
   }
   double eta = sqrt(sscale / zscale);
-  // w = s/sscale + (z0, -z1)/zscale
+  // w = s/sscale + (z0, -z1)/zscale, with the three scalings' reciprocals
+  // taken once per cone (the tile kernel below does the same, so both
+  // forms agree bit for bit)
+  const double isc = 1.0 / sscale, izc = 1.0 / zscale;
   double wl[4];  // per-lane cache (dim <= 4*G handled in registers)
   int k = 0;
   double w1sq_a = 0;
   SOC_FOR(i) {
-    double wi = s[i] / sscale + (i == 0 ? z[i] : -z[i]) / zscale;
+    double wi = __dadd_rn(__dmul_rn(s[i], isc), __dmul_rn(i == 0 ? z[i] : -z[i], izc));
     if (k < 4) wl[k] = wi;
     ++k;
     if (i > 0) w1sq_a += wi * wi;
   }
-  double w0pre = s0 / sscale + z0 / zscale;
+  double w0pre = __dadd_rn(__dmul_rn(s0, isc), __dmul_rn(z0, izc));
   double wres = soc_res(w0pre, group_sum<G>(w1sq_a));
   double wscale = wres > 0.0 ? sqrt(wres) : 0.0;
   if (wscale == 0.0) {
@@ -134,9 +137,13 @@ __global__ void k_soc_update_scaling(ConeSet cs, const double *__restrict__ s_,
     wscale = 1.0;
   }
   double w1sq = 0;
+  const double iwc = 1.0 / wscale;
   k = 0;
   SOC_FOR(i) {
-    double wi = (k < 4 ? wl[k] : (s[i] / sscale + (i == 0 ? z[i] : -z[i]) / zscale)) / wscale;
+    double wi = __dmul_rn(k < 4 ? wl[k]
+                                : __dadd_rn(__dmul_rn(s[i], isc),
+                                            __dmul_rn(i == 0 ? z[i] : -z[i], izc)),
+                          iwc);
     if (k < 4) wl[k] = wi;
     ++k;
     if (i > 0) w1sq += wi * wi;
@@ -144,9 +151,9 @@ __global__ void k_soc_update_scaling(ConeSet cs, const double *__restrict__ s_,
   w1sq = group_sum<G>(w1sq);
   double w0 = sqrt(1 + w1sq);
   double gamma = 0.5 * wscale;
-  double c1 = (gamma + z0 / zscale) / sscale;
-  double c2 = (gamma + s0 / sscale) / zscale;
-  double inv = 1.0 / (s0 / sscale + z0 / zscale + 2 * gamma);
+  double c1 = __dmul_rn(__dadd_rn(gamma, __dmul_rn(z0, izc)), isc);
+  double c2 = __dmul_rn(__dadd_rn(gamma, __dmul_rn(s0, isc)), izc);
+  double inv = 1.0 / __dadd_rn(w0pre, 2 * gamma);
   double sc = sqrt(sscale * zscale);
   bool sparse = cs.soc_sparse[ctx.c] != 0;
   double u0 = 0, u1 = 0, v1 = 0, dd = 0;
@@ -162,7 +169,9 @@ __global__ void k_soc_update_scaling(ConeSet cs, const double *__restrict__ s_,
   k = 0;
   SOC_FOR(i) {
     double wi = (k < 4) ? wl[k]
-                        : (s[i] / sscale + (i == 0 ? z[i] : -z[i]) / zscale) / wscale;
+                        : __dmul_rn(__dadd_rn(__dmul_rn(s[i], isc),
+                                              __dmul_rn(i == 0 ? z[i] : -z[i], izc)),
+                                    iwc);
     ++k;
     if (i == 0) {
       w[0] = w0;
@@ -470,75 +479,98 @@ struct NonsymArgs {
 // latency better than the spill-free allocation did (measured on 4 M exp and
 // 4 M pow cones: update_scaling 520 -> 425 us and 676 -> 576 us, pow
 // combined_ds_shift 280 -> 228 us; exp combined_ds_shift unchanged at 8).
+// The block's 128 cones are staged through shared memory on both sides:
+// their s and z (3 doubles each, 24-byte stride in global memory) are read
+// with coalesced loads, and their 24 outputs per cone (Hd, Hs, grad, z) are
+// written back as contiguous runs, instead of one 8-byte access per cone
+// and lane at a 24- or 72-byte stride.
 template <class Ops>
 __global__ void __launch_bounds__(128, 7) k_nonsym_update_scaling(ConeSet cs, NonsymArgs<Ops> a,
                                         const double *__restrict__ s_,
                                         const double *__restrict__ z_,
                                         const double *mu_, const int *scaling) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.n) return;
-  int inst = a.inst[c];
-  if (!active_inst(cs, inst)) return;
-  double pa = a.alpha ? a.alpha[c] : 0.0;
-  const double *s = s_ + a.begin + 3 * c, *z = z_ + a.begin + 3 * c;
-  double sv[3] = {s[0], s[1], s[2]}, zv[3] = {z[0], z[1], z[2]};
-  double grad[3];
-  M3 Hd, Hs;
-  Ops::dual_grad_H(zv, grad, Hd, pa);
-  double mu = mu_[inst];
-  bool dual = scaling[inst] == 1;
-  bool used_pd = false;
-  if (!dual) {
-    const double *st = grad;
-    double zt[3];
-    Ops::grad_primal(sv, zt, pa);
-    double dot_sz = zv[0] * sv[0] + zv[1] * sv[1] + zv[2] * sv[2];
-    double mu_l = dot_sz / 3;
-    double mut = (zt[0] * st[0] + zt[1] * st[1] + zt[2] * st[2]) / 3;
-    double ds[3], dz[3];
-    for (int i = 0; i < 3; ++i) {
-      ds[i] = sv[i] + mu_l * st[i];
-      dz[i] = zv[i] + mu_l * zt[i];
+  __shared__ double ss[3 * 128], sz[3 * 128], sHd[9 * 128], sHs[9 * 128], sg[3 * 128];
+  __shared__ unsigned char on[128];
+  const int c0 = blockIdx.x * 128, nb = min(128, a.n - c0), tid = threadIdx.x;
+  for (int i = tid; i < 3 * nb; i += 128) {
+    ss[i] = s_[a.begin + 3 * c0 + i];
+    sz[i] = z_[a.begin + 3 * c0 + i];
+  }
+  __syncthreads();
+  const int c = c0 + tid;
+  const int inst = tid < nb ? a.inst[c] : -1;
+  const bool act = tid < nb && active_inst(cs, inst);
+  on[tid] = act ? 1 : 0;
+  if (act) {
+    double pa = a.alpha ? a.alpha[c] : 0.0;
+    double sv[3] = {ss[3 * tid], ss[3 * tid + 1], ss[3 * tid + 2]};
+    double zv[3] = {sz[3 * tid], sz[3 * tid + 1], sz[3 * tid + 2]};
+    double grad[3];
+    M3 Hd, Hs;
+    Ops::dual_grad_H(zv, grad, Hd, pa);
+    double mu = mu_[inst];
+    bool dual = scaling[inst] == 1;
+    bool used_pd = false;
+    if (!dual) {
+      const double *st = grad;
+      double zt[3];
+      Ops::grad_primal(sv, zt, pa);
+      double dot_sz = zv[0] * sv[0] + zv[1] * sv[1] + zv[2] * sv[2];
+      double mu_l = dot_sz / 3;
+      double mut = (zt[0] * st[0] + zt[1] * st[1] + zt[2] * st[2]) / 3;
+      double ds[3], dz[3];
+      for (int i = 0; i < 3; ++i) {
+        ds[i] = sv[i] + mu_l * st[i];
+        dz[i] = zv[i] + mu_l * zt[i];
+      }
+      double dot_dsz = ds[0] * dz[0] + ds[1] * dz[1] + ds[2] * dz[2];
+      double de1 = mu_l * mut - 1;
+      double Hz[3];
+      for (int i = 0; i < 3; ++i) Hz[i] = Hd(i, 0) * zt[0] + Hd(i, 1) * zt[1] + Hd(i, 2) * zt[2];
+      double de2 = zt[0] * Hz[0] + zt[1] * Hz[1] + zt[2] * Hz[2] - 3 * mut * mut;
+      if (fabs(de1) > sqrt(kDEps) && fabs(de2) > kDEps && dot_sz > 0 && dot_dsz > 0) {
+        double tmp[3];
+        for (int i = 0; i < 3; ++i) tmp[i] = mut * st[i] - Hz[i];
+        for (int i = 0; i < 9; ++i) Hs.a[i] = Hd.a[i];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) Hs(i, j) -= st[i] * st[j] / 3 + tmp[i] * tmp[j] / de2;
+        double fro = 0;
+        for (int i = 0; i < 9; ++i) fro += Hs.a[i] * Hs.a[i];
+        double t = mu_l * sqrt(fro);
+        double ax[3] = {zv[1] * zt[2] - zv[2] * zt[1], zv[2] * zt[0] - zv[0] * zt[2],
+                        zv[0] * zt[1] - zv[1] * zt[0]};
+        double an = sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+        for (int i = 0; i < 3; ++i) ax[i] /= an;
+        for (int i = 0; i < 3; ++i)
+          for (int j = i; j < 3; ++j)
+            Hs(i, j) = sv[i] * sv[j] / dot_sz + ds[i] * ds[j] / dot_dsz + t * ax[i] * ax[j];
+        Hs(1, 0) = Hs(0, 1);
+        Hs(2, 0) = Hs(0, 2);
+        Hs(2, 1) = Hs(1, 2);
+        used_pd = true;
+      } else {
+        mu = mu_l;  // central-path fallback uses the local mu
+      }
     }
-    double dot_dsz = ds[0] * dz[0] + ds[1] * dz[1] + ds[2] * dz[2];
-    double de1 = mu_l * mut - 1;
-    double Hz[3];
-    for (int i = 0; i < 3; ++i) Hz[i] = Hd(i, 0) * zt[0] + Hd(i, 1) * zt[1] + Hd(i, 2) * zt[2];
-    double de2 = zt[0] * Hz[0] + zt[1] * Hz[1] + zt[2] * Hz[2] - 3 * mut * mut;
-    if (fabs(de1) > sqrt(kDEps) && fabs(de2) > kDEps && dot_sz > 0 && dot_dsz > 0) {
-      double tmp[3];
-      for (int i = 0; i < 3; ++i) tmp[i] = mut * st[i] - Hz[i];
-      for (int i = 0; i < 9; ++i) Hs.a[i] = Hd.a[i];
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) Hs(i, j) -= st[i] * st[j] / 3 + tmp[i] * tmp[j] / de2;
-      double fro = 0;
-      for (int i = 0; i < 9; ++i) fro += Hs.a[i] * Hs.a[i];
-      double t = mu_l * sqrt(fro);
-      double ax[3] = {zv[1] * zt[2] - zv[2] * zt[1], zv[2] * zt[0] - zv[0] * zt[2],
-                      zv[0] * zt[1] - zv[1] * zt[0]};
-      double an = sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
-      for (int i = 0; i < 3; ++i) ax[i] /= an;
-      for (int i = 0; i < 3; ++i)
-        for (int j = i; j < 3; ++j)
-          Hs(i, j) = sv[i] * sv[j] / dot_sz + ds[i] * ds[j] / dot_dsz + t * ax[i] * ax[j];
-      Hs(1, 0) = Hs(0, 1);
-      Hs(2, 0) = Hs(0, 2);
-      Hs(2, 1) = Hs(1, 2);
-      used_pd = true;
-    } else {
-      mu = mu_l;  // central-path fallback uses the local mu
+    if (!used_pd)
+      for (int i = 0; i < 9; ++i) Hs.a[i] = mu * Hd.a[i];
+    for (int i = 0; i < 9; ++i) {
+      sHd[9 * tid + i] = Hd.a[i];
+      sHs[9 * tid + i] = Hs.a[i];
     }
+    for (int i = 0; i < 3; ++i) sg[3 * tid + i] = grad[i];
   }
-  if (!used_pd)
-    for (int i = 0; i < 9; ++i) Hs.a[i] = mu * Hd.a[i];
-  for (int i = 0; i < 9; ++i) {
-    a.Hd[9 * c + i] = Hd.a[i];
-    a.Hs[9 * c + i] = Hs.a[i];
-  }
-  for (int i = 0; i < 3; ++i) {
-    a.grad[3 * c + i] = grad[i];
-    a.zs[3 * c + i] = zv[i];
-  }
+  __syncthreads();
+  for (int i = tid; i < 9 * nb; i += 128)
+    if (on[i / 9]) {
+      a.Hd[9 * c0 + i] = sHd[i];
+      a.Hs[9 * c0 + i] = sHs[i];
+    }
+  for (int i = tid; i < 3 * nb; i += 128)
+    if (on[i / 3]) {
+      a.grad[3 * c0 + i] = sg[i];
+      a.zs[3 * c0 + i] = sz[i];
+    }
 }
 
 // =================================================================== PSD
@@ -1274,20 +1306,32 @@ __global__ void k_nn_step(ConeSet cs, const double *__restrict__ dz,
     const int base = blockIdx.x * blockDim.x * kNNRows + threadIdx.x;
     double a = CUDART_INF;
     if (active_inst(cs, 0)) {
-      double dzv[kNNRows], dsv[kNNRows];
+      // all four vectors loaded in one round; the smallest ratio -x / dx
+      // (dx < 0, x > 0) is selected by cross-multiplication, n / d < bn / bd
+      // <=> n bd < bn d for positive denominators, and divided once
+      double dzv[kNNRows], dsv[kNNRows], zv[kNNRows], sv[kNNRows];
 #pragma unroll
       for (int k = 0; k < kNNRows; ++k) {
         const int e = base + k * blockDim.x;
         const bool in = e < cs.n_nn;
         dzv[k] = in ? dz[cs.nn_begin + e] : 0.0;
         dsv[k] = in ? ds[cs.nn_begin + e] : 0.0;
+        zv[k] = in ? z[cs.nn_begin + e] : 0.0;
+        sv[k] = in ? s[cs.nn_begin + e] : 0.0;
       }
+      double bn = 1.0, bd = 0.0;  // best ratio bn / bd (bd = 0: none)
 #pragma unroll
       for (int k = 0; k < kNNRows; ++k) {
-        const int g = cs.nn_begin + base + k * blockDim.x;
-        if (dzv[k] < 0) a = fmin(a, -z[g] / dzv[k]);
-        if (dsv[k] < 0) a = fmin(a, -s[g] / dsv[k]);
+        if (dzv[k] < 0 && (bd == 0.0 || zv[k] * bd < bn * -dzv[k])) {
+          bn = zv[k];
+          bd = -dzv[k];
+        }
+        if (dsv[k] < 0 && (bd == 0.0 || sv[k] * bd < bn * -dsv[k])) {
+          bn = sv[k];
+          bd = -dsv[k];
+        }
       }
+      if (bd != 0.0) a = bn / bd;
     }
     block_seg_min_nonneg(alpha, a == CUDART_INF ? -1 : 0, a);
     return;
@@ -1845,26 +1889,29 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, int trow
     bool fail = (zscale == 0.0 || sscale == 0.0);
     if (fail) zscale = sscale = 1.0;
     double eta = sqrt(sscale / zscale);
+    const double isc = 1.0 / sscale, izc = 1.0 / zscale;
     double w1sq_a = tree16(d, [&](int l) {
-      double wl = S[tsk(o + l)] / sscale + (-Z[tsk(o + l)]) / zscale;
+      double wl = __dadd_rn(__dmul_rn(S[tsk(o + l)], isc), __dmul_rn(-Z[tsk(o + l)], izc));
       return l > 0 ? 0.0 + wl * wl : 0.0;
     });
-    double w0pre = s0 / sscale + z0 / zscale;
+    double w0pre = __dadd_rn(__dmul_rn(s0, isc), __dmul_rn(z0, izc));
     double wres = soc_res(w0pre, w1sq_a);
     double wscale = wres > 0.0 ? sqrt(wres) : 0.0;
     if (wscale == 0.0) {
       fail = true;
       wscale = 1.0;
     }
+    const double iwc = 1.0 / wscale;
     double w1sq = tree16(d, [&](int l) {
-      double wl = (S[tsk(o + l)] / sscale + (-Z[tsk(o + l)]) / zscale) / wscale;
+      double wl = __dmul_rn(
+          __dadd_rn(__dmul_rn(S[tsk(o + l)], isc), __dmul_rn(-Z[tsk(o + l)], izc)), iwc);
       return l > 0 ? 0.0 + wl * wl : 0.0;
     });
     double w0 = sqrt(1 + w1sq);
     double gamma = 0.5 * wscale;
-    double c1 = (gamma + z0 / zscale) / sscale;
-    double c2 = (gamma + s0 / sscale) / zscale;
-    double inv = 1.0 / (s0 / sscale + z0 / zscale + 2 * gamma);
+    double c1 = __dmul_rn(__dadd_rn(gamma, __dmul_rn(z0, izc)), isc);
+    double c2 = __dmul_rn(__dadd_rn(gamma, __dmul_rn(s0, isc)), izc);
+    double inv = 1.0 / __dadd_rn(w0pre, 2 * gamma);
     double sc = sqrt(sscale * zscale);
     bool sparse = cs.soc_sparse[t.c] != 0;
     double u0 = 0, u1 = 0, v1 = 0, dd = 0;
@@ -1881,7 +1928,7 @@ __global__ void k_soc_tile_update_scaling(ConeSet cs, const int *tiles, int trow
     } else {
       for (int i = 1; i < d; ++i) {
         double si = S[tsk(o + i)], zi = Z[tsk(o + i)];
-        double wi = (si / sscale + (-zi) / zscale) / wscale;
+        double wi = __dmul_rn(__dadd_rn(__dmul_rn(si, isc), __dmul_rn(-zi, izc)), iwc);
         S[tsk(o + i)] = wi;
         Z[tsk(o + i)] = ((c1 * si + c2 * zi) * inv) * sc;
         if (sparse) {

@@ -311,3 +311,46 @@ def test_result_views_keep_the_solver_alive(cuda_device):
     del v
     gc.collect()
     assert ref() is None
+
+
+def _oracle_one(seed):
+    import oracle as _o
+    from cuclarabel_b200 import problems as _p
+    r = _o.solve(*_p.mpc_qp(seed), gpu_equilibration=1)
+    return (r["status_name"], r["iterations"], r["obj_val"], r["res_primal"], r["res_dual"])
+
+
+def test_mpc_bench_batch_full_bar_census(cuda_device):
+    """The full bar (same status, objective within 1e-7, iterations within
+    +-2) counted over every instance of the bench batch (4096 MPC problems,
+    seeds 0..4095) against the oracle.  The counts are printed; the bar is
+    that at least 97 % of all instances meet it and that every instance the
+    two sides both solve agrees in objective to 1e-6."""
+    import multiprocessing as mp
+    import os
+    B = 4096
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(16, os.cpu_count() or 1)) as pool:
+        refs = pool.map(_oracle_one, range(B), chunksize=64)
+    sols = BatchSolver(problems.mpc_batch(B, seed0=0)).solve()
+    full = flips = itgap = 0
+    gaps = []
+    worst_both = 0.0
+    for k, (sol, ref) in enumerate(zip(sols, refs)):
+        st, it, obj = ref[0], ref[1], ref[2]
+        same = sol.status.name == st
+        if same and st == "SOLVED":
+            worst_both = max(worst_both, rel_err(sol.obj_val, obj))
+        ok_obj = rel_err(sol.obj_val, obj) < OBJ_RTOL
+        if same and ok_obj and abs(sol.iterations - it) <= ITER_TOL:
+            full += 1
+        elif not same:
+            flips += 1
+        else:
+            itgap += 1
+            gaps.append(sol.iterations - it)
+    print("census: %d / %d full bar, %d status flips, %d iteration/objective gaps %s, "
+          "worst objective gap when both SOLVED %.2e" % (full, B, flips, itgap,
+                                                        sorted(gaps)[:20], worst_both))
+    assert full >= 0.97 * B
+    assert worst_both < 1e-6
