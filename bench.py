@@ -662,9 +662,14 @@ def serve_config5(pbs, lam, seconds, seed, method, budget_gb, new_frac, large_fr
                                    direct_solve_method=method)
     large = serving.SlotLane.build("resident config-2-like", large_pbs, streams[1].cuda_stream,
                                    budget, direct_solve_method=method)
+    # cohorts are set up while the other lanes run: no launch-shape timing
+    # (its L2 flushes and timed launches would disturb them)
     cohort = serving.CohortLane("new-structure MPC", streams[2].cuda_stream, budget,
                                 bytes_per_nnz=small.bytes / max(small.kkt_nnz, 1),
-                                direct_solve_method=method)
+                                direct_solve_method=method, autotune=False)
+    small.warm(0)
+    large.warm(0)  # the smallest configuration-2-like structure
+    torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
     jobs = [(small, (arrive[idx[0]], which[idx[0]], [qv[r] for r in idx[0]],
                      [bv[r] for r in idx[0]])),

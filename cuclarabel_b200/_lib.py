@@ -45,6 +45,7 @@ class ClgpuSettings(ctypes.Structure):
         ("iterative_refinement_stop_ratio", c_double),
         ("direct_solve_method", c_int), ("soc_threshold", c_int), ("verbose", c_int),
         ("setup_threads", c_int), ("fused_solves", c_int), ("device_setup", c_int),
+        ("autotune", c_int),
     ]
 
 

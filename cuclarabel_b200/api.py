@@ -182,6 +182,7 @@ class Settings:
     setup_threads: int = 0
     fused_solves: bool = True
     device_setup: bool = True
+    autotune: bool = True
 
     def to_c(self):
         if self.direct_solve_method not in _METHODS:

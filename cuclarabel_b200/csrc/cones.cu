@@ -661,7 +661,10 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
         a = warp_sum(a);
         b = warp_sum(b);
         g = warp_sum(g);
-        if (fabs(g) <= 1e-15 * sqrt(a * b) || g == 0) continue;
+        // columns orthogonal to 1e-14 of their norms: the rounding noise of
+        // the dot products of n <= 48 rows sits near n^(1/2) eps, so a
+        // tighter bound keeps rotating at noise level until the sweep cap
+        if (fabs(g) <= 1e-14 * sqrt(a * b) || g == 0) continue;
         rotated = 1;
         double zeta = (b - a) / (2 * g);
         double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
@@ -734,7 +737,12 @@ __device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
     }
     off = warp_sum(off);
     tot = warp_sum(tot);
-    if (off <= 1e-30 * tot || off == 0) break;
+    // converged when the off-diagonal part is below 1e-13 of the matrix
+    // (Frobenius norms): every eigenvalue is then within 1e-13 |A|_F of a
+    // diagonal entry.  (A tighter relative bound sits at the rounding
+    // noise of the rotations and is never reached, so the sweeps ran to
+    // their cap.)
+    if (off <= 1e-26 * tot || off == 0) break;
     // threshold Jacobi: a rotation whose effect on the diagonal is below
     // the rounding of its entries (apq^2 <= 2^-106 |app aqq|) or of the
     // matrix (apq^2 <= 1e-30 |A|_F^2 / n^2) is skipped; a sweep without a

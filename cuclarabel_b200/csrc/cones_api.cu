@@ -222,6 +222,13 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
     delete h;
     return rc;
   }
+  // the arena's zero fills run on the legacy stream: finished before any
+  // stream of the caller's can read the handle's state
+  cudaError_t se = cudaStreamSynchronize(0);
+  if (se != cudaSuccess) {
+    delete h;
+    return -1000 - (int)se;
+  }
   *out = h;
   return 0;
 }

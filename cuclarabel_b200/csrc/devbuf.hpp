@@ -32,21 +32,43 @@ struct DefaultInitAlloc : std::allocator<T> {
 template <class T>
 using hvec = std::vector<T, DefaultInitAlloc<T>>;
 
+// Where the device has memory pools, allocations come from the
+// stream-ordered pool on the legacy stream (cudaMallocAsync) and go back
+// with cudaFreeAsync, which does not synchronise the device: a solver can
+// be set up and destroyed while other solvers run on their own streams
+// (serving).  The owner must have no work of its own pending on another
+// stream when it releases (every solver entry point that launches work
+// finishes it or leaves it to a stream the caller synchronises before
+// destroying).  Plain cudaMalloc / cudaFree otherwise.
+inline bool arena_pool_alloc() {
+  static const bool on = [] {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMemoryPoolsSupported, dev) != cudaSuccess)
+      return false;
+    return v != 0;
+  }();
+  return on;
+}
+
 struct DevArena {
   std::vector<void *> ptrs;
   long long bytes = 0;
   cudaError_t err = cudaSuccess;
-  // zero-filled unless the caller overwrites it at once (upload)
+  bool pooled = arena_pool_alloc();
+  // zero-filled unless the caller overwrites it at once (upload); ordered
+  // on the legacy stream, which the setup synchronises before returning
   template <typename T>
   T *alloc(size_t count, bool zero = true) {
     if (count == 0) count = 1;
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    cudaError_t e = pooled ? cudaMallocAsync(&p, count * sizeof(T), 0)
+                           : cudaMalloc(&p, count * sizeof(T));
     if (e != cudaSuccess) {
       err = e;
       return nullptr;
     }
-    if (zero) cudaMemset(p, 0, count * sizeof(T));
+    if (zero) cudaMemsetAsync(p, 0, count * sizeof(T), 0);
     ptrs.push_back(p);
     bytes += (long long)(count * sizeof(T));
     return static_cast<T *>(p);
@@ -61,7 +83,12 @@ struct DevArena {
     return p;
   }
   void release() {
-    for (void *p : ptrs) cudaFree(p);
+    for (void *p : ptrs) {
+      if (pooled)
+        cudaFreeAsync(p, 0);
+      else
+        cudaFree(p);
+    }
     ptrs.clear();
     bytes = 0;
   }

@@ -1001,6 +1001,7 @@ extern "C" int clgpu_default_settings(clgpu_settings *s) {
   s->setup_threads = 0;
   s->fused_solves = 1;
   s->device_setup = 1;
+  s->autotune = 1;
   return 0;
 }
 
@@ -2057,7 +2058,9 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       if (A.err != cudaSuccess) return -5;
       equilibrate_on_device(q, ep, h->d_upd_pmap, h->d_upd_pxy, h->upd_np, h->d_upd_amap,
                             h->d_upd_axy, h->upd_na, h->kk.Kx, 0);
-      cudaError_t e = cudaDeviceSynchronize();
+      // setup runs on the legacy stream: waiting for it (not for the whole
+      // device) leaves other solvers' streams running
+      cudaError_t e = cudaStreamSynchronize(0);
       if (e == cudaSuccess) e = cudaGetLastError();
       if (e != cudaSuccess) return -1000 - (int)e;
     }
@@ -2105,7 +2108,8 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   h->slot_state.assign(B, 0);
   h->slot_t0.assign(B, std::chrono::steady_clock::now());
   if (A.err != cudaSuccess) return -1000 - (int)A.err;
-  cudaError_t e = cudaDeviceSynchronize();
+  cudaError_t e = cudaStreamSynchronize(0);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return -1000 - (int)e;
   mark("scratch + tail");
   return 0;
@@ -2177,7 +2181,7 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
   h->sd = make_sd(h->st);
   h->info.assign(nprob, clgpu_info{});
   // launch shapes of the nonnegative and SOC kernels, timed on this batch
-  rc = cones_autotune(h->cs, 0);
+  rc = h->st.autotune ? cones_autotune(h->cs, 0) : 0;
   if (rc != 0) {
     delete h;
     return rc;

@@ -140,6 +140,9 @@ extern "C" int clgpu_ldl_create(int N, const int *Kp, const int *Kj, const signe
   if (!sn_exec_create(plan, mixed, 1, 0, N, vinst, A, *h->sn)) return cuda_status(A.err ? A.err : cudaErrorMemoryAllocation);
   k.sn = h->sn.get();
   if (A.err != cudaSuccess) return cuda_status(A.err);
+  // the arena's zero fills run on the legacy stream: finished before any
+  // stream of the caller's uses the handle
+  if (cudaError_t se = cudaStreamSynchronize(0)) return cuda_status(se);
   LDLParams &lp = h->lp;
   lp.static_reg = st.static_regularization_enable;
   lp.static_c = st.static_regularization_constant;

@@ -108,6 +108,19 @@ class SlotLane:
         return cls(name, BatchSolver(problems, **settings), stream, budget,
                    sum(_kkt_nnz(pb) for pb in problems))
 
+    def warm(self, slot=0):
+        """Serve one request for `slot` to completion before the clock
+        starts: the first step of a solver captures its IPM pass (and, on
+        the supernodal path, its substitution pass) as CUDA graphs, and no
+        other thread may allocate device memory while a capture is open."""
+        s = self.solver
+        s.serve_admit([slot], stream=self.stream)
+        running = 1
+        while running:
+            fin, running = s.serve_step(self.stream)
+            if fin:
+                s.serve_collect(fin, self.stream)
+
     def close(self):
         if self.solver is not None:
             del self.solver

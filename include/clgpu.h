@@ -81,6 +81,10 @@ typedef struct {
                               result); 0: on the host.  Problems whose
                               matrices hold repeated or unsorted entries are
                               equilibrated on the host either way. */
+  int autotune;            /* 1: time the SOC / NN launch shapes at setup and
+                              keep the fastest (every shape gives the same
+                              bits); 0: default shapes, no timing launches
+                              (for solvers set up while others run) */
 } clgpu_settings;
 
 /* mirrors DefaultInfo (src/types.jl:227-255) plus solution scalars */

@@ -151,3 +151,11 @@ def test_cone_roofline_points_are_interior():
         M[ii[order], jj[order]] = vals
         M = M + np.triu(M, 1).T
         assert np.linalg.eigvalsh(M).min() > 0
+
+
+def test_slot_lane_warm_serves_one_request_outside_the_stats():
+    from cuclarabel_b200 import serving
+    fake = FakeSlots({0: 2, 1: 3})
+    lane = serving.SlotLane("fake", fake, 0, serving.Budget(10_000))
+    lane.warm(1)
+    assert fake.admitted == [1] and not fake.left and lane.stats.lat == []
