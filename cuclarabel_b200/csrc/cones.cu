@@ -574,16 +574,35 @@ __global__ void __launch_bounds__(128, 7) k_nonsym_update_scaling(ConeSet cs, No
 }
 
 // =================================================================== PSD
-// Warp-per-cone helpers on column-major n x n matrices in shared memory.
+// Group-per-cone helpers on column-major n x n matrices in shared memory.
+// A cone is handled by a group of G lanes of one warp: G = 16 when every
+// PSD side of the set is at most 16 (two cones per warp), else G = 32.
+// Groups of one warp run independently (their own loop trip counts), so
+// every barrier and shuffle names the group's lanes only.
+struct PsdGrp {
+  int lane, G;
+  unsigned mask;
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  __device__ __forceinline__ double sum(double v) const {
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+  }
+  __device__ __forceinline__ double min(double v) const {
+    for (int o = G / 2; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(mask, v, o));
+    return v;
+  }
+};
+__host__ __device__ __forceinline__ int psd_group(int nmax) { return nmax <= 16 ? 16 : 32; }
 struct PsdCtx {
   int c, lane, n, t, off, inst;
+  PsdGrp g;
   bool valid;
 };
 
-__device__ __forceinline__ void svec_to_mat(int n, const double *x, double *M, int lane) {
+__device__ __forceinline__ void svec_to_mat(int n, const double *x, double *M, const PsdGrp &g) {
   const double is2 = 0.70710678118654752440;  // 1/sqrt(2)
   int t = n * (n + 1) / 2;
-  for (int k = lane; k < t; k += 32) {
+  for (int k = g.lane; k < t; k += g.G) {
     int col = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
     while ((col + 1) * (col + 2) / 2 <= k) ++col;
     while (col * (col + 1) / 2 > k) --col;
@@ -597,10 +616,10 @@ __device__ __forceinline__ void svec_to_mat(int n, const double *x, double *M, i
     }
   }
 }
-__device__ __forceinline__ void mat_to_svec(int n, const double *M, double *x, int lane) {
+__device__ __forceinline__ void mat_to_svec(int n, const double *M, double *x, const PsdGrp &g) {
   const double is2 = 0.70710678118654752440;
   int t = n * (n + 1) / 2;
-  for (int k = lane; k < t; k += 32) {
+  for (int k = g.lane; k < t; k += g.G) {
     int col = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
     while ((col + 1) * (col + 2) / 2 <= k) ++col;
     while (col * (col + 1) / 2 > k) --col;
@@ -610,8 +629,8 @@ __device__ __forceinline__ void mat_to_svec(int n, const double *M, double *x, i
 }
 // C = op(A) * op(B)   (n x n), ta/tb: transpose flags
 __device__ void mm(int n, const double *A, bool ta, const double *B, bool tb, double *C,
-                   int lane) {
-  for (int e = lane; e < n * n; e += 32) {
+                   const PsdGrp &g) {
+  for (int e = g.lane; e < n * n; e += g.G) {
     int i = e % n, j = e / n;
     double t = 0;
     for (int k = 0; k < n; ++k) {
@@ -621,55 +640,55 @@ __device__ void mm(int n, const double *A, bool ta, const double *B, bool tb, do
     }
     C[e] = t;
   }
-  __syncwarp();
+  g.sync();
 }
 // in-place lower Cholesky; returns false if not positive definite
-__device__ bool warp_chol(int n, double *A, int lane) {
+__device__ bool warp_chol(int n, double *A, const PsdGrp &g) {
   bool ok = true;
   for (int j = 0; j < n; ++j) {
     double d = A[j + n * j];
     for (int k = 0; k < j; ++k) d -= A[j + n * k] * A[j + n * k];
     if (!(d > 0)) ok = false;
     d = ok ? sqrt(d) : 1.0;
-    __syncwarp();
-    for (int i = j + 1 + lane; i < n; i += 32) {
+    g.sync();
+    for (int i = j + 1 + g.lane; i < n; i += g.G) {
       double t = A[i + n * j];
       for (int k = 0; k < j; ++k) t -= A[i + n * k] * A[j + n * k];
       A[i + n * j] = t / d;
     }
-    if (lane == 0) A[j + n * j] = d;
-    for (int i = lane; i < j; i += 32) A[i + n * j] = 0;
-    __syncwarp();
+    if (g.lane == 0) A[j + n * j] = d;
+    for (int i = g.lane; i < j; i += g.G) A[i + n * j] = 0;
+    g.sync();
   }
   return ok;
 }
 // one-sided Jacobi SVD: M = U diag(S) V^T; S descending.  M overwritten by U.
-__device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, int lane) {
-  for (int e = lane; e < n * n; e += 32) V[e] = (e % n == e / n) ? 1.0 : 0.0;
-  __syncwarp();
+__device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, const PsdGrp &g) {
+  for (int e = g.lane; e < n * n; e += g.G) V[e] = (e % n == e / n) ? 1.0 : 0.0;
+  g.sync();
   for (int sweep = 0; sweep < 60; ++sweep) {
     int rotated = 0;
     for (int p = 0; p < n; ++p)
       for (int q = p + 1; q < n; ++q) {
-        double a = 0, b = 0, g = 0;
-        for (int r = lane; r < n; r += 32) {
+        double a = 0, b = 0, gd = 0;
+        for (int r = g.lane; r < n; r += g.G) {
           double mp = M[r + n * p], mq = M[r + n * q];
           a += mp * mp;
           b += mq * mq;
-          g += mp * mq;
+          gd += mp * mq;
         }
-        a = warp_sum(a);
-        b = warp_sum(b);
-        g = warp_sum(g);
+        a = g.sum(a);
+        b = g.sum(b);
+        gd = g.sum(gd);
         // columns orthogonal to 1e-14 of their norms: the rounding noise of
         // the dot products of n <= 48 rows sits near n^(1/2) eps, so a
         // tighter bound keeps rotating at noise level until the sweep cap
-        if (fabs(g) <= 1e-14 * sqrt(a * b) || g == 0) continue;
+        if (fabs(gd) <= 1e-14 * sqrt(a * b) || gd == 0) continue;
         rotated = 1;
-        double zeta = (b - a) / (2 * g);
+        double zeta = (b - a) / (2 * gd);
         double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
         double cs = 1 / sqrt(1 + t * t), sn = cs * t;
-        for (int r = lane; r < n; r += 32) {
+        for (int r = g.lane; r < n; r += g.G) {
           double mp = M[r + n * p], mq = M[r + n * q];
           M[r + n * p] = cs * mp - sn * mq;
           M[r + n * q] = sn * mp + cs * mq;
@@ -677,19 +696,19 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
           V[r + n * p] = cs * vp - sn * vq;
           V[r + n * q] = sn * vp + cs * vq;
         }
-        __syncwarp();
+        g.sync();
       }
     if (!rotated) break;
   }
-  // column norms, sort descending (selection on lane 0 into tmp perm)
-  for (int c = lane; c < n; c += 32) {
+  // column norms, sort descending (selection on the group's lane 0 into tmp perm)
+  for (int c = g.lane; c < n; c += g.G) {
     double t = 0;
     for (int k = 0; k < n; ++k) t += M[k + n * c] * M[k + n * c];
     S[c] = sqrt(t);
   }
-  __syncwarp();
+  g.sync();
   int *perm = reinterpret_cast<int *>(tmp + n * n);
-  if (lane == 0) {
+  if (g.lane == 0) {
     for (int i = 0; i < n; ++i) perm[i] = i;
     for (int i = 0; i < n; ++i)
       for (int j = i + 1; j < n; ++j)
@@ -699,44 +718,44 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, in
           perm[j] = x;
         }
   }
-  __syncwarp();
+  g.sync();
   // tmp <- U (sorted), M <- V (sorted) via copies
-  for (int e = lane; e < n * n; e += 32) {
+  for (int e = g.lane; e < n * n; e += g.G) {
     int i = e % n, j = e / n, pj = perm[j];
     double sj = S[pj];
     tmp[e] = sj > 0 ? M[i + n * pj] / sj : 0.0;
   }
-  __syncwarp();
-  for (int e = lane; e < n * n; e += 32) M[e] = tmp[e];
-  __syncwarp();
-  for (int e = lane; e < n * n; e += 32) {
+  g.sync();
+  for (int e = g.lane; e < n * n; e += g.G) M[e] = tmp[e];
+  g.sync();
+  for (int e = g.lane; e < n * n; e += g.G) {
     int i = e % n, j = e / n;
     tmp[e] = V[i + n * perm[j]];
   }
-  constexpr int kRows = (kPsdMaxSide + 31) / 32;  // rows per lane
+  constexpr int kRows = (kPsdMaxSide + 15) / 16;  // rows per lane (G >= 16)
   double sl[kRows];
 #pragma unroll
   for (int r = 0; r < kRows; ++r)
-    sl[r] = lane + 32 * r < n ? S[perm[lane + 32 * r]] : 0.0;
-  __syncwarp();
-  for (int e = lane; e < n * n; e += 32) V[e] = tmp[e];
+    sl[r] = g.lane + g.G * r < n ? S[perm[g.lane + g.G * r]] : 0.0;
+  g.sync();
+  for (int e = g.lane; e < n * n; e += g.G) V[e] = tmp[e];
 #pragma unroll
   for (int r = 0; r < kRows; ++r)
-    if (lane + 32 * r < n) S[lane + 32 * r] = sl[r];
-  __syncwarp();
+    if (g.lane + g.G * r < n) S[g.lane + g.G * r] = sl[r];
+  g.sync();
 }
 // cyclic Jacobi eigenvalues of symmetric A (destroyed); returns min eigenvalue,
 // and if ev != null writes all eigenvalues.
-__device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
+__device__ double warp_eig_min(int n, double *A, double *ev, const PsdGrp &g) {
   for (int sweep = 0; sweep < 60; ++sweep) {
     double off = 0, tot = 0;
-    for (int e = lane; e < n * n; e += 32) {
+    for (int e = g.lane; e < n * n; e += g.G) {
       double a = A[e] * A[e];
       tot += a;
       if (e % n != e / n) off += a;
     }
-    off = warp_sum(off);
-    tot = warp_sum(tot);
+    off = g.sum(off);
+    tot = g.sum(tot);
     // converged when the off-diagonal part is below 1e-13 of the matrix
     // (Frobenius norms): every eigenvalue is then within 1e-13 |A|_F of a
     // diagonal entry.  (A tighter relative bound sits at the rounding
@@ -760,36 +779,40 @@ __device__ double warp_eig_min(int n, double *A, double *ev, int lane) {
         double theta = (aqq - app) / (2 * apq);
         double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
         double c = 1 / sqrt(t * t + 1), s = t * c;
-        __syncwarp();
-        for (int r = lane; r < n; r += 32) {
+        g.sync();
+        for (int r = g.lane; r < n; r += g.G) {
           double akp = A[r + n * p], akq = A[r + n * q];
           A[r + n * p] = c * akp - s * akq;
           A[r + n * q] = s * akp + c * akq;
         }
-        __syncwarp();
-        for (int r = lane; r < n; r += 32) {
+        g.sync();
+        for (int r = g.lane; r < n; r += g.G) {
           double apk = A[p + n * r], aqk = A[q + n * r];
           A[p + n * r] = c * apk - s * aqk;
           A[q + n * r] = s * apk + c * aqk;
         }
-        __syncwarp();
+        g.sync();
       }
     if (!rotated) break;
   }
   double v = CUDART_INF;
-  for (int r = lane; r < n; r += 32) {
+  for (int r = g.lane; r < n; r += g.G) {
     const double a = A[r + n * r];
     v = fmin(v, a);
     if (ev) ev[r] = a;
   }
-  __syncwarp();
-  return warp_min(v);
+  g.sync();
+  return g.min(v);
 }
 
 __device__ __forceinline__ PsdCtx psd_ctx(const ConeSet &cs) {
   PsdCtx p;
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  p.lane = threadIdx.x & 31;
+  const int G = psd_group(cs.psd_nmax);
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  p.lane = threadIdx.x % G;
+  p.g.lane = p.lane;
+  p.g.G = G;
+  p.g.mask = G == 32 ? 0xffffffffu : (0xffffu << (threadIdx.x & 16));
   p.valid = w < cs.n_psd;
   p.c = p.valid ? w : cs.n_psd - 1;
   p.n = cs.psd_n[p.c];
@@ -801,7 +824,7 @@ __device__ __forceinline__ PsdCtx psd_ctx(const ConeSet &cs) {
 }
 __device__ __forceinline__ double *psd_smem(int nmax, int nmats) {
   extern __shared__ double smem[];
-  int wib = threadIdx.x >> 5;
+  int wib = threadIdx.x / psd_group(nmax);  // the group's slice
   return smem + (size_t)wib * nmats * nmax * nmax;
 }
 
@@ -809,27 +832,27 @@ __device__ __forceinline__ double *psd_smem(int nmax, int nmats) {
 __global__ void k_psd_update_scaling(ConeSet cs, const double *__restrict__ s,
                                      const double *__restrict__ z, int *scale_ok) {
   PsdCtx p = psd_ctx(cs);
-  if (!p.valid) return;  // whole warp shares p.valid
+  if (!p.valid) return;  // the whole group shares p.valid
   int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
   double *L1 = psd_smem(nm, 7), *L2 = L1 + nn, *M = L2 + nn, *V = M + nn,
          *T = V + nn, *S = T + 2 * nn;
-  for (int e = p.lane; e < n * n; e += 32) L1[e] = L2[e] = 0;
-  __syncwarp();
-  svec_to_mat(n, s + p.off, L1, p.lane);
-  svec_to_mat(n, z + p.off, L2, p.lane);
-  __syncwarp();
-  bool ok1 = warp_chol(n, L1, p.lane);
-  bool ok2 = warp_chol(n, L2, p.lane);
+  for (int e = p.lane; e < n * n; e += p.g.G) L1[e] = L2[e] = 0;
+  p.g.sync();
+  svec_to_mat(n, s + p.off, L1, p.g);
+  svec_to_mat(n, z + p.off, L2, p.g);
+  p.g.sync();
+  bool ok1 = warp_chol(n, L1, p.g);
+  bool ok2 = warp_chol(n, L2, p.g);
   if (!(ok1 && ok2)) {
     if (p.lane == 0) scale_ok[p.inst] = 0;
     return;
   }
-  mm(n, L2, true, L1, false, M, p.lane);  // M = L2' L1
-  warp_svd(n, M, V, S, T, p.lane);        // M <- U
+  mm(n, L2, true, L1, false, M, p.g);  // M = L2' L1
+  warp_svd(n, M, V, S, T, p.g);        // M <- U
   double *R = cs.psd_R + (size_t)p.c * nn, *Ri = cs.psd_Rinv + (size_t)p.c * nn;
   double *lam = cs.psd_lam + (size_t)p.c * nm;
   // R = L1 V Lis ; Rinv = Lis U' L2'
-  for (int e = p.lane; e < n * n; e += 32) {
+  for (int e = p.lane; e < n * n; e += p.g.G) {
     int i = e % n, j = e / n;
     double t = 0, u = 0;
     for (int k = 0; k < n; ++k) {
@@ -839,18 +862,18 @@ __global__ void k_psd_update_scaling(ConeSet cs, const double *__restrict__ s,
     R[e] = t * (1.0 / sqrt(S[j]));
     Ri[e] = (1.0 / sqrt(S[i])) * u;
   }
-  for (int r = p.lane; r < n; r += 32) lam[r] = S[r];
+  for (int r = p.lane; r < n; r += p.g.G) lam[r] = S[r];
 }
 
 // y = a*op(Rx)... helper: Y = Rx' X Rx (trans=false) or Rx X Rx' (trans=true)
 __device__ void psd_wmul(int n, const double *Rx, bool trans, const double *X, double *Y,
-                         double *T, int lane) {
+                         double *T, const PsdGrp &g) {
   if (trans) {
-    mm(n, X, false, Rx, true, T, lane);   // T = X Rx'
-    mm(n, Rx, false, T, false, Y, lane);  // Y = Rx T
+    mm(n, X, false, Rx, true, T, g);   // T = X Rx'
+    mm(n, Rx, false, T, false, Y, g);  // Y = Rx T
   } else {
-    mm(n, Rx, true, X, false, T, lane);   // T = Rx' X
-    mm(n, T, false, Rx, false, Y, lane);  // Y = T Rx
+    mm(n, Rx, true, X, false, T, g);   // T = Rx' X
+    mm(n, T, false, Rx, false, Y, g);  // Y = T Rx
   }
 }
 
@@ -952,10 +975,10 @@ __global__ void k_psd_refresh(ConeSet cs, KKTMapDev map, double *kv) {
   int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
   double *A = psd_smem(nm, 1);
   const double *R = cs.psd_R + (size_t)p.c * nn;
-  mm(n, R, false, R, true, A, p.lane);  // A = R R'
+  mm(n, R, false, R, true, A, p.g);  // A = R R'
   int tt = p.t * (p.t + 1) / 2;
   const int *pp = map.psd_pos + 2 * (size_t)map.psd_off[p.c];
-  for (int e = p.lane; e < tt; e += 32) {
+  for (int e = p.lane; e < tt; e += p.g.G) {
     int row, col;
     tri_coord(e, row, col);  // svec indices (row <= col)
     int i, j, k, l;
@@ -1011,10 +1034,10 @@ __global__ void k_psd_get_hs(ConeSet cs, const int *blk, double *Hs) {
   int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
   double *A = psd_smem(nm, 1);
   const double *R = cs.psd_R + (size_t)p.c * nn;
-  mm(n, R, false, R, true, A, p.lane);
+  mm(n, R, false, R, true, A, p.g);
   int tt = p.t * (p.t + 1) / 2;
   double *o = Hs + blk[p.c];
-  for (int e = p.lane; e < tt; e += 32) {
+  for (int e = p.lane; e < tt; e += p.g.G) {
     int row, col, i, j, k, l;
     tri_coord(e, row, col);
     tri_coord(row, i, j);
@@ -1072,15 +1095,15 @@ __global__ void k_psd_mul_hs(ConeSet cs, double *y, const double *__restrict__ x
   int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
   double *X = psd_smem(nm, 3), *Y = X + nn, *T = Y + nn;
   const double *R = cs.psd_R + (size_t)p.c * nn;
-  svec_to_mat(n, x + p.off, X, p.lane);
-  __syncwarp();
-  psd_wmul(n, R, false, X, Y, T, p.lane);  // Y = R' X R   (W x)
-  mat_to_svec(n, Y, T, p.lane);            // svec round trip of W x
-  __syncwarp();
-  svec_to_mat(n, T, Y, p.lane);
-  __syncwarp();
-  psd_wmul(n, R, true, Y, X, T, p.lane);   // X = R Y R'   (W^T W x)
-  mat_to_svec(n, X, y + p.off, p.lane);
+  svec_to_mat(n, x + p.off, X, p.g);
+  p.g.sync();
+  psd_wmul(n, R, false, X, Y, T, p.g);  // Y = R' X R   (W x)
+  mat_to_svec(n, Y, T, p.g);            // svec round trip of W x
+  p.g.sync();
+  svec_to_mat(n, T, Y, p.g);
+  p.g.sync();
+  psd_wmul(n, R, true, Y, X, T, p.g);   // X = R Y R'   (W^T W x)
+  mat_to_svec(n, X, y + p.off, p.g);
 }
 
 // ============================================================== affine_ds
@@ -1125,7 +1148,7 @@ __global__ void k_psd_affine_ds(ConeSet cs, double *ds) {
   PsdCtx p = psd_ctx(cs);
   if (!p.valid) return;
   const double *lam = cs.psd_lam + (size_t)p.c * cs.psd_nmax;
-  for (int k = p.lane; k < p.t; k += 32) {
+  for (int k = p.lane; k < p.t; k += p.g.G) {
     int row, col;
     tri_coord(k, row, col);
     ds[p.off + k] = (row == col) ? lam[row] * lam[row] : 0.0;
@@ -1213,35 +1236,35 @@ __global__ void k_psd_combined(ConeSet cs, double *shift, const double *__restri
   int n = p.n, nm = cs.psd_nmax, nn = nm * nm;
   double *X = psd_smem(nm, 5), *Z = X + nn, *S = Z + nn, *T = S + nn, *Y = T + nn;
   const double *R = cs.psd_R + (size_t)p.c * nn, *Ri = cs.psd_Rinv + (size_t)p.c * nn;
-  for (int e = p.lane; e < n * n; e += 32) X[e] = 0;
-  __syncwarp();
-  svec_to_mat(n, dz + p.off, X, p.lane);
-  __syncwarp();
-  psd_wmul(n, R, false, X, Z, T, p.lane);  // Z = R' dZ R   (W dz)
-  svec_to_mat(n, ds + p.off, X, p.lane);
-  __syncwarp();
-  psd_wmul(n, Ri, true, X, S, T, p.lane);  // S = Ri dS Ri'  (W^{-T} ds)
+  for (int e = p.lane; e < n * n; e += p.g.G) X[e] = 0;
+  p.g.sync();
+  svec_to_mat(n, dz + p.off, X, p.g);
+  p.g.sync();
+  psd_wmul(n, R, false, X, Z, T, p.g);  // Z = R' dZ R   (W dz)
+  svec_to_mat(n, ds + p.off, X, p.g);
+  p.g.sync();
+  psd_wmul(n, Ri, true, X, S, T, p.g);  // S = Ri dS Ri'  (W^{-T} ds)
   // svec round trip (the reference stores W dz and W^{-T} ds as svec)
-  mat_to_svec(n, Z, Y, p.lane);
-  __syncwarp();
-  svec_to_mat(n, Y, Z, p.lane);
-  mat_to_svec(n, S, Y, p.lane);
-  __syncwarp();
-  svec_to_mat(n, Y, S, p.lane);
-  __syncwarp();
+  mat_to_svec(n, Z, Y, p.g);
+  p.g.sync();
+  svec_to_mat(n, Y, Z, p.g);
+  mat_to_svec(n, S, Y, p.g);
+  p.g.sync();
+  svec_to_mat(n, Y, S, p.g);
+  p.g.sync();
   // X = (S Z + Z S)/2
-  for (int e = p.lane; e < n * n; e += 32) {
+  for (int e = p.lane; e < n * n; e += p.g.G) {
     int i = e % n, j = e / n;
     double t = 0;
     for (int k = 0; k < n; ++k) t += S[i + n * k] * Z[k + n * j] + Z[i + n * k] * S[k + n * j];
     X[e] = 0.5 * t;
   }
-  __syncwarp();
+  p.g.sync();
   double smv = sm[p.inst];
   double *out = shift + p.off;
-  mat_to_svec(n, X, out, p.lane);
-  __syncwarp();
-  for (int k = p.lane; k < n; k += 32) out[(k + 1) * (k + 2) / 2 - 1] -= smv;
+  mat_to_svec(n, X, out, p.g);
+  p.g.sync();
+  for (int k = p.lane; k < n; k += p.g.G) out[(k + 1) * (k + 2) / 2 - 1] -= smv;
 }
 
 // ===================================================== ds_from_dz_offset
@@ -1288,20 +1311,20 @@ __global__ void k_psd_ds_offset(ConeSet cs, double *out, const double *__restric
   double *X = psd_smem(nm, 4), *Z = X + nn, *T = Z + nn, *Y = T + nn;
   const double *R = cs.psd_R + (size_t)p.c * nn;
   const double *lam = cs.psd_lam + (size_t)p.c * nm;
-  svec_to_mat(n, ds + p.off, Z, p.lane);
-  __syncwarp();
-  for (int e = p.lane; e < n * n; e += 32) {
+  svec_to_mat(n, ds + p.off, Z, p.g);
+  p.g.sync();
+  for (int e = p.lane; e < n * n; e += p.g.G) {
     int i = e % n, j = e / n;
     X[e] = 2 * Z[e] / (lam[i] + lam[j]);
   }
-  __syncwarp();
+  p.g.sync();
   // work stored as svec then re-expanded (as the reference does)
-  mat_to_svec(n, X, Y, p.lane);
-  __syncwarp();
-  svec_to_mat(n, Y, X, p.lane);
-  __syncwarp();
-  psd_wmul(n, R, true, X, Z, T, p.lane);  // Z = R X R'
-  mat_to_svec(n, Z, out + p.off, p.lane);
+  mat_to_svec(n, X, Y, p.g);
+  p.g.sync();
+  svec_to_mat(n, Y, X, p.g);
+  p.g.sync();
+  psd_wmul(n, R, true, X, Z, T, p.g);  // Z = R X R'
+  mat_to_svec(n, Z, out + p.off, p.g);
 }
 
 // ============================================================ step length
@@ -1408,23 +1431,23 @@ __global__ void k_psd_step(ConeSet cs, const double *__restrict__ dz,
   double amax = alpha[p.inst];
   double res = amax;
   for (int side = 0; side < 2; ++side) {
-    svec_to_mat(n, (side == 0 ? dz : ds) + p.off, X, p.lane);
-    __syncwarp();
+    svec_to_mat(n, (side == 0 ? dz : ds) + p.off, X, p.g);
+    p.g.sync();
     if (side == 0)
-      psd_wmul(n, R, false, X, Y, T, p.lane);  // W dz = R' dZ R
+      psd_wmul(n, R, false, X, Y, T, p.g);  // W dz = R' dZ R
     else
-      psd_wmul(n, Ri, true, X, Y, T, p.lane);  // W^{-T} ds = Ri dS Ri'
+      psd_wmul(n, Ri, true, X, Y, T, p.g);  // W^{-T} ds = Ri dS Ri'
     // svec round trip then scale by Lis both sides
-    mat_to_svec(n, Y, V, p.lane);
-    __syncwarp();
-    svec_to_mat(n, V, Y, p.lane);
-    __syncwarp();
-    for (int e = p.lane; e < n * n; e += 32) {
+    mat_to_svec(n, Y, V, p.g);
+    p.g.sync();
+    svec_to_mat(n, V, Y, p.g);
+    p.g.sync();
+    for (int e = p.lane; e < n * n; e += p.g.G) {
       int i = e % n, j = e / n;
       Y[e] *= (1.0 / sqrt(lam[i])) * (1.0 / sqrt(lam[j]));
     }
-    __syncwarp();
-    double gmin = warp_eig_min(n, Y, nullptr, p.lane);
+    p.g.sync();
+    double gmin = warp_eig_min(n, Y, nullptr, p.g);
     double a = gmin < 0 ? fmin(1.0 / (-gmin), amax) : amax;
     res = fmin(res, a);
   }
@@ -1523,21 +1546,21 @@ __global__ void k_psd_barrier(ConeSet cs, const double *__restrict__ z,
   double total = 0;
   for (int side = 0; side < 2; ++side) {
     const double *x = side == 0 ? z : s, *dx = side == 0 ? dz : ds;
-    for (int k = p.lane; k < p.t; k += 32) q[k] = x[p.off + k] + a * dx[p.off + k];
-    __syncwarp();
-    svec_to_mat(n, q, Q, p.lane);
-    __syncwarp();
-    bool ok = warp_chol(n, Q, p.lane);
+    for (int k = p.lane; k < p.t; k += p.g.G) q[k] = x[p.off + k] + a * dx[p.off + k];
+    p.g.sync();
+    svec_to_mat(n, q, Q, p.g);
+    p.g.sync();
+    bool ok = warp_chol(n, Q, p.g);
     double ld;
     if (ok) {
       double t = 0.0;
-      for (int r = p.lane; r < n; r += 32) t += log(Q[r + n * r]);
-      ld = 2 * warp_sum(t);
+      for (int r = p.lane; r < n; r += p.g.G) t += log(Q[r + n * r]);
+      ld = 2 * p.g.sum(t);
     } else {
       ld = CUDART_INF;
     }
     total -= ld;
-    __syncwarp();
+    p.g.sync();
   }
   if (p.lane == 0) cs.cone_tmp[cs.n_soc + cs.n_exp + cs.n_pow + p.c] = total;
 }
@@ -1598,12 +1621,12 @@ __global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z) {
     }
     return;
   }
-  svec_to_mat(n, z + p.off, Z, p.lane);
-  __syncwarp();
-  double mn = warp_eig_min(n, Z, ev, p.lane);
+  svec_to_mat(n, z + p.off, Z, p.g);
+  p.g.sync();
+  double mn = warp_eig_min(n, Z, ev, p.g);
   double pos = 0.0;
-  for (int r = p.lane; r < n; r += 32) pos += ev[r] > 0 ? ev[r] : 0.0;
-  pos = warp_sum(pos);
+  for (int r = p.lane; r < n; r += p.g.G) pos += ev[r] > 0 ? ev[r] : 0.0;
+  pos = p.g.sum(pos);
   if (p.lane == 0) {
     cs.cone_tmp[slot] = mn;
     cs.cone_tmp2[slot] = pos;
@@ -2229,14 +2252,15 @@ static inline int nn_block(const ConeSet &cs) { return cs.nn_block > 0 ? cs.nn_b
 
 static inline void psd_launch_dims(const ConeSet &cs, int nmats, int &nb, int &nt,
                                    size_t &smem) {
-  // warps (cones) per block: kPsdWarps while their matrices fit 200 KB
+  // groups (cones) per block: 64 threads' worth while their matrices fit
+  // 200 KB
+  const int G = psd_group(cs.psd_nmax), want = 32 * kPsdWarps / G;
   const size_t per = (size_t)nmats * cs.psd_nmax * cs.psd_nmax * sizeof(double);
-  const int warps =
-      per == 0 ? kPsdWarps
-               : (int)std::max<size_t>(1, std::min<size_t>(kPsdWarps, (200 * 1024) / per));
-  nt = 32 * warps;
-  nb = blocks_for((long long)cs.n_psd * 32, nt);
-  smem = (size_t)warps * per + 256;
+  const int groups =
+      per == 0 ? want : (int)std::max<size_t>(1, std::min<size_t>(want, (200 * 1024) / per));
+  nt = G * groups;
+  nb = blocks_for((long long)cs.n_psd * G, nt);
+  smem = (size_t)groups * per + 256;
 }
 #define LAUNCH_PSD(KERNEL, NMATS, ...)                                                 \
   do {                                                                                 \

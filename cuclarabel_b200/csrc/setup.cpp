@@ -380,13 +380,19 @@ static void csc_transpose(const HostCSC &A, HostCSC &T) {
 // chunk word (ldl.cuh kStartMask)
 constexpr long long kStreamMaxEntries = (1LL << 22) - 1;
 
+// dense columns: a factor column longer than this belongs to a dense front
+// (the supernodal path factors it with tensor-core tiles; the single-warp
+// kernels are built for sparse columns)
+constexpr int kScalarMaxColumn = 512;
+
 // true when the scalar factor of the pattern (CSR graph, repeats allowed,
 // no self loops needed) under perm has more than `limit` entries below the
-// diagonal; elimination-tree path walk (Liu), stopping early
+// diagonal, or a column longer than kScalarMaxColumn; elimination-tree
+// path walk (Liu), stopping early
 static bool scalar_fill_exceeds(int N, const std::vector<int> &xadj,
                                 const std::vector<int> &adj, const std::vector<int> &perm,
                                 long long limit) {
-  std::vector<int> iperm(N), parent(N, -1), mark(N, -1);
+  std::vector<int> iperm(N), parent(N, -1), mark(N, -1), cnt(N, 0);
   for (int k = 0; k < N; ++k) iperm[perm[k]] = k;
   long long lnz = 0;
   for (int k = 0; k < N; ++k) {
@@ -398,6 +404,7 @@ static bool scalar_fill_exceeds(int N, const std::vector<int> &xadj,
       while (mark[i] != k) {
         if (parent[i] == -1) parent[i] = k;
         ++lnz;
+        if (++cnt[i] > kScalarMaxColumn) return true;
         mark[i] = k;
         i = parent[i];
       }
@@ -687,8 +694,9 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
         adjncy[cur[en.c]++] = en.r;
       }
     // instances whose work vector exceeds the single-warp kernels' budget
-    // (48 KB of FP64), or whose factor or matrix exceeds the range of their
-    // stream chunk words, take the supernodal factorisation
+    // (48 KB of FP64), whose factor or matrix exceeds the range of their
+    // stream chunk words, or whose factor has dense columns (> 512 entries)
+    // take the supernodal factorisation
     out.supernodal = (long long)N * 8 > 48 * 1024 || (long long)xadj[N] + N > kStreamMaxEntries;
     if (!out.supernodal) {
       out.perm = nd_order_csr(N, xadj, adjncy);
@@ -924,6 +932,33 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
 // Host replay of the device factorisation/solve on the prepared structures.
 // Used by tests (no GPU needed) to validate the ordering, symbolic
 // factorisation and every refresh map before any kernel reads them.
+extern "C" int clgpu_debug_instance_path(const clgpu_problem *pb, const clgpu_settings *st,
+                                         int *supernodal, long long *factor_entries) {
+  using namespace clgpu;
+  SetupOptions opt;
+  if (st) {
+    opt.soc_threshold = st->soc_threshold;
+    opt.equilibrate_enable = st->equilibrate_enable;
+    opt.equilibrate_max_iter = st->equilibrate_max_iter;
+  }
+  Prepared p;
+  if (!prepare_instance(*pb, opt, p)) return -2;
+  if (supernodal) *supernodal = p.supernodal ? 1 : 0;
+  if (factor_entries) {
+    long long e = 0;
+    if (p.supernodal) {
+      for (int t = 0; t < p.sym.ns(); ++t) {
+        const long long nc = p.sym.col0[t + 1] - p.sym.col0[t], nr = p.sym.rptr[t + 1] - p.sym.rptr[t];
+        e += nc * (nc - 1) / 2 + nc * nr;
+      }
+    } else {
+      e = (long long)p.Li.size();
+    }
+    *factor_entries = e;
+  }
+  return 0;
+}
+
 extern "C" int clgpu_debug_check_instance(const clgpu_problem *pb, const clgpu_settings *st,
                                           double *resid) {
   using namespace clgpu;

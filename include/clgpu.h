@@ -445,6 +445,12 @@ int clgpu_debug_soc_tiles(const int *off, const int *dim, int n, int max_cones,
                           int max_rows, int *tiles, int cap);
 int clgpu_debug_check_instance(const clgpu_problem *prob,
                                const clgpu_settings *settings, double *resid);
+/* Host-only view of the factorisation path setup picks for one instance
+ * (diagnostic, no reference counterpart): *supernodal = 1 for the
+ * supernodal (dense-front) LDL^T, 0 for the single-warp kernels, and the
+ * factor's strictly-lower entries.  Needs no GPU. */
+int clgpu_debug_instance_path(const clgpu_problem *prob, const clgpu_settings *settings,
+                              int *supernodal, long long *factor_entries);
 
 #ifdef __cplusplus
 }

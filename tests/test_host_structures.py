@@ -48,3 +48,28 @@ def test_psd_block_structures(side, ncones):
     streams' range and is prepared for the supernodal factorisation."""
     rc, res = check(problems.psd_lp(side, ncones, seed=0))
     assert rc == 0 and res < 1e-9
+
+
+def _path(pb):
+    cp, keep, n, m = _prep_problem(*pb)
+    st = Settings().to_c()
+    sn, ent = ctypes.c_int(), ctypes.c_longlong()
+    rc = _lib.load().clgpu_debug_instance_path(ctypes.byref(cp), ctypes.byref(st),
+                                               ctypes.byref(sn), ctypes.byref(ent))
+    assert rc == 0
+    return sn.value, ent.value
+
+
+def test_factorisation_paths():
+    """Sparse factors stay on the single-warp kernels (the bench batch's
+    instances, every 64th of the 4096 here), dense fronts take the
+    supernodal path: PSD blocks of side 32 to 40 (factor columns of 500+
+    entries) and the large configurations."""
+    for seed in range(0, 4096, 64):
+        sn, ent = _path(problems.mpc_qp(seed))
+        assert sn == 0, seed
+    assert _path(problems.psd_lp(24, 3, seed=0))[0] == 0
+    assert _path(problems.psd_lp(32, 3, seed=0))[0] == 1
+    assert _path(problems.psd_lp(36, 2, seed=0))[0] == 1
+    assert _path(problems.psd_lp(40, 1, seed=0))[0] == 1
+    assert _path(problems.mixed_socp(0.1))[0] == 1
