@@ -63,12 +63,14 @@ def _path(pb):
 def test_factorisation_paths():
     """Sparse factors stay on the single-warp kernels (the bench batch's
     instances, every 64th of the 4096 here), dense fronts take the
-    supernodal path: PSD blocks of side 32 to 40 (factor columns of 500+
+    supernodal path: linear SDPs whose PSD blocks reach side 24 to 40 with
+    three or fewer blocks coupled by equality rows (factor columns of 500+
     entries) and the large configurations."""
     for seed in range(0, 4096, 64):
         sn, ent = _path(problems.mpc_qp(seed))
         assert sn == 0, seed
-    assert _path(problems.psd_lp(24, 3, seed=0))[0] == 0
+    assert _path(problems.psd_lp(20, 3, seed=0))[0] == 0
+    assert _path(problems.psd_lp(24, 3, seed=0))[0] == 1
     assert _path(problems.psd_lp(32, 3, seed=0))[0] == 1
     assert _path(problems.psd_lp(36, 2, seed=0))[0] == 1
     assert _path(problems.psd_lp(40, 1, seed=0))[0] == 1
