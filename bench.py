@@ -666,7 +666,8 @@ def serve_config5(pbs, lam, seconds, seed, method, budget_gb, new_frac, large_fr
     # (its L2 flushes and timed launches would disturb them)
     cohort = serving.CohortLane("new-structure MPC", streams[2].cuda_stream, budget,
                                 bytes_per_nnz=small.bytes / max(small.kkt_nnz, 1),
-                                direct_solve_method=method, autotune=False)
+                                direct_solve_method=method, autotune=False,
+                                setup_threads=2)
     small.warm(0)
     large.warm(0)  # the smallest configuration-2-like structure
     torch.cuda.synchronize()
@@ -794,6 +795,8 @@ def main():
                          "on the supernodal factorisation; 0 skips them")
     ap.add_argument("--large-cpu-scale", type=float, default=0.05,
                     help="scale of the CPU oracle's sample of configurations 2 and 3")
+    ap.add_argument("--large-which", type=int, default=0, choices=(0, 2, 3),
+                    help="with --large-only: configuration 2 or 3 only (0: both)")
     ap.add_argument("--large-only", action="store_true",
                     help="run only configurations 2 and 3 and print their JSON")
     args = ap.parse_args()
@@ -819,9 +822,10 @@ def main():
         st_ = torch.cuda.Stream()
         pk = fp64_gemm_peak()
         out = {"fp64_gemm_tflops": pk}
-        for which in (2, 3):
+        for which in ((2, 3) if args.large_which == 0 else (args.large_which,)):
             out["config%d" % which] = large_single(which, args.large_scale, args.method,
-                                                   st_.cuda_stream, pk, args.large_cpu_scale)
+                                                   st_.cuda_stream, pk,
+                                                   0 if args.no_cpu else args.large_cpu_scale)
         print(json.dumps(out), flush=True)
         return
     dist = None

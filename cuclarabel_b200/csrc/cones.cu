@@ -581,7 +581,8 @@ __global__ void __launch_bounds__(128, 7) k_nonsym_update_scaling(ConeSet cs, No
 // every barrier and shuffle names the group's lanes only.
 struct PsdGrp {
   int lane, G;
-  unsigned mask;
+  unsigned mask;  // this group's lanes
+  unsigned warp;  // lanes of the warp's groups still working (for votes)
   __device__ __forceinline__ void sync() const { __syncwarp(mask); }
   __device__ __forceinline__ double sum(double v) const {
     for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
@@ -682,12 +683,18 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, co
         gd = g.sum(gd);
         // columns orthogonal to 1e-14 of their norms: the rounding noise of
         // the dot products of n <= 48 rows sits near n^(1/2) eps, so a
-        // tighter bound keeps rotating at noise level until the sweep cap
-        if (fabs(gd) <= 1e-14 * sqrt(a * b) || gd == 0) continue;
-        rotated = 1;
-        double zeta = (b - a) / (2 * gd);
-        double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
-        double cs = 1 / sqrt(1 + t * t), sn = cs * t;
+        // tighter bound keeps rotating at noise level until the sweep cap.
+        // A skipped pair applies the identity rotation (bit for bit no
+        // change), so both groups of a warp follow the same path.
+        const bool skip = fabs(gd) <= 1e-14 * sqrt(a * b) || gd == 0;
+        double cs = 1.0, sn = 0.0;
+        if (!skip) {
+          rotated = 1;
+          double zeta = (b - a) / (2 * gd);
+          double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
+          cs = 1 / sqrt(1 + t * t);
+          sn = cs * t;
+        }
         for (int r = g.lane; r < n; r += g.G) {
           double mp = M[r + n * p], mq = M[r + n * q];
           M[r + n * p] = cs * mp - sn * mq;
@@ -698,7 +705,7 @@ __device__ void warp_svd(int n, double *M, double *V, double *S, double *tmp, co
         }
         g.sync();
       }
-    if (!rotated) break;
+    if (!__any_sync(g.warp, rotated)) break;  // every group of the warp converged
   }
   // column norms, sort descending (selection on the group's lane 0 into tmp perm)
   for (int c = g.lane; c < n; c += g.G) {
@@ -761,24 +768,31 @@ __device__ double warp_eig_min(int n, double *A, double *ev, const PsdGrp &g) {
     // diagonal entry.  (A tighter relative bound sits at the rounding
     // noise of the rotations and is never reached, so the sweeps ran to
     // their cap.)
-    if (off <= 1e-26 * tot || off == 0) break;
+    const bool conv = off <= 1e-26 * tot || off == 0;
+    if (__all_sync(g.warp, conv)) break;  // every group of the warp converged
     // threshold Jacobi: a rotation whose effect on the diagonal is below
     // the rounding of its entries (apq^2 <= 2^-106 |app aqq|) or of the
     // matrix (apq^2 <= 1e-30 |A|_F^2 / n^2) is skipped; a sweep without a
-    // rotation ends the iteration
+    // rotation ends the iteration.  A skipped pair (and every pair of a
+    // converged group) applies the identity rotation, bit for bit no
+    // change, so both groups of a warp follow the same path.
     const double tiny = 1e-30 * tot / (double(n) * n);
     bool rotated = false;
     for (int p = 0; p < n; ++p)
       for (int q = p + 1; q < n; ++q) {
         double apq = A[p + n * q];
-        if (apq == 0) continue;
         double app = A[p + n * p], aqq = A[q + n * q];
         const double a2 = apq * apq;
-        if (a2 <= 1.2325951644078310e-32 * fabs(app * aqq) || a2 <= tiny) continue;
-        rotated = true;
-        double theta = (aqq - app) / (2 * apq);
-        double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-        double c = 1 / sqrt(t * t + 1), s = t * c;
+        const bool skip = conv || apq == 0 ||
+                          a2 <= 1.2325951644078310e-32 * fabs(app * aqq) || a2 <= tiny;
+        double c = 1.0, s = 0.0;
+        if (!skip) {
+          rotated = true;
+          double theta = (aqq - app) / (2 * apq);
+          double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+          c = 1 / sqrt(t * t + 1);
+          s = t * c;
+        }
         g.sync();
         for (int r = g.lane; r < n; r += g.G) {
           double akp = A[r + n * p], akq = A[r + n * q];
@@ -793,7 +807,7 @@ __device__ double warp_eig_min(int n, double *A, double *ev, const PsdGrp &g) {
         }
         g.sync();
       }
-    if (!rotated) break;
+    if (!__any_sync(g.warp, rotated)) break;
   }
   double v = CUDART_INF;
   for (int r = g.lane; r < n; r += g.G) {
@@ -820,6 +834,7 @@ __device__ __forceinline__ PsdCtx psd_ctx(const ConeSet &cs) {
   p.off = cs.psd_off[p.c];
   p.inst = cs.psd_inst[p.c];
   if (p.valid && !active_inst(cs, p.inst)) p.valid = false;
+  p.g.warp = __ballot_sync(0xffffffffu, p.valid);
   return p;
 }
 __device__ __forceinline__ double *psd_smem(int nmax, int nmats) {
@@ -843,6 +858,7 @@ __global__ void k_psd_update_scaling(ConeSet cs, const double *__restrict__ s,
   p.g.sync();
   bool ok1 = warp_chol(n, L1, p.g);
   bool ok2 = warp_chol(n, L2, p.g);
+  p.g.warp = __ballot_sync(p.g.warp, ok1 && ok2);  // groups going on to the SVD
   if (!(ok1 && ok2)) {
     if (p.lane == 0) scale_ok[p.inst] = 0;
     return;
@@ -1613,6 +1629,7 @@ __global__ void k_psd_margins(ConeSet cs, const double *__restrict__ z) {
   int n = p.n, nm = cs.psd_nmax;
   double *Z = psd_smem(nm, 2), *ev = Z + nm * nm;
   const int slot = cs.n_soc + cs.n_exp + cs.n_pow + p.c;
+  p.g.warp = __ballot_sync(p.g.warp, n != 0);  // groups going on to the eigenvalues
   if (n == 0) {
     // an empty cone: (floatmax, 0), coneops_psdtrianglecone.jl:16-19
     if (p.lane == 0) {

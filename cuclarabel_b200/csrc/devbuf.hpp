@@ -46,7 +46,15 @@ inline bool arena_pool_alloc() {
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMemoryPoolsSupported, dev) != cudaSuccess)
       return false;
-    return v != 0;
+    if (v == 0) return false;
+    // keep freed memory in the pool (no unmapping at each synchronisation;
+    // solvers set up and destroyed while others run reuse it)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    return true;
   }();
   return on;
 }
