@@ -24,6 +24,7 @@
 
 #include "cones.cuh"
 #include "devbuf.hpp"
+#include "pinned.hpp"
 #include "ldl.cuh"
 #include "equilibrate.cuh"
 #include "sn_exec.cuh"
@@ -876,7 +877,7 @@ struct clgpu_solver {
   ~clgpu_solver() {
     for (auto ex : pass_exec)
       if (ex) cudaGraphExecDestroy(ex);
-    if (h_counter) cudaFreeHost(h_counter);
+    if (h_counter) pinned_give(h_counter);
     if (st_admit) {
       cudaStreamSynchronize(st_admit);
       cudaStreamDestroy(st_admit);
@@ -884,10 +885,10 @@ struct clgpu_solver {
     for (auto ev : ev_admit)
       if (ev) cudaEventDestroy(ev);
     for (int *p : {h_list, h_list_admit, h_list_collect, h_list_act})
-      if (p) cudaFreeHost(p);
-    if (h_info) cudaFreeHost(h_info);
-    if (h_stage) cudaFreeHost(h_stage);
-    if (h_sol) cudaFreeHost(h_sol);
+      if (p) pinned_give(p);
+    if (h_info) pinned_give(h_info);
+    if (h_stage) pinned_give(h_stage);
+    if (h_sol) pinned_give(h_sol);
     for (auto e : ev_pool) cudaEventDestroy(e);
   }
   int next_event() {
@@ -2087,7 +2088,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     h->h_n[i] = prep[i].n;
     h->h_m[i] = prep[i].m;
   }
-  cudaMallocHost(&h->h_counter, 4 * sizeof(int));
+  pinned_take(&h->h_counter, 4 * sizeof(int));
   // serving buffers
   h->d_sel = A.alloc<int>(B);
   h->d_sel_admit = A.alloc<int>(B);
@@ -2098,13 +2099,13 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   h->d_list_collect = A.alloc<int>(B);
   h->d_list_act = A.alloc<int>(B);
   h->d_info = A.alloc<double>((size_t)B * (NUM_SCALARS + NUM_INTS));
-  cudaMallocHost(&h->h_list, (size_t)B * sizeof(int));
-  cudaMallocHost(&h->h_list_admit, (size_t)B * sizeof(int));
-  cudaMallocHost(&h->h_list_collect, (size_t)B * sizeof(int));
-  cudaMallocHost(&h->h_list_act, (size_t)B * sizeof(int));
-  cudaMallocHost(&h->h_info, (size_t)B * (NUM_SCALARS + NUM_INTS) * sizeof(double));
-  cudaMallocHost(&h->h_stage, ((size_t)nx + (size_t)mz) * sizeof(double));
-  cudaMallocHost(&h->h_sol, ((size_t)nx + 2 * (size_t)mz) * sizeof(double));
+  pinned_take(&h->h_list, (size_t)B * sizeof(int));
+  pinned_take(&h->h_list_admit, (size_t)B * sizeof(int));
+  pinned_take(&h->h_list_collect, (size_t)B * sizeof(int));
+  pinned_take(&h->h_list_act, (size_t)B * sizeof(int));
+  pinned_take(&h->h_info, (size_t)B * (NUM_SCALARS + NUM_INTS) * sizeof(double));
+  pinned_take(&h->h_stage, ((size_t)nx + (size_t)mz) * sizeof(double));
+  pinned_take(&h->h_sol, ((size_t)nx + 2 * (size_t)mz) * sizeof(double));
   h->slot_state.assign(B, 0);
   h->slot_t0.assign(B, std::chrono::steady_clock::now());
   if (A.err != cudaSuccess) return -1000 - (int)A.err;

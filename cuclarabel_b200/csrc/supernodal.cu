@@ -32,6 +32,7 @@
 #include "common.cuh"
 #include "ldl.cuh"
 #include "sn_exec.cuh"
+#include "pinned.hpp"
 
 namespace clgpu {
 
@@ -1293,9 +1294,9 @@ SnExec::~SnExec() {
   if (g_pass) cudaGraphExecDestroy(g_pass);
   if (cap) cudaStreamDestroy(cap);
   for (cudaEvent_t e : prof.pool) cudaEventDestroy(e);
-  if (h_srun) cudaFreeHost(h_srun);
-  if (h_flags) cudaFreeHost(h_flags);
-  if (h_nrm) cudaFreeHost(h_nrm);
+  if (h_srun) pinned_give(h_srun);
+  if (h_flags) pinned_give(h_flags);
+  if (h_nrm) pinned_give(h_nrm);
 }
 
 bool sn_exec_create(const SnPlan &P, bool fp32, int B, int vbase, int vcount,
@@ -1351,9 +1352,9 @@ bool sn_exec_create(const SnPlan &P, bool fp32, int B, int vbase, int vcount,
   d.vcount = vcount;
   ex.d_insts = A.upload(P.insts);
   ex.d_flags = A.alloc<int>(B);
-  if (cudaMallocHost(&ex.h_srun, sizeof(int) * B) != cudaSuccess) return false;
-  if (cudaMallocHost(&ex.h_flags, sizeof(int) * B) != cudaSuccess) return false;
-  if (cudaMallocHost(&ex.h_nrm, sizeof(unsigned long long) * 2 * B) != cudaSuccess) return false;
+  if (pinned_take(&ex.h_srun, sizeof(int) * B) != cudaSuccess) return false;
+  if (pinned_take(&ex.h_flags, sizeof(int) * B) != cudaSuccess) return false;
+  if (pinned_take(&ex.h_nrm, sizeof(unsigned long long) * 2 * B) != cudaSuccess) return false;
   return A.err == cudaSuccess;
 }
 
