@@ -296,7 +296,8 @@ def _pack_batch(problems):
     """clgpu_problem array for a batch: each field's arrays are concatenated
     once and every instance's pointers are computed from offsets, so the
     per-instance host cost is the validation alone."""
-    parts = {k: [] for k in ("Pp", "Pi", "Px", "q", "Ap", "Ai", "Ax", "b", "ct", "cd", "cp")}
+    parts = {k: [] for k in ("Pp", "Pi", "Px", "q", "Ap", "Ai", "Ax", "b")}
+    ct, cd, cp = [], [], []
     nm = np.zeros((len(problems), 3), np.int64)
     for k, (P, q, A, b, cones) in enumerate(problems):
         q = np.asarray(q, dtype=np.float64).ravel()
@@ -305,27 +306,39 @@ def _pack_batch(problems):
         if isinstance(cones, dict):
             cones = cones_from_dict(cones)
         specs = [c.spec() for c in cones]
+        nc = len(specs)
+        if nc:
+            t_, d_, a_ = zip(*specs)
+            ct.extend(t_)
+            cd.extend(d_)
+            cp.extend(a_)
+            nv = sum(d if t < 3 else (3 if t < 5 else d * (d + 1) // 2) for t, d in zip(t_, d_))
+        else:
+            nv = 0
         P = _as_csc(P, (n, n))
         A = _as_csc(A, (m, n))
-        if (A.shape != (m, n) or P.shape != (n, n)
-                or sum(_nvars(sp_) for sp_ in specs) != m):
+        if A.shape != (m, n) or P.shape != (n, n) or nv != m:
             _prep_problem(P, q, A, b, cones)  # raises the reference's message
         parts["Pp"].append(P.indptr); parts["Pi"].append(P.indices); parts["Px"].append(P.data)
         parts["q"].append(q)
         parts["Ap"].append(A.indptr); parts["Ai"].append(A.indices); parts["Ax"].append(A.data)
         parts["b"].append(b)
-        parts["ct"].append([t for t, _, _ in specs])
-        parts["cd"].append([d for _, d, _ in specs])
-        parts["cp"].append([a for _, _, a in specs])
-        nm[k] = (n, m, len(specs))
+        nm[k] = (n, m, nc)
     keep = {}
     arr = np.zeros(len(problems), _PROBLEM_DTYPE)
     arr["n"], arr["m"], arr["ncones"] = nm[:, 0], nm[:, 1], nm[:, 2]
+    n_, m_, c_ = nm[:, 0], nm[:, 1], nm[:, 2]
+    cone_lists = {"ct": np.asarray(ct + [0], np.int32), "cd": np.asarray(cd + [0], np.int32),
+                  "cp": np.asarray(cp + [0.0], np.float64)}
     for f, dt in (("Pp", np.int32), ("Pi", np.int32), ("Px", np.float64), ("q", np.float64),
                   ("Ap", np.int32), ("Ai", np.int32), ("Ax", np.float64), ("b", np.float64),
                   ("ct", np.int32), ("cd", np.int32), ("cp", np.float64)):
-        lens = np.fromiter((len(a) for a in parts[f]), np.int64, len(problems))
-        flat = np.concatenate([np.asarray(a, dt) for a in parts[f]] + [np.zeros(1, dt)])
+        if f in cone_lists:
+            flat, lens = cone_lists[f], c_
+        else:
+            flat = np.concatenate([a if a.dtype == dt else np.asarray(a, dt) for a in parts[f]]
+                                  + [np.zeros(1, dt)])
+            lens = np.fromiter((len(a) for a in parts[f]), np.int64, len(problems))
         keep[f] = flat
         offs = np.concatenate([[0], np.cumsum(lens)[:-1]]) * flat.itemsize
         field = {"ct": "cone_types", "cd": "cone_dims", "cp": "cone_params"}.get(f, f)

@@ -1624,6 +1624,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       nchk[i] = ((int)p.Kj.size() + kSChunk - 1) / kSChunk;
     }
   });
+  mark("  streams: entries");
   // chunk tables: start relative to the stream base | scan steps <<
   // kStepShift | (count - 1) << kCntShift
   const auto ofch = prefix(nchf), obch = prefix(nchb), okch = prefix(nchk);
@@ -1673,6 +1674,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   step_stats("fwd", fch.data(), fch.size(), false);
   step_stats("bwd", bch.data(), bch.size(), false);
   step_stats("resid", kch.data(), kch.size(), false);
+  mark("  streams: chunks + upload");
   // streamed factorisation: op streams, pivots and chunk tables, split over
   // the kFactorWarps warps of the instance's block level by level
   {
@@ -1824,6 +1826,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       std::vector<int4>().swap(iops[i]);
     });
     step_stats("factor", foch.data(), foch.size(), true);
+    mark("  factor ops: build");
     kk.fstream = A.upload(fs);
     kk.fop_base = A.upload(fop_base);
     kk.foch = A.upload(foch);
@@ -1831,6 +1834,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     kk.flcnt = A.upload(flcnt);
     kk.fop = A.upload(fop);
     kk.Lkpos = A.upload(Lkpos);
+    mark("  factor ops: upload");
     kk.has_fstream = any_fs ? 1 : 0;
     kk.has_small_legacy = 0;
     for (int i = 0; i < B; ++i)
@@ -2182,11 +2186,16 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
   h->sd = make_sd(h->st);
   h->info.assign(nprob, clgpu_info{});
   // launch shapes of the nonnegative and SOC kernels, timed on this batch
+  const auto t_at = std::chrono::steady_clock::now();
   rc = h->st.autotune ? cones_autotune(h->cs, 0) : 0;
   if (rc != 0) {
     delete h;
     return rc;
   }
+  if (h->st.verbose)
+    std::fprintf(stderr, "clgpu setup: %-22s %8.1f ms\n", "launch-shape timing",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                           t_at).count());
   *out = h;
   return 0;
 }
