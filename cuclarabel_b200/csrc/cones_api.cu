@@ -229,6 +229,7 @@ extern "C" int clgpu_cones_create(int ncones, const int *types, const int *dims,
     delete h;
     return -1000 - (int)se;
   }
+  A.settle();
   *out = h;
   return 0;
 }

@@ -2,35 +2,19 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <memory>
 #include <utility>
 #include <vector>
 
+#include "pinned.hpp"
+
 namespace clgpu {
 
-// Host vector whose elements are default-initialised (no zero fill): large
-// setup arrays are written in full by parallel threads, so the zeroing pass
-// (serial, and the first touch of every page) is skipped.
+// Host vector of a large setup array: page-locked pool memory, elements
+// default-initialised (PinnedInitAlloc).
 template <class T>
-struct DefaultInitAlloc : std::allocator<T> {
-  template <class U>
-  struct rebind {
-    using other = DefaultInitAlloc<U>;
-  };
-  DefaultInitAlloc() = default;
-  template <class U>
-  DefaultInitAlloc(const DefaultInitAlloc<U> &) {}
-  template <class U>
-  void construct(U *p) noexcept {
-    ::new (static_cast<void *>(p)) U;
-  }
-  template <class U, class... Args>
-  void construct(U *p, Args &&...args) {
-    ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
-  }
-};
-template <class T>
-using hvec = std::vector<T, DefaultInitAlloc<T>>;
+using hvec = std::vector<T, PinnedInitAlloc<T>>;
 
 // Where the device has memory pools, allocations come from the
 // stream-ordered pool on the legacy stream (cudaMallocAsync) and go back
@@ -64,6 +48,7 @@ struct DevArena {
   long long bytes = 0;
   cudaError_t err = cudaSuccess;
   bool pooled = arena_pool_alloc();
+  bool pending = false;  // uploads not yet settled
   // zero-filled unless the caller overwrites it at once (upload); ordered
   // on the legacy stream, which the setup synchronises before returning
   template <typename T>
@@ -81,16 +66,49 @@ struct DevArena {
     bytes += (long long)(count * sizeof(T));
     return static_cast<T *>(p);
   }
+  // Uploads are asynchronous on the legacy stream, so they overlap the
+  // host work that follows.  A page-locked source (an hvec) is copied from
+  // in place and kept out of the pool until settle(); a small pageable
+  // source is first copied into a page-locked pool buffer (a pageable copy
+  // would wait for every copy before it); a large one is copied directly
+  // (the call returns once the driver has staged it).  The caller must not
+  // change an hvec after uploading it, and must call settle() once it has
+  // synchronised the legacy stream.
   template <typename T, typename Al>
   T *upload(const std::vector<T, Al> &v) {
     T *p = alloc<T>(v.size(), v.empty());
-    if (p && !v.empty()) {
-      cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
-      if (e != cudaSuccess) err = e;
-    }
+    if (p && !v.empty()) copy_in(p, v.data(), v.size() * sizeof(T));
     return p;
   }
+  void copy_in(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kStageMax = 8u << 20;
+    PinnedPool &pool = PinnedPool::get();
+    const void *from = src;
+    if (pool.owns(src)) {
+      pool.hold_for(const_cast<void *>(src), this);
+    } else if (bytes <= kStageMax) {
+      void *stage = pool.take(bytes);
+      if (stage) {
+        std::memcpy(stage, src, bytes);
+        pool.hold_for(stage, this);
+        pool.give(stage);  // returns to the pool at settle()
+        from = stage;
+      }
+    }
+    cudaError_t e = cudaMemcpyAsync(dst, from, bytes, cudaMemcpyHostToDevice, 0);
+    if (e != cudaSuccess) err = e;
+    pending = true;
+  }
+  // the legacy stream has been synchronised: the upload sources go back
+  void settle() {
+    PinnedPool::get().settle(this);
+    pending = false;
+  }
   void release() {
+    if (pending) {
+      cudaStreamSynchronize(0);
+      settle();
+    }
     for (void *p : ptrs) {
       if (pooled)
         cudaFreeAsync(p, 0);

@@ -1072,6 +1072,200 @@ static int ffd_pack(std::vector<int> items, Need need, long long cap, int slots,
   return (int)used.size();
 }
 
+// KKT position of every L entry (i, j), i > j, in the instance's permuted
+// full CSR (rows sorted, pattern symmetric), offset by kb; -1 when K has no
+// such entry.  Walking the rows r in order meets the entries (c, r) of each
+// row c in increasing r, so tpos[t] (the position of entry t's transpose) is
+// one pass with a cursor per row; row j scattered into a stamped map then
+// gives (j, i), and tpos its transpose (i, j).  Linear in nnz(K) + nnz(L).
+struct FactorOpScratch {
+  std::vector<int4> lev;
+  std::vector<int> nodes, cnt, segs, rowpos, rowstamp, tpos, cur;
+  std::vector<int> wch[kFactorWarps];
+  int stamp = 0;
+  void fit(int n, int nk) {
+    if ((int)rowpos.size() < n) {
+      rowpos.resize(n);
+      rowstamp.assign(n, 0);
+      cur.resize(n);
+      stamp = 0;
+    }
+    if ((int)tpos.size() < nk) tpos.resize(nk);
+  }
+};
+
+static void l_kkt_positions(const Prepared &p, long long kb, int *Lkpos, FactorOpScratch &sc) {
+  const int Ni = p.N;
+  sc.fit(Ni, (int)p.Kj.size());
+  int *rowpos = sc.rowpos.data(), *rowstamp = sc.rowstamp.data();
+  int *tpos = sc.tpos.data(), *cur = sc.cur.data();
+  for (int r = 0; r < Ni; ++r) cur[r] = p.Kp[r];
+  for (int r = 0; r < Ni; ++r)
+    for (int t = p.Kp[r]; t < p.Kp[r + 1]; ++t) tpos[t] = cur[p.Kj[t]]++;
+  for (int j = 0; j < Ni; ++j) {
+    const int st = ++sc.stamp;
+    for (int t = p.Kp[j]; t < p.Kp[j + 1]; ++t) {
+      rowpos[p.Kj[t]] = t;
+      rowstamp[p.Kj[t]] = st;
+    }
+    for (int q = p.Lp[j]; q < p.Lp[j + 1]; ++q) {
+      const int r = p.Li[q];
+      Lkpos[q] = rowstamp[r] == st ? (int)(kb + tpos[rowpos[r]]) : -1;
+    }
+  }
+}
+
+// Number of ops of the instance's streamed factorisation: one per (j, k)
+// pair of its row structure and per entry of L(:,k) below row j, and one
+// pivot per column.
+static long long factor_op_count(const Prepared &p) {
+  long long t = p.N;
+  for (size_t r = 0; r < p.Rk.size(); ++r) t += p.Lp[p.Rk[r] + 1] - p.Rpos[r];
+  return t;
+}
+
+// The streamed factorisation's ops of one instance, written to op (exactly
+// factor_op_count(p) of them), level by level:
+//  - the level's updates grouped by target (a segment per target), targets
+//    increasing: first the diagonal targets j (update d_j -= U(j,k)^2 / d_k,
+//    {j, Ni + pjk, Ni + pjk, k}), then the column targets Ni + q (update
+//    L(i,j) -= L(i,k) U(j,k), {Ni + q, Ni + pp, Ni + pjk, k}); a segment keeps
+//    its ops in generation order (the pairs (j, k) in row-structure order);
+//  - split into kFactorWarps parts of about equal length at segment starts,
+//    each op's .w or'd with min(position in segment, kPosMax) << 16 and the
+//    last-of-segment bit, each part cut into chunk words;
+//  - then the level's pivots {j, sign, 0, 0} in kFactorWarps contiguous parts.
+// The column ranges of L follow the node order, so sorting the level's nodes
+// and bucketing each column by q (counting sort) lists the groups in target
+// order without a comparison sort.  Returns false when the structure of
+// L(:,k) below j is not inside L(:,j) (not reached for a valid symbolic
+// factorisation) or a part's chunk count leaves its 16-bit field.
+static bool build_factor_ops(const Prepared &p, int4 *op, int *flcnt, std::vector<int> &chk,
+                             std::array<int, kFactorWarps + 1> &woff, FactorOpScratch &sc) {
+  constexpr int W = kFactorWarps;
+  const int Ni = p.N;
+  const int nl = (int)p.lvl_ptr.size() - 1;
+  const int *lp = p.lvl_ptr.data();
+  sc.fit(Ni, 0);
+  int *rowpos = sc.rowpos.data(), *rowstamp = sc.rowstamp.data();
+  auto &lev = sc.lev;
+  auto &nodes = sc.nodes;
+  auto &cnt = sc.cnt;
+  auto &segs = sc.segs;
+  for (int w = 0; w < W; ++w) sc.wch[w].clear();
+  long long nops = 0;
+  bool bad = false;
+  auto put_chunks = [&](int w, long long c0, long long c1, bool pivot) {
+    int n = 0;
+    for (long long c = c0; c < c1; c += kChunk, ++n) {
+      const int cn = (int)std::min<long long>(kChunk, c1 - c);
+      const int steps = pivot ? 0 : chunk_scan_steps<2>(cn, [&](int e) {
+        return (op[c + e].w >> 16) & kPosMax;
+      });
+      sc.wch[w].push_back((int)(c | ((long long)steps << kStepShift) |
+                                ((long long)(cn - 1) << kCntShift) |
+                                (pivot ? (long long)1 << 31 : 0LL)));
+    }
+    return n;
+  };
+  for (int l = 0; l < nl && !bad; ++l) {
+    nodes.assign(p.lvl_nodes.begin() + lp[l], p.lvl_nodes.begin() + lp[l + 1]);
+    std::sort(nodes.begin(), nodes.end());
+    size_t nlev = 0;
+    for (int j : nodes)
+      for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) nlev += p.Lp[p.Rk[r] + 1] - p.Rpos[r];
+    if (lev.size() < nlev) lev.resize(nlev);
+    segs.clear();
+    int f = 0;
+    for (int j : nodes) {
+      if (p.Rp[j + 1] > p.Rp[j]) segs.push_back(f);
+      for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) {
+        const int pjk = p.Rpos[r];
+        lev[f++] = make_int4(j, Ni + pjk, Ni + pjk, p.Rk[r]);
+      }
+    }
+    for (int j : nodes) {
+      if (p.Rp[j + 1] == p.Rp[j]) continue;
+      const int q0 = p.Lp[j], qe = p.Lp[j + 1], len = qe - q0;
+      if ((int)cnt.size() < len + 1) cnt.resize(len + 1);
+      std::fill(cnt.begin(), cnt.begin() + len + 1, 0);
+      const int st = ++sc.stamp;
+      for (int q = q0; q < qe; ++q) {
+        rowpos[p.Li[q]] = q - q0;
+        rowstamp[p.Li[q]] = st;
+      }
+      for (int r = p.Rp[j]; r < p.Rp[j + 1] && !bad; ++r) {
+        const int k = p.Rk[r];
+        for (int pp = p.Rpos[r] + 1; pp < p.Lp[k + 1]; ++pp) {
+          const int row = p.Li[pp];
+          if (rowstamp[row] != st) {
+            bad = true;
+            break;
+          }
+          cnt[rowpos[row] + 1]++;
+        }
+      }
+      if (bad) break;
+      for (int a = 0; a < len; ++a) {
+        if (cnt[a + 1]) segs.push_back(f + cnt[a]);
+        cnt[a + 1] += cnt[a];
+      }
+      for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) {
+        const int k = p.Rk[r], pjk = p.Rpos[r];
+        for (int pp = pjk + 1; pp < p.Lp[k + 1]; ++pp) {
+          const int a = rowpos[p.Li[pp]];
+          lev[f + cnt[a]++] = make_int4(Ni + q0 + a, Ni + pp, Ni + pjk, k);
+        }
+      }
+      f += cnt[len - 1];  // bucket ends after placement
+    }
+    if (bad) break;
+    const int nseg = (int)segs.size();
+    segs.push_back(f);
+    int sb[W + 1];
+    sb[0] = 0;
+    sb[W] = nseg;
+    for (int w = 1; w < W; ++w) {
+      const int ideal = (int)((size_t)f * w / W);
+      const int g = (int)(std::lower_bound(segs.begin(), segs.end(), ideal) - segs.begin());
+      sb[w] = std::min(nseg, std::max(sb[w - 1], g));
+    }
+    int nop[W], npv[W];
+    for (int w = 0; w < W; ++w) {
+      const long long start = nops;
+      for (int g = sb[w]; g < sb[w + 1]; ++g) {
+        const int s0 = segs[g], s1 = segs[g + 1];
+        for (int t = s0; t < s1; ++t) {
+          int4 o4 = lev[t];
+          o4.w |= (std::min(t - s0, kPosMax) << 16) | ((t == s1 - 1 ? 1 : 0) << kLastBit);
+          op[nops++] = o4;
+        }
+      }
+      nop[w] = put_chunks(w, start, nops, false);
+    }
+    const int np = lp[l + 1] - lp[l];
+    for (int w = 0; w < W; ++w) {
+      const long long start = nops;
+      for (int t = lp[l] + np * w / W; t < lp[l] + np * (w + 1) / W; ++t) {
+        const int j = p.lvl_nodes[t];
+        op[nops++] = make_int4(j, (int)p.Dsign[j], 0, 0);
+      }
+      npv[w] = put_chunks(w, start, nops, true);
+    }
+    for (int w = 0; w < W; ++w) {
+      if (nop[w] > 0xffff || npv[w] > 0xffff) bad = true;
+      flcnt[(size_t)l * W + w] = nop[w] | (npv[w] << 16);
+    }
+  }
+  chk.clear();
+  woff[0] = 0;
+  for (int w = 0; w < W; ++w) {
+    chk.insert(chk.end(), sc.wch[w].begin(), sc.wch[w].end());
+    woff[w + 1] = (int)chk.size();
+  }
+  return !bad;
+}
+
 static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   DevArena &A = h->arena;
   const int B = (int)prep.size();
@@ -1682,136 +1876,43 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     constexpr int W = kFactorWarps;
     const long long ring_bytes = (long long)W * kFRingSlots * kChunk * 16;
     std::vector<int> fs(B, 0);
-    std::vector<long long> nops(B, 0), nch(B, 0);
-    std::vector<std::vector<int4>> iops(B);
+    std::vector<long long> nch(B, 0);
     std::vector<std::vector<int>> ich(B);
     std::vector<std::array<int, W + 1>> iwoff(B);
     hvec<int> flcnt((size_t)lvof[B] * W);
     hvec<int> Lkpos((size_t)lnz);
+    // instances on the streamed factorisation, their op counts, and the
+    // streams written in place at their final offsets
+    std::vector<long long> ocnt(B, 0);
     par_for(B, nth, [&](int i) {
       const auto &p = prep[i];
-      const int Ni = N[i];
-      const long long nli = (long long)p.Li.size(), kb = kof[i], lb = lof[i];
-      // KKT position of each L entry (i, j): row i of the permuted CSR
-      for (int j = 0; j < Ni; ++j)
-        for (int q = p.Lp[j]; q < p.Lp[j + 1]; ++q) {
-          const int r = p.Li[q];
-          auto b0 = p.Kj.begin() + p.Kp[r], b1 = p.Kj.begin() + p.Kp[r + 1];
-          auto it = std::lower_bound(b0, b1, j);
-          Lkpos[lb + q] = (it != b1 && *it == j) ? (int)(kb + (it - p.Kj.begin())) : -1;
-        }
-      if (cls[i] != 1 || (Ni + nli) * 8 + ring_bytes > kFactorSmemBytes) return;
+      if (cls[i] != 1 || (N[i] + (long long)p.Li.size()) * 8 + ring_bytes > kFactorSmemBytes)
+        return;
       fs[i] = 1;
-      auto &ops = iops[i];
-      const int nl = nlev[i];
-      const int *lp = p.lvl_ptr.data();
-      std::vector<int4> lev;  // {target, a, b, k}
-      std::vector<std::vector<int>> wch(W);
-      std::vector<size_t> segs;
-      bool bad = false;
-      // chunk ops[c0, c1) (all of one part) into warp w's list
-      auto put_chunks = [&](int w, long long c0, long long c1, bool pivot) {
-        int n = 0;
-        for (long long c = c0; c < c1; c += kChunk, ++n) {
-          const int cnt = (int)std::min<long long>(kChunk, c1 - c);
-          const int steps = pivot ? 0 : chunk_scan_steps<2>(cnt, [&](int e) {
-            return (ops[c + e].w >> 16) & kPosMax;
-          });
-          wch[w].push_back((int)(c | ((long long)steps << kStepShift) |
-                                 ((long long)(cnt - 1) << kCntShift) |
-                                 (pivot ? (long long)1 << 31 : 0LL)));
-        }
-        return n;
-      };
-      for (int l = 0; l < nl && !bad; ++l) {
-        lev.clear();
-        for (int t = lp[l]; t < lp[l + 1]; ++t) {
-          const int j = p.lvl_nodes[t];
-          for (int r = p.Rp[j]; r < p.Rp[j + 1]; ++r) {
-            const int k = p.Rk[r], pjk = p.Rpos[r];
-            lev.push_back(make_int4(j, Ni + pjk, Ni + pjk, k));  // d_j -= U(j,k)^2 / d_k
-            int q = p.Lp[j];
-            const int qe = p.Lp[j + 1];
-            for (int pp = pjk + 1; pp < p.Lp[k + 1]; ++pp) {
-              const int row = p.Li[pp];
-              while (q < qe && p.Li[q] != row) ++q;  // struct(L(:,k) below j) in L(:,j)
-              if (q == qe) {
-                bad = true;
-                break;
-              }
-              lev.push_back(make_int4(Ni + q, Ni + pp, Ni + pjk, k));
-            }
-          }
-        }
-        std::stable_sort(lev.begin(), lev.end(),
-                         [](const int4 &a, const int4 &b) { return a.x < b.x; });
-        // segment starts (one segment per target), then W parts of about
-        // equal length whose boundaries are segment starts
-        segs.clear();
-        for (size_t q = 0; q < lev.size(); ++q)
-          if (q == 0 || lev[q].x != lev[q - 1].x) segs.push_back(q);
-        segs.push_back(lev.size());
-        size_t pb[W + 1];
-        pb[0] = 0;
-        pb[W] = lev.size();
-        for (int w = 1; w < W; ++w) {
-          const size_t ideal = lev.size() * (size_t)w / W;
-          const size_t s0 = *std::lower_bound(segs.begin(), segs.end(), ideal);
-          pb[w] = std::max(pb[w - 1], s0);
-        }
-        int nop[W], npv[W];
-        for (int w = 0; w < W; ++w) {
-          const long long start = (long long)ops.size();
-          for (size_t q = pb[w]; q < pb[w + 1];) {
-            size_t r = q;
-            while (r + 1 < pb[w + 1] && lev[r + 1].x == lev[q].x) ++r;
-            for (size_t t = q; t <= r; ++t) {
-              const int pos = (int)std::min<size_t>(t - q, kPosMax);
-              int4 o = lev[t];
-              o.w = o.w | (pos << 16) | ((t == r ? 1 : 0) << kLastBit);
-              ops.push_back(o);
-            }
-            q = r + 1;
-          }
-          nop[w] = put_chunks(w, start, (long long)ops.size(), false);
-        }
-        // the level's pivots, in W contiguous parts
-        const int np = lp[l + 1] - lp[l];
-        for (int w = 0; w < W; ++w) {
-          const long long start = (long long)ops.size();
-          for (int t = lp[l] + np * w / W; t < lp[l] + np * (w + 1) / W; ++t) {
-            const int j = p.lvl_nodes[t];
-            ops.push_back(make_int4(j, (int)p.Dsign[j], 0, 0));
-          }
-          npv[w] = put_chunks(w, start, (long long)ops.size(), true);
-        }
-        for (int w = 0; w < W; ++w) {
-          if (nop[w] > 0xffff || npv[w] > 0xffff) bad = true;
-          flcnt[((size_t)lvl_off[i] + l) * W + w] = nop[w] | (npv[w] << 16);
-        }
-      }
-      // a pattern mismatch is not reached for a valid symbolic factorisation;
-      // an op stream longer than the chunk words address is; both fall back
-      // to the level-scheduled single-warp factorisation
-      if ((long long)ops.size() > (long long)kStartMask) bad = true;
-      auto &chk = ich[i];
-      iwoff[i][0] = 0;
-      for (int w = 0; w < W; ++w) {
-        chk.insert(chk.end(), wch[w].begin(), wch[w].end());
-        iwoff[i][w + 1] = (int)chk.size();
-      }
-      if (bad) {
+      ocnt[i] = factor_op_count(p);
+    });
+    const auto oop = prefix(ocnt);
+    if (oop[B] > 2000000000LL) return -4;
+    hvec<int4> fop(std::max<long long>(oop[B], 1));
+    par_for(B, nth, [&](int i) {
+      thread_local FactorOpScratch sc;
+      const auto &p = prep[i];
+      l_kkt_positions(p, kof[i], Lkpos.data() + lof[i], sc);
+      if (!fs[i]) return;
+      bool ok = build_factor_ops(p, fop.data() + oop[i], flcnt.data() + (size_t)lvl_off[i] * W,
+                                 ich[i], iwoff[i], sc);
+      // an op stream longer than the chunk words address, or a structure
+      // mismatch, falls back to the level-scheduled single-warp factorisation
+      if (ocnt[i] > (long long)kStartMask) ok = false;
+      if (!ok) {
         fs[i] = 0;
-        ops.clear();
-        chk.clear();
+        ich[i].clear();
         for (int w = 0; w <= W; ++w) iwoff[i][w] = 0;
       }
-      nops[i] = (long long)ops.size();
-      nch[i] = (long long)chk.size();
+      nch[i] = (long long)ich[i].size();
     });
-    const auto oop = prefix(nops), och = prefix(nch);
-    if (oop[B] > 2000000000LL || och[B] > 2000000000LL) return -4;
-    hvec<int4> fop(std::max<long long>(oop[B], 1));
+    const auto och = prefix(nch);
+    if (och[B] > 2000000000LL) return -4;
     hvec<int> foch(std::max<long long>(och[B], 1));
     std::vector<int> fop_base(B), fwoff((size_t)B * (W + 1));
     bool any_fs = false;
@@ -1821,9 +1922,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       if (fs[i]) any_fs = true;
     }
     par_for(B, nth, [&](int i) {
-      std::copy(iops[i].begin(), iops[i].end(), fop.begin() + oop[i]);
       std::copy(ich[i].begin(), ich[i].end(), foch.begin() + och[i]);
-      std::vector<int4>().swap(iops[i]);
     });
     step_stats("factor", foch.data(), foch.size(), true);
     mark("  factor ops: build");
@@ -2068,6 +2167,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
       cudaError_t e = cudaStreamSynchronize(0);
       if (e == cudaSuccess) e = cudaGetLastError();
       if (e != cudaSuccess) return -1000 - (int)e;
+      A.settle();
     }
     mark("device equilibration");
   }
@@ -2116,6 +2216,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   cudaError_t e = cudaStreamSynchronize(0);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return -1000 - (int)e;
+  A.settle();  // the uploads have completed: their host sources go back to the pool
   mark("scratch + tail");
   return 0;
 }

@@ -143,6 +143,7 @@ extern "C" int clgpu_ldl_create(int N, const int *Kp, const int *Kj, const signe
   // the arena's zero fills run on the legacy stream: finished before any
   // stream of the caller's uses the handle
   if (cudaError_t se = cudaStreamSynchronize(0)) return cuda_status(se);
+  A.settle();
   LDLParams &lp = h->lp;
   lp.static_reg = st.static_regularization_enable;
   lp.static_c = st.static_regularization_constant;

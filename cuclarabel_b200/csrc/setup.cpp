@@ -93,21 +93,9 @@ std::vector<int> amd_order(int n, std::vector<std::vector<int>> &adj) {
   return order;
 }
 
-// Nested dissection (George's level-structure bisection).  A connected
-// vertex set larger than kNdLeaf is split by a middle level of a breadth-first
-// level structure rooted at a pseudo-peripheral vertex; only the vertices of
-// that level with a neighbour in the next level form the separator.  The two
-// halves are ordered first (recursively), the separator last, so the halves
-// become independent subtrees of the elimination tree.  Small sets are
-// ordered by minimum degree.  The KKT graphs of stage-structured problems
-// are long and thin: minimum degree eliminates them from both ends inward
-// and leaves an elimination tree of height ~N/2, while dissection keeps the
-// height near (separator size) x log2(N), which is what bounds the
-// level-scheduled factorisation and substitutions.  Dense vertices (degree
-// above max(16, 10 sqrt(n))) are ordered last, as in amd_order.
 // Minimum degree on at most 32 vertices (adjacency as bit masks); ties go
-// to the lower local index, as in amd_order.
-static void md_small(const int *S, int k, const uint32_t *mask_in, std::vector<int> &order) {
+// to the lower local index, as in amd_order.  Appends to order[no..].
+static void md_small(const int *S, int k, const uint32_t *mask_in, int *order, int &no) {
   uint32_t m[32];
   for (int a = 0; a < k; ++a) m[a] = mask_in[a];
   uint32_t alive = k == 32 ? 0xffffffffu : ((1u << k) - 1u);
@@ -128,7 +116,7 @@ static void md_small(const int *S, int k, const uint32_t *mask_in, std::vector<i
       m[u] |= nb;
       m[u] &= ~(1u << u);
     }
-    order.push_back(S[best]);
+    order[no++] = S[best];
   }
 }
 
@@ -153,93 +141,122 @@ std::vector<int> nd_order(int n, std::vector<std::vector<int>> &adj) {
 // level-scheduled factorisation and substitutions.  Dense vertices (degree
 // above max(16, 10 sqrt(n))) are ordered last, as in amd_order.  The input
 // CSR may hold repeated neighbours; it is deduplicated in place.
+//
+// The pending vertex sets form a stack whose lists live in one array: the
+// set being split is always on top, its parts (which partition it) are
+// written back over it, so the array never holds more than n vertices and
+// the recursion allocates nothing.
 std::vector<int> nd_order_csr(int n, std::vector<int> &xadj0, std::vector<int> &adj0) {
   constexpr int kNdLeaf = 8;
-  // sort + deduplicate every row, compacting
+  // sort + deduplicate every row in place (rows are short: insertion sort)
   {
     int w = 0;
     for (int i = 0; i < n; ++i) {
-      const int b0 = xadj0[i], b1 = xadj0[i + 1];
-      std::sort(adj0.begin() + b0, adj0.begin() + b1);
+      const int b0 = xadj0[i], len = xadj0[i + 1] - b0;
+      int *r = adj0.data() + b0;
+      for (int a = 1; a < len; ++a) {
+        const int x = r[a];
+        int c = a - 1;
+        while (c >= 0 && r[c] > x) {
+          r[c + 1] = r[c];
+          --c;
+        }
+        r[c + 1] = x;
+      }
       const int start = w;
-      for (int p = b0; p < b1; ++p)
-        if (p == b0 || adj0[p] != adj0[p - 1]) adj0[w++] = adj0[p];
+      for (int q = 0; q < len; ++q)
+        if (q == 0 || r[q] != r[q - 1]) adj0[w++] = r[q];
       xadj0[i] = start;
     }
     xadj0[n] = w;
-    // xadj0[i] now holds row starts; shift into a proper pointer array
   }
-  std::vector<int> rowend(n);
-  for (int i = 0; i < n; ++i) rowend[i] = i + 1 < n ? xadj0[i + 1] : xadj0[n];
   const double dense_thr = std::max(16.0, 10.0 * std::sqrt((double)n));
   std::vector<char> dense(n, 0);
   bool any_dense = false;
   for (int i = 0; i < n; ++i) {
-    dense[i] = (double)(rowend[i] - xadj0[i]) > dense_thr;
+    dense[i] = (double)(xadj0[i + 1] - xadj0[i]) > dense_thr;
     any_dense |= dense[i] != 0;
   }
-  std::vector<int> xadj(n + 1, 0), adjncy;
-  adjncy.reserve(xadj0[n]);
-  for (int i = 0; i < n; ++i) {
-    if (!dense[i])
-      for (int p = xadj0[i]; p < rowend[i]; ++p)
-        if (!any_dense || !dense[adj0[p]]) adjncy.push_back(adj0[p]);
-    xadj[i + 1] = (int)adjncy.size();
+  // the graph without the dense vertices (a copy only when there are some:
+  // the caller reads the deduplicated CSR afterwards)
+  std::vector<int> xadj_nd, adj_nd;
+  const int *xa = xadj0.data(), *ad = adj0.data();
+  if (any_dense) {
+    xadj_nd.assign(n + 1, 0);
+    adj_nd.reserve(xadj0[n]);
+    for (int i = 0; i < n; ++i) {
+      if (!dense[i])
+        for (int q = xadj0[i]; q < xadj0[i + 1]; ++q)
+          if (!dense[adj0[q]]) adj_nd.push_back(adj0[q]);
+      xadj_nd[i + 1] = (int)adj_nd.size();
+    }
+    xa = xadj_nd.data();
+    ad = adj_nd.data();
   }
-  std::vector<int> order;
-  order.reserve(n);
-  std::vector<int> mark(n, -1), lidx(n, -1), indeg(n, 0);
+  std::vector<int> order(n);
+  int no = 0;
+  std::vector<int> work((size_t)n * 10 + 2);
+  int *mark = work.data(), *lidx = mark + n, *indeg = lidx + n;
   // two level structures (the current best and a candidate); queue[s] lists
   // structure s's vertices in visiting order
-  std::vector<int> level_buf[2] = {std::vector<int>(n, -1), std::vector<int>(n, -1)};
-  std::vector<int> queue_buf[2] = {std::vector<int>(n), std::vector<int>(n)};
-  int cnt_buf[2] = {0, 0};
+  int *level[2] = {indeg + n, indeg + 2 * n};
+  int *queue[2] = {indeg + 3 * n, indeg + 4 * n};
+  int *arena = indeg + 5 * n;    // the pending sets' vertex lists
+  int *scratch = indeg + 6 * n;  // a split's parts before they are written back
+  int *lcount = indeg + 7 * n;   // vertices per level (depth <= n)
+  for (int i = 0; i < n; ++i) {
+    mark[i] = -1;
+    level[0][i] = level[1][i] = -1;
+  }
+  int cnt[2] = {0, 0};
   int stamp = 0;
   struct Task {
-    std::vector<int> v;
-    bool emit;
+    int off, len;
+    bool emit;  // a separator: emitted as it is
   };
   std::vector<Task> stack;
+  stack.reserve(64);
   {
-    Task t;
-    t.emit = false;
+    int top = 0;
     for (int i = 0; i < n; ++i)
-      if (!dense[i]) t.v.push_back(i);
-    if (!t.v.empty()) stack.push_back(std::move(t));
+      if (!dense[i]) arena[top++] = i;
+    if (top) stack.push_back({0, top, false});
   }
+  std::vector<int> cstart;
   // breadth-first levels of the set marked sid from src into structure b
   // (clearing b's previous visit); also records every visited vertex's
   // degree inside the set.  Returns the depth.
   auto bfs = [&](int src, int sid, int b) {
-    std::vector<int> &level = level_buf[b], &queue = queue_buf[b];
-    for (int i = 0; i < cnt_buf[b]; ++i) level[queue[i]] = -1;
+    int *lv = level[b], *qu = queue[b];
+    for (int i = 0; i < cnt[b]; ++i) lv[qu[i]] = -1;
     int head = 0, tail = 0, depth = 0;
-    queue[tail++] = src;
-    level[src] = 0;
+    qu[tail++] = src;
+    lv[src] = 0;
     while (head < tail) {
-      const int v = queue[head++];
-      depth = std::max(depth, level[v] + 1);
+      const int v = qu[head++];
+      const int lnext = lv[v] + 1;
+      depth = std::max(depth, lnext);
       int d = 0;
-      for (int p = xadj[v]; p < xadj[v + 1]; ++p) {
-        const int u = adjncy[p];
+      for (int q = xa[v]; q < xa[v + 1]; ++q) {
+        const int u = ad[q];
         if (mark[u] != sid) continue;
         ++d;
-        if (level[u] < 0) {
-          level[u] = level[v] + 1;
-          queue[tail++] = u;
+        if (lv[u] < 0) {
+          lv[u] = lnext;
+          qu[tail++] = u;
         }
       }
       indeg[v] = d;
     }
-    cnt_buf[b] = tail;
+    cnt[b] = tail;
     return depth;
   };
   auto clear_levels = [&](int b) {
-    for (int i = 0; i < cnt_buf[b]; ++i) level_buf[b][queue_buf[b][i]] = -1;
-    cnt_buf[b] = 0;
+    for (int i = 0; i < cnt[b]; ++i) level[b][queue[b][i]] = -1;
+    cnt[b] = 0;
   };
-  auto md_leaf = [&](const std::vector<int> &S) {
-    const int k = (int)S.size();
+  std::vector<std::vector<int>> la;
+  auto md_leaf = [&](const int *S, int k) {
     const int sid = ++stamp;
     for (int a = 0; a < k; ++a) {
       mark[S[a]] = sid;
@@ -249,112 +266,138 @@ std::vector<int> nd_order_csr(int n, std::vector<int> &xadj0, std::vector<int> &
       uint32_t masks[32];
       for (int a = 0; a < k; ++a) {
         uint32_t mk = 0;
-        for (int p = xadj[S[a]]; p < xadj[S[a] + 1]; ++p)
-          if (mark[adjncy[p]] == sid) mk |= 1u << lidx[adjncy[p]];
+        for (int q = xa[S[a]]; q < xa[S[a] + 1]; ++q)
+          if (mark[ad[q]] == sid) mk |= 1u << lidx[ad[q]];
         masks[a] = mk;
       }
-      md_small(S.data(), k, masks, order);
+      md_small(S, k, masks, order.data(), no);
     } else {
-      std::vector<std::vector<int>> la(k);
+      la.assign(k, {});
       for (int a = 0; a < k; ++a)
-        for (int p = xadj[S[a]]; p < xadj[S[a] + 1]; ++p)
-          if (mark[adjncy[p]] == sid) la[a].push_back(lidx[adjncy[p]]);
-      for (int a : amd_order(k, la)) order.push_back(S[a]);
+        for (int q = xa[S[a]]; q < xa[S[a] + 1]; ++q)
+          if (mark[ad[q]] == sid) la[a].push_back(lidx[ad[q]]);
+      for (int a : amd_order(k, la)) order[no++] = S[a];
     }
   };
   while (!stack.empty()) {
-    Task t = std::move(stack.back());
+    const Task t = stack.back();
     stack.pop_back();
-    std::vector<int> &S = t.v;
+    int *S = arena + t.off;
+    const int ns = t.len;
     if (t.emit) {
-      for (int v : S) order.push_back(v);
+      for (int i = 0; i < ns; ++i) order[no++] = S[i];
       continue;
     }
-    if ((int)S.size() <= kNdLeaf) {
-      md_leaf(S);
+    if (ns <= kNdLeaf) {
+      md_leaf(S, ns);
       continue;
     }
     const int sid = ++stamp;
-    for (int v : S) mark[v] = sid;
+    for (int i = 0; i < ns; ++i) mark[S[i]] = sid;
     clear_levels(0);
     clear_levels(1);
     // connected components (dissect each on its own); the first search also
     // gives every vertex's degree inside the set
     bfs(S[0], sid, 0);
-    if (cnt_buf[0] < (int)S.size()) {
-      std::vector<std::vector<int>> comps;
+    if (cnt[0] < ns) {
+      // components in discovery order, each in its search order, written
+      // back so that the first one is on top
       const int comp_id = ++stamp;  // vertices already assigned get mark comp_id
-      for (int v : S) {
+      int nsc = 0;
+      cstart.clear();
+      for (int i = 0; i < ns; ++i) {
+        const int v = S[i];
         if (mark[v] == comp_id) continue;
         bfs(v, sid, 1);
-        comps.emplace_back(queue_buf[1].begin(), queue_buf[1].begin() + cnt_buf[1]);
-        for (int u : comps.back()) mark[u] = comp_id;
+        cstart.push_back(nsc);
+        for (int j = 0; j < cnt[1]; ++j) {
+          scratch[nsc++] = queue[1][j];
+          mark[queue[1][j]] = comp_id;
+        }
       }
+      cstart.push_back(nsc);
       clear_levels(0);
       clear_levels(1);
-      for (auto it = comps.rbegin(); it != comps.rend(); ++it)
-        stack.push_back({std::move(*it), false});
+      int w = t.off;
+      for (int c = (int)cstart.size() - 2; c >= 0; --c) {
+        const int len = cstart[c + 1] - cstart[c];
+        std::copy(scratch + cstart[c], scratch + cstart[c + 1], arena + w);
+        stack.push_back({w, len, false});
+        w += len;
+      }
       continue;
     }
     // pseudo-peripheral root: a vertex of least degree in the set, then a
     // least-degree vertex of the deepest level while that deepens the
     // structure (three moves at most)
     int root = S[0];
-    for (int v : S)
-      if (indeg[v] < indeg[root]) root = v;
+    for (int i = 0; i < ns; ++i)
+      if (indeg[S[i]] < indeg[root]) root = S[i];
     int cur = 0;
     int depth = bfs(root, sid, cur);
     for (int it = 0; it < 3; ++it) {
-      const std::vector<int> &lv = level_buf[cur], &qu = queue_buf[cur];
+      const int *lv = level[cur], *qu = queue[cur];
       int cand = -1;
-      for (int i = cnt_buf[cur] - 1; i >= 0 && lv[qu[i]] == depth - 1; --i)
+      for (int i = cnt[cur] - 1; i >= 0 && lv[qu[i]] == depth - 1; --i)
         if (cand < 0 || indeg[qu[i]] < indeg[cand]) cand = qu[i];
       const int d2 = bfs(cand, sid, 1 - cur);
       if (d2 <= depth) break;
       depth = d2;
       cur = 1 - cur;
     }
-    const std::vector<int> &level = level_buf[cur];
+    const int *lev = level[cur];
     if (depth < 3) {
-      md_leaf(S);
+      md_leaf(S, ns);
       continue;
     }
-    std::vector<int> lcount(depth, 0);
-    for (int v : S) lcount[level[v]]++;
+    for (int l = 0; l < depth; ++l) lcount[l] = 0;
+    for (int i = 0; i < ns; ++i) lcount[lev[S[i]]]++;
     int ell = 1, cum = 0;
     for (int l = 0; l < depth; ++l) {
       cum += lcount[l];
-      if (2 * cum >= (int)S.size()) {
+      if (2 * cum >= ns) {
         ell = std::max(1, std::min(depth - 2, l));
         break;
       }
     }
-    Task A, B, sep;
-    A.emit = B.emit = false;
-    sep.emit = true;
-    A.v.reserve(S.size());
-    B.v.reserve(S.size());
-    for (int v : S) {
-      const int lv = level[v];
-      if (lv < ell) {
-        A.v.push_back(v);
-      } else if (lv > ell) {
-        B.v.push_back(v);
-      } else {
-        bool touches_next = false;
-        for (int p = xadj[v]; p < xadj[v + 1] && !touches_next; ++p) {
-          const int u = adjncy[p];
-          touches_next = mark[u] == sid && level[u] == ell + 1;
+    // parts A (levels below ell, and the vertices of level ell without a
+    // neighbour in level ell + 1), B (levels above ell) and the separator,
+    // each in the set's order; written back as separator, B, A (A on top)
+    int na = 0, nb = 0, nsep = 0;
+    for (int i = 0; i < ns; ++i) {
+      const int v = S[i];
+      const int lv = lev[v];
+      int part = 0;
+      if (lv > ell) {
+        part = 1;
+      } else if (lv == ell) {
+        for (int q = xa[v]; q < xa[v + 1]; ++q) {
+          const int u = ad[q];
+          if (mark[u] == sid && lev[u] == ell + 1) {
+            part = 2;
+            break;
+          }
         }
-        (touches_next ? sep.v : A.v).push_back(v);
       }
+      lidx[v] = part;
+      na += part == 0;
+      nb += part == 1;
+      nsep += part == 2;
     }
-    stack.push_back(std::move(sep));
-    if (!B.v.empty()) stack.push_back(std::move(B));
-    if (!A.v.empty()) stack.push_back(std::move(A));
+    std::copy(S, S + ns, scratch);
+    int pa = t.off + nsep + nb, pb = t.off + nsep, ps = t.off;
+    for (int i = 0; i < ns; ++i) {
+      const int v = scratch[i];
+      const int part = lidx[v];
+      arena[part == 0 ? pa++ : (part == 1 ? pb++ : ps++)] = v;
+    }
+    stack.push_back({t.off, nsep, true});
+    if (nb) stack.push_back({t.off + nsep, nb, false});
+    if (na) stack.push_back({t.off + nsep + nb, na, false});
   }
   for (int i = 0; i < n; ++i)
-    if (dense[i]) order.push_back(i);
+    if (dense[i]) order[no++] = i;
+  order.resize(no);
   return order;
 }
 
