@@ -131,7 +131,8 @@ class SolverStatus(enum.IntEnum):
     INSUFFICIENT_PROGRESS = 10
 
 
-_METHODS = {"cudss": 0, "gpu": 0, "fp64": 0, "cudssmixed": 1, "gpumixed": 1, "mixed": 1}
+_METHODS = {"cudss": 0, "gpu": 0, "fp64": 0, "cudssmixed": 1, "gpumixed": 1, "mixed": 1,
+            "mixed_f64elim": 2}
 
 
 @dataclass
@@ -139,7 +140,9 @@ class Settings:
     """Solver settings (src/settings.jl:70-148).  ``direct_solve_method``
     accepts the reference names "cudss" (FP64 factorisation) and
     "cudssmixed" (FP32 factorisation + FP64 iterative refinement); both run
-    this library's batched LDL^T."""
+    this library's batched LDL^T.  "mixed_f64elim" is this library's variant
+    of the mixed form: FP64 elimination, the factor stored and applied in
+    FP32, FP64 refinement."""
     max_iter: int = 200
     time_limit: float = float("inf")
     verbose: bool = False

@@ -799,7 +799,8 @@ using namespace clgpu;
 struct clgpu_solver {
   clgpu_settings st{};
   int B = 0, nx = 0, mz = 0;
-  bool mixed = false;
+  bool mixed = false;    // factor stored in FP32
+  bool arith32 = false;  // and eliminated in FP32 arithmetic
   DevArena arena;
   Dev dv{};
   ConeSet cs{};
@@ -2229,7 +2230,13 @@ extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
     h->st = *settings;
   else
     clgpu_default_settings(&h->st);
-  h->mixed = h->st.direct_solve_method == CLGPU_METHOD_MIXED;
+  if (h->st.direct_solve_method < CLGPU_METHOD_FP64 ||
+      h->st.direct_solve_method > CLGPU_METHOD_MIXED_F64ELIM) {
+    delete h;
+    return -1;
+  }
+  h->mixed = h->st.direct_solve_method != CLGPU_METHOD_FP64;
+  h->arith32 = h->st.direct_solve_method == CLGPU_METHOD_MIXED;
   if (h->mixed) h->st.static_regularization_constant = std::sqrt(1.1920928955078125e-07);
   SetupOptions opt;
   opt.soc_threshold = h->st.soc_threshold;
@@ -2327,7 +2334,8 @@ struct Phase {
     h->prof_end(st);
     int *ok = D().I + I_KKT_OK * h->B;
     h->prof_begin(0, st);
-    ldl_factor(h->kk, h->mixed, h->lp, D().active, ok, D().S + F_KKT_EPS * h->B, st);
+    ldl_factor(h->kk, h->mixed, h->lp, D().active, ok, D().S + F_KKT_EPS * h->B, st,
+               h->arith32);
     h->prof_end(st);
     h->launches += 8;
   }

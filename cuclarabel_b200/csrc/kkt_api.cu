@@ -136,7 +136,8 @@ extern "C" int clgpu_ldl_create(int N, const int *Kp, const int *Kj, const signe
   h->d_eps = A.alloc<double>(1);
   std::vector<int> vinst(N, 0);
   h->sn.reset(new SnExec());
-  const bool mixed = st.direct_solve_method == CLGPU_METHOD_MIXED;
+  const bool mixed = st.direct_solve_method == CLGPU_METHOD_MIXED ||
+                     st.direct_solve_method == CLGPU_METHOD_MIXED_F64ELIM;
   if (!sn_exec_create(plan, mixed, 1, 0, N, vinst, A, *h->sn)) return cuda_status(A.err ? A.err : cudaErrorMemoryAllocation);
   k.sn = h->sn.get();
   if (A.err != cudaSuccess) return cuda_status(A.err);

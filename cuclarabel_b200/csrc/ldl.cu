@@ -115,8 +115,24 @@ __device__ __forceinline__ void store_l(T *Lx, double *Lacc, int q, double v) {
   Lx[q] = T(v);
   if (!std::is_same<T, double>::value) Lacc[q] = v;
 }
+// FP32 operations on FP32 values held in FP64 slots (the mixed form's
+// elimination)
+__device__ __forceinline__ double f32r(double x) { return double(float(x)); }
+__device__ __forceinline__ double f32mul(double a, double b) {
+  return double(__fmul_rn(float(a), float(b)));
+}
+__device__ __forceinline__ double f32add(double a, double b) {
+  return double(__fadd_rn(float(a), float(b)));
+}
+__device__ __forceinline__ double f32sub(double a, double b) {
+  return double(__fsub_rn(float(a), float(b)));
+}
+// the pivot the FP32 elimination continues with: its stored inverse
+__device__ __forceinline__ double f32inv(double dj) {
+  return double(float(1.0 / double(float(dj))));
+}
 
-template <typename T, int NT, bool SMEM>
+template <typename T, int NT, bool SMEM, bool AR32 = false>
 __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, LDLParams prm, const int *run,
                                                    int *ok, double *eps_out) {
   int inst = blockIdx.x;
@@ -124,6 +140,9 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
   int N = k.N[inst];
   if (k.cls[inst] != (SMEM ? 1 : 2)) return;
   if (SMEM && k.has_fstream && k.fstream[inst]) return;  // streamed factorisation
+  // AR32: FP32 arithmetic throughout (see k_ldl_factor_stream)
+  static_assert(!AR32 || std::is_same<T, float>::value, "FP32 arithmetic stores FP32");
+  constexpr bool F32 = AR32;
   __shared__ double red[NT / 32 + 1];
   extern __shared__ __align__(16) unsigned char sm_raw[];
   const int vo = k.voff[inst], po = k.poff[inst];
@@ -165,29 +184,45 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
           int c = k.Kj[p];
           if (c < j) continue;
           if (c == j) {
-            dj = k.Kx[p] + (sg[j] > 0 ? eps : -eps);
+            if constexpr (F32)
+              dj = f32add(f32r(k.Kx[p]), f32r(sg[j] > 0 ? eps : -eps));
+            else
+              dj = k.Kx[p] + (sg[j] > 0 ? eps : -eps);
             continue;
           }
           while (q < q1 && k.Li[q] != c) ++q;
-          if (q < q1) Lacc[q] = k.Kx[p];
+          if (q < q1) Lacc[q] = F32 ? f32r(k.Kx[p]) : k.Kx[p];
         }
         for (int r = Rp[j]; r < Rp[j + 1]; ++r) {
           const int kk = k.Rk[r], pos = k.Rpos[r];
           const double ljk = Lacc[pos];
-          const double f = ljk * Dacc[kk];
-          dj -= ljk * f;
+          double f;
+          if constexpr (F32) {
+            f = f32mul(ljk, Dacc[kk]);
+            dj = f32sub(dj, f32mul(ljk, f));
+          } else {
+            f = ljk * Dacc[kk];
+            dj -= ljk * f;
+          }
           const int pe = Lp[kk + 1];
           q = q0;
           for (int p = pos + 1; p < pe; ++p) {
             const int i = k.Li[p];
             while (q < q1 && k.Li[q] != i) ++q;
-            if (q < q1) Lacc[q] -= Lacc[p] * f;
+            if (q < q1) {
+              if constexpr (F32)
+                Lacc[q] = f32sub(Lacc[q], f32mul(Lacc[p], f));
+              else
+                Lacc[q] -= Lacc[p] * f;
+            }
           }
         }
         dj = pivot_value(dj, sg[j], prm);
-        const double dinv = 1.0 / dj;
+        if (F32) dj = f32r(dj);
+        const double dinv = F32 ? f32inv(dj) : 1.0 / dj;
         if (!isfinite(dinv)) finite = false;
-        for (int qq = q0; qq < q1; ++qq) store_l(Lx, Lacc, qq, Lacc[qq] * dinv);
+        for (int qq = q0; qq < q1; ++qq)
+          store_l(Lx, Lacc, qq, F32 ? f32mul(Lacc[qq], dinv) : Lacc[qq] * dinv);
         if (!store_pivot(D, Dinv, Dacc, j, dj)) finite = false;
       }
       bar_sync<NT>();
@@ -198,9 +233,10 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
         for (int p = Kp[j] + tid; p < Kp[j + 1]; p += NT) {
           int c = k.Kj[p];
           if (c > j)
-            w[c] = k.Kx[p];
+            w[c] = F32 ? f32r(k.Kx[p]) : k.Kx[p];
           else if (c == j)
-            w[c] = k.Kx[p] + (sg[j] > 0 ? eps : -eps);
+            w[c] = F32 ? f32add(f32r(k.Kx[p]), f32r(sg[j] > 0 ? eps : -eps))
+                       : k.Kx[p] + (sg[j] > 0 ? eps : -eps);
         }
         bar_sync<NT>();
         // update columns applied one after another (threads over the rows
@@ -216,7 +252,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
             mypos = k.Rpos[rb + lane];
             myend = Lp[kk + 1];
             myl = Lacc[mypos];
-            myf = myl * Dacc[kk];
+            myf = F32 ? f32mul(myl, Dacc[kk]) : myl * Dacc[kk];
           }
           const int cnt = min(32, r1 - rb);
           for (int t = 0; t < cnt; ++t) {
@@ -224,17 +260,24 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 20 : 4) k_ldl_factor(KKTDev k, 
             const int pe = __shfl_sync(0xffffffffu, myend, t);
             const double f = __shfl_sync(0xffffffffu, myf, t);
             const double ljk = __shfl_sync(0xffffffffu, myl, t);
-            if (tid == 0) w[j] -= ljk * f;
-            for (int p = pos + 1 + tid; p < pe; p += NT) w[k.Li[p]] -= Lacc[p] * f;
+            if constexpr (F32) {
+              if (tid == 0) w[j] = f32sub(w[j], f32mul(ljk, f));
+              for (int p = pos + 1 + tid; p < pe; p += NT)
+                w[k.Li[p]] = f32sub(w[k.Li[p]], f32mul(Lacc[p], f));
+            } else {
+              if (tid == 0) w[j] -= ljk * f;
+              for (int p = pos + 1 + tid; p < pe; p += NT) w[k.Li[p]] -= Lacc[p] * f;
+            }
             bar_sync<NT>();
           }
         }
-        const double dj = pivot_value(w[j], sg[j], prm);
-        const double dinv = 1.0 / dj;
+        double dj = pivot_value(w[j], sg[j], prm);
+        if (F32) dj = f32r(dj);
+        const double dinv = F32 ? f32inv(dj) : 1.0 / dj;
         if (!isfinite(dinv)) finite = false;
         for (int q = Lp[j] + tid; q < Lp[j + 1]; q += NT) {
           const int i = k.Li[q];
-          store_l(Lx, Lacc, q, w[i] * dinv);
+          store_l(Lx, Lacc, q, F32 ? f32mul(w[i], dinv) : w[i] * dinv);
           w[i] = 0.0;
         }
         bar_sync<NT>();
@@ -517,6 +560,23 @@ __device__ __forceinline__ void seg_scan2(double xA, double xB, int pA, int pB, 
   sB = v;
   const double prev = __shfl_up_sync(0xffffffffu, v, 1);
   sA = (pA > 0 && lane > 0) ? __dadd_rn(xA, prev) : xA;
+}
+// The same scan in FP32 arithmetic (the mixed form's factorisation).
+__device__ __forceinline__ void seg_scan2(float xA, float xB, int pA, int pB, int lane,
+                                          float carry, int nsteps, float &sA, float &sB) {
+  if (lane == 0 && pA > 0) xA = __fadd_rn(xA, carry);
+  float v = pB > 0 ? __fadd_rn(xA, xB) : xB;
+  const int reach = pB > 0 ? lane - ((2 * lane + 1 - pB) >> 1) : 0;
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    if (s >= nsteps) break;
+    const int d = 1 << s;
+    const float o = __shfl_up_sync(0xffffffffu, v, d);
+    if (d <= reach && d <= lane) v = __fadd_rn(v, o);
+  }
+  sB = v;
+  const float prev = __shfl_up_sync(0xffffffffu, v, 1);
+  sA = (pA > 0 && lane > 0) ? __fadd_rn(xA, prev) : xA;
 }
 
 // Segmented sums of one solve chunk held kSK consecutive entries per lane
@@ -956,12 +1016,21 @@ __global__ void __launch_bounds__(32 * kSolveWarps, kSolveBlocksPerSM)
 // updates read them).  Updates of a level only read columns and pivots of
 // lower levels, all final.  At the end L = U / d is written in CSC order and
 // in the two substitution-stream orders.
+// T is the storage type of L, D and D^-1.  AR32 (with T = float) is the
+// mixed form: the factorisation itself runs in FP32 arithmetic (the KKT
+// values rounded to FP32, every product, sum and pivot inverse an FP32
+// operation; V keeps FP32 values in its FP64 slots), as the FP32 sparse
+// factorisation of the reference's mixed form does.  T = float without
+// AR32 eliminates in FP64 and stores the factor in FP32.
 constexpr int kFRing = kFRingSlots;
 
-template <typename T>
+template <typename T, bool AR32 = false>
 __global__ void __launch_bounds__(32 * kFactorWarps, 6)
     k_ldl_factor_stream(KKTDev k, LDLParams prm, const int *run, int *ok, double *eps_out) {
   constexpr int NT = 32 * kFactorWarps;
+  static_assert(!AR32 || std::is_same<T, float>::value, "FP32 arithmetic stores FP32");
+  constexpr bool F32 = AR32;
+  using A = typename std::conditional<AR32, float, double>::type;  // elimination arithmetic
   const int inst = k.fs_inst[blockIdx.x];
   if (!run[inst]) return;  // the whole block
   __shared__ double red[kFactorWarps + 1];
@@ -991,14 +1060,19 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
 #pragma unroll
     for (int u = 0; u < kU; ++u)
       if (kd[u] >= 0) {
-        V[j0 + NT * u] = kv[u];
+        V[j0 + NT * u] = F32 ? double(float(kv[u])) : kv[u];
         mx = fmax(mx, fabs(kv[u]));
       }
   }
   double eps = 0.0;
   mx = block_max<NT>(mx, red);  // synchronises the block
   if (prm.static_reg) eps = prm.static_c + prm.static_prop * mx;
-  for (int j = tid; j < N; j += NT) V[j] += sg[j] > 0 ? eps : -eps;
+  if constexpr (F32) {
+    const float ef = float(eps);
+    for (int j = tid; j < N; j += NT) V[j] = double(__fadd_rn(float(V[j]), sg[j] > 0 ? ef : -ef));
+  } else {
+    for (int j = tid; j < N; j += NT) V[j] += sg[j] > 0 ? eps : -eps;
+  }
   {
     const int *kp = k.Lkpos + lbase;
     int pos[8];
@@ -1007,7 +1081,10 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
       for (int u = 0; u < 8; ++u) pos[u] = e0 + NT * u < nl ? kp[e0 + NT * u] : -1;
 #pragma unroll
       for (int u = 0; u < 8; ++u)
-        if (e0 + NT * u < nl) V[N + e0 + NT * u] = pos[u] >= 0 ? k.Kx[pos[u]] : 0.0;
+        if (e0 + NT * u < nl) {
+          const double kx = pos[u] >= 0 ? k.Kx[pos[u]] : 0.0;
+          V[N + e0 + NT * u] = F32 ? double(float(kx)) : kx;
+        }
     }
   }
   __syncthreads();
@@ -1048,7 +1125,7 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
 #pragma unroll
   for (int c = 0; c < kFRing; ++c) issue(c, c);
   int c = 0;
-  double carry = 0.0;
+  A carry = A(0);
   // one chunk of the stream: updates (segmented scan, one write per target)
   // or pivots
   auto step = [&]() {
@@ -1084,24 +1161,38 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
           const T dis = T(1.0 / double(djs));
           D[j] = djs;
           Dinv[j] = dis;
-          const double r = 1.0 / dj;
+          // FP32: the stored pivot and its stored inverse are the
+          // elimination's values
+          const double r = F32 ? double(dis) : 1.0 / dj;
           if (!isfinite(r) || !isfinite(double(djs)) || !isfinite(double(dis))) finite = false;
           V[j] = r;
         }
       }
-      carry = 0.0;
+      carry = A(0);
     } else {
       // each target is written once per level (by its last update), so its
       // old value is read before the scan, off the dependent chain
       const bool wA = vA && ((oA.w >> kLastBit) & 1), wB = vB && ((oB.w >> kLastBit) & 1);
-      const double tA = wA ? V[oA.x] : 0.0, tB = wB ? V[oB.x] : 0.0;
-      const double xA = vA ? __dmul_rn(__dmul_rn(V[oA.y], V[oA.z]), V[oA.w & 0xffff]) : 0.0;
-      const double xB = vB ? __dmul_rn(__dmul_rn(V[oB.y], V[oB.z]), V[oB.w & 0xffff]) : 0.0;
-      double sA, sB;
+      const A tA = wA ? A(V[oA.x]) : A(0), tB = wB ? A(V[oB.x]) : A(0);
+      A xA, xB, sA, sB;
+      if constexpr (F32) {
+        xA = vA ? __fmul_rn(__fmul_rn(float(V[oA.y]), float(V[oA.z])), float(V[oA.w & 0xffff]))
+                : 0.f;
+        xB = vB ? __fmul_rn(__fmul_rn(float(V[oB.y]), float(V[oB.z])), float(V[oB.w & 0xffff]))
+                : 0.f;
+      } else {
+        xA = vA ? __dmul_rn(__dmul_rn(V[oA.y], V[oA.z]), V[oA.w & 0xffff]) : 0.0;
+        xB = vB ? __dmul_rn(__dmul_rn(V[oB.y], V[oB.z]), V[oB.w & 0xffff]) : 0.0;
+      }
       seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
                 (int)((w >> kStepShift) & 7u), sA, sB);
-      if (wA) V[oA.x] = __dsub_rn(tA, sA);
-      if (wB) V[oB.x] = __dsub_rn(tB, sB);
+      if constexpr (F32) {
+        if (wA) V[oA.x] = double(__fsub_rn(tA, sA));
+        if (wB) V[oB.x] = double(__fsub_rn(tB, sB));
+      } else {
+        if (wA) V[oA.x] = __dsub_rn(tA, sA);
+        if (wB) V[oB.x] = __dsub_rn(tB, sB);
+      }
       const int ll = (cnt - 1) >> 1;
       carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
     }
@@ -1139,10 +1230,17 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
       for (int u = 0; u < kU; ++u) {
         const int e = e0 + NT * u;
         if (e < nl) {
-          const double l = V[N + (bq[u] - lbase)] * V[be[u].x & 0xffff];
-          Lx[bq[u]] = T(l);
-          LxB[lbase + e] = T(l);
-          LxF[lbase + e] = T(V[N + (fq[u] - lbase)] * V[fe[u].y]);
+          if constexpr (F32) {
+            const float l = __fmul_rn(float(V[N + (bq[u] - lbase)]), float(V[be[u].x & 0xffff]));
+            Lx[bq[u]] = l;
+            LxB[lbase + e] = l;
+            LxF[lbase + e] = __fmul_rn(float(V[N + (fq[u] - lbase)]), float(V[fe[u].y]));
+          } else {
+            const double l = V[N + (bq[u] - lbase)] * V[be[u].x & 0xffff];
+            Lx[bq[u]] = T(l);
+            LxB[lbase + e] = T(l);
+            LxF[lbase + e] = T(V[N + (fq[u] - lbase)] * V[fe[u].y]);
+          }
         }
       }
     }
@@ -1164,17 +1262,17 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
 }
 
 // dynamic shared memory = the largest single-warp instance's work vector
-template <typename T>
+template <typename T, bool AR32>
 static void launch_factor(const KKTDev &k, const LDLParams &p, const int *run, int *ok,
                           double *eps_out, cudaStream_t st) {
   size_t sm = ((size_t)k.max_small_N * sizeof(double) + 15) & ~(size_t)15;
   if (k.has_fstream)
-    k_ldl_factor_stream<T><<<k.fs_count, 32 * kFactorWarps, k.fs_smem, st>>>(k, p, run, ok,
-                                                                           eps_out);
+    k_ldl_factor_stream<T, AR32><<<k.fs_count, 32 * kFactorWarps, k.fs_smem, st>>>(
+        k, p, run, ok, eps_out);
   if (k.has_small_legacy)
-    k_ldl_factor<T, kSmallNT, true><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
+    k_ldl_factor<T, kSmallNT, true, AR32><<<k.B, kSmallNT, sm, st>>>(k, p, run, ok, eps_out);
   if (k.has_large)
-    k_ldl_factor<T, kLargeNT, false><<<k.B, kLargeNT, 0, st>>>(k, p, run, ok, eps_out);
+    k_ldl_factor<T, kLargeNT, false, AR32><<<k.B, kLargeNT, 0, st>>>(k, p, run, ok, eps_out);
 }
 template <typename T>
 static void launch_solve(const KKTDev &k, const LDLParams &p, const int *run,
@@ -1207,13 +1305,19 @@ static void launch_solve2(const KKTDev &k, const LDLParams &p, const int *run,
 static bool g_attr_done = false;
 static void set_attrs() {
   if (g_attr_done) return;
-  cudaFuncSetAttribute(k_ldl_factor_stream<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       96 * 1024 + 64);
-  cudaFuncSetAttribute(k_ldl_factor_stream<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       96 * 1024 + 64);
-  cudaFuncSetAttribute(k_ldl_factor<double, kSmallNT, true>,
+  auto stream_attrs = [](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024 + 64);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+  };
+  stream_attrs(k_ldl_factor_stream<double, false>);
+  stream_attrs(k_ldl_factor_stream<float, false>);
+  stream_attrs(k_ldl_factor_stream<float, true>);
+  cudaFuncSetAttribute(k_ldl_factor<double, kSmallNT, true, false>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
-  cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true>,
+  cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
+  cudaFuncSetAttribute(k_ldl_factor<float, kSmallNT, true, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimitBytes);
   // the packed kernels size their blocks for the SM's full shared memory
   auto solve_attrs = [](auto kern) {
@@ -1225,22 +1329,18 @@ static void set_attrs() {
   solve_attrs(k_ldl_solve_warp<float, 1>);
   solve_attrs(k_ldl_solve_warp<double, 2>);
   solve_attrs(k_ldl_solve_warp<float, 2>);
-  cudaFuncSetAttribute(k_ldl_factor_stream<double>,
-                       cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
-  cudaFuncSetAttribute(k_ldl_factor_stream<float>,
-                       cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
   g_attr_done = true;
 }
 
 void ldl_factor(const KKTDev &k, bool fp32, const LDLParams &p, const int *run, int *ok,
-                double *eps_out, cudaStream_t st) {
+                double *eps_out, cudaStream_t st, bool arith32) {
   set_attrs();
-  if (fp32)
-    launch_factor<float>(k, p, run, ok, eps_out, st);
+  if (fp32 && arith32)
+    launch_factor<float, true>(k, p, run, ok, eps_out, st);
+  else if (fp32)
+    launch_factor<float, false>(k, p, run, ok, eps_out, st);
   else
-    launch_factor<double>(k, p, run, ok, eps_out, st);
+    launch_factor<double, false>(k, p, run, ok, eps_out, st);
   if (k.sn) sn_factor(*k.sn, k, p, run, ok, eps_out, st);
 }
 

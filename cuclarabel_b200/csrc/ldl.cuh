@@ -186,9 +186,11 @@ struct LDLParams {
 
 // numeric refactorisation of every instance with run[i] != 0; sets
 // ok[i] = 0 if a pivot is not finite; eps_out[i] receives the static
-// regulariser used (diagonal_regularizer of the reference)
+// regulariser used (diagonal_regularizer of the reference).  fp32 stores the
+// factor in FP32; arith32 (with fp32) also eliminates in FP32 arithmetic,
+// otherwise the elimination is FP64.
 void ldl_factor(const KKTDev &k, bool fp32, const LDLParams &p, const int *run,
-                int *ok, double *eps_out, cudaStream_t st);
+                int *ok, double *eps_out, cudaStream_t st, bool arith32 = false);
 // solve K [lx; lz; *] = [rx; rz; 0] with iterative refinement for every
 // instance with run[i] != 0.  rx/lx are indexed by global x index, rz/lz by
 // global s/z row; lx or lz may be null.  ok[i] cleared on non-finite results.

@@ -46,8 +46,18 @@ enum {
 /* direct_solve_method (src/settings.jl:113-114, gpu_solver_list of
  * src/Clarabel.jl:27).  The reference names :cudss and :cudssmixed; this
  * library's own batched LDL^T takes their place with the same precision
- * policy. */
-enum { CLGPU_METHOD_FP64 = 0 /* :cudss */, CLGPU_METHOD_MIXED = 1 /* :cudssmixed */ };
+ * policy: CLGPU_METHOD_MIXED factors in FP32 arithmetic and stores the
+ * factor in FP32, refinement in FP64 (directldl_mixed_cudss.jl:42-78).
+ * CLGPU_METHOD_MIXED_F64ELIM is this library's variant of it: the
+ * elimination in FP64, the factor stored and applied in FP32, refinement in
+ * FP64 (the same factor bytes for the solves, a more accurate factor).  Both
+ * set the static regularisation to sqrt(eps(Float32)) (src/solver.jl:609-611);
+ * instances on the supernodal factorisation factor in FP32 under both. */
+enum {
+  CLGPU_METHOD_FP64 = 0 /* :cudss */,
+  CLGPU_METHOD_MIXED = 1 /* :cudssmixed */,
+  CLGPU_METHOD_MIXED_F64ELIM = 2
+};
 
 /* mirrors Settings (src/settings.jl:70-148), numeric fields only */
 typedef struct {

@@ -74,7 +74,11 @@ typedef struct {
    *    norms, src/problemdata.jl:337-338) */
   int gpu_equilibration;
   /* 1: round L, D to FP32 after every factorisation (models a factor held
-   *    in single precision; refinement stays FP64) */
+   *    in single precision; refinement stays FP64)
+   * 2: the factorisation in FP32 arithmetic (the KKT values rounded to FP32,
+   *    every operation of the elimination an FP32 one), as the FP32 sparse
+   *    factorisation of the reference's mixed form
+   *    (directldl_mixed_cudss.jl:42-78); refinement stays FP64 */
   int factor_fp32;
 } oracle_settings;
 

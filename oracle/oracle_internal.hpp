@@ -129,6 +129,7 @@ struct LDL {
   std::vector<int> Dsigns;                // permuted signs
   bool reg_enable = true;
   bool round_fp32 = false;
+  bool arith_fp32 = false;  // the elimination itself in FP32 arithmetic
   double reg_eps = 1e-13, reg_delta = 2e-7;
   int reg_count = 0;
   // workspaces
@@ -141,6 +142,7 @@ struct LDL {
   void update_value(int kidx, double v);
   void scale_values(const std::vector<int> &kidx, double scale, int count);
   bool refactor();
+  bool refactor_fp32();
   void solve(double *x) const;  // in place
 };
 

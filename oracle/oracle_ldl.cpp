@@ -144,7 +144,10 @@ void LDL::scale_values(const std::vector<int> &kidx, double scale, int count) {
 }
 
 // QDLDL_factor restated: up-looking, row k of L by sparse triangular solve.
+// With arith_fp32 every value is an FP32 one and every operation an FP32
+// operation (refactor_fp32).
 bool LDL::refactor() {
+  if (arith_fp32) return refactor_fp32();
   const int UNUSED = 0, USED = 1;
   reg_count = 0;
   std::fill(bwork.begin(), bwork.end(), UNUSED);
@@ -199,6 +202,73 @@ bool LDL::refactor() {
       D[k] = (double)(float)D[k];
       Dinv[k] = (double)(float)(1.0 / D[k]);
     }
+  }
+  for (int k = 0; k < n; ++k)
+    if (!std::isfinite(Dinv[k])) return false;
+  return true;
+}
+
+// The same elimination in FP32 arithmetic: values rounded to FP32 as they
+// enter, each product and difference an FP32 operation, the pivot inverse
+// the FP32 rounding of 1 / d.  L, D and D^-1 hold the FP32 values.
+bool LDL::refactor_fp32() {
+  const int UNUSED = 0, USED = 1;
+  reg_count = 0;
+  std::vector<float> fw(n, 0.f), Lf(Lx.size(), 0.f), Df(n, 0.f), Dif(n, 0.f);
+  std::fill(bwork.begin(), bwork.end(), UNUSED);
+  for (int i = 0; i < n; ++i) nextcol[i] = Lp[i];
+  for (int k = 0; k < n; ++k) {
+    int nnzY = 0;
+    float dk = 0.f;
+    for (int p = Ap[k]; p < Ap[k + 1]; ++p) {
+      int b = Ai[p];
+      if (b == k) {
+        dk += (float)Ax[p];
+        continue;
+      }
+      fw[b] = (float)Ax[p];
+      int nx = b;
+      if (bwork[nx] == UNUSED) {
+        bwork[nx] = USED;
+        ebuf[0] = nx;
+        int nnzE = 1;
+        nx = etree[b];
+        while (nx != -1 && nx < k) {
+          if (bwork[nx] == USED) break;
+          bwork[nx] = USED;
+          ebuf[nnzE++] = nx;
+          nx = etree[nx];
+        }
+        while (nnzE) yidx[nnzY++] = ebuf[--nnzE];
+      }
+    }
+    for (int i = nnzY - 1; i >= 0; --i) {
+      int c = yidx[i];
+      int t = nextcol[c];
+      const float yc = fw[c];
+      for (int j = Lp[c]; j < t; ++j) {
+        const volatile float prod = Lf[j] * yc;  // no contraction into an FMA
+        fw[Li[j]] -= prod;
+      }
+      Li[t] = k;
+      Lf[t] = yc * Dif[c];
+      const volatile float prod = yc * Lf[t];
+      dk -= prod;
+      nextcol[c]++;
+      fw[c] = 0.f;
+      bwork[c] = UNUSED;
+    }
+    if (reg_enable && (double)dk * Dsigns[k] <= reg_eps) {
+      dk = (float)(reg_delta * Dsigns[k]);
+      ++reg_count;
+    }
+    Df[k] = dk;
+    Dif[k] = (float)(1.0 / (double)dk);
+  }
+  for (size_t q = 0; q < Lx.size(); ++q) Lx[q] = Lf[q];
+  for (int k = 0; k < n; ++k) {
+    D[k] = Df[k];
+    Dinv[k] = Dif[k];
   }
   for (int k = 0; k < n; ++k)
     if (!std::isfinite(Dinv[k])) return false;

@@ -237,6 +237,7 @@ struct KKTSolver {
     ldl.reg_eps = st->dynamic_regularization_eps;
     ldl.reg_delta = st->dynamic_regularization_delta;
     ldl.round_fp32 = st->factor_fp32 != 0;
+    ldl.arith_fp32 = st->factor_fp32 == 2;
     ldl.setup(N, K.p, K.i, Dsigns);
     for (int q = 0; q < K.p[N]; ++q) ldl.Ax[ldl.mapK[q]] = K.x[q];
   }
