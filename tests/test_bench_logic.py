@@ -163,7 +163,7 @@ def test_slot_lane_warm_serves_one_request_outside_the_stats():
 
 def test_mixed_precision_error_summary():
     """obj_errors compares only instances converged by the run (SOLVED or
-    ALMOST_SOLVED) and SOLVED by the reference; status_counts names them."""
+    ALMOST_SOLVED) and SOLVED by the reference; status_mix names them."""
     st = np.array([1, 4, 10, 1], np.int32)  # SOLVED, ALMOST_SOLVED, INSUFFICIENT, SOLVED
     info = np.zeros(4, [("obj_val", "f8")])
     info["obj_val"] = [1.0, 2.0 + 2e-5, 50.0, -3.0]
@@ -173,5 +173,5 @@ def test_mixed_precision_error_summary():
     e = bench.obj_errors(res, ref_solved, ref_obj)
     assert e["instances"] == 2
     assert abs(e["max"] - 1e-5) < 1e-12
-    assert bench.status_counts(st) == {"SOLVED": 2, "ALMOST_SOLVED": 1,
+    assert bench.status_mix(st) == {"SOLVED": 2, "ALMOST_SOLVED": 1,
                                        "INSUFFICIENT_PROGRESS": 1}
