@@ -434,6 +434,16 @@ def cpu_baseline_sample(count):
 METRIC = "solves/s at 1e-8 (batched MPC QP/SOCP)"
 
 
+def pinned_stats():
+    """Counters of the library's page-locked host pool (reused, new, bytes,
+    failed)."""
+    import ctypes
+    from cuclarabel_b200 import _lib
+    out = (ctypes.c_longlong * 4)()
+    _lib.load().clgpu_debug_pinned_stats(out)
+    return list(out)
+
+
 def status_mix(status):
     from cuclarabel_b200 import SolverStatus
     out = {}
@@ -976,14 +986,23 @@ def main():
     # cold path for reference: Solver(...) setup from host CSC data + solve +
     # solutions, one pass
     torch.cuda.synchronize()
+    pool0 = pinned_stats()
     t0 = time.perf_counter()
     s3 = BatchSolver(pbs, direct_solve_method=args.method)
+    t1 = time.perf_counter()
+    pool1 = pinned_stats()
     s3.solve_only(sh)
+    t2 = time.perf_counter()
     res3 = s3.results()
     cold_t = time.perf_counter() - t0
     cold = {"value": float(np.sum(res3["status"] == int(SolverStatus.SOLVED))) / cold_t,
-            "unit": "solves/s", "note": "one pass: Solver(...) setup from host CSC data "
-                                        "(equilibration, ordering, symbolic LDL) + solve!"}
+            "unit": "solves/s", "setup_s": t1 - t0, "solve_s": t2 - t1,
+            "results_s": cold_t - (t2 - t0),
+            "pinned_pool": {"reused": pool1[0] - pool0[0], "new": pool1[1] - pool0[1],
+                            "new_mb": (pool1[2] - pool0[2]) / 2**20,
+                            "failed": pool1[3] - pool0[3], "held_mb": pool1[2] / 2**20},
+            "note": "one pass: Solver(...) setup from host CSC data (equilibration, "
+                    "ordering, symbolic LDL) + solve! + results"}
     del s3
 
     # ---- mixed precision: direct_solve_method = :cudssmixed (FP32

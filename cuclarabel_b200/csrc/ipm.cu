@@ -865,6 +865,7 @@ struct clgpu_solver {
   bool serving = false;
   // the pass as a CUDA graph (index 1: with the serving finished-list)
   bool use_graphs = true;
+  int solves_done = 0;  // completed clgpu_solver_solve calls
   cudaGraphExec_t pass_exec[2] = {nullptr, nullptr};
   long long pass_launches = 0;
   Dev dv_admit{};
@@ -2534,13 +2535,18 @@ static void ipm_pass_kernels(clgpu_solver *h, Phase &P, cudaStream_t st, double 
 // h->h_list (count in *nfin).  Without host decisions inside the pass (no
 // asymmetric-cone backtracking, no profiling or tracing, no time limit) the
 // pass is captured once as a CUDA graph and replayed: one launch instead of
-// ~60.
+// ~60.  A solver's first solve launches kernel by kernel: capturing and
+// instantiating the graph costs more than the launches of one solve, so a
+// solver used once (a cold pass) never pays it; the second solve captures.
+// The serving steps capture at once (their lanes warm up before serving, and
+// no capture may be open while other threads allocate).
 static int ipm_pass(clgpu_solver *h, Phase &P, cudaStream_t st, double elapsed, bool serve,
                     int *nfin) {
   Dev &dv = h->dv;
   const int B = h->B;
   const bool graph = h->use_graphs && !h->any_asym && !h->any_sn && !h->profiling && !h->st.verbose &&
-                     !std::isfinite(h->st.time_limit) && h->mask_sel == nullptr;
+                     !std::isfinite(h->st.time_limit) && h->mask_sel == nullptr &&
+                     (serve || h->solves_done > 0);
   bool done = false;
   if (graph) {
     cudaGraphExec_t &ex = h->pass_exec[serve ? 1 : 0];
@@ -2652,6 +2658,7 @@ extern "C" int clgpu_solver_solve(clgpu_solver *h, clgpu_stream_t stream) {
     if (ipm_pass(h, P, st, elapsed, false, nullptr) == 0) break;
   }
   h->passes = passes;
+  ++h->solves_done;
   if (h->profiling) {
     cudaStreamSynchronize(st);
     h->prof_collect();

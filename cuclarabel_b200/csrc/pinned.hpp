@@ -36,17 +36,31 @@ class PinnedPool {
         void *p = fl.back();
         fl.pop_back();
         cls_of_[p] = cls;
+        ++reused_;
         return p;
       }
     }
     void *p = nullptr;
     if (cudaMallocHost(&p, cls) != cudaSuccess) {
       cudaGetLastError();
+      std::lock_guard<std::mutex> lk(mu_);
+      ++failed_;
       return nullptr;
     }
     std::lock_guard<std::mutex> lk(mu_);
     cls_of_[p] = cls;
+    ++pinned_;
+    pinned_bytes_ += (long long)cls;
     return p;
+  }
+  // takes served from the pool, page-locked allocations made, bytes
+  // page-locked in all, failed allocations
+  void stats(long long out[4]) {
+    std::lock_guard<std::mutex> lk(mu_);
+    out[0] = reused_;
+    out[1] = pinned_;
+    out[2] = pinned_bytes_;
+    out[3] = failed_;
   }
   // returns p to the pool (false when p is not a pool buffer); a buffer
   // held for an owner's copies waits until the owner settles
@@ -97,6 +111,7 @@ class PinnedPool {
   std::map<size_t, std::vector<void *>> free_;
   std::map<void *, size_t> cls_of_;
   std::map<void *, const void *> held_;
+  long long reused_ = 0, pinned_ = 0, pinned_bytes_ = 0, failed_ = 0;
   std::map<const void *, std::vector<std::pair<void *, size_t>>> deferred_;
 };
 

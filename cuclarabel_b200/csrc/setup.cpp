@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <set>
 
+#include "pinned.hpp"
 #include "setup.hpp"
 
 namespace clgpu {
@@ -975,6 +976,12 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
 // Host replay of the device factorisation/solve on the prepared structures.
 // Used by tests (no GPU needed) to validate the ordering, symbolic
 // factorisation and every refresh map before any kernel reads them.
+extern "C" int clgpu_debug_pinned_stats(long long *out) {
+  if (!out) return -1;
+  clgpu::PinnedPool::get().stats(out);
+  return 0;
+}
+
 extern "C" int clgpu_debug_instance_path(const clgpu_problem *pb, const clgpu_settings *st,
                                          int *supernodal, long long *factor_entries) {
   using namespace clgpu;

@@ -461,6 +461,13 @@ int clgpu_debug_check_instance(const clgpu_problem *prob,
  * factor's strictly-lower entries.  Needs no GPU. */
 int clgpu_debug_instance_path(const clgpu_problem *prob, const clgpu_settings *settings,
                               int *supernodal, long long *factor_entries);
+/* Counters of the process-wide page-locked host pool that setup arrays,
+ * upload staging and result staging come from (diagnostic, no reference
+ * counterpart): out[0] buffers served from the pool, out[1] page-locked
+ * allocations made, out[2] bytes page-locked in all (the pool never
+ * shrinks), out[3] failed allocations (heap memory used instead).  Needs no
+ * GPU. */
+int clgpu_debug_pinned_stats(long long *out);
 
 #ifdef __cplusplus
 }

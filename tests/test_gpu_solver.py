@@ -164,15 +164,16 @@ def test_fused_constant_and_affine_solves_are_bitwise_separate_solves(cuda_devic
 
 
 def test_graph_replayed_pass_equals_direct_launches(cuda_device):
-    """The IPM pass is captured once as a CUDA graph and replayed; a profiled
-    solve launches the same kernels one by one.  Results must agree bitwise."""
+    """From a solver's second solve on, the IPM pass is captured once as a
+    CUDA graph and replayed; the first solve and a profiled solve launch the
+    same kernels one by one.  Results must agree bitwise."""
     pbs = problems.mpc_batch(16, seed0=400)
     s = BatchSolver(pbs)
-    a = s.solve()                 # captured and replayed
+    a = s.solve()                 # first solve: launched kernel by kernel
     s.set_profiling(True)
-    b = s.solve()                 # launched kernel by kernel
+    b = s.solve()                 # launched kernel by kernel (profiled)
     s.set_profiling(False)
-    c = s.solve()                 # replayed again
+    c = s.solve()                 # captured and replayed
     for x, y, z in zip(a, b, c):
         assert x.status == y.status == z.status and x.iterations == y.iterations
         assert np.array_equal(x.x, y.x) and np.array_equal(x.x, z.x)
