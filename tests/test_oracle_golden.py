@@ -48,3 +48,21 @@ def test_oracle_cone_identities():
     # mul_Hs agrees with the dense form
     x = rng.standard_normal(d)
     assert np.allclose(C.mul_Hs(x), H @ x, atol=1e-12)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_oracle_fp32_factorisation_model(case):
+    """The oracle's model of the mixed form (factor_fp32 = 2: the elimination
+    in FP32 arithmetic, FP64 refinement, static regularisation
+    sqrt(eps(Float32)) as src/solver.jl:609-611 sets it) reaches the FP64
+    status on the reference's golden cases, ALMOST_SOLVED counting for
+    SOLVED, and the FP64 objective to 1e-5."""
+    name, P, q, A, b, cones, e = case
+    ref = oracle.solve(P, q, A, b, cones)
+    r32 = oracle.solve(P, q, A, b, cones, factor_fp32=2,
+                       static_regularization_constant=float(np.sqrt(np.finfo(np.float32).eps)))
+    if ref["status_name"] == "SOLVED":
+        assert r32["status_name"] in ("SOLVED", "ALMOST_SOLVED"), name
+        assert abs(r32["obj_val"] - ref["obj_val"]) <= 1e-5 * max(1.0, abs(ref["obj_val"])), name
+    else:
+        assert r32["status_name"] == ref["status_name"], name
