@@ -15,6 +15,11 @@ import scipy.sparse as sp
 
 from . import _lib
 
+try:
+    from . import _pack  # compiled problem packer (csrc/pack.c)
+except ImportError:  # not built: the general packing path below
+    _pack = None
+
 
 # ---------------------------------------------------------------- cones
 class SupportedCone:
@@ -296,9 +301,19 @@ _PROBLEM_DTYPE = np.dtype([
 
 
 def _pack_batch(problems):
-    """clgpu_problem array for a batch: each field's arrays are concatenated
-    once and every instance's pointers are computed from offsets, so the
-    per-instance host cost is the validation alone."""
+    """clgpu_problem array for a batch.  The compiled packer (csrc/pack.c)
+    points the structs straight at the problems' own arrays when every
+    problem is a (P, q, A, b, cones) tuple of canonical CSC matrices and
+    float64 vectors; otherwise each field's arrays are concatenated once and
+    every instance's pointers are computed from offsets."""
+    if _pack is not None:
+        arr = np.zeros(len(problems), _PROBLEM_DTYPE)
+        r = _pack.pack(problems, arr)
+        if r is not None:
+            ct, cd, cp, dims, pn, an = r
+            d = np.frombuffer(dims, np.int32)[:2 * len(problems)].reshape(-1, 2)
+            keep = {"arr": arr, "ct": ct, "cd": cd, "cp": cp, "problems": problems}
+            return arr, keep, list(map(tuple, d.tolist())), (int(pn), int(an))
     parts = {k: [] for k in ("Pp", "Pi", "Px", "q", "Ap", "Ai", "Ax", "b")}
     ct, cd, cp = [], [], []
     nm = np.zeros((len(problems), 3), np.int64)

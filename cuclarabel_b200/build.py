@@ -32,6 +32,24 @@ def _headers():
             + glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
+def build_pack(verbose=False):
+    """The CPython extension that packs a batch's problem structs
+    (csrc/pack.c), compiled in place with the host compiler."""
+    import sysconfig
+    src = os.path.join(CSRC, "pack.c")
+    out = os.path.join(HERE, "_pack" + sysconfig.get_config_var("EXT_SUFFIX"))
+    deps = [src, os.path.join(ROOT, "include", "clgpu.h")]
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    cc = os.environ.get("CC", shutil.which("gcc") or "cc")
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-I" + sysconfig.get_paths()["include"],
+           "-I" + os.path.join(ROOT, "include"), src, "-o", out]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return out
+
+
 def build(verbose=False, ptxas_info=False):
     os.makedirs(BUILD, exist_ok=True)
     hdr_mtime = max([os.path.getmtime(h) for h in _headers()] + [0])
@@ -48,6 +66,7 @@ def build(verbose=False, ptxas_info=False):
         if verbose or ptxas_info:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
+    build_pack(verbose)
     need_link = (not os.path.exists(LIB)
                  or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs))
     if need_link:
