@@ -980,7 +980,7 @@ def main():
         e2e_solved += int(np.sum(res["status"] == int(SolverStatus.SOLVED)))
     h2d = 8 * (len(Pv) + len(qv) + len(Av) + len(bv))
     d2h = 8 * (s2.nx + 2 * s2.mz) + B * ctypes.sizeof(_lib.ClgpuInfo)
-    del s2
+    del s2, res, res_buf  # the result views hold the solver (and its staging) alive
     e2e_t, e2e_solved = aggregate_over_ranks(e2e_t, e2e_solved, dist, "cuda")
     e2e_val = e2e_solved / e2e_t
     # cold path for reference: Solver(...) setup from host CSC data + solve +
