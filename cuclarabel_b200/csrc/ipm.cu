@@ -1136,13 +1136,15 @@ static long long factor_op_count(const Prepared &p) {
 //  - split into kFactorWarps parts of about equal length at segment starts,
 //    each op's .w or'd with min(position in segment, kPosMax) << 16 and the
 //    last-of-segment bit, each part cut into chunk words;
-//  - then the level's pivots {j, sign, 0, 0} in kFactorWarps contiguous parts.
+//  - then the level's pivots (t = j, a = sign + 1) in kFactorWarps contiguous
+//    parts.
+// Each op is packed into 8 bytes (fop_pack).
 // The column ranges of L follow the node order, so sorting the level's nodes
 // and bucketing each column by q (counting sort) lists the groups in target
 // order without a comparison sort.  Returns false when the structure of
 // L(:,k) below j is not inside L(:,j) (not reached for a valid symbolic
 // factorisation) or a part's chunk count leaves its 16-bit field.
-static bool build_factor_ops(const Prepared &p, int4 *op, int *flcnt, std::vector<int> &chk,
+static bool build_factor_ops(const Prepared &p, uint2 *op, int *flcnt, std::vector<int> &chk,
                              std::array<int, kFactorWarps + 1> &woff, FactorOpScratch &sc) {
   constexpr int W = kFactorWarps;
   const int Ni = p.N;
@@ -1161,9 +1163,8 @@ static bool build_factor_ops(const Prepared &p, int4 *op, int *flcnt, std::vecto
     int n = 0;
     for (long long c = c0; c < c1; c += kChunk, ++n) {
       const int cn = (int)std::min<long long>(kChunk, c1 - c);
-      const int steps = pivot ? 0 : chunk_scan_steps<2>(cn, [&](int e) {
-        return (op[c + e].w >> 16) & kPosMax;
-      });
+      const int steps =
+          pivot ? 0 : chunk_scan_steps<2>(cn, [&](int e) { return fop_pos(op[c + e]); });
       sc.wch[w].push_back((int)(c | ((long long)steps << kStepShift) |
                                 ((long long)(cn - 1) << kCntShift) |
                                 (pivot ? (long long)1 << 31 : 0LL)));
@@ -1238,9 +1239,9 @@ static bool build_factor_ops(const Prepared &p, int4 *op, int *flcnt, std::vecto
       for (int g = sb[w]; g < sb[w + 1]; ++g) {
         const int s0 = segs[g], s1 = segs[g + 1];
         for (int t = s0; t < s1; ++t) {
-          int4 o4 = lev[t];
-          o4.w |= (std::min(t - s0, kPosMax) << 16) | ((t == s1 - 1 ? 1 : 0) << kLastBit);
-          op[nops++] = o4;
+          const int4 o4 = lev[t];
+          op[nops++] = fop_pack(o4.x, o4.y, o4.z, o4.w, std::min(t - s0, kPosMax),
+                                t == s1 - 1 ? 1 : 0);
         }
       }
       nop[w] = put_chunks(w, start, nops, false);
@@ -1250,7 +1251,7 @@ static bool build_factor_ops(const Prepared &p, int4 *op, int *flcnt, std::vecto
       const long long start = nops;
       for (int t = lp[l] + np * w / W; t < lp[l] + np * (w + 1) / W; ++t) {
         const int j = p.lvl_nodes[t];
-        op[nops++] = make_int4(j, (int)p.Dsign[j], 0, 0);
+        op[nops++] = fop_pack(j, (int)p.Dsign[j] + 1, 0, 0, 0, 0);
       }
       npv[w] = put_chunks(w, start, nops, true);
     }
@@ -1876,7 +1877,7 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   {
     constexpr long long kFactorSmemBytes = 96 * 1024;
     constexpr int W = kFactorWarps;
-    const long long ring_bytes = (long long)W * kFRingSlots * kChunk * 16;
+    const long long ring_bytes = (long long)W * kFRingSlots * kChunk * (long long)sizeof(uint2);
     std::vector<int> fs(B, 0);
     std::vector<long long> nch(B, 0);
     std::vector<std::vector<int>> ich(B);
@@ -1888,14 +1889,16 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
     std::vector<long long> ocnt(B, 0);
     par_for(B, nth, [&](int i) {
       const auto &p = prep[i];
-      if (cls[i] != 1 || (N[i] + (long long)p.Li.size()) * 8 + ring_bytes > kFactorSmemBytes)
+      // (the op words address at most kFopMaxPos work-vector positions)
+      if (cls[i] != 1 || (N[i] + (long long)p.Li.size()) * 8 + ring_bytes > kFactorSmemBytes ||
+          N[i] + (long long)p.Li.size() > kFopMaxPos)
         return;
       fs[i] = 1;
       ocnt[i] = factor_op_count(p);
     });
     const auto oop = prefix(ocnt);
     if (oop[B] > 2000000000LL) return -4;
-    hvec<int4> fop(std::max<long long>(oop[B], 1));
+    hvec<uint2> fop(std::max<long long>(oop[B], 1));
     par_for(B, nth, [&](int i) {
       thread_local FactorOpScratch sc;
       const auto &p = prep[i];

@@ -1040,8 +1040,8 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
   const int lbase = k.Lp[po], nl = k.Lp[po + N] - lbase;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   double *V = reinterpret_cast<double *>(sm_raw);
-  int4 *ring = reinterpret_cast<int4 *>(sm_raw + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15)) +
-               warp * kFRing * kChunk;
+  uint2 *ring = reinterpret_cast<uint2 *>(sm_raw + (((size_t)(N + nl) * 8 + 15) & ~(size_t)15)) +
+                warp * kFRing * kChunk;
   const signed char *sg = k.Dsign + vo;
   const int *Kdiag = k.Kdiag + vo;
   T *D = reinterpret_cast<T *>(k.D) + vo;
@@ -1092,7 +1092,7 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
   const int *wo = k.fwoff + (size_t)inst * (kFactorWarps + 1);
   const int *chunks = k.foch + wo[warp];
   const int nch = wo[warp + 1] - wo[warp];
-  const int4 *ops = k.fop + k.fop_base[inst];
+  const uint2 *ops = k.fop + k.fop_base[inst];
   const int *lc = k.flcnt + (size_t)k.lvl_off[inst] * kFactorWarps + warp;
   const int nlev = k.nlev[inst];
   bool finite = true;
@@ -1115,7 +1115,7 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
         if (e < cnt) {
           const unsigned dst =
               static_cast<unsigned>(__cvta_generic_to_shared(&ring[slot * kChunk + h * 32 + lane]));
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
                        "l"(&ops[p0 + e]));
         }
       }
@@ -1148,15 +1148,15 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
     const bool vA = eA < cnt, vB = eB < cnt;
     // entry 2 lane + h sits at h * 32 + lane: both reads contiguous across the warp
     static_assert(kChunk == 64, "two ring entries per lane");
-    const int4 oA = vA ? ring[slot * kChunk + lane] : make_int4(0, 0, 0, 0);
-    const int4 oB = vB ? ring[slot * kChunk + 32 + lane] : make_int4(0, 0, 0, 0);
+    const uint2 oA = vA ? ring[slot * kChunk + lane] : make_uint2(0u, 0u);
+    const uint2 oB = vB ? ring[slot * kChunk + 32 + lane] : make_uint2(0u, 0u);
     if (pivot) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int4 o = h ? oB : oA;
+        const uint2 o = h ? oB : oA;
         if (h ? vB : vA) {
-          const int j = o.x;
-          const double dj = pivot_value(V[j], (signed char)o.y, prm);
+          const int j = fop_t(o);
+          const double dj = pivot_value(V[j], (signed char)(fop_a(o) - 1), prm);
           const T djs = T(dj);
           const T dis = T(1.0 / double(djs));
           D[j] = djs;
@@ -1172,26 +1172,29 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
     } else {
       // each target is written once per level (by its last update), so its
       // old value is read before the scan, off the dependent chain
-      const bool wA = vA && ((oA.w >> kLastBit) & 1), wB = vB && ((oB.w >> kLastBit) & 1);
-      const A tA = wA ? A(V[oA.x]) : A(0), tB = wB ? A(V[oB.x]) : A(0);
+      const int tAi = fop_t(oA), tBi = fop_t(oB);
+      const bool wA = vA && fop_last(oA), wB = vB && fop_last(oB);
+      const A tA = wA ? A(V[tAi]) : A(0), tB = wB ? A(V[tBi]) : A(0);
       A xA, xB, sA, sB;
       if constexpr (F32) {
-        xA = vA ? __fmul_rn(__fmul_rn(float(V[oA.y]), float(V[oA.z])), float(V[oA.w & 0xffff]))
+        xA = vA ? __fmul_rn(__fmul_rn(float(V[fop_a(oA)]), float(V[fop_b(oA)])),
+                            float(V[fop_k(oA)]))
                 : 0.f;
-        xB = vB ? __fmul_rn(__fmul_rn(float(V[oB.y]), float(V[oB.z])), float(V[oB.w & 0xffff]))
+        xB = vB ? __fmul_rn(__fmul_rn(float(V[fop_a(oB)]), float(V[fop_b(oB)])),
+                            float(V[fop_k(oB)]))
                 : 0.f;
       } else {
-        xA = vA ? __dmul_rn(__dmul_rn(V[oA.y], V[oA.z]), V[oA.w & 0xffff]) : 0.0;
-        xB = vB ? __dmul_rn(__dmul_rn(V[oB.y], V[oB.z]), V[oB.w & 0xffff]) : 0.0;
+        xA = vA ? __dmul_rn(__dmul_rn(V[fop_a(oA)], V[fop_b(oA)]), V[fop_k(oA)]) : 0.0;
+        xB = vB ? __dmul_rn(__dmul_rn(V[fop_a(oB)], V[fop_b(oB)]), V[fop_k(oB)]) : 0.0;
       }
-      seg_scan2(xA, xB, (oA.w >> 16) & 63, (oB.w >> 16) & 63, lane, carry,
+      seg_scan2(xA, xB, fop_pos(oA), fop_pos(oB), lane, carry,
                 (int)((w >> kStepShift) & 7u), sA, sB);
       if constexpr (F32) {
-        if (wA) V[oA.x] = double(__fsub_rn(tA, sA));
-        if (wB) V[oB.x] = double(__fsub_rn(tB, sB));
+        if (wA) V[tAi] = double(__fsub_rn(tA, sA));
+        if (wB) V[tBi] = double(__fsub_rn(tB, sB));
       } else {
-        if (wA) V[oA.x] = __dsub_rn(tA, sA);
-        if (wB) V[oB.x] = __dsub_rn(tB, sB);
+        if (wA) V[tAi] = __dsub_rn(tA, sA);
+        if (wB) V[tBi] = __dsub_rn(tB, sB);
       }
       const int ll = (cnt - 1) >> 1;
       carry = __shfl_sync(full, ((cnt - 1) & 1) ? sB : sA, ll);
@@ -1247,11 +1250,11 @@ __global__ void __launch_bounds__(32 * kFactorWarps, 6)
   }
   const int bad = __syncthreads_or(finite ? 0 : 1);
   if (k.prof_bytes && lane == 0) {
-    // the op stream (16 B per entry) and chunk words of this warp; thread 0
+    // the op stream (8 B per entry) and chunk words of this warp; thread 0
     // adds the K diagonal and L-position values (8 + 4 B each), L written
     // three times with the stream indices read, D and D^-1 written
     const double ts = sizeof(T);
-    double by = 16.0 * nent + 4.0 * nch;
+    double by = 8.0 * nent + 4.0 * nch;
     if (tid == 0) by += 12.0 * N + 12.0 * nl + nl * (3.0 * ts + 16.0) + 2.0 * ts * N;
     atomicAdd(&k.prof_bytes[inst], by);
   }

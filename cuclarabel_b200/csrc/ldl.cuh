@@ -68,9 +68,10 @@ struct KKTDev {
   // and, once pivot j is final, 1/d_j in shared memory.  Per level of the
   // elimination tree the op stream lists, sorted by target, every update
   //     V[t] -= V[a] * V[b] * V[k]   (U(i,k) U(j,k) / d_k into U(i,j) or d_j)
-  // as int4 {t, a, b, k | position-in-segment << 16 | last << 22}, split into
-  // kFactorWarps parts at target boundaries (part w for warp w), followed by
-  // the level's pivots {j, sign, 0, 0}, also in kFactorWarps parts.
+  // as one 8-byte op word (fop_pack: t, a, b, k, position in segment, last),
+  // split into kFactorWarps parts at target boundaries (part w for warp w),
+  // followed by the level's pivots (t = j, a = sign + 1), also in
+  // kFactorWarps parts.
   // Indices address the shared array [d or 1/d (N) | U (nnz(L))].  Warp w of
   // instance i reads its chunk words foch[fwoff[(kFactorWarps+1) i + w] ..
   // fwoff[(kFactorWarps+1) i + w + 1]) (start relative to fop_base[i], pivot
@@ -81,7 +82,7 @@ struct KKTDev {
   // instances by decreasing shared-memory need (block b factors fs_inst[b]);
   // fs_smem bytes per block.
   const int *fstream, *fop_base, *foch, *fwoff, *flcnt, *Lkpos, *fs_inst;
-  const int4 *fop;
+  const uint2 *fop;
   int has_fstream, fs_count, fs_smem;
   // Packing of single-warp solves into blocks of kSolveWarps warps (first fit
   // by decreasing shared-memory need: the work vector y, N FP64 values, plus
@@ -147,13 +148,33 @@ constexpr int kSChunk = 32 * kSK;
 constexpr int kSPosMax = 127;
 constexpr int kSLastBit = 23;
 static_assert((1 << kSKShift) == kSK && kSPosMax + 1 >= kSChunk, "solve chunk layout");
-// Factorisation op streams: K = 2 entries per lane; op word .w = k |
-// min(position in segment, kPosMax) << 16 | last << kLastBit; count - 1 in
-// 6 bits; bit 31 marks a pivot chunk.
+// Factorisation op streams: K = 2 entries per lane; chunk words carry the
+// count - 1 in 6 bits; bit 31 marks a pivot chunk.
 constexpr int kChunk = 64;
 constexpr int kFactorWarps = 4;        // warps per streamed-factorisation block (one instance)
 constexpr int kPosMax = 63;
-constexpr int kLastBit = 22;
+// One op in 8 bytes: four 14-bit positions in the instance's shared work
+// vector (the streamed path holds at most 96 KB of it, 12288 FP64 values, so
+// every position is below 2^14), min(position in segment, kPosMax) in 6 bits
+// and the last-of-segment bit.  x: t | a << 14 | b << 28 (low 4 bits of b);
+// y: b >> 4 | k << 10 | pos << 24 | last << 30.
+constexpr int kFopBits = 14;
+constexpr int kFopMaxPos = 1 << kFopBits;
+__host__ __device__ __forceinline__ uint2 fop_pack(int t, int a, int b, int k, int pos,
+                                                   int last) {
+  uint2 w;
+  w.x = (unsigned)t | ((unsigned)a << 14) | ((unsigned)b << 28);
+  w.y = ((unsigned)b >> 4) | ((unsigned)k << 10) | ((unsigned)pos << 24) | ((unsigned)last << 30);
+  return w;
+}
+__host__ __device__ __forceinline__ int fop_t(uint2 w) { return (int)(w.x & 0x3fffu); }
+__host__ __device__ __forceinline__ int fop_a(uint2 w) { return (int)((w.x >> 14) & 0x3fffu); }
+__host__ __device__ __forceinline__ int fop_b(uint2 w) {
+  return (int)(((w.x >> 28) | (w.y << 4)) & 0x3fffu);
+}
+__host__ __device__ __forceinline__ int fop_k(uint2 w) { return (int)((w.y >> 10) & 0x3fffu); }
+__host__ __device__ __forceinline__ int fop_pos(uint2 w) { return (int)((w.y >> 24) & 63u); }
+__host__ __device__ __forceinline__ int fop_last(uint2 w) { return (int)((w.y >> 30) & 1u); }
 
 // Scan steps of a chunk of cnt entries, K per lane, whose segment positions
 // are pos(e) (clamped at or above the chunk length): lane l reaches back
