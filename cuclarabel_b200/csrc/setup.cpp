@@ -538,7 +538,41 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     Pu.p[j + 1] = (int)Pu.i.size();
   }
   out.p_nnz = Pu.p[n];
-  {
+  bool pu_sorted = true;  // every triu column strictly increasing
+  for (int j = 0; j < n && pu_sorted; ++j)
+    for (int k = Pu.p[j] + 1; k < Pu.p[j + 1]; ++k)
+      if (Pu.i[k] <= Pu.i[k - 1]) {
+        pu_sorted = false;
+        break;
+      }
+  if (pu_sorted) {
+    // full = triu + strict triu transposed, built in place: column j gets
+    // its own triu rows (<= j, ascending) when column j is visited, then the
+    // rows i > j from the later columns i, in increasing i -- sorted, as the
+    // general form's per-column sort leaves them
+    HostCSC &F = out.Pfull;
+    F.m = F.n = n;
+    F.p.assign(n + 1, 0);
+    for (int j = 0; j < n; ++j)
+      for (int k = Pu.p[j]; k < Pu.p[j + 1]; ++k) {
+        F.p[j + 1]++;
+        if (Pu.i[k] != j) F.p[Pu.i[k] + 1]++;
+      }
+    for (int j = 0; j < n; ++j) F.p[j + 1] += F.p[j];
+    F.i.resize(F.p[n]);
+    F.x.resize(F.p[n]);
+    std::vector<int> pos(F.p.begin(), F.p.end() - 1);
+    for (int j = 0; j < n; ++j)
+      for (int k = Pu.p[j]; k < Pu.p[j + 1]; ++k) {
+        const int i = Pu.i[k];
+        F.i[pos[j]] = i;
+        F.x[pos[j]++] = Pu.x[k];
+        if (i != j) {
+          F.i[pos[i]] = j;
+          F.x[pos[i]++] = Pu.x[k];
+        }
+      }
+  } else {
     // full = triu + strict triu transposed
     std::vector<std::vector<std::pair<int, double>>> cols(n);
     for (int j = 0; j < n; ++j)
