@@ -66,7 +66,10 @@ def build(verbose=False, ptxas_info=False):
         if verbose or ptxas_info:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
-    build_pack(verbose)
+    try:
+        build_pack(verbose)
+    except (OSError, subprocess.CalledProcessError) as e:  # no host compiler or headers:
+        print("packer not built (%s); batches pack in Python" % e, file=sys.stderr)
     need_link = (not os.path.exists(LIB)
                  or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs))
     if need_link:
