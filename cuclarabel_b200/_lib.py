@@ -86,6 +86,7 @@ EXPORTED = [
     "clgpu_ds_from_dz_offset", "clgpu_step_length", "clgpu_compute_barrier",
     "clgpu_margins", "clgpu_scaled_unit_shift", "clgpu_unit_initialization",
     "clgpu_debug_check_instance", "clgpu_debug_instance_path", "clgpu_debug_pinned_stats",
+    "clgpu_debug_factor_stream",
     "clgpu_margins_static",
     "clgpu_cones_set_profiling", "clgpu_cones_last_kernel_ms",
     "clgpu_cones_get_launch_shapes", "clgpu_cones_set_launch_shapes",
@@ -155,6 +156,8 @@ def _declare(L):
                                             ctypes.POINTER(ClgpuSettings), ip,
                                             ctypes.POINTER(ctypes.c_longlong)]
     L.clgpu_debug_pinned_stats.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
+    L.clgpu_debug_factor_stream.argtypes = [ctypes.POINTER(ClgpuProblem),
+                                            ctypes.POINTER(ClgpuSettings), dp]
     # KKT-level boundary (device pointers as integers)
     L.clgpu_mul_Hs_diag.argtypes = [c_void_p, V, V, c_void_p]
     L.clgpu_rectify_equilibration.argtypes = [c_void_p, V, V, ip, c_void_p]

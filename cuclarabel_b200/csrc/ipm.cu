@@ -2226,6 +2226,124 @@ static int build_batch(clgpu_solver *h, std::vector<Prepared> &prep, int nth) {
   return 0;
 }
 
+// Host replay of one instance's streamed-factorisation op stream (the
+// records, chunk words and level counts build_batch uploads) on a
+// quasi-definite matrix with the instance's KKT pattern, against a dense
+// LDL^T of the same permuted matrix.  The replay follows the kernel's
+// schedule: per level, every warp part's update chunks (a segment's sum is
+// subtracted from its target at the segment's last record, carried across
+// chunk boundaries), then every part's pivot chunks (V[j] becomes 1/d_j);
+// at the end L(i,j) = U(i,j) / d_j.  *resid receives the largest difference
+// of L and D entries relative to the largest |D|.  Returns 0, -2 when the
+// instance cannot be prepared, -3 when it does not take the streamed path,
+// -4 when it is too large for the dense reference (N > 2000), or a negative
+// structure code.
+extern "C" int clgpu_debug_factor_stream(const clgpu_problem *pb, const clgpu_settings *st,
+                                         double *resid) {
+  using namespace clgpu;
+  constexpr int W = kFactorWarps;
+  if (!pb) return -1;
+  SetupOptions opt;
+  if (st) {
+    opt.soc_threshold = st->soc_threshold;
+    opt.equilibrate_enable = st->equilibrate_enable;
+    opt.equilibrate_max_iter = st->equilibrate_max_iter;
+  }
+  Prepared p;
+  if (!prepare_instance(*pb, opt, p)) return -2;
+  const int N = p.N, nli = (int)p.Li.size();
+  if (p.supernodal || N + nli > kFopMaxPos) return -3;
+  if (N > 2000) return -4;
+  FactorOpScratch sc;
+  std::vector<int> Lkpos(nli);
+  l_kkt_positions(p, 0, Lkpos.data(), sc);
+  const int nl = (int)p.lvl_ptr.size() - 1;
+  std::vector<uint2> ops(factor_op_count(p));
+  std::vector<int> flcnt((size_t)nl * W), chk;
+  std::array<int, W + 1> woff;
+  if (!build_factor_ops(p, ops.data(), flcnt.data(), chk, woff, sc)) return -5;
+  // the quasi-definite test matrix of clgpu_debug_check_instance
+  const int knz = (int)p.Kj.size();
+  std::vector<double> Kx(knz, 0.0);
+  for (int r = 0; r < N; ++r)
+    for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) {
+      const int c = p.Kj[q];
+      if (c != r) Kx[q] = 0.01 * std::sin(1.0 + r + 7.0 * c) * std::sin(1.0 + c + 7.0 * r);
+    }
+  for (int r = 0; r < N; ++r) Kx[p.Kdiag[r]] = p.Dsign[r] * 2.0;
+  // replay
+  std::vector<double> V(N + nli, 0.0), D(N, 0.0);
+  for (int j = 0; j < N; ++j) V[j] = Kx[p.Kdiag[j]];
+  for (int q = 0; q < nli; ++q) V[N + q] = Lkpos[q] >= 0 ? Kx[Lkpos[q]] : 0.0;
+  int cur[W];
+  for (int w = 0; w < W; ++w) cur[w] = woff[w];
+  auto chunk = [&](int w, bool pivot_expected, double &acc) {
+    if (cur[w] >= woff[w + 1]) return -6;
+    const unsigned word = (unsigned)chk[cur[w]++];
+    const bool pivot = (word >> 31) != 0;
+    if (pivot != pivot_expected) return -7;
+    const int p0 = (int)(word & kStartMask), cnt = (int)((word >> kCntShift) & 63u) + 1;
+    if (p0 + cnt > (int)ops.size()) return -8;
+    for (int e = 0; e < cnt; ++e) {
+      const uint2 o = ops[p0 + e];
+      const int t = fop_t(o), a = fop_a(o);
+      if (t >= N + nli || a >= N + nli) return -9;
+      if (pivot) {
+        const int sgn = a - 1;
+        if (t >= N || (sgn != 1 && sgn != -1) || sgn != p.Dsign[t]) return -10;
+        D[t] = V[t];
+        V[t] = 1.0 / V[t];
+      } else {
+        const int b = fop_b(o), k = fop_k(o);
+        if (b >= N + nli || k >= N) return -11;
+        if (fop_pos(o) == 0) acc = 0.0;
+        acc += V[a] * V[b] * V[k];
+        if (fop_last(o)) V[t] -= acc;
+      }
+    }
+    return 0;
+  };
+  for (int l = 0; l < nl; ++l) {
+    for (int w = 0; w < W; ++w) {
+      double acc = 0.0;
+      const int nop = flcnt[(size_t)l * W + w] & 0xffff;
+      for (int c = 0; c < nop; ++c)
+        if (int rc = chunk(w, false, acc)) return rc;
+    }
+    for (int w = 0; w < W; ++w) {
+      double acc = 0.0;
+      const int npv = (flcnt[(size_t)l * W + w] >> 16) & 0xffff;
+      for (int c = 0; c < npv; ++c)
+        if (int rc = chunk(w, true, acc)) return rc;
+    }
+  }
+  for (int w = 0; w < W; ++w)
+    if (cur[w] != woff[w + 1]) return -12;  // every chunk replayed
+  // dense LDL^T of the same permuted matrix
+  std::vector<double> Ad((size_t)N * N, 0.0), Ld((size_t)N * N, 0.0), Dd(N, 0.0);
+  for (int r = 0; r < N; ++r)
+    for (int q = p.Kp[r]; q < p.Kp[r + 1]; ++q) Ad[(size_t)r * N + p.Kj[q]] = Kx[q];
+  for (int j = 0; j < N; ++j) {
+    double dj = Ad[(size_t)j * N + j];
+    for (int k = 0; k < j; ++k) dj -= Ld[(size_t)j * N + k] * Ld[(size_t)j * N + k] * Dd[k];
+    Dd[j] = dj;
+    for (int i = j + 1; i < N; ++i) {
+      double v = Ad[(size_t)i * N + j];
+      for (int k = 0; k < j; ++k) v -= Ld[(size_t)i * N + k] * Ld[(size_t)j * N + k] * Dd[k];
+      Ld[(size_t)i * N + j] = v / dj;
+    }
+  }
+  double dmax = 0.0, err = 0.0;
+  for (int j = 0; j < N; ++j) dmax = std::max(dmax, std::fabs(Dd[j]));
+  for (int j = 0; j < N; ++j) {
+    err = std::max(err, std::fabs(D[j] - Dd[j]));
+    for (int q = p.Lp[j]; q < p.Lp[j + 1]; ++q)
+      err = std::max(err, std::fabs(V[N + q] * V[j] - Ld[(size_t)p.Li[q] * N + j]));
+  }
+  if (resid) *resid = err / std::max(dmax, 1e-300);
+  return 0;
+}
+
 extern "C" int clgpu_solver_create(const clgpu_problem *probs, int nprob,
                                    const clgpu_settings *settings, clgpu_solver **out) {
   if (!probs || nprob < 1 || !out) return -1;

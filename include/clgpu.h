@@ -461,6 +461,16 @@ int clgpu_debug_check_instance(const clgpu_problem *prob,
  * factor's strictly-lower entries.  Needs no GPU. */
 int clgpu_debug_instance_path(const clgpu_problem *prob, const clgpu_settings *settings,
                               int *supernodal, long long *factor_entries);
+/* Host replay of one instance's streamed-factorisation op stream (the 8-byte
+ * records, chunk words and per-level counts that setup uploads for
+ * k_ldl_factor_stream) on a quasi-definite matrix with the instance's KKT
+ * pattern, compared with a dense LDL^T of the same permuted matrix
+ * (diagnostic, no reference counterpart): *resid = largest difference of
+ * the L and D entries relative to the largest |D|.  Returns 0, or -3 when
+ * the instance does not take the streamed path, -4 when N > 2000, other
+ * negative codes for structure errors.  Needs no GPU. */
+int clgpu_debug_factor_stream(const clgpu_problem *prob, const clgpu_settings *settings,
+                              double *resid);
 /* Counters of the process-wide page-locked host pool that setup arrays,
  * upload staging and result staging come from (diagnostic, no reference
  * counterpart): out[0] buffers served from the pool, out[1] page-locked

@@ -75,3 +75,31 @@ def test_factorisation_paths():
     assert _path(problems.psd_lp(36, 2, seed=0))[0] == 1
     assert _path(problems.psd_lp(40, 1, seed=0))[0] == 1
     assert _path(problems.mixed_socp(0.1))[0] == 1
+
+
+def replay(pb, **kw):
+    cp, keep, n, m = _prep_problem(*pb)
+    st = Settings(**kw).to_c()
+    r = ctypes.c_double()
+    rc = _lib.load().clgpu_debug_factor_stream(ctypes.byref(cp), ctypes.byref(st),
+                                               ctypes.byref(r))
+    return rc, r.value
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_factor_op_stream_replays_to_the_dense_factor(seed):
+    """The streamed factorisation's op stream (8-byte records: four 14-bit
+    work-vector positions, segment position, last bit), replayed on the host
+    in the kernel's schedule, gives the L and D of a dense LDL^T of the same
+    permuted matrix."""
+    rc, res = replay(problems.mpc_qp(seed))
+    assert rc == 0 and res < 1e-12, (rc, res)
+
+
+def test_factor_op_stream_other_families():
+    pbs = [problems.portfolio()]
+    for name, P, q, A, b, cones, e in golden_cases()[:6]:
+        pbs.append((P, q, A, b, to_cone_objects(cones)))
+    for pb in pbs:
+        rc, res = replay(pb)
+        assert rc == 0 and res < 1e-12, (rc, res)
