@@ -433,10 +433,15 @@ constexpr int kScalarMaxColumn = 512;
 // no self loops needed) under perm has more than `limit` entries below the
 // diagonal, or a column longer than kScalarMaxColumn; elimination-tree
 // path walk (Liu), stopping early
+// When it returns false, parent and cnt hold the elimination tree and the
+// column counts of L under perm (the symbolic factorisation reuses them).
 static bool scalar_fill_exceeds(int N, const std::vector<int> &xadj,
                                 const std::vector<int> &adj, const std::vector<int> &perm,
-                                long long limit) {
-  std::vector<int> iperm(N), parent(N, -1), mark(N, -1), cnt(N, 0);
+                                long long limit, std::vector<int> &parent,
+                                std::vector<int> &cnt) {
+  std::vector<int> iperm(N), mark(N, -1);
+  parent.assign(N, -1);
+  cnt.assign(N, 0);
   for (int k = 0; k < N; ++k) iperm[perm[k]] = k;
   long long lnz = 0;
   for (int k = 0; k < N; ++k) {
@@ -757,6 +762,7 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     }
   }
   // ---- ordering (graph of the off-diagonal pattern, CSR with repeats)
+  std::vector<int> etree, colcnt;  // from the fill check (scalar path)
   {
     std::vector<int> xadj(N + 1, 0);
     for (auto &en : ents)
@@ -778,7 +784,8 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     out.supernodal = (long long)N * 8 > 48 * 1024 || (long long)xadj[N] + N > kStreamMaxEntries;
     if (!out.supernodal) {
       out.perm = nd_order_csr(N, xadj, adjncy);
-      out.supernodal = scalar_fill_exceeds(N, xadj, adjncy, out.perm, kStreamMaxEntries);
+      out.supernodal = scalar_fill_exceeds(N, xadj, adjncy, out.perm, kStreamMaxEntries,
+                                           etree, colcnt);
     }
     if (out.supernodal) {
       if (!sn_analyse(N, xadj, adjncy, out.perm, out.sym, &out.error)) return false;
@@ -854,17 +861,26 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
     out.Rp.assign(N + 1, 0);
     out.lvl_ptr.assign(1, 0);
   } else {
-    std::vector<int> parent(N, -1), Lnz(N, 0), work(N, -1);
-    for (int k = 0; k < N; ++k) {
-      work[k] = k;
-      for (int p = out.Kp[k]; p < out.Kp[k + 1]; ++p) {
-        int i = out.Kj[p];
-        if (i >= k) break;
-        while (work[i] != k) {
-          if (parent[i] == -1) parent[i] = k;
-          Lnz[i]++;
-          work[i] = k;
-          i = parent[i];
+    // elimination tree and column counts: those of the fill check (the same
+    // pattern and ordering), else from the permuted matrix
+    std::vector<int> parent, Lnz, work(N, -1);
+    if ((int)etree.size() == N && (int)colcnt.size() == N) {
+      parent.swap(etree);
+      Lnz.swap(colcnt);
+    } else {
+      parent.assign(N, -1);
+      Lnz.assign(N, 0);
+      for (int k = 0; k < N; ++k) {
+        work[k] = k;
+        for (int p = out.Kp[k]; p < out.Kp[k + 1]; ++p) {
+          int i = out.Kj[p];
+          if (i >= k) break;
+          while (work[i] != k) {
+            if (parent[i] == -1) parent[i] = k;
+            Lnz[i]++;
+            work[i] = k;
+            i = parent[i];
+          }
         }
       }
     }
