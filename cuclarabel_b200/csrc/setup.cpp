@@ -941,27 +941,55 @@ bool prepare_instance(const clgpu_problem &pb, const SetupOptions &opt, Prepared
       auto it = std::lower_bound(beg, end, r);
       return (it != end && *it == r) ? (int)(it - F.i.begin()) : -1;
     };
-    for (int j = 0; j < n; ++j)
+    // KKT positions by row scatter: every lookup of a column j below is in
+    // KKT row iperm[j] (scattered into kcol, stamped by row), and the
+    // transposed entry's position comes from ktr: rows of the symmetric
+    // pattern are sorted, so walking the rows in order meets the entries
+    // (c, r) of each row c in increasing r (one cursor per row)
+    const int KN = (int)out.Kp.size() - 1, knz = (int)out.Kj.size();
+    std::vector<int> ktr(knz), kcur(out.Kp.begin(), out.Kp.end() - 1), kcol(KN, -1),
+        kstamp(KN, -1);
+    for (int r = 0; r < KN; ++r)
+      for (int q = out.Kp[r]; q < out.Kp[r + 1]; ++q) ktr[q] = kcur[out.Kj[q]]++;
+    auto scatter_row = [&](int lr) {  // row of local (unpermuted) index lr
+      const int a = out.iperm[lr];
+      for (int q = out.Kp[a]; q < out.Kp[a + 1]; ++q) {
+        kcol[out.Kj[q]] = q;
+        kstamp[out.Kj[q]] = a;
+      }
+      return a;
+    };
+    auto in_row = [&](int a, int lc) {  // position of (row a, local column lc), or -1
+      const int bb = out.iperm[lc];
+      return kstamp[bb] == a ? kcol[bb] : -1;
+    };
+    for (int j = 0; j < n; ++j) {
+      const int a = scatter_row(j);
       for (int k = pb.Pp[j]; k < pb.Pp[j + 1]; ++k) {
         const int i = pb.Pi[k];
         if (i > j) continue;
         if (k > pb.Pp[j] && pb.Pi[k - 1] >= i) out.updatable = false;  // repeats / unsorted
         out.pmap[4 * (size_t)k] = fpos(i, j);
         out.pmap[4 * (size_t)k + 1] = i != j ? fpos(j, i) : -1;
-        out.pmap[4 * (size_t)k + 2] = pos_of(i, j);
-        out.pmap[4 * (size_t)k + 3] = i != j ? pos_of(j, i) : -1;
+        const int pji = in_row(a, i);  // (j, i); its transpose is (i, j)
+        out.pmap[4 * (size_t)k + 2] = pji >= 0 ? ktr[pji] : -1;
+        out.pmap[4 * (size_t)k + 3] = i != j ? pji : -1;
         out.pxy[2 * (size_t)k] = i;
         out.pxy[2 * (size_t)k + 1] = j;
       }
+    }
     const int anz = A.p[n];
     out.amapk.assign(2 * (size_t)anz, -1);
-    for (int j = 0; j < n; ++j)
+    for (int j = 0; j < n; ++j) {
+      const int a = scatter_row(j);
       for (int k = A.p[j]; k < A.p[j + 1]; ++k) {
         if (k > A.p[j] && A.i[k - 1] >= A.i[k]) out.updatable = false;
         const int zr = n + local_of_user[A.i[k]];
-        out.amapk[2 * (size_t)k] = pos_of(j, zr);
-        out.amapk[2 * (size_t)k + 1] = pos_of(zr, j);
+        const int pjz = in_row(a, zr);
+        out.amapk[2 * (size_t)k] = pjz;
+        out.amapk[2 * (size_t)k + 1] = pjz >= 0 ? ktr[pjz] : -1;
       }
+    }
   }
   // ---- refresh positions
   for (size_t c = 0; c < out.ctype.size(); ++c) {
